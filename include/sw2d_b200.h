@@ -1,0 +1,190 @@
+/*
+ * sw2d_b200.h — C ABI of the B200 implementation of SW2D's single-porosity (SP) explicit
+ * finite-volume step.
+ *
+ * The reference exposes this path through C++ class seams, not a C ABI:
+ *   - the model interface swParent::init(swMesh*) / importAttributesFromSolverParam() /
+ *     execute()  (src/sw2dSolver/models/swParent.h:25-27), implemented for SP by
+ *     swSp::init (src/sw2dSolver/models/sp/swSp.cpp:720-969), importAttributesFromSolverParam
+ *     (swSp.cpp:685-717) and execute (swSp.cpp:482-670);
+ *   - the driver that builds and runs it, sw2dSolver's main (src/sw2dSolver/main.cpp:99-173).
+ * Each entry point below names the reference routine it replaces.  A binding for another
+ * host language sees plain pointers, sizes and int status codes only.
+ *
+ * Conventions (the reference's, restated):
+ *   - mesh arrays are in the reference numbering (cells, internal edges, boundary edges as
+ *     read from geometry.sw2d, src/common/geometry/swMesh.cpp:213-471); the library
+ *     renumbers internally and always returns per-cell data in the caller's numbering;
+ *   - per-cell contributions are summed in the reference's order (boundary edges by
+ *     increasing index, then internal edges by increasing index), so results do not
+ *     depend on the internal numbering;
+ *   - all arithmetic is IEEE binary64;
+ *   - status: 0 = success, < 0 = error (SW2D_E_*); the reference calls exit(1) instead
+ *     (src/common/swMessage.cpp:74-84).  sw2d_last_error() returns the message text;
+ *   - one CUDA stream per handle; calls on one handle are not thread-safe, calls on
+ *     different handles are.
+ */
+#ifndef SW2D_B200_H
+#define SW2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SW2D_ABI_VERSION 1
+
+/* status codes */
+#define SW2D_OK 0
+#define SW2D_E_ARG (-1)          /* invalid argument / inconsistent sizes                   */
+#define SW2D_E_CUDA (-2)         /* CUDA runtime error (message in sw2d_last_error)         */
+#define SW2D_E_NAN_FLUX (-3)     /* NaN mass flux: src/sw2dSolver/models/sp/swSpHyp.cpp:374-392 */
+#define SW2D_E_HLLC_CONFIG (-4)  /* impossible wet/dry configuration: swSpHyp.cpp:728-739     */
+#define SW2D_E_NEG_DEPTH (-5)    /* negative depth with detection active: swSpHyp.cpp:184-196 */
+#define SW2D_E_BC_TYPE (-6)      /* unknown boundary type: swSpHyp.cpp:116-120               */
+#define SW2D_E_BC_FR (-7)        /* 'fr' boundary value outside [0,1]: swSpHyp.cpp:57-62     */
+#define SW2D_E_UNSUPPORTED (-8)  /* option outside the implemented path                     */
+#define SW2D_E_NO_DEVICE (-9)    /* no usable CUDA device                                    */
+
+/* enumerations of the input.solv string keys (src/sw2dSolver/common/swSolverParam.h:130-153) */
+enum sw2d_scheme { SW2D_SCHEME_GODUNOV = 0, SW2D_SCHEME_MUSCL_EVR = 1 };
+enum sw2d_topo { SW2D_TOPO_DISCONTINUOUS = 0, SW2D_TOPO_BLENDING = 1 };
+enum sw2d_friction { SW2D_FRICTION_NONE = 0, SW2D_FRICTION_CHEZY = 1, SW2D_FRICTION_MANNING = 2,
+                     SW2D_FRICTION_STRICKLER = 3 };
+enum sw2d_bc_type { SW2D_BC_Q = 0, SW2D_BC_H = 1, SW2D_BC_Z = 2, SW2D_BC_FR = 3 };
+enum sw2d_variant { SW2D_VARIANT_NATIVE = 0, SW2D_VARIANT_ENZYME_E = 1 };
+
+/* Mesh tables, as swParent::setMeshTables builds them (src/sw2dSolver/models/swParent.cpp:391-501).
+ * Normals of internal edges point from the L cell to the R cell; normals of boundary edges
+ * point into the domain (swEdgeIntern.cpp:97-112, swEdgeBoundary.cpp:98-112). */
+typedef struct sw2d_mesh {
+    int64_t cell_nb;
+    int64_t edge_int_nb;
+    int64_t edge_bnd_nb;
+    const double* cell_area;       /* [cell_nb] */
+    const double* cell_x;          /* [cell_nb] centroid */
+    const double* cell_y;          /* [cell_nb] */
+    const double* cell_z_b;        /* [cell_nb] bottom level */
+    const int64_t* edge_int_cells; /* [2*edge_int_nb] (L, R) pairs */
+    const double* edge_int_length; /* [edge_int_nb] */
+    const double* edge_int_nx;
+    const double* edge_int_ny;
+    const double* edge_int_mx;     /* midpoint */
+    const double* edge_int_my;
+    const int64_t* edge_bnd_cell;  /* [edge_bnd_nb] */
+    const double* edge_bnd_length;
+    const double* edge_bnd_nx;
+    const double* edge_bnd_ny;
+    const int32_t* edge_bnd_bc;    /* [edge_bnd_nb] index into the boundary table (0..bc_nb-1) */
+} sw2d_mesh;
+
+/* The input.solv keys this path reads (swSp::importAttributesFromSolverParam, swSp.cpp:685-717;
+ * defaults in src/sw2dSolver/common/swSolverParam.h:144-194). */
+typedef struct sw2d_params {
+    int32_t scheme;                   /* enum sw2d_scheme   (num_scheme)                 */
+    int32_t topo;                     /* enum sw2d_topo     (topo_discretization)        */
+    int32_t friction;                 /* enum sw2d_friction (model_friction)             */
+    int32_t singular_head_loss;       /* 0 none, 1 active   (model_singular_head_loss)   */
+    int32_t negative_depth_detection; /* 0 none, 1 active                                 */
+    int32_t variant;                  /* enum sw2d_variant; only NATIVE is implemented    */
+    double cfl_max;
+    double dt_max;
+    double dt_map;
+    double h_min;
+    double phi_min;
+    double v_max;
+    double fr_max;
+    double t_0;
+    double t_max;
+} sw2d_params;
+
+/* Per-cell model parameters (swSp::setPorosityParameter, setBoussinesqParameter,
+ * setFrictionParameters, setSingularHeadLossParameters: swSp.cpp:997-1072,1250-1273,1330-1360).
+ * Angles are in degrees, as in the map files.  Arrays not needed by the chosen options may be NULL. */
+typedef struct sw2d_cell_fields {
+    const double* phi;            /* [cell_nb] porosity                                   */
+    const double* boussinesq;     /* [cell_nb]                                            */
+    const double* friction_1;     /* [cell_nb] coefficient, 1st principal direction       */
+    const double* friction_2;     /* [cell_nb] coefficient, 2nd principal direction       */
+    const double* friction_alpha; /* [cell_nb] degrees                                    */
+    const double* hl_h_sing;      /* [cell_nb] singular head loss threshold depth         */
+    const double* hl_coeff_1;
+    const double* hl_coeff_2;
+    const double* hl_alpha;       /* degrees */
+} sw2d_cell_fields;
+
+/* Boundary time series (swBoundaryConditionTimeSeries, models/common/swBoundaryConditionTimeSeries.cpp:17-96).
+ * Series k has type[k] and records times[offset[k] .. offset[k+1]), values[...] alike. */
+typedef struct sw2d_bc_table {
+    int32_t bc_nb;
+    const int32_t* type;     /* [bc_nb] enum sw2d_bc_type */
+    const int64_t* offset;   /* [bc_nb+1] */
+    const double* times;
+    const double* values;
+} sw2d_bc_table;
+
+typedef struct sw2d_handle sw2d_handle;
+
+/* Replaces swParent::create + importAttributesFromSolverParam + swSp::init
+ * (swParent.cpp:125-173, swSp.cpp:685-969): validates, renumbers, uploads, computes the
+ * edge factors (swSp::computeEdgeFactors, swSp.cpp:338-444) and sets t = t_0.
+ * `device` is the CUDA ordinal. */
+int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                const sw2d_bc_table* bc, const double* h0, const double* q0, const double* r0,
+                int device, sw2d_handle** out);
+
+/* Advances at most n_steps passes of the body of swSp::execute's time loop
+ * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),
+ * stopping once t >= t_max.  The loop runs on the device (CUDA graph); the host does not
+ * synchronise between steps.  *steps_done receives the number of steps taken (may be NULL). */
+int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done);
+
+/* Replaces swSp::execute (swSp.cpp:482-670) without result storage: runs until t >= t_max. */
+int sw2d_execute(sw2d_handle* h, int64_t* steps_done);
+
+/* State access (swSp members water_depth, unit_discharge_x/_y, swSp.h:170-180), host buffers
+ * of cell_nb doubles in the caller's numbering.  The copies are synchronous. */
+int sw2d_get_state(sw2d_handle* h, double* water_depth, double* unit_discharge_x, double* unit_discharge_y);
+int sw2d_set_state(sw2d_handle* h, const double* water_depth, const double* unit_discharge_x,
+                   const double* unit_discharge_y);
+
+/* Same, on device buffers (caller's numbering) already on the handle's device, ordered on
+ * the handle's stream. */
+int sw2d_get_state_device(sw2d_handle* h, double* d_water_depth, double* d_unit_discharge_x,
+                          double* d_unit_discharge_y);
+int sw2d_set_state_device(sw2d_handle* h, const double* d_water_depth, const double* d_unit_discharge_x,
+                          const double* d_unit_discharge_y);
+
+/* Simulation time t and the last time step dt (swSp members t, dt, swSp.h:154-156). */
+int sw2d_get_time(sw2d_handle* h, double* t, double* dt);
+int sw2d_set_time(sw2d_handle* h, double t, double dt);
+
+/* Per-edge intermediate arrays of the last step, in the caller's edge numbering, for
+ * kernel-level checks: name is one of "F1_int","F2_int","F3_int","s2L_int","s2R_int",
+ * "F1_bnd","F2_bnd","F3_bnd","s2R_bnd","lambda_max_int","lambda_max_bnd",
+ * "slope_x","slope_y" (per cell).  Returns the element count written, or < 0. */
+int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity);
+
+/* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
+int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
+
+/* CUDA stream of the handle (cudaStream_t), for callers that order their own work on it. */
+void* sw2d_get_stream(sw2d_handle* h);
+
+/* Launches of this library's kernels per time step (for the bench's launch count). */
+int sw2d_kernels_per_step(sw2d_handle* h);
+
+int sw2d_destroy(sw2d_handle* h);
+
+/* Text of the last error on this handle (or of the last failed sw2d_create when h is NULL). */
+const char* sw2d_last_error(sw2d_handle* h);
+
+int sw2d_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SW2D_B200_H */

@@ -1,0 +1,13 @@
+"""sw2d_b200: SW2D's single-porosity explicit finite-volume step on the NVIDIA B200.
+
+Modules:
+  case       -- SW2D case folders (geometry.sw2d v2, maps, boundary series, input.solv)
+  mesh       -- synthetic triangle meshes with the reference's geometry conventions
+  workloads  -- seeded synthetic cases (dam break, Gaussian bumps, feature channel)
+  capi       -- ctypes view of include/sw2d_b200.h and the CUDA library loader
+  solver     -- SpModel, the host-side mirror of the reference's swSp interface
+"""
+from . import case, mesh, workloads, capi  # noqa: F401
+from .case import Case, read_case, write_case  # noqa: F401
+
+__all__ = ["case", "mesh", "workloads", "capi", "Case", "read_case", "write_case"]

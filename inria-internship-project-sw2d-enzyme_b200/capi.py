@@ -1,0 +1,193 @@
+"""ctypes view of the C ABI in include/sw2d_b200.h and the loader of the CUDA library.
+
+``native_inputs(case)`` turns a :class:`Case` into the C structures (keeping the numpy arrays
+alive); ``load_library()`` loads ``libsw2d_b200.so`` built in-tree and fails loudly when it is
+missing: there is no CPU fallback for the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import List
+
+import numpy as np
+
+from .case import BC_TYPES, Case
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libsw2d_b200.so")
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int64_p = ctypes.POINTER(ctypes.c_int64)
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+
+SCHEMES = {"godunov": 0, "muscl_evr": 1}
+TOPOS = {"discontinuous": 0, "blending": 1}
+FRICTIONS = {"none": 0, "chezy": 1, "manning": 2, "strickler": 3}
+
+
+class Sw2dMesh(ctypes.Structure):
+    _fields_ = [("cell_nb", ctypes.c_int64), ("edge_int_nb", ctypes.c_int64), ("edge_bnd_nb", ctypes.c_int64),
+                ("cell_area", c_double_p), ("cell_x", c_double_p), ("cell_y", c_double_p),
+                ("cell_z_b", c_double_p), ("edge_int_cells", c_int64_p), ("edge_int_length", c_double_p),
+                ("edge_int_nx", c_double_p), ("edge_int_ny", c_double_p), ("edge_int_mx", c_double_p),
+                ("edge_int_my", c_double_p), ("edge_bnd_cell", c_int64_p), ("edge_bnd_length", c_double_p),
+                ("edge_bnd_nx", c_double_p), ("edge_bnd_ny", c_double_p), ("edge_bnd_bc", c_int32_p)]
+
+
+class Sw2dParams(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int32), ("topo", ctypes.c_int32), ("friction", ctypes.c_int32),
+                ("singular_head_loss", ctypes.c_int32), ("negative_depth_detection", ctypes.c_int32),
+                ("variant", ctypes.c_int32), ("cfl_max", ctypes.c_double), ("dt_max", ctypes.c_double),
+                ("dt_map", ctypes.c_double), ("h_min", ctypes.c_double), ("phi_min", ctypes.c_double),
+                ("v_max", ctypes.c_double), ("fr_max", ctypes.c_double), ("t_0", ctypes.c_double),
+                ("t_max", ctypes.c_double)]
+
+
+class Sw2dCellFields(ctypes.Structure):
+    _fields_ = [("phi", c_double_p), ("boussinesq", c_double_p), ("friction_1", c_double_p),
+                ("friction_2", c_double_p), ("friction_alpha", c_double_p), ("hl_h_sing", c_double_p),
+                ("hl_coeff_1", c_double_p), ("hl_coeff_2", c_double_p), ("hl_alpha", c_double_p)]
+
+
+class Sw2dBcTable(ctypes.Structure):
+    _fields_ = [("bc_nb", ctypes.c_int32), ("type", c_int32_p), ("offset", c_int64_p), ("times", c_double_p),
+                ("values", c_double_p)]
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(c_double_p)
+
+
+@dataclass
+class NativeInputs:
+    mesh: Sw2dMesh
+    params: Sw2dParams
+    fields: Sw2dCellFields
+    bc: Sw2dBcTable
+    h0: np.ndarray
+    q0: np.ndarray
+    r0: np.ndarray
+    keep: List[np.ndarray]
+
+
+def params_from_opts(opts) -> Sw2dParams:
+    """input.solv keys -> sw2d_params (defaults of swSolverParam.h:144-194)."""
+    def f(k, d):
+        return float(opts.get(k, d))
+    scheme = str(opts.get("num_scheme", "godunov")).lower()
+    topo = str(opts.get("topo_discretization", "discontinuous")).lower()
+    fric = str(opts.get("model_friction", "none")).lower()
+    if scheme not in SCHEMES:
+        raise ValueError(f"num_scheme {scheme!r} not implemented")
+    if topo not in TOPOS:
+        raise ValueError(f"topo_discretization {topo!r} not recognised")
+    if fric not in FRICTIONS:
+        raise ValueError(f"model_friction {fric!r} not handled")
+    if str(opts.get("div_corr", "none")).lower() != "none":
+        raise ValueError("div_corr other than 'none' is outside the implemented path")
+    return Sw2dParams(
+        scheme=SCHEMES[scheme], topo=TOPOS[topo], friction=FRICTIONS[fric],
+        singular_head_loss=int(str(opts.get("model_singular_head_loss", "none")).lower() != "none"),
+        negative_depth_detection=int(str(opts.get("negative_depth_detection", "none")).lower() == "active"),
+        variant=0, cfl_max=f("cfl_max", 1.0), dt_max=f("dt_max", 10.0), dt_map=f("dt_map", 100.0),
+        h_min=f("h_min", 1e-5), phi_min=f("phi_min", 1e-16), v_max=f("v_max", 100.0), fr_max=f("fr_max", 100.0),
+        t_0=f("t_0", 0.0), t_max=f("t_max", 100.0))
+
+
+def native_inputs(case: Case) -> NativeInputs:
+    m = case.mesh
+    keep: List[np.ndarray] = []
+
+    def d(a):
+        arr = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(arr)
+        return _dp(arr)
+
+    cells = np.ascontiguousarray(m.edge_int_cells, dtype=np.int64).reshape(-1)
+    bcell = np.ascontiguousarray(m.edge_bnd_cell, dtype=np.int64)
+    series_codes = list(case.bc.codes)
+    try:
+        bc_index = np.array([series_codes.index(int(c)) for c in m.edge_bnd_code], dtype=np.int32)
+    except ValueError as exc:
+        raise ValueError("a boundary code of the mesh has no time series") from exc
+    keep += [cells, bcell, bc_index]
+    mesh = Sw2dMesh(m.cell_nb, m.edge_int_nb, m.edge_bnd_nb, d(m.cell_area), d(m.cell_x), d(m.cell_y),
+                    d(m.cell_z_b), cells.ctypes.data_as(c_int64_p), d(m.edge_int_length), d(m.edge_int_nx),
+                    d(m.edge_int_ny), d(m.edge_int_mx), d(m.edge_int_my), bcell.ctypes.data_as(c_int64_p),
+                    d(m.edge_bnd_length), d(m.edge_bnd_nx), d(m.edge_bnd_ny), bc_index.ctypes.data_as(c_int32_p))
+    params = params_from_opts(case.opts)
+    null = c_double_p()
+    fr = case.friction
+    hl = case.head_loss
+    fields = Sw2dCellFields(d(case.phi), d(case.boussinesq),
+                            d(fr[0]) if fr is not None else null, d(fr[1]) if fr is not None else null,
+                            d(fr[2]) if fr is not None else null,
+                            d(hl[0]) if hl is not None else null, d(hl[1]) if hl is not None else null,
+                            d(hl[2]) if hl is not None else null, d(hl[3]) if hl is not None else null)
+    ns = len(series_codes)
+    types = np.array([BC_TYPES.get(t.lower(), 99) for t in case.bc.types], dtype=np.int32)
+    nrec = case.bc.times.shape[0]
+    offset = np.arange(ns + 1, dtype=np.int64) * nrec
+    times = np.tile(np.asarray(case.bc.times, dtype=np.float64), ns)
+    values = np.ascontiguousarray(np.asarray(case.bc.values, dtype=np.float64).reshape(-1))
+    keep += [types, offset, times, values]
+    bc = Sw2dBcTable(ns, types.ctypes.data_as(c_int32_p), offset.ctypes.data_as(c_int64_p), _dp(times), _dp(values))
+    h0 = np.ascontiguousarray(case.h0, dtype=np.float64)
+    q0 = np.ascontiguousarray(case.q0, dtype=np.float64)
+    r0 = np.ascontiguousarray(case.r0, dtype=np.float64)
+    return NativeInputs(mesh, params, fields, bc, h0, q0, r0, keep)
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the CUDA library (fails loudly when it was not built: no CPU fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with __graft_entry__.build() (nvcc, sm_100a)")
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    lib.sw2d_create.argtypes = [ctypes.POINTER(Sw2dMesh), ctypes.POINTER(Sw2dParams), ctypes.POINTER(Sw2dCellFields),
+                                ctypes.POINTER(Sw2dBcTable), c_double_p, c_double_p, c_double_p, ctypes.c_int,
+                                ctypes.POINTER(P)]
+    lib.sw2d_create.restype = ctypes.c_int
+    lib.sw2d_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
+    lib.sw2d_step_n.restype = ctypes.c_int
+    lib.sw2d_execute.argtypes = [P, c_int64_p]
+    lib.sw2d_execute.restype = ctypes.c_int
+    for name in ("sw2d_get_state", "sw2d_set_state", "sw2d_get_state_device", "sw2d_set_state_device"):
+        fn = getattr(lib, name)
+        fn.argtypes = [P, P, P, P]
+        fn.restype = ctypes.c_int
+    lib.sw2d_get_time.argtypes = [P, c_double_p, c_double_p]
+    lib.sw2d_get_time.restype = ctypes.c_int
+    lib.sw2d_set_time.argtypes = [P, ctypes.c_double, ctypes.c_double]
+    lib.sw2d_set_time.restype = ctypes.c_int
+    lib.sw2d_get_array.argtypes = [P, ctypes.c_char_p, c_double_p, ctypes.c_int64]
+    lib.sw2d_get_array.restype = ctypes.c_int64
+    lib.sw2d_get_cell_permutation.argtypes = [P, c_int64_p]
+    lib.sw2d_get_cell_permutation.restype = ctypes.c_int
+    lib.sw2d_get_stream.argtypes = [P]
+    lib.sw2d_get_stream.restype = P
+    lib.sw2d_kernels_per_step.argtypes = [P]
+    lib.sw2d_kernels_per_step.restype = ctypes.c_int
+    lib.sw2d_destroy.argtypes = [P]
+    lib.sw2d_destroy.restype = ctypes.c_int
+    lib.sw2d_last_error.argtypes = [P]
+    lib.sw2d_last_error.restype = ctypes.c_char_p
+    lib.sw2d_abi_version.argtypes = []
+    lib.sw2d_abi_version.restype = ctypes.c_int
+    _LIB = lib
+    return lib
+
+
+# every symbol include/sw2d_b200.h declares (checked by the CPU test suite)
+EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+            "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
+            "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
+            "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version"]

@@ -1,0 +1,158 @@
+"""Seeded synthetic SP cases with the shapes of the benchmark configurations.
+
+The reference ships no benchmark suite; these constructions stand in for it:
+
+* ``dam_break``: plain SP dam break in a 100 m x 20 m channel (jittered Delaunay-like
+  triangles, seed 1), flat bed, h = 1.0 m for x < 50 and 0.1 m elsewhere, u = v = 0,
+  porosity U[0.6, 1.0] per cell (seed 2), Manning n = 0.03, MUSCL-EVR + the reference's
+  slope limiter + HLLC (discontinuous topography), CFL 0.9, reflective walls (q = 0);
+* ``gaussian_bumps``: 2 km x 2 km, bed = sum of 50 Gaussian bumps (A ~ U[0,3] m,
+  sigma ~ U[20,200] m, seed 3) + 1e-3 x, h = max(0, 2 - z_b) (wet/dry fronts), porosity a
+  smoothed random field in [0.3, 1] (seed 4), Manning n lognormal (median 0.03, sigma 0.3,
+  seed 5), MUSCL-EVR + HLLC, walls;
+* ``channel_features``: a small case exercising every other branch of the path (blending
+  topography, Strickler or Chezy friction, singular head loss, 'q' inflow and 'fr'/'h'/'z'
+  outflow time series).
+"""
+from __future__ import annotations
+
+import math
+from typing import Dict, Optional
+
+import numpy as np
+
+from .case import BoundarySeries, Case
+from .mesh import jittered_triangle_mesh
+
+
+def _grid_for(n_cells: int, aspect: float):
+    """nx, ny with 2*nx*ny ~ n_cells and nx/ny ~ aspect."""
+    ny = max(2, int(round(math.sqrt(n_cells / (2.0 * aspect)))))
+    nx = max(2, int(round(n_cells / (2.0 * ny))))
+    return nx, ny
+
+
+def _wall_series(codes):
+    # two records: with a single record the reference's cursor interpolation
+    # (swBoundaryConditionTimeSeries.cpp:81-95) divides 0 by 0 when t equals that record's time
+    return BoundarySeries(codes=list(codes), types=["q"] * len(codes), times=np.array([0.0, 1.0e9]),
+                          values=np.zeros((len(codes), 2)))
+
+
+def dam_break(n_cells: int = 20000, scheme: str = "muscl_evr", friction: str = "manning",
+              t_max: float = 1.0e6, seed_mesh: int = 1, seed_phi: int = 2) -> Case:
+    nx, ny = _grid_for(n_cells, 5.0)
+    mesh = jittered_triangle_mesh(nx, ny, 100.0, 20.0, seed=seed_mesh)
+    n = mesh.cell_nb
+    h0 = np.where(mesh.cell_x < 50.0, 1.0, 0.1)
+    rng = np.random.default_rng(seed_phi)
+    phi = rng.uniform(0.6, 1.0, size=n)
+    opts = {"model_hyperb": "sp", "model_friction": friction, "num_scheme": scheme,
+            "topo_discretization": "discontinuous", "cfl_max": 0.9, "dt_max": 10.0, "dt_map": 100.0,
+            "h_min": 1e-5, "t_max": t_max, "store_flag": "none", "output_format": "txt"}
+    fr = None
+    if friction != "none":
+        fr = np.stack([np.full(n, 0.03 if friction == "manning" else 33.3), np.full(n, 0.03 if friction == "manning" else 33.3),
+                       np.zeros(n)])
+    return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
+                boussinesq=np.ones(n), friction=fr, bc=_wall_series(mesh.bc_codes()),
+                extra={"name": "dam_break", "nx": nx, "ny": ny})
+
+
+def _smooth_field(x, y, lx, ly, seed, coarse=24):
+    """Bilinear interpolation of a seeded coarse random grid: a smooth field in [0, 1]."""
+    rng = np.random.default_rng(seed)
+    g = rng.uniform(0.0, 1.0, size=(coarse + 1, coarse + 1))
+    fx = np.clip(x / lx * coarse, 0, coarse - 1e-9)
+    fy = np.clip(y / ly * coarse, 0, coarse - 1e-9)
+    i = fx.astype(np.int64)
+    j = fy.astype(np.int64)
+    tx = fx - i
+    ty = fy - j
+    v = (g[j, i] * (1 - tx) * (1 - ty) + g[j, i + 1] * tx * (1 - ty) + g[j + 1, i] * (1 - tx) * ty +
+         g[j + 1, i + 1] * tx * ty)
+    lo, hi = v.min(), v.max()
+    return (v - lo) / (hi - lo) if hi > lo else np.zeros_like(v)
+
+
+def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: float = 1.0e6,
+                   seed_mesh: int = 1, seed_bed: int = 3, seed_phi: int = 4, seed_n: int = 5) -> Case:
+    L = 2000.0
+    rng = np.random.default_rng(seed_bed)
+    amp = rng.uniform(0.0, 3.0, 50)
+    sig = rng.uniform(20.0, 200.0, 50)
+    bx = rng.uniform(0.0, L, 50)
+    by = rng.uniform(0.0, L, 50)
+
+    def bed(x, y):
+        z = 1e-3 * x
+        for k in range(50):
+            z = z + amp[k] * np.exp(-((x - bx[k]) ** 2 + (y - by[k]) ** 2) / (2 * sig[k] ** 2))
+        return z
+
+    nx, ny = _grid_for(n_cells, 1.0)
+    mesh = jittered_triangle_mesh(nx, ny, L, L, seed=seed_mesh, z_fn=bed)
+    n = mesh.cell_nb
+    h0 = np.maximum(0.0, 2.0 - mesh.cell_z_b)
+    phi = 0.3 + 0.7 * _smooth_field(mesh.cell_x, mesh.cell_y, L, L, seed_phi)
+    rng_n = np.random.default_rng(seed_n)
+    man = np.exp(np.log(0.03) + 0.3 * rng_n.standard_normal(n))
+    opts = {"model_hyperb": "sp", "model_friction": "manning", "num_scheme": scheme,
+            "topo_discretization": "discontinuous", "cfl_max": 0.9, "dt_max": 10.0, "dt_map": 100.0,
+            "h_min": 1e-5, "t_max": t_max, "store_flag": "none", "output_format": "txt"}
+    return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
+                boussinesq=np.ones(n), friction=np.stack([man, man, np.zeros(n)]),
+                bc=_wall_series(mesh.bc_codes()), extra={"name": "gaussian_bumps", "nx": nx, "ny": ny})
+
+
+def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "blending",
+                     friction: str = "strickler", outflow: str = "fr", head_loss: bool = True,
+                     boussinesq: float = 1.0, t_max: float = 40.0, seed: int = 7,
+                     impervious: bool = False) -> Case:
+    """Sloped 60 m x 12 m channel with bumps, an inflow hydrograph on the left ('q', code -2),
+    an outflow condition on the right (code -3) and walls elsewhere (code -1)."""
+    rng = np.random.default_rng(seed)
+    lx, ly = 60.0, 12.0
+
+    def bed(x, y):
+        return 0.5 - 0.005 * x + 0.25 * np.exp(-((x - 35.0) ** 2 + (y - 6.0) ** 2) / 8.0)
+
+    def codes(mx, my):
+        c = np.full(mx.shape, -1, dtype=np.int32)
+        c[mx < 1e-9] = -2
+        c[mx > lx - 1e-9] = -3
+        return c
+
+    nx, ny = _grid_for(n_cells, 5.0)
+    mesh = jittered_triangle_mesh(nx, ny, lx, ly, seed=seed, z_fn=bed, bc_code_fn=codes)
+    n = mesh.cell_nb
+    h0 = np.maximum(0.0, 0.45 - mesh.cell_z_b)     # partly dry bed
+    phi = rng.uniform(0.5, 1.0, size=n)
+    if impervious:
+        # phi = 0 next to a dry cell is the configuration the reference rejects as
+        # impossible (swSpHyp.cpp:728-739); used by the error-path tests
+        phi[rng.uniform(size=n) < 0.02] = 0.0
+    opts: Dict[str, object] = {"model_hyperb": "sp", "model_friction": friction, "num_scheme": scheme,
+                               "topo_discretization": topo, "cfl_max": 0.8, "dt_max": 0.1, "dt_map": 1.0,
+                               "h_min": 1e-5, "t_max": t_max, "fr_max": 10.0, "store_flag": "none",
+                               "output_format": "txt"}
+    if head_loss:
+        opts["model_singular_head_loss"] = "active"
+    fr = None
+    if friction != "none":
+        k = {"strickler": 40.0, "manning": 0.025, "chezy": 30.0}[friction]
+        fr = np.stack([k * rng.uniform(0.8, 1.2, n), k * rng.uniform(0.8, 1.2, n), rng.uniform(0.0, 90.0, n)])
+    hl = None
+    if head_loss:
+        hl = np.stack([np.full(n, 0.05), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 45.0, n)])
+    times = np.array([0.0, 5.0, 10.0, 20.0, 30.0, 40.0])
+    inflow = np.array([0.0, 0.2, 0.5, 0.5, 0.3, 0.3])
+    out_val = {"fr": np.full(6, 0.6), "h": np.full(6, 0.15), "z": np.full(6, 0.35), "q": np.full(6, -0.1)}[outflow]
+    mesh_codes = mesh.bc_codes()
+    series_codes = [-1, -2, -3]
+    assert set(mesh_codes) <= set(series_codes)
+    bc = BoundarySeries(codes=series_codes, types=["q", "q", outflow], times=times,
+                        values=np.stack([np.zeros(6), inflow, out_val]))
+    return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
+                boussinesq=np.full(n, boussinesq), friction=fr, head_loss=hl, bc=bc,
+                extra={"name": "channel_features", "nx": nx, "ny": ny})

@@ -1,0 +1,177 @@
+"""ctypes bindings of the two CPU checkers (TEST INFRASTRUCTURE, never the product path).
+
+* :class:`SpOracle` — the plain-C restatement ``sp_oracle.c`` (built into ``_build/``);
+* :class:`RefSolver` — the reference's own native solver compiled from its sources with
+  ``ref_driver.cpp`` (``_ref/libsw2d_ref.so``), run on a case folder.
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libsp_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libsw2d_ref.so")
+REF_BIN = os.path.join(HERE, "_ref", "sw2dSolver")
+REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "/root/reference")
+
+_pkg = importlib.import_module("inria-internship-project-sw2d-enzyme_b200")
+capi = _pkg.capi
+
+
+def build(reference: bool = True) -> None:
+    """Compiles the C restatement and, when the reference sources are present, the reference."""
+    targets = ["oracle"]
+    if reference and os.path.isdir(os.path.join(REFERENCE_SRC, "src")):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-j8", f"REF={REFERENCE_SRC}"] + targets, cwd=HERE, check=True)
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+_P = ctypes.c_void_p
+_D = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+def _oracle_lib():
+    if not os.path.exists(ORACLE_SO):
+        build(reference=False)
+    lib = ctypes.CDLL(ORACLE_SO)
+    lib.spo_create.argtypes = [ctypes.POINTER(capi.Sw2dMesh), ctypes.POINTER(capi.Sw2dParams),
+                               ctypes.POINTER(capi.Sw2dCellFields), ctypes.POINTER(capi.Sw2dBcTable),
+                               capi.c_double_p, capi.c_double_p, capi.c_double_p]
+    lib.spo_create.restype = _P
+    lib.spo_step.argtypes = [_P, ctypes.c_int]
+    lib.spo_step.restype = ctypes.c_int
+    lib.spo_get_state.argtypes = [_P, _D, _D, _D]
+    lib.spo_set_state.argtypes = [_P, _D, _D, _D]
+    lib.spo_time.argtypes = [_P]
+    lib.spo_time.restype = ctypes.c_double
+    lib.spo_dt.argtypes = [_P]
+    lib.spo_dt.restype = ctypes.c_double
+    lib.spo_set_time.argtypes = [_P, ctypes.c_double, ctypes.c_double]
+    lib.spo_get_array.argtypes = [_P, ctypes.c_char_p, _D]
+    lib.spo_get_array.restype = ctypes.c_long
+    lib.spo_destroy.argtypes = [_P]
+    return lib
+
+
+class SpOracle:
+    """The C restatement of the native SP step on a :class:`Case`."""
+
+    def __init__(self, case):
+        self.lib = _oracle_lib()
+        self.case = case
+        self.n = case.mesh.cell_nb
+        self._in = capi.native_inputs(case)
+        i = self._in
+        self.h = self.lib.spo_create(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
+                                     ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0), capi._dp(i.r0))
+
+    def step(self, n: int) -> int:
+        k = self.lib.spo_step(self.h, int(n))
+        if k < 0:
+            raise RuntimeError(f"oracle step failed with status {k}")
+        return k
+
+    def state(self):
+        h, q, r = (np.empty(self.n) for _ in range(3))
+        self.lib.spo_get_state(self.h, h, q, r)
+        return h, q, r
+
+    def set_state(self, h, q, r):
+        self.lib.spo_set_state(self.h, *(np.ascontiguousarray(a, dtype=np.float64) for a in (h, q, r)))
+
+    @property
+    def t(self) -> float:
+        return self.lib.spo_time(self.h)
+
+    @property
+    def dt(self) -> float:
+        return self.lib.spo_dt(self.h)
+
+    def array(self, name: str) -> np.ndarray:
+        m = self.case.mesh
+        out = np.empty(max(m.cell_nb, m.edge_int_nb, m.edge_bnd_nb, 1))
+        k = self.lib.spo_get_array(self.h, name.encode(), out)
+        if k < 0:
+            raise KeyError(name)
+        return out[:k].copy()
+
+    def __del__(self):
+        try:
+            self.lib.spo_destroy(self.h)
+        except Exception:
+            pass
+
+
+class RefSolver:
+    """The reference's native SP solver (built from its own sources) on a case folder."""
+
+    def __init__(self, folder: str, quiet: bool = True):
+        if not os.path.exists(REF_SO):
+            raise RuntimeError("reference library not built (oracle/_ref/libsw2d_ref.so)")
+        lib = ctypes.CDLL(REF_SO)
+        lib.sw2dref_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        lib.sw2dref_open.restype = _P
+        lib.sw2dref_step.argtypes = [_P, ctypes.c_int]
+        lib.sw2dref_step.restype = ctypes.c_int
+        lib.sw2dref_run.argtypes = [_P]
+        for f in ("sw2dref_time", "sw2dref_dt", "sw2dref_t_max"):
+            getattr(lib, f).argtypes = [_P]
+            getattr(lib, f).restype = ctypes.c_double
+        for f in ("sw2dref_cell_nb", "sw2dref_edge_int_nb", "sw2dref_edge_bnd_nb"):
+            getattr(lib, f).argtypes = [_P]
+            getattr(lib, f).restype = ctypes.c_long
+        lib.sw2dref_get_state.argtypes = [_P, _D, _D, _D]
+        lib.sw2dref_set_state.argtypes = [_P, _D, _D, _D]
+        lib.sw2dref_get_array.argtypes = [_P, ctypes.c_char_p, _D]
+        lib.sw2dref_get_array.restype = ctypes.c_int
+        lib.sw2dref_slopes.argtypes = [_P, _D, _D]
+        self.lib = lib
+        self.h = lib.sw2dref_open(folder.encode(), 1 if quiet else 0)
+        if not self.h:
+            raise RuntimeError(f"reference failed to open {folder}")
+        self.n = lib.sw2dref_cell_nb(self.h)
+        self.ni = lib.sw2dref_edge_int_nb(self.h)
+        self.nb = lib.sw2dref_edge_bnd_nb(self.h)
+
+    def step(self, n: int) -> int:
+        return self.lib.sw2dref_step(self.h, int(n))
+
+    def run(self) -> int:
+        return self.lib.sw2dref_run(self.h)
+
+    def state(self):
+        h, q, r = (np.empty(self.n) for _ in range(3))
+        self.lib.sw2dref_get_state(self.h, h, q, r)
+        return h, q, r
+
+    def set_state(self, h, q, r):
+        self.lib.sw2dref_set_state(self.h, *(np.ascontiguousarray(a, dtype=np.float64) for a in (h, q, r)))
+
+    @property
+    def t(self) -> float:
+        return self.lib.sw2dref_time(self.h)
+
+    @property
+    def dt(self) -> float:
+        return self.lib.sw2dref_dt(self.h)
+
+    def array(self, name: str) -> np.ndarray:
+        out = np.empty(max(self.n, self.ni, self.nb, 1))
+        k = self.lib.sw2dref_get_array(self.h, name.encode(), out)
+        if k < 0:
+            raise KeyError(name)
+        return out[:k].copy()
+
+    def slopes(self):
+        sx, sy = np.empty(self.n), np.empty(self.n)
+        self.lib.sw2dref_slopes(self.h, sx, sy)
+        return sx, sy

@@ -1,0 +1,220 @@
+// Test harness around the reference's own native SP solver (compiled from the reference
+// sources by oracle/Makefile).  It is a checker, never part of the product.
+//
+// The reference only runs a whole simulation (`swSp::execute`, src/sw2dSolver/models/sp/swSp.cpp:482-670).
+// This subclass reaches the protected members the same way the reference's own assimilation
+// layer does (assim/swSpE.h:50 subclasses swSp) and re-states the body of the time loop
+// (swSp.cpp:522-589) without the result storage, so that a test can advance the reference N
+// steps and read its state, fluxes and Riemann states at full precision.
+//
+// C entry points (ctypes):
+//   sw2dref_open(folder, quiet)        init exactly as src/sw2dSolver/main.cpp:99-163 does
+//   sw2dref_step(handle, n)            n passes of the loop body; stops when t >= t_max
+//   sw2dref_run(handle)                the reference's own execute() (whole loop, with storage)
+//   sw2dref_get/set_state, sw2dref_get_array, sw2dref_time, sw2dref_dt, sizes
+
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../common/swFile.h"
+#include "../common/swIO.h"
+#include "../common/swLog.h"
+#include "../common/swMessage.h"
+#include "../common/geometry/swMesh.h"
+#include "common/swSolverParam.h"
+#include "models/sp/swSp.h"
+
+namespace {
+
+class RefSp : public swSp
+{
+public:
+    // One pass of the body of swSp::execute's time loop (sp/swSp.cpp:522-589), storage left out.
+    bool stepOnce()
+    {
+        if (!(t < t_max)) return false;
+        computeBC(t);
+        hypCompute(div_corr_option, n_it_div_max, num_scheme, dt);
+        if (model_momentum_diffusion != "none") parabComputeExplicit();
+        if (model_friction != "none") sourceFriction(model_friction, dt);
+        if (model_singular_head_loss != "none") sourceSingularHeadLoss(dt);
+        if (model_runoff != "none")
+        {
+            if (model_porosity_rainfall == "everywhere") sourceRunoffEverywhere();
+            else if (model_porosity_rainfall == "water_only") sourceRunoffWateronly();
+        }
+        if (model_infiltration != "none") sourceInfiltration();
+        if (model_wind != "none") sourceWind();
+        correctVelocity();
+        t += dt;
+        return true;
+    }
+
+    void beginTime() { t = t_0; }
+
+    // Limited free-surface slopes exactly as the MUSCL-EVR reconstruction computes them
+    // (sp/swSpHypMusclEvr.cpp:126-139), for kernel-level checks.
+    void slopes(double* sx, double* sy)
+    {
+        std::vector<double> z_cell(cell_nb), dzx(cell_nb), dzy(cell_nb);
+        for (size_t i = 0; i < cell_nb; i++) z_cell[i] = water_depth[i] + cell_z_b[i];
+        computeMusclSlopes(cell_centre_x, cell_centre_y, cell_neigh_cell_idx,
+                           edge_int_midpoint_x, edge_int_midpoint_y,
+                           edge_int_celL_idx, edge_int_celR_idx, z_cell, dzx, dzy);
+        std::memcpy(sx, dzx.data(), cell_nb * sizeof(double));
+        std::memcpy(sy, dzy.data(), cell_nb * sizeof(double));
+    }
+
+    int getArray(const std::string& name, double* out)
+    {
+        auto put = [&](const std::vector<double>& v) { std::memcpy(out, v.data(), v.size() * sizeof(double)); return (int)v.size(); };
+        auto put2 = [&](const std::vector<std::array<double, 2>>& v, int side) {
+            for (size_t i = 0; i < v.size(); i++) out[i] = v[i][side];
+            return (int)v.size();
+        };
+        if (name == "h") return put(water_depth);
+        if (name == "q") return put(unit_discharge_x);
+        if (name == "r") return put(unit_discharge_y);
+        if (name == "F1_int") return put(F1_int);
+        if (name == "F2_int") return put(F2_int);
+        if (name == "F3_int") return put(F3_int);
+        if (name == "s2L_int") return put(s2L_int);
+        if (name == "s2R_int") return put(s2R_int);
+        if (name == "F1_bnd") return put(F1_bnd);
+        if (name == "F2_bnd") return put(F2_bnd);
+        if (name == "F3_bnd") return put(F3_bnd);
+        if (name == "s2R_bnd") return put(s2R_bnd);
+        if (name == "lambda_max_int") return put(lambda_max_int);
+        if (name == "lambda_max_bnd") return put(lambda_max_bnd);
+        if (name == "z_riemann_L") return put2(z_riemann_int, 0);
+        if (name == "z_riemann_R") return put2(z_riemann_int, 1);
+        if (name == "q_riemann_L") return put2(q_riemann_int, 0);
+        if (name == "q_riemann_R") return put2(q_riemann_int, 1);
+        if (name == "r_riemann_L") return put2(r_riemann_int, 0);
+        if (name == "r_riemann_R") return put2(r_riemann_int, 1);
+        if (name == "lambda_minus_L") return put2(lambda_minus_int, 0);
+        if (name == "lambda_minus_R") return put2(lambda_minus_int, 1);
+        if (name == "lambda_plus_L") return put2(lambda_plus_int, 0);
+        if (name == "lambda_plus_R") return put2(lambda_plus_int, 1);
+        if (name == "phi") return put(phi);
+        if (name == "area") return put(cell_area);
+        if (name == "z_b") return put(cell_z_b);
+        if (name == "cx") return put(cell_centre_x);
+        if (name == "cy") return put(cell_centre_y);
+        return -1;
+    }
+
+    void setState(const double* h, const double* q, const double* r)
+    {
+        std::memcpy(water_depth.data(), h, cell_nb * sizeof(double));
+        std::memcpy(unit_discharge_x.data(), q, cell_nb * sizeof(double));
+        std::memcpy(unit_discharge_y.data(), r, cell_nb * sizeof(double));
+    }
+
+    size_t nCells() const { return cell_nb; }
+    size_t nInt() const { return edge_int_nb; }
+    size_t nBnd() const { return edge_bnd_nb; }
+    double time() const { return t; }
+    double timeStep() const { return dt; }
+    double tMax() const { return t_max; }
+};
+
+struct Handle
+{
+    swIO* io = nullptr;
+    RefSp* model = nullptr;
+    std::ofstream* log = nullptr;
+};
+
+struct QuietErr
+{
+    std::streambuf* saved = nullptr;
+    std::ostringstream sink;
+    explicit QuietErr(bool on) { if (on) saved = std::cerr.rdbuf(sink.rdbuf()); }
+    ~QuietErr() { if (saved) std::cerr.rdbuf(saved); }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Mirrors src/sw2dSolver/main.cpp:76-163 for an SP case (model_hyperb sp).
+void* sw2dref_open(const char* folder, int quiet)
+{
+    QuietErr q(quiet != 0);
+    Handle* hd = new Handle();
+    hd->io = new swIO(folder);
+    hd->io->createEmptyFolders(swFile::log_solver_file);
+    hd->log = new std::ofstream(hd->io->absolutePath(swFile::log_solver_file));
+    swMessage::outfile = hd->log;
+    swSolverParam* param = new swSolverParam(hd->io);
+    if (param->readParameters() != EXIT_SUCCESS) return nullptr;
+    if (param->getModelHyp() != "sp") return nullptr;
+    swMesh* mesh = new swMesh(hd->io);
+    if (mesh->build() != EXIT_SUCCESS) return nullptr;
+    if (param->getHotstart() == false) hd->io->createEmptyOutputFolder(true);
+    hd->model = new RefSp();
+    hd->model->setIOPointer(hd->io);
+    hd->model->importAttributesFromSolverParam(param);
+    if (hd->model->init(mesh) != EXIT_SUCCESS) return nullptr;
+    delete param;
+    delete mesh;
+    hd->model->beginTime();
+    return hd;
+}
+
+int sw2dref_step(void* h, int n)
+{
+    QuietErr q(true);
+    Handle* hd = static_cast<Handle*>(h);
+    int done = 0;
+    for (int i = 0; i < n; i++)
+    {
+        if (!hd->model->stepOnce()) break;
+        done++;
+    }
+    return done;
+}
+
+int sw2dref_run(void* h)
+{
+    QuietErr q(true);
+    Handle* hd = static_cast<Handle*>(h);
+    return hd->model->execute() == EXIT_SUCCESS ? 0 : 1;
+}
+
+double sw2dref_time(void* h) { return static_cast<Handle*>(h)->model->time(); }
+double sw2dref_dt(void* h) { return static_cast<Handle*>(h)->model->timeStep(); }
+double sw2dref_t_max(void* h) { return static_cast<Handle*>(h)->model->tMax(); }
+long sw2dref_cell_nb(void* h) { return (long)static_cast<Handle*>(h)->model->nCells(); }
+long sw2dref_edge_int_nb(void* h) { return (long)static_cast<Handle*>(h)->model->nInt(); }
+long sw2dref_edge_bnd_nb(void* h) { return (long)static_cast<Handle*>(h)->model->nBnd(); }
+
+void sw2dref_get_state(void* h, double* hh, double* q, double* r)
+{
+    RefSp* m = static_cast<Handle*>(h)->model;
+    m->getArray("h", hh);
+    m->getArray("q", q);
+    m->getArray("r", r);
+}
+
+void sw2dref_set_state(void* h, const double* hh, const double* q, const double* r)
+{
+    static_cast<Handle*>(h)->model->setState(hh, q, r);
+}
+
+int sw2dref_get_array(void* h, const char* name, double* out)
+{
+    return static_cast<Handle*>(h)->model->getArray(name, out);
+}
+
+void sw2dref_slopes(void* h, double* sx, double* sy)
+{
+    static_cast<Handle*>(h)->model->slopes(sx, sy);
+}
+
+}  // extern "C"
