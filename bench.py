@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the SW2D single-porosity MUSCL-EVR/HLLC step on B200.
+
+Workload: the large SP forward solve: a 4M-cell jittered triangle mesh over 2 km x 2 km, bed
+= 50 seeded Gaussian bumps + 1e-3 slope, h = max(0, 2 - z_b) (wet/dry fronts), porosity a
+seeded smooth field in [0.3, 1], Manning n lognormal (median 0.03, sigma 0.3), walls, FP64,
+MUSCL-EVR + the reference's slope limiter + HLLC.  A "step" is one explicit time step over all
+cells (the body of the reference's time loop).  Synthetic data, seeded.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (launched with torchrun, one rank per GPU) every rank runs its own replica of the
+workload (the step does not shard across GPUs in this build): value = all ranks' cell updates
+/ max-over-ranks device time, scaling "weak".
+
+The reference arm (--impl reference) times the reference's own native solver, compiled from
+its sources (oracle/_ref), on the host cores: one independent replica per core on a bounded
+sample of the same workload (same construction at 250k cells).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import multiprocessing as mp
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "inria-internship-project-sw2d-enzyme_b200"
+
+METRIC = "MUSCL-HLLC cell-updates/s"
+UNIT = "cell-updates/s"
+ALGO_BYTES_PER_CELL_UPDATE = 188   # FP64 MUSCL step: state r/w 48 + cell statics 56 + edge statics 72 + CSR 12
+CPU_SAMPLE_CELLS = 250_000
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cells", type=int, default=4_000_000)
+    ap.add_argument("--e2e-chunk", type=int, default=50, help="time steps per state upload/download in e2e")
+    ap.add_argument("--cpu-steps", type=int, default=150, help="timed steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--phase-steps", type=int, default=20)
+    return ap.parse_args()
+
+
+def _config(args, world):
+    return {"workload": f"SP gaussian-bumps forward solve, {args.cells} cells (2 km x 2 km), MUSCL-EVR + HLLC, "
+                        "Manning, FP64", "cells": args.cells, "scheme": "muscl_evr", "friction": "manning",
+            "global_cells": args.cells * world, "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "inputs larger than L2 (state + mesh tables ~0.9 GB per replica)"}
+
+
+# ------------------------------------------------------------------------------------------
+# reference solver on the host (CPU baseline and reference arm)
+# ------------------------------------------------------------------------------------------
+def _ref_worker(folder, warmup, steps, barrier, out):
+    from oracle.binding import RefSolver
+    ref = RefSolver(folder)
+    ref.step(warmup)
+    barrier.wait()
+    t0 = time.perf_counter()
+    done = ref.step(steps)
+    t1 = time.perf_counter()
+    out.put((done, t1 - t0, ref.n))
+
+
+def reference_timing(n_procs: int, warmup: int, steps: int, cells: int = CPU_SAMPLE_CELLS):
+    """Runs n_procs independent replicas of the reference on the sample (spawned processes)."""
+    pkg = importlib.import_module(PKG)
+    case = pkg.workloads.gaussian_bumps(n_cells=cells)
+    tmp = tempfile.mkdtemp(prefix="sw2d_ref_")
+    try:
+        folders = []
+        for i in range(n_procs):
+            f = os.path.join(tmp, f"r{i}")
+            if i == 0:
+                pkg.write_case(f, case)
+            else:
+                shutil.copytree(os.path.join(tmp, "r0", "input"), os.path.join(f, "input"))
+            folders.append(f)
+        ctx = mp.get_context("spawn")
+        barrier = ctx.Barrier(n_procs)
+        out = ctx.Queue()
+        procs = [ctx.Process(target=_ref_worker, args=(f, warmup, steps, barrier, out)) for f in folders]
+        for p in procs:
+            p.start()
+        res = [out.get() for _ in procs]
+        for p in procs:
+            p.join()
+        done = min(r[0] for r in res)
+        wall = max(r[1] for r in res)
+        n = res[0][2]
+        return {"value": n_procs * n * done / wall, "cells": n, "steps": done, "seconds": wall}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def _cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle.binding import reference_available
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": _config(args, world)}
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference solver library oracle/_ref not built"}))
+        return
+    cores = os.cpu_count() or 1
+    r = reference_timing(cores, args.warmup, args.steps)
+    sample = (f"same construction at {r['cells']} cells, {r['steps']} MUSCL steps per replica, "
+              f"{cores} independent single-threaded replicas (one per host core; the reference is serial), {_cpu_model()}")
+    base.update({"value": r["value"], "ms_per_step": 1e3 * r["seconds"] / max(r["steps"], 1),
+                 "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": cores, "kind": "reference",
+                                  "sample": sample},
+                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(base))
+
+
+# ------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.proc = None
+        self.dev = device_index
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        rows = []
+        for ln in open(self.path):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+def _measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_per_step():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except ValueError:
+            return None
+    return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # before any GPU call; spawned processes
+        from oracle.binding import reference_available
+        if reference_available():
+            r = reference_timing(1, 3, args.cpu_steps)
+            cpu = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference native solver (oracle/_ref), same construction at {r['cells']} cells, "
+                             f"{r['steps']} MUSCL steps, 1 thread ({_cpu_model()}); "
+                             f"{r['seconds']:.1f} s of CPU time"}
+
+    import torch
+
+    pkg = importlib.import_module(PKG)
+    pkg.build.build()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    case = pkg.workloads.gaussian_bumps(n_cells=args.cells)
+    model = pkg.SpModel(case, device=local_rank)
+    stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
+    n = case.mesh.cell_nb
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (also builds the CUDA graph)
+    model.step(args.warmup)
+    phases = model.phase_times(args.phase_steps)
+
+    # ---- timed region: K graph-captured steps with inputs resident in HBM
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        done = model.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if done != args.steps:
+        raise RuntimeError(f"only {done} of {args.steps} steps ran (t_max reached?)")
+    t_max_rank = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(t_max_rank, op=dist.ReduceOp.MAX)
+    ms = float(t_max_rank.item())
+
+    # ---- e2e: the C ABI with host buffers, state uploaded and read back every chunk of steps
+    chunk = max(1, min(args.e2e_chunk, args.steps))
+    n_chunks = max(1, args.steps // chunk)
+    hb = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    model.lib.sw2d_get_state(model.handle, *(t.data_ptr() for t in hb))
+    lib = model.lib
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    import ctypes
+    k = ctypes.c_int64(0)
+    for _ in range(n_chunks):
+        if lib.sw2d_set_state(model.handle, *(t.data_ptr() for t in hb)) != 0:
+            raise RuntimeError(lib.sw2d_last_error(model.handle).decode())
+        if lib.sw2d_step_n(model.handle, chunk, ctypes.byref(k)) != 0 or k.value != chunk:
+            raise RuntimeError("e2e step failed")
+        if lib.sw2d_get_state(model.handle, *(t.data_ptr() for t in hb)) != 0:
+            raise RuntimeError(lib.sw2d_last_error(model.handle).decode())
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms.item())
+    h_final = hb[0].numpy()
+    if not np.all(np.isfinite(h_final)):
+        raise RuntimeError("non-finite depth")
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    steps = args.steps
+    value = n * steps * world / (ms / 1e3)
+    e2e_steps = n_chunks * chunk
+    e2e_value = n * e2e_steps * world / (e2e_ms / 1e3)
+    peak, peak_kind = _measured_peak()
+    step_ms = ms / steps
+    algo_bytes = ALGO_BYTES_PER_CELL_UPDATE * n
+    achieved = algo_bytes / (step_ms / 1e3) / 1e9
+    traffic = _traffic_per_step()
+    kps = model.kernels_per_step
+    tot_phase = sum(phases.values())
+    kernels = {k2: {"ms": v, "share": v / tot_phase if tot_phase > 0 else None} for k2, v in phases.items()}
+    dominant = max(phases, key=phases.get)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian-bump bed, smooth porosity field, lognormal Manning n)",
+        "config": _config(args, world),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * n / chunk,
+                "d2h_bytes_per_step": (3 * 8 * n + 2 * 48) / chunk,
+                "note": f"sw2d_set_state + sw2d_step_n({chunk}) + sw2d_get_state from pinned host buffers per chunk"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind,
+                     "traffic": (traffic.get("bytes_per_cell_update") * n if traffic else None),
+                     "scope": f"whole step ({kps} kernels); algorithmic bytes {ALGO_BYTES_PER_CELL_UPDATE} B per "
+                              f"cell-update x {n} cells per step / device time per step in the timed region",
+                     "dominant_kernel": dominant, "kernels": kernels},
+        "gpu_launches": steps * kps,
+        "clocks": clk.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+
+
+def main():
+    args = _args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -167,6 +167,15 @@ int sw2d_set_time(sw2d_handle* h, double t, double dt);
  * "slope_x","slope_y" (per cell).  Returns the element count written, or < 0. */
 int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity);
 
+/* Device time of each phase of the step, averaged over n_steps steps that this call runs
+ * (they advance the simulation).  The analogue of the reference's per-phase clock() totals
+ * (LRStates / TimeStep / Fluxes / Balance + sources, swSp.cpp:491-501,645-667): the phases are
+ * the kernels "k_slopes", "k_edges", "k_cfl", "k_update" (sw2d_phase_name).  Launches each
+ * kernel separately with CUDA events on the handle's stream.  Returns the number of phases
+ * written to ms (milliseconds), or < 0. */
+int sw2d_phase_times(sw2d_handle* h, int64_t n_steps, double* ms, int capacity);
+const char* sw2d_phase_name(int i);
+
 /* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
 int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
 

@@ -7,7 +7,8 @@ Modules:
   capi       -- ctypes view of include/sw2d_b200.h and the CUDA library loader
   solver     -- SpModel, the host-side mirror of the reference's swSp interface
 """
-from . import case, mesh, workloads, capi  # noqa: F401
+from . import build, case, mesh, workloads, capi, solver  # noqa: F401
 from .case import Case, read_case, write_case  # noqa: F401
+from .solver import SpModel, Sw2dError  # noqa: F401
 
-__all__ = ["case", "mesh", "workloads", "capi", "Case", "read_case", "write_case"]
+__all__ = ["case", "mesh", "workloads", "capi", "solver", "Case", "read_case", "write_case", "SpModel", "Sw2dError"]

@@ -1,0 +1,68 @@
+"""Builds the CUDA library ``lib/libsw2d_b200.so`` in-tree with nvcc for sm_100a.
+
+``-fmad=false`` keeps every multiply and add separately rounded, as the reference's host
+build does (g++ on x86-64 without FMA), which is what makes the FP64 results bit-identical.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+SOURCES = ["sw2d_sp.cu"]
+HEADERS = ["sp_math.cuh"]
+OUT = os.path.join(LIBDIR, "libsw2d_b200.so")
+
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
+              "-Xcompiler", "-fPIC,-O2", "-shared", "-Xptxas", "-v"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _host_compiler():
+    # the system g++ links libstdc++ dynamically, which a library loaded by Python needs
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else None
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(OUT):
+        return False
+    t = os.path.getmtime(OUT)
+    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
+    deps.append(os.path.join(HERE, "..", "include", "sw2d_b200.h"))
+    deps.append(__file__)
+    return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
+        return OUT
+    os.makedirs(LIBDIR, exist_ok=True)
+    cmd = [_nvcc()] + NVCC_FLAGS
+    hc = _host_compiler()
+    if hc:
+        cmd += ["-ccbin", hc]
+    cmd += ["-o", OUT + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed")
+    if verbose:
+        sys.stderr.write(res.stderr)
+    os.replace(OUT + ".tmp", OUT)
+    with open(os.path.join(LIBDIR, "ptxas.log"), "w") as fh:
+        fh.write(res.stderr)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -180,6 +180,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_destroy.restype = ctypes.c_int
     lib.sw2d_last_error.argtypes = [P]
     lib.sw2d_last_error.restype = ctypes.c_char_p
+    lib.sw2d_phase_times.argtypes = [P, ctypes.c_int64, c_double_p, ctypes.c_int]
+    lib.sw2d_phase_times.restype = ctypes.c_int
+    lib.sw2d_phase_name.argtypes = [ctypes.c_int]
+    lib.sw2d_phase_name.restype = ctypes.c_char_p
     lib.sw2d_abi_version.argtypes = []
     lib.sw2d_abi_version.restype = ctypes.c_int
     _LIB = lib
@@ -190,4 +194,4 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
-            "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version"]
+            "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name"]

@@ -443,9 +443,15 @@ def write_case(folder: str, case: Case) -> None:
     n = case.mesh.cell_nb
     write_geometry(os.path.join(inp, "geometry.sw2d"), case.mesh)
     write_solv(os.path.join(inp, "input.solv"), case.opts)
-    write_map(os.path.join(inp, "initial_conditions_map.txt"), ["h", "q", "r"], [case.h0, case.q0, case.r0], n)
+    ic_z = case.extra.get("ic_z") if case.extra else None
+    if ic_z is not None and not np.any(case.q0) and not np.any(case.r0):
+        # uniform free surface at rest: "z u v" (swSp::setInitialConditions sets h = max(z - z_b, 0))
+        write_map(os.path.join(inp, "initial_conditions_map.txt"), ["z", "u", "v"], [float(ic_z), 0.0, 0.0], n)
+    else:
+        write_map(os.path.join(inp, "initial_conditions_map.txt"), ["h", "q", "r"],
+                  [_collapse(case.h0), _collapse(case.q0), _collapse(case.r0)], n)
     write_map(os.path.join(inp, "SP_cell_porosity_map.txt"), ["SpPhiW"], [case.phi], n)
-    write_map(os.path.join(inp, "Boussinesq_map.txt"), ["Beta"], [case.boussinesq], n)
+    write_map(os.path.join(inp, "Boussinesq_map.txt"), ["Beta"], [_collapse(case.boussinesq)], n)
     fm = case.opts.get("model_friction", "none")
     if fm != "none":
         f = case.friction

@@ -1,0 +1,151 @@
+"""SpModel: the host-side mirror of the reference's SP model interface over the C ABI.
+
+The reference drives a model through ``swParent::create`` / ``importAttributesFromSolverParam``
+/ ``init(mesh)`` / ``execute()`` (src/sw2dSolver/models/swParent.h:19-27, called from
+src/sw2dSolver/main.cpp:138-173).  ``SpModel`` keeps those names and meanings:
+
+* ``SpModel.from_folder(folder)`` / ``SpModel(case)`` — read the case and ``init`` (upload,
+  renumber, edge factors, t = t_0);
+* ``execute()`` — run until t >= t_max (no result storage), returns the number of steps;
+* ``step(n)`` — at most n passes of the time-loop body;
+* ``state()``, ``set_state()``, ``t``, ``dt``, ``array(name)``.
+
+Where the reference calls ``exit(1)`` (src/common/swMessage.cpp:74-84), SpModel raises
+:class:`Sw2dError` carrying the C status code and message.  There is no CPU fallback: without
+the CUDA library or a GPU the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import capi
+from .case import Case, read_case
+
+
+class Sw2dError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"sw2d error {code}: {message}")
+        self.code = code
+        self.message = message
+
+
+class SpModel:
+    """SW2D single-porosity model running on one GPU."""
+
+    def __init__(self, case: Case, device: int = 0):
+        self.lib = capi.load_library()
+        self.case = case
+        self.n = case.mesh.cell_nb
+        self.ni = case.mesh.edge_int_nb
+        self.nb = case.mesh.edge_bnd_nb
+        self._in = capi.native_inputs(case)
+        i = self._in
+        handle = ctypes.c_void_p()
+        st = self.lib.sw2d_create(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
+                                  ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0), capi._dp(i.r0), int(device),
+                                  ctypes.byref(handle))
+        if st != 0:
+            raise Sw2dError(st, self.lib.sw2d_last_error(None).decode())
+        self.handle = handle
+
+    @classmethod
+    def from_folder(cls, folder: str, device: int = 0) -> "SpModel":
+        case = read_case(folder)
+        if str(case.opts.get("model_hyperb", "sp")).lower() != "sp":
+            raise Sw2dError(-8, f"model_hyperb {case.opts.get('model_hyperb')!r}: only 'sp' is implemented")
+        return cls(case, device)
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise Sw2dError(st, self.lib.sw2d_last_error(self.handle).decode())
+
+    def step(self, n: int) -> int:
+        done = ctypes.c_int64(0)
+        self._check(self.lib.sw2d_step_n(self.handle, int(n), ctypes.byref(done)))
+        return int(done.value)
+
+    def execute(self) -> int:
+        done = ctypes.c_int64(0)
+        self._check(self.lib.sw2d_execute(self.handle, ctypes.byref(done)))
+        return int(done.value)
+
+    def state(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        h, q, r = (np.empty(self.n) for _ in range(3))
+        self._check(self.lib.sw2d_get_state(self.handle, h.ctypes.data, q.ctypes.data, r.ctypes.data))
+        return h, q, r
+
+    def set_state(self, h, q, r) -> None:
+        h, q, r = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, q, r))
+        self._check(self.lib.sw2d_set_state(self.handle, h.ctypes.data, q.ctypes.data, r.ctypes.data))
+
+    def get_state_device(self, h_ptr: int, q_ptr: int, r_ptr: int) -> None:
+        self._check(self.lib.sw2d_get_state_device(self.handle, h_ptr, q_ptr, r_ptr))
+
+    def set_state_device(self, h_ptr: int, q_ptr: int, r_ptr: int) -> None:
+        self._check(self.lib.sw2d_set_state_device(self.handle, h_ptr, q_ptr, r_ptr))
+
+    @property
+    def time(self) -> Tuple[float, float]:
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.sw2d_get_time(self.handle, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    @property
+    def t(self) -> float:
+        return self.time[0]
+
+    @property
+    def dt(self) -> float:
+        return self.time[1]
+
+    def set_time(self, t: float, dt: float) -> None:
+        self._check(self.lib.sw2d_set_time(self.handle, float(t), float(dt)))
+
+    def array(self, name: str) -> np.ndarray:
+        out = np.empty(max(self.n, self.ni, self.nb, 1))
+        k = self.lib.sw2d_get_array(self.handle, name.encode(), out.ctypes.data_as(capi.c_double_p), out.size)
+        if k < 0:
+            self._check(int(k))
+        return out[:k].copy()
+
+    def cell_permutation(self) -> np.ndarray:
+        perm = np.empty(self.n, dtype=np.int64)
+        self._check(self.lib.sw2d_get_cell_permutation(self.handle, perm.ctypes.data_as(capi.c_int64_p)))
+        return perm
+
+    def phase_times(self, n_steps: int):
+        """{kernel name: average device ms per step} over n_steps steps (which advance the run)."""
+        ms = np.zeros(8)
+        k = self.lib.sw2d_phase_times(self.handle, int(n_steps), ms.ctypes.data_as(capi.c_double_p), ms.size)
+        if k < 0:
+            self._check(int(k))
+        return {self.lib.sw2d_phase_name(i).decode(): float(ms[i]) for i in range(k)}
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.sw2d_get_stream(self.handle) or 0)
+
+    @property
+    def kernels_per_step(self) -> int:
+        return int(self.lib.sw2d_kernels_per_step(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.sw2d_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_case(folder: str, device: int = 0, n_steps: Optional[int] = None):
+    """`sw2dSolver <folder>` without result storage: returns (model, steps taken)."""
+    model = SpModel.from_folder(folder, device)
+    steps = model.execute() if n_steps is None else model.step(n_steps)
+    return model, steps

@@ -93,7 +93,7 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
     nx, ny = _grid_for(n_cells, 1.0)
     mesh = jittered_triangle_mesh(nx, ny, L, L, seed=seed_mesh, z_fn=bed)
     n = mesh.cell_nb
-    h0 = np.maximum(0.0, 2.0 - mesh.cell_z_b)
+    h0 = np.where(2.0 - mesh.cell_z_b < 0.0, 0.0, 2.0 - mesh.cell_z_b)   # std::max(z - z_b, 0.0)
     phi = 0.3 + 0.7 * _smooth_field(mesh.cell_x, mesh.cell_y, L, L, seed_phi)
     rng_n = np.random.default_rng(seed_n)
     man = np.exp(np.log(0.03) + 0.3 * rng_n.standard_normal(n))
@@ -102,7 +102,7 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
             "h_min": 1e-5, "t_max": t_max, "store_flag": "none", "output_format": "txt"}
     return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
                 boussinesq=np.ones(n), friction=np.stack([man, man, np.zeros(n)]),
-                bc=_wall_series(mesh.bc_codes()), extra={"name": "gaussian_bumps", "nx": nx, "ny": ny})
+                bc=_wall_series(mesh.bc_codes()), extra={"name": "gaussian_bumps", "nx": nx, "ny": ny, "ic_z": 2.0})
 
 
 def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "blending",

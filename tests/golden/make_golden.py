@@ -1,0 +1,115 @@
+"""Generates the golden fixtures of tests/golden/ by running the REFERENCE solver, compiled from
+its own sources (oracle/Makefile -> oracle/_ref/libsw2d_ref.so), on:
+
+* the synthetic cases of ``CASES`` (inputs are regenerated from their seeds by the tests; the
+  fixture stores a digest of those inputs and the reference's state after ``STEPS`` steps);
+* the reference's own functional case ``configue_fonctionels/sp_toce`` (native input.solv keys
+  only; the fixture stores the mesh tables and parameters the SP step reads, and the
+  reference's state after 100 steps and at t_max).
+
+Run here (the reference tree must be present):  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import importlib
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+pkg = importlib.import_module("inria-internship-project-sw2d-enzyme_b200")
+W = pkg.workloads
+
+STEPS = 200
+CASES = {
+    "dam_muscl_manning": ("dam_break", {"n_cells": 2000}),
+    "dam_godunov_manning": ("dam_break", {"n_cells": 2000, "scheme": "godunov"}),
+    "dam_muscl_nofriction": ("dam_break", {"n_cells": 2000, "friction": "none"}),
+    "bumps_muscl_manning": ("gaussian_bumps", {"n_cells": 3000}),
+    "chan_godunov_blending_strickler_fr": ("channel_features", {}),
+    "chan_muscl_disc_manning_h": ("channel_features", {"scheme": "muscl_evr", "topo": "discontinuous",
+                                                       "friction": "manning", "outflow": "h"}),
+    "chan_muscl_blend_chezy_z_b11": ("channel_features", {"scheme": "muscl_evr", "topo": "blending",
+                                                          "friction": "chezy", "outflow": "z", "boussinesq": 1.1}),
+    "chan_godunov_disc_none_q": ("channel_features", {"friction": "none", "outflow": "q", "head_loss": False}),
+}
+NATIVE_KEYS = ["model_hyperb", "model_friction", "model_singular_head_loss", "num_scheme", "topo_discretization",
+               "t_max", "dt_max", "dt_map", "dt_time_series", "h_min", "fr_max", "store_flag"]
+
+
+def build_case(builder: str, kwargs: dict):
+    return getattr(W, builder)(**kwargs)
+
+
+def case_digest(case) -> str:
+    """Digest of every input the step reads (detects drift of the seeded generators)."""
+    m = case.mesh
+    h = hashlib.sha256()
+    for a in (m.cell_area, m.cell_x, m.cell_y, m.cell_z_b, m.edge_int_cells, m.edge_int_length, m.edge_int_nx,
+              m.edge_int_ny, m.edge_int_mx, m.edge_int_my, m.edge_bnd_cell, m.edge_bnd_length, m.edge_bnd_nx,
+              m.edge_bnd_ny, m.edge_bnd_code, case.h0, case.q0, case.r0, case.phi, case.boussinesq):
+        h.update(np.ascontiguousarray(a).tobytes())
+    for a in (case.friction, case.head_loss):
+        if a is not None:
+            h.update(np.ascontiguousarray(a).tobytes())
+    h.update(json.dumps(case.opts, sort_keys=True, default=str).encode())
+    return h.hexdigest()
+
+
+def main():
+    from oracle.binding import RefSolver, build, reference_available
+    build(reference=True)
+    assert reference_available(), "reference sources not found: cannot make golden fixtures"
+    tmp = tempfile.mkdtemp(prefix="sw2d_golden_")
+    try:
+        for name, (builder, kwargs) in CASES.items():
+            case = build_case(builder, kwargs)
+            folder = os.path.join(tmp, name)
+            pkg.write_case(folder, case)
+            ref = RefSolver(folder)
+            done = ref.step(STEPS)
+            h, q, r = ref.state()
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), builder=builder, kwargs=json.dumps(kwargs),
+                                digest=case_digest(case), steps=done, t=ref.t, dt=ref.dt, h=h, q=q, r=r)
+            print(name, case.mesh.cell_nb, done, ref.t)
+
+        src = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
+        folder = os.path.join(tmp, "sp_toce")
+        shutil.copytree(src, folder)
+        solv = os.path.join(folder, "input", "input.solv")
+        lines = [ln for ln in open(solv).read().splitlines() if ln.strip() and ln.split()[0].lower() in NATIVE_KEYS]
+        open(solv, "w").write("\n".join(lines) + "\n")
+        case = pkg.read_case(folder)
+        ref = RefSolver(folder)
+        s100 = ref.step(100)
+        h100, q100, r100 = ref.state()
+        t100 = ref.t
+        s_end = s100 + ref.step(10 ** 7)
+        h, q, r = ref.state()
+        m = case.mesh
+        np.savez_compressed(
+            os.path.join(HERE, "sp_toce.npz"), opts=json.dumps(case.opts),
+            cell_area=m.cell_area, cell_x=m.cell_x, cell_y=m.cell_y, cell_z_b=m.cell_z_b,
+            edge_int_cells=m.edge_int_cells.astype(np.int32), edge_int_length=m.edge_int_length,
+            edge_int_nx=m.edge_int_nx, edge_int_ny=m.edge_int_ny, edge_int_mx=m.edge_int_mx,
+            edge_int_my=m.edge_int_my, edge_bnd_cell=m.edge_bnd_cell.astype(np.int32),
+            edge_bnd_length=m.edge_bnd_length, edge_bnd_nx=m.edge_bnd_nx, edge_bnd_ny=m.edge_bnd_ny,
+            edge_bnd_code=m.edge_bnd_code, h0=case.h0, q0=case.q0, r0=case.r0, phi=case.phi,
+            boussinesq=case.boussinesq, friction=case.friction, head_loss=case.head_loss,
+            bc_codes=np.array(case.bc.codes), bc_types=json.dumps(case.bc.types), bc_times=case.bc.times,
+            bc_values=case.bc.values, steps100=s100, t100=t100, h100=h100, q100=q100, r100=r100,
+            steps_end=s_end, t_end=ref.t, h_end=h, q_end=q, r_end=r)
+        print("sp_toce", m.cell_nb, s100, s_end, ref.t)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()
