@@ -176,6 +176,16 @@ int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t ca
 int sw2d_phase_times(sw2d_handle* h, int64_t n_steps, double* ms, int capacity);
 const char* sw2d_phase_name(int i);
 
+/* Run-time options.  "record_wave_speeds" (0/1): also keep lambda_max per edge for
+ * sw2d_get_array("lambda_max_int"/"lambda_max_bnd") (the reference's lambda_max_int/_bnd
+ * members, swSp.h:201-203); off by default since the step itself only needs lambda_max * length. */
+int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value);
+
+/* Evaluates, on device `device`, fn = 0: the portable exp, 1: the portable log used by the step
+ * (no counterpart in the reference, which calls the host libm's exp/log), 2: CUDA's exp,
+ * 3: CUDA's log, on n host values; for the tests of the elementary functions. */
+int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n);
+
 /* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
 int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
 

@@ -3,14 +3,16 @@
 // Every function restates one routine of the reference (paths relative to the reference
 // project) with the same operand order.  The library is compiled with -fmad=false so that no
 // multiply-add is contracted: +, -, *, / and sqrt are then IEEE binary64 round-to-nearest on
-// both sides and the results match the reference bit for bit.  exp and log are CUDA's, which
-// may differ from the host libm by an ulp (friction, head loss and critical depth only).
+// both sides and the results match the reference bit for bit.  exp and log are the portable
+// versions of portable_math.h, which give the same bits on the host.
 //
 // std::max(a,b) is (a < b ? b : a) and std::min(a,b) is (b < a ? b : a); smax/smin keep that
 // literal form, including what happens with NaN.
 #pragma once
 
 #include <cstdint>
+
+#include "portable_math.h"
 
 namespace sw2d {
 
@@ -105,13 +107,14 @@ __device__ __forceinline__ SideState evr_side(bool left, double h, double q, dou
 
 struct EdgeFlux {
     double f1, f2, f3, sl, sr;
+    unsigned bad;  // kStatusHllcConfig for the configuration the reference rejects
 };
 
 // swSp::hypHllc (swSpHyp.cpp:664-821) and swSp::hypHllcBlending (swSpHyp.cpp:824-998).
-// Sets *bad to kStatusHllcConfig for the configuration the reference rejects (:728-739).
+// Flags kStatusHllcConfig for the configuration the reference rejects (:728-739).
 __device__ __forceinline__ EdgeFlux hllc(bool blending, double bL, double bR, double phiL, double phiR, double zbL,
                                          double zbR, const SideState& L, const SideState& R, double h_min,
-                                         double phi_min, unsigned* bad)
+                                         double phi_min)
 {
     double hL, hR;
     if (blending) {
@@ -136,8 +139,9 @@ __device__ __forceinline__ EdgeFlux hllc(bool blending, double bL, double bR, do
         }
     }
     EdgeFlux f;
+    f.bad = 0;
     if ((int)both + (int)lhs + (int)rhs + (int)none != 1) {
-        *bad |= kStatusHllcConfig;
+        f.bad = kStatusHllcConfig;
         f.f1 = f.f2 = f.f3 = f.sl = f.sr = 0.0;
         return f;
     }
@@ -230,14 +234,15 @@ __device__ __forceinline__ double bc_value(const double* tv, const double* vv, i
 // swSp::hypHCritical (swSpHyp.cpp:651-661)
 __device__ __forceinline__ double h_critical(double phi, double q)
 {
-    return exp((1. / 3.) * log((q / smax(phi, kSmallReal)) / kGravity));
+    return sw2d_exp((1. / 3.) * sw2d_log((q / smax(phi, kSmallReal)) / kGravity));
 }
 
-// swSp::hypBoundaryFlux (swSpHyp.cpp:13-135); the boundary geometric source stays 0.
-__device__ __forceinline__ void boundary_flux(double bR, double phiR, double zbR, const SideState& S, int type,
-                                              double bcv, double h_min, double* f1o, double* f2o, double* f3o,
-                                              unsigned* bad)
+// swSp::hypBoundaryFlux (swSpHyp.cpp:13-135); the boundary geometric source stays 0.  Returns
+// kStatusBcFr / kStatusBcType where the reference stops, else 0.
+__device__ __forceinline__ unsigned boundary_flux(double bR, double phiR, double zbR, const SideState& S, int type,
+                                                  double bcv, double h_min, double* f1o, double* f2o, double* f3o)
 {
+    unsigned bad = 0;
     double hR = S.z - zbR;
     double q1 = S.q, r1 = S.r;
     if (hR < h_min) {
@@ -251,7 +256,7 @@ __device__ __forceinline__ void boundary_flux(double bR, double phiR, double zbR
     double flux2R = spec_force(bR, phiR, hR, uR);
     double flux1 = 0.0, flux2 = 0.0;
     if (type == 3) {  // fr
-        if ((bcv < 0.) | (bcv > 1.)) *bad |= kStatusBcFr;
+        if ((bcv < 0.) | (bcv > 1.)) bad |= kStatusBcFr;
         double c = (uR - 2. * cR) / (-bcv - 2.);
         c = smax(c, 0.);
         double u = -bcv * c;
@@ -274,7 +279,7 @@ __device__ __forceinline__ void boundary_flux(double bR, double phiR, double zbR
         if (hc >= hR) flux1 = phiR * 1.5 * sqrt(kGravity * hc) * hc;
         flux2 = flux2R + (flux1 - q1 * phiR) * L1;
     } else {
-        *bad |= kStatusBcType;
+        bad |= kStatusBcType;
     }
     double flux3;
     if (flux1 > 0) {
@@ -286,6 +291,7 @@ __device__ __forceinline__ void boundary_flux(double bR, double phiR, double zbR
     *f1o = flux1;
     *f2o = flux2;
     *f3o = flux3;
+    return bad;
 }
 
 // swSource::frictionChezy1D / frictionManning1D / frictionStrickler1D
@@ -294,13 +300,13 @@ __device__ __forceinline__ double friction_factor(int model, double k, double h,
 {
     double factor = 1.0;
     if (model == 1) {
-        if ((h > kSmallReal) && (k > kSmallReal)) factor = exp(-kGravity * un / k / k / h * dt);
+        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k / h * dt);
         else factor = 0.0;
     } else if (model == 2) {
-        if (h > kSmallReal) factor = exp(-kGravity * un * k * k * exp(-4.0 / 3.0 * log(h)) * dt);
+        if (h > kSmallReal) factor = sw2d_exp(-kGravity * un * k * k * sw2d_exp(-4.0 / 3.0 * sw2d_log(h)) * dt);
         else factor = 0.0;
     } else {
-        if ((h > kSmallReal) && (k > kSmallReal)) factor = exp(-kGravity * un / k / k * exp(-4.0 / 3.0 * log(h)) * dt);
+        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k * sw2d_exp(-4.0 / 3.0 * sw2d_log(h)) * dt);
         else factor = 0.0;
     }
     return factor;

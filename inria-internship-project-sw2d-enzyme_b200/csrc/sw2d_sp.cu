@@ -7,12 +7,20 @@
 //
 //   k_slopes   per cell   limited free-surface slopes (MUSCL-EVR only)      swSpHypMusclEvr.cpp:11-115
 //   k_edges    per edge   Riemann states, max wave speed, HLLC / boundary    swSpHypGodunov.cpp, swSpHypMusclEvr.cpp:119-277,
-//                         fluxes                                            swSpHyp.cpp:13-135,276-402,664-998
+//                         fluxes, per-side CFL contributions                 swSpHyp.cpp:13-135,276-402,664-998
 //   k_cfl      per cell   swept length, CFL dt, warp -> block -> grid min,   swSpHyp.cpp:430-512
 //                         dt_map snap and t_max clip on the device
 //   k_update   per cell   flux balance (CSR gather in the reference's per-   swSpHyp.cpp:214-273,184-209,
 //                         cell order), round-off flush, negative-depth clamp, swSpSourceFriction.cpp:11-219,
 //                         friction, singular head loss, velocity cap, t += dt swSp.cpp:447-479
+//
+// Data layout (all in HBM, internal numbering): the state of a cell is one 32-byte record
+// {h, q, r, z = h + z_b} so that a neighbour gather touches one sector; cell statics
+// {z_b, boussinesq, phi, area}, centroids {x, y} and slopes {sx, sy} are 32/16-byte records;
+// edges keep {L, R}, normals {nx, ny}, midpoints {mx, my}, edge-factor coefficients
+// {w/(A_L phi_L), w/(A_R phi_R)} and a 48-byte flux record {F1, F2, F3, S2L, S2R, -}.  The flux
+// records persist between steps: the reference keeps the previous fluxes of an edge whose two
+// sides are dry (swSpHyp.cpp:339).
 //
 // Cells are renumbered along a Hilbert curve and internal edges by their first cell, for
 // locality; every per-cell sum still runs in the reference's order (boundary edges, then
@@ -53,33 +61,54 @@ struct Ctrl {
 struct DevMesh {
     int nc, ni, nb;
     // cells
-    double *h, *q, *r;
-    const double *zb, *area, *cx, *cy, *phi, *bous;
-    const double *fk1, *fk2, *fcos, *fsin;               // friction (may be null)
-    const double *hs, *hk1, *hk2, *hcos, *hsin;          // singular head loss (may be null)
-    const int *cb_off, *cb_idx;                          // boundary edges of each cell
-    const int *ci_off, *ci_ent, *ci_nbr;                 // internal edges (edge*2 + side) and neighbour
-    double *sx, *sy;                                      // MUSCL slopes
+    double4* st;             // {h, q, r, z}
+    const double4* cst;      // {z_b, boussinesq, phi, area}
+    const double2* cxy;      // centroid
+    double2* slope;          // MUSCL slopes
+    const double4* fric;     // {k1, k2, cos a, sin a} (friction)
+    const double4* hla;      // {h_sing, k1, k2, -} (singular head loss)
+    const double2* hlb;      // {cos a, sin a}
+    const int2* coff;        // [nc+1] {first internal entry, first boundary entry}
+    const int2* cint;        // {edge*2 + side, neighbour}
+    const int* cbnd;         // boundary edge
     // internal edges
     const int2* lr;
-    const double *len, *nx, *ny, *mx, *my, *coefL, *coefR;
-    double *F1, *F2, *F3, *S2L, *S2R, *lmax;
+    const double2* nxy;
+    const double2* mxy;
+    const double* len;
+    const double2* coef;     // {coefL, coefR}
+    double2* flux;           // 3 x double2 per edge: {F1,F2},{F3,S2L},{S2R,-}
+    double2* swc;            // {lambda_max*len counted for L, for R}
+    double* lmax;            // optional copy of lambda_max (tests)
     // boundary edges
     const int* bcell;
     const int* bbc;
-    const double *blen, *bnx, *bny, *bcoef;
-    double *F1b, *F2b, *F3b, *lmaxb;
+    const double4* bgeo;     // {nx, ny, length, coef}
+    double4* bflux;          // {F1, F2, F3, -}
+    double* bswc;            // lambda_max*len when the cell is wet, else 0
+    double* lmaxb;           // optional copy of lambda_max (tests)
     // boundary series
     const int* bctype;
     const long long* bcoff;
     const double *bctimes, *bcvals;
     // parameters
     double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
-    int scheme, topo, friction, head_loss, neg_detect;
+    int neg_detect;
     // dt reduction scratch
     double* part;
     Ctrl* ctrl;
 };
+
+// read-only loads through the non-coherent path (data not written by the same kernel)
+template <class T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+__device__ __forceinline__ double4 ld(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
 
 __device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_max; }
 
@@ -89,23 +118,25 @@ __device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_
 // in the same order, the under/overshoot rescaling of this cell's slope (that rescaling only
 // reads this cell's slope, so the reference's global edge loop decomposes exactly per cell).
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_slopes(DevMesh m)
+__global__ void __launch_bounds__(kBlock, 4) k_slopes(DevMesh m)
 {
     if (!step_active(m.ctrl)) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
-    const double zc = m.h[c] + m.zb[c];
-    const double xc = m.cx[c], yc = m.cy[c];
-    const int k0 = m.ci_off[c], k1 = m.ci_off[c + 1];
+    const double zc = ld(&m.st[c].w);
+    const double2 xy = ld(&m.cxy[c]);
+    const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
+    const int k0 = o0.x, k1 = o1.x;
     double sx = 0.0, sy = 0.0, wsum = 0.0;
     if (k1 - k0 > 1) {
         for (int k = k0; k < k1; k++) {
-            int j = m.ci_nbr[k];
-            double dx = m.cx[j] - xc;
-            double dy = m.cy[j] - yc;
+            const int j = ld(&m.cint[k]).y;
+            const double2 xj = ld(&m.cxy[j]);
+            double dx = xj.x - xy.x;
+            double dy = xj.y - xy.y;
             double dist = sqrt(dx * dx + dy * dy);
             double w = 1.0 / dist;
-            double zj = m.h[j] + m.zb[j];
+            double zj = ld(&m.st[j].w);
             sx += (zj - zc) * dx / dist / dist * w;
             sy += (zj - zc) * dy / dist / dist * w;
             wsum += w;
@@ -114,15 +145,15 @@ __global__ void __launch_bounds__(kBlock) k_slopes(DevMesh m)
         sy /= wsum;
     }
     for (int k = k0; k < k1; k++) {
-        int ent = m.ci_ent[k];
-        int e = ent >> 1;
-        int j = m.ci_nbr[k];
-        double zj = m.h[j] + m.zb[j];
-        double zL = (ent & 1) ? zj : zc;
-        double zR = (ent & 1) ? zc : zj;
-        double fmx = smax(zL, zR);
-        double fmn = smin(zL, zR);
-        double rec = zc + (m.mx[e] - xc) * sx + (m.my[e] - yc) * sy;
+        const int2 en = ld(&m.cint[k]);
+        const int e = en.x >> 1;
+        const double zj = ld(&m.st[en.y].w);
+        const double zL = (en.x & 1) ? zj : zc;
+        const double zR = (en.x & 1) ? zc : zj;
+        const double fmx = smax(zL, zR);
+        const double fmn = smin(zL, zR);
+        const double2 mp = ld(&m.mxy[e]);
+        const double rec = zc + (mp.x - xy.x) * sx + (mp.y - xy.y) * sy;
         if (rec < fmn) {
             double fac = (fmn - zc) / (rec - zc);
             sx *= fac;
@@ -134,75 +165,81 @@ __global__ void __launch_bounds__(kBlock) k_slopes(DevMesh m)
             sy *= fac;
         }
     }
-    m.sx[c] = sx;
-    m.sy[c] = sy;
+    m.slope[c] = make_double2(sx, sy);
 }
 
 // ------------------------------------------------------------------------------------------
-// k_edges: one thread per internal edge, then one per boundary edge.
+// k_edges: one thread per internal edge, then one per boundary edge.  Also writes, per edge
+// side, the contribution lambda_max * length the CFL sum of that cell takes (hypComputeTimeStep,
+// swSpHyp.cpp:437-477: the L cell counts it when it is wet; the R cell when L or R is wet,
+// because the reference carries `lambda` over from the L test).
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_edges(DevMesh m)
+template <int kScheme, bool kBlending>
+__global__ void __launch_bounds__(kBlock, 3) k_edges(DevMesh m)
 {
     if (!step_active(m.ctrl)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned bad = 0;
     if (i < m.ni) {
         const int e = i;
-        const int2 lr = m.lr[e];
+        const int2 lr = ld(&m.lr[e]);
         const int a = lr.x, b = lr.y;
-        const double nx = m.nx[e], ny = m.ny[e];
-        const double zbL = m.zb[a], zbR = m.zb[b];
-        const double bL = m.bous[a], bR = m.bous[b];
+        const double2 n = ld(&m.nxy[e]);
+        const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
+        const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
         SideState SL, SR;
-        if (m.scheme == SW2D_SCHEME_GODUNOV) {
-            SL = godunov_side(m.h[a], m.q[a], m.r[a], zbL, bL, nx, ny);
-            SR = godunov_side(m.h[b], m.q[b], m.r[b], zbR, bR, nx, ny);
+        if (kScheme == SW2D_SCHEME_GODUNOV) {
+            SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
+            SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
         } else {
             const double dtp = m.ctrl->dt;
-            const double mx = m.mx[e], my = m.my[e];
-            const double ha = m.h[a], hb = m.h[b];
-            SL = evr_side(true, ha, m.q[a], m.r[a], zbL, bL, ha + zbL, m.sx[a], m.sy[a], m.cx[a], m.cy[a], mx, my, nx,
-                          ny, dtp);
-            SR = evr_side(false, hb, m.q[b], m.r[b], zbR, bR, hb + zbR, m.sx[b], m.sy[b], m.cx[b], m.cy[b], mx, my, nx,
-                          ny, dtp);
+            const double2 mp = ld(&m.mxy[e]);
+            const double2 xa = ld(&m.cxy[a]), xb = ld(&m.cxy[b]);
+            const double2 ga = ld(&m.slope[a]), gb = ld(&m.slope[b]);
+            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y, dtp);
+            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y, dtp);
         }
-        m.lmax[e] = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
-        const double hL = SL.z - zbL, hR = SR.z - zbR;
+        const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
+        if (m.lmax) m.lmax[e] = lm;
+        const double lw = lm * ld(&m.len[e]);
+        const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;
+        m.swc[e] = make_double2(wetL ? lw : 0.0, (wetL || wetR) ? lw : 0.0);
+        const double hL = SL.z - ca.x, hR = SR.z - cb.x;
         if ((hL > m.h_min) || (hR > m.h_min)) {
-            EdgeFlux f = hllc(m.topo == SW2D_TOPO_BLENDING, bL, bR, m.phi[a], m.phi[b], zbL, zbR, SL, SR, m.h_min,
-                              m.phi_min, &bad);
+            EdgeFlux f = hllc(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min);
+            bad |= f.bad;
             if (isnan(f.f1)) bad |= kStatusNanFlux;
-            m.F1[e] = f.f1;
-            m.F2[e] = f.f2;
-            m.F3[e] = f.f3;
-            m.S2L[e] = f.sl;
-            m.S2R[e] = f.sr;
+            double2* fp = m.flux + 3 * (size_t)e;
+            fp[0] = make_double2(f.f1, f.f2);
+            fp[1] = make_double2(f.f3, f.sl);
+            fp[2] = make_double2(f.sr, 0.0);
         }
     } else if (i < m.ni + m.nb) {
         const int e = i - m.ni;
-        const int c = m.bcell[e];
-        const double zbc = m.zb[c];
-        SideState S = godunov_side(m.h[c], m.q[c], m.r[c], zbc, m.bous[c], m.bnx[e], m.bny[e]);
-        m.lmaxb[e] = (m.scheme == SW2D_SCHEME_GODUNOV) ? smax(fabs(S.lp), fabs(S.lm)) : smax(fabs(S.lm), fabs(S.lp));
-        const int k = m.bbc[e];
-        const long long o0 = m.bcoff[k], o1 = m.bcoff[k + 1];
+        const int c = ld(&m.bcell[e]);
+        const double4 s = ld(&m.st[c]);
+        const double4 cs = ld(&m.cst[c]);
+        const double4 g = ld(&m.bgeo[e]);
+        SideState S = godunov_side(s.x, s.y, s.z, cs.x, cs.y, g.x, g.y);
+        const double lm = (kScheme == SW2D_SCHEME_GODUNOV) ? smax(fabs(S.lp), fabs(S.lm)) : smax(fabs(S.lm), fabs(S.lp));
+        if (m.lmaxb) m.lmaxb[e] = lm;
+        m.bswc[e] = (s.x > m.h_min) ? lm * g.z : 0.0;
+        const int k = ld(&m.bbc[e]);
+        const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
         const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, m.ctrl->t);
         double f1, f2, f3;
-        boundary_flux(m.bous[c], m.phi[c], zbc, S, m.bctype[k], v, m.h_min, &f1, &f2, &f3, &bad);
-        m.F1b[e] = f1;
-        m.F2b[e] = f2;
-        m.F3b[e] = f3;
+        bad |= boundary_flux(cs.y, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
+        m.bflux[e] = make_double4(f1, f2, f3, 0.0);
     }
     if (bad) atomicOr(&m.ctrl->status, bad);
 }
 
 // ------------------------------------------------------------------------------------------
 // k_cfl: swSp::hypComputeTimeStep (swSpHyp.cpp:430-512).  swept[c] gathers, in the reference's
-// order, lambda_max * length over the boundary edges (cell wet) and internal edges; on an
-// internal edge the R cell also counts when only L is wet, because the reference carries the
-// variable `lambda` over from the L test to the R side (:456-476).  dt = min over cells of
-// cfl * area / max(swept, 1e-16), reduced warp -> block -> grid (last block done), then the
-// dt_map snap (:496-504) and the t_max clip, all on the device.
+// order, the contributions k_edges prepared; dt = min over cells of cfl * area / max(swept,
+// 1e-16), reduced warp -> block -> grid (last block done), then the dt_map snap (:496-504)
+// and the t_max clip, all on the device.  Adding a skipped (zero) contribution would not
+// change the sum, so the gather adds exactly what the reference adds.
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double min_keep(double a, double b) { return (b < a) ? b : a; }
 
@@ -213,33 +250,25 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
         if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->go = 0;
         return;
     }
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double best = m.dt_max;
     if (c < m.nc) {
-        const double hc = m.h[c];
-        const bool wet = hc > m.h_min;
+        const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
         double sw = 0.0;
-        if (wet) {
-            for (int k = m.cb_off[c]; k < m.cb_off[c + 1]; k++) {
-                int e = m.cb_idx[k];
-                sw += m.lmaxb[e] * m.blen[e];
-            }
+        for (int k = o0.y; k < o1.y; k++) sw += ld(&m.bswc[ld(&m.cbnd[k])]);
+        for (int k = o0.x; k < o1.x; k++) {
+            const int ent = ld(&m.cint[k]).x;
+            const double2 w = ld(&m.swc[ent >> 1]);
+            sw += (ent & 1) ? w.y : w.x;
         }
-        for (int k = m.ci_off[c]; k < m.ci_off[c + 1]; k++) {
-            int ent = m.ci_ent[k];
-            int e = ent >> 1;
-            bool count = wet;
-            if ((ent & 1) && !wet) count = m.h[m.ci_nbr[k]] > m.h_min;
-            if (count) sw += m.lmax[e] * m.len[e];
-        }
-        double x = m.cfl_max * (m.area[c] / smax(sw, kSmallReal));
+        double x = m.cfl_max * (ld(&m.cst[c].w) / smax(sw, kSmallReal));
         if (x < best) best = x;
     }
     // warp then block minimum (NaN candidates never win: comparisons with NaN are false)
     for (int off = 16; off > 0; off >>= 1) best = min_keep(best, __shfl_down_sync(0xffffffffu, best, off));
     __shared__ double wmin[kBlock / 32];
     __shared__ bool last;
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) wmin[wid] = best;
     __syncthreads();
     if (wid == 0) {
@@ -257,7 +286,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
     // last block: reduce the per-block minima
     __threadfence();
     double b2 = m.dt_max;
-    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) b2 = min_keep(b2, ((volatile double*)m.part)[i]);
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) b2 = min_keep(b2, ((volatile double*)m.part)[i]);
     for (int off = 16; off > 0; off >>= 1) b2 = min_keep(b2, __shfl_down_sync(0xffffffffu, b2, off));
     if (lane == 0) wmin[wid] = b2;
     __syncthreads();
@@ -279,48 +308,57 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
 }
 
 // ------------------------------------------------------------------------------------------
-// k_update: balance + sources for one cell, then t += dt (block 0).
+// k_update: balance + sources for one cell, then t += dt (thread 0).
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_update(DevMesh m)
+template <int kFriction, bool kHeadLoss>
+__global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
 {
     Ctrl* ctrl = m.ctrl;
     if (!ctrl->go) return;
     const double dt = ctrl->dt;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c == 0) {
         ctrl->t = ctrl->t + dt;  // swSp.cpp:592; no other thread of this kernel reads t
         ctrl->steps += 1;
     }
     if (c >= m.nc) return;
-    double hh = m.h[c], qq = m.q[c], rr = m.r[c];
+    const double4 s0 = m.st[c];
+    double hh = s0.x, qq = s0.y, rr = s0.z;
+    const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
     // hypComputeBalance (swSpHyp.cpp:214-273): boundary edges, then internal edges, each in
     // increasing original index; factors of swSp::computeEdgeFactors (swSp.cpp:338-444)
-    for (int k = m.cb_off[c]; k < m.cb_off[c + 1]; k++) {
-        const int e = m.cb_idx[k];
-        const double cf = m.bcoef[e], nx = m.bnx[e], ny = m.bny[e];
+    for (int k = o0.y; k < o1.y; k++) {
+        const int e = ld(&m.cbnd[k]);
+        const double4 g = ld(&m.bgeo[e]);
+        const double4 F = m.bflux[e];
+        const double cf = g.w, nx = g.x, ny = g.y;
         const double f1 = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
         const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
         const double s2 = 0.0;  // boundary geometric source: never set by hypBoundaryFlux
-        hh += f1 * m.F1b[e] * dt;
-        qq += (f2F2 * m.F2b[e] + f2S2 * s2 + f2F3 * m.F3b[e]) * dt;
-        rr += (f3F2 * m.F2b[e] + f3S2 * s2 + f3F3 * m.F3b[e]) * dt;
+        hh += f1 * F.x * dt;
+        qq += (f2F2 * F.y + f2S2 * s2 + f2F3 * F.z) * dt;
+        rr += (f3F2 * F.y + f3S2 * s2 + f3F3 * F.z) * dt;
     }
-    for (int k = m.ci_off[c]; k < m.ci_off[c + 1]; k++) {
-        const int ent = m.ci_ent[k];
+    for (int k = o0.x; k < o1.x; k++) {
+        const int ent = ld(&m.cint[k]).x;
         const int e = ent >> 1;
-        const double nx = m.nx[e], ny = m.ny[e];
-        const double F1 = m.F1[e], F2 = m.F2[e], F3 = m.F3[e];
+        const double2 n = ld(&m.nxy[e]);
+        const double2 cfp = ld(&m.coef[e]);
+        const double2* fp = m.flux + 3 * (size_t)e;
+        const double2 fa = fp[0], fb = fp[1];
+        const double nx = n.x, ny = n.y;
+        const double F1 = fa.x, F2 = fa.y, F3 = fb.x;
         if (ent & 1) {  // this cell is R
-            const double cf = m.coefR[e];
-            const double s2 = m.S2R[e];
+            const double cf = cfp.y;
+            const double s2 = fp[2].x;
             const double f1 = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
             const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
             hh += f1 * F1 * dt;
             qq += (f2F2 * F2 + f2S2 * s2 + f2F3 * F3) * dt;
             rr += (f3F2 * F2 + f3S2 * s2 + f3F3 * F3) * dt;
         } else {        // this cell is L
-            const double cf = m.coefL[e];
-            const double s2 = m.S2L[e];
+            const double cf = cfp.x;
+            const double s2 = fb.y;
             const double f1 = -cf, f2F2 = -cf * nx, f2F3 = +cf * ny, f2S2 = +cf * nx;
             const double f3F2 = -cf * ny, f3F3 = -cf * nx, f3S2 = +cf * ny;
             hh += f1 * F1 * dt;
@@ -341,16 +379,17 @@ __global__ void __launch_bounds__(kBlock) k_update(DevMesh m)
     }
     const double hthr = smax(m.h_min, kSmallReal);
     // friction (swSpSourceFriction.cpp:39-171)
-    if (m.friction != SW2D_FRICTION_NONE) {
+    if (kFriction != SW2D_FRICTION_NONE) {
         if (hh > hthr) {
+            const double4 fr = ld(&m.fric[c]);
             double u = qq / hh;
             double v = rr / hh;
-            double ca = m.fcos[c], sa = m.fsin[c];
+            double ca = fr.z, sa = fr.w;
             double ul = u * ca + v * sa;
             double vl = -u * sa + v * ca;
             double un = sqrt(u * u + v * v);
-            double f1 = friction_factor(m.friction, m.fk1[c], hh, un, dt);
-            double f2 = friction_factor(m.friction, m.fk2[c], hh, un, dt);
+            double f1 = friction_factor(kFriction, fr.x, hh, un, dt);
+            double f2 = friction_factor(kFriction, fr.y, hh, un, dt);
             ul *= f1;
             vl *= f2;
             qq = (ul * ca - vl * sa) * hh;
@@ -361,18 +400,20 @@ __global__ void __launch_bounds__(kBlock) k_update(DevMesh m)
         }
     }
     // singular head loss (swSpSourceFriction.cpp:174-219)
-    if (m.head_loss) {
-        double ca = m.hcos[c], sa = m.hsin[c];
+    if (kHeadLoss) {
+        const double2 cs = ld(&m.hlb[c]);
+        double ca = cs.x, sa = cs.y;
         double qx = qq * ca + rr * sa;
         double qy = -qq * sa + rr * ca;
         if (hh > hthr) {
+            const double4 hl = ld(&m.hla[c]);
             double ax = 0, ay = 0;
-            if (hh > m.hs[c]) {
-                ax = sqrt(qx * qx + qy * qy) * m.hk1[c] / hh;
-                ay = sqrt(qx * qx + qy * qy) * m.hk2[c] / hh;
+            if (hh > hl.x) {
+                ax = sqrt(qx * qx + qy * qy) * hl.y / hh;
+                ay = sqrt(qx * qx + qy * qy) * hl.z / hh;
             }
-            qx = qx * exp(-ax * dt);
-            qy = qy * exp(-ay * dt);
+            qx = qx * sw2d_exp(-ax * dt);
+            qy = qy * sw2d_exp(-ay * dt);
         } else {
             qx = 0.;
             qy = 0.;
@@ -391,56 +432,68 @@ __global__ void __launch_bounds__(kBlock) k_update(DevMesh m)
             rr = rr / fact;
         }
     }
-    m.h[c] = hh;
-    m.q[c] = qq;
-    m.r[c] = rr;
+    // z = h + z_b of the new state, as the next step's reconstruction computes it
+    // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
+    m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.cst[c].x));
 }
 
 // swSp::computeEdgeFactors coefficient w / area / phi (swSp.cpp:364-368, 397-405)
-__global__ void k_edge_coefficients(DevMesh m, double* coefL, double* coefR, double* bcoef)
+__global__ void k_edge_coefficients(DevMesh m, double2* coef, double4* bgeo)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m.ni) {
-        int2 lr = m.lr[i];
-        double w = m.len[i];
-        coefL[i] = (m.phi[lr.x] > m.phi_min) ? w / m.area[lr.x] / m.phi[lr.x] : 0.0;
-        coefR[i] = (m.phi[lr.y] > m.phi_min) ? w / m.area[lr.y] / m.phi[lr.y] : 0.0;
+        const int2 lr = m.lr[i];
+        const double w = m.len[i];
+        const double4 a = m.cst[lr.x], b = m.cst[lr.y];
+        coef[i] = make_double2((a.z > m.phi_min) ? w / a.w / a.z : 0.0, (b.z > m.phi_min) ? w / b.w / b.z : 0.0);
     } else if (i < m.ni + m.nb) {
-        int e = i - m.ni;
-        int c = m.bcell[e];
-        bcoef[e] = (m.phi[c] > m.phi_min) ? m.blen[e] / m.area[c] / m.phi[c] : 0.0;
+        const int e = i - m.ni;
+        const double4 c = m.cst[m.bcell[e]];
+        double4 g = bgeo[e];
+        g.w = (c.z > m.phi_min) ? g.z / c.w / c.z : 0.0;
+        bgeo[e] = g;
     }
 }
 
 // caller numbering <-> internal numbering
-__global__ void k_gather3(const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
-                          const int* __restrict__ perm, double* oa, double* ob, double* oc, int n)
+__global__ void k_gather_state(const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+                               const int* __restrict__ perm, const double4* __restrict__ cst, double4* st, int n)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        int p = perm[i];
-        oa[i] = a[p];
-        ob[i] = b[p];
-        oc[i] = c[p];
+        const int p = perm[i];
+        const double h = a[p];
+        st[i] = make_double4(h, b[p], c[p], h + cst[i].x);
     }
 }
 
-__global__ void k_scatter3(const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
-                           const int* __restrict__ perm, double* oa, double* ob, double* oc, int n)
+__global__ void k_scatter_state(const double4* __restrict__ st, const int* __restrict__ perm, double* oa, double* ob,
+                                double* oc, int n)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        int p = perm[i];
-        oa[p] = a[i];
-        ob[p] = b[i];
-        oc[p] = c[i];
+        const int p = perm[i];
+        const double4 s = st[i];
+        oa[p] = s.x;
+        ob[p] = s.y;
+        oc[p] = s.z;
     }
 }
 
-__global__ void k_scatter1(const double* __restrict__ a, const int* __restrict__ perm, double* oa, int n)
+// per-edge/per-cell arrays back to the caller's numbering: out[perm[i]] = src[i*stride + offset]
+__global__ void k_scatter_strided(const double* __restrict__ src, int stride, int offset, const int* __restrict__ perm,
+                                  double* out, int n)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) oa[perm[i]] = a[i];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[perm[i]] = src[(size_t)i * stride + offset];
+}
+
+__global__ void k_eval_math(int fn, const double* __restrict__ x, double* y, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = x[i];
+    y[i] = fn == 0 ? sw2d_exp(v) : fn == 1 ? sw2d_log(v) : fn == 2 ? exp(v) : log(v);
 }
 
 inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
@@ -483,6 +536,8 @@ struct sw2d_handle {
     int* d_int_perm = nullptr;
     int* d_bnd_perm = nullptr;
     double* stage = nullptr;    // 3 * nc doubles
+    double* lmax_buf = nullptr;
+    double* lmaxb_buf = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     std::string err;
@@ -539,14 +594,55 @@ int status_to_code(sw2d_handle* h, unsigned st)
     return SW2D_OK;
 }
 
-int launch_step(sw2d_handle* h)
+void launch_edges(sw2d_handle* h)
+{
+    const DevMesh& m = h->m;
+    const unsigned g = grid_for((long long)m.ni + m.nb);
+    const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
+    if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
+        if (bl) k_edges<SW2D_SCHEME_GODUNOV, true><<<g, kBlock, 0, h->stream>>>(m);
+        else k_edges<SW2D_SCHEME_GODUNOV, false><<<g, kBlock, 0, h->stream>>>(m);
+    } else {
+        if (bl) k_edges<SW2D_SCHEME_MUSCL_EVR, true><<<g, kBlock, 0, h->stream>>>(m);
+        else k_edges<SW2D_SCHEME_MUSCL_EVR, false><<<g, kBlock, 0, h->stream>>>(m);
+    }
+}
+
+template <int kF>
+void launch_update_f(sw2d_handle* h, unsigned g)
+{
+    if (h->p.singular_head_loss) k_update<kF, true><<<g, kBlock, 0, h->stream>>>(h->m);
+    else k_update<kF, false><<<g, kBlock, 0, h->stream>>>(h->m);
+}
+
+void launch_update(sw2d_handle* h)
+{
+    const unsigned g = grid_for(h->m.nc);
+    switch (h->p.friction) {
+        case SW2D_FRICTION_CHEZY: launch_update_f<SW2D_FRICTION_CHEZY>(h, g); break;
+        case SW2D_FRICTION_MANNING: launch_update_f<SW2D_FRICTION_MANNING>(h, g); break;
+        case SW2D_FRICTION_STRICKLER: launch_update_f<SW2D_FRICTION_STRICKLER>(h, g); break;
+        default: launch_update_f<SW2D_FRICTION_NONE>(h, g); break;
+    }
+}
+
+// phase i of one step on the handle's stream: 0 slopes, 1 edges, 2 cfl, 3 update
+void launch_phase(sw2d_handle* h, int i)
 {
     DevMesh& m = h->m;
-    if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) k_slopes<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
-    k_edges<<<grid_for((long long)m.ni + m.nb), kBlock, 0, h->stream>>>(m);
-    k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
-    k_update<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
-    return SW2D_OK;
+    switch (i) {
+        case 0:
+            if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) k_slopes<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
+            break;
+        case 1: launch_edges(h); break;
+        case 2: k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); break;
+        default: launch_update(h); break;
+    }
+}
+
+void launch_step(sw2d_handle* h)
+{
+    for (int i = 0; i < 4; i++) launch_phase(h, i);
 }
 
 int ensure_graph(sw2d_handle* h, int steps)
@@ -692,76 +788,80 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
 
     // ---- per-cell lists in the reference's order (swParent::setMeshTables, swParent.cpp:469-486):
     // walking edges by increasing original index appends them in that order.
-    std::vector<int> cb_off(nc + 1, 0), ci_off(nc + 1, 0);
-    for (int64_t e = 0; e < nb; e++) cb_off[inv[mesh->edge_bnd_cell[e]] + 1]++;
+    std::vector<int> cb_cnt(nc + 1, 0), ci_cnt(nc + 1, 0);
+    for (int64_t e = 0; e < nb; e++) cb_cnt[inv[mesh->edge_bnd_cell[e]] + 1]++;
     for (int64_t e = 0; e < ni; e++) {
-        ci_off[inv[mesh->edge_int_cells[2 * e]] + 1]++;
-        ci_off[inv[mesh->edge_int_cells[2 * e + 1]] + 1]++;
+        ci_cnt[inv[mesh->edge_int_cells[2 * e]] + 1]++;
+        ci_cnt[inv[mesh->edge_int_cells[2 * e + 1]] + 1]++;
     }
     for (int64_t c = 0; c < nc; c++) {
-        cb_off[c + 1] += cb_off[c];
-        ci_off[c + 1] += ci_off[c];
+        cb_cnt[c + 1] += cb_cnt[c];
+        ci_cnt[c + 1] += ci_cnt[c];
     }
-    std::vector<int> cb_idx(nb), ci_ent(2 * ni), ci_nbr(2 * ni);
+    std::vector<int2> coff(nc + 1);
+    for (int64_t c = 0; c <= nc; c++) coff[c] = make_int2(ci_cnt[c], cb_cnt[c]);
+    std::vector<int> cbnd(nb);
+    std::vector<int2> cint(2 * ni);
     {
-        std::vector<int> fb(cb_off.begin(), cb_off.end() - 1), fi(ci_off.begin(), ci_off.end() - 1);
-        for (int64_t e = 0; e < nb; e++) cb_idx[fb[inv[mesh->edge_bnd_cell[e]]]++] = inv_bnd[e];
+        std::vector<int> fb(cb_cnt.begin(), cb_cnt.end() - 1), fi(ci_cnt.begin(), ci_cnt.end() - 1);
+        for (int64_t e = 0; e < nb; e++) cbnd[fb[inv[mesh->edge_bnd_cell[e]]]++] = inv_bnd[e];
         for (int64_t e = 0; e < ni; e++) {
             int a = inv[mesh->edge_int_cells[2 * e]], b = inv[mesh->edge_int_cells[2 * e + 1]];
             int ne = inv_int[e];
-            ci_ent[fi[a]] = ne * 2 + 0;
-            ci_nbr[fi[a]++] = b;
-            ci_ent[fi[b]] = ne * 2 + 1;
-            ci_nbr[fi[b]++] = a;
+            cint[fi[a]++] = make_int2(ne * 2 + 0, b);
+            cint[fi[b]++] = make_int2(ne * 2 + 1, a);
         }
     }
 
-    // ---- gather host tables into the new numbering
-    auto cellv = [&](const double* src, double fill) {
-        std::vector<double> v(nc);
-        for (int64_t i = 0; i < nc; i++) v[i] = src ? src[h->cell_perm[i]] : fill;
-        return v;
-    };
-    auto intv = [&](const double* src) {
-        std::vector<double> v(ni);
-        for (int64_t i = 0; i < ni; i++) v[i] = src[h->int_perm[i]];
-        return v;
-    };
-    auto bndv = [&](const double* src) {
-        std::vector<double> v(nb);
-        for (int64_t i = 0; i < nb; i++) v[i] = src[h->bnd_perm[i]];
-        return v;
-    };
+    // ---- tables in the new numbering
+    std::vector<double4> st(nc), cst(nc);
+    std::vector<double2> cxy(nc);
+    for (int64_t i = 0; i < nc; i++) {
+        const int o = h->cell_perm[i];
+        const double zb = mesh->cell_z_b[o];
+        st[i] = make_double4(h0[o], q0[o], r0[o], h0[o] + zb);
+        cst[i] = make_double4(zb, fields->boussinesq[o], fields->phi[o], mesh->cell_area[o]);
+        cxy[i] = make_double2(mesh->cell_x[o], mesh->cell_y[o]);
+    }
     std::vector<int2> lr(ni);
+    std::vector<double2> nxy(ni), mxy(ni);
+    std::vector<double> len(ni);
     for (int64_t i = 0; i < ni; i++) {
-        int oe = h->int_perm[i];
+        const int oe = h->int_perm[i];
         lr[i] = make_int2(inv[mesh->edge_int_cells[2 * oe]], inv[mesh->edge_int_cells[2 * oe + 1]]);
+        nxy[i] = make_double2(mesh->edge_int_nx[oe], mesh->edge_int_ny[oe]);
+        mxy[i] = make_double2(mesh->edge_int_mx[oe], mesh->edge_int_my[oe]);
+        len[i] = mesh->edge_int_length[oe];
     }
     std::vector<int> bcell(nb), bbc(nb);
+    std::vector<double4> bgeo(nb);
     for (int64_t i = 0; i < nb; i++) {
-        bcell[i] = inv[mesh->edge_bnd_cell[h->bnd_perm[i]]];
-        bbc[i] = mesh->edge_bnd_bc[h->bnd_perm[i]];
+        const int oe = h->bnd_perm[i];
+        bcell[i] = inv[mesh->edge_bnd_cell[oe]];
+        bbc[i] = mesh->edge_bnd_bc[oe];
+        bgeo[i] = make_double4(mesh->edge_bnd_nx[oe], mesh->edge_bnd_ny[oe], mesh->edge_bnd_length[oe], 0.0);
     }
     // friction and head-loss angles: degrees -> radians and cos/sin on the host, with the
     // expressions of swSp::setFrictionParameters (swSp.cpp:1063-1068) and
     // sourceSingularHeadLoss (swSpSourceFriction.cpp:185-187)
-    std::vector<double> fcos, fsin, hcos, hsin;
+    std::vector<double4> fric, hla;
+    std::vector<double2> hlb;
     if (params->friction != SW2D_FRICTION_NONE) {
-        fcos.resize(nc);
-        fsin.resize(nc);
+        fric.resize(nc);
         for (int64_t i = 0; i < nc; i++) {
-            double a = fields->friction_alpha[h->cell_perm[i]] * atan(1.0) / 45.0;
-            fcos[i] = cos(a);
-            fsin[i] = sin(a);
+            const int o = h->cell_perm[i];
+            double a = fields->friction_alpha[o] * atan(1.0) / 45.0;
+            fric[i] = make_double4(fields->friction_1[o], fields->friction_2[o], cos(a), sin(a));
         }
     }
     if (params->singular_head_loss) {
-        hcos.resize(nc);
-        hsin.resize(nc);
+        hla.resize(nc);
+        hlb.resize(nc);
         for (int64_t i = 0; i < nc; i++) {
-            double a = fields->hl_alpha[h->cell_perm[i]] * atan(1.0) / 45.0;
-            hcos[i] = cos(a);
-            hsin[i] = sin(a);
+            const int o = h->cell_perm[i];
+            double a = fields->hl_alpha[o] * atan(1.0) / 45.0;
+            hla[i] = make_double4(fields->hl_h_sing[o], fields->hl_coeff_1[o], fields->hl_coeff_2[o], 0.0);
+            hlb[i] = make_double2(cos(a), sin(a));
         }
     }
 
@@ -769,97 +869,59 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     m.nc = (int)nc;
     m.ni = (int)ni;
     m.nb = (int)nb;
-    double* tmp = nullptr;
-    int st = SW2D_OK;
+    int rc = SW2D_OK;
 #define UP(vec, dst)                                        \
     do {                                                    \
-        st = dev_upload(h, vec, &tmp);                      \
-        if (st) return bail(st);                            \
-        dst = tmp;                                          \
+        auto* tmp_ = (decltype(vec.data()))nullptr;         \
+        rc = dev_upload(h, vec, &tmp_);                     \
+        if (rc) return bail(rc);                            \
+        dst = tmp_;                                         \
     } while (0)
-    double *dh, *dq, *dr;
-    UP(cellv(h0, 0), dh);
-    UP(cellv(q0, 0), dq);
-    UP(cellv(r0, 0), dr);
-    m.h = dh;
-    m.q = dq;
-    m.r = dr;
-    UP(cellv(mesh->cell_z_b, 0), m.zb);
-    UP(cellv(mesh->cell_area, 0), m.area);
-    UP(cellv(mesh->cell_x, 0), m.cx);
-    UP(cellv(mesh->cell_y, 0), m.cy);
-    UP(cellv(fields->phi, 1), m.phi);
-    UP(cellv(fields->boussinesq, 1), m.bous);
-    if (params->friction != SW2D_FRICTION_NONE) {
-        UP(cellv(fields->friction_1, 0), m.fk1);
-        UP(cellv(fields->friction_2, 0), m.fk2);
-        UP(fcos, m.fcos);
-        UP(fsin, m.fsin);
+    UP(st, m.st);
+    UP(cst, m.cst);
+    UP(cxy, m.cxy);
+    if (!fric.empty()) UP(fric, m.fric);
+    if (!hla.empty()) {
+        UP(hla, m.hla);
+        UP(hlb, m.hlb);
     }
-    if (params->singular_head_loss) {
-        UP(cellv(fields->hl_h_sing, 0), m.hs);
-        UP(cellv(fields->hl_coeff_1, 0), m.hk1);
-        UP(cellv(fields->hl_coeff_2, 0), m.hk2);
-        UP(hcos, m.hcos);
-        UP(hsin, m.hsin);
-    }
-    UP(intv(mesh->edge_int_length), m.len);
-    UP(intv(mesh->edge_int_nx), m.nx);
-    UP(intv(mesh->edge_int_ny), m.ny);
-    UP(intv(mesh->edge_int_mx), m.mx);
-    UP(intv(mesh->edge_int_my), m.my);
-    UP(bndv(mesh->edge_bnd_length), m.blen);
-    UP(bndv(mesh->edge_bnd_nx), m.bnx);
-    UP(bndv(mesh->edge_bnd_ny), m.bny);
-#undef UP
+    UP(coff, m.coff);
+    UP(cint, m.cint);
+    UP(cbnd, m.cbnd);
+    UP(lr, m.lr);
+    UP(nxy, m.nxy);
+    UP(mxy, m.mxy);
+    UP(len, m.len);
+    UP(bcell, m.bcell);
+    UP(bbc, m.bbc);
+    double4* bgeo_d = nullptr;
+    if ((rc = dev_upload(h, bgeo, &bgeo_d))) return bail(rc);
+    m.bgeo = bgeo_d;
+    UP(h->cell_perm, h->d_cell_perm);
+    UP(h->int_perm, h->d_int_perm);
+    UP(h->bnd_perm, h->d_bnd_perm);
     {
-        int* ip = nullptr;
-        int2* lp = nullptr;
-        if ((st = dev_upload(h, lr, &lp))) return bail(st);
-        m.lr = lp;
-        if ((st = dev_upload(h, bcell, &ip))) return bail(st);
-        m.bcell = ip;
-        if ((st = dev_upload(h, bbc, &ip))) return bail(st);
-        m.bbc = ip;
-        if ((st = dev_upload(h, cb_off, &ip))) return bail(st);
-        m.cb_off = ip;
-        if ((st = dev_upload(h, cb_idx, &ip))) return bail(st);
-        m.cb_idx = ip;
-        if ((st = dev_upload(h, ci_off, &ip))) return bail(st);
-        m.ci_off = ip;
-        if ((st = dev_upload(h, ci_ent, &ip))) return bail(st);
-        m.ci_ent = ip;
-        if ((st = dev_upload(h, ci_nbr, &ip))) return bail(st);
-        m.ci_nbr = ip;
-        if ((st = dev_upload(h, h->cell_perm, &h->d_cell_perm))) return bail(st);
-        if ((st = dev_upload(h, h->int_perm, &h->d_int_perm))) return bail(st);
-        if ((st = dev_upload(h, h->bnd_perm, &h->d_bnd_perm))) return bail(st);
         std::vector<int> bct(bc->type, bc->type + bc->bc_nb);
         std::vector<long long> bco(bc->offset, bc->offset + bc->bc_nb + 1);
-        int64_t nrec = bc->offset[bc->bc_nb];
+        const int64_t nrec = bc->offset[bc->bc_nb];
         std::vector<double> bt(bc->times, bc->times + nrec), bv(bc->values, bc->values + nrec);
-        if ((st = dev_upload(h, bct, &ip))) return bail(st);
-        m.bctype = ip;
-        long long* lp2 = nullptr;
-        if ((st = dev_upload(h, bco, &lp2))) return bail(st);
-        m.bcoff = lp2;
-        if ((st = dev_upload(h, bt, &tmp))) return bail(st);
-        m.bctimes = tmp;
-        if ((st = dev_upload(h, bv, &tmp))) return bail(st);
-        m.bcvals = tmp;
+        UP(bct, m.bctype);
+        UP(bco, m.bcoff);
+        UP(bt, m.bctimes);
+        UP(bv, m.bcvals);
     }
-    double *cl, *cr, *cbf;
-    if ((st = dev_alloc(h, ni, &cl)) || (st = dev_alloc(h, ni, &cr)) || (st = dev_alloc(h, nb, &cbf))) return bail(st);
-    m.coefL = cl;
-    m.coefR = cr;
-    m.bcoef = cbf;
-    // persistent flux arrays start at zero, like the reference's resized member vectors
-    if ((st = dev_alloc(h, ni, &m.F1)) || (st = dev_alloc(h, ni, &m.F2)) || (st = dev_alloc(h, ni, &m.F3)) ||
-        (st = dev_alloc(h, ni, &m.S2L)) || (st = dev_alloc(h, ni, &m.S2R)) || (st = dev_alloc(h, ni, &m.lmax)) ||
-        (st = dev_alloc(h, nb, &m.F1b)) || (st = dev_alloc(h, nb, &m.F2b)) || (st = dev_alloc(h, nb, &m.F3b)) ||
-        (st = dev_alloc(h, nb, &m.lmaxb)) || (st = dev_alloc(h, nc, &m.sx)) || (st = dev_alloc(h, nc, &m.sy)) ||
-        (st = dev_alloc(h, grid_for(nc) + 1, &m.part)) || (st = dev_alloc(h, 3 * nc, &h->stage)))
-        return bail(st);
+#undef UP
+    double2* coef_d = nullptr;
+    if ((rc = dev_alloc(h, ni, &coef_d))) return bail(rc);
+    m.coef = coef_d;
+    // persistent flux records start at zero, like the reference's resized member vectors
+    if ((rc = dev_alloc(h, 3 * ni, &m.flux)) || (rc = dev_alloc(h, ni, &m.swc)) || (rc = dev_alloc(h, nb, &m.bflux)) ||
+        (rc = dev_alloc(h, nb, &m.bswc)) || (rc = dev_alloc(h, nc, &m.slope)) ||
+        (rc = dev_alloc(h, grid_for(nc) + 1, &m.part)) || (rc = dev_alloc(h, 3 * nc, &h->stage)) ||
+        (rc = dev_alloc(h, ni, &h->lmax_buf)) || (rc = dev_alloc(h, nb, &h->lmaxb_buf)))
+        return bail(rc);
+    m.lmax = nullptr;
+    m.lmaxb = nullptr;
     m.h_min = params->h_min;
     m.phi_min = params->phi_min;
     m.cfl_max = params->cfl_max;
@@ -867,10 +929,6 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     m.dt_map = params->dt_map;
     m.v_max = params->v_max;
     m.fr_max = params->fr_max;
-    m.scheme = params->scheme;
-    m.topo = params->topo;
-    m.friction = params->friction;
-    m.head_loss = params->singular_head_loss ? 1 : 0;
     m.neg_detect = params->negative_depth_detection ? 1 : 0;
     if (cudaMalloc(&h->ctrl, sizeof(Ctrl)) != cudaSuccess) return bail(fail(h, SW2D_E_CUDA, "cudaMalloc ctrl"));
     h->allocs.push_back(h->ctrl);
@@ -883,7 +941,7 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     *h->ctrl_host = c0;
     if (cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
         return bail(fail(h, SW2D_E_CUDA, "ctrl upload"));
-    k_edge_coefficients<<<grid_for(ni + nb), kBlock, 0, h->stream>>>(m, cl, cr, cbf);
+    k_edge_coefficients<<<grid_for(ni + nb), kBlock, 0, h->stream>>>(m, coef_d, bgeo_d);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return bail(fail(h, SW2D_E_CUDA, "initialisation kernels failed"));
     *out = h;
@@ -898,7 +956,7 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
     CK(cudaStreamSynchronize(h->stream));
     const long long before = h->ctrl_host->steps;
     const int chunk = 32;
-    int64_t full = n_steps / chunk, rem = n_steps % chunk;
+    const int64_t full = n_steps / chunk, rem = n_steps % chunk;
     if (full > 0) {
         int st = ensure_graph(h, chunk);
         if (st) return st;
@@ -939,18 +997,13 @@ int sw2d_phase_times(sw2d_handle* h, int64_t n_steps, double* ms, int capacity)
     cudaEvent_t ev[nph + 1];
     for (int i = 0; i <= nph; i++) CK(cudaEventCreate(&ev[i]));
     double acc[nph] = {0, 0, 0, 0};
-    DevMesh& m = h->m;
     for (int64_t s = 0; s < n_steps; s++) {
-        cudaEventRecord(ev[0], h->stream);
-        if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) k_slopes<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
-        cudaEventRecord(ev[1], h->stream);
-        k_edges<<<grid_for((long long)m.ni + m.nb), kBlock, 0, h->stream>>>(m);
-        cudaEventRecord(ev[2], h->stream);
-        k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
-        cudaEventRecord(ev[3], h->stream);
-        k_update<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
-        cudaEventRecord(ev[4], h->stream);
-        CK(cudaEventSynchronize(ev[4]));
+        for (int i = 0; i < nph; i++) {
+            cudaEventRecord(ev[i], h->stream);
+            launch_phase(h, i);
+        }
+        cudaEventRecord(ev[nph], h->stream);
+        CK(cudaEventSynchronize(ev[nph]));
         for (int i = 0; i < nph; i++) {
             float t = 0.f;
             cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
@@ -972,11 +1025,26 @@ const char* sw2d_phase_name(int i)
     return (i >= 0 && i < 4) ? names[i] : "";
 }
 
+int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
+{
+    if (!h || !name) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (std::strcmp(name, "record_wave_speeds") == 0) {
+        h->m.lmax = value ? h->lmax_buf : nullptr;
+        h->m.lmaxb = value ? h->lmaxb_buf : nullptr;
+        if (h->graph) {  // the captured kernels hold the previous parameters
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+        }
+        return SW2D_OK;
+    }
+    return fail(h, SW2D_E_ARG, std::string("unknown option ") + name);
+}
+
 int sw2d_get_state_device(sw2d_handle* h, double* dh, double* dq, double* dr)
 {
     if (!h || !dh || !dq || !dr) return fail(h, SW2D_E_ARG, "invalid arguments");
     CK(cudaSetDevice(h->device));
-    k_scatter3<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m.h, h->m.q, h->m.r, h->d_cell_perm, dh, dq, dr, (int)h->nc);
+    k_scatter_state<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m.st, h->d_cell_perm, dh, dq, dr, (int)h->nc);
     CK(cudaGetLastError());
     return SW2D_OK;
 }
@@ -985,7 +1053,7 @@ int sw2d_set_state_device(sw2d_handle* h, const double* dh, const double* dq, co
 {
     if (!h || !dh || !dq || !dr) return fail(h, SW2D_E_ARG, "invalid arguments");
     CK(cudaSetDevice(h->device));
-    k_gather3<<<grid_for(h->nc), kBlock, 0, h->stream>>>(dh, dq, dr, h->d_cell_perm, h->m.h, h->m.q, h->m.r, (int)h->nc);
+    k_gather_state<<<grid_for(h->nc), kBlock, 0, h->stream>>>(dh, dq, dr, h->d_cell_perm, h->m.cst, h->m.st, (int)h->nc);
     CK(cudaGetLastError());
     return SW2D_OK;
 }
@@ -995,7 +1063,7 @@ int sw2d_get_state(sw2d_handle* h, double* wd, double* qx, double* qy)
     if (!h || !wd || !qx || !qy) return fail(h, SW2D_E_ARG, "invalid arguments");
     int st = sw2d_get_state_device(h, h->stage, h->stage + h->nc, h->stage + 2 * h->nc);
     if (st) return st;
-    size_t bytes = h->nc * sizeof(double);
+    const size_t bytes = h->nc * sizeof(double);
     CK(cudaMemcpyAsync(wd, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(qx, h->stage + h->nc, bytes, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(qy, h->stage + 2 * h->nc, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -1007,7 +1075,7 @@ int sw2d_set_state(sw2d_handle* h, const double* wd, const double* qx, const dou
 {
     if (!h || !wd || !qx || !qy) return fail(h, SW2D_E_ARG, "invalid arguments");
     CK(cudaSetDevice(h->device));
-    size_t bytes = h->nc * sizeof(double);
+    const size_t bytes = h->nc * sizeof(double);
     CK(cudaMemcpyAsync(h->stage, wd, bytes, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->stage + h->nc, qx, bytes, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->stage + 2 * h->nc, qy, bytes, cudaMemcpyHostToDevice, h->stream));
@@ -1047,23 +1115,31 @@ int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t ca
     struct Entry {
         const char* n;
         const double* p;
+        int stride, offset;
         int64_t len;
         const int* perm;
     } tab[] = {
-        {"F1_int", h->m.F1, h->ni, h->d_int_perm},        {"F2_int", h->m.F2, h->ni, h->d_int_perm},
-        {"F3_int", h->m.F3, h->ni, h->d_int_perm},        {"s2L_int", h->m.S2L, h->ni, h->d_int_perm},
-        {"s2R_int", h->m.S2R, h->ni, h->d_int_perm},      {"lambda_max_int", h->m.lmax, h->ni, h->d_int_perm},
-        {"F1_bnd", h->m.F1b, h->nb, h->d_bnd_perm},       {"F2_bnd", h->m.F2b, h->nb, h->d_bnd_perm},
-        {"F3_bnd", h->m.F3b, h->nb, h->d_bnd_perm},       {"lambda_max_bnd", h->m.lmaxb, h->nb, h->d_bnd_perm},
-        {"slope_x", h->m.sx, h->nc, h->d_cell_perm},      {"slope_y", h->m.sy, h->nc, h->d_cell_perm},
+        {"F1_int", (const double*)h->m.flux, 6, 0, h->ni, h->d_int_perm},
+        {"F2_int", (const double*)h->m.flux, 6, 1, h->ni, h->d_int_perm},
+        {"F3_int", (const double*)h->m.flux, 6, 2, h->ni, h->d_int_perm},
+        {"s2L_int", (const double*)h->m.flux, 6, 3, h->ni, h->d_int_perm},
+        {"s2R_int", (const double*)h->m.flux, 6, 4, h->ni, h->d_int_perm},
+        {"F1_bnd", (const double*)h->m.bflux, 4, 0, h->nb, h->d_bnd_perm},
+        {"F2_bnd", (const double*)h->m.bflux, 4, 1, h->nb, h->d_bnd_perm},
+        {"F3_bnd", (const double*)h->m.bflux, 4, 2, h->nb, h->d_bnd_perm},
+        {"lambda_max_int", h->m.lmax, 1, 0, h->ni, h->d_int_perm},
+        {"lambda_max_bnd", h->m.lmaxb, 1, 0, h->nb, h->d_bnd_perm},
+        {"slope_x", (const double*)h->m.slope, 2, 0, h->nc, h->d_cell_perm},
+        {"slope_y", (const double*)h->m.slope, 2, 1, h->nc, h->d_cell_perm},
     };
     for (const Entry& e : tab) {
         if (std::strcmp(e.n, name) != 0) continue;
+        if (!e.p) return fail(h, SW2D_E_ARG, "wave speeds are recorded only with the option record_wave_speeds");
         if (capacity < e.len) return fail(h, SW2D_E_ARG, "output buffer too small");
         CK(cudaSetDevice(h->device));
         double* tmp = nullptr;
         CK(cudaMalloc(&tmp, std::max<int64_t>(1, e.len) * sizeof(double)));
-        k_scatter1<<<grid_for(e.len), kBlock, 0, h->stream>>>(e.p, e.perm, tmp, (int)e.len);
+        k_scatter_strided<<<grid_for(e.len), kBlock, 0, h->stream>>>(e.p, e.stride, e.offset, e.perm, tmp, (int)e.len);
         cudaError_t ce = cudaMemcpyAsync(out, tmp, e.len * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
         cudaStreamSynchronize(h->stream);
         cudaFree(tmp);
@@ -1091,6 +1167,32 @@ int sw2d_kernels_per_step(sw2d_handle* h)
 {
     if (!h) return 0;
     return h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3;
+}
+
+int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n)
+{
+    sw2d_handle* h = nullptr;
+    if (!x || !y || n < 0 || fn < 0 || fn > 3) return fail(h, SW2D_E_ARG, "invalid arguments");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(h, SW2D_E_NO_DEVICE, "no usable CUDA device");
+    CK(cudaSetDevice(device));
+    double *dx = nullptr, *dy = nullptr;
+    CK(cudaMalloc(&dx, std::max<int64_t>(1, n) * sizeof(double)));
+    if (cudaMalloc(&dy, std::max<int64_t>(1, n) * sizeof(double)) != cudaSuccess) {
+        cudaFree(dx);
+        return fail(h, SW2D_E_CUDA, "cudaMalloc");
+    }
+    cudaError_t e = cudaMemcpy(dx, x, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n > 0) {
+        k_eval_math<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock>>>(fn, dx, dy, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, dy, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dy);
+    if (e != cudaSuccess) return fail(h, SW2D_E_CUDA, cudaGetErrorString(e));
+    return SW2D_OK;
 }
 
 int sw2d_destroy(sw2d_handle* h)

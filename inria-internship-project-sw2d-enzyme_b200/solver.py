@@ -124,6 +124,9 @@ class SpModel:
             self._check(int(k))
         return {self.lib.sw2d_phase_name(i).decode(): float(ms[i]) for i in range(k)}
 
+    def set_option(self, name: str, value: int) -> None:
+        self._check(self.lib.sw2d_set_option(self.handle, name.encode(), int(value)))
+
     @property
     def stream(self) -> int:
         return int(self.lib.sw2d_get_stream(self.handle) or 0)
@@ -142,6 +145,20 @@ class SpModel:
             self.close()
         except Exception:
             pass
+
+
+def eval_math(fn: str, x, device: int = 0) -> np.ndarray:
+    """Device evaluation of the step's elementary functions: fn in ("exp", "log") for the
+    portable versions the step uses, ("cuda_exp", "cuda_log") for CUDA's."""
+    lib = capi.load_library()
+    code = {"exp": 0, "log": 1, "cuda_exp": 2, "cuda_log": 3}[fn]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    st = lib.sw2d_eval_math(int(device), code, x.ctypes.data_as(capi.c_double_p), y.ctypes.data_as(capi.c_double_p),
+                            x.size)
+    if st != 0:
+        raise Sw2dError(st, lib.sw2d_last_error(None).decode())
+    return y
 
 
 def run_case(folder: str, device: int = 0, n_steps: Optional[int] = None):

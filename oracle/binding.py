@@ -16,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libsp_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libsw2d_ref.so")
+REF_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_pm.so")
 REF_BIN = os.path.join(HERE, "_ref", "sw2dSolver")
 REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "/root/reference")
 
@@ -59,13 +60,15 @@ def _oracle_lib():
     lib.spo_get_array.argtypes = [_P, ctypes.c_char_p, _D]
     lib.spo_get_array.restype = ctypes.c_long
     lib.spo_destroy.argtypes = [_P]
+    lib.spo_set_portable_math.argtypes = [_P, ctypes.c_int]
     return lib
 
 
 class SpOracle:
-    """The C restatement of the native SP step on a :class:`Case`."""
+    """The C restatement of the native SP step on a :class:`Case`.  ``portable_math`` selects the
+    portable exp/log of the CUDA build instead of the host libm."""
 
-    def __init__(self, case):
+    def __init__(self, case, portable_math: bool = False):
         self.lib = _oracle_lib()
         self.case = case
         self.n = case.mesh.cell_nb
@@ -73,6 +76,7 @@ class SpOracle:
         i = self._in
         self.h = self.lib.spo_create(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
                                      ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0), capi._dp(i.r0))
+        self.lib.spo_set_portable_math(self.h, 1 if portable_math else 0)
 
     def step(self, n: int) -> int:
         k = self.lib.spo_step(self.h, int(n))
@@ -112,12 +116,14 @@ class SpOracle:
 
 
 class RefSolver:
-    """The reference's native SP solver (built from its own sources) on a case folder."""
+    """The reference's native SP solver (built from its own sources) on a case folder.
+    ``portable_math`` loads the build linked with the portable exp/log of the CUDA build."""
 
-    def __init__(self, folder: str, quiet: bool = True):
-        if not os.path.exists(REF_SO):
-            raise RuntimeError("reference library not built (oracle/_ref/libsw2d_ref.so)")
-        lib = ctypes.CDLL(REF_SO)
+    def __init__(self, folder: str, quiet: bool = True, portable_math: bool = False):
+        so = REF_PM_SO if portable_math else REF_SO
+        if not os.path.exists(so):
+            raise RuntimeError(f"reference library not built ({so})")
+        lib = ctypes.CDLL(so)
         lib.sw2dref_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
         lib.sw2dref_open.restype = _P
         lib.sw2dref_step.argtypes = [_P, ctypes.c_int]

@@ -18,8 +18,16 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "../inria-internship-project-sw2d-enzyme_b200/csrc/portable_math.h"
+
 #define SMALL_REAL 1e-16 /* src/common/param.h:2 */
 #define GRAVITY 9.81     /* src/common/param.h:3 */
+
+/* exp/log used by the step: the host libm (as the reference built with g++), or the portable
+ * versions the CUDA build uses (spo_set_portable_math) */
+typedef double (*math_fn)(double);
+static double pm_exp(double x) { return sw2d_exp(x); }
+static double pm_log(double x) { return sw2d_log(x); }
 
 static inline double smax(double a, double b) { return (a < b) ? b : a; } /* std::max */
 static inline double smin(double a, double b) { return (b < a) ? b : a; } /* std::min */
@@ -57,6 +65,7 @@ struct sp_oracle {
     double *F1b, *F2b, *F3b, *S2b;
     double *F1, *F2, *F3, *S2L, *S2R;
     double *sx, *sy, *zc, *swept;
+    math_fn fexp, flog;
 };
 
 static double* dup_or(const double* src, long n, double fill)
@@ -163,7 +172,15 @@ sp_oracle* spo_create(const sw2d_mesh* m, const sw2d_params* p, const sw2d_cell_
     o->F1b = zeros(nb); o->F2b = zeros(nb); o->F3b = zeros(nb); o->S2b = zeros(nb);
     o->F1 = zeros(ni); o->F2 = zeros(ni); o->F3 = zeros(ni); o->S2L = zeros(ni); o->S2R = zeros(ni);
     o->sx = zeros(nc); o->sy = zeros(nc); o->zc = zeros(nc); o->swept = zeros(nc);
+    o->fexp = exp;
+    o->flog = log;
     return o;
+}
+
+void spo_set_portable_math(sp_oracle* o, int on)
+{
+    o->fexp = on ? pm_exp : exp;
+    o->flog = on ? pm_log : log;
 }
 
 /* swSp::lambdaMinus / lambdaPlus (swSp.cpp:972-995) */
@@ -373,7 +390,10 @@ static double bc_value(const sp_oracle* o, int k, double time)
 }
 
 /* swSp::hypHCritical (swSpHyp.cpp:651-661) */
-static double h_critical(double phi, double q) { return exp((1. / 3.) * log((q / smax(phi, SMALL_REAL)) / GRAVITY)); }
+static double h_critical(const sp_oracle* o, double phi, double q)
+{
+    return o->fexp((1. / 3.) * o->flog((q / smax(phi, SMALL_REAL)) / GRAVITY));
+}
 
 /* swSp::hypBoundaryFlux (swSpHyp.cpp:13-135); source_right stays 0. */
 static int boundary_flux(const sp_oracle* o, double bR, double phiR, double zbR, double zR, double qR, double rR,
@@ -407,7 +427,7 @@ static int boundary_flux(const sp_oracle* o, double bR, double phiR, double zbR,
         }
     } else if (type == SW2D_BC_Q) {
         flux1 = bcv;
-        double hc = h_critical(phiR, bcv);
+        double hc = h_critical(o, phiR, bcv);
         if (hc >= hR) flux1 = phiR * 1.5 * sqrt(GRAVITY * hc) * hc;
         flux2 = flux2R + (flux1 - q1 * phiR) * L1;
     } else {
@@ -564,8 +584,9 @@ static void balance(sp_oracle* o, double dt)
 
 /* swSource::frictionChezy1D / frictionManning1D / frictionStrickler1D
  * (models/common/swSourceFriction.cpp:7-79) */
-static double friction_factor(int model, double k, double h, double un, double dt)
+static double friction_factor(const sp_oracle* o, int model, double k, double h, double un, double dt)
 {
+    math_fn exp = o->fexp, log = o->flog;
     double factor = 1.0;
     if (model == SW2D_FRICTION_CHEZY) {
         if ((h > SMALL_REAL) && (k > SMALL_REAL)) factor = exp(-GRAVITY * un / k / k / h * dt);
@@ -593,8 +614,8 @@ static void friction(sp_oracle* o, double dt)
             double ul = u * ca + v * sa;
             double vl = -u * sa + v * ca;
             double un = sqrt(u * u + v * v);
-            double f1 = friction_factor(o->p.friction, o->fr1[c], h, un, dt);
-            double f2 = friction_factor(o->p.friction, o->fr2[c], h, un, dt);
+            double f1 = friction_factor(o, o->p.friction, o->fr1[c], h, un, dt);
+            double f2 = friction_factor(o, o->p.friction, o->fr2[c], h, un, dt);
             ul *= f1;
             vl *= f2;
             o->q[c] = (ul * ca - vl * sa) * h;
@@ -621,8 +642,8 @@ static void head_loss(sp_oracle* o, double dt)
                 ax = sqrt(qx * qx + qy * qy) * o->hk1[c] / h;
                 ay = sqrt(qx * qx + qy * qy) * o->hk2[c] / h;
             }
-            qx = qx * exp(-ax * dt);
-            qy = qy * exp(-ay * dt);
+            qx = qx * o->fexp(-ax * dt);
+            qy = qy * o->fexp(-ay * dt);
         } else {
             qx = 0.;
             qy = 0.;

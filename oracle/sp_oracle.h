@@ -30,6 +30,9 @@ double spo_dt(const sp_oracle* o);
 void spo_set_time(sp_oracle* o, double t, double dt);
 /* Same names as sw2d_get_array; returns the element count, or -1 for an unknown name. */
 long spo_get_array(const sp_oracle* o, const char* name, double* out);
+/* 0: exp/log of the host libm (default, as the reference); 1: the portable exp/log of the
+ * CUDA build (inria-internship-project-sw2d-enzyme_b200/csrc/portable_math.h). */
+void spo_set_portable_math(sp_oracle* o, int on);
 void spo_destroy(sp_oracle* o);
 
 #ifdef __cplusplus

@@ -7,6 +7,11 @@ its own sources (oracle/Makefile -> oracle/_ref/libsw2d_ref.so), on:
   only; the fixture stores the mesh tables and parameters the SP step reads, and the
   reference's state after 100 steps and at t_max).
 
+Each state is recorded twice: from the reference linked with the host libm (glibc, fields
+h/q/r...) and from the same reference objects linked with the portable exp/log of the CUDA
+build (oracle/_ref/libsw2d_ref_pm.so, fields ..._pm).  ``libm_stable`` records whether the two
+agree within 1e-10 (relative, infinity norm; discharges scaled by max(|q|max, h_max sqrt(g h_max))).
+
 Run here (the reference tree must be present):  python tests/golden/make_golden.py
 """
 from __future__ import annotations
@@ -63,6 +68,25 @@ def case_digest(case) -> str:
     return h.hexdigest()
 
 
+def state_rel_err(got, want) -> float:
+    """max over (h, q, r) of the infinity-norm relative error; discharges are scaled by
+    max(|q|max, Q) with Q = h_max sqrt(g h_max), the discharge of the deepest water at the wave
+    speed, so that fields at rest (round-off-sized q) are judged on the flow's own scale."""
+    h = np.asarray(want[0])
+    hmax = float(np.max(np.abs(h))) if h.size else 0.0
+    qs = hmax * np.sqrt(9.81 * hmax)
+    errs = []
+    for k, (a, b) in enumerate(zip(got, want)):
+        a = np.asarray(a, dtype=np.float64)
+        b = np.asarray(b, dtype=np.float64)
+        d = float(np.max(np.abs(a - b))) if a.size else 0.0
+        scale = float(np.max(np.abs(b))) if b.size else 0.0
+        if k > 0:
+            scale = max(scale, qs)
+        errs.append(0.0 if d == 0.0 else d / max(scale, 1e-300))
+    return max(errs)
+
+
 def main():
     from oracle.binding import RefSolver, build, reference_available
     build(reference=True)
@@ -76,9 +100,16 @@ def main():
             ref = RefSolver(folder)
             done = ref.step(STEPS)
             h, q, r = ref.state()
+            pm = RefSolver(folder, portable_math=True)
+            done_pm = pm.step(STEPS)
+            hp, qp, rp = pm.state()
+            stable = state_rel_err((h, q, r), (hp, qp, rp)) <= 1e-10
             np.savez_compressed(os.path.join(HERE, f"{name}.npz"), builder=builder, kwargs=json.dumps(kwargs),
-                                digest=case_digest(case), steps=done, t=ref.t, dt=ref.dt, h=h, q=q, r=r)
-            print(name, case.mesh.cell_nb, done, ref.t)
+                                digest=case_digest(case), steps=done, t=ref.t, dt=ref.dt, h=h, q=q, r=r,
+                                steps_pm=done_pm, t_pm=pm.t, dt_pm=pm.dt, h_pm=hp, q_pm=qp, r_pm=rp,
+                                libm_stable=stable)
+            print(name, case.mesh.cell_nb, done, ref.t, "libm-stable" if stable else "libm-sensitive",
+                  "%.2e" % state_rel_err((h, q, r), (hp, qp, rp)))
 
         src = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
         folder = os.path.join(tmp, "sp_toce")
@@ -93,6 +124,12 @@ def main():
         t100 = ref.t
         s_end = s100 + ref.step(10 ** 7)
         h, q, r = ref.state()
+        pm = RefSolver(folder, portable_math=True)
+        pm.step(100)
+        h100p, q100p, r100p = pm.state()
+        t100p = pm.t
+        s_end_p = 100 + pm.step(10 ** 7)
+        hp, qp, rp = pm.state()
         m = case.mesh
         np.savez_compressed(
             os.path.join(HERE, "sp_toce.npz"), opts=json.dumps(case.opts),
@@ -105,8 +142,11 @@ def main():
             boussinesq=case.boussinesq, friction=case.friction, head_loss=case.head_loss,
             bc_codes=np.array(case.bc.codes), bc_types=json.dumps(case.bc.types), bc_times=case.bc.times,
             bc_values=case.bc.values, steps100=s100, t100=t100, h100=h100, q100=q100, r100=r100,
-            steps_end=s_end, t_end=ref.t, h_end=h, q_end=q, r_end=r)
-        print("sp_toce", m.cell_nb, s100, s_end, ref.t)
+            steps_end=s_end, t_end=ref.t, h_end=h, q_end=q, r_end=r,
+            t100_pm=t100p, h100_pm=h100p, q100_pm=q100p, r100_pm=r100p,
+            steps_end_pm=s_end_p, t_end_pm=pm.t, h_end_pm=hp, q_end_pm=qp, r_end_pm=rp,
+            libm_stable=state_rel_err((h, q, r), (hp, qp, rp)) <= 1e-10)
+        print("sp_toce", m.cell_nb, s100, s_end, ref.t, "%.2e" % state_rel_err((h, q, r), (hp, qp, rp)))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 
