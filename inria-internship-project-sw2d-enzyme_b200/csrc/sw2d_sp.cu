@@ -17,10 +17,18 @@
 // Data layout (all in HBM, internal numbering): the state of a cell is one 32-byte record
 // {h, q, r, z = h + z_b} so that a neighbour gather touches one sector; cell statics
 // {z_b, boussinesq, phi, area}, centroids {x, y} and slopes {sx, sy} are 32/16-byte records;
-// edges keep {L, R}, normals {nx, ny}, midpoints {mx, my}, edge-factor coefficients
-// {w/(A_L phi_L), w/(A_R phi_R)} and a 48-byte flux record {F1, F2, F3, S2L, S2R, -}.  The flux
-// records persist between steps: the reference keeps the previous fluxes of an edge whose two
-// sides are dry (swSpHyp.cpp:339).
+// edges keep {L, R}, normals {nx, ny}, midpoints {mx, my} and the edge-factor coefficients
+// {w/(A_L phi_L), w/(A_R phi_R)}.
+//
+// Balance slots.  The reference adds each edge's contribution to a cell as
+//   h += (factor * F1) * dt,  q += (f2F2*F2 + f2S2*S2 + f2F3*F3) * dt,  r += (...) * dt
+// (swSpHyp.cpp:221-263): the products before "* dt" do not depend on dt.  k_edges therefore
+// writes, for every (cell, edge) pair, the three dt-free terms {a, b, c} into a per-cell slot
+// range laid out in the reference's summation order (boundary edges, then internal edges, by
+// increasing original index), plus the edge's CFL contribution.  k_cfl and k_update then read
+// their cell's slots contiguously, without any gather.  The slots persist between steps: the
+// reference keeps the previous fluxes of an edge whose two sides are dry (swSpHyp.cpp:339), and
+// since the factors are static, keeping the previous {a, b, c} is the same thing.
 //
 // Cells are renumbered along a Hilbert curve and internal edges by their first cell, for
 // locality; every per-cell sum still runs in the reference's order (boundary edges, then
@@ -68,24 +76,27 @@ struct DevMesh {
     const double4* fric;     // {k1, k2, cos a, sin a} (friction)
     const double4* hla;      // {h_sing, k1, k2, -} (singular head loss)
     const double2* hlb;      // {cos a, sin a}
-    const int2* coff;        // [nc+1] {first internal entry, first boundary entry}
-    const int2* cint;        // {edge*2 + side, neighbour}
-    const int* cbnd;         // boundary edge
+    const double* zbv;       // z_b
+    const double* area;
+    const int2* coff;        // [nc+1] {first internal-neighbour entry, first balance slot}
+    const int2* cint;        // {edge*2 + side, neighbour} (MUSCL slopes)
+    double4* slot;           // balance slots {a, b, c, -}
+    double* slot_w;          // CFL contribution of the slot
     // internal edges
     const int2* lr;
+    const int2* eslot;       // {slot of (L, e), slot of (R, e)}
     const double2* nxy;
     const double2* mxy;
     const double* len;
     const double2* coef;     // {coefL, coefR}
-    double2* flux;           // 3 x double2 per edge: {F1,F2},{F3,S2L},{S2R,-}
-    double2* swc;            // {lambda_max*len counted for L, for R}
+    double2* flux;           // optional copy: 3 x double2 per edge {F1,F2},{F3,S2L},{S2R,-} (tests)
     double* lmax;            // optional copy of lambda_max (tests)
     // boundary edges
     const int* bcell;
     const int* bbc;
+    const int* bslot;
     const double4* bgeo;     // {nx, ny, length, coef}
-    double4* bflux;          // {F1, F2, F3, -}
-    double* bswc;            // lambda_max*len when the cell is wet, else 0
+    double4* bflux;          // optional copy {F1, F2, F3, -} (tests)
     double* lmaxb;           // optional copy of lambda_max (tests)
     // boundary series
     const int* bctype;
@@ -117,7 +128,43 @@ __device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_
 // neighbour contributions in increasing internal-edge order; step 2 applies, edge after edge
 // in the same order, the under/overshoot rescaling of this cell's slope (that rescaling only
 // reads this cell's slope, so the reference's global edge loop decomposes exactly per cell).
+// Cells with up to kUnroll neighbours issue all their neighbour loads up front.
 // ------------------------------------------------------------------------------------------
+constexpr int kUnroll = 4;        // balance slots handled without a loop (cell degree)
+constexpr int kUnrollSlopes = 3;  // neighbours gathered up front in k_slopes (triangles)
+
+__device__ __forceinline__ void limit_slope(double zc, double zj, bool is_r, double2 mp, double2 xy, double& sx,
+                                            double& sy)
+{
+    const double zL = is_r ? zj : zc;
+    const double zR = is_r ? zc : zj;
+    const double fmx = smax(zL, zR);
+    const double fmn = smin(zL, zR);
+    const double rec = zc + (mp.x - xy.x) * sx + (mp.y - xy.y) * sy;
+    if (rec < fmn) {
+        double fac = (fmn - zc) / (rec - zc);
+        sx *= fac;
+        sy *= fac;
+    }
+    if (rec > fmx) {
+        double fac = (fmx - zc) / (rec - zc);
+        sx *= fac;
+        sy *= fac;
+    }
+}
+
+__device__ __forceinline__ void grad_term(double zc, double zj, double2 xy, double2 xj, double& sx, double& sy,
+                                          double& wsum)
+{
+    double dx = xj.x - xy.x;
+    double dy = xj.y - xy.y;
+    double dist = sqrt(dx * dx + dy * dy);
+    double w = 1.0 / dist;
+    sx += (zj - zc) * dx / dist / dist * w;
+    sy += (zj - zc) * dy / dist / dist * w;
+    wsum += w;
+}
+
 __global__ void __launch_bounds__(kBlock, 4) k_slopes(DevMesh m)
 {
     if (!step_active(m.ctrl)) return;
@@ -125,53 +172,52 @@ __global__ void __launch_bounds__(kBlock, 4) k_slopes(DevMesh m)
     if (c >= m.nc) return;
     const double zc = ld(&m.st[c].w);
     const double2 xy = ld(&m.cxy[c]);
-    const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
-    const int k0 = o0.x, k1 = o1.x;
+    const int k0 = ld(&m.coff[c].x), k1 = ld(&m.coff[c + 1].x);
+    const int cnt = k1 - k0;
     double sx = 0.0, sy = 0.0, wsum = 0.0;
-    if (k1 - k0 > 1) {
+    if (cnt <= kUnrollSlopes) {
+        int2 en[kUnrollSlopes];
+        double zj[kUnrollSlopes];
+        double2 xj[kUnrollSlopes];
+#pragma unroll
+        for (int i = 0; i < kUnrollSlopes; i++)
+            if (i < cnt) en[i] = ld(&m.cint[k0 + i]);
+#pragma unroll
+        for (int i = 0; i < kUnrollSlopes; i++)
+            if (i < cnt) {
+                zj[i] = ld(&m.st[en[i].y].w);
+                xj[i] = ld(&m.cxy[en[i].y]);
+            }
+        if (cnt > 1) {
+#pragma unroll
+            for (int i = 0; i < kUnrollSlopes; i++)
+                if (i < cnt) grad_term(zc, zj[i], xy, xj[i], sx, sy, wsum);
+            sx /= wsum;
+            sy /= wsum;
+        }
+#pragma unroll
+        for (int i = 0; i < kUnrollSlopes; i++)
+            if (i < cnt) limit_slope(zc, zj[i], en[i].x & 1, ld(&m.mxy[en[i].x >> 1]), xy, sx, sy);
+    } else {
         for (int k = k0; k < k1; k++) {
             const int j = ld(&m.cint[k]).y;
-            const double2 xj = ld(&m.cxy[j]);
-            double dx = xj.x - xy.x;
-            double dy = xj.y - xy.y;
-            double dist = sqrt(dx * dx + dy * dy);
-            double w = 1.0 / dist;
-            double zj = ld(&m.st[j].w);
-            sx += (zj - zc) * dx / dist / dist * w;
-            sy += (zj - zc) * dy / dist / dist * w;
-            wsum += w;
+            grad_term(zc, ld(&m.st[j].w), xy, ld(&m.cxy[j]), sx, sy, wsum);
         }
         sx /= wsum;
         sy /= wsum;
-    }
-    for (int k = k0; k < k1; k++) {
-        const int2 en = ld(&m.cint[k]);
-        const int e = en.x >> 1;
-        const double zj = ld(&m.st[en.y].w);
-        const double zL = (en.x & 1) ? zj : zc;
-        const double zR = (en.x & 1) ? zc : zj;
-        const double fmx = smax(zL, zR);
-        const double fmn = smin(zL, zR);
-        const double2 mp = ld(&m.mxy[e]);
-        const double rec = zc + (mp.x - xy.x) * sx + (mp.y - xy.y) * sy;
-        if (rec < fmn) {
-            double fac = (fmn - zc) / (rec - zc);
-            sx *= fac;
-            sy *= fac;
-        }
-        if (rec > fmx) {
-            double fac = (fmx - zc) / (rec - zc);
-            sx *= fac;
-            sy *= fac;
+        for (int k = k0; k < k1; k++) {
+            const int2 en = ld(&m.cint[k]);
+            limit_slope(zc, ld(&m.st[en.y].w), en.x & 1, ld(&m.mxy[en.x >> 1]), xy, sx, sy);
         }
     }
     m.slope[c] = make_double2(sx, sy);
 }
 
 // ------------------------------------------------------------------------------------------
-// k_edges: one thread per internal edge, then one per boundary edge.  Also writes, per edge
-// side, the contribution lambda_max * length the CFL sum of that cell takes (hypComputeTimeStep,
-// swSpHyp.cpp:437-477: the L cell counts it when it is wet; the R cell when L or R is wet,
+// k_edges: one thread per internal edge, then one per boundary edge.  Writes the balance
+// terms {a, b, c} of the edge into the slots of its cells (when the flux is computed) and,
+// every step, the CFL contributions lambda_max * length that hypComputeTimeStep adds
+// (swSpHyp.cpp:437-477: the L cell counts it when it is wet; the R cell when L or R is wet,
 // because the reference carries `lambda` over from the L test).
 // ------------------------------------------------------------------------------------------
 template <int kScheme, bool kBlending>
@@ -203,16 +249,38 @@ __global__ void __launch_bounds__(kBlock, 3) k_edges(DevMesh m)
         if (m.lmax) m.lmax[e] = lm;
         const double lw = lm * ld(&m.len[e]);
         const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;
-        m.swc[e] = make_double2(wetL ? lw : 0.0, (wetL || wetR) ? lw : 0.0);
+        const int2 sl = ld(&m.eslot[e]);
+        m.slot_w[sl.x] = wetL ? lw : 0.0;
+        m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
         const double hL = SL.z - ca.x, hR = SR.z - cb.x;
         if ((hL > m.h_min) || (hR > m.h_min)) {
             EdgeFlux f = hllc(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min);
             bad |= f.bad;
             if (isnan(f.f1)) bad |= kStatusNanFlux;
-            double2* fp = m.flux + 3 * (size_t)e;
-            fp[0] = make_double2(f.f1, f.f2);
-            fp[1] = make_double2(f.f3, f.sl);
-            fp[2] = make_double2(f.sr, 0.0);
+            if (m.flux) {
+                double2* fp = m.flux + 3 * (size_t)e;
+                fp[0] = make_double2(f.f1, f.f2);
+                fp[1] = make_double2(f.f3, f.sl);
+                fp[2] = make_double2(f.sr, 0.0);
+            }
+            // factors of swSp::computeEdgeFactors (swSp.cpp:398-427) and the dt-free products of
+            // hypComputeBalance (swSpHyp.cpp:237-262)
+            const double2 cf = ld(&m.coef[e]);
+            const double nx = n.x, ny = n.y;
+            {
+                const double c = cf.x;
+                const double f1 = -c, f2F2 = -c * nx, f2F3 = +c * ny, f2S2 = +c * nx;
+                const double f3F2 = -c * ny, f3F3 = -c * nx, f3S2 = +c * ny;
+                m.slot[sl.x] = make_double4(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sl + f2F3 * f.f3,
+                                            f3F2 * f.f2 + f3S2 * f.sl + f3F3 * f.f3, 0.0);
+            }
+            {
+                const double c = cf.y;
+                const double f1 = +c, f2F2 = +c * nx, f2F3 = -c * ny, f2S2 = +c * nx;
+                const double f3F2 = +c * ny, f3F3 = +c * nx, f3S2 = +c * ny;
+                m.slot[sl.y] = make_double4(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sr + f2F3 * f.f3,
+                                            f3F2 * f.f2 + f3S2 * f.sr + f3F3 * f.f3, 0.0);
+            }
         }
     } else if (i < m.ni + m.nb) {
         const int e = i - m.ni;
@@ -223,23 +291,29 @@ __global__ void __launch_bounds__(kBlock, 3) k_edges(DevMesh m)
         SideState S = godunov_side(s.x, s.y, s.z, cs.x, cs.y, g.x, g.y);
         const double lm = (kScheme == SW2D_SCHEME_GODUNOV) ? smax(fabs(S.lp), fabs(S.lm)) : smax(fabs(S.lm), fabs(S.lp));
         if (m.lmaxb) m.lmaxb[e] = lm;
-        m.bswc[e] = (s.x > m.h_min) ? lm * g.z : 0.0;
+        const int sb = ld(&m.bslot[e]);
+        m.slot_w[sb] = (s.x > m.h_min) ? lm * g.z : 0.0;
         const int k = ld(&m.bbc[e]);
         const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
         const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, m.ctrl->t);
         double f1, f2, f3;
         bad |= boundary_flux(cs.y, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
-        m.bflux[e] = make_double4(f1, f2, f3, 0.0);
+        if (m.bflux) m.bflux[e] = make_double4(f1, f2, f3, 0.0);
+        const double cf = g.w, nx = g.x, ny = g.y;
+        const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
+        const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
+        const double s2 = 0.0;  // boundary geometric source: never set by hypBoundaryFlux
+        m.slot[sb] = make_double4(fa * f1, f2F2 * f2 + f2S2 * s2 + f2F3 * f3, f3F2 * f2 + f3S2 * s2 + f3F3 * f3, 0.0);
     }
     if (bad) atomicOr(&m.ctrl->status, bad);
 }
 
 // ------------------------------------------------------------------------------------------
-// k_cfl: swSp::hypComputeTimeStep (swSpHyp.cpp:430-512).  swept[c] gathers, in the reference's
-// order, the contributions k_edges prepared; dt = min over cells of cfl * area / max(swept,
+// k_cfl: swSp::hypComputeTimeStep (swSpHyp.cpp:430-512).  swept[c] sums the cell's slot
+// contributions in the reference's order; dt = min over cells of cfl * area / max(swept,
 // 1e-16), reduced warp -> block -> grid (last block done), then the dt_map snap (:496-504)
-// and the t_max clip, all on the device.  Adding a skipped (zero) contribution would not
-// change the sum, so the gather adds exactly what the reference adds.
+// and the t_max clip, all on the device.  A skipped contribution is stored as 0, and adding
+// +0 to the (non-negative) sum changes no bit, so the sum is the reference's.
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double min_keep(double a, double b) { return (b < a) ? b : a; }
 
@@ -253,15 +327,19 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double best = m.dt_max;
     if (c < m.nc) {
-        const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
+        const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
         double sw = 0.0;
-        for (int k = o0.y; k < o1.y; k++) sw += ld(&m.bswc[ld(&m.cbnd[k])]);
-        for (int k = o0.x; k < o1.x; k++) {
-            const int ent = ld(&m.cint[k]).x;
-            const double2 w = ld(&m.swc[ent >> 1]);
-            sw += (ent & 1) ? w.y : w.x;
+        if (k1 - k0 <= kUnroll) {
+            double w[kUnroll];
+#pragma unroll
+            for (int i = 0; i < kUnroll; i++) w[i] = (i < k1 - k0) ? ld(&m.slot_w[k0 + i]) : 0.0;
+#pragma unroll
+            for (int i = 0; i < kUnroll; i++)
+                if (i < k1 - k0) sw += w[i];
+        } else {
+            for (int k = k0; k < k1; k++) sw += ld(&m.slot_w[k]);
         }
-        double x = m.cfl_max * (ld(&m.cst[c].w) / smax(sw, kSmallReal));
+        double x = m.cfl_max * (ld(&m.area[c]) / smax(sw, kSmallReal));
         if (x < best) best = x;
     }
     // warp then block minimum (NaN candidates never win: comparisons with NaN are false)
@@ -324,46 +402,27 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
     if (c >= m.nc) return;
     const double4 s0 = m.st[c];
     double hh = s0.x, qq = s0.y, rr = s0.z;
-    const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
-    // hypComputeBalance (swSpHyp.cpp:214-273): boundary edges, then internal edges, each in
-    // increasing original index; factors of swSp::computeEdgeFactors (swSp.cpp:338-444)
-    for (int k = o0.y; k < o1.y; k++) {
-        const int e = ld(&m.cbnd[k]);
-        const double4 g = ld(&m.bgeo[e]);
-        const double4 F = m.bflux[e];
-        const double cf = g.w, nx = g.x, ny = g.y;
-        const double f1 = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
-        const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
-        const double s2 = 0.0;  // boundary geometric source: never set by hypBoundaryFlux
-        hh += f1 * F.x * dt;
-        qq += (f2F2 * F.y + f2S2 * s2 + f2F3 * F.z) * dt;
-        rr += (f3F2 * F.y + f3S2 * s2 + f3F3 * F.z) * dt;
-    }
-    for (int k = o0.x; k < o1.x; k++) {
-        const int ent = ld(&m.cint[k]).x;
-        const int e = ent >> 1;
-        const double2 n = ld(&m.nxy[e]);
-        const double2 cfp = ld(&m.coef[e]);
-        const double2* fp = m.flux + 3 * (size_t)e;
-        const double2 fa = fp[0], fb = fp[1];
-        const double nx = n.x, ny = n.y;
-        const double F1 = fa.x, F2 = fa.y, F3 = fb.x;
-        if (ent & 1) {  // this cell is R
-            const double cf = cfp.y;
-            const double s2 = fp[2].x;
-            const double f1 = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
-            const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
-            hh += f1 * F1 * dt;
-            qq += (f2F2 * F2 + f2S2 * s2 + f2F3 * F3) * dt;
-            rr += (f3F2 * F2 + f3S2 * s2 + f3F3 * F3) * dt;
-        } else {        // this cell is L
-            const double cf = cfp.x;
-            const double s2 = fb.y;
-            const double f1 = -cf, f2F2 = -cf * nx, f2F3 = +cf * ny, f2S2 = +cf * nx;
-            const double f3F2 = -cf * ny, f3F3 = -cf * nx, f3S2 = +cf * ny;
-            hh += f1 * F1 * dt;
-            qq += (f2F2 * F2 + f2S2 * s2 + f2F3 * F3) * dt;
-            rr += (f3F2 * F2 + f3S2 * s2 + f3F3 * F3) * dt;
+    // hypComputeBalance (swSpHyp.cpp:214-273): h += (factor*F1)*dt, q += (...)*dt, r += (...)*dt
+    // over the cell's slots, in the reference's order
+    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
+    if (k1 - k0 <= kUnroll) {
+        double4 v[kUnroll];
+#pragma unroll
+        for (int i = 0; i < kUnroll; i++)
+            if (i < k1 - k0) v[i] = m.slot[k0 + i];
+#pragma unroll
+        for (int i = 0; i < kUnroll; i++)
+            if (i < k1 - k0) {
+                hh += v[i].x * dt;
+                qq += v[i].y * dt;
+                rr += v[i].z * dt;
+            }
+    } else {
+        for (int k = k0; k < k1; k++) {
+            const double4 v = m.slot[k];
+            hh += v.x * dt;
+            qq += v.y * dt;
+            rr += v.z * dt;
         }
     }
     if (fabs(hh) < kSmallReal) hh = 0.;
@@ -434,7 +493,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
     }
     // z = h + z_b of the new state, as the next step's reconstruction computes it
     // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
-    m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.cst[c].x));
+    m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));
 }
 
 // swSp::computeEdgeFactors coefficient w / area / phi (swSp.cpp:364-368, 397-405)
@@ -536,8 +595,10 @@ struct sw2d_handle {
     int* d_int_perm = nullptr;
     int* d_bnd_perm = nullptr;
     double* stage = nullptr;    // 3 * nc doubles
-    double* lmax_buf = nullptr;
+    double* lmax_buf = nullptr;   // allocated by the option record_wave_speeds
     double* lmaxb_buf = nullptr;
+    double2* flux_buf = nullptr;  // allocated by the option record_fluxes
+    double4* bflux_buf = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     std::string err;
@@ -787,41 +848,55 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     for (int64_t i = 0; i < nb; i++) inv_bnd[h->bnd_perm[i]] = (int)i;
 
     // ---- per-cell lists in the reference's order (swParent::setMeshTables, swParent.cpp:469-486):
-    // walking edges by increasing original index appends them in that order.
+    // walking edges by increasing original index appends them in that order.  Balance slots of
+    // a cell: its boundary edges, then its internal edges (hypComputeBalance, swSpHyp.cpp:221-263).
     std::vector<int> cb_cnt(nc + 1, 0), ci_cnt(nc + 1, 0);
     for (int64_t e = 0; e < nb; e++) cb_cnt[inv[mesh->edge_bnd_cell[e]] + 1]++;
     for (int64_t e = 0; e < ni; e++) {
         ci_cnt[inv[mesh->edge_int_cells[2 * e]] + 1]++;
         ci_cnt[inv[mesh->edge_int_cells[2 * e + 1]] + 1]++;
     }
-    for (int64_t c = 0; c < nc; c++) {
-        cb_cnt[c + 1] += cb_cnt[c];
-        ci_cnt[c + 1] += ci_cnt[c];
-    }
     std::vector<int2> coff(nc + 1);
-    for (int64_t c = 0; c <= nc; c++) coff[c] = make_int2(ci_cnt[c], cb_cnt[c]);
-    std::vector<int> cbnd(nb);
-    std::vector<int2> cint(2 * ni);
     {
-        std::vector<int> fb(cb_cnt.begin(), cb_cnt.end() - 1), fi(ci_cnt.begin(), ci_cnt.end() - 1);
-        for (int64_t e = 0; e < nb; e++) cbnd[fb[inv[mesh->edge_bnd_cell[e]]]++] = inv_bnd[e];
+        int ci = 0, sl = 0;
+        for (int64_t c = 0; c < nc; c++) {
+            coff[c] = make_int2(ci, sl);
+            ci += ci_cnt[c + 1];
+            sl += cb_cnt[c + 1] + ci_cnt[c + 1];
+        }
+        coff[nc] = make_int2(ci, sl);
+    }
+    std::vector<int2> cint(2 * ni), eslot(ni);
+    std::vector<int> bslot(nb);
+    {
+        std::vector<int> fi(nc), fs(nc);
+        for (int64_t c = 0; c < nc; c++) {
+            fi[c] = coff[c].x;
+            fs[c] = coff[c].y;
+        }
+        for (int64_t e = 0; e < nb; e++) bslot[inv_bnd[e]] = fs[inv[mesh->edge_bnd_cell[e]]]++;
         for (int64_t e = 0; e < ni; e++) {
             int a = inv[mesh->edge_int_cells[2 * e]], b = inv[mesh->edge_int_cells[2 * e + 1]];
             int ne = inv_int[e];
             cint[fi[a]++] = make_int2(ne * 2 + 0, b);
             cint[fi[b]++] = make_int2(ne * 2 + 1, a);
+            eslot[ne] = make_int2(fs[a]++, fs[b]++);
         }
     }
+    const int64_t nslot = (int64_t)coff[nc].y;
 
     // ---- tables in the new numbering
     std::vector<double4> st(nc), cst(nc);
     std::vector<double2> cxy(nc);
+    std::vector<double> zbv(nc), area(nc);
     for (int64_t i = 0; i < nc; i++) {
         const int o = h->cell_perm[i];
         const double zb = mesh->cell_z_b[o];
         st[i] = make_double4(h0[o], q0[o], r0[o], h0[o] + zb);
         cst[i] = make_double4(zb, fields->boussinesq[o], fields->phi[o], mesh->cell_area[o]);
         cxy[i] = make_double2(mesh->cell_x[o], mesh->cell_y[o]);
+        zbv[i] = zb;
+        area[i] = mesh->cell_area[o];
     }
     std::vector<int2> lr(ni);
     std::vector<double2> nxy(ni), mxy(ni);
@@ -885,9 +960,12 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
         UP(hla, m.hla);
         UP(hlb, m.hlb);
     }
+    UP(zbv, m.zbv);
+    UP(area, m.area);
     UP(coff, m.coff);
     UP(cint, m.cint);
-    UP(cbnd, m.cbnd);
+    UP(eslot, m.eslot);
+    UP(bslot, m.bslot);
     UP(lr, m.lr);
     UP(nxy, m.nxy);
     UP(mxy, m.mxy);
@@ -914,12 +992,13 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     double2* coef_d = nullptr;
     if ((rc = dev_alloc(h, ni, &coef_d))) return bail(rc);
     m.coef = coef_d;
-    // persistent flux records start at zero, like the reference's resized member vectors
-    if ((rc = dev_alloc(h, 3 * ni, &m.flux)) || (rc = dev_alloc(h, ni, &m.swc)) || (rc = dev_alloc(h, nb, &m.bflux)) ||
-        (rc = dev_alloc(h, nb, &m.bswc)) || (rc = dev_alloc(h, nc, &m.slope)) ||
-        (rc = dev_alloc(h, grid_for(nc) + 1, &m.part)) || (rc = dev_alloc(h, 3 * nc, &h->stage)) ||
-        (rc = dev_alloc(h, ni, &h->lmax_buf)) || (rc = dev_alloc(h, nb, &h->lmaxb_buf)))
+    // persistent balance slots start at zero, like the reference's resized flux vectors
+    if ((rc = dev_alloc(h, nslot, &m.slot)) || (rc = dev_alloc(h, nslot, &m.slot_w)) ||
+        (rc = dev_alloc(h, nc, &m.slope)) || (rc = dev_alloc(h, grid_for(nc) + 1, &m.part)) ||
+        (rc = dev_alloc(h, 3 * nc, &h->stage)))
         return bail(rc);
+    m.flux = nullptr;
+    m.bflux = nullptr;
     m.lmax = nullptr;
     m.lmaxb = nullptr;
     m.h_min = params->h_min;
@@ -1028,16 +1107,34 @@ const char* sw2d_phase_name(int i)
 int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
 {
     if (!h || !name) return fail(h, SW2D_E_ARG, "invalid arguments");
+    CK(cudaSetDevice(h->device));
     if (std::strcmp(name, "record_wave_speeds") == 0) {
+        if (value && !h->lmax_buf) {
+            int rc = dev_alloc(h, h->ni, &h->lmax_buf);
+            if (!rc) rc = dev_alloc(h, h->nb, &h->lmaxb_buf);
+            if (rc) return rc;
+        }
         h->m.lmax = value ? h->lmax_buf : nullptr;
         h->m.lmaxb = value ? h->lmaxb_buf : nullptr;
-        if (h->graph) {  // the captured kernels hold the previous parameters
-            cudaGraphExecDestroy(h->graph);
-            h->graph = nullptr;
+    } else if (std::strcmp(name, "record_fluxes") == 0) {
+        // F1, F2, F3, S2L, S2R as the reference keeps them (swSp.h:183-193), for sw2d_get_array;
+        // turn on before the first step so that edges left dry keep their (zero) initial values
+        if (value && !h->flux_buf) {
+            int rc = dev_alloc(h, 3 * h->ni, &h->flux_buf);
+            if (!rc) rc = dev_alloc(h, h->nb, &h->bflux_buf);
+            if (rc) return rc;
         }
-        return SW2D_OK;
+        h->m.flux = value ? h->flux_buf : nullptr;
+        h->m.bflux = value ? h->bflux_buf : nullptr;
+    } else {
+        return fail(h, SW2D_E_ARG, std::string("unknown option ") + name);
     }
-    return fail(h, SW2D_E_ARG, std::string("unknown option ") + name);
+    if (h->graph) {  // the captured kernels hold the previous parameters
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
 }
 
 int sw2d_get_state_device(sw2d_handle* h, double* dh, double* dq, double* dr)
@@ -1134,7 +1231,8 @@ int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t ca
     };
     for (const Entry& e : tab) {
         if (std::strcmp(e.n, name) != 0) continue;
-        if (!e.p) return fail(h, SW2D_E_ARG, "wave speeds are recorded only with the option record_wave_speeds");
+        if (!e.p)
+            return fail(h, SW2D_E_ARG, "recorded only with the option record_wave_speeds / record_fluxes");
         if (capacity < e.len) return fail(h, SW2D_E_ARG, "output buffer too small");
         CK(cudaSetDevice(h->device));
         double* tmp = nullptr;

@@ -67,6 +67,7 @@ def test_gpu_intermediates_match_oracle(pkg, kind, kwargs):
     case = getattr(pkg.workloads, kind)(**kwargs)
     model = pkg.SpModel(case)
     model.set_option("record_wave_speeds", 1)
+    model.set_option("record_fluxes", 1)
     o = oracle_binding.SpOracle(case, portable_math=True)
     names = ["F1_int", "F2_int", "F3_int", "s2L_int", "s2R_int", "F1_bnd", "F2_bnd", "F3_bnd", "lambda_max_int",
              "lambda_max_bnd"]
