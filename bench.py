@@ -52,6 +52,8 @@ def _args():
     ap.add_argument("--cpu-steps", type=int, default=150, help="timed steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--phase-steps", type=int, default=20)
+    ap.add_argument("--launch-config", default=None,
+                    help="'S,E': slope and edge kernel launch variants instead of autotuning (profiling runs)")
     return ap.parse_args()
 
 
@@ -239,7 +241,14 @@ def run_ours(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    # warm-up (also builds the CUDA graph)
+    # launch-configuration autotune on the live state (no step taken), then warm-up (also
+    # builds the CUDA graph)
+    if args.launch_config:
+        sv, ev = (int(v) for v in args.launch_config.split(","))
+        model._check(model.lib.sw2d_set_launch_config(model.handle, sv, ev))
+        tune = {"report": f"fixed variants slopes={sv} edges={ev}"}
+    else:
+        tune = pkg.tuning.autotune(model, iters=5, device=local_rank, cache_path=None)
     model.step(args.warmup)
     phases = model.phase_times(args.phase_steps)
 
@@ -326,6 +335,7 @@ def run_ours(args, rank, world, local_rank):
                               f"cell-update x {n} cells per step / device time per step in the timed region",
                      "dominant_kernel": dominant, "kernels": kernels},
         "gpu_launches": steps * kps,
+        "launch_config": tune["report"],
         "clocks": clk.summary(),
     }
     if cpu is not None:

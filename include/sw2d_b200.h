@@ -181,6 +181,15 @@ const char* sw2d_phase_name(int i);
  * members, swSp.h:201-203); off by default since the step itself only needs lambda_max * length. */
 int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value);
 
+/* Launch-configuration autotuner (no counterpart in the reference): times every
+ * {threads per block, register cap} variant of the slope and edge kernels `iters` times on the
+ * current state (those kernels recompute the same outputs from the same state, so the run does
+ * not advance), keeps the fastest and writes a one-line report.  The chosen variants can be
+ * read back and set again (sw2d_get/set_launch_config) so that a caller can persist them. */
+int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity);
+int sw2d_get_launch_config(sw2d_handle* h, int* slopes_variant, int* edges_variant);
+int sw2d_set_launch_config(sw2d_handle* h, int slopes_variant, int edges_variant);
+
 /* Evaluates, on device `device`, fn = 0: the portable exp, 1: the portable log used by the step
  * (no counterpart in the reference, which calls the host libm's exp/log), 2: CUDA's exp,
  * 3: CUDA's log, on n host values; for the tests of the elementary functions. */

@@ -6,8 +6,9 @@ Modules:
   workloads  -- seeded synthetic cases (dam break, Gaussian bumps, feature channel)
   capi       -- ctypes view of include/sw2d_b200.h and the CUDA library loader
   solver     -- SpModel, the host-side mirror of the reference's swSp interface
+  tuning     -- launch-configuration autotuner with a JSON cache
 """
-from . import build, case, mesh, workloads, capi, solver  # noqa: F401
+from . import build, case, mesh, workloads, capi, solver, tuning  # noqa: F401
 from .case import Case, read_case, write_case  # noqa: F401
 from .solver import SpModel, Sw2dError  # noqa: F401
 

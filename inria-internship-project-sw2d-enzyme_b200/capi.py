@@ -188,6 +188,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_set_option.restype = ctypes.c_int
     lib.sw2d_eval_math.argtypes = [ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, ctypes.c_int64]
     lib.sw2d_eval_math.restype = ctypes.c_int
+    lib.sw2d_autotune.argtypes = [P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    lib.sw2d_autotune.restype = ctypes.c_int
+    lib.sw2d_get_launch_config.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    lib.sw2d_get_launch_config.restype = ctypes.c_int
+    lib.sw2d_set_launch_config.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    lib.sw2d_set_launch_config.restype = ctypes.c_int
     lib.sw2d_abi_version.argtypes = []
     lib.sw2d_abi_version.restype = ctypes.c_int
     _LIB = lib
@@ -199,4 +205,5 @@ EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",
-            "sw2d_set_option", "sw2d_eval_math"]
+            "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_get_launch_config",
+            "sw2d_set_launch_config"]

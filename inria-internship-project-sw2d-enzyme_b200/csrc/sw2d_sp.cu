@@ -165,7 +165,8 @@ __device__ __forceinline__ void grad_term(double zc, double zj, double2 xy, doub
     wsum += w;
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_slopes(DevMesh m)
+template <int kB, int kMinB>
+__global__ void __launch_bounds__(kB, kMinB) k_slopes(DevMesh m)
 {
     if (!step_active(m.ctrl)) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,8 +221,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_slopes(DevMesh m)
 // (swSpHyp.cpp:437-477: the L cell counts it when it is wet; the R cell when L or R is wet,
 // because the reference carries `lambda` over from the L test).
 // ------------------------------------------------------------------------------------------
-template <int kScheme, bool kBlending>
-__global__ void __launch_bounds__(kBlock, 3) k_edges(DevMesh m)
+template <int kScheme, bool kBlending, int kB, int kMinB>
+__global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
 {
     if (!step_active(m.ctrl)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -601,6 +602,8 @@ struct sw2d_handle {
     double4* bflux_buf = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    int edge_variant = 0;   // index into kVariants (sw2d_autotune)
+    int slope_variant = 2;
     std::string err;
 };
 
@@ -655,17 +658,63 @@ int status_to_code(sw2d_handle* h, unsigned st)
     return SW2D_OK;
 }
 
-void launch_edges(sw2d_handle* h)
+// Launch variants {threads per block, minimum resident blocks per SM (register cap)} of the
+// two heaviest kernels; sw2d_autotune times them on the live state and keeps the fastest.
+struct Variant {
+    int block, minb;
+};
+constexpr Variant kVariants[] = {{256, 3}, {256, 2}, {256, 4}, {128, 4}, {128, 8}, {512, 1}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+template <int kScheme, bool kBlending, int V>
+void launch_edges_v(sw2d_handle* h, unsigned n)
 {
-    const DevMesh& m = h->m;
-    const unsigned g = grid_for((long long)m.ni + m.nb);
+    constexpr int B = kVariants[V].block, M = kVariants[V].minb;
+    k_edges<kScheme, kBlending, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(h->m);
+}
+
+template <int kScheme, bool kBlending>
+void launch_edges_s(sw2d_handle* h, unsigned n, int v)
+{
+    switch (v) {
+        case 1: launch_edges_v<kScheme, kBlending, 1>(h, n); break;
+        case 2: launch_edges_v<kScheme, kBlending, 2>(h, n); break;
+        case 3: launch_edges_v<kScheme, kBlending, 3>(h, n); break;
+        case 4: launch_edges_v<kScheme, kBlending, 4>(h, n); break;
+        case 5: launch_edges_v<kScheme, kBlending, 5>(h, n); break;
+        default: launch_edges_v<kScheme, kBlending, 0>(h, n); break;
+    }
+}
+
+void launch_edges(sw2d_handle* h, int v)
+{
+    const unsigned n = (unsigned)(h->m.ni + h->m.nb);
     const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
     if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
-        if (bl) k_edges<SW2D_SCHEME_GODUNOV, true><<<g, kBlock, 0, h->stream>>>(m);
-        else k_edges<SW2D_SCHEME_GODUNOV, false><<<g, kBlock, 0, h->stream>>>(m);
+        if (bl) launch_edges_s<SW2D_SCHEME_GODUNOV, true>(h, n, v);
+        else launch_edges_s<SW2D_SCHEME_GODUNOV, false>(h, n, v);
     } else {
-        if (bl) k_edges<SW2D_SCHEME_MUSCL_EVR, true><<<g, kBlock, 0, h->stream>>>(m);
-        else k_edges<SW2D_SCHEME_MUSCL_EVR, false><<<g, kBlock, 0, h->stream>>>(m);
+        if (bl) launch_edges_s<SW2D_SCHEME_MUSCL_EVR, true>(h, n, v);
+        else launch_edges_s<SW2D_SCHEME_MUSCL_EVR, false>(h, n, v);
+    }
+}
+
+template <int V>
+void launch_slopes_v(sw2d_handle* h)
+{
+    constexpr int B = kVariants[V].block, M = kVariants[V].minb;
+    k_slopes<B, M><<<((unsigned)h->m.nc + B - 1) / B, B, 0, h->stream>>>(h->m);
+}
+
+void launch_slopes(sw2d_handle* h, int v)
+{
+    switch (v) {
+        case 1: launch_slopes_v<1>(h); break;
+        case 2: launch_slopes_v<2>(h); break;
+        case 3: launch_slopes_v<3>(h); break;
+        case 4: launch_slopes_v<4>(h); break;
+        case 5: launch_slopes_v<5>(h); break;
+        default: launch_slopes_v<0>(h); break;
     }
 }
 
@@ -693,9 +742,9 @@ void launch_phase(sw2d_handle* h, int i)
     DevMesh& m = h->m;
     switch (i) {
         case 0:
-            if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) k_slopes<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m);
+            if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) launch_slopes(h, h->slope_variant);
             break;
-        case 1: launch_edges(h); break;
+        case 1: launch_edges(h, h->edge_variant); break;
         case 2: k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); break;
         default: launch_update(h); break;
     }
@@ -1102,6 +1151,89 @@ const char* sw2d_phase_name(int i)
 {
     static const char* names[] = {"k_slopes", "k_edges", "k_cfl", "k_update"};
     return (i >= 0 && i < 4) ? names[i] : "";
+}
+
+int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
+{
+    if (!h || iters <= 0) return fail(h, SW2D_E_ARG, "invalid arguments");
+    CK(cudaSetDevice(h->device));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::string rep;
+    auto time_it = [&](auto&& launch) {
+        launch();  // warm
+        cudaEventRecord(e0, h->stream);
+        for (int i = 0; i < iters; i++) launch();
+        cudaEventRecord(e1, h->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return (double)ms / iters;
+    };
+    // k_slopes and k_edges recompute the same outputs from the same state every time they run
+    // (slopes, balance slots, CFL contributions), so timing them does not advance the run.
+    if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) {
+        double best = 1e300;
+        for (int v = 0; v < kNumVariants; v++) {
+            double ms = time_it([&] { launch_slopes(h, v); });
+            rep += "k_slopes/" + std::to_string(kVariants[v].block) + "x" + std::to_string(kVariants[v].minb) + "=" +
+                   std::to_string(ms) + "ms ";
+            if (ms < best) {
+                best = ms;
+                h->slope_variant = v;
+            }
+        }
+        launch_slopes(h, h->slope_variant);
+    }
+    double best = 1e300;
+    for (int v = 0; v < kNumVariants; v++) {
+        double ms = time_it([&] { launch_edges(h, v); });
+        rep += "k_edges/" + std::to_string(kVariants[v].block) + "x" + std::to_string(kVariants[v].minb) + "=" +
+               std::to_string(ms) + "ms ";
+        if (ms < best) {
+            best = ms;
+            h->edge_variant = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    rep += "chosen k_slopes/" + std::to_string(kVariants[h->slope_variant].block) + "x" +
+           std::to_string(kVariants[h->slope_variant].minb) + " k_edges/" +
+           std::to_string(kVariants[h->edge_variant].block) + "x" + std::to_string(kVariants[h->edge_variant].minb);
+    if (report && capacity > 0) {
+        std::strncpy(report, rep.c_str(), (size_t)capacity - 1);
+        report[capacity - 1] = '\0';
+    }
+    return SW2D_OK;
+}
+
+int sw2d_get_launch_config(sw2d_handle* h, int* slopes_variant, int* edges_variant)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    if (slopes_variant) *slopes_variant = h->slope_variant;
+    if (edges_variant) *edges_variant = h->edge_variant;
+    return SW2D_OK;
+}
+
+int sw2d_set_launch_config(sw2d_handle* h, int slopes_variant, int edges_variant)
+{
+    if (!h || slopes_variant < 0 || slopes_variant >= kNumVariants || edges_variant < 0 ||
+        edges_variant >= kNumVariants)
+        return fail(h, SW2D_E_ARG, "invalid launch variant");
+    h->slope_variant = slopes_variant;
+    h->edge_variant = edges_variant;
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    return SW2D_OK;
 }
 
 int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)

@@ -1,0 +1,65 @@
+"""Launch-configuration autotuner with a persistent JSON cache.
+
+``autotune(model)`` asks the library (sw2d_autotune) to time every {threads per block,
+register cap} variant of the slope and edge kernels on the model's current state and keeps
+the fastest; the choice is stored in a JSON file keyed by GPU, scheme, options and mesh size
+(power-of-two bucket), and reused by later runs without timing again.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import os
+from typing import Dict, Optional
+
+CACHE = os.path.join(os.environ.get("XDG_CACHE_HOME", os.path.expanduser("~/.cache")), "sw2d_b200", "autotune.json")
+
+
+def _device_name(device: int) -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(device)
+    except Exception:  # noqa: BLE001 - the key only needs to be stable
+        return f"cuda{device}"
+
+
+def _key(model, device: int) -> str:
+    o = model.case.opts
+    bucket = int(math.log2(max(1, model.n)))
+    return "|".join([_device_name(device), str(o.get("num_scheme", "godunov")), str(o.get("topo_discretization", "discontinuous")),
+                     str(o.get("model_friction", "none")), str(o.get("model_singular_head_loss", "none")), f"2^{bucket}"])
+
+
+def _load(path: str) -> Dict[str, dict]:
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def autotune(model, iters: int = 10, device: int = 0, cache_path: Optional[str] = CACHE, force: bool = False) -> dict:
+    """Chooses the launch variants for `model`; returns {"slopes", "edges", "report", "cached"}."""
+    key = _key(model, device)
+    db = _load(cache_path) if cache_path else {}
+    if not force and key in db:
+        e = db[key]
+        model._check(model.lib.sw2d_set_launch_config(model.handle, int(e["slopes"]), int(e["edges"])))
+        return {**e, "cached": True}
+    buf = ctypes.create_string_buffer(4096)
+    model._check(model.lib.sw2d_autotune(model.handle, int(iters), buf, len(buf)))
+    sv, ev = ctypes.c_int(), ctypes.c_int()
+    model._check(model.lib.sw2d_get_launch_config(model.handle, ctypes.byref(sv), ctypes.byref(ev)))
+    entry = {"slopes": sv.value, "edges": ev.value, "report": buf.value.decode()}
+    if cache_path:
+        db[key] = entry
+        try:
+            os.makedirs(os.path.dirname(cache_path), exist_ok=True)
+            tmp = cache_path + ".tmp"
+            with open(tmp, "w") as fh:
+                json.dump(db, fh, indent=1, sort_keys=True)
+            os.replace(tmp, cache_path)
+        except OSError:
+            pass
+    return {**entry, "cached": False}
