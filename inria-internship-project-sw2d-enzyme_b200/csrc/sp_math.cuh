@@ -53,6 +53,25 @@ struct SideState {
     double z, q, r, lm, lp;
 };
 
+// Exact shortcuts for dry cells.  Each replaces an operation by its IEEE result under a
+// condition where that result is known exactly, so the bits never change:
+//   sqrt(x) == x                         when x == +-0;
+//   x / d   == x                         when x == +-0 and d > 0;
+//   sqrt(g * max(1e-16, h)) == kC0       when !(1e-16 < h), kC0 = sqrt(g * 1e-16) (host value);
+//   sqrt((b-1) b u u + kC0 kC0) == kR0   when u == +-0 and 1 <= b finite (the first term is
+//                                        then +0), kR0 = sqrt(kC0 * kC0).
+// The shortcut is taken only when every active lane of the warp qualifies (a warp-uniform
+// branch); otherwise all lanes run the full operation, whose result is the same.
+struct DryConsts {
+    double c0, r0;
+};
+
+__device__ __forceinline__ bool warp_all(bool p) { return __all_sync(__activemask(), p); }
+
+__device__ __forceinline__ double sqrt_z(double x) { return warp_all(x == 0.0) ? x : sqrt(x); }
+
+__device__ __forceinline__ double div_z(double x, double d) { return warp_all(x == 0.0) ? x : x / d; }  // d > 0
+
 // First-order rotated state of a cell on an edge (swSpHypGodunov.cpp:17-35 and 44-76; the
 // boundary loop of swSpHypMusclEvr.cpp:142-159 is the same expression).
 __device__ __forceinline__ SideState godunov_side(double h, double q, double r, double zb, double b, double nx, double ny)
@@ -61,10 +80,18 @@ __device__ __forceinline__ SideState godunov_side(double h, double q, double r, 
     s.z = h + zb;
     s.q = q * nx + r * ny;
     s.r = -q * ny + r * nx;
-    double u = s.q / smax(h, kSmallReal);
-    double c = sqrt(kGravity * h);
-    s.lm = lam_minus(b, c, u);
-    s.lp = lam_plus(b, c, u);
+    const double d = smax(h, kSmallReal);
+    double u, c;
+    if (warp_all(h == 0.0 && s.q == 0.0)) {  // d == 1e-16 > 0; sqrt(g * +-0) == g * +-0
+        u = s.q;
+        c = kGravity * h;
+    } else {
+        u = s.q / d;
+        c = sqrt(kGravity * h);
+    }
+    const double root = sqrt_z((b - 1.0) * b * u * u + c * c);
+    s.lm = b * u - root;
+    s.lp = b * u + root;
     return s;
 }
 
@@ -74,15 +101,25 @@ __device__ __forceinline__ SideState godunov_side(double h, double q, double r, 
 // previous step's time step.
 __device__ __forceinline__ SideState evr_side(bool left, double h, double q, double r, double zb, double b, double zc,
                                               double sx, double sy, double cx, double cy, double mx, double my,
-                                              double nx, double ny, double dt)
+                                              double nx, double ny, double dt, const DryConsts& k)
 {
-    double ql = q * nx + r * ny;
-    double rl = r * nx - q * ny;
-    double cl = sqrt(kGravity * smax(kSmallReal, h));
-    double ul = ql / smax(kSmallReal, h);
-    double vl = rl / smax(kSmallReal, h);
-    double lmv = lam_minus(b, cl, ul);
-    double lpv = lam_plus(b, cl, ul);
+    const double ql = q * nx + r * ny;
+    const double rl = r * nx - q * ny;
+    double cl, ul, vl, root1;
+    if (warp_all(!(kSmallReal < h) && ql == 0.0 && rl == 0.0 && b < 1.0e308)) {  // b >= 1 and finite
+        cl = k.c0;
+        ul = ql;
+        vl = rl;
+        root1 = k.r0;
+    } else {
+        const double hd = smax(kSmallReal, h);
+        cl = sqrt(kGravity * hd);
+        ul = ql / hd;
+        vl = rl / hd;
+        root1 = sqrt((b - 1.0) * b * ul * ul + cl * cl);
+    }
+    const double lmv = b * ul - root1;
+    const double lpv = b * ul + root1;
     double l1 = left ? smax(0.0, lmv) : smin(0.0, lmv);
     double dx1 = mx - cx - 0.5 * l1 * dt * nx;
     double dy1 = my - cy - 0.5 * l1 * dt * ny;
@@ -98,10 +135,11 @@ __device__ __forceinline__ SideState evr_side(bool left, double h, double q, dou
     s.z = hr + zb;
     s.q = hr * ul;
     s.r = hr * vl;
-    double u = s.q / smax(hr, kSmallReal);
-    double c = sqrt(kGravity * hr);
-    s.lm = lam_minus(b, c, u);
-    s.lp = lam_plus(b, c, u);
+    const double u = div_z(s.q, smax(hr, kSmallReal));
+    const double c = sqrt_z(kGravity * hr);
+    const double root = sqrt_z((b - 1.0) * b * u * u + c * c);
+    s.lm = b * u - root;
+    s.lp = b * u + root;
     return s;
 }
 

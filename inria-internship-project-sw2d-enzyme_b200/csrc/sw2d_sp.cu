@@ -104,6 +104,7 @@ struct DevMesh {
     const double *bctimes, *bcvals;
     // parameters
     double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
+    DryConsts dry;
     int neg_detect;
     // dt reduction scratch
     double* part;
@@ -243,8 +244,10 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
             const double2 mp = ld(&m.mxy[e]);
             const double2 xa = ld(&m.cxy[a]), xb = ld(&m.cxy[b]);
             const double2 ga = ld(&m.slope[a]), gb = ld(&m.slope[b]);
-            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y, dtp);
-            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y, dtp);
+            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y, dtp,
+                          m.dry);
+            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y, dtp,
+                          m.dry);
         }
         const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
         if (m.lmax) m.lmax[e] = lm;
@@ -1058,6 +1061,13 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     m.v_max = params->v_max;
     m.fr_max = params->fr_max;
     m.neg_detect = params->negative_depth_detection ? 1 : 0;
+    // constants of the dry-cell shortcuts, by the same IEEE operations the step would do
+    {
+        volatile double g = kGravity, sr = kSmallReal;
+        m.dry.c0 = std::sqrt(g * sr);
+        volatile double c0 = m.dry.c0;
+        m.dry.r0 = std::sqrt(c0 * c0);
+    }
     if (cudaMalloc(&h->ctrl, sizeof(Ctrl)) != cudaSuccess) return bail(fail(h, SW2D_E_CUDA, "cudaMalloc ctrl"));
     h->allocs.push_back(h->ctrl);
     if (cudaMallocHost(&h->ctrl_host, sizeof(Ctrl)) != cudaSuccess) return bail(fail(h, SW2D_E_CUDA, "cudaMallocHost"));
