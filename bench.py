@@ -198,7 +198,7 @@ def _measured_peak():
 
 
 def _traffic_per_step():
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+    p = os.path.join(ROOT, "profiles", "sp_step_traffic_gaussian_bumps_4M.json")
     if os.path.exists(p):
         try:
             return json.load(open(p))
