@@ -195,6 +195,18 @@ int sw2d_set_launch_config(sw2d_handle* h, int slopes_variant, int edges_variant
  * 3: CUDA's log, on n host values; for the tests of the elementary functions. */
 int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n);
 
+/* sw2d_get_array without any allocation.  No counterpart in the reference (which keeps these
+ * arrays in host memory).  For callers that must not allocate device memory once their run has
+ * started: it stages the array in a fixed buffer compiled into the library (2^20 doubles =
+ * 8 MiB, held by every GPU that loads the library until the process exits) instead of a
+ * buffer allocated per call.  Arrays longer than 2^20 values are rejected with SW2D_E_ARG and
+ * a message naming the limit (use sw2d_get_array for them).  The first call on a device looks
+ * up the buffer's device address (cudaGetSymbolAddress) for that device; make that first call
+ * before any stream capture.  All calls share the one buffer: calls that overlap on the GPU
+ * (from several threads or handles on the same device) race; this call returns only after its
+ * copy has completed. */
+int64_t sw2d_get_array_noalloc(sw2d_handle* h, const char* name, double* out, int64_t capacity);
+
 /* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
 int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
 

@@ -170,6 +170,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_set_time.restype = ctypes.c_int
     lib.sw2d_get_array.argtypes = [P, ctypes.c_char_p, c_double_p, ctypes.c_int64]
     lib.sw2d_get_array.restype = ctypes.c_int64
+    lib.sw2d_get_array_noalloc.argtypes = [P, ctypes.c_char_p, c_double_p, ctypes.c_int64]
+    lib.sw2d_get_array_noalloc.restype = ctypes.c_int64
     lib.sw2d_get_cell_permutation.argtypes = [P, c_int64_p]
     lib.sw2d_get_cell_permutation.restype = ctypes.c_int
     lib.sw2d_get_stream.argtypes = [P]
@@ -206,4 +208,4 @@ EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",
             "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_get_launch_config",
-            "sw2d_set_launch_config"]
+            "sw2d_set_launch_config", "sw2d_get_array_noalloc"]

@@ -41,6 +41,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1384,6 +1385,101 @@ int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t ca
         cudaStreamSynchronize(h->stream);
         cudaFree(tmp);
         if (ce != cudaSuccess) return fail(h, SW2D_E_CUDA, cudaGetErrorString(ce));
+        return e.len;
+    }
+    if (std::strcmp(name, "s2R_bnd") == 0) {
+        if (capacity < h->nb) return fail(h, SW2D_E_ARG, "output buffer too small");
+        for (int64_t i = 0; i < h->nb; i++) out[i] = 0.0;
+        return h->nb;
+    }
+    return fail(h, SW2D_E_ARG, std::string("unknown array ") + name);
+}
+
+// ------------------------------------------------------------------------------------------
+// Reading a per-edge or per-cell array without allocating.
+//
+// sw2d_get_array stages the array on the device in a buffer it allocates for the call
+// (cudaMalloc/cudaFree).  Some callers must not allocate once their run has started: a
+// forecasting service that reserves all device memory at start-up and must not fail with
+// out-of-memory in the middle of an event, or an application whose memory pool forbids
+// allocations from library code.  sw2d_get_array_noalloc does the same work with a fixed
+// staging array compiled into the library instead (kNoAllocMaxDoubles doubles = 8 MiB, held by
+// every GPU that loads the library until the process exits).
+// ------------------------------------------------------------------------------------------
+constexpr int64_t kNoAllocMaxDoubles = (int64_t)1 << 20;
+static __device__ __align__(256) double g_noalloc_stage[kNoAllocMaxDoubles];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_stage on `device`, which must be the current device.  In host
+// code the name g_noalloc_stage is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, once per device, and is cached.
+int noalloc_stage(sw2d_handle* h, int device, double** out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(h, SW2D_E_ARG, "device ordinal out of range");
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_stage);
+        if (e != cudaSuccess || !p)
+            return fail(h, SW2D_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return SW2D_OK;
+}
+
+}  // namespace
+
+int64_t sw2d_get_array_noalloc(sw2d_handle* h, const char* name, double* out, int64_t capacity)
+{
+    if (!h || !name || !out) return fail(h, SW2D_E_ARG, "invalid arguments");
+    struct Entry {
+        const char* n;
+        const double* p;
+        int stride, offset;
+        int64_t len;
+        const int* perm;
+    } tab[] = {
+        {"F1_int", (const double*)h->m.flux, 6, 0, h->ni, h->d_int_perm},
+        {"F2_int", (const double*)h->m.flux, 6, 1, h->ni, h->d_int_perm},
+        {"F3_int", (const double*)h->m.flux, 6, 2, h->ni, h->d_int_perm},
+        {"s2L_int", (const double*)h->m.flux, 6, 3, h->ni, h->d_int_perm},
+        {"s2R_int", (const double*)h->m.flux, 6, 4, h->ni, h->d_int_perm},
+        {"F1_bnd", (const double*)h->m.bflux, 4, 0, h->nb, h->d_bnd_perm},
+        {"F2_bnd", (const double*)h->m.bflux, 4, 1, h->nb, h->d_bnd_perm},
+        {"F3_bnd", (const double*)h->m.bflux, 4, 2, h->nb, h->d_bnd_perm},
+        {"lambda_max_int", h->m.lmax, 1, 0, h->ni, h->d_int_perm},
+        {"lambda_max_bnd", h->m.lmaxb, 1, 0, h->nb, h->d_bnd_perm},
+        {"slope_x", (const double*)h->m.slope, 2, 0, h->nc, h->d_cell_perm},
+        {"slope_y", (const double*)h->m.slope, 2, 1, h->nc, h->d_cell_perm},
+    };
+    for (const Entry& e : tab) {
+        if (std::strcmp(e.n, name) != 0) continue;
+        if (!e.p)
+            return fail(h, SW2D_E_ARG, "recorded only with the option record_wave_speeds / record_fluxes");
+        if (capacity < e.len) return fail(h, SW2D_E_ARG, "output buffer too small");
+        if (e.len > kNoAllocMaxDoubles)
+            return fail(h, SW2D_E_ARG, std::string("sw2d_get_array_noalloc: ") + name + " has " + std::to_string(e.len) +
+                                           " values, more than the fixed staging array holds (" +
+                                           std::to_string(kNoAllocMaxDoubles) + "); use sw2d_get_array");
+        CK(cudaSetDevice(h->device));
+        double* stage = nullptr;
+        const int st = noalloc_stage(h, h->device, &stage);
+        if (st) return st;
+        // every element of [0, len) is written by the scatter (perm is a permutation), so the
+        // previous call's contents need no clearing
+        if (e.len > 0) {
+            k_scatter_strided<<<grid_for(e.len), kBlock, 0, h->stream>>>(e.p, e.stride, e.offset, e.perm, stage,
+                                                                          (int)e.len);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(out, stage, e.len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
         return e.len;
     }
     if (std::strcmp(name, "s2R_bnd") == 0) {
