@@ -207,6 +207,90 @@ int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n);
  * copy has completed. */
 int64_t sw2d_get_array_noalloc(sw2d_handle* h, const char* name, double* out, int64_t capacity);
 
+/* ---- Adjoint: gradient of an observation misfit along a recorded trajectory ----------------
+ *
+ * The reference differentiates its AD variant of the step with Enzyme along a frozen dt
+ * sequence: swSpE::get_spatial_gradient_checkpointed (assim/swSpE_checkpoint.cpp:722-1281) over
+ * ckpt_segment_E (assim/swSpE_checkpoint.cpp:584-715, assim/swSpE.h:237-251), with
+ * replay_trajectory_cost as the matching cost (`func()`), gauge or frame costs
+ * (assim/swSpE_gauges.cpp:166-179, assim/swSpE_ad.cpp:273-308).  Here the native step is
+ * differentiated by hand-written reverse kernels, with respect to the per-cell friction
+ * coefficients (Manning n for the Manning law), the initial state and the bed elevation, along
+ * a trajectory whose dt sequence and boundary values are recorded once and then frozen.
+ *
+ * J = scale * sum over observation k, observed cell p of
+ *        w_h[p] (h - h_obs[k][p])^2 + w_q[p] ((q - q_obs[k][p])^2 + (r - r_obs[k][p])^2)
+ * with h, q, r the replayed state after steps[k] steps of the trajectory, scale = 1 / n_times
+ * when normalize is set (the reference's cost_normalize), else 1. */
+typedef struct sw2d_obs {
+    int64_t n_points;       /* observed cells (gauges, or every cell for a full frame) */
+    const int64_t* cells;   /* [n_points] cell indices (caller numbering), all distinct */
+    const double* w_h;      /* [n_points] weights of the depth misfit */
+    const double* w_q;      /* [n_points] weights of the discharge misfit, or NULL for none */
+    int64_t n_times;        /* observations */
+    const int64_t* steps;   /* [n_times] step index after the trajectory's start (0 = initial
+                               state), strictly increasing */
+    const double* h_obs;    /* [n_times * n_points], observation-major */
+    const double* q_obs;    /* [n_times * n_points] or NULL when w_q is NULL */
+    const double* r_obs;
+    int normalize;
+} sw2d_obs;
+
+/* Gradient outputs of sw2d_adjoint: host arrays of cell_nb doubles (caller numbering); any may
+ * be NULL.  friction_1 / friction_2 are the coefficients along the two friction directions
+ * (swSp members friction_coeff_direction_1/_2): Manning n, Strickler K or Chezy C. */
+typedef struct sw2d_gradient {
+    double* h0;
+    double* q0;
+    double* r0;
+    double* z_b;
+    double* friction_1;
+    double* friction_2;
+} sw2d_gradient;
+
+/* Runs n_steps CFL-driven steps from the current state (as sw2d_step_n) and records them as
+ * the trajectory: the dt sequence, and checkpoints (state, balance terms, time) every
+ * checkpoint_every steps.  Stops early at t_max (*steps_done tells).  The analogue of the
+ * reference's dry run before its reverse loop (build_checkpoint_records,
+ * assim/swSpE_checkpoint.cpp:210-425). */
+int sw2d_record(sw2d_handle* h, int64_t n_steps, int64_t checkpoint_every, int64_t* steps_done);
+
+/* Recorded length, checkpoint interval, start time and end time of the trajectory. */
+int sw2d_trajectory_info(sw2d_handle* h, int64_t* n_steps, int64_t* checkpoint_every, double* t_start,
+                         double* t_end);
+
+/* The recorded dt sequence (capacity >= n_steps). */
+int sw2d_get_trajectory_dt(sw2d_handle* h, double* dt, int64_t capacity);
+
+/* Replaces the trajectory's initial state (a control of the adjoint). */
+int sw2d_set_trajectory_start(sw2d_handle* h, const double* h0, const double* q0, const double* r0);
+
+/* Per-cell parameters (caller numbering): "friction_1", "friction_2", "friction" (both
+ * directions; set only) and "z_b".  The analogue of the reference's control transform
+ * (assim/swSpE.h:59-107), which writes the control into the solver before each replay.
+ * Changing z_b keeps h and moves z = h + z_b, for the current state and the trajectory's
+ * initial state. */
+int sw2d_set_param(sw2d_handle* h, const char* name, const double* values);
+int sw2d_get_param(sw2d_handle* h, const char* name, double* values);
+
+/* Observation set of the cost (copied). */
+int sw2d_set_observations(sw2d_handle* h, const sw2d_obs* obs);
+
+/* Replays the trajectory from its initial state with the recorded dt and the current
+ * parameters and returns J (replay_trajectory_cost, assim/swSpE_checkpoint.cpp:1380-1453).
+ * Leaves the model at the end of the trajectory. */
+int sw2d_replay_cost(sw2d_handle* h, double* J);
+
+/* Replays the trajectory and returns h (and q, r when non-NULL) at the given cells after each
+ * of the given steps: [n_times * n_points], observation-major.  For twin experiments. */
+int sw2d_replay_sample(sw2d_handle* h, int64_t n_points, const int64_t* cells, int64_t n_times, const int64_t* steps,
+                       double* h_out, double* q_out, double* r_out);
+
+/* J and its gradient (get_spatial_gradient_checkpointed, assim/swSpE_checkpoint.cpp:722-1281):
+ * one reverse sweep over the checkpointed segments, each recomputed forward once.  The same J
+ * as sw2d_replay_cost, bit for bit.  Leaves the model at the end of the trajectory. */
+int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad);
+
 /* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
 int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
 

@@ -56,6 +56,17 @@ class Sw2dBcTable(ctypes.Structure):
                 ("values", c_double_p)]
 
 
+class Sw2dObs(ctypes.Structure):
+    _fields_ = [("n_points", ctypes.c_int64), ("cells", c_int64_p), ("w_h", c_double_p), ("w_q", c_double_p),
+                ("n_times", ctypes.c_int64), ("steps", c_int64_p), ("h_obs", c_double_p), ("q_obs", c_double_p),
+                ("r_obs", c_double_p), ("normalize", ctypes.c_int)]
+
+
+class Sw2dGradient(ctypes.Structure):
+    _fields_ = [("h0", c_double_p), ("q0", c_double_p), ("r0", c_double_p), ("z_b", c_double_p),
+                ("friction_1", c_double_p), ("friction_2", c_double_p)]
+
+
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(c_double_p)
 
@@ -198,6 +209,27 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_set_launch_config.restype = ctypes.c_int
     lib.sw2d_abi_version.argtypes = []
     lib.sw2d_abi_version.restype = ctypes.c_int
+    # adjoint
+    lib.sw2d_record.argtypes = [P, ctypes.c_int64, ctypes.c_int64, c_int64_p]
+    lib.sw2d_record.restype = ctypes.c_int
+    lib.sw2d_trajectory_info.argtypes = [P, c_int64_p, c_int64_p, c_double_p, c_double_p]
+    lib.sw2d_trajectory_info.restype = ctypes.c_int
+    lib.sw2d_get_trajectory_dt.argtypes = [P, c_double_p, ctypes.c_int64]
+    lib.sw2d_get_trajectory_dt.restype = ctypes.c_int
+    lib.sw2d_set_trajectory_start.argtypes = [P, P, P, P]
+    lib.sw2d_set_trajectory_start.restype = ctypes.c_int
+    lib.sw2d_set_param.argtypes = [P, ctypes.c_char_p, P]
+    lib.sw2d_set_param.restype = ctypes.c_int
+    lib.sw2d_get_param.argtypes = [P, ctypes.c_char_p, P]
+    lib.sw2d_get_param.restype = ctypes.c_int
+    lib.sw2d_set_observations.argtypes = [P, ctypes.POINTER(Sw2dObs)]
+    lib.sw2d_set_observations.restype = ctypes.c_int
+    lib.sw2d_replay_cost.argtypes = [P, c_double_p]
+    lib.sw2d_replay_cost.restype = ctypes.c_int
+    lib.sw2d_replay_sample.argtypes = [P, ctypes.c_int64, c_int64_p, ctypes.c_int64, c_int64_p, P, P, P]
+    lib.sw2d_replay_sample.restype = ctypes.c_int
+    lib.sw2d_adjoint.argtypes = [P, c_double_p, ctypes.POINTER(Sw2dGradient)]
+    lib.sw2d_adjoint.restype = ctypes.c_int
     _LIB = lib
     return lib
 
@@ -208,4 +240,6 @@ EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",
             "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_get_launch_config",
-            "sw2d_set_launch_config", "sw2d_get_array_noalloc"]
+            "sw2d_set_launch_config", "sw2d_get_array_noalloc", "sw2d_record", "sw2d_trajectory_info",
+            "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
+            "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint"]

@@ -10,11 +10,23 @@
 // literal form, including what happens with NaN.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #include "portable_math.h"
 
+// The same functions compile for the device (the product) and for the host (the adjoint's
+// finite-difference tests build them with g++ -ffp-contract=off).
+#if defined(__CUDACC__)
+#define SW2D_HD __host__ __device__ __forceinline__
+#else
+#define SW2D_HD inline
+#endif
+
 namespace sw2d {
+
+using std::fabs;
+using std::sqrt;
 
 constexpr double kSmallReal = 1e-16;  // src/common/param.h:2
 constexpr double kGravity = 9.81;     // src/common/param.h:3
@@ -25,22 +37,23 @@ constexpr unsigned kStatusHllcConfig = 2u;
 constexpr unsigned kStatusNegDepth = 4u;
 constexpr unsigned kStatusBcType = 8u;
 constexpr unsigned kStatusBcFr = 16u;
+constexpr unsigned kStatusUnsupported = 32u;  // a case the reverse kernels do not handle
 
-__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+SW2D_HD double smax(double a, double b) { return (a < b) ? b : a; }
+SW2D_HD double smin(double a, double b) { return (b < a) ? b : a; }
 
 // swSp::lambdaMinus / lambdaPlus (src/sw2dSolver/models/sp/swSp.cpp:972-995)
-__device__ __forceinline__ double lam_minus(double b, double c, double u) { return b * u - sqrt((b - 1.0) * b * u * u + c * c); }
-__device__ __forceinline__ double lam_plus(double b, double c, double u) { return b * u + sqrt((b - 1.0) * b * u * u + c * c); }
+SW2D_HD double lam_minus(double b, double c, double u) { return b * u - sqrt((b - 1.0) * b * u * u + c * c); }
+SW2D_HD double lam_plus(double b, double c, double u) { return b * u + sqrt((b - 1.0) * b * u * u + c * c); }
 
 // swSp::specificForce (swSp.cpp:1388-1399)
-__device__ __forceinline__ double spec_force(double b, double phi, double h, double u)
+SW2D_HD double spec_force(double b, double phi, double h, double u)
 {
     return phi * (b * h * u * u + 0.5 * kGravity * h * h);
 }
 
 // std::max({a,b,c,d}): the first largest under operator<
-__device__ __forceinline__ double max4(double a, double b, double c, double d)
+SW2D_HD double max4(double a, double b, double c, double d)
 {
     double m = a;
     if (m < b) m = b;
@@ -66,15 +79,22 @@ struct DryConsts {
     double c0, r0;
 };
 
-__device__ __forceinline__ bool warp_all(bool p) { return __all_sync(__activemask(), p); }
+SW2D_HD bool warp_all(bool p)
+{
+#if defined(__CUDA_ARCH__)
+    return __all_sync(__activemask(), p);
+#else
+    return p;
+#endif
+}
 
-__device__ __forceinline__ double sqrt_z(double x) { return warp_all(x == 0.0) ? x : sqrt(x); }
+SW2D_HD double sqrt_z(double x) { return warp_all(x == 0.0) ? x : sqrt(x); }
 
-__device__ __forceinline__ double div_z(double x, double d) { return warp_all(x == 0.0) ? x : x / d; }  // d > 0
+SW2D_HD double div_z(double x, double d) { return warp_all(x == 0.0) ? x : x / d; }  // d > 0
 
 // First-order rotated state of a cell on an edge (swSpHypGodunov.cpp:17-35 and 44-76; the
 // boundary loop of swSpHypMusclEvr.cpp:142-159 is the same expression).
-__device__ __forceinline__ SideState godunov_side(double h, double q, double r, double zb, double b, double nx, double ny)
+SW2D_HD SideState godunov_side(double h, double q, double r, double zb, double b, double nx, double ny)
 {
     SideState s;
     s.z = h + zb;
@@ -99,7 +119,7 @@ __device__ __forceinline__ SideState godunov_side(double h, double q, double r, 
 // reconstruction at the edge midpoint with the limited free-surface slope (sx, sy) of the
 // cell.  `left` selects max(0,.) (L side) or min(0,.) (R side) for the wave speeds; dt is the
 // previous step's time step.
-__device__ __forceinline__ SideState evr_side(bool left, double h, double q, double r, double zb, double b, double zc,
+SW2D_HD SideState evr_side(bool left, double h, double q, double r, double zb, double b, double zc,
                                               double sx, double sy, double cx, double cy, double mx, double my,
                                               double nx, double ny, double dt, const DryConsts& k)
 {
@@ -150,7 +170,7 @@ struct EdgeFlux {
 
 // swSp::hypHllc (swSpHyp.cpp:664-821) and swSp::hypHllcBlending (swSpHyp.cpp:824-998).
 // Flags kStatusHllcConfig for the configuration the reference rejects (:728-739).
-__device__ __forceinline__ EdgeFlux hllc(bool blending, double bL, double bR, double phiL, double phiR, double zbL,
+SW2D_HD EdgeFlux hllc(bool blending, double bL, double bR, double phiL, double phiR, double zbL,
                                          double zbR, const SideState& L, const SideState& R, double h_min,
                                          double phi_min)
 {
@@ -242,7 +262,7 @@ __device__ __forceinline__ EdgeFlux hllc(bool blending, double bL, double bR, do
 // swBoundaryConditionTimeSeries::initialise + computeValBC
 // (models/common/swBoundaryConditionTimeSeries.cpp:17-96), walked from the initial cursor.
 // Simulation time never decreases, so this equals the reference's incremental cursor.
-__device__ __forceinline__ double bc_value(const double* tv, const double* vv, int64_t n, double time)
+SW2D_HD double bc_value(const double* tv, const double* vv, int64_t n, double time)
 {
     double v_inf = vv[0], t_inf = tv[0], v_sup, t_sup;
     bool at_end = false;
@@ -270,14 +290,14 @@ __device__ __forceinline__ double bc_value(const double* tv, const double* vv, i
 }
 
 // swSp::hypHCritical (swSpHyp.cpp:651-661)
-__device__ __forceinline__ double h_critical(double phi, double q)
+SW2D_HD double h_critical(double phi, double q)
 {
     return sw2d_exp((1. / 3.) * sw2d_log((q / smax(phi, kSmallReal)) / kGravity));
 }
 
 // swSp::hypBoundaryFlux (swSpHyp.cpp:13-135); the boundary geometric source stays 0.  Returns
 // kStatusBcFr / kStatusBcType where the reference stops, else 0.
-__device__ __forceinline__ unsigned boundary_flux(double bR, double phiR, double zbR, const SideState& S, int type,
+SW2D_HD unsigned boundary_flux(double bR, double phiR, double zbR, const SideState& S, int type,
                                                   double bcv, double h_min, double* f1o, double* f2o, double* f3o)
 {
     unsigned bad = 0;
@@ -334,7 +354,7 @@ __device__ __forceinline__ unsigned boundary_flux(double bR, double phiR, double
 
 // swSource::frictionChezy1D / frictionManning1D / frictionStrickler1D
 // (models/common/swSourceFriction.cpp:7-79); model 1 chezy, 2 manning, 3 strickler.
-__device__ __forceinline__ double friction_factor(int model, double k, double h, double un, double dt)
+SW2D_HD double friction_factor(int model, double k, double h, double un, double dt)
 {
     double factor = 1.0;
     if (model == 1) {

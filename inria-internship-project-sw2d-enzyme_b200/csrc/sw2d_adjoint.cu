@@ -1,0 +1,1105 @@
+// sw2d_adjoint.cu — reverse mode of the SP step on the B200: recorded trajectories with
+// checkpoints, frozen-dt replays, the observation misfit J and its gradient with respect to the
+// per-cell friction coefficients (Manning n for the Manning law), the initial state and the
+// bed elevation.
+//
+// What is differentiated.  As in the reference's assimilation (assim/swSpE_checkpoint.cpp:
+// 1436-1453, `ckpt_segment_E` with a frozen dt sequence, assim/swSpE.h:237-251), the time
+// steps and the boundary values are those of a recorded run: J(m) is the cost of replaying the
+// recorded dt sequence with controls m.  J sums, over observation steps, weighted squared
+// misfits of h (and optionally q, r) at observed cells (compute_cost_gauges_ptr,
+// assim/swSpE_gauges.cpp:166-179; compute_cost_frame_ptr, assim/swSpE_ad.cpp:273-308),
+// optionally divided by the number of observations (cost_normalize).
+//
+// Checkpointing.  sw2d_record runs the CFL-driven step and keeps the dt sequence; the state,
+// the balance slots and the control block are stored every K steps.  The reverse sweep walks
+// the segments backwards: it restores a checkpoint, recomputes the K forward steps storing each
+// step's state and post-balance state, then runs the reverse kernels step by step:
+//
+//   k_obs_rev       per observed cell   misfit gradient at an observation step
+//   k_update_rev    per cell            reverse of flush / clamp / friction / head loss / velocity
+//                                       cap; friction-coefficient gradient; slot adjoints
+//                                       sigma += dt * (adjoint of the post-balance state)
+//   k_slopes        per cell            forward slopes of the step (recomputed)
+//   k_edges_rev     per edge            reverse of the Riemann states and HLLC / boundary fluxes for
+//                                       the edges whose flux the step computed; per-slot
+//                                       contributions to the cells; those slots' adjoints reset
+//   k_cells_rev     per cell            ordered gather of the slot contributions; reverse of the
+//                                       cell's slope limiter (per-neighbour contributions)
+//   k_nbr_rev       per cell            ordered gather of the neighbours' slope contributions
+//
+// Edges left dry keep their previous balance terms in the forward step (swSpHyp.cpp:339), so a
+// slot's adjoint carries over to the previous step until a step that computed that flux.  All
+// sums run in a fixed order; no floating-point atomics are used, so gradients are bitwise
+// reproducible and independent of the checkpoint interval.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sw2d_internal.cuh"
+#include "sp_adjoint.cuh"
+
+using namespace sw2d;
+
+namespace sw2d {
+
+struct AdjointState {
+    int64_t nslot = 0, ncint = 0;
+    // trajectory
+    int64_t n_steps = 0, every = 0, n_ck = 0;
+    long long base_steps = 0;
+    double dt_before = 0.0;              // dt of the step before the trajectory (MUSCL-EVR uses it)
+    std::vector<double> dt_seq, t_seq;   // dt_j and the time at the start of step j
+    double* d_dt_seq = nullptr;
+    double* d_t_seq = nullptr;
+    // checkpoints k = 0 .. n_ck-1 at step k*every, and the end of the trajectory
+    double4* ck_st = nullptr;            // (n_ck + 1) * nc
+    double4* ck_slot = nullptr;          // (n_ck + 1) * nslot
+    Ctrl* ck_ctrl = nullptr;             // n_ck + 1
+    bool ck_valid = false;
+    // one segment of recomputed steps
+    double4* seg_st = nullptr;           // (every + 1) * nc
+    double4* seg_bal = nullptr;          // every * nc
+    // adjoint buffers
+    double4* lam = nullptr;              // nc: adjoint of the state {h, q, r, -}
+    double4* sig = nullptr;              // nslot: adjoint of the balance slots {a, b, c, -}
+    double4* ctb = nullptr;              // nslot: per-slot contributions {h, q, r, z_b}
+    double2* cts = nullptr;              // nslot: per-slot slope contributions {sx, sy}
+    double* znb = nullptr;               // ncint: per-neighbour-entry z contributions
+    int* mirror = nullptr;               // ncint: entry of the same edge in the neighbour's list
+    double* g_zb = nullptr;
+    double* g_k1 = nullptr;
+    double* g_k2 = nullptr;
+    Ctrl* ctrl_rev = nullptr;            // control block that keeps recomputed slopes active
+    double* d_Jobs = nullptr;            // n_obs: cost of each observation
+    double* d_part = nullptr;
+    double* stage = nullptr;             // nc doubles for parameter transfers
+    // observations
+    int64_t n_pts = 0, n_obs = 0;
+    int normalize = 0;
+    std::vector<int64_t> obs_steps;
+    std::vector<int> obs_at;             // [n_steps + 1] observation index of a step, or -1
+    int* d_pts = nullptr;
+    double *d_wh = nullptr, *d_wq = nullptr, *d_hobs = nullptr, *d_qobs = nullptr, *d_robs = nullptr;
+    std::vector<void*> traj_allocs, obs_allocs, fixed_allocs;
+};
+
+}  // namespace sw2d
+
+namespace {
+
+constexpr int kCostBlocks = 256;
+
+// ------------------------------------------------------------------------------------------
+// small kernels of the record / replay loop
+// ------------------------------------------------------------------------------------------
+
+// after k_cfl in a recorded run: keep dt_j and t_j of the step about to be taken
+__global__ void k_note_dt(const Ctrl* ctrl, double* dt_seq, double* t_seq, long long base)
+{
+    if (ctrl->go) {
+        const long long j = ctrl->steps - base;
+        dt_seq[j] = ctrl->dt;
+        t_seq[j] = ctrl->t;
+    }
+}
+
+// in place of k_cfl in a replay: the recorded dt of step j (the host launches exactly the
+// recorded number of steps, so j stays inside dt_seq)
+__global__ void k_frozen_dt(Ctrl* ctrl, const double* dt_seq, long long base)
+{
+    const long long j = ctrl->steps - base;
+    ctrl->dt = dt_seq[j];
+    ctrl->go = 1;
+}
+
+// z = h + z_b of a state array after a change of z_b
+__global__ void k_refresh_z(double4* st, const double* zbv, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        double4 s = st[i];
+        s.w = s.x + zbv[i];
+        st[i] = s;
+    }
+}
+
+// dst[i*stride + offset] = src[perm[i]]: a caller-numbered array into one component of an
+// internal-numbered record array
+__global__ void k_gather_component(const double* __restrict__ src, const int* __restrict__ perm, double* dst, int stride,
+                                   int offset, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[(size_t)i * stride + offset] = src[perm[i]];
+}
+
+// out[perm[i]] = src[i*stride + offset]: an internal-numbered array back to the caller's numbering
+__global__ void k_scatter_cells(const double* __restrict__ src, int stride, int offset, const int* __restrict__ perm,
+                                double* out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[perm[i]] = src[(size_t)i * stride + offset];
+}
+
+// mirror[k] = the entry of the same internal edge in the neighbour's list
+__global__ void k_mirror(const int2* __restrict__ coff, const int2* __restrict__ cint, int* mirror, int nc)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    for (int k = coff[c].x; k < coff[c + 1].x; k++) {
+        const int2 e = cint[k];
+        const int want = e.x ^ 1;
+        int found = -1;
+        for (int kk = coff[e.y].x; kk < coff[e.y + 1].x; kk++)
+            if (cint[kk].x == want) found = kk;
+        mirror[k] = found;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// cost: per-block partial sums in a fixed tree, then one thread adds them in block order
+// ------------------------------------------------------------------------------------------
+struct ObsView {
+    const int* pts;
+    const double *wh, *wq;       // wq may be null
+    const double *hobs, *qobs, *robs;  // this observation's values
+    int n;
+    double scale;                // 1 or 1 / n_obs
+};
+
+__device__ __forceinline__ double obs_term(const ObsView& o, const double4* st, int i)
+{
+    const double4 s = st[o.pts[i]];
+    const double dh = s.x - o.hobs[i];
+    double v = o.wh[i] * (dh * dh);
+    if (o.wq) {
+        const double dq = s.y - o.qobs[i], dr = s.z - o.robs[i];
+        v += o.wq[i] * ((dq * dq) + (dr * dr));
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_obs_cost(ObsView o, const double4* st, double* part)
+{
+    __shared__ double sh[kBlock];
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += gridDim.x * blockDim.x) acc += obs_term(o, st, i);
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_obs_finish(const double* part, int nblocks, double scale, double* J_obs)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += part[b];
+        *J_obs = s * scale;
+    }
+}
+
+// d(scale * term)/d(state) at the observed cells; cells are distinct, so no two threads meet
+__global__ void k_obs_rev(ObsView o, const double4* st, double4* lam)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= o.n) return;
+    const int c = o.pts[i];
+    const double4 s = st[c];
+    double4 l = lam[c];
+    l.x += 2.0 * o.wh[i] * (s.x - o.hobs[i]) * o.scale;
+    if (o.wq) {
+        l.y += 2.0 * o.wq[i] * (s.y - o.qobs[i]) * o.scale;
+        l.z += 2.0 * o.wq[i] * (s.z - o.robs[i]) * o.scale;
+    }
+    lam[c] = l;
+}
+
+// ------------------------------------------------------------------------------------------
+// reverse kernels
+// ------------------------------------------------------------------------------------------
+
+// Reverse of k_update for one step: lam holds the adjoint of the state after the step and
+// becomes the adjoint of the state before it (balance part); the slots' adjoints gain
+// dt * (adjoint of the post-balance state); friction-coefficient gradients accumulate.
+template <int kFriction, bool kHeadLoss>
+__global__ void __launch_bounds__(kBlock) k_update_rev(DevMesh m, const double4* __restrict__ bal, double4* lam,
+                                                       double4* sig, double* gk1, double* gk2, double dt)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    UpdateParams p;
+    p.friction = kFriction;
+    p.head_loss = kHeadLoss;
+    p.clamp_negative = !m.neg_detect;
+    p.h_min = m.h_min;
+    p.v_max = m.v_max;
+    p.fr_max = m.fr_max;
+    p.dt = dt;
+    p.k1 = p.k2 = 0.0;
+    p.fcos = 1.0;
+    p.fsin = 0.0;
+    p.hs = p.hk1 = p.hk2 = 0.0;
+    p.hcos = 1.0;
+    p.hsin = 0.0;
+    if (kFriction != SW2D_FRICTION_NONE) {
+        const double4 f = ld(&m.fric[c]);
+        p.k1 = f.x;
+        p.k2 = f.y;
+        p.fcos = f.z;
+        p.fsin = f.w;
+    }
+    if (kHeadLoss) {
+        const double4 a = ld(&m.hla[c]);
+        const double2 b = ld(&m.hlb[c]);
+        p.hs = a.x;
+        p.hk1 = a.y;
+        p.hk2 = a.z;
+        p.hcos = b.x;
+        p.hsin = b.y;
+    }
+    const double4 B = bal[c];
+    const double4 l = lam[c];
+    double hb, qb, rb, k1b = 0.0, k2b = 0.0;
+    update_cell_rev(p, B.x, B.y, B.z, l.x, l.y, l.z, hb, qb, rb, k1b, k2b);
+    if (kFriction != SW2D_FRICTION_NONE) {
+        gk1[c] += k1b;
+        gk2[c] += k2b;
+    }
+    lam[c] = make_double4(hb, qb, rb, 0.0);
+    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
+    const double a = hb * dt, b = qb * dt, cc = rb * dt;
+    for (int k = k0; k < k1; k++) {
+        double4 s = sig[k];
+        s.x += a;
+        s.y += b;
+        s.z += cc;
+        sig[k] = s;
+    }
+}
+
+// Flux adjoints of one balance slot {a, b, c} = {f1 F1, f2F2 F2 + f2S2 S + f2F3 F3,
+// f3F2 F2 + f3S2 S + f3F3 F3} (factors of swSp::computeEdgeFactors, swSp.cpp:398-427)
+struct SlotFactors {
+    double f1, f2F2, f2F3, f2S2, f3F2, f3F3, f3S2;
+};
+
+__device__ __forceinline__ void slot_rev(const SlotFactors& f, const double4& s, double& F1b, double& F2b, double& F3b,
+                                         double& Sb)
+{
+    F1b += f.f1 * s.x;
+    F2b += f.f2F2 * s.y + f.f3F2 * s.z;
+    F3b += f.f2F3 * s.y + f.f3F3 * s.z;
+    Sb += f.f2S2 * s.y + f.f3S2 * s.z;
+}
+
+template <int kScheme, bool kBlending>
+__global__ void __launch_bounds__(kBlock) k_edges_rev(DevMesh m, double4* sig, double4* ctb, double2* cts, double t,
+                                                      double dtp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m.ni) {
+        const int e = i;
+        const int2 lr = ld(&m.lr[e]);
+        const int a = lr.x, b = lr.y;
+        const double2 n = ld(&m.nxy[e]);
+        const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
+        const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
+        double2 mp = make_double2(0.0, 0.0), xa = mp, xb = mp, ga = mp, gb = mp;
+        SideState SL, SR;
+        if (kScheme == SW2D_SCHEME_GODUNOV) {
+            SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
+            SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
+        } else {
+            mp = ld(&m.mxy[e]);
+            xa = ld(&m.cxy[a]);
+            xb = ld(&m.cxy[b]);
+            ga = m.slope[a];
+            gb = m.slope[b];
+            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y, dtp,
+                          m.dry);
+            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y, dtp,
+                          m.dry);
+        }
+        const int2 sl = ld(&m.eslot[e]);
+        const double hL = SL.z - ca.x, hR = SR.z - cb.x;
+        if (!((hL > m.h_min) || (hR > m.h_min))) {
+            // flux not computed at this step: the slots keep their values and their adjoints
+            ctb[sl.x] = make_double4(0.0, 0.0, 0.0, 0.0);
+            ctb[sl.y] = make_double4(0.0, 0.0, 0.0, 0.0);
+            cts[sl.x] = make_double2(0.0, 0.0);
+            cts[sl.y] = make_double2(0.0, 0.0);
+            return;
+        }
+        const double2 cf = ld(&m.coef[e]);
+        const double nx = n.x, ny = n.y;
+        EdgeFlux fb;
+        fb.f1 = fb.f2 = fb.f3 = fb.sl = fb.sr = 0.0;
+        fb.bad = 0;
+        {
+            const double c = cf.x;
+            const SlotFactors f{-c, -c * nx, +c * ny, +c * nx, -c * ny, -c * nx, +c * ny};
+            slot_rev(f, sig[sl.x], fb.f1, fb.f2, fb.f3, fb.sl);
+        }
+        {
+            const double c = cf.y;
+            const SlotFactors f{+c, +c * nx, -c * ny, +c * nx, +c * ny, +c * nx, +c * ny};
+            slot_rev(f, sig[sl.y], fb.f1, fb.f2, fb.f3, fb.sr);
+        }
+        sig[sl.x] = make_double4(0.0, 0.0, 0.0, 0.0);
+        sig[sl.y] = make_double4(0.0, 0.0, 0.0, 0.0);
+        SideBar Lb{0, 0, 0, 0, 0}, Rb{0, 0, 0, 0, 0};
+        double zbLb = 0.0, zbRb = 0.0;
+        hllc_rev(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min, fb, Lb, Rb, zbLb, zbRb);
+        CellBar A{0, 0, 0, 0, 0, 0, 0}, Bc{0, 0, 0, 0, 0, 0, 0};
+        if (kScheme == SW2D_SCHEME_GODUNOV) {
+            godunov_side_rev(sa.x, sa.y, sa.z, ca.y, nx, ny, Lb, A);
+            godunov_side_rev(sb.x, sb.y, sb.z, cb.y, nx, ny, Rb, Bc);
+        } else {
+            evr_side_rev(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, nx, ny, dtp, Lb, A);
+            evr_side_rev(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, nx, ny, dtp, Rb,
+                         Bc);
+        }
+        // z_c = h + z_b of the cell
+        ctb[sl.x] = make_double4(A.h + A.zc, A.q, A.r, A.zb + zbLb + A.zc);
+        ctb[sl.y] = make_double4(Bc.h + Bc.zc, Bc.q, Bc.r, Bc.zb + zbRb + Bc.zc);
+        cts[sl.x] = make_double2(A.sx, A.sy);
+        cts[sl.y] = make_double2(Bc.sx, Bc.sy);
+    } else if (i < m.ni + m.nb) {
+        const int e = i - m.ni;
+        const int c = ld(&m.bcell[e]);
+        const double4 s = ld(&m.st[c]);
+        const double4 cs = ld(&m.cst[c]);
+        const double4 g = ld(&m.bgeo[e]);
+        const SideState S = godunov_side(s.x, s.y, s.z, cs.x, cs.y, g.x, g.y);
+        const int k = ld(&m.bbc[e]);
+        const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
+        const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, t);
+        const int sb = ld(&m.bslot[e]);
+        const double cf = g.w, nx = g.x, ny = g.y;
+        const SlotFactors f{+cf, +cf * nx, -cf * ny, +cf * nx, +cf * ny, +cf * nx, +cf * ny};
+        double F1b = 0.0, F2b = 0.0, F3b = 0.0, Sb = 0.0;
+        slot_rev(f, sig[sb], F1b, F2b, F3b, Sb);
+        sig[sb] = make_double4(0.0, 0.0, 0.0, 0.0);
+        SideBar sbar{0, 0, 0, 0, 0};
+        double zbb = 0.0;
+        boundary_flux_rev(cs.y, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, F1b, F2b, F3b, sbar, zbb);
+        CellBar A{0, 0, 0, 0, 0, 0, 0};
+        godunov_side_rev(s.x, s.y, s.z, cs.y, nx, ny, sbar, A);
+        ctb[sb] = make_double4(A.h, A.q, A.r, A.zb + zbb);
+        cts[sb] = make_double2(0.0, 0.0);
+    }
+}
+
+// Ordered gather of the slot contributions of each cell, then (MUSCL-EVR) the reverse of its
+// slope limiter: the cell's own z contribution is applied here, the neighbours' go to znb.
+template <bool kMuscl>
+__global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, const double4* __restrict__ ctb,
+                                                      const double2* __restrict__ cts, double* gzb, double* znb)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
+    double hb = 0.0, qb = 0.0, rb = 0.0, zbb = 0.0, sxb = 0.0, syb = 0.0;
+    for (int k = k0; k < k1; k++) {
+        const double4 v = ctb[k];
+        hb += v.x;
+        qb += v.y;
+        rb += v.z;
+        zbb += v.w;
+        if (kMuscl) {
+            const double2 w = cts[k];
+            sxb += w.x;
+            syb += w.y;
+        }
+    }
+    if (kMuscl) {
+        const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
+        const int cnt = e1 - e0;
+        if (sxb != 0.0 || syb != 0.0) {
+            if (cnt > kMaxNbr) {
+                atomicOr(&m.ctrl->status, kStatusUnsupported);  // degree beyond the reverse's table
+            } else {
+                SlopeNbr nb[kMaxNbr];
+                const double zc = m.st[c].w;
+                const double2 xy = ld(&m.cxy[c]);
+                for (int i = 0; i < cnt; i++) {
+                    const int2 en = ld(&m.cint[e0 + i]);
+                    const double2 xj = ld(&m.cxy[en.y]);
+                    const double2 mp = ld(&m.mxy[en.x >> 1]);
+                    nb[i].zj = m.st[en.y].w;
+                    nb[i].dx = xj.x - xy.x;
+                    nb[i].dy = xj.y - xy.y;
+                    nb[i].ax = mp.x - xy.x;
+                    nb[i].ay = mp.y - xy.y;
+                    nb[i].c_is_r = (en.x & 1) != 0;
+                }
+                double zcb = 0.0, zjb[kMaxNbr];
+                slopes_rev(zc, cnt, nb, sxb, syb, zcb, zjb);
+                hb += zcb;
+                zbb += zcb;
+                for (int i = 0; i < cnt; i++) znb[e0 + i] = zjb[i];
+            }
+        } else {
+            for (int i = e0; i < e1; i++) znb[i] = 0.0;
+        }
+    }
+    double4 l = lam[c];
+    l.x += hb;
+    l.y += qb;
+    l.z += rb;
+    lam[c] = l;
+    gzb[c] += zbb;
+}
+
+// z contributions of the neighbours' slope limiters, gathered in the cell's entry order
+__global__ void __launch_bounds__(kBlock) k_nbr_rev(DevMesh m, const int* __restrict__ mirror,
+                                                    const double* __restrict__ znb, double4* lam, double* gzb)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
+    double s = 0.0;
+    for (int k = e0; k < e1; k++) {
+        const int mk = ld(&mirror[k]);  // every internal edge has an entry on both sides
+        if (mk >= 0) s += znb[mk];
+    }
+    lam[c].x += s;
+    gzb[c] += s;
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+template <class T>
+int adj_alloc(sw2d_handle* h, std::vector<void*>& list, size_t n, T** out)
+{
+    void* p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)));
+    list.push_back(p);
+    CK(cudaMemsetAsync(p, 0, std::max<size_t>(1, n) * sizeof(T), h->stream));
+    *out = static_cast<T*>(p);
+    return SW2D_OK;
+}
+
+void free_list(std::vector<void*>& list)
+{
+    for (void* p : list) cudaFree(p);
+    list.clear();
+}
+
+// buffers that depend only on the mesh
+int adjoint_fixed(sw2d_handle* h)
+{
+    if (h->adj) return SW2D_OK;
+    AdjointState* a = new AdjointState();
+    h->adj = a;
+    int2 last{0, 0};
+    CK(cudaMemcpyAsync(&last, h->m.coff + h->nc, sizeof(int2), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    a->ncint = last.x;
+    a->nslot = last.y;
+    int rc = SW2D_OK;
+    auto& L = a->fixed_allocs;
+    if ((rc = adj_alloc(h, L, h->nc, &a->lam)) || (rc = adj_alloc(h, L, a->nslot, &a->sig)) ||
+        (rc = adj_alloc(h, L, a->nslot, &a->ctb)) || (rc = adj_alloc(h, L, a->nslot, &a->cts)) ||
+        (rc = adj_alloc(h, L, a->ncint, &a->znb)) || (rc = adj_alloc(h, L, a->ncint, &a->mirror)) ||
+        (rc = adj_alloc(h, L, h->nc, &a->g_zb)) || (rc = adj_alloc(h, L, h->nc, &a->g_k1)) ||
+        (rc = adj_alloc(h, L, h->nc, &a->g_k2)) || (rc = adj_alloc(h, L, 1, &a->ctrl_rev)) ||
+        (rc = adj_alloc(h, L, kCostBlocks, &a->d_part)) ||
+        (rc = adj_alloc(h, L, h->nc, &a->stage)))
+        return rc;
+    Ctrl cr{};
+    cr.t = 0.0;
+    cr.t_max = 1.0;
+    CK(cudaMemcpyAsync(a->ctrl_rev, &cr, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
+    if (h->nc > 0) k_mirror<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m.coff, h->m.cint, a->mirror, (int)h->nc);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
+int require_trajectory(sw2d_handle* h)
+{
+    if (!h->adj || h->adj->n_steps <= 0) return fail(h, SW2D_E_ARG, "no recorded trajectory (call sw2d_record first)");
+    return SW2D_OK;
+}
+
+// copies of the state, the slots and the control block into / out of checkpoint k
+int ck_save(sw2d_handle* h, int64_t k)
+{
+    AdjointState* a = h->adj;
+    CK(cudaMemcpyAsync(a->ck_st + k * h->nc, h->m.st, h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(a->ck_slot + k * a->nslot, h->m.slot, a->nslot * sizeof(double4), cudaMemcpyDeviceToDevice,
+                       h->stream));
+    CK(cudaMemcpyAsync(a->ck_ctrl + k, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, h->stream));
+    return SW2D_OK;
+}
+
+int ck_load(sw2d_handle* h, int64_t k)
+{
+    AdjointState* a = h->adj;
+    CK(cudaMemcpyAsync(h->m.st, a->ck_st + k * h->nc, h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->m.slot, a->ck_slot + k * a->nslot, a->nslot * sizeof(double4), cudaMemcpyDeviceToDevice,
+                       h->stream));
+    CK(cudaMemcpyAsync(h->ctrl, a->ck_ctrl + k, sizeof(Ctrl), cudaMemcpyDeviceToDevice, h->stream));
+    return SW2D_OK;
+}
+
+ObsView obs_view(const AdjointState* a, int k)
+{
+    ObsView o;
+    o.pts = a->d_pts;
+    o.wh = a->d_wh;
+    o.wq = a->d_wq;
+    o.hobs = a->d_hobs + (size_t)k * a->n_pts;
+    o.qobs = a->d_qobs ? a->d_qobs + (size_t)k * a->n_pts : nullptr;
+    o.robs = a->d_robs ? a->d_robs + (size_t)k * a->n_pts : nullptr;
+    o.n = (int)a->n_pts;
+    o.scale = (a->normalize && a->n_obs > 0) ? 1.0 / (double)a->n_obs : 1.0;
+    return o;
+}
+
+void cost_at(sw2d_handle* h, int k, const double4* st)
+{
+    AdjointState* a = h->adj;
+    const ObsView o = obs_view(a, k);
+    const int nb = std::max(1, std::min(kCostBlocks, (int)grid_for(a->n_pts)));
+    k_obs_cost<<<nb, kBlock, 0, h->stream>>>(o, st, a->d_part);
+    k_obs_finish<<<1, 32, 0, h->stream>>>(a->d_part, nb, o.scale, a->d_Jobs + k);
+}
+
+int obs_index(const AdjointState* a, int64_t step)
+{
+    if (a->n_obs == 0 || step < 0 || step >= (int64_t)a->obs_at.size()) return -1;
+    return a->obs_at[step];
+}
+
+// Forward over the recorded trajectory from checkpoint 0 with the recorded dt (replay) or the
+// CFL dt (record), storing checkpoints and adding the observation cost.
+int run_trajectory(sw2d_handle* h, bool record, bool with_cost)
+{
+    AdjointState* a = h->adj;
+    int rc = ck_load(h, 0);
+    if (rc) return rc;
+    if (with_cost) {
+        const int k = obs_index(a, 0);
+        if (k >= 0) cost_at(h, k, h->m.st);
+    }
+    for (int64_t j = 0; j < a->n_steps; j++) {
+        if (j % a->every == 0 && j > 0 && (rc = ck_save(h, j / a->every))) return rc;
+        launch_slopes_on(h, h->m);
+        launch_edges_on(h, h->m);
+        if (record) {
+            launch_cfl_on(h, h->m);
+            k_note_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->d_t_seq, a->base_steps);
+        } else {
+            k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
+        }
+        launch_update_on(h, h->m, false);
+        if (with_cost) {
+            const int k = obs_index(a, j + 1);
+            if (k >= 0) cost_at(h, k, h->m.st);
+        }
+    }
+    if ((rc = ck_save(h, a->n_ck))) return rc;
+    CK(cudaGetLastError());
+    return SW2D_OK;
+}
+
+int read_status(sw2d_handle* h)
+{
+    CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return status_to_code(h, h->ctrl_host->status);
+}
+
+template <int kF>
+void launch_update_rev_f(sw2d_handle* h, const double4* bal, double dt)
+{
+    AdjointState* a = h->adj;
+    const unsigned g = grid_for(h->nc);
+    if (h->p.singular_head_loss)
+        k_update_rev<kF, true><<<g, kBlock, 0, h->stream>>>(h->m, bal, a->lam, a->sig, a->g_k1, a->g_k2, dt);
+    else
+        k_update_rev<kF, false><<<g, kBlock, 0, h->stream>>>(h->m, bal, a->lam, a->sig, a->g_k1, a->g_k2, dt);
+}
+
+void launch_update_rev(sw2d_handle* h, const double4* bal, double dt)
+{
+    switch (h->p.friction) {
+        case SW2D_FRICTION_CHEZY: launch_update_rev_f<SW2D_FRICTION_CHEZY>(h, bal, dt); break;
+        case SW2D_FRICTION_MANNING: launch_update_rev_f<SW2D_FRICTION_MANNING>(h, bal, dt); break;
+        case SW2D_FRICTION_STRICKLER: launch_update_rev_f<SW2D_FRICTION_STRICKLER>(h, bal, dt); break;
+        default: launch_update_rev_f<SW2D_FRICTION_NONE>(h, bal, dt); break;
+    }
+}
+
+void launch_edges_rev(sw2d_handle* h, const DevMesh& m, double t, double dtp)
+{
+    AdjointState* a = h->adj;
+    const unsigned g = grid_for(m.ni + m.nb);
+    const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
+    if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
+        if (bl) k_edges_rev<SW2D_SCHEME_GODUNOV, true><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+        else k_edges_rev<SW2D_SCHEME_GODUNOV, false><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+    } else {
+        if (bl) k_edges_rev<SW2D_SCHEME_MUSCL_EVR, true><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+        else k_edges_rev<SW2D_SCHEME_MUSCL_EVR, false><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+    }
+}
+
+int scatter_cells(sw2d_handle* h, const double* src, int stride, int offset, double* out)
+{
+    if (!out) return SW2D_OK;
+    AdjointState* a = h->adj;
+    k_scatter_cells<<<grid_for(h->nc), kBlock, 0, h->stream>>>(src, stride, offset, h->d_cell_perm, a->stage,
+                                                                       (int)h->nc);
+    CK(cudaMemcpyAsync(out, a->stage, h->nc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// sum of the per-observation costs, in observation order
+int total_cost(sw2d_handle* h, double* J)
+{
+    AdjointState* a = h->adj;
+    std::vector<double> v(a->n_obs, 0.0);
+    if (a->n_obs > 0)
+        CK(cudaMemcpyAsync(v.data(), a->d_Jobs, a->n_obs * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double s = 0.0;
+    for (double x : v) s += x;
+    if (J) *J = s;
+    return SW2D_OK;
+}
+
+int check_observations(sw2d_handle* h)
+{
+    AdjointState* a = h->adj;
+    if (a->n_obs <= 0) return fail(h, SW2D_E_ARG, "no observations (call sw2d_set_observations)");
+    if (a->obs_steps.back() > a->n_steps)
+        return fail(h, SW2D_E_ARG, "an observation step lies beyond the recorded trajectory");
+    a->obs_at.assign(a->n_steps + 1, -1);
+    for (int64_t k = 0; k < a->n_obs; k++) a->obs_at[a->obs_steps[k]] = (int)k;
+    return SW2D_OK;
+}
+
+// Reverse sweep over the segments (checkpoints must be valid).  Leaves the gradients in lam,
+// g_zb, g_k1, g_k2, the per-observation costs in d_Jobs, and the model at the trajectory's end.
+int reverse_sweep(sw2d_handle* h)
+{
+    AdjointState* a = h->adj;
+    const int64_t nc = h->nc;
+    const bool muscl = h->p.scheme == SW2D_SCHEME_MUSCL_EVR;
+    CK(cudaMemsetAsync(a->lam, 0, nc * sizeof(double4), h->stream));
+    CK(cudaMemsetAsync(a->sig, 0, a->nslot * sizeof(double4), h->stream));
+    CK(cudaMemsetAsync(a->g_zb, 0, nc * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(a->g_k1, 0, nc * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(a->g_k2, 0, nc * sizeof(double), h->stream));
+    const unsigned gc = grid_for(nc);
+    int rc = SW2D_OK;
+    for (int64_t s = a->n_ck - 1; s >= 0; s--) {
+        const int64_t j0 = s * a->every, j1 = std::min(a->n_steps, j0 + a->every);
+        if ((rc = ck_load(h, s))) return rc;
+        // recompute the segment, keeping each step's state and post-balance state
+        for (int64_t j = j0; j < j1; j++) {
+            double4* stj = a->seg_st + (j - j0) * nc;
+            CK(cudaMemcpyAsync(stj, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+            DevMesh mj = h->m;
+            mj.bal = a->seg_bal + (j - j0) * nc;
+            launch_slopes_on(h, mj);
+            launch_edges_on(h, mj);
+            k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
+            launch_update_on(h, mj, true);
+            const int k = obs_index(a, j + 1);
+            if (k >= 0) cost_at(h, k, h->m.st);
+        }
+        CK(cudaMemcpyAsync(a->seg_st + (j1 - j0) * nc, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice,
+                           h->stream));
+        // reverse steps
+        for (int64_t j = j1 - 1; j >= j0; j--) {
+            const int k = obs_index(a, j + 1);
+            if (k >= 0 && a->n_pts > 0)
+                k_obs_rev<<<grid_for(a->n_pts), kBlock, 0, h->stream>>>(obs_view(a, k), a->seg_st + (j + 1 - j0) * nc,
+                                                                        a->lam);
+            launch_update_rev(h, a->seg_bal + (j - j0) * nc, a->dt_seq[j]);
+            DevMesh mr = h->m;
+            mr.st = a->seg_st + (j - j0) * nc;
+            if (muscl) {
+                DevMesh ms = mr;
+                ms.ctrl = a->ctrl_rev;  // always active: recompute the slopes of step j
+                launch_slopes_on(h, ms);
+            }
+            launch_edges_rev(h, mr, a->t_seq[j], j > 0 ? a->dt_seq[j - 1] : a->dt_before);
+            if (muscl) {
+                k_cells_rev<true><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb, a->znb);
+                k_nbr_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->mirror, a->znb, a->lam, a->g_zb);
+            } else {
+                k_cells_rev<false><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb, a->znb);
+            }
+        }
+        CK(cudaGetLastError());
+    }
+    const int k0 = obs_index(a, 0);
+    if (k0 >= 0 && a->n_pts > 0) {
+        k_obs_rev<<<grid_for(a->n_pts), kBlock, 0, h->stream>>>(obs_view(a, k0), a->ck_st, a->lam);
+        cost_at(h, k0, a->ck_st);
+    }
+    if ((rc = ck_load(h, a->n_ck))) return rc;
+    CK(cudaGetLastError());
+    return SW2D_OK;
+}
+
+int alloc_trajectory(sw2d_handle* h, int64_t n_steps, int64_t every)
+{
+    AdjointState* a = h->adj;
+    free_list(a->traj_allocs);
+    a->ck_valid = false;
+    a->n_steps = n_steps;
+    a->every = every;
+    a->n_ck = (n_steps + every - 1) / every;
+    const int64_t nc = h->nc, seg = std::min(every, n_steps);
+    auto& L = a->traj_allocs;
+    int rc = SW2D_OK;
+    if ((rc = adj_alloc(h, L, (a->n_ck + 1) * nc, &a->ck_st)) ||
+        (rc = adj_alloc(h, L, (a->n_ck + 1) * a->nslot, &a->ck_slot)) ||
+        (rc = adj_alloc(h, L, a->n_ck + 1, &a->ck_ctrl)) || (rc = adj_alloc(h, L, (seg + 1) * nc, &a->seg_st)) ||
+        (rc = adj_alloc(h, L, seg * nc, &a->seg_bal)) || (rc = adj_alloc(h, L, n_steps, &a->d_dt_seq)) ||
+        (rc = adj_alloc(h, L, n_steps, &a->d_t_seq))) {
+        free_list(a->traj_allocs);
+        a->n_steps = 0;
+        return rc;
+    }
+    return SW2D_OK;
+}
+
+}  // namespace
+
+namespace sw2d {
+
+void adjoint_release(sw2d_handle* h)
+{
+    if (!h || !h->adj) return;
+    free_list(h->adj->traj_allocs);
+    free_list(h->adj->obs_allocs);
+    free_list(h->adj->fixed_allocs);
+    delete h->adj;
+    h->adj = nullptr;
+}
+
+void adjoint_invalidate(sw2d_handle* h)
+{
+    if (h && h->adj) h->adj->ck_valid = false;
+}
+
+}  // namespace sw2d
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int sw2d_record(sw2d_handle* h, int64_t n_steps, int64_t checkpoint_every, int64_t* steps_done)
+{
+    if (!h || n_steps <= 0 || checkpoint_every <= 0) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (n_steps >= (int64_t)1 << 31) return fail(h, SW2D_E_ARG, "trajectory too long");
+    CK(cudaSetDevice(h->device));
+    int rc = adjoint_fixed(h);
+    if (rc) return rc;
+    AdjointState* a = h->adj;
+    if ((rc = alloc_trajectory(h, n_steps, checkpoint_every))) return rc;
+    CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->ctrl_host->status) return status_to_code(h, h->ctrl_host->status);
+    a->base_steps = h->ctrl_host->steps;
+    a->dt_before = h->ctrl_host->dt;
+    if ((rc = ck_save(h, 0))) return rc;
+    if ((rc = run_trajectory(h, true, false))) return rc;
+    CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int64_t done = h->ctrl_host->steps - a->base_steps;
+    if (steps_done) *steps_done = done;
+    if ((rc = status_to_code(h, h->ctrl_host->status))) {
+        a->n_steps = 0;
+        return rc;
+    }
+    if (done <= 0) {
+        a->n_steps = 0;
+        return fail(h, SW2D_E_ARG, "no step recorded: the run is already at t_max");
+    }
+    if (done < n_steps) {  // t_max reached: the trajectory ends there
+        a->n_steps = done;
+        a->n_ck = (done + checkpoint_every - 1) / checkpoint_every;
+        if ((rc = ck_save(h, a->n_ck))) return rc;
+    }
+    a->dt_seq.resize(a->n_steps);
+    a->t_seq.resize(a->n_steps);
+    CK(cudaMemcpyAsync(a->dt_seq.data(), a->d_dt_seq, a->n_steps * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(a->t_seq.data(), a->d_t_seq, a->n_steps * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    a->ck_valid = true;
+    return SW2D_OK;
+}
+
+int sw2d_trajectory_info(sw2d_handle* h, int64_t* n_steps, int64_t* checkpoint_every, double* t_start, double* t_end)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    int rc = require_trajectory(h);
+    if (rc) return rc;
+    const AdjointState* a = h->adj;
+    if (n_steps) *n_steps = a->n_steps;
+    if (checkpoint_every) *checkpoint_every = a->every;
+    if (t_start) *t_start = a->t_seq.front();
+    if (t_end) *t_end = a->t_seq.back() + a->dt_seq.back();
+    return SW2D_OK;
+}
+
+int sw2d_get_trajectory_dt(sw2d_handle* h, double* dt, int64_t capacity)
+{
+    if (!h || !dt) return fail(h, SW2D_E_ARG, "invalid arguments");
+    int rc = require_trajectory(h);
+    if (rc) return rc;
+    if (capacity < h->adj->n_steps) return fail(h, SW2D_E_ARG, "output buffer too small");
+    std::memcpy(dt, h->adj->dt_seq.data(), h->adj->n_steps * sizeof(double));
+    return SW2D_OK;
+}
+
+int sw2d_set_trajectory_start(sw2d_handle* h, const double* h0, const double* q0, const double* r0)
+{
+    if (!h || !h0 || !q0 || !r0) return fail(h, SW2D_E_ARG, "invalid arguments");
+    int rc = require_trajectory(h);
+    if (rc) return rc;
+    CK(cudaSetDevice(h->device));
+    AdjointState* a = h->adj;
+    const int64_t nc = h->nc;
+    const size_t bytes = nc * sizeof(double);
+    double* ck0 = reinterpret_cast<double*>(a->ck_st);
+    const double* src[3] = {h0, q0, r0};
+    for (int c = 0; c < 3; c++) {
+        CK(cudaMemcpyAsync(a->stage, src[c], bytes, cudaMemcpyHostToDevice, h->stream));
+        k_gather_component<<<grid_for(nc), kBlock, 0, h->stream>>>(a->stage, h->d_cell_perm, ck0, 4, c, (int)nc);
+    }
+    k_refresh_z<<<grid_for(nc), kBlock, 0, h->stream>>>(a->ck_st, h->m.zbv, (int)nc);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    a->ck_valid = false;
+    return SW2D_OK;
+}
+
+int sw2d_set_param(sw2d_handle* h, const char* name, const double* values)
+{
+    if (!h || !name || !values) return fail(h, SW2D_E_ARG, "invalid arguments");
+    CK(cudaSetDevice(h->device));
+    const int64_t nc = h->nc;
+    double* dst = nullptr;
+    int stride = 0, off = 0;
+    const bool f1 = std::strcmp(name, "friction_1") == 0, f2 = std::strcmp(name, "friction_2") == 0;
+    const bool fb = std::strcmp(name, "friction") == 0, zb = std::strcmp(name, "z_b") == 0;
+    if (f1 || f2 || fb) {
+        if (h->p.friction == SW2D_FRICTION_NONE) return fail(h, SW2D_E_ARG, "the model has no friction law");
+        dst = reinterpret_cast<double*>(const_cast<double4*>(h->m.fric));
+        stride = 4;
+        off = f2 ? 1 : 0;
+    } else if (zb) {
+        dst = reinterpret_cast<double*>(const_cast<double4*>(h->m.cst));
+        stride = 4;
+        off = 0;
+    } else {
+        return fail(h, SW2D_E_ARG, std::string("unknown parameter ") + name);
+    }
+    CK(cudaMemcpyAsync(h->stage, values, nc * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    k_gather_component<<<grid_for(nc), kBlock, 0, h->stream>>>(h->stage, h->d_cell_perm, dst, stride, off, (int)nc);
+    if (fb)
+        k_gather_component<<<grid_for(nc), kBlock, 0, h->stream>>>(h->stage, h->d_cell_perm, dst, stride, 1, (int)nc);
+    if (zb) {
+        k_gather_component<<<grid_for(nc), kBlock, 0, h->stream>>>(h->stage, h->d_cell_perm, const_cast<double*>(h->m.zbv),
+                                                                   1, 0, (int)nc);
+        // z = h + z_b of the current state and of the trajectory's initial state
+        k_refresh_z<<<grid_for(nc), kBlock, 0, h->stream>>>(h->m.st, h->m.zbv, (int)nc);
+        if (h->adj && h->adj->n_steps > 0)
+            k_refresh_z<<<grid_for(nc), kBlock, 0, h->stream>>>(h->adj->ck_st, h->m.zbv, (int)nc);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    adjoint_invalidate(h);
+    return SW2D_OK;
+}
+
+int sw2d_get_param(sw2d_handle* h, const char* name, double* values)
+{
+    if (!h || !name || !values) return fail(h, SW2D_E_ARG, "invalid arguments");
+    CK(cudaSetDevice(h->device));
+    const double* src = nullptr;
+    int off = 0;
+    if (std::strcmp(name, "friction_1") == 0 || std::strcmp(name, "friction_2") == 0) {
+        if (h->p.friction == SW2D_FRICTION_NONE) return fail(h, SW2D_E_ARG, "the model has no friction law");
+        src = reinterpret_cast<const double*>(h->m.fric);
+        off = name[9] == '2' ? 1 : 0;
+    } else if (std::strcmp(name, "z_b") == 0) {
+        src = reinterpret_cast<const double*>(h->m.cst);
+    } else {
+        return fail(h, SW2D_E_ARG, std::string("unknown parameter ") + name);
+    }
+    k_scatter_cells<<<grid_for(h->nc), kBlock, 0, h->stream>>>(src, 4, off, h->d_cell_perm, h->stage, (int)h->nc);
+    CK(cudaMemcpyAsync(values, h->stage, h->nc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
+int sw2d_set_observations(sw2d_handle* h, const sw2d_obs* obs)
+{
+    if (!h || !obs) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (obs->n_points < 0 || obs->n_times <= 0 || (obs->n_points > 0 && (!obs->cells || !obs->w_h || !obs->h_obs)) ||
+        !obs->steps)
+        return fail(h, SW2D_E_ARG, "incomplete observation set");
+    if (obs->w_q && (!obs->q_obs || !obs->r_obs)) return fail(h, SW2D_E_ARG, "w_q given without q_obs / r_obs");
+    CK(cudaSetDevice(h->device));
+    int rc = adjoint_fixed(h);
+    if (rc) return rc;
+    AdjointState* a = h->adj;
+    const int64_t np = obs->n_points, nt = obs->n_times;
+    std::vector<int> inv(h->nc), pts(np);
+    for (int64_t i = 0; i < h->nc; i++) inv[h->cell_perm[i]] = (int)i;
+    std::vector<char> seen(h->nc, 0);
+    for (int64_t i = 0; i < np; i++) {
+        const int64_t c = obs->cells[i];
+        if (c < 0 || c >= h->nc) return fail(h, SW2D_E_ARG, "observed cell out of range");
+        if (seen[c]) return fail(h, SW2D_E_ARG, "an observed cell appears twice");
+        seen[c] = 1;
+        pts[i] = inv[c];
+    }
+    for (int64_t k = 0; k < nt; k++)
+        if (obs->steps[k] < 0 || (k > 0 && obs->steps[k] <= obs->steps[k - 1]))
+            return fail(h, SW2D_E_ARG, "observation steps must be non-negative and increasing");
+    free_list(a->obs_allocs);
+    a->n_pts = 0;
+    a->n_obs = 0;
+    auto& L = a->obs_allocs;
+    a->d_wq = a->d_qobs = a->d_robs = nullptr;
+    if ((rc = adj_alloc(h, L, np, &a->d_pts)) || (rc = adj_alloc(h, L, np, &a->d_wh)) ||
+        (rc = adj_alloc(h, L, np * nt, &a->d_hobs)) || (rc = adj_alloc(h, L, nt, &a->d_Jobs)))
+        return rc;
+    if (obs->w_q && ((rc = adj_alloc(h, L, np, &a->d_wq)) || (rc = adj_alloc(h, L, np * nt, &a->d_qobs)) ||
+                     (rc = adj_alloc(h, L, np * nt, &a->d_robs))))
+        return rc;
+    if (np > 0) {
+        CK(cudaMemcpyAsync(a->d_pts, pts.data(), np * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(a->d_wh, obs->w_h, np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(a->d_hobs, obs->h_obs, np * nt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        if (obs->w_q) {
+            CK(cudaMemcpyAsync(a->d_wq, obs->w_q, np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(a->d_qobs, obs->q_obs, np * nt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(a->d_robs, obs->r_obs, np * nt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    a->n_pts = np;
+    a->n_obs = nt;
+    a->normalize = obs->normalize ? 1 : 0;
+    a->obs_steps.assign(obs->steps, obs->steps + nt);
+    return SW2D_OK;
+}
+
+int sw2d_replay_cost(sw2d_handle* h, double* J)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    int rc = require_trajectory(h);
+    if (rc) return rc;
+    CK(cudaSetDevice(h->device));
+    if ((rc = check_observations(h))) return rc;
+    if ((rc = run_trajectory(h, false, true))) return rc;
+    if ((rc = read_status(h))) return rc;
+    h->adj->ck_valid = true;
+    return total_cost(h, J);
+}
+
+int sw2d_replay_sample(sw2d_handle* h, int64_t n_points, const int64_t* cells, int64_t n_times, const int64_t* steps,
+                       double* h_out, double* q_out, double* r_out)
+{
+    if (!h || n_points <= 0 || n_times <= 0 || !cells || !steps || !h_out)
+        return fail(h, SW2D_E_ARG, "invalid arguments");
+    int rc = require_trajectory(h);
+    if (rc) return rc;
+    CK(cudaSetDevice(h->device));
+    AdjointState* a = h->adj;
+    for (int64_t k = 0; k < n_times; k++)
+        if (steps[k] < 0 || steps[k] > a->n_steps) return fail(h, SW2D_E_ARG, "sample step outside the trajectory");
+    // replay once (fresh checkpoints for the current parameters), then recompute each requested
+    // step from the checkpoint before it
+    if ((rc = run_trajectory(h, false, false))) return rc;
+    if ((rc = read_status(h))) return rc;
+    a->ck_valid = true;
+    std::vector<double4> st(h->nc);
+    std::vector<int> inv(h->nc);
+    for (int64_t i = 0; i < h->nc; i++) inv[h->cell_perm[i]] = (int)i;
+    for (int64_t k = 0; k < n_times; k++) {
+        const int64_t j = steps[k];
+        const int64_t s = std::min(j / a->every, a->n_ck);
+        if ((rc = ck_load(h, s))) return rc;
+        for (int64_t i = s * a->every; i < j; i++) {
+            launch_slopes_on(h, h->m);
+            launch_edges_on(h, h->m);
+            k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
+            launch_update_on(h, h->m, false);
+        }
+        CK(cudaMemcpyAsync(st.data(), h->m.st, h->nc * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int64_t p = 0; p < n_points; p++) {
+            const int64_t c = cells[p];
+            if (c < 0 || c >= h->nc) return fail(h, SW2D_E_ARG, "sampled cell out of range");
+            const double4 v = st[inv[c]];
+            h_out[k * n_points + p] = v.x;
+            if (q_out) q_out[k * n_points + p] = v.y;
+            if (r_out) r_out[k * n_points + p] = v.z;
+        }
+    }
+    if ((rc = ck_load(h, a->n_ck))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return read_status(h);
+}
+
+int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    int rc = require_trajectory(h);
+    if (rc) return rc;
+    CK(cudaSetDevice(h->device));
+    AdjointState* a = h->adj;
+    if ((rc = check_observations(h))) return rc;
+    if (!a->ck_valid) {
+        if ((rc = run_trajectory(h, false, false))) return rc;
+        if ((rc = read_status(h))) return rc;
+        a->ck_valid = true;
+    }
+    if ((rc = reverse_sweep(h))) return rc;
+    if ((rc = read_status(h))) return rc;
+    if ((rc = total_cost(h, J))) return rc;
+    if (grad) {
+        const double* lam = reinterpret_cast<const double*>(a->lam);
+        if ((rc = scatter_cells(h, lam, 4, 0, grad->h0)) || (rc = scatter_cells(h, lam, 4, 1, grad->q0)) ||
+            (rc = scatter_cells(h, lam, 4, 2, grad->r0)) || (rc = scatter_cells(h, a->g_zb, 1, 0, grad->z_b)))
+            return rc;
+        if (h->p.friction != SW2D_FRICTION_NONE) {
+            if ((rc = scatter_cells(h, a->g_k1, 1, 0, grad->friction_1)) ||
+                (rc = scatter_cells(h, a->g_k2, 1, 0, grad->friction_2)))
+                return rc;
+        } else {
+            if (grad->friction_1) std::memset(grad->friction_1, 0, h->nc * sizeof(double));
+            if (grad->friction_2) std::memset(grad->friction_2, 0, h->nc * sizeof(double));
+        }
+    }
+    return SW2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// sw2d_internal.cuh — definitions shared by the forward step (sw2d_sp.cu) and its adjoint
+// (sw2d_adjoint.cu): the device-resident loop control, the device view of the mesh and state,
+// the handle behind the C ABI, and the host helpers both translation units use.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/sw2d_b200.h"
+#include "sp_math.cuh"
+
+namespace sw2d {
+
+constexpr int kBlock = 256;
+
+// Device-resident loop control.  t and t_max decide whether a step runs; `go` and `dt` are
+// written by the CFL kernel's last block (or by the frozen-dt kernel of a replay) and read by
+// the update kernel.
+struct Ctrl {
+    double t;
+    double dt;
+    double t_max;
+    long long steps;
+    unsigned int status;
+    unsigned int blocks_done;
+    int go;
+    int pad;
+};
+
+struct DevMesh {
+    int nc, ni, nb;
+    // cells
+    double4* st;             // {h, q, r, z}
+    const double4* cst;      // {z_b, boussinesq, phi, area}
+    const double2* cxy;      // centroid
+    double2* slope;          // MUSCL slopes
+    const double4* fric;     // {k1, k2, cos a, sin a} (friction)
+    const double4* hla;      // {h_sing, k1, k2, -} (singular head loss)
+    const double2* hlb;      // {cos a, sin a}
+    const double* zbv;       // z_b
+    const double* area;
+    const int2* coff;        // [nc+1] {first internal-neighbour entry, first balance slot}
+    const int2* cint;        // {edge*2 + side, neighbour} (MUSCL slopes)
+    double4* slot;           // balance slots {a, b, c, -}
+    double* slot_w;          // CFL contribution of the slot
+    double4* bal;            // post-balance state {h, q, r, -} (written only by the recording update)
+    // internal edges
+    const int2* lr;
+    const int2* eslot;       // {slot of (L, e), slot of (R, e)}
+    const double2* nxy;
+    const double2* mxy;
+    const double* len;
+    const double2* coef;     // {coefL, coefR}
+    double2* flux;           // optional copy: 3 x double2 per edge {F1,F2},{F3,S2L},{S2R,-} (tests)
+    double* lmax;            // optional copy of lambda_max (tests)
+    // boundary edges
+    const int* bcell;
+    const int* bbc;
+    const int* bslot;
+    const double4* bgeo;     // {nx, ny, length, coef}
+    double4* bflux;          // optional copy {F1, F2, F3, -} (tests)
+    double* lmaxb;           // optional copy of lambda_max (tests)
+    // boundary series
+    const int* bctype;
+    const long long* bcoff;
+    const double *bctimes, *bcvals;
+    // parameters
+    double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
+    DryConsts dry;
+    int neg_detect;
+    // dt reduction scratch
+    double* part;
+    Ctrl* ctrl;
+};
+
+// read-only loads through the non-coherent path (data not written by the same kernel)
+template <class T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+__device__ __forceinline__ double4 ld(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_max; }
+
+inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+struct AdjointState;  // sw2d_adjoint.cu
+
+}  // namespace sw2d
+
+struct sw2d_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t nc = 0, ni = 0, nb = 0;
+    sw2d_params p{};
+    std::vector<int> cell_perm, int_perm, bnd_perm;  // [new] = caller index
+    std::vector<void*> allocs;
+    sw2d::DevMesh m{};
+    sw2d::Ctrl* ctrl = nullptr;
+    sw2d::Ctrl* ctrl_host = nullptr;  // pinned
+    int* d_cell_perm = nullptr;
+    int* d_int_perm = nullptr;
+    int* d_bnd_perm = nullptr;
+    double* stage = nullptr;    // 3 * nc doubles
+    double* lmax_buf = nullptr;   // allocated by the option record_wave_speeds
+    double* lmaxb_buf = nullptr;
+    double2* flux_buf = nullptr;  // allocated by the option record_fluxes
+    double4* bflux_buf = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int edge_variant = 0;   // index into kVariants (sw2d_autotune)
+    int slope_variant = 2;
+    sw2d::AdjointState* adj = nullptr;  // recorded trajectory, checkpoints and adjoint buffers
+    std::string err;
+};
+
+namespace sw2d {
+
+// Records `msg` as the handle's last error (or the creation error) and returns `code`.
+int fail(sw2d_handle* h, int code, const std::string& msg);
+// Maps the device status word to an SW2D_E_* code (and its message).
+int status_to_code(sw2d_handle* h, unsigned st);
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return ::sw2d::fail(h, SW2D_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dev_upload(sw2d_handle* h, const std::vector<T>& v, T** out)
+{
+    size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+    void* p = nullptr;
+    CK(cudaMalloc(&p, bytes));
+    h->allocs.push_back(p);
+    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    *out = static_cast<T*>(p);
+    return SW2D_OK;
+}
+
+template <class T>
+int dev_alloc(sw2d_handle* h, size_t n, T** out)
+{
+    void* p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)));
+    h->allocs.push_back(p);
+    CK(cudaMemsetAsync(p, 0, std::max<size_t>(1, n) * sizeof(T), h->stream));
+    *out = static_cast<T*>(p);
+    return SW2D_OK;
+}
+
+// Forward kernels on an explicit device view `m` (the handle's own, or one whose state points
+// into a replay buffer), on the handle's stream, with the handle's launch variants.
+void launch_slopes_on(sw2d_handle* h, const DevMesh& m);
+void launch_edges_on(sw2d_handle* h, const DevMesh& m);
+void launch_cfl_on(sw2d_handle* h, const DevMesh& m);
+// The update kernel; with store_balance it also writes the post-balance state to m.bal.
+void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance);
+
+// Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
+void adjoint_release(sw2d_handle* h);
+// Called when the physical parameters or the state change under a recorded trajectory.
+void adjoint_invalidate(sw2d_handle* h);
+
+}  // namespace sw2d

@@ -45,85 +45,12 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sw2d_b200.h"
-#include "sp_math.cuh"
+#include "sw2d_internal.cuh"
 
 using namespace sw2d;
 
 namespace {
 
-constexpr int kBlock = 256;
-
-// Device-resident loop control.  t and t_max decide whether a step runs; `go` and `dt` are
-// written by the CFL kernel's last block and read by the update kernel.
-struct Ctrl {
-    double t;
-    double dt;
-    double t_max;
-    long long steps;
-    unsigned int status;
-    unsigned int blocks_done;
-    int go;
-    int pad;
-};
-
-struct DevMesh {
-    int nc, ni, nb;
-    // cells
-    double4* st;             // {h, q, r, z}
-    const double4* cst;      // {z_b, boussinesq, phi, area}
-    const double2* cxy;      // centroid
-    double2* slope;          // MUSCL slopes
-    const double4* fric;     // {k1, k2, cos a, sin a} (friction)
-    const double4* hla;      // {h_sing, k1, k2, -} (singular head loss)
-    const double2* hlb;      // {cos a, sin a}
-    const double* zbv;       // z_b
-    const double* area;
-    const int2* coff;        // [nc+1] {first internal-neighbour entry, first balance slot}
-    const int2* cint;        // {edge*2 + side, neighbour} (MUSCL slopes)
-    double4* slot;           // balance slots {a, b, c, -}
-    double* slot_w;          // CFL contribution of the slot
-    // internal edges
-    const int2* lr;
-    const int2* eslot;       // {slot of (L, e), slot of (R, e)}
-    const double2* nxy;
-    const double2* mxy;
-    const double* len;
-    const double2* coef;     // {coefL, coefR}
-    double2* flux;           // optional copy: 3 x double2 per edge {F1,F2},{F3,S2L},{S2R,-} (tests)
-    double* lmax;            // optional copy of lambda_max (tests)
-    // boundary edges
-    const int* bcell;
-    const int* bbc;
-    const int* bslot;
-    const double4* bgeo;     // {nx, ny, length, coef}
-    double4* bflux;          // optional copy {F1, F2, F3, -} (tests)
-    double* lmaxb;           // optional copy of lambda_max (tests)
-    // boundary series
-    const int* bctype;
-    const long long* bcoff;
-    const double *bctimes, *bcvals;
-    // parameters
-    double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
-    DryConsts dry;
-    int neg_detect;
-    // dt reduction scratch
-    double* part;
-    Ctrl* ctrl;
-};
-
-// read-only loads through the non-coherent path (data not written by the same kernel)
-template <class T>
-__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
-
-__device__ __forceinline__ double4 ld(const double4* p)
-{
-    const double2* q = reinterpret_cast<const double2*>(p);
-    const double2 a = __ldg(q), b = __ldg(q + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
-}
-
-__device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_max; }
 
 // ------------------------------------------------------------------------------------------
 // k_slopes: swSp::computeMusclSlopes (swSpHypMusclEvr.cpp:11-115) per cell.  Step 1 sums the
@@ -393,7 +320,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
 // ------------------------------------------------------------------------------------------
 // k_update: balance + sources for one cell, then t += dt (thread 0).
 // ------------------------------------------------------------------------------------------
-template <int kFriction, bool kHeadLoss>
+template <int kFriction, bool kHeadLoss, bool kStoreB>
 __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
 {
     Ctrl* ctrl = m.ctrl;
@@ -430,6 +357,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
             rr += v.z * dt;
         }
     }
+    if (kStoreB) m.bal[c] = make_double4(hh, qq, rr, 0.0);  // for the reverse sweep
     if (fabs(hh) < kSmallReal) hh = 0.;
     if (fabs(qq) < kSmallReal) qq = 0.;
     if (fabs(rr) < kSmallReal) rr = 0.;
@@ -560,7 +488,6 @@ __global__ void k_eval_math(int fn, const double* __restrict__ x, double* y, lon
     y[i] = fn == 0 ? sw2d_exp(v) : fn == 1 ? sw2d_log(v) : fn == 2 ? exp(v) : log(v);
 }
 
-inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 // Hilbert index of (x, y) on a 2^16 x 2^16 grid (the classic rotate-and-flip walk).
 uint64_t hilbert_d(uint32_t x, uint32_t y)
@@ -583,73 +510,20 @@ uint64_t hilbert_d(uint32_t x, uint32_t y)
 
 }  // namespace
 
-// ------------------------------------------------------------------------------------------
-// handle
-// ------------------------------------------------------------------------------------------
-struct sw2d_handle {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int64_t nc = 0, ni = 0, nb = 0;
-    sw2d_params p{};
-    std::vector<int> cell_perm, int_perm, bnd_perm;  // [new] = caller index
-    std::vector<void*> allocs;
-    DevMesh m{};
-    Ctrl* ctrl = nullptr;
-    Ctrl* ctrl_host = nullptr;  // pinned
-    int* d_cell_perm = nullptr;
-    int* d_int_perm = nullptr;
-    int* d_bnd_perm = nullptr;
-    double* stage = nullptr;    // 3 * nc doubles
-    double* lmax_buf = nullptr;   // allocated by the option record_wave_speeds
-    double* lmaxb_buf = nullptr;
-    double2* flux_buf = nullptr;  // allocated by the option record_fluxes
-    double4* bflux_buf = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0;
-    int edge_variant = 0;   // index into kVariants (sw2d_autotune)
-    int slope_variant = 2;
-    std::string err;
-};
 
 namespace {
 
 std::string g_create_error;
+
+}  // namespace
+
+namespace sw2d {
 
 int fail(sw2d_handle* h, int code, const std::string& msg)
 {
     if (h) h->err = msg;
     else g_create_error = msg;
     return code;
-}
-
-#define CK(call)                                                                                  \
-    do {                                                                                          \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            return fail(h, SW2D_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-    } while (0)
-
-template <class T>
-int dev_upload(sw2d_handle* h, const std::vector<T>& v, T** out)
-{
-    size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
-    void* p = nullptr;
-    CK(cudaMalloc(&p, bytes));
-    h->allocs.push_back(p);
-    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
-    *out = static_cast<T*>(p);
-    return SW2D_OK;
-}
-
-template <class T>
-int dev_alloc(sw2d_handle* h, size_t n, T** out)
-{
-    void* p = nullptr;
-    CK(cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)));
-    h->allocs.push_back(p);
-    CK(cudaMemsetAsync(p, 0, std::max<size_t>(1, n) * sizeof(T), h->stream));
-    *out = static_cast<T*>(p);
-    return SW2D_OK;
 }
 
 int status_to_code(sw2d_handle* h, unsigned st)
@@ -659,8 +533,14 @@ int status_to_code(sw2d_handle* h, unsigned st)
     if (st & kStatusNegDepth) return fail(h, SW2D_E_NEG_DEPTH, "SP - negative water depth");
     if (st & kStatusBcType) return fail(h, SW2D_E_BC_TYPE, "boundary condition type not handled");
     if (st & kStatusBcFr) return fail(h, SW2D_E_BC_FR, "incorrect value for 'fr'-type boundary condition");
+    if (st & kStatusUnsupported)
+        return fail(h, SW2D_E_UNSUPPORTED, "cell with more neighbours than the adjoint's slope reverse handles");
     return SW2D_OK;
 }
+
+}  // namespace sw2d
+
+namespace {
 
 // Launch variants {threads per block, minimum resident blocks per SM (register cap)} of the
 // two heaviest kernels; sw2d_autotune times them on the live state and keeps the fastest.
@@ -671,72 +551,77 @@ constexpr Variant kVariants[] = {{256, 3}, {256, 2}, {256, 4}, {128, 4}, {128, 8
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 template <int kScheme, bool kBlending, int V>
-void launch_edges_v(sw2d_handle* h, unsigned n)
+void launch_edges_v(sw2d_handle* h, const DevMesh& m, unsigned n)
 {
     constexpr int B = kVariants[V].block, M = kVariants[V].minb;
-    k_edges<kScheme, kBlending, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(h->m);
+    k_edges<kScheme, kBlending, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(m);
 }
 
 template <int kScheme, bool kBlending>
-void launch_edges_s(sw2d_handle* h, unsigned n, int v)
+void launch_edges_s(sw2d_handle* h, const DevMesh& m, unsigned n, int v)
 {
     switch (v) {
-        case 1: launch_edges_v<kScheme, kBlending, 1>(h, n); break;
-        case 2: launch_edges_v<kScheme, kBlending, 2>(h, n); break;
-        case 3: launch_edges_v<kScheme, kBlending, 3>(h, n); break;
-        case 4: launch_edges_v<kScheme, kBlending, 4>(h, n); break;
-        case 5: launch_edges_v<kScheme, kBlending, 5>(h, n); break;
-        default: launch_edges_v<kScheme, kBlending, 0>(h, n); break;
+        case 1: launch_edges_v<kScheme, kBlending, 1>(h, m, n); break;
+        case 2: launch_edges_v<kScheme, kBlending, 2>(h, m, n); break;
+        case 3: launch_edges_v<kScheme, kBlending, 3>(h, m, n); break;
+        case 4: launch_edges_v<kScheme, kBlending, 4>(h, m, n); break;
+        case 5: launch_edges_v<kScheme, kBlending, 5>(h, m, n); break;
+        default: launch_edges_v<kScheme, kBlending, 0>(h, m, n); break;
     }
 }
 
-void launch_edges(sw2d_handle* h, int v)
+void launch_edges(sw2d_handle* h, const DevMesh& m, int v)
 {
-    const unsigned n = (unsigned)(h->m.ni + h->m.nb);
+    const unsigned n = (unsigned)(m.ni + m.nb);
     const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
     if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
-        if (bl) launch_edges_s<SW2D_SCHEME_GODUNOV, true>(h, n, v);
-        else launch_edges_s<SW2D_SCHEME_GODUNOV, false>(h, n, v);
+        if (bl) launch_edges_s<SW2D_SCHEME_GODUNOV, true>(h, m, n, v);
+        else launch_edges_s<SW2D_SCHEME_GODUNOV, false>(h, m, n, v);
     } else {
-        if (bl) launch_edges_s<SW2D_SCHEME_MUSCL_EVR, true>(h, n, v);
-        else launch_edges_s<SW2D_SCHEME_MUSCL_EVR, false>(h, n, v);
+        if (bl) launch_edges_s<SW2D_SCHEME_MUSCL_EVR, true>(h, m, n, v);
+        else launch_edges_s<SW2D_SCHEME_MUSCL_EVR, false>(h, m, n, v);
     }
 }
+
+void launch_edges(sw2d_handle* h, int v) { launch_edges(h, h->m, v); }
 
 template <int V>
-void launch_slopes_v(sw2d_handle* h)
+void launch_slopes_v(sw2d_handle* h, const DevMesh& m)
 {
     constexpr int B = kVariants[V].block, M = kVariants[V].minb;
-    k_slopes<B, M><<<((unsigned)h->m.nc + B - 1) / B, B, 0, h->stream>>>(h->m);
+    k_slopes<B, M><<<((unsigned)m.nc + B - 1) / B, B, 0, h->stream>>>(m);
 }
 
-void launch_slopes(sw2d_handle* h, int v)
+void launch_slopes(sw2d_handle* h, const DevMesh& m, int v)
 {
     switch (v) {
-        case 1: launch_slopes_v<1>(h); break;
-        case 2: launch_slopes_v<2>(h); break;
-        case 3: launch_slopes_v<3>(h); break;
-        case 4: launch_slopes_v<4>(h); break;
-        case 5: launch_slopes_v<5>(h); break;
-        default: launch_slopes_v<0>(h); break;
+        case 1: launch_slopes_v<1>(h, m); break;
+        case 2: launch_slopes_v<2>(h, m); break;
+        case 3: launch_slopes_v<3>(h, m); break;
+        case 4: launch_slopes_v<4>(h, m); break;
+        case 5: launch_slopes_v<5>(h, m); break;
+        default: launch_slopes_v<0>(h, m); break;
     }
 }
 
-template <int kF>
-void launch_update_f(sw2d_handle* h, unsigned g)
+void launch_slopes(sw2d_handle* h, int v) { launch_slopes(h, h->m, v); }
+
+template <int kF, bool kStoreB>
+void launch_update_f(sw2d_handle* h, const DevMesh& m, unsigned g)
 {
-    if (h->p.singular_head_loss) k_update<kF, true><<<g, kBlock, 0, h->stream>>>(h->m);
-    else k_update<kF, false><<<g, kBlock, 0, h->stream>>>(h->m);
+    if (h->p.singular_head_loss) k_update<kF, true, kStoreB><<<g, kBlock, 0, h->stream>>>(m);
+    else k_update<kF, false, kStoreB><<<g, kBlock, 0, h->stream>>>(m);
 }
 
-void launch_update(sw2d_handle* h)
+template <bool kStoreB>
+void launch_update_s(sw2d_handle* h, const DevMesh& m)
 {
-    const unsigned g = grid_for(h->m.nc);
+    const unsigned g = grid_for(m.nc);
     switch (h->p.friction) {
-        case SW2D_FRICTION_CHEZY: launch_update_f<SW2D_FRICTION_CHEZY>(h, g); break;
-        case SW2D_FRICTION_MANNING: launch_update_f<SW2D_FRICTION_MANNING>(h, g); break;
-        case SW2D_FRICTION_STRICKLER: launch_update_f<SW2D_FRICTION_STRICKLER>(h, g); break;
-        default: launch_update_f<SW2D_FRICTION_NONE>(h, g); break;
+        case SW2D_FRICTION_CHEZY: launch_update_f<SW2D_FRICTION_CHEZY, kStoreB>(h, m, g); break;
+        case SW2D_FRICTION_MANNING: launch_update_f<SW2D_FRICTION_MANNING, kStoreB>(h, m, g); break;
+        case SW2D_FRICTION_STRICKLER: launch_update_f<SW2D_FRICTION_STRICKLER, kStoreB>(h, m, g); break;
+        default: launch_update_f<SW2D_FRICTION_NONE, kStoreB>(h, m, g); break;
     }
 }
 
@@ -750,7 +635,7 @@ void launch_phase(sw2d_handle* h, int i)
             break;
         case 1: launch_edges(h, h->edge_variant); break;
         case 2: k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); break;
-        default: launch_update(h); break;
+        default: launch_update_s<false>(h, m); break;
     }
 }
 
@@ -758,6 +643,29 @@ void launch_step(sw2d_handle* h)
 {
     for (int i = 0; i < 4; i++) launch_phase(h, i);
 }
+
+}  // namespace
+
+namespace sw2d {
+
+void launch_slopes_on(sw2d_handle* h, const DevMesh& m)
+{
+    if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) launch_slopes(h, m, h->slope_variant);
+}
+
+void launch_edges_on(sw2d_handle* h, const DevMesh& m) { launch_edges(h, m, h->edge_variant); }
+
+void launch_cfl_on(sw2d_handle* h, const DevMesh& m) { k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
+
+void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance)
+{
+    if (store_balance) launch_update_s<true>(h, m);
+    else launch_update_s<false>(h, m);
+}
+
+}  // namespace sw2d
+
+namespace {
 
 int ensure_graph(sw2d_handle* h, int steps)
 {
@@ -1537,6 +1445,7 @@ int sw2d_destroy(sw2d_handle* h)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    adjoint_release(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -135,6 +135,103 @@ class SpModel:
     def kernels_per_step(self) -> int:
         return int(self.lib.sw2d_kernels_per_step(self.handle))
 
+    # ---- adjoint: J and its gradient along a recorded trajectory (frozen dt) -------------------
+    # The reference's assimilation front-end (swSpE, assim/swSpE.h) records a dry run, then
+    # replays it with the control for J (replay_trajectory_cost) and differentiates the replay
+    # (get_spatial_gradient_checkpointed).  These methods are the same steps over the C ABI.
+
+    GRADIENTS = ("h0", "q0", "r0", "z_b", "friction_1", "friction_2")
+
+    def record(self, n_steps: int, checkpoint_every: int = 100) -> int:
+        """Runs n_steps CFL-driven steps from the current state and records them as the
+        trajectory (dt sequence, checkpoints every `checkpoint_every` steps).  Returns the number
+        of steps recorded (fewer when t_max is reached)."""
+        done = ctypes.c_int64(0)
+        self._check(self.lib.sw2d_record(self.handle, int(n_steps), int(checkpoint_every), ctypes.byref(done)))
+        return int(done.value)
+
+    def trajectory_info(self) -> dict:
+        n, k = ctypes.c_int64(), ctypes.c_int64()
+        t0, t1 = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.sw2d_trajectory_info(self.handle, ctypes.byref(n), ctypes.byref(k), ctypes.byref(t0),
+                                                  ctypes.byref(t1)))
+        return {"n_steps": n.value, "checkpoint_every": k.value, "t_start": t0.value, "t_end": t1.value}
+
+    def trajectory_dt(self) -> np.ndarray:
+        n = self.trajectory_info()["n_steps"]
+        dt = np.empty(n)
+        self._check(self.lib.sw2d_get_trajectory_dt(self.handle, dt.ctypes.data_as(capi.c_double_p), n))
+        return dt
+
+    def set_trajectory_start(self, h, q, r) -> None:
+        h, q, r = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, q, r))
+        self._check(self.lib.sw2d_set_trajectory_start(self.handle, h.ctypes.data, q.ctypes.data, r.ctypes.data))
+
+    def set_param(self, name: str, values) -> None:
+        """Per-cell parameter: "friction_1", "friction_2", "friction" (both) or "z_b"."""
+        v = np.ascontiguousarray(np.broadcast_to(np.asarray(values, dtype=np.float64), (self.n,)))
+        self._check(self.lib.sw2d_set_param(self.handle, name.encode(), v.ctypes.data))
+
+    def get_param(self, name: str) -> np.ndarray:
+        v = np.empty(self.n)
+        self._check(self.lib.sw2d_get_param(self.handle, name.encode(), v.ctypes.data))
+        return v
+
+    def set_observations(self, cells, steps, h_obs, w_h=None, q_obs=None, r_obs=None, w_q=None,
+                         normalize: bool = False) -> None:
+        """Observation set of J: `cells` (distinct cell indices), `steps` (increasing step
+        indices after the trajectory's start), h_obs[k, p] (and q_obs, r_obs with weights w_q)."""
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        steps = np.ascontiguousarray(steps, dtype=np.int64)
+        npts, nt = cells.size, steps.size
+        h_obs = np.ascontiguousarray(np.asarray(h_obs, dtype=np.float64).reshape(nt, npts))
+        w_h = np.ascontiguousarray(np.broadcast_to(np.asarray(1.0 if w_h is None else w_h, dtype=np.float64), (npts,)))
+        o = capi.Sw2dObs()
+        o.n_points, o.cells, o.w_h = npts, cells.ctypes.data_as(capi.c_int64_p), w_h.ctypes.data_as(capi.c_double_p)
+        o.n_times, o.steps = nt, steps.ctypes.data_as(capi.c_int64_p)
+        o.h_obs = h_obs.ctypes.data_as(capi.c_double_p)
+        keep = [cells, steps, h_obs, w_h]
+        if w_q is not None:
+            w_q = np.ascontiguousarray(np.broadcast_to(np.asarray(w_q, dtype=np.float64), (npts,)))
+            q_obs = np.ascontiguousarray(np.asarray(q_obs, dtype=np.float64).reshape(nt, npts))
+            r_obs = np.ascontiguousarray(np.asarray(r_obs, dtype=np.float64).reshape(nt, npts))
+            o.w_q, o.q_obs, o.r_obs = (a.ctypes.data_as(capi.c_double_p) for a in (w_q, q_obs, r_obs))
+            keep += [w_q, q_obs, r_obs]
+        o.normalize = 1 if normalize else 0
+        self._check(self.lib.sw2d_set_observations(self.handle, ctypes.byref(o)))
+        del keep
+
+    def replay_cost(self) -> float:
+        J = ctypes.c_double()
+        self._check(self.lib.sw2d_replay_cost(self.handle, ctypes.byref(J)))
+        return J.value
+
+    def replay_sample(self, cells, steps, discharge: bool = False):
+        """h[k, p] (and q, r) at the given cells after each given step of the replayed trajectory."""
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        steps = np.ascontiguousarray(steps, dtype=np.int64)
+        h = np.empty((steps.size, cells.size))
+        q = np.empty_like(h) if discharge else None
+        r = np.empty_like(h) if discharge else None
+        self._check(self.lib.sw2d_replay_sample(self.handle, cells.size, cells.ctypes.data_as(capi.c_int64_p),
+                                                steps.size, steps.ctypes.data_as(capi.c_int64_p), h.ctypes.data,
+                                                q.ctypes.data if discharge else None,
+                                                r.ctypes.data if discharge else None))
+        return (h, q, r) if discharge else h
+
+    def adjoint(self, wrt=GRADIENTS):
+        """(J, {name: dJ/dname}) for the names in `wrt` (a subset of GRADIENTS)."""
+        g = capi.Sw2dGradient()
+        out = {}
+        for name in wrt:
+            if name not in self.GRADIENTS:
+                raise ValueError(f"unknown gradient {name!r}")
+            out[name] = np.empty(self.n)
+            setattr(g, name, out[name].ctypes.data_as(capi.c_double_p))
+        J = ctypes.c_double()
+        self._check(self.lib.sw2d_adjoint(self.handle, ctypes.byref(J), ctypes.byref(g)))
+        return J.value, out
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self.lib.sw2d_destroy(self.handle)
