@@ -178,7 +178,13 @@ const char* sw2d_phase_name(int i);
 
 /* Run-time options.  "record_wave_speeds" (0/1): also keep lambda_max per edge for
  * sw2d_get_array("lambda_max_int"/"lambda_max_bnd") (the reference's lambda_max_int/_bnd
- * members, swSp.h:201-203); off by default since the step itself only needs lambda_max * length. */
+ * members, swSp.h:201-203); off by default since the step itself only needs lambda_max * length.
+ * "record_fluxes" (0/1): keep F1, F2, F3, s2L, s2R per edge for sw2d_get_array.
+ * "adjoint_flush_branch" (0/1): how sw2d_adjoint differentiates the round-off flush
+ * |x| < 1e-16 -> 0 after the balance (swSpHyp.cpp:197-199, assim/swSpE_hyp.cpp:390-392).  0 (the
+ * default): as the identity, which is what finite differences see (a state at rest sits exactly
+ * on the flush).  1: as the branch taken (zero derivative for flushed values), which is what
+ * differentiating the reference's code line by line gives. */
 int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value);
 
 /* Launch-configuration autotuner (no counterpart in the reference): times every

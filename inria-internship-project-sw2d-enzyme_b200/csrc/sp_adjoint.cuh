@@ -460,6 +460,8 @@ struct UpdateParams {
     int friction;        // 0 none, 1 chezy, 2 manning, 3 strickler
     bool head_loss;
     bool clamp_negative; // negative_depth_detection off: h < 0 -> (0, 0, 0)
+    bool flush_branch;   // round-off flush |x| < 1e-16 -> 0: zero derivative (the branch taken)
+                         // instead of the identity
     double h_min, v_max, fr_max, dt;
     double k1, k2, fcos, fsin;           // friction
     double hs, hk1, hk2, hcos, hsin;     // head loss
@@ -653,9 +655,14 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
     (void)q_f;
     (void)r_f;
     if (neg) { h_bar = 0.; q_bar = 0.; r_bar = 0.; }
-    if (fh) h_bar = 0.;
-    if (fq) q_bar = 0.;
-    if (fr_) r_bar = 0.;
+    // The flush moves a value by less than 1e-16.  Differentiating the branch taken gives 0 (what
+    // line-by-line AD of the reference's balance gives); a state at rest sits exactly there, so
+    // by default the flush is differentiated as the identity, which central differences see.
+    if (p.flush_branch) {
+        if (fh) h_bar = 0.;
+        if (fq) q_bar = 0.;
+        if (fr_) r_bar = 0.;
+    }
     hb = h_bar;
     qb = q_bar;
     rb = r_bar;

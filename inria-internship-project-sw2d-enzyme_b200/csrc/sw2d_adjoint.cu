@@ -230,7 +230,8 @@ __global__ void k_obs_rev(ObsView o, const double4* st, double4* lam)
 // dt * (adjoint of the post-balance state); friction-coefficient gradients accumulate.
 template <int kFriction, bool kHeadLoss>
 __global__ void __launch_bounds__(kBlock) k_update_rev(DevMesh m, const double4* __restrict__ bal, double4* lam,
-                                                       double4* sig, double* gk1, double* gk2, double dt)
+                                                       double4* sig, double* gk1, double* gk2, double dt,
+                                                       int flush_branch)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
@@ -238,6 +239,7 @@ __global__ void __launch_bounds__(kBlock) k_update_rev(DevMesh m, const double4*
     p.friction = kFriction;
     p.head_loss = kHeadLoss;
     p.clamp_negative = !m.neg_detect;
+    p.flush_branch = flush_branch != 0;
     p.h_min = m.h_min;
     p.v_max = m.v_max;
     p.fr_max = m.fr_max;
@@ -626,9 +628,11 @@ void launch_update_rev_f(sw2d_handle* h, const double4* bal, double dt)
     AdjointState* a = h->adj;
     const unsigned g = grid_for(h->nc);
     if (h->p.singular_head_loss)
-        k_update_rev<kF, true><<<g, kBlock, 0, h->stream>>>(h->m, bal, a->lam, a->sig, a->g_k1, a->g_k2, dt);
+        k_update_rev<kF, true><<<g, kBlock, 0, h->stream>>>(h->m, bal, a->lam, a->sig, a->g_k1, a->g_k2, dt,
+                                                            h->adj_flush_branch);
     else
-        k_update_rev<kF, false><<<g, kBlock, 0, h->stream>>>(h->m, bal, a->lam, a->sig, a->g_k1, a->g_k2, dt);
+        k_update_rev<kF, false><<<g, kBlock, 0, h->stream>>>(h->m, bal, a->lam, a->sig, a->g_k1, a->g_k2, dt,
+                                                             h->adj_flush_branch);
 }
 
 void launch_update_rev(sw2d_handle* h, const double4* bal, double dt)

@@ -119,6 +119,7 @@ struct sw2d_handle {
     int edge_variant = 0;   // index into kVariants (sw2d_autotune)
     int slope_variant = 2;
     sw2d::AdjointState* adj = nullptr;  // recorded trajectory, checkpoints and adjoint buffers
+    int adj_flush_branch = 0;           // option "adjoint_flush_branch"
     std::string err;
 };
 

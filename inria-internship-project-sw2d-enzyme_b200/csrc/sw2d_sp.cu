@@ -1177,6 +1177,9 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         }
         h->m.flux = value ? h->flux_buf : nullptr;
         h->m.bflux = value ? h->bflux_buf : nullptr;
+    } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
+        h->adj_flush_branch = value ? 1 : 0;
+        return SW2D_OK;
     } else {
         return fail(h, SW2D_E_ARG, std::string("unknown option ") + name);
     }

@@ -216,6 +216,7 @@ int main()
                     p.friction = fric;
                     p.head_loss = hl;
                     p.clamp_negative = true;
+                    p.flush_branch = false;
                     p.h_min = 1e-5;
                     p.v_max = cap ? 0.5 : 100.0;
                     p.fr_max = cap ? ((it & 1) ? 0.3 : 100.0) : 100.0;

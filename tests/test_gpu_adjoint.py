@@ -10,6 +10,14 @@ clang/Enzyme), so these tests pin the GPU gradient by:
 * the Taylor ratio (J(m + e v) - J(m)) / (e g.v) -> 1;
 * invariants of the implementation: the replay reproduces the recorded CFL run bit for bit,
   and the gradient does not depend on the checkpoint interval (bitwise).
+
+J is only piecewise smooth.  Where the evaluation point itself sits on a switch, J has no
+gradient and central differences average two one-sided slopes; the finite-difference tests
+therefore start from states that do not: a free surface with small waves for MUSCL (a flat
+surface puts every limiter test on its switch), directions that keep dry cells dry, and bed
+directions that keep equal beds equal (the blending weight jumps there).  States at rest sit on
+the round-off flush after the balance, which the adjoint differentiates as the identity (the
+option adjoint_flush_branch selects the branch-taken derivative instead).
 """
 import zlib
 
@@ -50,18 +58,27 @@ CASES = {
 }
 
 
-def _case(pkg, spec, n_cells=3000):
+def _case(pkg, spec, n_cells=3000, wavy=False):
+    """The case of `spec`; with `wavy`, its initial free surface carries smooth waves of a few
+    centimetres: a flat surface at rest sits exactly on the MUSCL limiter's switches (every
+    reconstruction equals its neighbours' values), where J has no gradient, only one-sided
+    directional derivatives."""
     w = pkg.workloads
     if spec["kind"] == "dam":
-        return w.dam_break(n_cells=n_cells, scheme=spec["scheme"], friction="manning")
-    return w.channel_features(n_cells=n_cells, scheme=spec["scheme"], topo=spec["topo"], friction="manning",
-                              head_loss=True, t_max=40.0)
+        case = w.dam_break(n_cells=n_cells, scheme=spec["scheme"], friction="manning")
+    else:
+        case = w.channel_features(n_cells=n_cells, scheme=spec["scheme"], topo=spec["topo"], friction="manning",
+                                  head_loss=True, t_max=40.0)
+    if wavy:
+        wet = case.h0 > 0.0
+        case.h0 = np.where(wet, np.maximum(0.0, case.h0 + 0.03 * _smooth(case, 101)), 0.0)
+    return case
 
 
-def _twin(pkg, spec, every=16, n_gauges=24, obs_every=5, discharge=False, seed=3):
+def _twin(pkg, spec, every=16, n_gauges=24, obs_every=5, discharge=False, seed=3, wavy=False):
     """A model with a recorded trajectory and gauge observations from a twin replay whose
     friction is perturbed by a smooth +-20 % field."""
-    case = _case(pkg, spec)
+    case = _case(pkg, spec, wavy=wavy)
     model = pkg.SpModel(case)
     h0, q0, r0 = model.state()
     assert model.record(N_STEPS, every) == N_STEPS
@@ -126,62 +143,105 @@ def test_adjoint_cost_equals_replay_cost_and_is_deterministic(pkg):
         assert np.array_equal(ga[k].view(np.int64), gb[k].view(np.int64)), k
 
 
-def _fd_check(model, case, start, control, seed, eps, tol):
-    """Central difference of J along a smooth direction v of `control` against g . v."""
-    h0, q0, r0 = start
+# central-difference steps tried, largest first: J is only piecewise smooth (limiter switches,
+# wet/dry cut-offs, upwinding), so a large step may straddle a switch; a small one is limited by
+# the rounding of J.  The check passes when one of them agrees with the adjoint.
+EPS = (1e-5, 1e-6, 1e-7, 3e-8, 1e-8, 3e-9)
+
+
+def _direction(model, case, start, control, seed):
+    """A smooth perturbation of `control` that keeps dry cells dry and equal beds equal."""
     v = _smooth(case, seed)
-    J, g = model.adjoint()
     if control in ("friction_1", "friction_2"):
-        base = model.get_param(control)
-        v = v * base                       # relative perturbation
-        grad = g[control]
+        return v * model.get_param(control)          # relative perturbation
+    if control == "z_b" and case.opts.get("topo_discretization") == "blending":
+        # a function of z_b itself: neighbours with equal beds (cells whose nodes lie on a
+        # straight boundary of a planar bed) stay equal; the blending weight of the HLLC
+        # solver is 0 there and jumps for any bed difference (swSpHyp.cpp:824-998)
+        zb = model.get_param("z_b")
+        return np.sin(7.0 * zb + seed) + 0.5 * np.cos(3.0 * zb)
+    if control == "z_b":
+        return v
+    return v * (start[0] > 0.05)                     # initial state: wet cells only
 
-        def J_at(s):
-            model.set_param(control, base + s * v)
-            return model.replay_cost()
 
-        restore = lambda: model.set_param(control, base)  # noqa: E731
-    elif control == "z_b":
-        base = model.get_param("z_b")
-        grad = g["z_b"]
-
-        def J_at(s):
-            model.set_param("z_b", base + s * v)
-            return model.replay_cost()
-
-        restore = lambda: model.set_param("z_b", base)  # noqa: E731
-    else:  # initial state: perturb wet cells only, so that no dry cell becomes wet
+def _J_along(model, start, control, base, v, s):
+    if control in ("friction_1", "friction_2", "z_b"):
+        model.set_param(control, base + s * v)
+    else:
+        st = list(start)
         k = {"h0": 0, "q0": 1, "r0": 2}[control]
-        v = v * (h0 > 0.05)
-        grad = g[control]
+        st[k] = st[k] + s * v
+        model.set_trajectory_start(*st)
+    return model.replay_cost()
 
-        def J_at(s):
-            st = [h0, q0, r0]
-            st[k] = st[k] + s * v
-            model.set_trajectory_start(*st)
-            return model.replay_cost()
 
-        restore = lambda: model.set_trajectory_start(h0, q0, r0)  # noqa: E731
-    ad = float(np.dot(grad, v))
-    fd = (J_at(eps) - J_at(-eps)) / (2 * eps)
-    restore()
+def _restore(model, start, control, base):
+    if control in ("friction_1", "friction_2", "z_b"):
+        model.set_param(control, base)
+    else:
+        model.set_trajectory_start(*start)
+
+
+def _fd_check(model, case, start, control, seed, tol):
+    """Central differences of J along a smooth direction v of `control` against g . v;
+    returns the best relative error over the steps of EPS."""
+    v = _direction(model, case, start, control, seed)
+    J, g = model.adjoint()
+    base = model.get_param(control) if control in ("friction_1", "friction_2", "z_b") else None
+    ad = float(np.dot(g[control], v))
+    scale = max(abs(ad), 1e-300)
+    errs = []
+    for eps in EPS:
+        fd = (_J_along(model, start, control, base, v, eps) - _J_along(model, start, control, base, v, -eps)) / (2 * eps)
+        errs.append(abs(fd - ad) / scale)
+        if errs[-1] <= tol:
+            break
+    _restore(model, start, control, base)
     assert model.replay_cost() == J
-    scale = float(np.sum(np.abs(grad * v)))
-    assert abs(fd - ad) <= tol * max(abs(ad), scale, 1e-12), f"{control}: fd={fd:.10e} ad={ad:.10e}"
-    return fd, ad
+    assert min(errs) <= tol, f"{control}: ad={ad:.10e}, relative errors per step {dict(zip(EPS, errs))}"
+    return min(errs)
 
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("control", ["friction_1", "friction_2", "h0", "q0", "r0", "z_b"])
 def test_gradient_matches_central_differences(pkg, name, control):
-    model, case, start = _twin(pkg, CASES[name], discharge=(name == "dam_muscl"))
-    eps = 1e-6
-    _fd_check(model, case, start, control, seed=zlib.crc32(f"{name}/{control}".encode()) % 1000, eps=eps, tol=2e-5)
+    """From a free surface with small waves (no state sits on a limiter switch)."""
+    model, case, start = _twin(pkg, CASES[name], discharge=(name == "dam_muscl"), wavy=True)
+    # MUSCL: states within 1e-16 of the round-off flush flip under any perturbation, which puts
+    # a noise of order 1e-16 / eps on the differences; the channel's J is small (gauges far
+    # from the inflow), so its differences are the noisiest
+    tol = 1e-6 if CASES[name]["scheme"] == "godunov" else 5e-5
+    _fd_check(model, case, start, control, seed=zlib.crc32(f"{name}/{control}".encode()) % 1000, tol=tol)
+
+
+@pytest.mark.parametrize("control", ["friction_1", "h0", "q0", "r0", "z_b"])
+def test_gradient_at_rest_matches_central_differences(pkg, control):
+    """The dam break from rest (flat water on both sides, u = v = 0), first order: every cell
+    at rest sits on the round-off flush, which the adjoint differentiates as the identity."""
+    model, case, start = _twin(pkg, CASES["dam_godunov"])
+    _fd_check(model, case, start, control, seed=zlib.crc32(f"rest/{control}".encode()) % 1000, tol=1e-6)
+
+
+def test_flush_branch_option(pkg):
+    """adjoint_flush_branch = 1 differentiates the flush as the branch taken (zero derivative
+    for flushed values): from rest the discharge gradient then misses the first step's pressure
+    imbalance.  J is the same; both gradients are deterministic."""
+    model, _, _ = _twin(pkg, CASES["dam_godunov"])
+    J0, g0 = model.adjoint()
+    model.set_option("adjoint_flush_branch", 1)
+    J1, g1 = model.adjoint()
+    J2, g2 = model.adjoint()
+    model.set_option("adjoint_flush_branch", 0)
+    assert J0 == J1 == J2
+    assert np.array_equal(g1["q0"], g2["q0"])
+    assert not np.allclose(g0["q0"], g1["q0"])
+    assert all(np.isfinite(g1[k]).all() for k in g1)
 
 
 def test_taylor_ratio_tends_to_one(pkg):
     """The reference's Taylor protocol (assim/swSpE_checkpoint.cpp:1454-1663) on friction."""
-    model, case, _ = _twin(pkg, CASES["channel_muscl_blending"])
+    model, case, _ = _twin(pkg, CASES["channel_muscl_blending"], wavy=True)
     J, g = model.adjoint()
     base = model.get_param("friction_1")
     v = _smooth(case, 5) * base
