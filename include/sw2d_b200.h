@@ -261,6 +261,12 @@ typedef struct sw2d_gradient {
  * assim/swSpE_checkpoint.cpp:210-425). */
 int sw2d_record(sw2d_handle* h, int64_t n_steps, int64_t checkpoint_every, int64_t* steps_done);
 
+/* Records the trajectory again from its initial state with the current parameters (new CFL dt
+ * sequence, same requested length and checkpoint interval).  The reference re-runs its dry run
+ * at each gradient evaluation of the minimisation (swSpE_minimize.cpp:404-410); the
+ * observations stay attached to step indices. */
+int sw2d_rerecord(sw2d_handle* h, int64_t* steps_done);
+
 /* Recorded length, checkpoint interval, start time and end time of the trajectory. */
 int sw2d_trajectory_info(sw2d_handle* h, int64_t* n_steps, int64_t* checkpoint_every, double* t_start,
                          double* t_end);

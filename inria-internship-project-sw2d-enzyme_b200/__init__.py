@@ -7,9 +7,12 @@ Modules:
   capi       -- ctypes view of include/sw2d_b200.h and the CUDA library loader
   solver     -- SpModel, the host-side mirror of the reference's swSp interface
   tuning     -- launch-configuration autotuner with a JSON cache
+  assimilation -- friction assimilation over the GPU adjoint (the reference's swSpE_minimize)
+  autograd   -- torch.autograd bridge to the replayed cost and its adjoint (imported on demand)
 """
-from . import build, case, mesh, workloads, capi, solver, tuning  # noqa: F401
+from . import build, case, mesh, workloads, capi, solver, tuning, assimilation  # noqa: F401
 from .case import Case, read_case, write_case  # noqa: F401
 from .solver import SpModel, Sw2dError  # noqa: F401
 
-__all__ = ["case", "mesh", "workloads", "capi", "solver", "Case", "read_case", "write_case", "SpModel", "Sw2dError"]
+__all__ = ["case", "mesh", "workloads", "capi", "solver", "assimilation", "Case", "read_case", "write_case",
+           "SpModel", "Sw2dError"]

@@ -212,6 +212,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     # adjoint
     lib.sw2d_record.argtypes = [P, ctypes.c_int64, ctypes.c_int64, c_int64_p]
     lib.sw2d_record.restype = ctypes.c_int
+    lib.sw2d_rerecord.argtypes = [P, c_int64_p]
+    lib.sw2d_rerecord.restype = ctypes.c_int
     lib.sw2d_trajectory_info.argtypes = [P, c_int64_p, c_int64_p, c_double_p, c_double_p]
     lib.sw2d_trajectory_info.restype = ctypes.c_int
     lib.sw2d_get_trajectory_dt.argtypes = [P, c_double_p, ctypes.c_int64]
@@ -240,6 +242,6 @@ EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",
             "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_get_launch_config",
-            "sw2d_set_launch_config", "sw2d_get_array_noalloc", "sw2d_record", "sw2d_trajectory_info",
+            "sw2d_set_launch_config", "sw2d_get_array_noalloc", "sw2d_record", "sw2d_rerecord", "sw2d_trajectory_info",
             "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
             "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint"]

@@ -49,7 +49,7 @@ namespace sw2d {
 struct AdjointState {
     int64_t nslot = 0, ncint = 0;
     // trajectory
-    int64_t n_steps = 0, every = 0, n_ck = 0;
+    int64_t n_requested = 0, n_steps = 0, every = 0, n_ck = 0;
     long long base_steps = 0;
     double dt_before = 0.0;              // dt of the step before the trajectory (MUSCL-EVR uses it)
     std::vector<double> dt_seq, t_seq;   // dt_j and the time at the start of step j
@@ -142,6 +142,13 @@ __global__ void k_scatter_cells(const double* __restrict__ src, int stride, int 
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[perm[i]] = src[(size_t)i * stride + offset];
+}
+
+// out[p] = st[pts[p]]: the state at sampled cells
+__global__ void k_sample(const double4* __restrict__ st, const int* __restrict__ pts, double4* out, int n)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) out[p] = st[pts[p]];
 }
 
 // mirror[k] = the entry of the same internal edge in the neighbour's list
@@ -584,16 +591,15 @@ int obs_index(const AdjointState* a, int64_t step)
 }
 
 // Forward over the recorded trajectory from checkpoint 0 with the recorded dt (replay) or the
-// CFL dt (record), storing checkpoints and adding the observation cost.
-int run_trajectory(sw2d_handle* h, bool record, bool with_cost)
+// CFL dt (record), storing checkpoints; `at_step(j)` is called with the state after j steps
+// (j = 0 .. n_steps) in the model's state buffer.
+template <class F>
+int run_trajectory(sw2d_handle* h, bool record, F&& at_step)
 {
     AdjointState* a = h->adj;
     int rc = ck_load(h, 0);
     if (rc) return rc;
-    if (with_cost) {
-        const int k = obs_index(a, 0);
-        if (k >= 0) cost_at(h, k, h->m.st);
-    }
+    at_step(0);
     for (int64_t j = 0; j < a->n_steps; j++) {
         if (j % a->every == 0 && j > 0 && (rc = ck_save(h, j / a->every))) return rc;
         launch_slopes_on(h, h->m);
@@ -605,14 +611,23 @@ int run_trajectory(sw2d_handle* h, bool record, bool with_cost)
             k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
         }
         launch_update_on(h, h->m, false);
-        if (with_cost) {
-            const int k = obs_index(a, j + 1);
-            if (k >= 0) cost_at(h, k, h->m.st);
-        }
+        at_step(j + 1);
     }
     if ((rc = ck_save(h, a->n_ck))) return rc;
     CK(cudaGetLastError());
     return SW2D_OK;
+}
+
+int run_trajectory(sw2d_handle* h, bool record) { return run_trajectory(h, record, [](int64_t) {}); }
+
+// replay adding the cost of every observation step
+int replay_with_cost(sw2d_handle* h)
+{
+    AdjointState* a = h->adj;
+    return run_trajectory(h, false, [&](int64_t j) {
+        const int k = obs_index(a, j);
+        if (k >= 0) cost_at(h, k, h->m.st);
+    });
 }
 
 int read_status(sw2d_handle* h)
@@ -770,6 +785,7 @@ int alloc_trajectory(sw2d_handle* h, int64_t n_steps, int64_t every)
     AdjointState* a = h->adj;
     free_list(a->traj_allocs);
     a->ck_valid = false;
+    a->n_requested = 0;
     a->n_steps = n_steps;
     a->every = every;
     a->n_ck = (n_steps + every - 1) / every;
@@ -785,6 +801,47 @@ int alloc_trajectory(sw2d_handle* h, int64_t n_steps, int64_t every)
         a->n_steps = 0;
         return rc;
     }
+    a->n_requested = n_steps;
+    return SW2D_OK;
+}
+
+// The CFL-driven run from checkpoint 0 that fixes the trajectory's dt sequence (sw2d_record,
+// and sw2d_rerecord at new parameters); stops early at t_max.
+int record_from_start(sw2d_handle* h, int64_t* steps_done)
+{
+    AdjointState* a = h->adj;
+    const int64_t n_steps = a->n_requested, every = a->every;
+    a->n_steps = n_steps;
+    a->n_ck = (n_steps + every - 1) / every;
+    a->ck_valid = false;
+    int rc = run_trajectory(h, true);
+    if (rc) {
+        a->n_steps = 0;
+        return rc;
+    }
+    CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int64_t done = h->ctrl_host->steps - a->base_steps;
+    if (steps_done) *steps_done = done;
+    if ((rc = status_to_code(h, h->ctrl_host->status))) {
+        a->n_steps = 0;
+        return rc;
+    }
+    if (done <= 0) {
+        a->n_steps = 0;
+        return fail(h, SW2D_E_ARG, "no step recorded: the run is already at t_max");
+    }
+    if (done < n_steps) {  // t_max reached: the trajectory ends there
+        a->n_steps = done;
+        a->n_ck = (done + every - 1) / every;
+        if ((rc = ck_save(h, a->n_ck))) return rc;
+    }
+    a->dt_seq.resize(a->n_steps);
+    a->t_seq.resize(a->n_steps);
+    CK(cudaMemcpyAsync(a->dt_seq.data(), a->d_dt_seq, a->n_steps * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(a->t_seq.data(), a->d_t_seq, a->n_steps * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    a->ck_valid = true;
     return SW2D_OK;
 }
 
@@ -829,31 +886,16 @@ int sw2d_record(sw2d_handle* h, int64_t n_steps, int64_t checkpoint_every, int64
     a->base_steps = h->ctrl_host->steps;
     a->dt_before = h->ctrl_host->dt;
     if ((rc = ck_save(h, 0))) return rc;
-    if ((rc = run_trajectory(h, true, false))) return rc;
-    CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    const int64_t done = h->ctrl_host->steps - a->base_steps;
-    if (steps_done) *steps_done = done;
-    if ((rc = status_to_code(h, h->ctrl_host->status))) {
-        a->n_steps = 0;
-        return rc;
-    }
-    if (done <= 0) {
-        a->n_steps = 0;
-        return fail(h, SW2D_E_ARG, "no step recorded: the run is already at t_max");
-    }
-    if (done < n_steps) {  // t_max reached: the trajectory ends there
-        a->n_steps = done;
-        a->n_ck = (done + checkpoint_every - 1) / checkpoint_every;
-        if ((rc = ck_save(h, a->n_ck))) return rc;
-    }
-    a->dt_seq.resize(a->n_steps);
-    a->t_seq.resize(a->n_steps);
-    CK(cudaMemcpyAsync(a->dt_seq.data(), a->d_dt_seq, a->n_steps * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(a->t_seq.data(), a->d_t_seq, a->n_steps * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    a->ck_valid = true;
-    return SW2D_OK;
+    return record_from_start(h, steps_done);
+}
+
+int sw2d_rerecord(sw2d_handle* h, int64_t* steps_done)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    if (!h->adj || h->adj->n_requested <= 0)
+        return fail(h, SW2D_E_ARG, "no recorded trajectory (call sw2d_record first)");
+    CK(cudaSetDevice(h->device));
+    return record_from_start(h, steps_done);
 }
 
 int sw2d_trajectory_info(sw2d_handle* h, int64_t* n_steps, int64_t* checkpoint_every, double* t_start, double* t_end)
@@ -1022,7 +1064,7 @@ int sw2d_replay_cost(sw2d_handle* h, double* J)
     if (rc) return rc;
     CK(cudaSetDevice(h->device));
     if ((rc = check_observations(h))) return rc;
-    if ((rc = run_trajectory(h, false, true))) return rc;
+    if ((rc = replay_with_cost(h))) return rc;
     if ((rc = read_status(h))) return rc;
     h->adj->ck_valid = true;
     return total_cost(h, J);
@@ -1037,40 +1079,50 @@ int sw2d_replay_sample(sw2d_handle* h, int64_t n_points, const int64_t* cells, i
     if (rc) return rc;
     CK(cudaSetDevice(h->device));
     AdjointState* a = h->adj;
-    for (int64_t k = 0; k < n_times; k++)
+    std::vector<int> at(a->n_steps + 1, -1);
+    for (int64_t k = 0; k < n_times; k++) {
         if (steps[k] < 0 || steps[k] > a->n_steps) return fail(h, SW2D_E_ARG, "sample step outside the trajectory");
-    // replay once (fresh checkpoints for the current parameters), then recompute each requested
-    // step from the checkpoint before it
-    if ((rc = run_trajectory(h, false, false))) return rc;
+        if (k > 0 && steps[k] <= steps[k - 1]) return fail(h, SW2D_E_ARG, "sample steps must be increasing");
+        at[steps[k]] = (int)k;
+    }
+    std::vector<int> inv(h->nc), pts(n_points);
+    for (int64_t i = 0; i < h->nc; i++) inv[h->cell_perm[i]] = (int)i;
+    for (int64_t p = 0; p < n_points; p++) {
+        if (cells[p] < 0 || cells[p] >= h->nc) return fail(h, SW2D_E_ARG, "sampled cell out of range");
+        pts[p] = inv[cells[p]];
+    }
+    std::vector<void*> tmp;
+    int* d_pts = nullptr;
+    double4* d_out = nullptr;
+    auto release = [&] { free_list(tmp); };
+    if ((rc = adj_alloc(h, tmp, n_points, &d_pts)) || (rc = adj_alloc(h, tmp, n_points * n_times, &d_out))) {
+        release();
+        return rc;
+    }
+    if (cudaMemcpyAsync(d_pts, pts.data(), n_points * sizeof(int), cudaMemcpyHostToDevice, h->stream) != cudaSuccess) {
+        release();
+        return fail(h, SW2D_E_CUDA, "sample upload");
+    }
+    const unsigned g = grid_for(n_points);
+    rc = run_trajectory(h, false, [&](int64_t j) {
+        if (at[j] >= 0)
+            k_sample<<<g, kBlock, 0, h->stream>>>(h->m.st, d_pts, d_out + (size_t)at[j] * n_points, (int)n_points);
+    });
+    std::vector<double4> out(n_points * n_times);
+    if (!rc && cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double4), cudaMemcpyDeviceToHost, h->stream) !=
+                   cudaSuccess)
+        rc = fail(h, SW2D_E_CUDA, "sample read-back");
+    if (!rc && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = fail(h, SW2D_E_CUDA, "sample synchronise");
+    release();
+    if (rc) return rc;
     if ((rc = read_status(h))) return rc;
     a->ck_valid = true;
-    std::vector<double4> st(h->nc);
-    std::vector<int> inv(h->nc);
-    for (int64_t i = 0; i < h->nc; i++) inv[h->cell_perm[i]] = (int)i;
-    for (int64_t k = 0; k < n_times; k++) {
-        const int64_t j = steps[k];
-        const int64_t s = std::min(j / a->every, a->n_ck);
-        if ((rc = ck_load(h, s))) return rc;
-        for (int64_t i = s * a->every; i < j; i++) {
-            launch_slopes_on(h, h->m);
-            launch_edges_on(h, h->m);
-            k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
-            launch_update_on(h, h->m, false);
-        }
-        CK(cudaMemcpyAsync(st.data(), h->m.st, h->nc * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        for (int64_t p = 0; p < n_points; p++) {
-            const int64_t c = cells[p];
-            if (c < 0 || c >= h->nc) return fail(h, SW2D_E_ARG, "sampled cell out of range");
-            const double4 v = st[inv[c]];
-            h_out[k * n_points + p] = v.x;
-            if (q_out) q_out[k * n_points + p] = v.y;
-            if (r_out) r_out[k * n_points + p] = v.z;
-        }
+    for (size_t i = 0; i < out.size(); i++) {
+        h_out[i] = out[i].x;
+        if (q_out) q_out[i] = out[i].y;
+        if (r_out) r_out[i] = out[i].z;
     }
-    if ((rc = ck_load(h, a->n_ck))) return rc;
-    CK(cudaStreamSynchronize(h->stream));
-    return read_status(h);
+    return SW2D_OK;
 }
 
 int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad)
@@ -1082,7 +1134,7 @@ int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad)
     AdjointState* a = h->adj;
     if ((rc = check_observations(h))) return rc;
     if (!a->ck_valid) {
-        if ((rc = run_trajectory(h, false, false))) return rc;
+        if ((rc = run_trajectory(h, false))) return rc;
         if ((rc = read_status(h))) return rc;
         a->ck_valid = true;
     }

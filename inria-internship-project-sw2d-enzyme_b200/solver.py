@@ -150,6 +150,12 @@ class SpModel:
         self._check(self.lib.sw2d_record(self.handle, int(n_steps), int(checkpoint_every), ctypes.byref(done)))
         return int(done.value)
 
+    def rerecord(self) -> int:
+        """Records the trajectory again from its initial state with the current parameters."""
+        done = ctypes.c_int64(0)
+        self._check(self.lib.sw2d_rerecord(self.handle, ctypes.byref(done)))
+        return int(done.value)
+
     def trajectory_info(self) -> dict:
         n, k = ctypes.c_int64(), ctypes.c_int64()
         t0, t1 = ctypes.c_double(), ctypes.c_double()
