@@ -56,6 +56,8 @@ def _args():
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--adjoint-every", type=int, default=100, help="checkpoint interval of the adjoint")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="print only the adjoint measurement (one JSON line), e.g. for profiling")
     ap.add_argument("--launch-config", default=None,
                     help="'S,E': slope and edge kernel launch variants instead of autotuning (profiling runs)")
     return ap.parse_args()
@@ -273,6 +275,15 @@ def run_adjoint(pkg, args, local_rank):
     }
 
 
+def run_adjoint_only(args, local_rank):
+    import torch
+
+    pkg = importlib.import_module(PKG)
+    pkg.build.build()
+    torch.cuda.set_device(local_rank)
+    print(json.dumps(run_adjoint(pkg, args, local_rank)))
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
 
@@ -419,6 +430,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+    elif args.adjoint_only:
+        if rank == 0:
+            run_adjoint_only(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

@@ -676,50 +676,72 @@ struct SlopeNbr {
     bool c_is_r;                // the cell is the R side of the shared edge
 };
 
+// The slope functions loop over a compile-time capacity N (with n <= N used entries); for
+// N <= 4 the loops are unrolled so that a kernel instantiated for triangles (N = 3) keeps every
+// per-neighbour value in registers, larger capacities keep plain loops (local memory).
+#if defined(__CUDACC__)
+#define SW2D_UNROLL_KU _Pragma("unroll kU")
+#else
+#define SW2D_UNROLL_KU
+#endif
+
 // Forward with the intermediate slopes before each limiter test (for the reverse).
-SW2D_HD void slopes_fwd(double zc, int n, const SlopeNbr* nb, double& sx, double& sy, double* sxk, double* syk)
+template <int N>
+SW2D_HD void slopes_fwd_t(double zc, int n, const SlopeNbr* nb, double& sx, double& sy, double* sxk, double* syk)
 {
+    constexpr int kU = N <= 4 ? N : 1;
     sx = 0.0;
     sy = 0.0;
     double wsum = 0.0;
     if (n > 1) {
-        for (int k = 0; k < n; k++) {
-            const double dist = sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
-            const double w = 1.0 / dist;
-            sx += (nb[k].zj - zc) * nb[k].dx / dist / dist * w;
-            sy += (nb[k].zj - zc) * nb[k].dy / dist / dist * w;
-            wsum += w;
+        SW2D_UNROLL_KU
+        for (int k = 0; k < N; k++) {
+            if (k < n) {
+                const double dist = sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
+                const double w = 1.0 / dist;
+                sx += (nb[k].zj - zc) * nb[k].dx / dist / dist * w;
+                sy += (nb[k].zj - zc) * nb[k].dy / dist / dist * w;
+                wsum += w;
+            }
         }
         sx /= wsum;
         sy /= wsum;
     }
-    for (int k = 0; k < n; k++) {
-        sxk[k] = sx;
-        syk[k] = sy;
-        const double zL = nb[k].c_is_r ? nb[k].zj : zc;
-        const double zR = nb[k].c_is_r ? zc : nb[k].zj;
-        const double fmx = smax(zL, zR), fmn = smin(zL, zR);
-        const double rec = zc + nb[k].ax * sx + nb[k].ay * sy;
-        if (rec < fmn) {
-            const double fac = (fmn - zc) / (rec - zc);
-            sx *= fac;
-            sy *= fac;
-        }
-        if (rec > fmx) {
-            const double fac = (fmx - zc) / (rec - zc);
-            sx *= fac;
-            sy *= fac;
+    SW2D_UNROLL_KU
+    for (int k = 0; k < N; k++) {
+        if (k < n) {
+            sxk[k] = sx;
+            syk[k] = sy;
+            const double zL = nb[k].c_is_r ? nb[k].zj : zc;
+            const double zR = nb[k].c_is_r ? zc : nb[k].zj;
+            const double fmx = smax(zL, zR), fmn = smin(zL, zR);
+            const double rec = zc + nb[k].ax * sx + nb[k].ay * sy;
+            if (rec < fmn) {
+                const double fac = (fmn - zc) / (rec - zc);
+                sx *= fac;
+                sy *= fac;
+            }
+            if (rec > fmx) {
+                const double fac = (fmx - zc) / (rec - zc);
+                sx *= fac;
+                sy *= fac;
+            }
         }
     }
 }
 
-// (sxb, syb) = bars of the final slopes -> zc_bar and zj_bar[k]
-SW2D_HD void slopes_rev(double zc, int n, const SlopeNbr* nb, double sxb, double syb, double& zc_bar, double* zj_bar)
+// (sxb, syb) = bars of the final slopes -> zc_bar and zj_bar[k], k < n <= N
+template <int N>
+SW2D_HD void slopes_rev_t(double zc, int n, const SlopeNbr* nb, double sxb, double syb, double& zc_bar, double* zj_bar)
 {
-    double sx, sy, sxk[kMaxNbr], syk[kMaxNbr];
-    slopes_fwd(zc, n, nb, sx, sy, sxk, syk);
-    for (int k = 0; k < n; k++) zj_bar[k] = 0.0;
-    for (int k = n - 1; k >= 0; k--) {
+    constexpr int kU = N <= 4 ? N : 1;
+    double sx, sy, sxk[N], syk[N];
+    slopes_fwd_t<N>(zc, n, nb, sx, sy, sxk, syk);
+    SW2D_UNROLL_KU
+    for (int k = 0; k < N; k++) zj_bar[k] = 0.0;
+    SW2D_UNROLL_KU
+    for (int k = N - 1; k >= 0; k--) {
+        if (k >= n) continue;
         const double sx0 = sxk[k], sy0 = syk[k];
         const double zL = nb[k].c_is_r ? nb[k].zj : zc;
         const double zR = nb[k].c_is_r ? zc : nb[k].zj;
@@ -749,16 +771,31 @@ SW2D_HD void slopes_rev(double zc, int n, const SlopeNbr* nb, double sxb, double
     }
     if (n > 1) {
         double wsum = 0.0;
-        for (int k = 0; k < n; k++) wsum += 1.0 / sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
+        SW2D_UNROLL_KU
+        for (int k = 0; k < N; k++)
+            if (k < n) wsum += 1.0 / sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
         const double Sx_bar = sxb / wsum, Sy_bar = syb / wsum;
-        for (int k = 0; k < n; k++) {
-            const double dist = sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
-            const double w = 1.0 / dist;
-            const double t_bar = Sx_bar * (nb[k].dx / dist / dist * w) + Sy_bar * (nb[k].dy / dist / dist * w);
-            zj_bar[k] += t_bar;
-            zc_bar -= t_bar;
+        SW2D_UNROLL_KU
+        for (int k = 0; k < N; k++) {
+            if (k < n) {
+                const double dist = sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
+                const double w = 1.0 / dist;
+                const double t_bar = Sx_bar * (nb[k].dx / dist / dist * w) + Sy_bar * (nb[k].dy / dist / dist * w);
+                zj_bar[k] += t_bar;
+                zc_bar -= t_bar;
+            }
         }
     }
+}
+
+SW2D_HD void slopes_fwd(double zc, int n, const SlopeNbr* nb, double& sx, double& sy, double* sxk, double* syk)
+{
+    slopes_fwd_t<kMaxNbr>(zc, n, nb, sx, sy, sxk, syk);
+}
+
+SW2D_HD void slopes_rev(double zc, int n, const SlopeNbr* nb, double sxb, double syb, double& zc_bar, double* zj_bar)
+{
+    slopes_rev_t<kMaxNbr>(zc, n, nb, sxb, syb, zc_bar, zj_bar);
 }
 
 }  // namespace sw2d

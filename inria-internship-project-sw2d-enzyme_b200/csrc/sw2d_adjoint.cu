@@ -21,11 +21,15 @@
 //                                       cap; friction-coefficient gradient; slot adjoints
 //                                       sigma += dt * (adjoint of the post-balance state)
 //   k_slopes        per cell            forward slopes of the step (recomputed)
-//   k_edges_rev     per edge            reverse of the Riemann states and HLLC / boundary fluxes for
-//                                       the edges whose flux the step computed; per-slot
-//                                       contributions to the cells; those slots' adjoints reset
-//   k_cells_rev     per cell            ordered gather of the slot contributions; reverse of the
-//                                       cell's slope limiter (per-neighbour contributions)
+//   k_edges_rev     per edge            Riemann states recomputed, reverse of the HLLC flux (internal
+//                                       edges: adjoints of the two Riemann states per slot) or of the
+//                                       boundary flux and state (boundary edges: final contributions),
+//                                       for the edges whose flux the step computed; those slots'
+//                                       adjoints reset
+//   k_cells_rev     per cell            ordered gather over the cell's slots, with the reverse of the
+//                                       cell's reconstruction on each internal slot
+//   k_limiter_rev   per cell            reverse of the cell's slope limiter (per-neighbour
+//                                       contributions) (MUSCL-EVR)
 //   k_nbr_rev       per cell            ordered gather of the neighbours' slope contributions
 //
 // Edges left dry keep their previous balance terms in the forward step (swSpHyp.cpp:339), so a
@@ -69,6 +73,7 @@ struct AdjointState {
     double4* ctb = nullptr;              // nslot: per-slot contributions {h, q, r, z_b}
     double2* cts = nullptr;              // nslot: per-slot slope contributions {sx, sy}
     double* znb = nullptr;               // ncint: per-neighbour-entry z contributions
+    double2* sgb = nullptr;              // nc: adjoint of each cell's limited slope
     int* mirror = nullptr;               // ncint: entry of the same edge in the neighbour's list
     double* g_zb = nullptr;
     double* g_k1 = nullptr;
@@ -308,9 +313,9 @@ __device__ __forceinline__ void slot_rev(const SlotFactors& f, const double4& s,
     Sb += f.f2S2 * s.y + f.f3S2 * s.z;
 }
 
-template <int kScheme, bool kBlending>
-__global__ void __launch_bounds__(kBlock) k_edges_rev(DevMesh m, double4* sig, double4* ctb, double2* cts, double t,
-                                                      double dtp)
+template <int kScheme, bool kBlending, int kB, int kMinB>
+__global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig, double4* ctb, double2* cts, double t,
+                                                         double dtp)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m.ni) {
@@ -366,20 +371,12 @@ __global__ void __launch_bounds__(kBlock) k_edges_rev(DevMesh m, double4* sig, d
         SideBar Lb{0, 0, 0, 0, 0}, Rb{0, 0, 0, 0, 0};
         double zbLb = 0.0, zbRb = 0.0;
         hllc_rev(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min, fb, Lb, Rb, zbLb, zbRb);
-        CellBar A{0, 0, 0, 0, 0, 0, 0}, Bc{0, 0, 0, 0, 0, 0, 0};
-        if (kScheme == SW2D_SCHEME_GODUNOV) {
-            godunov_side_rev(sa.x, sa.y, sa.z, ca.y, nx, ny, Lb, A);
-            godunov_side_rev(sb.x, sb.y, sb.z, cb.y, nx, ny, Rb, Bc);
-        } else {
-            evr_side_rev(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, nx, ny, dtp, Lb, A);
-            evr_side_rev(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, nx, ny, dtp, Rb,
-                         Bc);
-        }
-        // z_c = h + z_b of the cell
-        ctb[sl.x] = make_double4(A.h + A.zc, A.q, A.r, A.zb + zbLb + A.zc);
-        ctb[sl.y] = make_double4(Bc.h + Bc.zc, Bc.q, Bc.r, Bc.zb + zbRb + Bc.zc);
-        cts[sl.x] = make_double2(A.sx, A.sy);
-        cts[sl.y] = make_double2(Bc.sx, Bc.sy);
+        // adjoints of the two Riemann states; k_cells_rev takes them back through the
+        // reconstruction of each side
+        ctb[sl.x] = make_double4(Lb.z, Lb.q, Lb.r, Lb.lm);
+        cts[sl.x] = make_double2(Lb.lp, zbLb);
+        ctb[sl.y] = make_double4(Rb.z, Rb.q, Rb.r, Rb.lm);
+        cts[sl.y] = make_double2(Rb.lp, zbRb);
     } else if (i < m.ni + m.nb) {
         const int e = i - m.ni;
         const int c = ld(&m.bcell[e]);
@@ -406,65 +403,124 @@ __global__ void __launch_bounds__(kBlock) k_edges_rev(DevMesh m, double4* sig, d
     }
 }
 
-// Ordered gather of the slot contributions of each cell, then (MUSCL-EVR) the reverse of its
-// slope limiter: the cell's own z contribution is applied here, the neighbours' go to znb.
-template <bool kMuscl>
+// Reverse of the slope limiter of cell c with up to N neighbours (entries e0 .. e0+cnt of
+// cint), N fixed so that the per-neighbour values stay in registers: the cell's own z
+// contribution is returned, the neighbours' go to znb.
+template <int N>
+__device__ __forceinline__ double slope_rev_cell(const DevMesh& m, int e0, int cnt, double zc, double2 xy, double sxb,
+                                                 double syb, double* znb)
+{
+    constexpr int kU = N <= 4 ? N : 1;
+    SlopeNbr nb[N];
+    SW2D_UNROLL_KU
+    for (int i = 0; i < N; i++) {
+        if (i < cnt) {
+            const int2 en = ld(&m.cint[e0 + i]);
+            const double2 xj = ld(&m.cxy[en.y]);
+            const double2 mp = ld(&m.mxy[en.x >> 1]);
+            nb[i].zj = m.st[en.y].w;
+            nb[i].dx = xj.x - xy.x;
+            nb[i].dy = xj.y - xy.y;
+            nb[i].ax = mp.x - xy.x;
+            nb[i].ay = mp.y - xy.y;
+            nb[i].c_is_r = (en.x & 1) != 0;
+        }
+    }
+    double zcb = 0.0, zjb[N];
+    slopes_rev_t<N>(zc, cnt, nb, sxb, syb, zcb, zjb);
+    SW2D_UNROLL_KU
+    for (int i = 0; i < N; i++)
+        if (i < cnt) znb[e0 + i] = zjb[i];
+    return zcb;
+}
+
+// Ordered gather, over the slots of each cell in the reference's order: boundary slots hold
+// their final contributions; internal slots hold the adjoints of this cell's Riemann state,
+// taken back here through the cell's reconstruction (godunov_side / evr_side).  For MUSCL-EVR
+// the adjoint of the cell's limited slope goes to sgb for k_limiter_rev.
+template <int kScheme>
 __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, const double4* __restrict__ ctb,
-                                                      const double2* __restrict__ cts, double* gzb, double* znb)
+                                                      const double2* __restrict__ cts, double* gzb, double2* sgb,
+                                                      double dtp)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
+    constexpr bool kMuscl = kScheme == SW2D_SCHEME_MUSCL_EVR;
     const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
+    const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
+    const int nbnd = (k1 - k0) - (e1 - e0);
     double hb = 0.0, qb = 0.0, rb = 0.0, zbb = 0.0, sxb = 0.0, syb = 0.0;
-    for (int k = k0; k < k1; k++) {
+    for (int k = k0; k < k0 + nbnd; k++) {
         const double4 v = ctb[k];
         hb += v.x;
         qb += v.y;
         rb += v.z;
         zbb += v.w;
-        if (kMuscl) {
-            const double2 w = cts[k];
-            sxb += w.x;
-            syb += w.y;
-        }
     }
+    const double4 s = m.st[c];
+    const double4 cs = ld(&m.cst[c]);
+    double2 xy = make_double2(0.0, 0.0), g = xy;
     if (kMuscl) {
-        const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
-        const int cnt = e1 - e0;
-        if (sxb != 0.0 || syb != 0.0) {
-            if (cnt > kMaxNbr) {
-                atomicOr(&m.ctrl->status, kStatusUnsupported);  // degree beyond the reverse's table
-            } else {
-                SlopeNbr nb[kMaxNbr];
-                const double zc = m.st[c].w;
-                const double2 xy = ld(&m.cxy[c]);
-                for (int i = 0; i < cnt; i++) {
-                    const int2 en = ld(&m.cint[e0 + i]);
-                    const double2 xj = ld(&m.cxy[en.y]);
-                    const double2 mp = ld(&m.mxy[en.x >> 1]);
-                    nb[i].zj = m.st[en.y].w;
-                    nb[i].dx = xj.x - xy.x;
-                    nb[i].dy = xj.y - xy.y;
-                    nb[i].ax = mp.x - xy.x;
-                    nb[i].ay = mp.y - xy.y;
-                    nb[i].c_is_r = (en.x & 1) != 0;
-                }
-                double zcb = 0.0, zjb[kMaxNbr];
-                slopes_rev(zc, cnt, nb, sxb, syb, zcb, zjb);
-                hb += zcb;
-                zbb += zcb;
-                for (int i = 0; i < cnt; i++) znb[e0 + i] = zjb[i];
-            }
-        } else {
-            for (int i = e0; i < e1; i++) znb[i] = 0.0;
-        }
+        xy = ld(&m.cxy[c]);
+        g = m.slope[c];
     }
+    for (int i = 0; i < e1 - e0; i++) {
+        const int k = k0 + nbnd + i;
+        const double4 a = ctb[k];
+        const double2 b = cts[k];
+        if (a.x == 0.0 && a.y == 0.0 && a.z == 0.0 && a.w == 0.0 && b.x == 0.0 && b.y == 0.0) continue;
+        const int2 en = ld(&m.cint[e0 + i]);
+        const int e = en.x >> 1;
+        const double2 n = ld(&m.nxy[e]);
+        const SideBar sb{a.x, a.y, a.z, a.w, b.x};
+        CellBar cb{0, 0, 0, 0, 0, 0, 0};
+        if (kMuscl) {
+            const double2 mp = ld(&m.mxy[e]);
+            evr_side_rev((en.x & 1) == 0, s.x, s.y, s.z, cs.x, cs.y, s.w, g.x, g.y, xy.x, xy.y, mp.x, mp.y, n.x, n.y,
+                         dtp, sb, cb);
+        } else {
+            godunov_side_rev(s.x, s.y, s.z, cs.y, n.x, n.y, sb, cb);
+        }
+        // z_c = h + z_b of the cell
+        hb += cb.h + cb.zc;
+        qb += cb.q;
+        rb += cb.r;
+        zbb += cb.zb + b.y + cb.zc;
+        sxb += cb.sx;
+        syb += cb.sy;
+    }
+    if (kMuscl) sgb[c] = make_double2(sxb, syb);
     double4 l = lam[c];
     l.x += hb;
     l.y += qb;
     l.z += rb;
     lam[c] = l;
     gzb[c] += zbb;
+}
+
+// Reverse of each cell's slope limiter (MUSCL-EVR): the cell's own z contribution is applied
+// here, the neighbours' go to znb (one value per internal-neighbour entry).
+__global__ void __launch_bounds__(kBlock) k_limiter_rev(DevMesh m, const double2* __restrict__ sgb, double4* lam,
+                                                        double* gzb, double* znb)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
+    const int cnt = e1 - e0;
+    const double2 b = sgb[c];
+    if (b.x == 0.0 && b.y == 0.0) {
+        for (int i = e0; i < e1; i++) znb[i] = 0.0;
+        return;
+    }
+    const double zc = m.st[c].w;
+    const double2 xy = ld(&m.cxy[c]);
+    double zcb = 0.0;
+    if (cnt <= 3) zcb = slope_rev_cell<3>(m, e0, cnt, zc, xy, b.x, b.y, znb);
+    else if (cnt == 4) zcb = slope_rev_cell<4>(m, e0, cnt, zc, xy, b.x, b.y, znb);
+    else if (cnt <= kMaxNbr) zcb = slope_rev_cell<kMaxNbr>(m, e0, cnt, zc, xy, b.x, b.y, znb);
+    else atomicOr(&m.ctrl->status, kStatusUnsupported);  // degree beyond the reverse's table
+    lam[c].x += zcb;
+    gzb[c] += zcb;
 }
 
 // z contributions of the neighbours' slope limiters, gathered in the cell's entry order
@@ -518,7 +574,7 @@ int adjoint_fixed(sw2d_handle* h)
     auto& L = a->fixed_allocs;
     if ((rc = adj_alloc(h, L, h->nc, &a->lam)) || (rc = adj_alloc(h, L, a->nslot, &a->sig)) ||
         (rc = adj_alloc(h, L, a->nslot, &a->ctb)) || (rc = adj_alloc(h, L, a->nslot, &a->cts)) ||
-        (rc = adj_alloc(h, L, a->ncint, &a->znb)) || (rc = adj_alloc(h, L, a->ncint, &a->mirror)) ||
+        (rc = adj_alloc(h, L, a->ncint, &a->znb)) || (rc = adj_alloc(h, L, h->nc, &a->sgb)) || (rc = adj_alloc(h, L, a->ncint, &a->mirror)) ||
         (rc = adj_alloc(h, L, h->nc, &a->g_zb)) || (rc = adj_alloc(h, L, h->nc, &a->g_k1)) ||
         (rc = adj_alloc(h, L, h->nc, &a->g_k2)) || (rc = adj_alloc(h, L, 1, &a->ctrl_rev)) ||
         (rc = adj_alloc(h, L, kCostBlocks, &a->d_part)) ||
@@ -660,17 +716,44 @@ void launch_update_rev(sw2d_handle* h, const double4* bal, double dt)
     }
 }
 
+// Launch variants {threads per block, minimum resident blocks per SM} of k_edges_rev (its
+// register cap); the option "adjoint_edge_variant" selects one.
+struct RevVariant {
+    int block, minb;
+};
+constexpr RevVariant kRevVariants[] = {{128, 3}, {256, 1}, {256, 2}, {128, 4}, {256, 3}};
+constexpr int kNumRevVariants = sizeof(kRevVariants) / sizeof(kRevVariants[0]);
+
+template <int kScheme, bool kBlending, int V>
+void launch_edges_rev_v(sw2d_handle* h, const DevMesh& m, double t, double dtp)
+{
+    constexpr int B = kRevVariants[V].block, M = kRevVariants[V].minb;
+    AdjointState* a = h->adj;
+    const unsigned n = (unsigned)(m.ni + m.nb);
+    k_edges_rev<kScheme, kBlending, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+}
+
+template <int kScheme, bool kBlending>
+void launch_edges_rev_s(sw2d_handle* h, const DevMesh& m, double t, double dtp)
+{
+    switch (h->adj_edge_variant) {
+        case 1: launch_edges_rev_v<kScheme, kBlending, 1>(h, m, t, dtp); break;
+        case 2: launch_edges_rev_v<kScheme, kBlending, 2>(h, m, t, dtp); break;
+        case 3: launch_edges_rev_v<kScheme, kBlending, 3>(h, m, t, dtp); break;
+        case 4: launch_edges_rev_v<kScheme, kBlending, 4>(h, m, t, dtp); break;
+        default: launch_edges_rev_v<kScheme, kBlending, 0>(h, m, t, dtp); break;
+    }
+}
+
 void launch_edges_rev(sw2d_handle* h, const DevMesh& m, double t, double dtp)
 {
-    AdjointState* a = h->adj;
-    const unsigned g = grid_for(m.ni + m.nb);
     const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
     if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
-        if (bl) k_edges_rev<SW2D_SCHEME_GODUNOV, true><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
-        else k_edges_rev<SW2D_SCHEME_GODUNOV, false><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+        if (bl) launch_edges_rev_s<SW2D_SCHEME_GODUNOV, true>(h, m, t, dtp);
+        else launch_edges_rev_s<SW2D_SCHEME_GODUNOV, false>(h, m, t, dtp);
     } else {
-        if (bl) k_edges_rev<SW2D_SCHEME_MUSCL_EVR, true><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
-        else k_edges_rev<SW2D_SCHEME_MUSCL_EVR, false><<<g, kBlock, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+        if (bl) launch_edges_rev_s<SW2D_SCHEME_MUSCL_EVR, true>(h, m, t, dtp);
+        else launch_edges_rev_s<SW2D_SCHEME_MUSCL_EVR, false>(h, m, t, dtp);
     }
 }
 
@@ -761,11 +844,15 @@ int reverse_sweep(sw2d_handle* h)
                 launch_slopes_on(h, ms);
             }
             launch_edges_rev(h, mr, a->t_seq[j], j > 0 ? a->dt_seq[j - 1] : a->dt_before);
+            const double dtp = j > 0 ? a->dt_seq[j - 1] : a->dt_before;
             if (muscl) {
-                k_cells_rev<true><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb, a->znb);
+                k_cells_rev<SW2D_SCHEME_MUSCL_EVR><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
+                                                                                  a->sgb, dtp);
+                k_limiter_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->sgb, a->lam, a->g_zb, a->znb);
                 k_nbr_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->mirror, a->znb, a->lam, a->g_zb);
             } else {
-                k_cells_rev<false><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb, a->znb);
+                k_cells_rev<SW2D_SCHEME_GODUNOV><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
+                                                                                a->sgb, dtp);
             }
         }
         CK(cudaGetLastError());

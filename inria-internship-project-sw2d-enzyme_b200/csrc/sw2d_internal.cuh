@@ -120,6 +120,7 @@ struct sw2d_handle {
     int slope_variant = 2;
     sw2d::AdjointState* adj = nullptr;  // recorded trajectory, checkpoints and adjoint buffers
     int adj_flush_branch = 0;           // option "adjoint_flush_branch"
+    int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     std::string err;
 };
 
