@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SW2D_ABI_VERSION 1
+#define SW2D_ABI_VERSION 2
 
 /* status codes */
 #define SW2D_OK 0
@@ -47,13 +47,16 @@ extern "C" {
 #define SW2D_E_BC_FR (-7)        /* 'fr' boundary value outside [0,1]: swSpHyp.cpp:57-62     */
 #define SW2D_E_UNSUPPORTED (-8)  /* option outside the implemented path                     */
 #define SW2D_E_NO_DEVICE (-9)    /* no usable CUDA device                                    */
+#define SW2D_E_PHIG (-10)        /* DIP connectivity porosity < 1e-16 in a specific force:
+                                    src/sw2dSolver/models/dip/swDip.cpp:1524-1528            */
 
 /* enumerations of the input.solv string keys (src/sw2dSolver/common/swSolverParam.h:130-153) */
 enum sw2d_scheme { SW2D_SCHEME_GODUNOV = 0, SW2D_SCHEME_MUSCL_EVR = 1 };
 enum sw2d_topo { SW2D_TOPO_DISCONTINUOUS = 0, SW2D_TOPO_BLENDING = 1 };
 enum sw2d_friction { SW2D_FRICTION_NONE = 0, SW2D_FRICTION_CHEZY = 1, SW2D_FRICTION_MANNING = 2,
                      SW2D_FRICTION_STRICKLER = 3 };
-enum sw2d_bc_type { SW2D_BC_Q = 0, SW2D_BC_H = 1, SW2D_BC_Z = 2, SW2D_BC_FR = 3 };
+enum sw2d_bc_type { SW2D_BC_Q = 0, SW2D_BC_H = 1, SW2D_BC_Z = 2, SW2D_BC_FR = 3,
+                    SW2D_BC_PHIWQ = 4 /* DIP only */ };
 enum sw2d_variant { SW2D_VARIANT_NATIVE = 0, SW2D_VARIANT_ENZYME_E = 1 };
 
 /* Mesh tables, as swParent::setMeshTables builds them (src/sw2dSolver/models/swParent.cpp:391-501).
@@ -134,6 +137,26 @@ typedef struct sw2d_handle sw2d_handle;
 int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
                 const sw2d_bc_table* bc, const double* h0, const double* q0, const double* r0,
                 int device, sw2d_handle** out);
+
+/* The dual integral porosity (DIP) model: fields beyond the SP ones.  fields->phi of
+ * sw2d_create_dip is the cell (storage) porosity phiW (DIP_cell_porosity_map.txt). */
+typedef struct sw2d_dip_fields {
+    const double* phi_g_int;       /* [edge_int_nb] connectivity porosity (DIP_edge_int_porosity_map.txt) */
+    const double* phi_g_bnd;       /* [edge_bnd_nb] (DIP_edge_bnd_porosity_map.txt)                     */
+    int32_t momentum_dissipation;  /* 0 none, 1 active (model_momentum_dissipation)                     */
+    const double* mu_1;            /* [cell_nb] dissipation coefficients and direction (degrees)        */
+    const double* mu_2;            /* (cell_momentum_dissipation_map.txt); NULL when inactive           */
+    const double* mu_alpha;
+} sw2d_dip_fields;
+
+/* Replaces swParent::create + swDip::init (swParent.cpp:125-173, dip/swDip.cpp:900-1030) for
+ * model_hyperb dip: the SP arguments plus the DIP fields, checked as
+ * swDip::checkParameterConsistency does (phiG in [0,1] and not above the adjacent cells' phiW).
+ * The step is swDip's (dip/swDipHyp.cpp): DIP wave speeds and specific force, DIP HLLC and
+ * boundary fluxes (boundary types q, h, z, fr, phiWq), momentum dissipation. */
+int sw2d_create_dip(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                    const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
+                    const double* r0, int device, sw2d_handle** out);
 
 /* Advances at most n_steps passes of the body of swSp::execute's time loop
  * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),

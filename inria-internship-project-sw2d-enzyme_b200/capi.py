@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes
 import os
 from dataclasses import dataclass
-from typing import List
+from typing import List, Optional
 
 import numpy as np
 
@@ -56,6 +56,11 @@ class Sw2dBcTable(ctypes.Structure):
                 ("values", c_double_p)]
 
 
+class Sw2dDipFields(ctypes.Structure):
+    _fields_ = [("phi_g_int", c_double_p), ("phi_g_bnd", c_double_p), ("momentum_dissipation", ctypes.c_int32),
+                ("mu_1", c_double_p), ("mu_2", c_double_p), ("mu_alpha", c_double_p)]
+
+
 class Sw2dObs(ctypes.Structure):
     _fields_ = [("n_points", ctypes.c_int64), ("cells", c_int64_p), ("w_h", c_double_p), ("w_q", c_double_p),
                 ("n_times", ctypes.c_int64), ("steps", c_int64_p), ("h_obs", c_double_p), ("q_obs", c_double_p),
@@ -81,6 +86,7 @@ class NativeInputs:
     q0: np.ndarray
     r0: np.ndarray
     keep: List[np.ndarray]
+    dip: Optional[Sw2dDipFields] = None
 
 
 def params_from_opts(opts) -> Sw2dParams:
@@ -138,7 +144,7 @@ def native_inputs(case: Case) -> NativeInputs:
                             d(hl[0]) if hl is not None else null, d(hl[1]) if hl is not None else null,
                             d(hl[2]) if hl is not None else null, d(hl[3]) if hl is not None else null)
     ns = len(series_codes)
-    types = np.array([BC_TYPES.get(t.lower(), 99) for t in case.bc.types], dtype=np.int32)
+    types = np.array([BC_TYPES.get(t, 99) for t in case.bc.types], dtype=np.int32)  # exact, as the reference
     nrec = case.bc.times.shape[0]
     offset = np.arange(ns + 1, dtype=np.int64) * nrec
     times = np.tile(np.asarray(case.bc.times, dtype=np.float64), ns)
@@ -148,7 +154,13 @@ def native_inputs(case: Case) -> NativeInputs:
     h0 = np.ascontiguousarray(case.h0, dtype=np.float64)
     q0 = np.ascontiguousarray(case.q0, dtype=np.float64)
     r0 = np.ascontiguousarray(case.r0, dtype=np.float64)
-    return NativeInputs(mesh, params, fields, bc, h0, q0, r0, keep)
+    dip = None
+    if case.is_dip:
+        mu = case.mu
+        diss = str(case.opts.get("model_momentum_dissipation", "none")).lower() == "active"
+        dip = Sw2dDipFields(d(case.phi_g_int), d(case.phi_g_bnd), 1 if diss else 0,
+                            d(mu[0]) if diss else null, d(mu[1]) if diss else null, d(mu[2]) if diss else null)
+    return NativeInputs(mesh, params, fields, bc, h0, q0, r0, keep, dip)
 
 
 _LIB = None
@@ -167,6 +179,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                 ctypes.POINTER(Sw2dBcTable), c_double_p, c_double_p, c_double_p, ctypes.c_int,
                                 ctypes.POINTER(P)]
     lib.sw2d_create.restype = ctypes.c_int
+    lib.sw2d_create_dip.argtypes = [ctypes.POINTER(Sw2dMesh), ctypes.POINTER(Sw2dParams),
+                                    ctypes.POINTER(Sw2dCellFields), ctypes.POINTER(Sw2dDipFields),
+                                    ctypes.POINTER(Sw2dBcTable), c_double_p, c_double_p, c_double_p, ctypes.c_int,
+                                    ctypes.POINTER(P)]
+    lib.sw2d_create_dip.restype = ctypes.c_int
     lib.sw2d_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
     lib.sw2d_step_n.restype = ctypes.c_int
     lib.sw2d_execute.argtypes = [P, c_int64_p]
@@ -237,7 +254,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 # every symbol include/sw2d_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["sw2d_create", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",

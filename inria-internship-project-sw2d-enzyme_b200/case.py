@@ -334,7 +334,7 @@ def read_map(path: str, n_params: int, n_records: int):
 # ---------------------------------------------------------------------------------------
 # boundary time series
 # ---------------------------------------------------------------------------------------
-BC_TYPES = {"q": 0, "h": 1, "z": 2, "fr": 3}
+BC_TYPES = {"q": 0, "h": 1, "z": 2, "fr": 3, "phiWq": 4}   # phiWq: DIP only (dip/swDipHyp.cpp:88-101)
 
 
 @dataclass
@@ -386,7 +386,7 @@ SOLV_DEFAULTS: Dict[str, str] = {
     "num_scheme": "godunov", "topo_discretization": "discontinuous", "negative_depth_detection": "none",
     "cfl_max": "1", "dt_max": "10", "dt_map": "100", "dt_time_series": "100", "h_min": "1e-5",
     "phi_min": "1e-16", "v_max": "100", "fr_max": "100", "t_0": "0", "t_max": "100",
-    "div_corr": "none", "store_flag": "default", "output_format": "all",
+    "div_corr": "none", "store_flag": "default", "output_format": "all", "model_momentum_dissipation": "none",
 }
 
 
@@ -417,7 +417,7 @@ def write_solv(path: str, opts: Dict[str, object]) -> None:
 # ---------------------------------------------------------------------------------------
 @dataclass
 class Case:
-    """Everything the SP step needs, in the reference numbering."""
+    """Everything the SP or DIP step needs, in the reference numbering."""
 
     mesh: Mesh
     opts: Dict[str, str]
@@ -430,6 +430,16 @@ class Case:
     head_loss: Optional[np.ndarray] = None     # (4, n): h_sing, k1, k2, alpha (degrees)
     bc: Optional[BoundarySeries] = None
     extra: Dict[str, object] = field(default_factory=dict)
+    # DIP (model_hyperb dip): phi is the cell porosity phiW; these hold the connectivity porosity
+    # of the internal and boundary edges and, with model_momentum_dissipation active, the
+    # dissipation map (3, n): mu_1, mu_2, alpha (degrees)
+    phi_g_int: Optional[np.ndarray] = None
+    phi_g_bnd: Optional[np.ndarray] = None
+    mu: Optional[np.ndarray] = None
+
+    @property
+    def is_dip(self) -> bool:
+        return str(self.opts.get("model_hyperb", "sp")).lower() == "dip"
 
 
 FRICTION_FILES = {"chezy": "friction_chezy_map.txt", "manning": "friction_manning_map.txt",
@@ -450,7 +460,19 @@ def write_case(folder: str, case: Case) -> None:
     else:
         write_map(os.path.join(inp, "initial_conditions_map.txt"), ["h", "q", "r"],
                   [_collapse(case.h0), _collapse(case.q0), _collapse(case.r0)], n)
-    write_map(os.path.join(inp, "SP_cell_porosity_map.txt"), ["SpPhiW"], [case.phi], n)
+    if case.is_dip:
+        # swDip::setPorosityParameters / setMomentumDissipationParameters (dip/swDip.cpp:1302-1406)
+        write_map(os.path.join(inp, "DIP_cell_porosity_map.txt"), ["DipPhiW"], [case.phi], n)
+        write_map(os.path.join(inp, "DIP_edge_int_porosity_map.txt"), ["DipPhiG"], [case.phi_g_int],
+                  case.mesh.edge_int_nb)
+        write_map(os.path.join(inp, "DIP_edge_bnd_porosity_map.txt"), ["DipPhiG"], [case.phi_g_bnd],
+                  case.mesh.edge_bnd_nb)
+        if case.opts.get("model_momentum_dissipation", "none") != "none":
+            mu = case.mu
+            write_map(os.path.join(inp, "cell_momentum_dissipation_map.txt"), ["mu1", "mu2", "alpha"],
+                      [mu[0], mu[1], mu[2]], n)
+    else:
+        write_map(os.path.join(inp, "SP_cell_porosity_map.txt"), ["SpPhiW"], [case.phi], n)
     write_map(os.path.join(inp, "Boussinesq_map.txt"), ["Beta"], [_collapse(case.boussinesq)], n)
     fm = case.opts.get("model_friction", "none")
     if fm != "none":
@@ -492,7 +514,17 @@ def read_case(folder: str) -> Case:
         r = h * ic[names.index("v")]
     if q is None or r is None:
         raise ValueError("initial conditions: discharge columns missing")
-    _, phi = read_map(os.path.join(inp, "SP_cell_porosity_map.txt"), 1, n)
+    dip = str(opts.get("model_hyperb", "sp")).lower() == "dip"
+    pgi = pgb = mu = None
+    if dip:
+        _, phi = read_map(os.path.join(inp, "DIP_cell_porosity_map.txt"), 1, n)
+        _, pgi = read_map(os.path.join(inp, "DIP_edge_int_porosity_map.txt"), 1, mesh.edge_int_nb)
+        _, pgb = read_map(os.path.join(inp, "DIP_edge_bnd_porosity_map.txt"), 1, mesh.edge_bnd_nb)
+        pgi, pgb = pgi[0].copy(), pgb[0].copy()
+        if opts.get("model_momentum_dissipation", "none") != "none":
+            _, mu = read_map(os.path.join(inp, "cell_momentum_dissipation_map.txt"), 3, n)
+    else:
+        _, phi = read_map(os.path.join(inp, "SP_cell_porosity_map.txt"), 1, n)
     _, bous = read_map(os.path.join(inp, "Boussinesq_map.txt"), 1, n)
     fr = None
     fm = opts.get("model_friction", "none")
@@ -503,4 +535,4 @@ def read_case(folder: str) -> Case:
         _, hl = read_map(os.path.join(inp, "singular_head_loss_map.txt"), 4, n)
     bc = read_bc_series(os.path.join(inp, "hydro_boundary_time_series.txt"))
     return Case(mesh=mesh, opts=opts, h0=h, q0=q, r0=r, phi=phi[0].copy(), boussinesq=bous[0].copy(),
-                friction=fr, head_loss=hl, bc=bc)
+                friction=fr, head_loss=hl, bc=bc, phi_g_int=pgi, phi_g_bnd=pgb, mu=mu)

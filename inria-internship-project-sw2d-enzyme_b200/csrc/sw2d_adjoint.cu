@@ -962,6 +962,7 @@ int sw2d_record(sw2d_handle* h, int64_t n_steps, int64_t checkpoint_every, int64
 {
     if (!h || n_steps <= 0 || checkpoint_every <= 0) return fail(h, SW2D_E_ARG, "invalid arguments");
     if (n_steps >= (int64_t)1 << 31) return fail(h, SW2D_E_ARG, "trajectory too long");
+    if (h->model != kModelSp) return fail(h, SW2D_E_UNSUPPORTED, "the adjoint covers the SP model only");
     CK(cudaSetDevice(h->device));
     int rc = adjoint_fixed(h);
     if (rc) return rc;

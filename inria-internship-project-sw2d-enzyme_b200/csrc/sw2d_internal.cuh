@@ -11,11 +11,15 @@
 #include <vector>
 
 #include "../../include/sw2d_b200.h"
-#include "sp_math.cuh"
+#include "dip_math.cuh"
 
 namespace sw2d {
 
 constexpr int kBlock = 256;
+
+// porosity model of a handle
+constexpr int kModelSp = 0;
+constexpr int kModelDip = 1;
 
 // Device-resident loop control.  t and t_max decide whether a step runs; `go` and `dt` are
 // written by the CFL kernel's last block (or by the frozen-dt kernel of a replay) and read by
@@ -68,6 +72,11 @@ struct DevMesh {
     const int* bctype;
     const long long* bcoff;
     const double *bctimes, *bcvals;
+    // DIP: connectivity porosity of internal and boundary edges, momentum dissipation
+    // {mu1, mu2, cos a, sin a} per cell (the cell statics' phi holds the storage porosity)
+    const double* phig;
+    const double* phigb;
+    const double4* mu;
     // parameters
     double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
     DryConsts dry;
@@ -101,6 +110,8 @@ struct sw2d_handle {
     cudaStream_t stream = nullptr;
     int64_t nc = 0, ni = 0, nb = 0;
     sw2d_params p{};
+    int model = 0;             // kModelSp or kModelDip
+    int dissipation = 0;       // DIP momentum dissipation active
     std::vector<int> cell_perm, int_perm, bnd_perm;  // [new] = caller index
     std::vector<void*> allocs;
     sw2d::DevMesh m{};

@@ -150,9 +150,10 @@ __global__ void __launch_bounds__(kB, kMinB) k_slopes(DevMesh m)
 // (swSpHyp.cpp:437-477: the L cell counts it when it is wet; the R cell when L or R is wet,
 // because the reference carries `lambda` over from the L test).
 // ------------------------------------------------------------------------------------------
-template <int kScheme, bool kBlending, int kB, int kMinB>
+template <int kScheme, bool kBlending, int kModel, int kB, int kMinB>
 __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
 {
+    constexpr bool kDip = kModel == kModelDip;
     if (!step_active(m.ctrl)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned bad = 0;
@@ -164,18 +165,36 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
         const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
         const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
         SideState SL, SR;
+        double phiG = 0.0, xL = 1.0, xR = 1.0;
+        if (kDip) {
+            phiG = ld(&m.phig[e]);
+            xL = dip_x(ca.z, phiG);
+            xR = dip_x(cb.z, phiG);
+        }
         if (kScheme == SW2D_SCHEME_GODUNOV) {
-            SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
-            SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
+            if (kDip) {
+                SL = godunov_side_dip(sa.x, sa.y, sa.z, ca.x, ca.y, xL, n.x, n.y);
+                SR = godunov_side_dip(sb.x, sb.y, sb.z, cb.x, cb.y, xR, n.x, n.y);
+            } else {
+                SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
+                SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
+            }
         } else {
             const double dtp = m.ctrl->dt;
             const double2 mp = ld(&m.mxy[e]);
             const double2 xa = ld(&m.cxy[a]), xb = ld(&m.cxy[b]);
             const double2 ga = ld(&m.slope[a]), gb = ld(&m.slope[b]);
-            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y, dtp,
-                          m.dry);
-            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y, dtp,
-                          m.dry);
+            if (kDip) {
+                SL = evr_side_dip(true, sa.x, sa.y, sa.z, ca.x, ca.y, xL, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x,
+                                  n.y, dtp);
+                SR = evr_side_dip(false, sb.x, sb.y, sb.z, cb.x, cb.y, xR, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x,
+                                  n.y, dtp);
+            } else {
+                SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y,
+                              dtp, m.dry);
+                SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y,
+                              dtp, m.dry);
+            }
         }
         const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
         if (m.lmax) m.lmax[e] = lm;
@@ -186,7 +205,8 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
         m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
         const double hL = SL.z - ca.x, hR = SR.z - cb.x;
         if ((hL > m.h_min) || (hR > m.h_min)) {
-            EdgeFlux f = hllc(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min);
+            EdgeFlux f = kDip ? hllc_dip(kBlending, ca.y, cb.y, phiG, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min)
+                              : hllc(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min);
             bad |= f.bad;
             if (isnan(f.f1)) bad |= kStatusNanFlux;
             if (m.flux) {
@@ -220,7 +240,9 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
         const double4 s = ld(&m.st[c]);
         const double4 cs = ld(&m.cst[c]);
         const double4 g = ld(&m.bgeo[e]);
-        SideState S = godunov_side(s.x, s.y, s.z, cs.x, cs.y, g.x, g.y);
+        const double phiGb = kDip ? ld(&m.phigb[e]) : 0.0;
+        SideState S = kDip ? godunov_side_dip(s.x, s.y, s.z, cs.x, cs.y, dip_x(cs.z, phiGb), g.x, g.y)
+                           : godunov_side(s.x, s.y, s.z, cs.x, cs.y, g.x, g.y);
         const double lm = (kScheme == SW2D_SCHEME_GODUNOV) ? smax(fabs(S.lp), fabs(S.lm)) : smax(fabs(S.lm), fabs(S.lp));
         if (m.lmaxb) m.lmaxb[e] = lm;
         const int sb = ld(&m.bslot[e]);
@@ -229,7 +251,8 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
         const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
         const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, m.ctrl->t);
         double f1, f2, f3;
-        bad |= boundary_flux(cs.y, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
+        bad |= kDip ? boundary_flux_dip(cs.y, phiGb, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3)
+                    : boundary_flux(cs.y, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
         if (m.bflux) m.bflux[e] = make_double4(f1, f2, f3, 0.0);
         const double cf = g.w, nx = g.x, ny = g.y;
         const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
@@ -320,7 +343,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
 // ------------------------------------------------------------------------------------------
 // k_update: balance + sources for one cell, then t += dt (thread 0).
 // ------------------------------------------------------------------------------------------
-template <int kFriction, bool kHeadLoss, bool kStoreB>
+template <int kFriction, bool kHeadLoss, bool kStoreB, bool kDissip>
 __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
 {
     Ctrl* ctrl = m.ctrl;
@@ -356,6 +379,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
             qq += v.y * dt;
             rr += v.z * dt;
         }
+    }
+    if (kDissip) {  // DIP momentum dissipation, before the round-off flush (dip/swDipHyp.cpp:295-324)
+        const double4 mu = ld(&m.mu[c]);
+        momentum_dissipation(mu.x, mu.y, mu.z, mu.w, s0.x, s0.y, s0.z, hh, qq, rr);
     }
     if (kStoreB) m.bal[c] = make_double4(hh, qq, rr, 0.0);  // for the reverse sweep
     if (fabs(hh) < kSmallReal) hh = 0.;
@@ -533,6 +560,7 @@ int status_to_code(sw2d_handle* h, unsigned st)
     if (st & kStatusNegDepth) return fail(h, SW2D_E_NEG_DEPTH, "SP - negative water depth");
     if (st & kStatusBcType) return fail(h, SW2D_E_BC_TYPE, "boundary condition type not handled");
     if (st & kStatusBcFr) return fail(h, SW2D_E_BC_FR, "incorrect value for 'fr'-type boundary condition");
+    if (st & kStatusPhiG) return fail(h, SW2D_E_PHIG, "specificForce : phiG is < small");
     if (st & kStatusUnsupported)
         return fail(h, SW2D_E_UNSUPPORTED, "cell with more neighbours than the adjoint's slope reverse handles");
     return SW2D_OK;
@@ -550,37 +578,44 @@ struct Variant {
 constexpr Variant kVariants[] = {{256, 3}, {256, 2}, {256, 4}, {128, 4}, {128, 8}, {512, 1}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-template <int kScheme, bool kBlending, int V>
+template <int kScheme, bool kBlending, int kModel, int V>
 void launch_edges_v(sw2d_handle* h, const DevMesh& m, unsigned n)
 {
     constexpr int B = kVariants[V].block, M = kVariants[V].minb;
-    k_edges<kScheme, kBlending, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(m);
+    k_edges<kScheme, kBlending, kModel, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(m);
 }
 
-template <int kScheme, bool kBlending>
+template <int kScheme, bool kBlending, int kModel>
 void launch_edges_s(sw2d_handle* h, const DevMesh& m, unsigned n, int v)
 {
     switch (v) {
-        case 1: launch_edges_v<kScheme, kBlending, 1>(h, m, n); break;
-        case 2: launch_edges_v<kScheme, kBlending, 2>(h, m, n); break;
-        case 3: launch_edges_v<kScheme, kBlending, 3>(h, m, n); break;
-        case 4: launch_edges_v<kScheme, kBlending, 4>(h, m, n); break;
-        case 5: launch_edges_v<kScheme, kBlending, 5>(h, m, n); break;
-        default: launch_edges_v<kScheme, kBlending, 0>(h, m, n); break;
+        case 1: launch_edges_v<kScheme, kBlending, kModel, 1>(h, m, n); break;
+        case 2: launch_edges_v<kScheme, kBlending, kModel, 2>(h, m, n); break;
+        case 3: launch_edges_v<kScheme, kBlending, kModel, 3>(h, m, n); break;
+        case 4: launch_edges_v<kScheme, kBlending, kModel, 4>(h, m, n); break;
+        case 5: launch_edges_v<kScheme, kBlending, kModel, 5>(h, m, n); break;
+        default: launch_edges_v<kScheme, kBlending, kModel, 0>(h, m, n); break;
+    }
+}
+
+template <int kModel>
+void launch_edges_m(sw2d_handle* h, const DevMesh& m, int v)
+{
+    const unsigned n = (unsigned)(m.ni + m.nb);
+    const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
+    if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
+        if (bl) launch_edges_s<SW2D_SCHEME_GODUNOV, true, kModel>(h, m, n, v);
+        else launch_edges_s<SW2D_SCHEME_GODUNOV, false, kModel>(h, m, n, v);
+    } else {
+        if (bl) launch_edges_s<SW2D_SCHEME_MUSCL_EVR, true, kModel>(h, m, n, v);
+        else launch_edges_s<SW2D_SCHEME_MUSCL_EVR, false, kModel>(h, m, n, v);
     }
 }
 
 void launch_edges(sw2d_handle* h, const DevMesh& m, int v)
 {
-    const unsigned n = (unsigned)(m.ni + m.nb);
-    const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
-    if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
-        if (bl) launch_edges_s<SW2D_SCHEME_GODUNOV, true>(h, m, n, v);
-        else launch_edges_s<SW2D_SCHEME_GODUNOV, false>(h, m, n, v);
-    } else {
-        if (bl) launch_edges_s<SW2D_SCHEME_MUSCL_EVR, true>(h, m, n, v);
-        else launch_edges_s<SW2D_SCHEME_MUSCL_EVR, false>(h, m, n, v);
-    }
+    if (h->model == kModelDip) launch_edges_m<kModelDip>(h, m, v);
+    else launch_edges_m<kModelSp>(h, m, v);
 }
 
 void launch_edges(sw2d_handle* h, int v) { launch_edges(h, h->m, v); }
@@ -606,23 +641,31 @@ void launch_slopes(sw2d_handle* h, const DevMesh& m, int v)
 
 void launch_slopes(sw2d_handle* h, int v) { launch_slopes(h, h->m, v); }
 
-template <int kF, bool kStoreB>
+template <int kF, bool kStoreB, bool kDissip>
 void launch_update_f(sw2d_handle* h, const DevMesh& m, unsigned g)
 {
-    if (h->p.singular_head_loss) k_update<kF, true, kStoreB><<<g, kBlock, 0, h->stream>>>(m);
-    else k_update<kF, false, kStoreB><<<g, kBlock, 0, h->stream>>>(m);
+    if (h->p.singular_head_loss) k_update<kF, true, kStoreB, kDissip><<<g, kBlock, 0, h->stream>>>(m);
+    else k_update<kF, false, kStoreB, kDissip><<<g, kBlock, 0, h->stream>>>(m);
 }
 
-template <bool kStoreB>
-void launch_update_s(sw2d_handle* h, const DevMesh& m)
+template <bool kStoreB, bool kDissip>
+void launch_update_d(sw2d_handle* h, const DevMesh& m)
 {
     const unsigned g = grid_for(m.nc);
     switch (h->p.friction) {
-        case SW2D_FRICTION_CHEZY: launch_update_f<SW2D_FRICTION_CHEZY, kStoreB>(h, m, g); break;
-        case SW2D_FRICTION_MANNING: launch_update_f<SW2D_FRICTION_MANNING, kStoreB>(h, m, g); break;
-        case SW2D_FRICTION_STRICKLER: launch_update_f<SW2D_FRICTION_STRICKLER, kStoreB>(h, m, g); break;
-        default: launch_update_f<SW2D_FRICTION_NONE, kStoreB>(h, m, g); break;
+        case SW2D_FRICTION_CHEZY: launch_update_f<SW2D_FRICTION_CHEZY, kStoreB, kDissip>(h, m, g); break;
+        case SW2D_FRICTION_MANNING: launch_update_f<SW2D_FRICTION_MANNING, kStoreB, kDissip>(h, m, g); break;
+        case SW2D_FRICTION_STRICKLER: launch_update_f<SW2D_FRICTION_STRICKLER, kStoreB, kDissip>(h, m, g); break;
+        default: launch_update_f<SW2D_FRICTION_NONE, kStoreB, kDissip>(h, m, g); break;
     }
+}
+
+// the recorded post-balance state serves the adjoint, which covers the SP model only
+template <bool kStoreB>
+void launch_update_s(sw2d_handle* h, const DevMesh& m)
+{
+    if (!kStoreB && h->dissipation) launch_update_d<false, true>(h, m);
+    else launch_update_d<kStoreB, false>(h, m);
 }
 
 // phase i of one step on the handle's stream: 0 slopes, 1 edges, 2 cfl, 3 update
@@ -704,6 +747,10 @@ int check_mesh(const sw2d_mesh* m)
     return SW2D_OK;
 }
 
+int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                 const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
+                 const double* r0, int device, sw2d_handle** out);
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
@@ -716,6 +763,26 @@ int sw2d_abi_version(void) { return SW2D_ABI_VERSION; }
 int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
                 const sw2d_bc_table* bc, const double* h0, const double* q0, const double* r0, int device,
                 sw2d_handle** out)
+{
+    return create_model(mesh, params, fields, nullptr, bc, h0, q0, r0, device, out);
+}
+
+int sw2d_create_dip(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                    const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
+                    const double* r0, int device, sw2d_handle** out)
+{
+    if (!dip) return fail(nullptr, SW2D_E_ARG, "DIP fields missing");
+    return create_model(mesh, params, fields, dip, bc, h0, q0, r0, device, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// sw2d_create / sw2d_create_dip: `dip` selects the DIP model
+int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                 const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
+                 const double* r0, int device, sw2d_handle** out)
 {
     sw2d_handle* h = nullptr;
     if (!out) return fail(h, SW2D_E_ARG, "out is NULL");
@@ -747,6 +814,24 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
         if (!(fields->boussinesq[c] >= 1.0)) return fail(h, SW2D_E_ARG, "boussinesq coeff. should be >= 1");
         if ((fields->phi[c] < 0.0) || (fields->phi[c] > 1.0)) return fail(h, SW2D_E_ARG, "porosity should belong to [0,1]");
     }
+    // swDip::checkParameterConsistency (dip/swDip.cpp:121-240): phiG in [0,1], not above phiW
+    if (dip) {
+        if ((mesh->edge_int_nb && !dip->phi_g_int) || (mesh->edge_bnd_nb && !dip->phi_g_bnd))
+            return fail(h, SW2D_E_ARG, "DIP edge porosity map missing");
+        if (dip->momentum_dissipation && (!dip->mu_1 || !dip->mu_2 || !dip->mu_alpha))
+            return fail(h, SW2D_E_ARG, "momentum dissipation map missing");
+        for (int64_t e = 0; e < mesh->edge_bnd_nb; e++) {
+            const double g = dip->phi_g_bnd[e];
+            if (g < 0.0 || g > 1.0 || g > fields->phi[mesh->edge_bnd_cell[e]])
+                return fail(h, SW2D_E_ARG, "boundary edge porosity outside [0, cell porosity]");
+        }
+        for (int64_t e = 0; e < mesh->edge_int_nb; e++) {
+            const double g = dip->phi_g_int[e];
+            if (g < 0.0 || g > 1.0 || g > fields->phi[mesh->edge_int_cells[2 * e]] ||
+                g > fields->phi[mesh->edge_int_cells[2 * e + 1]])
+                return fail(h, SW2D_E_ARG, "internal edge porosity outside [0, cell porosity]");
+        }
+    }
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
@@ -755,6 +840,8 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     h = new sw2d_handle();
     h->device = device;
     h->p = *params;
+    h->model = dip ? kModelDip : kModelSp;
+    h->dissipation = (dip && dip->momentum_dissipation) ? 1 : 0;
     h->nc = mesh->cell_nb;
     h->ni = mesh->edge_int_nb;
     h->nb = mesh->edge_bnd_nb;
@@ -936,6 +1023,23 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     double4* bgeo_d = nullptr;
     if ((rc = dev_upload(h, bgeo, &bgeo_d))) return bail(rc);
     m.bgeo = bgeo_d;
+    if (dip) {
+        std::vector<double> pgi(ni), pgb(nb);
+        for (int64_t i = 0; i < ni; i++) pgi[i] = dip->phi_g_int[h->int_perm[i]];
+        for (int64_t i = 0; i < nb; i++) pgb[i] = dip->phi_g_bnd[h->bnd_perm[i]];
+        UP(pgi, m.phig);
+        UP(pgb, m.phigb);
+        if (dip->momentum_dissipation) {
+            // swDip::setMomentumDissipationParameters (dip/swDip.cpp:1302-1334)
+            std::vector<double4> mu(nc);
+            for (int64_t i = 0; i < nc; i++) {
+                const int o = h->cell_perm[i];
+                double a = dip->mu_alpha[o] * atan(1.0) / 45.0;
+                mu[i] = make_double4(dip->mu_1[o], dip->mu_2[o], cos(a), sin(a));
+            }
+            UP(mu, m.mu);
+        }
+    }
     UP(h->cell_perm, h->d_cell_perm);
     UP(h->int_perm, h->d_int_perm);
     UP(h->bnd_perm, h->d_bnd_perm);
@@ -994,6 +1098,10 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
     *out = h;
     return SW2D_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
 {

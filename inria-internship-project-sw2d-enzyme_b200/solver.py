@@ -33,7 +33,8 @@ class Sw2dError(RuntimeError):
 
 
 class SpModel:
-    """SW2D single-porosity model running on one GPU."""
+    """SW2D porosity model (single porosity, or dual integral porosity when the case says
+    model_hyperb dip) running on one GPU."""
 
     def __init__(self, case: Case, device: int = 0):
         self.lib = capi.load_library()
@@ -44,9 +45,14 @@ class SpModel:
         self._in = capi.native_inputs(case)
         i = self._in
         handle = ctypes.c_void_p()
-        st = self.lib.sw2d_create(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
-                                  ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0), capi._dp(i.r0), int(device),
-                                  ctypes.byref(handle))
+        if i.dip is not None:  # model_hyperb dip: swDip
+            st = self.lib.sw2d_create_dip(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
+                                          ctypes.byref(i.dip), ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0),
+                                          capi._dp(i.r0), int(device), ctypes.byref(handle))
+        else:
+            st = self.lib.sw2d_create(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
+                                      ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0), capi._dp(i.r0),
+                                      int(device), ctypes.byref(handle))
         if st != 0:
             raise Sw2dError(st, self.lib.sw2d_last_error(None).decode())
         self.handle = handle
@@ -54,8 +60,8 @@ class SpModel:
     @classmethod
     def from_folder(cls, folder: str, device: int = 0) -> "SpModel":
         case = read_case(folder)
-        if str(case.opts.get("model_hyperb", "sp")).lower() != "sp":
-            raise Sw2dError(-8, f"model_hyperb {case.opts.get('model_hyperb')!r}: only 'sp' is implemented")
+        if str(case.opts.get("model_hyperb", "sp")).lower() not in ("sp", "dip"):
+            raise Sw2dError(-8, f"model_hyperb {case.opts.get('model_hyperb')!r}: only 'sp' and 'dip' are implemented")
         return cls(case, device)
 
     def _check(self, st: int) -> None:

@@ -156,3 +156,38 @@ def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "
     return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
                 boussinesq=np.full(n, boussinesq), friction=fr, head_loss=hl, bc=bc,
                 extra={"name": "channel_features", "nx": nx, "ny": ny})
+
+
+def dip_channel(n_cells: int = 3000, scheme: str = "muscl_evr", topo: str = "discontinuous",
+                friction: str = "manning", inflow: str = "q", outflow: str = "fr", dissipation: bool = True,
+                boussinesq: float = 1.0, t_max: float = 40.0, seed: int = 11) -> Case:
+    """The feature channel as a dual integral porosity (DIP) case: a seeded smooth storage
+    porosity phiW in [0.4, 1] per cell (building blocks), a connectivity porosity per edge in
+    [0.5, 1] x the smaller phiW of its cells (the reference requires phiG <= phiW,
+    dip/swDip.cpp:121-240), an inflow of type 'q' (phi q) or 'phiWq' on the left, an outflow
+    condition on the right, walls elsewhere, and a momentum-dissipation map."""
+    base = channel_features(n_cells=n_cells, scheme=scheme, topo=topo, friction=friction, outflow=outflow,
+                            head_loss=False, boussinesq=boussinesq, t_max=t_max, seed=seed)
+    mesh = base.mesh
+    n = mesh.cell_nb
+    rng = np.random.default_rng(seed + 1)
+    phiW = 0.4 + 0.6 * _smooth_field(mesh.cell_x, mesh.cell_y, 60.0, 12.0, seed + 2, coarse=12)
+    L, R = mesh.edge_int_cells[:, 0], mesh.edge_int_cells[:, 1]
+    phi_g_int = np.minimum(phiW[L], phiW[R]) * rng.uniform(0.5, 1.0, size=mesh.edge_int_nb)
+    phi_g_bnd = phiW[mesh.edge_bnd_cell] * rng.uniform(0.5, 1.0, size=mesh.edge_bnd_nb)
+    opts = dict(base.opts)
+    opts["model_hyperb"] = "dip"
+    mu = None
+    if dissipation:
+        opts["model_momentum_dissipation"] = "active"
+        mu = np.stack([rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 90.0, n)])
+    bc = base.bc
+    types = list(bc.types)
+    types[1] = inflow
+    values = np.array(bc.values, copy=True)
+    if inflow == "phiWq":
+        values[1] = values[1] * 0.7   # phiW q prescribed directly
+    bc = BoundarySeries(codes=bc.codes, types=types, times=bc.times, values=values)
+    return Case(mesh=mesh, opts=opts, h0=base.h0, q0=base.q0, r0=base.r0, phi=phiW, boussinesq=base.boussinesq,
+                friction=base.friction, head_loss=None, bc=bc, extra={"name": "dip_channel"},
+                phi_g_int=phi_g_int, phi_g_bnd=phi_g_bnd, mu=mu)

@@ -1,11 +1,12 @@
-// Test harness around the reference's own native SP solver (compiled from the reference
+// Test harness around the reference's own native SP and DIP solvers (compiled from the reference
 // sources by oracle/Makefile).  It is a checker, never part of the product.
 //
-// The reference only runs a whole simulation (`swSp::execute`, src/sw2dSolver/models/sp/swSp.cpp:482-670).
-// This subclass reaches the protected members the same way the reference's own assimilation
-// layer does (assim/swSpE.h:50 subclasses swSp) and re-states the body of the time loop
-// (swSp.cpp:522-589) without the result storage, so that a test can advance the reference N
-// steps and read its state, fluxes and Riemann states at full precision.
+// The reference only runs a whole simulation (`swSp::execute`, src/sw2dSolver/models/sp/swSp.cpp:482-670;
+// `swDip::execute`, models/dip/swDip.cpp, the same loop).  This subclass template reaches the
+// protected members the same way the reference's own assimilation layer does (assim/swSpE.h:50
+// subclasses swSp) and re-states the body of the time loop (swSp.cpp:522-589) without the
+// result storage, so that a test can advance the reference N steps and read its state, fluxes
+// and Riemann states at full precision.
 //
 // C entry points (ctypes):
 //   sw2dref_open(folder, quiet)        init exactly as src/sw2dSolver/main.cpp:99-163 does
@@ -26,107 +27,141 @@
 #include "../common/swMessage.h"
 #include "../common/geometry/swMesh.h"
 #include "common/swSolverParam.h"
+#include "models/dip/swDip.h"
 #include "models/sp/swSp.h"
+
+#include <type_traits>
 
 namespace {
 
-class RefSp : public swSp
+// The operations a test needs, whichever model runs.
+class RefModel
 {
 public:
+    virtual ~RefModel() {}
+    virtual swParent* parent() = 0;
+    virtual bool stepOnce() = 0;
+    virtual void beginTime() = 0;
+    virtual void slopes(double* sx, double* sy) = 0;
+    virtual int getArray(const std::string& name, double* out) = 0;
+    virtual void setState(const double* h, const double* q, const double* r) = 0;
+    virtual size_t nCells() const = 0;
+    virtual size_t nInt() const = 0;
+    virtual size_t nBnd() const = 0;
+    virtual double time() const = 0;
+    virtual double timeStep() const = 0;
+    virtual double tMax() const = 0;
+    virtual bool run() = 0;
+};
+
+template <class M>
+class Ref : public M, public RefModel
+{
+public:
+    swParent* parent() override { return this; }
+    bool run() override { return this->execute(); }
+
     // One pass of the body of swSp::execute's time loop (sp/swSp.cpp:522-589), storage left out.
-    bool stepOnce()
+    bool stepOnce() override
     {
-        if (!(t < t_max)) return false;
-        computeBC(t);
-        hypCompute(div_corr_option, n_it_div_max, num_scheme, dt);
-        if (model_momentum_diffusion != "none") parabComputeExplicit();
-        if (model_friction != "none") sourceFriction(model_friction, dt);
-        if (model_singular_head_loss != "none") sourceSingularHeadLoss(dt);
-        if (model_runoff != "none")
+        if (!(this->t < this->t_max)) return false;
+        this->computeBC(this->t);
+        this->hypCompute(this->div_corr_option, this->n_it_div_max, this->num_scheme, this->dt);
+        if (this->model_momentum_diffusion != "none") this->parabComputeExplicit();
+        if (this->model_friction != "none") this->sourceFriction(this->model_friction, this->dt);
+        if (this->model_singular_head_loss != "none") this->sourceSingularHeadLoss(this->dt);
+        if (this->model_runoff != "none")
         {
-            if (model_porosity_rainfall == "everywhere") sourceRunoffEverywhere();
-            else if (model_porosity_rainfall == "water_only") sourceRunoffWateronly();
+            if (this->model_porosity_rainfall == "everywhere") this->sourceRunoffEverywhere();
+            else if (this->model_porosity_rainfall == "water_only") this->sourceRunoffWateronly();
         }
-        if (model_infiltration != "none") sourceInfiltration();
-        if (model_wind != "none") sourceWind();
-        correctVelocity();
-        t += dt;
+        if (this->model_infiltration != "none") this->sourceInfiltration();
+        if (this->model_wind != "none") this->sourceWind();
+        this->correctVelocity();
+        this->t += this->dt;
         return true;
     }
 
-    void beginTime() { t = t_0; }
+    void beginTime() override { this->t = this->t_0; }
 
     // Limited free-surface slopes exactly as the MUSCL-EVR reconstruction computes them
     // (sp/swSpHypMusclEvr.cpp:126-139), for kernel-level checks.
-    void slopes(double* sx, double* sy)
+    void slopes(double* sx, double* sy) override
     {
-        std::vector<double> z_cell(cell_nb), dzx(cell_nb), dzy(cell_nb);
-        for (size_t i = 0; i < cell_nb; i++) z_cell[i] = water_depth[i] + cell_z_b[i];
-        computeMusclSlopes(cell_centre_x, cell_centre_y, cell_neigh_cell_idx,
-                           edge_int_midpoint_x, edge_int_midpoint_y,
-                           edge_int_celL_idx, edge_int_celR_idx, z_cell, dzx, dzy);
-        std::memcpy(sx, dzx.data(), cell_nb * sizeof(double));
-        std::memcpy(sy, dzy.data(), cell_nb * sizeof(double));
+        std::vector<double> z_cell(this->cell_nb), dzx(this->cell_nb), dzy(this->cell_nb);
+        for (size_t i = 0; i < this->cell_nb; i++) z_cell[i] = this->water_depth[i] + this->cell_z_b[i];
+        this->computeMusclSlopes(this->cell_centre_x, this->cell_centre_y, this->cell_neigh_cell_idx,
+                           this->edge_int_midpoint_x, this->edge_int_midpoint_y,
+                           this->edge_int_celL_idx, this->edge_int_celR_idx, z_cell, dzx, dzy);
+        std::memcpy(sx, dzx.data(), this->cell_nb * sizeof(double));
+        std::memcpy(sy, dzy.data(), this->cell_nb * sizeof(double));
     }
 
-    int getArray(const std::string& name, double* out)
+    int getArray(const std::string& name, double* out) override
     {
         auto put = [&](const std::vector<double>& v) { std::memcpy(out, v.data(), v.size() * sizeof(double)); return (int)v.size(); };
         auto put2 = [&](const std::vector<std::array<double, 2>>& v, int side) {
             for (size_t i = 0; i < v.size(); i++) out[i] = v[i][side];
             return (int)v.size();
         };
-        if (name == "h") return put(water_depth);
-        if (name == "q") return put(unit_discharge_x);
-        if (name == "r") return put(unit_discharge_y);
-        if (name == "F1_int") return put(F1_int);
-        if (name == "F2_int") return put(F2_int);
-        if (name == "F3_int") return put(F3_int);
-        if (name == "s2L_int") return put(s2L_int);
-        if (name == "s2R_int") return put(s2R_int);
-        if (name == "F1_bnd") return put(F1_bnd);
-        if (name == "F2_bnd") return put(F2_bnd);
-        if (name == "F3_bnd") return put(F3_bnd);
-        if (name == "s2R_bnd") return put(s2R_bnd);
-        if (name == "lambda_max_int") return put(lambda_max_int);
-        if (name == "lambda_max_bnd") return put(lambda_max_bnd);
-        if (name == "z_riemann_L") return put2(z_riemann_int, 0);
-        if (name == "z_riemann_R") return put2(z_riemann_int, 1);
-        if (name == "q_riemann_L") return put2(q_riemann_int, 0);
-        if (name == "q_riemann_R") return put2(q_riemann_int, 1);
-        if (name == "r_riemann_L") return put2(r_riemann_int, 0);
-        if (name == "r_riemann_R") return put2(r_riemann_int, 1);
-        if (name == "lambda_minus_L") return put2(lambda_minus_int, 0);
-        if (name == "lambda_minus_R") return put2(lambda_minus_int, 1);
-        if (name == "lambda_plus_L") return put2(lambda_plus_int, 0);
-        if (name == "lambda_plus_R") return put2(lambda_plus_int, 1);
-        if (name == "phi") return put(phi);
-        if (name == "area") return put(cell_area);
-        if (name == "z_b") return put(cell_z_b);
-        if (name == "cx") return put(cell_centre_x);
-        if (name == "cy") return put(cell_centre_y);
+        if (name == "h") return put(this->water_depth);
+        if (name == "q") return put(this->unit_discharge_x);
+        if (name == "r") return put(this->unit_discharge_y);
+        if (name == "F1_int") return put(this->F1_int);
+        if (name == "F2_int") return put(this->F2_int);
+        if (name == "F3_int") return put(this->F3_int);
+        if (name == "s2L_int") return put(this->s2L_int);
+        if (name == "s2R_int") return put(this->s2R_int);
+        if (name == "F1_bnd") return put(this->F1_bnd);
+        if (name == "F2_bnd") return put(this->F2_bnd);
+        if (name == "F3_bnd") return put(this->F3_bnd);
+        if (name == "s2R_bnd") return put(this->s2R_bnd);
+        if (name == "lambda_max_int") return put(this->lambda_max_int);
+        if (name == "lambda_max_bnd") return put(this->lambda_max_bnd);
+        if (name == "z_riemann_L") return put2(this->z_riemann_int, 0);
+        if (name == "z_riemann_R") return put2(this->z_riemann_int, 1);
+        if (name == "q_riemann_L") return put2(this->q_riemann_int, 0);
+        if (name == "q_riemann_R") return put2(this->q_riemann_int, 1);
+        if (name == "r_riemann_L") return put2(this->r_riemann_int, 0);
+        if (name == "r_riemann_R") return put2(this->r_riemann_int, 1);
+        if (name == "lambda_minus_L") return put2(this->lambda_minus_int, 0);
+        if (name == "lambda_minus_R") return put2(this->lambda_minus_int, 1);
+        if (name == "lambda_plus_L") return put2(this->lambda_plus_int, 0);
+        if (name == "lambda_plus_R") return put2(this->lambda_plus_int, 1);
+        if (name == "phi") {
+            if constexpr (std::is_same<M, swDip>::value) return put(this->phiW);
+            else return put(this->phi);
+        }
+        if constexpr (std::is_same<M, swDip>::value) {
+            if (name == "phiG_int") return put(this->phiG_int);
+            if (name == "phiG_bnd") return put(this->phiG_bnd);
+        }
+        if (name == "area") return put(this->cell_area);
+        if (name == "z_b") return put(this->cell_z_b);
+        if (name == "cx") return put(this->cell_centre_x);
+        if (name == "cy") return put(this->cell_centre_y);
         return -1;
     }
 
-    void setState(const double* h, const double* q, const double* r)
+    void setState(const double* h, const double* q, const double* r) override
     {
-        std::memcpy(water_depth.data(), h, cell_nb * sizeof(double));
-        std::memcpy(unit_discharge_x.data(), q, cell_nb * sizeof(double));
-        std::memcpy(unit_discharge_y.data(), r, cell_nb * sizeof(double));
+        std::memcpy(this->water_depth.data(), h, this->cell_nb * sizeof(double));
+        std::memcpy(this->unit_discharge_x.data(), q, this->cell_nb * sizeof(double));
+        std::memcpy(this->unit_discharge_y.data(), r, this->cell_nb * sizeof(double));
     }
 
-    size_t nCells() const { return cell_nb; }
-    size_t nInt() const { return edge_int_nb; }
-    size_t nBnd() const { return edge_bnd_nb; }
-    double time() const { return t; }
-    double timeStep() const { return dt; }
-    double tMax() const { return t_max; }
+    size_t nCells() const override { return this->cell_nb; }
+    size_t nInt() const override { return this->edge_int_nb; }
+    size_t nBnd() const override { return this->edge_bnd_nb; }
+    double time() const override { return this->t; }
+    double timeStep() const override { return this->dt; }
+    double tMax() const override { return this->t_max; }
 };
 
 struct Handle
 {
     swIO* io = nullptr;
-    RefSp* model = nullptr;
+    RefModel* model = nullptr;
     std::ofstream* log = nullptr;
 };
 
@@ -142,7 +177,7 @@ struct QuietErr
 
 extern "C" {
 
-// Mirrors src/sw2dSolver/main.cpp:76-163 for an SP case (model_hyperb sp).
+// Mirrors src/sw2dSolver/main.cpp:76-163 for an SP or DIP case (model_hyperb sp | dip).
 void* sw2dref_open(const char* folder, int quiet)
 {
     QuietErr q(quiet != 0);
@@ -153,14 +188,17 @@ void* sw2dref_open(const char* folder, int quiet)
     swMessage::outfile = hd->log;
     swSolverParam* param = new swSolverParam(hd->io);
     if (param->readParameters() != EXIT_SUCCESS) return nullptr;
-    if (param->getModelHyp() != "sp") return nullptr;
+    const std::string hyp = param->getModelHyp();
+    if (hyp != "sp" && hyp != "dip") return nullptr;
     swMesh* mesh = new swMesh(hd->io);
     if (mesh->build() != EXIT_SUCCESS) return nullptr;
     if (param->getHotstart() == false) hd->io->createEmptyOutputFolder(true);
-    hd->model = new RefSp();
-    hd->model->setIOPointer(hd->io);
-    hd->model->importAttributesFromSolverParam(param);
-    if (hd->model->init(mesh) != EXIT_SUCCESS) return nullptr;
+    if (hyp == "dip") hd->model = new Ref<swDip>();
+    else hd->model = new Ref<swSp>();
+    swParent* p = hd->model->parent();
+    p->setIOPointer(hd->io);
+    p->importAttributesFromSolverParam(param);
+    if (p->init(mesh) != EXIT_SUCCESS) return nullptr;
     delete param;
     delete mesh;
     hd->model->beginTime();
@@ -184,7 +222,7 @@ int sw2dref_run(void* h)
 {
     QuietErr q(true);
     Handle* hd = static_cast<Handle*>(h);
-    return hd->model->execute() == EXIT_SUCCESS ? 0 : 1;
+    return hd->model->run() == EXIT_SUCCESS ? 0 : 1;
 }
 
 double sw2dref_time(void* h) { return static_cast<Handle*>(h)->model->time(); }
@@ -196,7 +234,7 @@ long sw2dref_edge_bnd_nb(void* h) { return (long)static_cast<Handle*>(h)->model-
 
 void sw2dref_get_state(void* h, double* hh, double* q, double* r)
 {
-    RefSp* m = static_cast<Handle*>(h)->model;
+    RefModel* m = static_cast<Handle*>(h)->model;
     m->getArray("h", hh);
     m->getArray("q", q);
     m->getArray("r", r);

@@ -12,7 +12,9 @@ h/q/r...) and from the same reference objects linked with the portable exp/log o
 build (oracle/_ref/libsw2d_ref_pm.so, fields ..._pm).  ``libm_stable`` records whether the two
 agree within 1e-10 (relative, infinity norm; discharges scaled by max(|q|max, h_max sqrt(g h_max))).
 
-Run here (the reference tree must be present):  python tests/golden/make_golden.py
+The dip_* cases are dual integral porosity cases (the reference's swDip).
+
+Run here (the reference tree must be present):  python tests/golden/make_golden.py [name ...]
 """
 from __future__ import annotations
 
@@ -44,7 +46,15 @@ CASES = {
     "chan_muscl_blend_chezy_z_b11": ("channel_features", {"scheme": "muscl_evr", "topo": "blending",
                                                           "friction": "chezy", "outflow": "z", "boussinesq": 1.1}),
     "chan_godunov_disc_none_q": ("channel_features", {"friction": "none", "outflow": "q", "head_loss": False}),
+    # dual integral porosity (model_hyperb dip)
+    "dip_muscl_disc_manning_q_fr": ("dip_channel", {"n_cells": 2000}),
+    "dip_godunov_blend_strickler_phiwq_h": ("dip_channel", {"n_cells": 2000, "scheme": "godunov", "topo": "blending",
+                                                             "friction": "strickler", "inflow": "phiWq",
+                                                             "outflow": "h", "dissipation": False}),
+    "dip_muscl_blend_chezy_q_z_b11": ("dip_channel", {"n_cells": 2000, "topo": "blending", "friction": "chezy",
+                                                       "outflow": "z", "boussinesq": 1.1}),
 }
+DIP_BUILDERS = {"dip_channel"}
 NATIVE_KEYS = ["model_hyperb", "model_friction", "model_singular_head_loss", "num_scheme", "topo_discretization",
                "t_max", "dt_max", "dt_map", "dt_time_series", "h_min", "fr_max", "store_flag"]
 
@@ -61,7 +71,7 @@ def case_digest(case) -> str:
               m.edge_int_ny, m.edge_int_mx, m.edge_int_my, m.edge_bnd_cell, m.edge_bnd_length, m.edge_bnd_nx,
               m.edge_bnd_ny, m.edge_bnd_code, case.h0, case.q0, case.r0, case.phi, case.boussinesq):
         h.update(np.ascontiguousarray(a).tobytes())
-    for a in (case.friction, case.head_loss):
+    for a in (case.friction, case.head_loss, case.phi_g_int, case.phi_g_bnd, case.mu):
         if a is not None:
             h.update(np.ascontiguousarray(a).tobytes())
     h.update(json.dumps(case.opts, sort_keys=True, default=str).encode())
@@ -87,13 +97,16 @@ def state_rel_err(got, want) -> float:
     return max(errs)
 
 
-def main():
+def main(only=None):
+    """Regenerates every fixture, or only the named ones (command-line arguments)."""
     from oracle.binding import RefSolver, build, reference_available
     build(reference=True)
     assert reference_available(), "reference sources not found: cannot make golden fixtures"
     tmp = tempfile.mkdtemp(prefix="sw2d_golden_")
     try:
         for name, (builder, kwargs) in CASES.items():
+            if only and name not in only:
+                continue
             case = build_case(builder, kwargs)
             folder = os.path.join(tmp, name)
             pkg.write_case(folder, case)
@@ -111,6 +124,8 @@ def main():
             print(name, case.mesh.cell_nb, done, ref.t, "libm-stable" if stable else "libm-sensitive",
                   "%.2e" % state_rel_err((h, q, r), (hp, qp, rp)))
 
+        if only and "sp_toce" not in only:
+            return
         src = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
         folder = os.path.join(tmp, "sp_toce")
         shutil.copytree(src, folder)
@@ -152,4 +167,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
