@@ -56,6 +56,8 @@ def _args():
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--adjoint-every", type=int, default=100, help="checkpoint interval of the adjoint")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--dip-cells", type=int, default=4_000_000, help="cells of the DIP forward line (0: skip)")
+    ap.add_argument("--dip-steps", type=int, default=200)
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint measurement (one JSON line), e.g. for profiling")
     ap.add_argument("--launch-config", default=None,
@@ -275,6 +277,30 @@ def run_adjoint(pkg, args, local_rank):
     }
 
 
+def run_dip(pkg, args, local_rank):
+    """The dual integral porosity forward step on the DIP feature channel at `--dip-cells`
+    cells (MUSCL-EVR, HLLC, Manning, momentum dissipation, q inflow, fr outflow), graph-launched
+    steps timed with CUDA events on the library's stream."""
+    import torch
+
+    case = pkg.workloads.dip_channel(n_cells=args.dip_cells, t_max=1.0e9)
+    model = pkg.SpModel(case, device=local_rank)
+    tune = pkg.tuning.autotune(model, iters=3, device=local_rank, cache_path=None)
+    stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
+    model.step(5)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done = model.step(args.dip_steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    n = case.mesh.cell_nb
+    return {"workload": f"DIP feature channel at {n} cells, MUSCL-EVR + DIP HLLC, Manning, momentum dissipation, "
+                        f"q inflow, fr outflow", "metric": "DIP cell-updates/s", "value": n * done / (ms / 1e3),
+            "unit": "cell-updates/s", "steps": done, "ms_per_step": ms / done, "launch_config": tune["report"]}
+
+
 def run_adjoint_only(args, local_rank):
     import torch
 
@@ -384,6 +410,7 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     adjoint = None if (args.no_adjoint or world > 1) else run_adjoint(pkg, args, local_rank)
+    dip = None if (args.dip_cells <= 0 or world > 1) else run_dip(pkg, args, local_rank)
 
     steps = args.steps
     value = n * steps * world / (ms / 1e3)
@@ -420,6 +447,8 @@ def run_ours(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if dip is not None:
+        line["dip"] = dip
     print(json.dumps(line))
 
 

@@ -27,8 +27,9 @@ def _device_name(device: int) -> str:
 def _key(model, device: int) -> str:
     o = model.case.opts
     bucket = int(math.log2(max(1, model.n)))
-    return "|".join([_device_name(device), str(o.get("num_scheme", "godunov")), str(o.get("topo_discretization", "discontinuous")),
-                     str(o.get("model_friction", "none")), str(o.get("model_singular_head_loss", "none")), f"2^{bucket}"])
+    return "|".join([_device_name(device), str(o.get("model_hyperb", "sp")), str(o.get("num_scheme", "godunov")),
+                     str(o.get("topo_discretization", "discontinuous")), str(o.get("model_friction", "none")),
+                     str(o.get("model_singular_head_loss", "none")), f"2^{bucket}"])
 
 
 def _load(path: str) -> Dict[str, dict]:
