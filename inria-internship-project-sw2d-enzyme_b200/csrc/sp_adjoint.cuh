@@ -467,13 +467,30 @@ struct UpdateParams {
     double hs, hk1, hk2, hcos, hsin;     // head loss
 };
 
-SW2D_HD void friction_factor_rev(int model, double k, double h, double un, double dt, double f_bar, double& k_bar,
-                                 double& h_bar, double& un_bar)
+// friction_factor (sp_math.cuh) with P = exp(-4/3 log h) given: the same operations, hence the
+// same value, for a cell whose two directions share P
+SW2D_HD double friction_factor_p(int model, double k, double h, double un, double dt, double P)
+{
+    double factor = 1.0;
+    if (model == 1) {
+        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k / h * dt);
+        else factor = 0.0;
+    } else if (model == 2) {
+        if (h > kSmallReal) factor = sw2d_exp(-kGravity * un * k * k * P * dt);
+        else factor = 0.0;
+    } else {
+        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k * P * dt);
+        else factor = 0.0;
+    }
+    return factor;
+}
+
+// Reverse of friction_factor: f is the forward factor, P = exp(-4/3 log h) (Manning, Strickler)
+SW2D_HD void friction_factor_rev(int model, double k, double h, double un, double dt, double P, double f,
+                                 double f_bar, double& k_bar, double& h_bar, double& un_bar)
 {
     if (model == 1) {
         if ((h > kSmallReal) && (k > kSmallReal)) {
-            const double A = -kGravity * un / k / k / h;
-            const double f = sw2d_exp(A * dt);
             const double A_bar = f_bar * f * dt;
             un_bar += A_bar * (-kGravity / k / k / h);
             k_bar += A_bar * 2.0 * kGravity * un / (k * k * k) / h;
@@ -481,9 +498,6 @@ SW2D_HD void friction_factor_rev(int model, double k, double h, double un, doubl
         }
     } else if (model == 2) {
         if (h > kSmallReal) {
-            const double P = sw2d_exp(-4.0 / 3.0 * sw2d_log(h));
-            const double A = -kGravity * un * k * k * P;
-            const double f = sw2d_exp(A * dt);
             const double A_bar = f_bar * f * dt;
             un_bar += A_bar * (-kGravity * k * k * P);
             k_bar += A_bar * (-kGravity * un * 2.0 * k * P);
@@ -491,9 +505,6 @@ SW2D_HD void friction_factor_rev(int model, double k, double h, double un, doubl
         }
     } else {
         if ((h > kSmallReal) && (k > kSmallReal)) {
-            const double P = sw2d_exp(-4.0 / 3.0 * sw2d_log(h));
-            const double A = -kGravity * un / k / k * P;
-            const double f = sw2d_exp(A * dt);
             const double A_bar = f_bar * f * dt;
             un_bar += A_bar * (-kGravity / k / k * P);
             k_bar += A_bar * 2.0 * kGravity * un / (k * k * k) * P;
@@ -518,7 +529,7 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
     // friction
     const double h_f = hh, q_f = qq, r_f = rr;   // inputs of the friction stage
     bool fr_wet = false;
-    double u = 0, v = 0, ul0 = 0, vl0 = 0, un = 0, f1 = 1, f2 = 1;
+    double u = 0, v = 0, ul0 = 0, vl0 = 0, un = 0, f1 = 1, f2 = 1, P = 0;
     if (p.friction != 0) {
         if (hh > hthr) {
             fr_wet = true;
@@ -527,8 +538,9 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
             ul0 = u * p.fcos + v * p.fsin;
             vl0 = -u * p.fsin + v * p.fcos;
             un = sqrt(u * u + v * v);
-            f1 = friction_factor(p.friction, p.k1, hh, un, p.dt);
-            f2 = friction_factor(p.friction, p.k2, hh, un, p.dt);
+            if (p.friction != 1 && hh > kSmallReal) P = sw2d_exp(-4.0 / 3.0 * sw2d_log(hh));
+            f1 = friction_factor_p(p.friction, p.k1, hh, un, p.dt, P);
+            f2 = friction_factor_p(p.friction, p.k2, hh, un, p.dt, P);
             const double ul = ul0 * f1, vl = vl0 * f2;
             qq = (ul * p.fcos - vl * p.fsin) * hh;
             rr = (ul * p.fsin + vl * p.fcos) * hh;
@@ -635,8 +647,8 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
             double ul0_bar = ul_bar * f1, vl0_bar = vl_bar * f2;
             const double f1_bar = ul_bar * ul0, f2_bar = vl_bar * vl0;
             double un_bar = 0.0;
-            friction_factor_rev(p.friction, p.k1, h_f, un, p.dt, f1_bar, k1b, h_bar, un_bar);
-            friction_factor_rev(p.friction, p.k2, h_f, un, p.dt, f2_bar, k2b, h_bar, un_bar);
+            friction_factor_rev(p.friction, p.k1, h_f, un, p.dt, P, f1, f1_bar, k1b, h_bar, un_bar);
+            friction_factor_rev(p.friction, p.k2, h_f, un, p.dt, P, f2, f2_bar, k2b, h_bar, un_bar);
             double u_bar = ul0_bar * p.fcos - vl0_bar * p.fsin;
             double v_bar = ul0_bar * p.fsin + vl0_bar * p.fcos;
             if (un > 0.0) {
