@@ -166,6 +166,14 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.dev)], stdout=self.fh, stderr=subprocess.DEVNULL)
+            # nvidia-smi's own start-up (NVML initialisation) must not fall inside the timed
+            # region: wait for its first sample (at most 10 s), then a little more
+            t0 = time.time()
+            while time.time() - t0 < 10.0 and self.proc.poll() is None:
+                self.fh.flush()
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.05)
             time.sleep(0.3)
         return self
 

@@ -48,7 +48,7 @@ SW2D_HD SideState godunov_side_dip(double h, double q, double r, double zb, doub
 // One side of swDip::hypMusclEvrComputeLRStates (dip/swDipHypMusclEvr.cpp:170-272): the SP
 // reconstruction (evr_side) with the DIP wave speeds
 SW2D_HD SideState evr_side_dip(bool left, double h, double q, double r, double zb, double b, double x, double zc,
-                               double sx, double sy, double cx, double cy, double mx, double my, double nx, double ny,
+                               double sx, double sy, double dmx, double dmy, double nx, double ny,
                                double dt)
 {
     const double ql = q * nx + r * ny;
@@ -60,13 +60,13 @@ SW2D_HD SideState evr_side_dip(bool left, double h, double q, double r, double z
     const double lmv = lam_minus_dip(b, x, cl, ul);
     const double lpv = lam_plus_dip(b, x, cl, ul);
     double l1 = left ? smax(0.0, lmv) : smin(0.0, lmv);
-    double dx1 = mx - cx - 0.5 * l1 * dt * nx;
-    double dy1 = my - cy - 0.5 * l1 * dt * ny;
+    double dx1 = dmx - 0.5 * l1 * dt * nx;
+    double dy1 = dmy - 0.5 * l1 * dt * ny;
     double z1 = zc + dx1 * sx + dy1 * sy;
     double h1 = smax(0.0, z1 - zb);
     double l2 = left ? smax(0.0, lpv) : smin(0.0, lpv);
-    double dx2 = mx - cx - 0.5 * l2 * dt * nx;
-    double dy2 = my - cy - 0.5 * l2 * dt * ny;
+    double dx2 = dmx - 0.5 * l2 * dt * nx;
+    double dy2 = dmy - 0.5 * l2 * dt * ny;
     double z2 = zc + dx2 * sx + dy2 * sy;
     double h2 = smax(0.0, z2 - zb);
     SideState s;

@@ -55,7 +55,7 @@ SW2D_HD void godunov_side_rev(double h, double q, double r, double b, double nx,
 
 // ---- evr_side (swSpHypMusclEvr.cpp:176-272).  zc = h + z_b of the cell, (sx, sy) its slopes.
 SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, double b, double zc, double sx,
-                          double sy, double cx, double cy, double mx, double my, double nx, double ny, double dt,
+                          double sy, double dmx, double dmy, double nx, double ny, double dt,
                           const SideBar& sb, CellBar& cb)
 {
     // forward recomputation
@@ -70,12 +70,12 @@ SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, do
     const double lmv = b * ul - root1;
     const double lpv = b * ul + root1;
     const double l1 = left ? smax(0.0, lmv) : smin(0.0, lmv);
-    const double dx1 = mx - cx - 0.5 * l1 * dt * nx;
-    const double dy1 = my - cy - 0.5 * l1 * dt * ny;
+    const double dx1 = dmx - 0.5 * l1 * dt * nx;
+    const double dy1 = dmy - 0.5 * l1 * dt * ny;
     const double z1 = zc + dx1 * sx + dy1 * sy;
     const double l2 = left ? smax(0.0, lpv) : smin(0.0, lpv);
-    const double dx2 = mx - cx - 0.5 * l2 * dt * nx;
-    const double dy2 = my - cy - 0.5 * l2 * dt * ny;
+    const double dx2 = dmx - 0.5 * l2 * dt * nx;
+    const double dy2 = dmy - 0.5 * l2 * dt * ny;
     const double z2 = zc + dx2 * sx + dy2 * sy;
     const double h1 = smax(0.0, z1 - zb);
     const double h2 = smax(0.0, z2 - zb);

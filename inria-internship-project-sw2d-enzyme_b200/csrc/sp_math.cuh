@@ -118,9 +118,10 @@ SW2D_HD SideState godunov_side(double h, double q, double r, double zb, double b
 // One side of swSp::hypMusclEvrComputeLRStates (swSpHypMusclEvr.cpp:176-272): EVR half-step
 // reconstruction at the edge midpoint with the limited free-surface slope (sx, sy) of the
 // cell.  `left` selects max(0,.) (L side) or min(0,.) (R side) for the wave speeds; dt is the
-// previous step's time step.
+// previous step's time step; (dmx, dmy) = edge midpoint - cell centroid, the first difference the
+// reference evaluates in `mx - cx - 0.5 * l * dt * nx` (a static of the mesh).
 SW2D_HD SideState evr_side(bool left, double h, double q, double r, double zb, double b, double zc,
-                                              double sx, double sy, double cx, double cy, double mx, double my,
+                                              double sx, double sy, double dmx, double dmy,
                                               double nx, double ny, double dt, const DryConsts& k)
 {
     const double ql = q * nx + r * ny;
@@ -141,13 +142,13 @@ SW2D_HD SideState evr_side(bool left, double h, double q, double r, double zb, d
     const double lmv = b * ul - root1;
     const double lpv = b * ul + root1;
     double l1 = left ? smax(0.0, lmv) : smin(0.0, lmv);
-    double dx1 = mx - cx - 0.5 * l1 * dt * nx;
-    double dy1 = my - cy - 0.5 * l1 * dt * ny;
+    double dx1 = dmx - 0.5 * l1 * dt * nx;
+    double dy1 = dmy - 0.5 * l1 * dt * ny;
     double z1 = zc + dx1 * sx + dy1 * sy;
     double h1 = smax(0.0, z1 - zb);
     double l2 = left ? smax(0.0, lpv) : smin(0.0, lpv);
-    double dx2 = mx - cx - 0.5 * l2 * dt * nx;
-    double dy2 = my - cy - 0.5 * l2 * dt * ny;
+    double dx2 = dmx - 0.5 * l2 * dt * nx;
+    double dy2 = dmy - 0.5 * l2 * dt * ny;
     double z2 = zc + dx2 * sx + dy2 * sy;
     double h2 = smax(0.0, z2 - zb);
     SideState s;

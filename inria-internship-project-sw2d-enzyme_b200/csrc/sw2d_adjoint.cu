@@ -325,21 +325,15 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig
         const double2 n = ld(&m.nxy[e]);
         const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
         const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
-        double2 mp = make_double2(0.0, 0.0), xa = mp, xb = mp, ga = mp, gb = mp;
         SideState SL, SR;
         if (kScheme == SW2D_SCHEME_GODUNOV) {
             SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
             SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
         } else {
-            mp = ld(&m.mxy[e]);
-            xa = ld(&m.cxy[a]);
-            xb = ld(&m.cxy[b]);
-            ga = m.slope[a];
-            gb = m.slope[b];
-            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y, dtp,
-                          m.dry);
-            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y, dtp,
-                          m.dry);
+            const double4 d = ld(&m.emc[e]);
+            const double2 ga = m.slope[a], gb = m.slope[b];
+            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp, m.dry);
+            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp, m.dry);
         }
         const int2 sl = ld(&m.eslot[e]);
         const double hL = SL.z - ca.x, hR = SR.z - cb.x;
@@ -459,11 +453,8 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
     }
     const double4 s = m.st[c];
     const double4 cs = ld(&m.cst[c]);
-    double2 xy = make_double2(0.0, 0.0), g = xy;
-    if (kMuscl) {
-        xy = ld(&m.cxy[c]);
-        g = m.slope[c];
-    }
+    double2 g = make_double2(0.0, 0.0);
+    if (kMuscl) g = m.slope[c];
     for (int i = 0; i < e1 - e0; i++) {
         const int k = k0 + nbnd + i;
         const double4 a = ctb[k];
@@ -475,8 +466,9 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
         const SideBar sb{a.x, a.y, a.z, a.w, b.x};
         CellBar cb{0, 0, 0, 0, 0, 0, 0};
         if (kMuscl) {
-            const double2 mp = ld(&m.mxy[e]);
-            evr_side_rev((en.x & 1) == 0, s.x, s.y, s.z, cs.x, cs.y, s.w, g.x, g.y, xy.x, xy.y, mp.x, mp.y, n.x, n.y,
+            const bool left = (en.x & 1) == 0;
+            const double4 d = ld(&m.emc[e]);
+            evr_side_rev(left, s.x, s.y, s.z, cs.x, cs.y, s.w, g.x, g.y, left ? d.x : d.z, left ? d.y : d.w, n.x, n.y,
                          dtp, sb, cb);
         } else {
             godunov_side_rev(s.x, s.y, s.z, cs.y, n.x, n.y, sb, cb);

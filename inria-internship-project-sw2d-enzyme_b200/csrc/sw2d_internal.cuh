@@ -57,6 +57,7 @@ struct DevMesh {
     const int2* eslot;       // {slot of (L, e), slot of (R, e)}
     const double2* nxy;
     const double2* mxy;
+    const double4* emc;      // {mx - cx_L, my - cy_L, mx - cx_R, my - cy_R}
     const double* len;
     const double2* coef;     // {coefL, coefR}
     double2* flux;           // optional copy: 3 x double2 per edge {F1,F2},{F3,S2L},{S2R,-} (tests)

@@ -181,19 +181,14 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
             }
         } else {
             const double dtp = m.ctrl->dt;
-            const double2 mp = ld(&m.mxy[e]);
-            const double2 xa = ld(&m.cxy[a]), xb = ld(&m.cxy[b]);
+            const double4 d = ld(&m.emc[e]);  // midpoint - centroid of L and R
             const double2 ga = ld(&m.slope[a]), gb = ld(&m.slope[b]);
             if (kDip) {
-                SL = evr_side_dip(true, sa.x, sa.y, sa.z, ca.x, ca.y, xL, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x,
-                                  n.y, dtp);
-                SR = evr_side_dip(false, sb.x, sb.y, sb.z, cb.x, cb.y, xR, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x,
-                                  n.y, dtp);
+                SL = evr_side_dip(true, sa.x, sa.y, sa.z, ca.x, ca.y, xL, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp);
+                SR = evr_side_dip(false, sb.x, sb.y, sb.z, cb.x, cb.y, xR, sb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp);
             } else {
-                SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, xa.x, xa.y, mp.x, mp.y, n.x, n.y,
-                              dtp, m.dry);
-                SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, xb.x, xb.y, mp.x, mp.y, n.x, n.y,
-                              dtp, m.dry);
+                SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp, m.dry);
+                SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp, m.dry);
             }
         }
         const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
@@ -956,6 +951,13 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
         mxy[i] = make_double2(mesh->edge_int_mx[oe], mesh->edge_int_my[oe]);
         len[i] = mesh->edge_int_length[oe];
     }
+    // per internal edge, midpoint - centroid of L and R: the first difference of the MUSCL-EVR
+    // reconstruction (swSpHypMusclEvr.cpp:197-207), a static of the mesh computed once
+    std::vector<double4> emc(ni);
+    for (int64_t i = 0; i < ni; i++) {
+        const double2 a = cxy[lr[i].x], b = cxy[lr[i].y], mp = mxy[i];
+        emc[i] = make_double4(mp.x - a.x, mp.y - a.y, mp.x - b.x, mp.y - b.y);
+    }
     std::vector<int> bcell(nb), bbc(nb);
     std::vector<double4> bgeo(nb);
     for (int64_t i = 0; i < nb; i++) {
@@ -1017,6 +1019,7 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     UP(lr, m.lr);
     UP(nxy, m.nxy);
     UP(mxy, m.mxy);
+    UP(emc, m.emc);
     UP(len, m.len);
     UP(bcell, m.bcell);
     UP(bbc, m.bbc);

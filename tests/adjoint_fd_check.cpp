@@ -105,12 +105,12 @@ int main()
             const double zb = U(-0.5, 0.5), h = (it % 5 == 0) ? U(0.001, 0.05) : U(0.05, 2.0);
             Vec x{h, U(-2, 2), U(-2, 2), zb, h + zb + U(-0.05, 0.05), U(-0.5, 0.5), U(-0.5, 0.5)};
             auto f = [&](const Vec& x) {
-                SideState S = evr_side(left, x[0], x[1], x[2], x[3], b, x[4], x[5], x[6], cx, cy, mx, my, nx, ny, dt, dry);
+                SideState S = evr_side(left, x[0], x[1], x[2], x[3], b, x[4], x[5], x[6], mx - cx, my - cy, nx, ny, dt, dry);
                 return Vec{S.z, S.q, S.r, S.lm, S.lp};
             };
             auto r = [&](const Vec& x, const Vec& w) {
                 CellBar cb{0, 0, 0, 0, 0, 0, 0};
-                evr_side_rev(left, x[0], x[1], x[2], x[3], b, x[4], x[5], x[6], cx, cy, mx, my, nx, ny, dt,
+                evr_side_rev(left, x[0], x[1], x[2], x[3], b, x[4], x[5], x[6], mx - cx, my - cy, nx, ny, dt,
                              SideBar{w[0], w[1], w[2], w[3], w[4]}, cb);
                 return Vec{cb.h, cb.q, cb.r, cb.zb, cb.zc, cb.sx, cb.sy};
             };
