@@ -57,6 +57,9 @@ def _args():
     ap.add_argument("--adjoint-every", type=int, default=100, help="checkpoint interval of the adjoint")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--dip-cells", type=int, default=4_000_000, help="cells of the DIP forward line (0: skip)")
+    ap.add_argument("--ensemble-members", type=int, default=256, help="members of the ensemble line (0: skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--ensemble-every", type=int, default=50, help="checkpoint interval of the ensemble adjoints")
     ap.add_argument("--dip-steps", type=int, default=200)
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint measurement (one JSON line), e.g. for profiling")
@@ -282,6 +285,7 @@ def run_adjoint(pkg, args, local_rank):
         "device_memory_gb": (free0 - free1) / 1e9,
         "gpu_launches_per_gradient": done * kinds,
         "check": "gradient vs central differences and bitwise checkpoint invariance: tests/test_gpu_adjoint.py",
+        "nonfinite_entries_set_to_zero": int(sum(model.adjoint_nonfinite().values())),
     }
 
 
@@ -307,6 +311,80 @@ def run_dip(pkg, args, local_rank):
     return {"workload": f"DIP feature channel at {n} cells, MUSCL-EVR + DIP HLLC, Manning, momentum dissipation, "
                         f"q inflow, fr outflow", "metric": "DIP cell-updates/s", "value": n * done / (ms / 1e3),
             "unit": "cell-updates/s", "steps": done, "ms_per_step": ms / done, "launch_config": tune["report"]}
+
+
+def run_ensemble(pkg, args, local_rank):
+    """Batched ensemble: `--ensemble-members` independent SP solves, sizes log-uniform in
+    [5k, 200k] cells (seeded), alternately the dam-break and the Gaussian-bump constructions,
+    MUSCL-EVR + HLLC, Manning n perturbed by +-20 % (smooth field, per member).  Forward:
+    `--ensemble-steps` steps of every member as one batch (one graph launch per 32-step chunk,
+    members on concurrent stream branches) against the same members stepped one after another
+    (each with its own graph).  Adjoint: each member records its trajectory and observes 16
+    gauges every 10 steps; the members' gradients run concurrently (batch) and one after
+    another.  Host wall time around synchronous calls (both arms alike)."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(17)
+    M = args.ensemble_members
+    sizes = np.exp(rng.uniform(np.log(5_000), np.log(200_000), M)).astype(int)
+    models = []
+    for i, nc in enumerate(sizes):
+        if i % 2 == 0:
+            case = pkg.workloads.dam_break(n_cells=int(nc), scheme="muscl_evr", seed_mesh=100 + i, seed_phi=300 + i)
+        else:
+            case = pkg.workloads.gaussian_bumps(n_cells=int(nc), seed_mesh=100 + i)
+        m = pkg.SpModel(case, device=local_rank)
+        x, y = case.mesh.cell_x, case.mesh.cell_y
+        f = np.sin(2 * np.pi * (x - x.min()) / (np.ptp(x) or 1.0) + i) * np.cos(np.pi * (y - y.min()) / (np.ptp(y) or 1.0))
+        n1 = m.get_param("friction_1")
+        m.set_param("friction", n1 * (1.0 + 0.2 * f))
+        models.append(m)
+    cells = int(sum(m.n for m in models))
+    batch = pkg.Batch(models)
+    K = args.ensemble_steps
+    batch.step(3)
+    for m in models:
+        m.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done = batch.step(K)
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    done_seq = [m.step(K) for m in models]
+    t_seq = time.perf_counter() - t0
+    if int(np.sum(done)) != M * K or sum(done_seq) != M * K:
+        raise RuntimeError("ensemble: a member stopped early")
+    # adjoints: record, observe, then concurrent vs sequential gradients
+    for m in models:
+        m.record(K, args.ensemble_every)
+        g = np.sort(rng.choice(m.n, size=16, replace=False))
+        st = np.arange(10, K + 1, 10)
+        m.set_observations(g, st, m.replay_sample(g, st) * 1.01)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = batch.adjoint(n_threads=16)
+    t_adj_batch = time.perf_counter() - t0
+    nonfinite = sum(sum(m.adjoint_nonfinite().values()) for m in models)
+    t0 = time.perf_counter()
+    res_seq = [m.adjoint() for m in models]
+    t_adj_seq = time.perf_counter() - t0
+    same = all(a[0] == b[0] and all(np.array_equal(a[1][k], b[1][k]) for k in a[1]) for a, b in zip(res, res_seq))
+    free, total = torch.cuda.mem_get_info(local_rank)
+    batch.close()
+    return {
+        "workload": f"{M} SP members, {int(sizes.min())}-{int(sizes.max())} cells (log-uniform, {cells} in all), "
+                    f"dam break / Gaussian bumps, MUSCL-EVR + HLLC, Manning n +-20 %, {K} steps each",
+        "metric": "ensemble cell-updates/s", "unit": "cell-updates/s",
+        "value": cells * K / t_batch, "sequential_value": cells * K / t_seq, "speedup": t_seq / t_batch,
+        "s_batched": t_batch, "s_sequential": t_seq,
+        "adjoint": {"gradients_per_s": M / t_adj_batch, "sequential_gradients_per_s": M / t_adj_seq,
+                    "speedup": t_adj_seq / t_adj_batch, "s_batched": t_adj_batch, "s_sequential": t_adj_seq,
+                    "checkpoint_every": args.ensemble_every, "bitwise_same_as_sequential": bool(same),
+                    "nonfinite_entries_set_to_zero": int(nonfinite)},
+        "device_memory_in_use_gb": (total - free) / 1e9,
+        "timing": "host wall time around synchronous calls, both arms alike",
+    }
 
 
 def run_adjoint_only(args, local_rank):
@@ -419,6 +497,7 @@ def run_ours(args, rank, world, local_rank):
         return
     adjoint = None if (args.no_adjoint or world > 1) else run_adjoint(pkg, args, local_rank)
     dip = None if (args.dip_cells <= 0 or world > 1) else run_dip(pkg, args, local_rank)
+    ensemble = None if (args.ensemble_members <= 0 or world > 1) else run_ensemble(pkg, args, local_rank)
 
     steps = args.steps
     value = n * steps * world / (ms / 1e3)
@@ -457,6 +536,8 @@ def run_ours(args, rank, world, local_rank):
         line["adjoint"] = adjoint
     if dip is not None:
         line["dip"] = dip
+    if ensemble is not None:
+        line["ensemble"] = ensemble
     print(json.dumps(line))
 
 

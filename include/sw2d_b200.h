@@ -326,6 +326,39 @@ int sw2d_replay_sample(sw2d_handle* h, int64_t n_points, const int64_t* cells, i
  * as sw2d_replay_cost, bit for bit.  Leaves the model at the end of the trajectory. */
 int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad);
 
+/* Gradient entries that came out NaN or infinite in the last sw2d_adjoint and were set to 0,
+ * per control: counts[6] = {h0, q0, r0, z_b, friction_1, friction_2}.  The reference cleans its
+ * gradient the same way (assim/swSpE_checkpoint.cpp:1196-1207): near-dry cells carry the
+ * 1/max(h, 1e-16) factors of the wave speeds and velocities, and over long windows their
+ * adjoint can overflow. */
+int sw2d_adjoint_nonfinite(sw2d_handle* h, int64_t* counts);
+
+/* ---- Ensembles ---------------------------------------------------------------------------------
+ * The reference runs one simulation per process; its assimilation evaluates line-search trial
+ * points and perturbed members one after another (assim/swSpE_minimize.cpp:749-840).  A batch
+ * advances M independent member handles (created as usual, any sizes, models and options, on one
+ * device) together: one CUDA graph holds every member's step kernels on its own stream branch,
+ * so one launch advances the whole ensemble and small members run side by side.  Each member
+ * keeps its own CFL time steps, t_max and status; its results are bit for bit those of the
+ * member run alone.  The batch captures the members' options and launch variants when it first
+ * steps; change them before that. */
+typedef struct sw2d_batch sw2d_batch;
+
+int sw2d_batch_create(sw2d_handle* const* members, int n_members, sw2d_batch** out);
+
+/* At most n_steps steps of every member (each stops at its own t_max); steps_done[i] (may be
+ * NULL) receives member i's count.  Returns the first member error, if any
+ * (sw2d_batch_last_error names the member). */
+int sw2d_batch_step_n(sw2d_batch* b, int64_t n_steps, int64_t* steps_done);
+
+/* sw2d_adjoint of every member (each with its recorded trajectory and observations), run
+ * concurrently from n_threads host threads (<= 0: 16): J[i] and grads[i] (grads may be NULL). */
+int sw2d_batch_adjoint(sw2d_batch* b, double* J, const sw2d_gradient* grads, int n_threads);
+
+int sw2d_batch_size(sw2d_batch* b);
+int sw2d_batch_destroy(sw2d_batch* b);   /* the member handles stay valid */
+const char* sw2d_batch_last_error(sw2d_batch* b);
+
 /* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
 int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
 

@@ -249,6 +249,21 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_replay_sample.restype = ctypes.c_int
     lib.sw2d_adjoint.argtypes = [P, c_double_p, ctypes.POINTER(Sw2dGradient)]
     lib.sw2d_adjoint.restype = ctypes.c_int
+    lib.sw2d_adjoint_nonfinite.argtypes = [P, c_int64_p]
+    lib.sw2d_adjoint_nonfinite.restype = ctypes.c_int
+    # ensembles
+    lib.sw2d_batch_create.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P)]
+    lib.sw2d_batch_create.restype = ctypes.c_int
+    lib.sw2d_batch_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
+    lib.sw2d_batch_step_n.restype = ctypes.c_int
+    lib.sw2d_batch_adjoint.argtypes = [P, c_double_p, ctypes.POINTER(Sw2dGradient), ctypes.c_int]
+    lib.sw2d_batch_adjoint.restype = ctypes.c_int
+    lib.sw2d_batch_size.argtypes = [P]
+    lib.sw2d_batch_size.restype = ctypes.c_int
+    lib.sw2d_batch_destroy.argtypes = [P]
+    lib.sw2d_batch_destroy.restype = ctypes.c_int
+    lib.sw2d_batch_last_error.argtypes = [P]
+    lib.sw2d_batch_last_error.restype = ctypes.c_char_p
     _LIB = lib
     return lib
 
@@ -261,4 +276,6 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_step_n", "sw2d_execute", "sw
             "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_get_launch_config",
             "sw2d_set_launch_config", "sw2d_get_array_noalloc", "sw2d_record", "sw2d_rerecord", "sw2d_trajectory_info",
             "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
-            "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint"]
+            "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint", "sw2d_adjoint_nonfinite",
+            "sw2d_batch_create", "sw2d_batch_step_n", "sw2d_batch_adjoint", "sw2d_batch_size",
+            "sw2d_batch_destroy", "sw2d_batch_last_error"]

@@ -82,6 +82,8 @@ struct AdjointState {
     double* d_Jobs = nullptr;            // n_obs: cost of each observation
     double* d_part = nullptr;
     double* stage = nullptr;             // nc doubles for parameter transfers
+    unsigned long long* d_nonfinite = nullptr;  // 6 counters of the last gradient's clean-up
+    int64_t nonfinite[6] = {0, 0, 0, 0, 0, 0};
     // observations
     int64_t n_pts = 0, n_obs = 0;
     int normalize = 0;
@@ -531,6 +533,35 @@ __global__ void __launch_bounds__(kBlock) k_nbr_rev(DevMesh m, const int* __rest
     gzb[c] += s;
 }
 
+// Non-finite gradient entries -> 0, counted per control (h0, q0, r0, z_b, friction_1,
+// friction_2): the reference's final clean-up of its gradient (assim/swSpE_checkpoint.cpp:
+// 1196-1207).  Near-dry cells carry the 1/max(h, 1e-16) factors of the wave speeds and
+// velocities; over long windows their adjoint can overflow, in the reference as here.
+__device__ __forceinline__ void clean(double& v, unsigned long long* count)
+{
+    if (!isfinite(v)) {
+        v = 0.0;
+        atomicAdd(count, 1ull);
+    }
+}
+
+__global__ void k_sanitize(double4* lam, double* gzb, double* gk1, double* gk2, unsigned long long* counts, int n,
+                           int with_friction)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double4 l = lam[c];
+    clean(l.x, counts + 0);
+    clean(l.y, counts + 1);
+    clean(l.z, counts + 2);
+    lam[c] = l;
+    clean(gzb[c], counts + 3);
+    if (with_friction) {
+        clean(gk1[c], counts + 4);
+        clean(gk2[c], counts + 5);
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------------
@@ -570,7 +601,7 @@ int adjoint_fixed(sw2d_handle* h)
         (rc = adj_alloc(h, L, h->nc, &a->g_zb)) || (rc = adj_alloc(h, L, h->nc, &a->g_k1)) ||
         (rc = adj_alloc(h, L, h->nc, &a->g_k2)) || (rc = adj_alloc(h, L, 1, &a->ctrl_rev)) ||
         (rc = adj_alloc(h, L, kCostBlocks, &a->d_part)) ||
-        (rc = adj_alloc(h, L, h->nc, &a->stage)))
+        (rc = adj_alloc(h, L, h->nc, &a->stage)) || (rc = adj_alloc(h, L, 6, &a->d_nonfinite)))
         return rc;
     Ctrl cr{};
     cr.t = 0.0;
@@ -854,7 +885,14 @@ int reverse_sweep(sw2d_handle* h)
         k_obs_rev<<<grid_for(a->n_pts), kBlock, 0, h->stream>>>(obs_view(a, k0), a->ck_st, a->lam);
         cost_at(h, k0, a->ck_st);
     }
+    CK(cudaMemsetAsync(a->d_nonfinite, 0, 6 * sizeof(unsigned long long), h->stream));
+    k_sanitize<<<gc, kBlock, 0, h->stream>>>(a->lam, a->g_zb, a->g_k1, a->g_k2, a->d_nonfinite, (int)nc,
+                                              h->p.friction != SW2D_FRICTION_NONE);
+    unsigned long long cnt[6];
+    CK(cudaMemcpyAsync(cnt, a->d_nonfinite, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
     if ((rc = ck_load(h, a->n_ck))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < 6; k++) a->nonfinite[k] = (int64_t)cnt[k];
     CK(cudaGetLastError());
     return SW2D_OK;
 }
@@ -1235,6 +1273,14 @@ int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad)
             if (grad->friction_2) std::memset(grad->friction_2, 0, h->nc * sizeof(double));
         }
     }
+    return SW2D_OK;
+}
+
+int sw2d_adjoint_nonfinite(sw2d_handle* h, int64_t* counts)
+{
+    if (!h || !counts) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (!h->adj) return fail(h, SW2D_E_ARG, "no gradient computed yet");
+    for (int k = 0; k < 6; k++) counts[k] = h->adj->nonfinite[k];
     return SW2D_OK;
 }
 

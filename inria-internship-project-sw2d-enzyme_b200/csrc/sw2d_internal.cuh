@@ -180,6 +180,8 @@ void launch_edges_on(sw2d_handle* h, const DevMesh& m);
 void launch_cfl_on(sw2d_handle* h, const DevMesh& m);
 // The update kernel; with store_balance it also writes the post-balance state to m.bal.
 void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance);
+// One whole time step of the handle (its four kernels, its launch variants) on its stream.
+void launch_step_on(sw2d_handle* h);
 
 // Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
 void adjoint_release(sw2d_handle* h);

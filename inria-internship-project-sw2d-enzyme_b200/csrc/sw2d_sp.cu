@@ -695,6 +695,8 @@ void launch_edges_on(sw2d_handle* h, const DevMesh& m) { launch_edges(h, m, h->e
 
 void launch_cfl_on(sw2d_handle* h, const DevMesh& m) { k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
 
+void launch_step_on(sw2d_handle* h) { launch_step(h); }
+
 void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance)
 {
     if (store_balance) launch_update_s<true>(h, m);

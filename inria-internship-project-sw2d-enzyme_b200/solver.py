@@ -244,6 +244,12 @@ class SpModel:
         self._check(self.lib.sw2d_adjoint(self.handle, ctypes.byref(J), ctypes.byref(g)))
         return J.value, out
 
+    def adjoint_nonfinite(self) -> dict:
+        """Entries of the last gradient that were NaN or infinite and were set to 0, per control."""
+        c = np.zeros(6, dtype=np.int64)
+        self._check(self.lib.sw2d_adjoint_nonfinite(self.handle, c.ctypes.data_as(capi.c_int64_p)))
+        return dict(zip(self.GRADIENTS, (int(v) for v in c)))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self.lib.sw2d_destroy(self.handle)

@@ -256,6 +256,29 @@ def test_taylor_ratio_tends_to_one(pkg):
     assert errs[2] < errs[0]
 
 
+def test_long_window_over_dry_islands_gives_a_finite_gradient(pkg):
+    """500 steps over a bed with dry islands: near-dry cells carry the 1/max(h, 1e-16) factors
+    of the wave speeds and velocities, and their adjoint can overflow (the reference sees the
+    same and zeroes non-finite gradient entries, assim/swSpE_checkpoint.cpp:1196-1207).  The
+    gradient handed back is finite, the count of zeroed entries is reported, and both are the
+    same on a second sweep."""
+    case = pkg.workloads.gaussian_bumps(n_cells=14000, seed_mesh=137)
+    model = pkg.SpModel(case)
+    model.record(500, 50)
+    rng = np.random.default_rng(2)
+    cells = np.sort(rng.choice(model.n, size=16, replace=False))
+    steps = np.arange(10, 501, 10)
+    model.set_observations(cells, steps, model.replay_sample(cells, steps) * 1.01)
+    J, g = model.adjoint()
+    counts = model.adjoint_nonfinite()
+    assert np.isfinite(J) and all(np.isfinite(v).all() for v in g.values())
+    assert set(counts) == set(g) and all(c >= 0 for c in counts.values())
+    J2, g2 = model.adjoint()
+    assert J2 == J and model.adjoint_nonfinite() == counts
+    for k in g:
+        assert np.array_equal(g[k].view(np.int64), g2[k].view(np.int64)), k
+
+
 def test_adjoint_errors(pkg):
     case = _case(pkg, CASES["dam_godunov"])
     model = pkg.SpModel(case)
