@@ -1,5 +1,5 @@
 /*
- * portable_math.h — exp and log that give the same bits on the GPU and on the host.
+ * portable_math.h — exp, log and cbrt that give the same bits on the GPU and on the host.
  *
  * The SP step calls exp and log in the friction factors, the singular head loss and the
  * critical depth of 'q' boundaries.  CUDA's and the host libm's versions differ in the last
@@ -17,8 +17,9 @@
  *  - log: x = m 2^e with m in [sqrt(1/2), sqrt(2)); log m = 2 atanh(s), s = (m-1)/(m+1),
  *    |s| <= 0.1716, by the odd series 2(s + s^3/3 + ... + s^23/23) (truncation < 2^-56);
  *    log x = e ln2_hi + (e ln2_lo + log m).
- * Accuracy: within 2 ulp of the true value over the argument ranges the step uses (checked
- * against the host libm by tests/test_portable_math.py and against CUDA's exp/log on the GPU).
+ * Accuracy: exp and log within 2 ulp of the true value over the argument ranges the step uses,
+ * cbrt within 1 ulp (checked against the host libm by tests/test_portable_math.py and against
+ * CUDA's exp/log/cbrt on the GPU).
  *
  * Constants: 1/n! and 1/(2n+1) are the binary64 values nearest the exact rationals; ln2,
  * 1/ln2 and sqrt(2) are the nearest binary64 values of the real numbers.
@@ -133,6 +134,40 @@ SW2D_PM_FN double sw2d_log(double x)
     double lm = s2 + s2 * t;
     double ed = (double)e;
     return ed * kLn2Hi + (ed * kLn2Lo + lm);
+}
+
+/*
+ * cbrt (the Strickler friction of the differentiated step takes h^(4/3) = h cbrt(h)):
+ * |x| = m 2^e with m in [1, 2); e = 3k + j, j in {0, 1, 2}; t = m 2^j in [1, 8) (exact);
+ * cbrt|x| = 2^k cbrt(t).  A first guess (3/4 + m/4) c_j, within 2 % of cbrt(t), is refined by
+ * five steps of Newton's iteration for y^3 = t, y <- y - (y^3 - t) / (3 y^2) (quadratic
+ * convergence: 2e-2, 4e-4, 2e-7, 3e-14, then rounding level); the sign of x is restored.
+ * The c_j are rough guesses of 2^(j/3); their error only changes the starting point.
+ */
+SW2D_PM_FN double sw2d_cbrt(double x)
+{
+    if (x != x || x == 0.0) return x;                                 /* NaN, +-0 */
+    uint64_t b = sw2d_pm_bits(x);
+    const uint64_t sign = b & 0x8000000000000000ULL;
+    b &= 0x7fffffffffffffffULL;
+    if ((b >> 52) == 0x7ff) return x;                                 /* +-inf */
+    int e = 0;
+    if ((b >> 52) == 0) {                                             /* subnormal: scale by 2^54 */
+        b = sw2d_pm_bits(sw2d_pm_from_bits(b) * 18014398509481984.0);
+        e = -54;
+    }
+    e += (int)(b >> 52) - 1023;
+    const double m = sw2d_pm_from_bits((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
+    int k = e / 3, j = e - 3 * k;
+    if (j < 0) {
+        j += 3;
+        k -= 1;
+    }
+    const double t = (j == 0) ? m : ((j == 1) ? m * 2.0 : m * 4.0);
+    double y = (0.75 + 0.25 * m) * ((j == 0) ? 1.0 : ((j == 1) ? 1.26 : 1.5874));
+    for (int it = 0; it < 5; it++) y = y - (y * y * y - t) / (3.0 * (y * y));
+    const double r = y * sw2d_pm_pow2(k);
+    return sw2d_pm_from_bits(sw2d_pm_bits(r) | sign);
 }
 
 #endif

@@ -507,7 +507,8 @@ __global__ void k_eval_math(int fn, const double* __restrict__ x, double* y, lon
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double v = x[i];
-    y[i] = fn == 0 ? sw2d_exp(v) : fn == 1 ? sw2d_log(v) : fn == 2 ? exp(v) : log(v);
+    y[i] = fn == 0 ? sw2d_exp(v) : fn == 1 ? sw2d_log(v) : fn == 2 ? exp(v) : fn == 3 ? log(v)
+         : fn == 4 ? sw2d_cbrt(v) : cbrt(v);
 }
 
 
@@ -1536,7 +1537,7 @@ int sw2d_kernels_per_step(sw2d_handle* h)
 int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n)
 {
     sw2d_handle* h = nullptr;
-    if (!x || !y || n < 0 || fn < 0 || fn > 3) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (!x || !y || n < 0 || fn < 0 || fn > 5) return fail(h, SW2D_E_ARG, "invalid arguments");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
         return fail(h, SW2D_E_NO_DEVICE, "no usable CUDA device");

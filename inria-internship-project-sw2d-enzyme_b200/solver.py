@@ -263,10 +263,10 @@ class SpModel:
 
 
 def eval_math(fn: str, x, device: int = 0) -> np.ndarray:
-    """Device evaluation of the step's elementary functions: fn in ("exp", "log") for the
-    portable versions the step uses, ("cuda_exp", "cuda_log") for CUDA's."""
+    """Device evaluation of the step's elementary functions: fn in ("exp", "log", "cbrt") for
+    the portable versions the step uses, ("cuda_exp", "cuda_log", "cuda_cbrt") for CUDA's."""
     lib = capi.load_library()
-    code = {"exp": 0, "log": 1, "cuda_exp": 2, "cuda_log": 3}[fn]
+    code = {"exp": 0, "log": 1, "cuda_exp": 2, "cuda_log": 3, "cbrt": 4, "cuda_cbrt": 5}[fn]
     x = np.ascontiguousarray(x, dtype=np.float64)
     y = np.empty_like(x)
     st = lib.sw2d_eval_math(int(device), code, x.ctypes.data_as(capi.c_double_p), y.ctypes.data_as(capi.c_double_p),

@@ -1,6 +1,6 @@
-"""The portable exp/log of the CUDA build (csrc/portable_math.h): accuracy against the host
-libm, special values, and (GPU) identical bits on the device and the host, within 2 ulp of
-CUDA's own exp/log."""
+"""The portable exp/log/cbrt of the CUDA build (csrc/portable_math.h): accuracy against the host
+libm (cbrt: against the 80-bit long-double cube root), special values, and (GPU) identical bits
+on the device and the host, within a few ulp of CUDA's own functions."""
 import ctypes
 import math
 import os
@@ -20,12 +20,13 @@ def host_pm(tmp_path_factory):
     d = tmp_path_factory.mktemp("pm")
     src = d / "pm.c"
     src.write_text(f'#include "{HDR}"\ndouble pexp(double x) {{ return sw2d_exp(x); }}\n'
-                   'double plog(double x) { return sw2d_log(x); }\n')
+                   'double plog(double x) { return sw2d_log(x); }\n'
+                   'double pcbrt(double x) { return sw2d_cbrt(x); }\n')
     so = d / "libpm.so"
     subprocess.run(["gcc", "-std=c11", "-O2", "-fPIC", "-ffp-contract=off", "-shared", "-o", str(so), str(src)],
                    check=True)
     lib = ctypes.CDLL(str(so))
-    for f in (lib.pexp, lib.plog):
+    for f in (lib.pexp, lib.plog, lib.pcbrt):
         f.argtypes = [ctypes.c_double]
         f.restype = ctypes.c_double
     return lib
@@ -55,6 +56,27 @@ def test_portable_math_accuracy(host_pm):
     assert _ulps(pl, np.log(xl)).max() <= 2.0
 
 
+def _cbrt_samples():
+    rng = np.random.default_rng(6)
+    x = np.concatenate([np.ldexp(rng.uniform(0.5, 1.0, 20000), rng.integers(-1070, 1020, 20000)),
+                        rng.uniform(1e-16, 10.0, 20000), np.logspace(-16, 2, 5000), -rng.uniform(0.0, 5.0, 2000)])
+    return x
+
+
+def test_portable_cbrt_accuracy(host_pm):
+    """Within 1 ulp of the cube root taken in 80-bit long double (the host libm's double cbrt
+    itself is off by up to ~3.5 ulp on these samples)."""
+    x = _cbrt_samples()
+    p = np.array([host_pm.pcbrt(float(v)) for v in x])
+    truth = np.cbrt(x.astype(np.longdouble))
+    err = np.abs(p.astype(np.longdouble) - truth) / np.abs(np.spacing(truth.astype(np.float64))).astype(np.longdouble)
+    assert float(err.max()) <= 1.0
+    for v in (0.0, -0.0, 1.0, 8.0, 27.0, 0.125, -8.0, 1e-300, 5e-324):
+        assert host_pm.pcbrt(v) == v if v == 0.0 else abs(host_pm.pcbrt(v) - math.cbrt(v)) <= 2 * math.ulp(math.cbrt(v))
+    assert host_pm.pcbrt(float("inf")) == float("inf") and math.isnan(host_pm.pcbrt(float("nan")))
+    assert math.copysign(1.0, host_pm.pcbrt(-0.0)) < 0
+
+
 def test_portable_math_special_values(host_pm):
     inf = float("inf")
     assert host_pm.pexp(0.0) == 1.0 and host_pm.pexp(-inf) == 0.0 and host_pm.pexp(inf) == inf
@@ -79,3 +101,7 @@ def test_portable_math_device_matches_host(host_pm):
     cl = pkg.solver.eval_math("cuda_log", xl)
     assert _ulps(de, ce).max() <= 2.0
     assert _ulps(dl, cl).max() <= 2.0
+    dc = pkg.solver.eval_math("cbrt", _cbrt_samples())
+    hc = np.array([host_pm.pcbrt(float(v)) for v in _cbrt_samples()])
+    assert np.array_equal(dc.view(np.int64), hc.view(np.int64))
+    assert _ulps(dc, pkg.solver.eval_math("cuda_cbrt", _cbrt_samples())).max() <= 2.0
