@@ -359,6 +359,98 @@ int sw2d_batch_size(sw2d_batch* b);
 int sw2d_batch_destroy(sw2d_batch* b);   /* the member handles stay valid */
 const char* sw2d_batch_last_error(sw2d_batch* b);
 
+/* ---- Porosity assimilation: the reference's differentiated step and its gradient ---------------
+ * The reference's assimilation engine (class swSpE, assim/swSpE*.cpp) runs its own variant of
+ * the SP step, the "_E" step (assim/swSpE_hyp.cpp, swSpE_muscl.cpp, swSpE_friction.cpp):
+ * desingularised MUSCL velocities, an HLLC with a smooth min of the porosities, every edge's
+ * flux computed each step, semi-implicit Strickler friction.  These calls are its seam
+ * (assim/main_enzyme.cpp:113-264), on any SP handle:
+ *   sw2d_assim_record       swSpE::build_checkpoint_records  (swSpE_checkpoint.cpp:97-455)
+ *   sw2d_assim_replay_cost  swSpE::replay_trajectory_cost    (swSpE_checkpoint.cpp:1311-1427)
+ *   sw2d_assim_gradient     swSpE::get_spatial_gradient_checkpointed (swSpE_checkpoint.cpp:722-1281),
+ *                           which the reference differentiates with Enzyme; here a hand-written
+ *                           reverse sweep.
+ * The control is the per-cell map m, with porosity phi = T(m) (phi_transform, swSpE.h:59-107).
+ * The trajectory starts from the state and time the handle has when sw2d_assim_configure is
+ * called (swSpE::save_initial_state after init) and runs to t_max.  These calls overwrite the
+ * handle's state buffer (it holds the end of the last record or replay). */
+#define SW2D_PHI_NONE 0
+#define SW2D_PHI_CLAMP 1
+#define SW2D_PHI_TANH 2
+#define SW2D_PHI_NORMALIZE 3
+
+#define SW2D_OBS_FRAMES 0   /* full-field (h, qx, qy) maps: compute_cost_frame_ptr (swSpE_ad.cpp:273-308) */
+#define SW2D_OBS_GAUGES 1   /* depths at gauge cells: compute_cost_gauges_ptr (swSpE_gauges.cpp:166-179) */
+
+/* The assimilation keys of input.solv (assim/assimConfig.h:17-55) this path reads. */
+typedef struct sw2d_assim_params {
+    int32_t phi_transform;           /* SW2D_PHI_*                                                */
+    double lambda_tanh;              /* slope of the tanh transform                               */
+    int32_t windowed;                /* windowed_assimilation                                     */
+    double window_duration;          /* assimilation_window_duration (s); <= 0: unused            */
+    int64_t window_steps;            /* assimilation_window_steps; <= 0: unused                   */
+    int64_t n_windows;               /* n_assimilation_windows: tiles of the window (>= 1)        */
+    double t_state_assimilation;     /* fallback start of the window                              */
+    int32_t cost_normalize;          /* divide each observation's cost by the number of frames    */
+    int32_t mask_wall_gradient;      /* zero the gradient where phi <= phi_min                    */
+    int64_t forced_first_segment;    /* forced_first_seg_ of the L-BFGS-B driver; -1: none        */
+} sw2d_assim_params;
+
+typedef struct sw2d_assim_obs {
+    int32_t kind;                    /* SW2D_OBS_FRAMES or SW2D_OBS_GAUGES                        */
+    int32_t n_obs;
+    const double* times;             /* [n_obs], increasing (s)                                   */
+    const double* frames;            /* FRAMES: [n_obs][3][n_cells] h, qx, qy, caller order       */
+    const double* h_weight;          /* FRAMES: [n_cells] weight of dh^2 (NULL: 1)                */
+    const double* q_weight;          /* FRAMES: [n_cells] weight of dqx^2 + dqy^2 (NULL: 1)       */
+    int32_t n_gauges;                /* GAUGES                                                    */
+    const int64_t* gauge_cells;      /* [n_gauges] cell of each gauge (repeats allowed)           */
+    const double* gauge_weight;      /* [n_gauges]                                                */
+    const double* gauge_h;           /* [n_obs][n_gauges] observed depths                         */
+} sw2d_assim_obs;
+
+/* What get_spatial_gradient_checkpointed reports (its diagnostics, swSpE_checkpoint.cpp:1214-1234). */
+typedef struct sw2d_assim_info {
+    double J;                        /* replay cost at m (the cost the gradient belongs to)       */
+    double grad_l2;                  /* ||dJ/dm||_2                                               */
+    double grad_max;                 /* the entry of largest magnitude (signed)                   */
+    int64_t grad_argmax;             /* its cell (caller numbering)                               */
+    double dh_peak;                  /* largest ||adjoint of h||_2 at a segment start             */
+    int64_t n_steps, n_segments;     /* of the recorded trajectory                                */
+    int64_t first_segment;           /* first segment of the window                               */
+    int64_t truncation_segment;      /* the replay starts after it (-1: from the first segment)   */
+    int64_t n_tiles;                 /* tiles of the window (0: one continuous window)            */
+    int64_t exploded_segment;        /* segment where the adjoint blew up (-1: none)              */
+    int64_t n_nonfinite;             /* gradient entries set to 0 because not finite              */
+    int64_t n_masked;                /* entries set to 0 in all (non-finite + walls)              */
+} sw2d_assim_info;
+
+int sw2d_assim_configure(sw2d_handle* h, const sw2d_assim_params* params);
+int sw2d_assim_set_observations(sw2d_handle* h, const sw2d_assim_obs* obs);
+
+/* The dry run at control m (caller numbering): the CFL time steps, snapped onto the observation
+ * times, the boundary values, the observation triggers and a checkpoint every `stride` steps;
+ * then the window and tiles of the gradient.  n_steps / n_segments may be NULL. */
+int sw2d_assim_record(sw2d_handle* h, const double* m, int64_t stride, int64_t* n_steps, int64_t* n_segments);
+
+/* J(m) on the recorded trajectory (frozen time steps, boundary values and triggers), from the
+ * window's first checkpoint, or per tile from each tile's checkpoint. */
+int sw2d_assim_replay_cost(sw2d_handle* h, const double* m, double* J);
+
+/* record at m, then the reverse sweep: dJ/dm (required), and optionally dJ/dK1, dJ/dK2 (the
+ * Strickler coefficients the _E friction reads) and dJ/d(h, qx, qy) at the start of the window
+ * ([3][n_cells]); all in the caller's numbering.  info may be NULL. */
+int sw2d_assim_gradient(sw2d_handle* h, const double* m, int64_t stride, double* dJ_dm, double* dJ_dk1,
+                        double* dJ_dk2, double* dJ_dstate, sw2d_assim_info* info);
+
+/* The recorded trajectory: per segment its start time and step count; per step its dt and
+ * observation trigger (-1 or the observation index).  Capacities in entries. */
+int sw2d_assim_segments(sw2d_handle* h, double* t_start, int64_t* n_steps, int64_t capacity);
+int sw2d_assim_steps(sw2d_handle* h, double* dt, int32_t* obs_trig, int64_t capacity);
+/* Checkpoint k (the state at the start of segment k), caller numbering. */
+int sw2d_assim_checkpoint(sw2d_handle* h, int64_t k, double* water_depth, double* unit_discharge_x,
+                          double* unit_discharge_y);
+
 /* Internal numbering (for tests and tools): perm[new] = caller index, for cells. */
 int sw2d_get_cell_permutation(sw2d_handle* h, int64_t* perm);
 

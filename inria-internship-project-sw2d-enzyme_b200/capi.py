@@ -72,6 +72,27 @@ class Sw2dGradient(ctypes.Structure):
                 ("friction_1", c_double_p), ("friction_2", c_double_p)]
 
 
+class Sw2dAssimParams(ctypes.Structure):
+    _fields_ = [("phi_transform", ctypes.c_int32), ("lambda_tanh", ctypes.c_double), ("windowed", ctypes.c_int32),
+                ("window_duration", ctypes.c_double), ("window_steps", ctypes.c_int64), ("n_windows", ctypes.c_int64),
+                ("t_state_assimilation", ctypes.c_double), ("cost_normalize", ctypes.c_int32),
+                ("mask_wall_gradient", ctypes.c_int32), ("forced_first_segment", ctypes.c_int64)]
+
+
+class Sw2dAssimObs(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("n_obs", ctypes.c_int32), ("times", c_double_p), ("frames", c_double_p),
+                ("h_weight", c_double_p), ("q_weight", c_double_p), ("n_gauges", ctypes.c_int32),
+                ("gauge_cells", c_int64_p), ("gauge_weight", c_double_p), ("gauge_h", c_double_p)]
+
+
+class Sw2dAssimInfo(ctypes.Structure):
+    _fields_ = [("J", ctypes.c_double), ("grad_l2", ctypes.c_double), ("grad_max", ctypes.c_double),
+                ("grad_argmax", ctypes.c_int64), ("dh_peak", ctypes.c_double), ("n_steps", ctypes.c_int64),
+                ("n_segments", ctypes.c_int64), ("first_segment", ctypes.c_int64),
+                ("truncation_segment", ctypes.c_int64), ("n_tiles", ctypes.c_int64),
+                ("exploded_segment", ctypes.c_int64), ("n_nonfinite", ctypes.c_int64), ("n_masked", ctypes.c_int64)]
+
+
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(c_double_p)
 
@@ -264,6 +285,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_batch_destroy.restype = ctypes.c_int
     lib.sw2d_batch_last_error.argtypes = [P]
     lib.sw2d_batch_last_error.restype = ctypes.c_char_p
+    # porosity assimilation (the differentiated step)
+    lib.sw2d_assim_configure.argtypes = [P, ctypes.POINTER(Sw2dAssimParams)]
+    lib.sw2d_assim_configure.restype = ctypes.c_int
+    lib.sw2d_assim_set_observations.argtypes = [P, ctypes.POINTER(Sw2dAssimObs)]
+    lib.sw2d_assim_set_observations.restype = ctypes.c_int
+    lib.sw2d_assim_record.argtypes = [P, c_double_p, ctypes.c_int64, c_int64_p, c_int64_p]
+    lib.sw2d_assim_record.restype = ctypes.c_int
+    lib.sw2d_assim_replay_cost.argtypes = [P, c_double_p, c_double_p]
+    lib.sw2d_assim_replay_cost.restype = ctypes.c_int
+    lib.sw2d_assim_gradient.argtypes = [P, c_double_p, ctypes.c_int64, c_double_p, c_double_p, c_double_p, c_double_p,
+                                        ctypes.POINTER(Sw2dAssimInfo)]
+    lib.sw2d_assim_gradient.restype = ctypes.c_int
+    lib.sw2d_assim_segments.argtypes = [P, c_double_p, c_int64_p, ctypes.c_int64]
+    lib.sw2d_assim_segments.restype = ctypes.c_int
+    lib.sw2d_assim_steps.argtypes = [P, c_double_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_int64]
+    lib.sw2d_assim_steps.restype = ctypes.c_int
+    lib.sw2d_assim_checkpoint.argtypes = [P, ctypes.c_int64, c_double_p, c_double_p, c_double_p]
+    lib.sw2d_assim_checkpoint.restype = ctypes.c_int
     _LIB = lib
     return lib
 
@@ -278,4 +317,6 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_step_n", "sw2d_execute", "sw
             "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
             "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint", "sw2d_adjoint_nonfinite",
             "sw2d_batch_create", "sw2d_batch_step_n", "sw2d_batch_adjoint", "sw2d_batch_size",
-            "sw2d_batch_destroy", "sw2d_batch_last_error"]
+            "sw2d_batch_destroy", "sw2d_batch_last_error", "sw2d_assim_configure", "sw2d_assim_set_observations",
+            "sw2d_assim_record", "sw2d_assim_replay_cost", "sw2d_assim_gradient", "sw2d_assim_segments",
+            "sw2d_assim_steps", "sw2d_assim_checkpoint"]

@@ -63,6 +63,7 @@ struct ObsView {
     const double *hobs, *qobs, *robs;  // this observation's values
     int n;
     double scale;                // 1 or 1 / n_obs
+    int wdh;                     // term (w dh) dh instead of w (dh dh) (the reference's gauge cost)
 };
 
 
@@ -70,7 +71,7 @@ __device__ __forceinline__ double obs_term(const ObsView& o, const double4* st, 
 {
     const double4 s = st[o.pts[i]];
     const double dh = s.x - o.hobs[i];
-    double v = o.wh[i] * (dh * dh);
+    double v = o.wdh ? (o.wh[i] * dh) * dh : o.wh[i] * (dh * dh);
     if (o.wq) {
         const double dq = s.y - o.qobs[i], dr = s.z - o.robs[i];
         v += o.wq[i] * ((dq * dq) + (dr * dr));

@@ -456,6 +456,7 @@ ObsView obs_view(const AdjointState* a, int k)
     o.robs = a->d_robs ? a->d_robs + (size_t)k * a->n_pts : nullptr;
     o.n = (int)a->n_pts;
     o.scale = (a->normalize && a->n_obs > 0) ? 1.0 / (double)a->n_obs : 1.0;
+    o.wdh = 0;
     return o;
 }
 

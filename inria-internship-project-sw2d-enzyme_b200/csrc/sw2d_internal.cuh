@@ -103,6 +103,7 @@ __device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_
 inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 struct AdjointState;  // sw2d_adjoint.cu
+struct AssimState;    // sw2d_assim.cu
 
 }  // namespace sw2d
 
@@ -133,6 +134,7 @@ struct sw2d_handle {
     sw2d::AdjointState* adj = nullptr;  // recorded trajectory, checkpoints and adjoint buffers
     int adj_flush_branch = 0;           // option "adjoint_flush_branch"
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
+    sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step
     std::string err;
 };
 
@@ -185,6 +187,8 @@ void launch_step_on(sw2d_handle* h);
 
 // Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
 void adjoint_release(sw2d_handle* h);
+// Releases the assimilation buffers of the handle (sw2d_assim.cu).
+void assim_release(sw2d_handle* h);
 // Called when the physical parameters or the state change under a recorded trajectory.
 void adjoint_invalidate(sw2d_handle* h);
 

@@ -1567,6 +1567,7 @@ int sw2d_destroy(sw2d_handle* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     adjoint_release(h);
+    assim_release(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);

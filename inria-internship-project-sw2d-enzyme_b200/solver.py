@@ -25,6 +25,10 @@ from . import capi
 from .case import Case, read_case
 
 
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(capi.c_double_p)
+
+
 class Sw2dError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"sw2d error {code}: {message}")
@@ -249,6 +253,99 @@ class SpModel:
         c = np.zeros(6, dtype=np.int64)
         self._check(self.lib.sw2d_adjoint_nonfinite(self.handle, c.ctypes.data_as(capi.c_int64_p)))
         return dict(zip(self.GRADIENTS, (int(v) for v in c)))
+
+    # ---- porosity assimilation with the reference's differentiated step (sw2d_assim_*) ----
+    PHI_TRANSFORMS = {"none": 0, "clamp": 1, "tanh": 2, "normalize": 3}
+
+    def assim_configure(self, phi_transform: str = "none", lambda_tanh: float = 1.0, windowed: bool = False,
+                        window_duration: float = -1.0, window_steps: int = -1, n_windows: int = 1,
+                        t_state_assimilation: float = 0.0, cost_normalize: bool = False,
+                        mask_wall_gradient: bool = False, forced_first_segment: int = -1) -> None:
+        """The assimilation keys of input.solv (assim/assimConfig.h); the trajectory starts from the
+        model's state and time at the first call."""
+        p = capi.Sw2dAssimParams(self.PHI_TRANSFORMS[phi_transform.lower()], float(lambda_tanh), int(bool(windowed)),
+                                 float(window_duration), int(window_steps), int(n_windows),
+                                 float(t_state_assimilation), int(bool(cost_normalize)), int(bool(mask_wall_gradient)),
+                                 int(forced_first_segment))
+        self._check(self.lib.sw2d_assim_configure(self.handle, ctypes.byref(p)))
+
+    def assim_set_frames(self, times, frames, h_weight=None, q_weight=None) -> None:
+        """Full-field observations: frames[k] = (h, qx, qy) of every cell at times[k]."""
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        f = np.ascontiguousarray(frames, dtype=np.float64).reshape(len(t), 3, self.n)
+        wh = None if h_weight is None else np.ascontiguousarray(h_weight, dtype=np.float64)
+        wq = None if q_weight is None else np.ascontiguousarray(q_weight, dtype=np.float64)
+        o = capi.Sw2dAssimObs(0, len(t), _p(t), _p(f), _p(wh), _p(wq), 0, None, None, None)
+        self._check(self.lib.sw2d_assim_set_observations(self.handle, ctypes.byref(o)))
+
+    def assim_set_gauges(self, times, cells, weights, values) -> None:
+        """Gauge observations: values[k][g] is the depth at cells[g] at times[k]."""
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        c = np.ascontiguousarray(cells, dtype=np.int64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(len(t), len(c))
+        o = capi.Sw2dAssimObs(1, len(t), _p(t), None, None, None, len(c), c.ctypes.data_as(capi.c_int64_p), _p(w), _p(v))
+        self._check(self.lib.sw2d_assim_set_observations(self.handle, ctypes.byref(o)))
+
+    def assim_record(self, m, stride: int = 30) -> Tuple[int, int]:
+        """build_checkpoint_records at control m: (steps, segments)."""
+        mm = np.ascontiguousarray(m, dtype=np.float64)
+        ns, nk = ctypes.c_int64(0), ctypes.c_int64(0)
+        self._check(self.lib.sw2d_assim_record(self.handle, _p(mm), int(stride), ctypes.byref(ns), ctypes.byref(nk)))
+        return ns.value, nk.value
+
+    def assim_replay_cost(self, m) -> float:
+        """replay_trajectory_cost at control m on the recorded trajectory."""
+        mm = np.ascontiguousarray(m, dtype=np.float64)
+        J = ctypes.c_double(0.0)
+        self._check(self.lib.sw2d_assim_replay_cost(self.handle, _p(mm), ctypes.byref(J)))
+        return J.value
+
+    def assim_gradient(self, m, stride: int = 30, extras: bool = False):
+        """get_spatial_gradient_checkpointed at control m: (dJ/dm, info); with extras also
+        {"k1", "k2", "h0", "q0", "r0"} (Strickler coefficients, state at the window start)."""
+        mm = np.ascontiguousarray(m, dtype=np.float64)
+        g = np.zeros(self.n)
+        k1 = np.zeros(self.n) if extras else None
+        k2 = np.zeros(self.n) if extras else None
+        s0 = np.zeros(3 * self.n) if extras else None
+        inf = capi.Sw2dAssimInfo()
+        self._check(self.lib.sw2d_assim_gradient(self.handle, _p(mm), int(stride), _p(g), _p(k1), _p(k2), _p(s0),
+                                                 ctypes.byref(inf)))
+        info = {name: getattr(inf, name) for name, _ in capi.Sw2dAssimInfo._fields_}
+        if not extras:
+            return g, info
+        n = self.n
+        return g, info, {"k1": k1, "k2": k2, "h0": s0[:n], "q0": s0[n:2 * n], "r0": s0[2 * n:]}
+
+    def assim_segments(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(t_start, n_steps) of each recorded segment."""
+        cap = 1
+        while True:
+            t = np.zeros(cap)
+            n = np.zeros(cap, dtype=np.int64)
+            st = self.lib.sw2d_assim_segments(self.handle, _p(t), n.ctypes.data_as(capi.c_int64_p), cap)
+            if st == 0:
+                k = int(np.count_nonzero(n))
+                return t[:k], n[:k]
+            if cap > 1 << 26:
+                self._check(st)
+            cap *= 4
+
+    def assim_steps(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(dt, observation trigger) of each recorded step."""
+        _, n = self.assim_segments()
+        total = int(n.sum())
+        dt = np.zeros(max(1, total))
+        tr = np.zeros(max(1, total), dtype=np.int32)
+        self._check(self.lib.sw2d_assim_steps(self.handle, _p(dt), tr.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                              max(1, total)))
+        return dt[:total], tr[:total]
+
+    def assim_checkpoint(self, k: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        h, q, r = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self._check(self.lib.sw2d_assim_checkpoint(self.handle, int(k), _p(h), _p(q), _p(r)))
+        return h, q, r
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -2,7 +2,10 @@
 
 * :class:`SpOracle` — the plain-C restatement ``sp_oracle.c`` (built into ``_build/``);
 * :class:`RefSolver` — the reference's own native solver compiled from its sources with
-  ``ref_driver.cpp`` (``_ref/libsw2d_ref.so``), run on a case folder.
+  ``ref_driver.cpp`` (``_ref/libsw2d_ref.so``), run on a case folder;
+* :class:`RefE` — the reference's assimilation layer (class swSpE, assim/*.cpp, with an Enzyme
+  stub) through ``ref_e_driver.cpp`` (``_ref/libsw2d_ref_e.so``): its dry run, its segment
+  function and its frozen-trajectory cost.
 """
 from __future__ import annotations
 
@@ -18,6 +21,8 @@ ORACLE_SO = os.path.join(HERE, "_build", "libsp_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libsw2d_ref.so")
 REF_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_pm.so")
 REF_BIN = os.path.join(HERE, "_ref", "sw2dSolver")
+REF_E_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e.so")
+REF_E_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e_pm.so")
 REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "/root/reference")
 
 _pkg = importlib.import_module("inria-internship-project-sw2d-enzyme_b200")
@@ -181,3 +186,150 @@ class RefSolver:
         sx, sy = np.empty(self.n), np.empty(self.n)
         self.lib.sw2dref_slopes(self.h, sx, sy)
         return sx, sy
+
+
+class RefE:
+    """The reference's porosity-assimilation engine (swSpE) on a case folder whose input.solv may
+    hold the assimilation keys.  ``portable_math`` loads the build whose exp, log and cbrt are the
+    portable versions of the CUDA build."""
+
+    def __init__(self, folder: str, quiet: bool = True, portable_math: bool = False):
+        so = REF_E_PM_SO if portable_math else REF_E_SO
+        if not os.path.exists(so):
+            raise RuntimeError(f"reference assimilation library not built ({so})")
+        lib = ctypes.CDLL(so)
+        L = ctypes.c_long
+        lib.sw2dref_e_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        lib.sw2dref_e_open.restype = _P
+        lib.sw2dref_e_cell_nb.argtypes = [_P]
+        lib.sw2dref_e_cell_nb.restype = L
+        lib.sw2dref_e_config.argtypes = [_P, _D]
+        lib.sw2dref_e_get_phi.argtypes = [_P, _D]
+        lib.sw2dref_e_load_phi_map.argtypes = [_P, ctypes.c_char_p, _D]
+        lib.sw2dref_e_load_phi_map.restype = ctypes.c_int
+        lib.sw2dref_e_set_options.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        lib.sw2dref_e_set_weights.argtypes = [_P, _D, _D]
+        lib.sw2dref_e_set_window_keys.argtypes = [_P, ctypes.c_int, ctypes.c_double, L, L, ctypes.c_double]
+        lib.sw2dref_e_load_observations.argtypes = [_P, ctypes.c_int]
+        lib.sw2dref_e_load_observations.restype = ctypes.c_int
+        lib.sw2dref_e_get_observation.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _D]
+        lib.sw2dref_e_set_frames.argtypes = [_P, ctypes.c_int, _D, _D]
+        _I = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+        lib.sw2dref_e_set_gauges.argtypes = [_P, ctypes.c_int, _D, ctypes.c_int, _I, _D, _D]
+        lib.sw2dref_e_record.argtypes = [_P, _D, L, ctypes.c_int]
+        lib.sw2dref_e_record.restype = L
+        lib.sw2dref_e_segment.argtypes = [_P, L, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]
+        lib.sw2dref_e_segment.restype = L
+        lib.sw2dref_e_set_window.argtypes = [_P, ctypes.POINTER(L), _I]
+        lib.sw2dref_e_set_window.restype = ctypes.c_int
+        lib.sw2dref_e_set_truncation.argtypes = [_P, L]
+        lib.sw2dref_e_replay_cost.argtypes = [_P, _D, ctypes.c_int]
+        lib.sw2dref_e_replay_cost.restype = ctypes.c_double
+        lib.sw2dref_e_get_state.argtypes = [_P, _D, _D, _D]
+        lib.sw2dref_e_time.argtypes = [_P]
+        lib.sw2dref_e_time.restype = ctypes.c_double
+        lib.sw2dref_e_close.argtypes = [_P]
+        self.lib = lib
+        self.h = lib.sw2dref_e_open(folder.encode(), 1 if quiet else 0)
+        if not self.h:
+            raise RuntimeError(f"reference assimilation layer failed to open {folder}")
+        self.n = lib.sw2dref_e_cell_nb(self.h)
+        self.K = 0
+
+    CONFIG = ("checkpoint_stride", "windowed", "window_duration", "window_steps", "n_windows",
+              "t_state_assimilation", "cost_normalize", "phi_transform", "lambda_tanh", "dt_map_ad",
+              "mask_wall_gradient", "alpha_reg", "t_0", "t_max")
+
+    def config(self) -> dict:
+        out = np.zeros(len(self.CONFIG))
+        self.lib.sw2dref_e_config(self.h, out)
+        return dict(zip(self.CONFIG, out.tolist()))
+
+    def phi(self) -> np.ndarray:
+        out = np.empty(self.n)
+        self.lib.sw2dref_e_get_phi(self.h, out)
+        return out
+
+    def load_phi_map(self, path: str) -> np.ndarray:
+        out = np.zeros(self.n)
+        if self.lib.sw2dref_e_load_phi_map(self.h, path.encode(), out) != 0:
+            raise RuntimeError(f"cannot read {path}")
+        return out
+
+    def set_options(self, cost_normalize: bool, phi_transform: int = 0, lambda_tanh: float = 1.0) -> None:
+        self.lib.sw2dref_e_set_options(self.h, int(cost_normalize), int(phi_transform), float(lambda_tanh))
+
+    def set_window_keys(self, windowed: bool, duration: float = -1.0, steps: int = -1, n_windows: int = 1,
+                        t_state: float = 0.0) -> None:
+        self.lib.sw2dref_e_set_window_keys(self.h, int(windowed), float(duration), int(steps), int(n_windows),
+                                           float(t_state))
+
+    def set_weights(self, wh, wq) -> None:
+        self.lib.sw2dref_e_set_weights(self.h, np.ascontiguousarray(wh, np.float64), np.ascontiguousarray(wq, np.float64))
+
+    def load_observations(self):
+        """The reference's reader of reference/ResultHydro_p*.txt: (times, frames[k][3][n])."""
+        n_obs = self.lib.sw2dref_e_load_observations(self.h, 1)
+        if n_obs < 0:
+            raise RuntimeError("observations could not be loaded")
+        times = np.zeros(n_obs)
+        frames = np.zeros((n_obs, 3, self.n))
+        t = ctypes.c_double()
+        for k in range(n_obs):
+            buf = np.zeros(3 * self.n)
+            self.lib.sw2dref_e_get_observation(self.h, k, ctypes.byref(t), buf)
+            times[k] = t.value
+            frames[k] = buf.reshape(3, self.n)
+        return times, frames
+
+    def set_frames(self, times, frames) -> None:
+        t = np.ascontiguousarray(times, np.float64)
+        self.lib.sw2dref_e_set_frames(self.h, len(t), t, np.ascontiguousarray(frames, np.float64).ravel())
+
+    def set_gauges(self, times, cells, weights, values) -> None:
+        t = np.ascontiguousarray(times, np.float64)
+        c = np.ascontiguousarray(cells, np.int64)
+        self.lib.sw2dref_e_set_gauges(self.h, len(t), t, len(c), c, np.ascontiguousarray(weights, np.float64),
+                                      np.ascontiguousarray(values, np.float64).ravel())
+
+    def record(self, m, stride: int) -> int:
+        self.K = int(self.lib.sw2dref_e_record(self.h, np.ascontiguousarray(m, np.float64), int(stride), 1))
+        return self.K
+
+    def segments(self):
+        """[(t_start, dt_seq, obs_trig, (h, q, r) checkpoint)] of the record."""
+        out = []
+        for k in range(self.K):
+            ts = ctypes.c_double()
+            n = self.lib.sw2dref_e_segment(self.h, k, ctypes.addressof(ts), None, None, None, None, None)
+            dt = np.zeros(n)
+            tr = np.zeros(n, dtype=np.int32)
+            h, q, r = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+            self.lib.sw2dref_e_segment(self.h, k, None, dt.ctypes.data, tr.ctypes.data, h.ctypes.data, q.ctypes.data,
+                                       r.ctypes.data)
+            out.append((ts.value, dt, tr, (h, q, r)))
+        return out
+
+    def set_window(self):
+        """The window and tiles get_spatial_gradient_checkpointed would set: (first, tiles)."""
+        first = ctypes.c_long()
+        tiles = np.zeros(max(1, self.K), dtype=np.int64)
+        nt = self.lib.sw2dref_e_set_window(self.h, ctypes.byref(first), tiles)
+        return first.value, tiles[:nt].copy()
+
+    def set_truncation(self, seg: int) -> None:
+        self.lib.sw2dref_e_set_truncation(self.h, int(seg))
+
+    def replay_cost(self, m) -> float:
+        return float(self.lib.sw2dref_e_replay_cost(self.h, np.ascontiguousarray(m, np.float64), 1))
+
+    def state(self):
+        h, q, r = np.empty(self.n), np.empty(self.n), np.empty(self.n)
+        self.lib.sw2dref_e_get_state(self.h, h, q, r)
+        return h, q, r
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.sw2dref_e_close(self.h)
+            self.h = None

@@ -247,6 +247,17 @@ void sw2dref_e_set_options(void* h, int cost_normalize, int phi_transform, doubl
     m->lambda_tanh = lambda_tanh;
 }
 
+// The window keys of input.solv (AssimConfig::apply_to, assim/assimConfig.cpp:37-66).
+void sw2dref_e_set_window_keys(void* h, int windowed, double duration, long steps, long n_windows, double t_state)
+{
+    swSpE* m = static_cast<HandleE*>(h)->m;
+    m->windowed_assimilation = windowed != 0;
+    m->assimilation_window_duration = duration;
+    m->assimilation_window_steps = steps;
+    m->n_assimilation_windows = n_windows;
+    m->t_state_assimilation = t_state;
+}
+
 void sw2dref_e_set_weights(void* h, const double* wh, const double* wq)
 {
     RefE* m = static_cast<HandleE*>(h)->m;

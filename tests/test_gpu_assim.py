@@ -1,0 +1,190 @@
+"""Porosity assimilation with the reference's differentiated step on the GPU (sw2d_assim_*),
+against the reference's own assimilation layer (assim/*.cpp through oracle/ref_e_driver.cpp,
+linked with the portable exp/log/cbrt; the library built from the reference sources travels with
+the repository as oracle/_ref):
+
+* the dry run (build_checkpoint_records): every time step, observation trigger and segment start,
+  and every checkpoint state, bit for bit;
+* the frozen-trajectory cost (replay_trajectory_cost), continuous, truncated or tiled: within
+  1e-12 relative (the per-observation sums run in a tree on the GPU, in cell order on the CPU);
+* the gradient dJ/dm (the reference differentiates with Enzyme, absent here): against central
+  differences of the reference's own replay cost, eps = 1e-6, in seeded directions;
+* sp_toce, the reference's own assimilation case, from the committed fixture
+  tests/golden/sp_toce_assim.npz; its gradient statistics are printed beside the Enzyme run's
+  (descent_log_reference_-75.8pct.csv), which used the host libm.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.conftest import GOLDEN, load_pkg, sp_toce_case
+
+pytestmark = pytest.mark.gpu
+
+EPS = 1e-6
+DESCENT_LOG = dict(J=3.1042911536e+00, grad_l2=8.189797e-02, grad_max=-4.373691e-02, argmax=3931, dh_peak=2.377364e+04)
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    p = load_pkg()
+    p.build.build()
+    return p
+
+
+def _bits_equal(a, b):
+    return np.array_equal(np.asarray(a, np.float64).view(np.int64), np.asarray(b, np.float64).view(np.int64))
+
+
+def _ck_hash(h, q, r):
+    d = hashlib.sha256()
+    for a in (h, q, r):
+        d.update(np.ascontiguousarray(a, np.float64).tobytes())
+    return d.hexdigest()
+
+
+# ---------------------------------------------------------------------------------------------
+# sp_toce
+# ---------------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def toce(pkg):
+    from tests.golden.make_assim_golden import decimals_to_float
+    case, _ = sp_toce_case()
+    ax = np.load(os.path.join(GOLDEN, "sp_toce_assim.npz"))
+    cfg = json.loads(str(ax["config"]))
+    model = pkg.SpModel(case)
+    model.assim_configure(phi_transform="none", windowed=cfg["windowed"] > 0, window_duration=cfg["window_duration"],
+                          window_steps=int(cfg["window_steps"]), n_windows=int(cfg["n_windows"]),
+                          t_state_assimilation=cfg["t_state_assimilation"], cost_normalize=cfg["cost_normalize"] > 0)
+    model.assim_set_frames(ax["obs_times"], decimals_to_float(ax["obs_mant"], ax["obs_exp"]))
+    return model, ax, int(cfg["checkpoint_stride"])
+
+
+def test_toce_record_matches_reference(toce):
+    model, ax, stride = toce
+    ns, nk = model.assim_record(ax["m"], stride)
+    assert nk == len(ax["seg_n"]) and ns == int(ax["seg_n"].sum())
+    t0, n = model.assim_segments()
+    assert np.array_equal(n, ax["seg_n"]) and _bits_equal(t0, ax["seg_t_start"])
+    dt, trig = model.assim_steps()
+    assert _bits_equal(dt, ax["dt_seq"]), f"first dt difference at step {int(np.argmax(dt != ax['dt_seq']))}"
+    assert np.array_equal(trig, ax["obs_trig"])
+    bad = [k for k in range(nk) if _ck_hash(*model.assim_checkpoint(k)) != str(ax["ck_sha256"][k])]
+    assert not bad, f"checkpoints differing from the reference's: {bad[:10]}"
+
+
+def test_toce_replay_cost_matches_reference(toce):
+    model, ax, stride = toce
+    model.assim_record(ax["m"], stride)
+    J = model.assim_replay_cost(ax["m"])
+    assert abs(J - float(ax["J_pm"])) <= 1e-12 * abs(float(ax["J_pm"])), f"{J:.15e} vs {float(ax['J_pm']):.15e}"
+
+
+def test_toce_gradient_matches_reference_differences(toce):
+    model, ax, stride = toce
+    g, info = model.assim_gradient(ax["m"], stride)
+    eps = float(ax["eps"])
+    for d, (jp, jm) in zip(ax["fd_dirs"], ax["fd_J"]):
+        fd = (jp - jm) / (2.0 * eps)
+        ad = float(g @ d)
+        assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-9, f"adjoint {ad:.9e} vs central difference {fd:.9e}"
+    assert abs(info["J"] - float(ax["J_pm"])) <= 1e-12 * float(ax["J_pm"])
+    assert info["n_tiles"] == len(ax["tiles"]) and info["first_segment"] == int(ax["first_segment"])
+    # beside the Enzyme run of the reference (host libm: the trajectory differs by ~1e-5)
+    print("sp_toce gradient at phi = 1:", {k: info[k] for k in ("J", "grad_l2", "grad_max", "grad_argmax", "dh_peak")},
+          "descent log:", DESCENT_LOG)
+    assert abs(info["J"] - DESCENT_LOG["J"]) / DESCENT_LOG["J"] < 2e-5
+
+
+# ---------------------------------------------------------------------------------------------
+# synthetic cases against the live reference
+# ---------------------------------------------------------------------------------------------
+CONFIGS = [
+    dict(scheme="godunov", friction="strickler", head_loss=True, outflow="fr", obs="frames", transform="none",
+         windowed=False, n_windows=1, stride=10),
+    dict(scheme="muscl_evr", friction="manning", head_loss=False, outflow="h", obs="frames", transform="tanh",
+         windowed=True, window_steps=40, n_windows=3, stride=8),
+    dict(scheme="muscl_evr", friction="none", head_loss=True, outflow="z", obs="gauges", transform="clamp",
+         windowed=True, window_duration=3.0, n_windows=1, stride=12),
+    dict(scheme="godunov", friction="chezy", head_loss=False, outflow="fr", obs="gauges", transform="normalize",
+         windowed=False, n_windows=4, stride=6),
+]
+TRANSFORM = {"none": 0, "clamp": 1, "tanh": 2, "normalize": 3}
+
+
+def _synthetic(pkg, tmp_path, cfg):
+    from oracle.binding import RefE, REF_E_PM_SO
+    if not os.path.exists(REF_E_PM_SO):
+        pytest.skip("reference assimilation library (oracle/_ref) not built")
+    case = pkg.workloads.channel_features(n_cells=1500, scheme=cfg["scheme"], topo="discontinuous",
+                                          friction=cfg["friction"], outflow=cfg["outflow"], head_loss=cfg["head_loss"],
+                                          t_max=6.0, seed=11)
+    folder = str(tmp_path / "case")
+    pkg.write_case(folder, case)
+    ref = RefE(folder, portable_math=True)
+    n = case.mesh.cell_nb
+    rng = np.random.default_rng(5)
+    times = np.arange(0.5, 6.0 + 1e-9, 0.5)
+    win = dict(windowed=cfg["windowed"], duration=cfg.get("window_duration", -1.0), steps=cfg.get("window_steps", -1),
+               n_windows=cfg["n_windows"], t_state=0.0)
+    ref.set_window_keys(**win)
+    ref.set_options(True, TRANSFORM[cfg["transform"]], 1.5)
+    model = pkg.SpModel(case)
+    model.assim_configure(phi_transform=cfg["transform"], lambda_tanh=1.5, windowed=cfg["windowed"],
+                          window_duration=win["duration"], window_steps=win["steps"], n_windows=cfg["n_windows"],
+                          cost_normalize=True)
+    if cfg["obs"] == "frames":
+        frames = np.stack([np.stack([case.h0 * (1.0 + 0.1 * np.sin(0.3 * k)), 0.02 * rng.standard_normal(n),
+                                     0.02 * rng.standard_normal(n)]) for k in range(len(times))])
+        wh, wq = rng.uniform(0.5, 1.5, n), rng.uniform(0.0, 0.5, n)
+        ref.set_frames(times, frames)
+        ref.set_weights(wh, wq)
+        model.assim_set_frames(times, frames, wh, wq)
+    else:
+        cells = rng.choice(n, size=24, replace=False)
+        cells[3] = cells[7]  # two gauges in one cell
+        w = rng.uniform(0.5, 2.0, 24)
+        vals = 0.1 + 0.2 * rng.uniform(size=(len(times), 24))
+        ref.set_gauges(times, cells, w, vals)
+        model.assim_set_gauges(times, cells, w, vals)
+    phi = case.phi
+    if cfg["transform"] == "tanh":
+        m = np.log(phi / (1.0 - np.minimum(phi, 0.99))) / 1.5
+    else:
+        m = phi.copy()
+    return case, ref, model, m
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=lambda c: "-".join(str(v) for v in c.values()))
+def test_synthetic_matches_live_reference(pkg, tmp_path, cfg):
+    case, ref, model, m = _synthetic(pkg, tmp_path, cfg)
+    K = ref.record(m, cfg["stride"])
+    first, tiles = ref.set_window()
+    ns, nk = model.assim_record(m, cfg["stride"])
+    assert nk == K
+    segs = ref.segments()
+    dt, trig = model.assim_steps()
+    assert _bits_equal(dt, np.concatenate([s[1] for s in segs]))
+    assert np.array_equal(trig, np.concatenate([s[2] for s in segs]))
+    t0, _ = model.assim_segments()
+    assert _bits_equal(t0, [s[0] for s in segs])
+    for k in range(K):
+        for a, b in zip(model.assim_checkpoint(k), segs[k][3]):
+            assert _bits_equal(a, b), f"checkpoint {k}"
+    J_ref = ref.replay_cost(m)
+    J = model.assim_replay_cost(m)
+    assert abs(J - J_ref) <= 1e-12 * abs(J_ref) + 1e-300, f"{J:.15e} vs {J_ref:.15e}"
+    # gradient against central differences of the reference's replay cost
+    g, info = model.assim_gradient(m, cfg["stride"])
+    assert info["first_segment"] == first and info["n_tiles"] == len(tiles)
+    assert abs(info["J"] - J_ref) <= 1e-12 * abs(J_ref)
+    rng = np.random.default_rng(17)
+    for _ in range(2):
+        d = rng.standard_normal(case.mesh.cell_nb)
+        d[np.argmin(m)] = d[np.argmax(m)] = 0.0   # the normalize bounds stay those of the record
+        fd = (ref.replay_cost(m + EPS * d) - ref.replay_cost(m - EPS * d)) / (2.0 * EPS)
+        ad = float(g @ d)
+        assert abs(ad - fd) <= 2e-5 * abs(fd) + 1e-10, f"adjoint {ad:.9e} vs central difference {fd:.9e}"
