@@ -30,7 +30,7 @@ def pkg():
 
 
 def golden_names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f != "sp_toce.npz")
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("sp_toce"))
 
 
 def golden_case(name):
