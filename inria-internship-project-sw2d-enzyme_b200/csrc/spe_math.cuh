@@ -34,8 +34,14 @@ constexpr double kFricEps = 1e-10;       // assim/swSpE_friction.cpp:24
 constexpr double kFricDefaultK = 20.0;   // assim/swSpE_friction.cpp:49-50
 constexpr double kDtFloor = 1e-6;        // assim/swSpE_hyp.cpp:634
 
-// adjoint of sqrt(x) given the adjoint of its value s = sqrt(x): 0 at x == 0
-SW2D_HD double dsqrt(double s, double sb) { return (s > 0.0) ? sb * 0.5 / s : 0.0; }
+// Adjoint of sqrt(x) given the adjoint sb of its value s = sqrt(x).  At x == 0: 0 (subgradient
+// 0), or with `ieee` the literal sb / (2 sqrt(0)), non-finite unless sb == 0 (what a
+// source-transformation AD tool produces; the reference's gradient then zeroes non-finite entries).
+SW2D_HD double dsqrt(double s, double sb, bool ieee = false)
+{
+    if (s > 0.0) return sb * 0.5 / s;
+    return (ieee && sb != 0.0) ? sb * 0.5 / s : 0.0;
+}
 
 // ---- desingVelocity (assim/swSpDesingVelocity.h:27-34) --------------------------------------
 SW2D_HD double desing(double q, double h)
@@ -65,14 +71,18 @@ SW2D_HD void desing_rev(double q, double h, double yb, double& qb, double& hb)
 
 // ---- wave speeds lambda-/+ = b u -/+ sqrt((b-1) b u^2 + c^2) (swSp.cpp:972-995) -----------
 // adds the adjoints of u and c given those of lambda- and lambda+
-SW2D_HD void lam_rev(double b, double c, double u, double lmb, double lpb, double& ub, double& cb)
+SW2D_HD void lam_rev(double b, double c, double u, double lmb, double lpb, double& ub, double& cb, bool ieee = false)
 {
     const double R = sqrt((b - 1.0) * b * u * u + c * c);
     ub += b * (lmb + lpb);
+    const double Rb = lpb - lmb;
     if (R > 0.0) {
-        const double Rb = lpb - lmb;
         ub += Rb * (b - 1.0) * b * u / R;
         cb += Rb * c / R;
+    } else if (ieee && Rb != 0.0) {
+        const double xb = Rb * 0.5 / R;  // adjoint of the radicand: +-inf
+        ub += xb * (2.0 * (b - 1.0) * b * u);
+        cb += xb * (2.0 * c);
     }
 }
 
@@ -99,15 +109,15 @@ SW2D_HD ESide god_side(double h, double q, double r, double zb, double b, double
 
 // adds the adjoints of the cell's (h, q, r)
 SW2D_HD void god_side_rev(double h, double q, double r, double b, double nx, double ny, double h_min,
-                          const ESideBar& sb, double& hb, double& qb, double& rb)
+                          const ESideBar& sb, double& hb, double& qb, double& rb, bool ieee = false)
 {
     const double qn = q * nx + r * ny;
     const double u = (h > h_min) ? qn / h : 0.0;
     const double c = sqrt(kGravity * h);
     double ub = 0.0, cb = 0.0;
-    lam_rev(b, c, u, sb.lm, sb.lp, ub, cb);
+    lam_rev(b, c, u, sb.lm, sb.lp, ub, cb, ieee);
     hb += sb.z;
-    hb += dsqrt(c, cb) * kGravity;
+    hb += dsqrt(c, cb, ieee) * kGravity;
     double qnb = sb.q;
     if (h > h_min) {
         qnb += ub / h;
@@ -132,15 +142,15 @@ SW2D_HD ESide evr_bnd_side(double h, double q, double r, double zb, double b, do
 }
 
 SW2D_HD void evr_bnd_side_rev(double h, double q, double r, double b, double nx, double ny, const ESideBar& sb,
-                              double& hb, double& qb, double& rb)
+                              double& hb, double& qb, double& rb, bool ieee = false)
 {
     const double qn = q * nx + r * ny;
     const double u = desing(qn, h);
     const double c = sqrt(kGravity * h);
     double ub = 0.0, cb = 0.0;
-    lam_rev(b, c, u, sb.lm, sb.lp, ub, cb);
+    lam_rev(b, c, u, sb.lm, sb.lp, ub, cb, ieee);
     hb += sb.z;
-    hb += dsqrt(c, cb) * kGravity;
+    hb += dsqrt(c, cb, ieee) * kGravity;
     double qnb = sb.q;
     desing_rev(qn, h, ub, qnb, hb);
     qb += qnb * nx - sb.r * ny;
@@ -185,7 +195,7 @@ SW2D_HD ESide evr_side(bool left, double h, double q, double r, double zb, doubl
 // Adds the adjoints of the cell's (h, q, r), of zc and of the slope (sx, sy).
 SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, double b, double zc, double sx, double sy,
                           double dmx, double dmy, double nx, double ny, double dt, const ESideBar& sb, double& hb,
-                          double& qb, double& rb, double& zcb, double& sxb, double& syb)
+                          double& qb, double& rb, double& zcb, double& sxb, double& syb, bool ieee = false)
 {
     // forward values
     const double ql = q * nx + r * ny;
@@ -211,8 +221,8 @@ SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, do
     const double c = sqrt(kGravity * hr);
     // Riemann state's wave speeds
     double ub = 0.0, cb = 0.0;
-    lam_rev(b, c, u, sb.lm, sb.lp, ub, cb);
-    double hrb = sb.z + dsqrt(c, cb) * kGravity;
+    lam_rev(b, c, u, sb.lm, sb.lp, ub, cb, ieee);
+    double hrb = sb.z + dsqrt(c, cb, ieee) * kGravity;
     double qrb = sb.q;
     desing_rev(qr, hr, ub, qrb, hrb);
     hrb += qrb * ul + sb.r * vl;
@@ -234,7 +244,7 @@ SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, do
         lpvb = (lpv < 0.0) ? l2b : 0.0;
     }
     double clb = 0.0;
-    lam_rev(b, cl, ul, lmvb, lpvb, ulb, clb);
+    lam_rev(b, cl, ul, lmvb, lpvb, ulb, clb, ieee);
     if (kSmallReal < h) hb += dsqrt(cl, clb) * kGravity;
     double qlb = 0.0, rlb = 0.0;
     desing_rev(ql, h, ulb, qlb, hb);

@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(kBlock) k_e_update_rev(DevMesh m, const double
 // contribution goes to its slot: ctb = {h, q, r, phi} adjoints of that cell, cts = its slope's.
 template <int kScheme>
 __global__ void __launch_bounds__(kBlock) k_e_edges_rev(DevMesh m, EView v, const double4* __restrict__ lamb,
-                                                        double4* ctb, double2* cts, double dt)
+                                                        double4* ctb, double2* cts, double dt, int ieee)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m.ni) {
@@ -530,22 +530,22 @@ __global__ void __launch_bounds__(kBlock) k_e_edges_rev(DevMesh m, EView v, cons
         const int2 sl = ld(&m.eslot[e]);
         double hb = 0, qb = 0, rb = 0;
         if (kScheme == SW2D_SCHEME_GODUNOV) {
-            spe::god_side_rev(sa.x, sa.y, sa.z, ca.y, nx, ny, m.h_min, Lb, hb, qb, rb);
+            spe::god_side_rev(sa.x, sa.y, sa.z, ca.y, nx, ny, m.h_min, Lb, hb, qb, rb, ieee);
             ctb[sl.x] = make_double4(hb, qb, rb, pLb);
             hb = qb = rb = 0.0;
-            spe::god_side_rev(sb.x, sb.y, sb.z, cb.y, nx, ny, m.h_min, Rb, hb, qb, rb);
+            spe::god_side_rev(sb.x, sb.y, sb.z, cb.y, nx, ny, m.h_min, Rb, hb, qb, rb, ieee);
             ctb[sl.y] = make_double4(hb, qb, rb, pRb);
         } else {
             const double4 d = ld(&m.emc[e]);
             const double2 ga = ld(&m.slope[a]), gb = ld(&m.slope[b]);
             double zcb = 0, sxb = 0, syb = 0;
             spe::evr_side_rev(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, d.x, d.y, nx, ny, dt, Lb, hb, qb, rb,
-                              zcb, sxb, syb);
+                              zcb, sxb, syb, ieee);
             ctb[sl.x] = make_double4(hb + zcb, qb, rb, pLb);
             cts[sl.x] = make_double2(sxb, syb);
             hb = qb = rb = zcb = sxb = syb = 0.0;
             spe::evr_side_rev(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, d.z, d.w, nx, ny, dt, Rb, hb, qb, rb,
-                              zcb, sxb, syb);
+                              zcb, sxb, syb, ieee);
             ctb[sl.y] = make_double4(hb + zcb, qb, rb, pRb);
             cts[sl.y] = make_double2(sxb, syb);
         }
@@ -570,8 +570,8 @@ __global__ void __launch_bounds__(kBlock) k_e_edges_rev(DevMesh m, EView v, cons
         spe::ESideBar Sb{0, 0, 0, 0, 0};
         spe::boundary_flux_rev(cs.y, phi, cs.x, S, type, bcv, m.h_min, m.phi_min, f1b, f2b, f3b, pb, Sb);
         double hb = 0, qb = 0, rb = 0;
-        if (kScheme == SW2D_SCHEME_GODUNOV) spe::god_side_rev(s.x, s.y, s.z, cs.y, nx, ny, m.h_min, Sb, hb, qb, rb);
-        else spe::evr_bnd_side_rev(s.x, s.y, s.z, cs.y, nx, ny, Sb, hb, qb, rb);
+        if (kScheme == SW2D_SCHEME_GODUNOV) spe::god_side_rev(s.x, s.y, s.z, cs.y, nx, ny, m.h_min, Sb, hb, qb, rb, ieee);
+        else spe::evr_bnd_side_rev(s.x, s.y, s.z, cs.y, nx, ny, Sb, hb, qb, rb, ieee);
         const int sb = ld(&m.bslot[e]);
         ctb[sb] = make_double4(hb, qb, rb, pb);
         if (kScheme != SW2D_SCHEME_GODUNOV) cts[sb] = make_double2(0.0, 0.0);
@@ -1120,8 +1120,10 @@ int reverse_segment(sw2d_handle* h, int64_t k)
         if (muscl) launch_slopes_on(h, mr);
         const EView v = eview(a, a->d_dt + j, a->d_t + j);
         if (ge > 0) {
-            if (muscl) k_e_edges_rev<SW2D_SCHEME_MUSCL_EVR><<<ge, kBlock, 0, h->stream>>>(mr, v, a->lamb, a->ctb, a->cts, dt);
-            else k_e_edges_rev<SW2D_SCHEME_GODUNOV><<<ge, kBlock, 0, h->stream>>>(mr, v, a->lamb, a->ctb, a->cts, dt);
+            const int ieee = h->assim_sqrt_zero;
+            if (muscl)
+                k_e_edges_rev<SW2D_SCHEME_MUSCL_EVR><<<ge, kBlock, 0, h->stream>>>(mr, v, a->lamb, a->ctb, a->cts, dt, ieee);
+            else k_e_edges_rev<SW2D_SCHEME_GODUNOV><<<ge, kBlock, 0, h->stream>>>(mr, v, a->lamb, a->ctb, a->cts, dt, ieee);
         }
         if (gc > 0) {
             if (muscl) {

@@ -135,6 +135,7 @@ struct sw2d_handle {
     int adj_flush_branch = 0;           // option "adjoint_flush_branch"
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step
+    int assim_sqrt_zero = 0;            // option "assim_sqrt_zero"
     std::string err;
 };
 

@@ -1294,6 +1294,11 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
     } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
         h->adj_flush_branch = value ? 1 : 0;
         return SW2D_OK;
+    } else if (std::strcmp(name, "assim_sqrt_zero") == 0) {
+        // reverse of sqrt at 0 in the assimilation sweep: 0 (subgradient 0, default) or 1
+        // (IEEE: dy / (2 sqrt(0)), non-finite unless dy == 0, as source-transformation AD gives)
+        h->assim_sqrt_zero = value ? 1 : 0;
+        return SW2D_OK;
     } else if (std::strcmp(name, "adjoint_edge_variant") == 0) {
         if (value < 0 || value > 4) return fail(h, SW2D_E_ARG, "adjoint_edge_variant outside 0..4");
         h->adj_edge_variant = (int)value;

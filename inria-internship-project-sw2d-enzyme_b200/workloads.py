@@ -108,9 +108,11 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
 def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "blending",
                      friction: str = "strickler", outflow: str = "fr", head_loss: bool = True,
                      boussinesq: float = 1.0, t_max: float = 40.0, seed: int = 7,
-                     impervious: bool = False) -> Case:
+                     impervious: bool = False, h_floor: float = 0.0, h_sing: float = 0.05) -> Case:
     """Sloped 60 m x 12 m channel with bumps, an inflow hydrograph on the left ('q', code -2),
-    an outflow condition on the right (code -3) and walls elsewhere (code -1)."""
+    an outflow condition on the right (code -3) and walls elsewhere (code -1).  The initial
+    depth is max(h_floor, 0.45 - z_b) (h_floor > 0: wet everywhere); h_sing is the head-loss
+    threshold depth."""
     rng = np.random.default_rng(seed)
     lx, ly = 60.0, 12.0
 
@@ -126,7 +128,7 @@ def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "
     nx, ny = _grid_for(n_cells, 5.0)
     mesh = jittered_triangle_mesh(nx, ny, lx, ly, seed=seed, z_fn=bed, bc_code_fn=codes)
     n = mesh.cell_nb
-    h0 = np.maximum(0.0, 0.45 - mesh.cell_z_b)     # partly dry bed
+    h0 = np.maximum(h_floor, 0.45 - mesh.cell_z_b)     # partly dry bed unless h_floor > 0
     phi = rng.uniform(0.5, 1.0, size=n)
     if impervious:
         # phi = 0 next to a dry cell is the configuration the reference rejects as
@@ -144,7 +146,7 @@ def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "
         fr = np.stack([k * rng.uniform(0.8, 1.2, n), k * rng.uniform(0.8, 1.2, n), rng.uniform(0.0, 90.0, n)])
     hl = None
     if head_loss:
-        hl = np.stack([np.full(n, 0.05), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 45.0, n)])
+        hl = np.stack([np.full(n, h_sing), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 45.0, n)])
     times = np.array([0.0, 5.0, 10.0, 20.0, 30.0, 40.0])
     inflow = np.array([0.0, 0.2, 0.5, 0.5, 0.3, 0.3])
     out_val = {"fr": np.full(6, 0.6), "h": np.full(6, 0.15), "z": np.full(6, 0.35), "q": np.full(6, -0.1)}[outflow]
