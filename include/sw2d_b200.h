@@ -447,6 +447,10 @@ int sw2d_assim_gradient(sw2d_handle* h, const double* m, int64_t stride, double*
  * observation trigger (-1 or the observation index).  Capacities in entries. */
 int sw2d_assim_segments(sw2d_handle* h, double* t_start, int64_t* n_steps, int64_t capacity);
 int sw2d_assim_steps(sw2d_handle* h, double* dt, int32_t* obs_trig, int64_t capacity);
+/* Replaces the start state of the trajectory (swSpE::save_initial_state); with a recorded
+ * trajectory, its first checkpoint too (time steps, boundary values and triggers stay frozen). */
+int sw2d_assim_set_start(sw2d_handle* h, const double* water_depth, const double* unit_discharge_x,
+                         const double* unit_discharge_y);
 /* Checkpoint k (the state at the start of segment k), caller numbering. */
 int sw2d_assim_checkpoint(sw2d_handle* h, int64_t k, double* water_depth, double* unit_discharge_x,
                           double* unit_discharge_y);

@@ -160,6 +160,13 @@ __global__ void k_e_coef(DevMesh m, const double* __restrict__ phi, double2* coe
     }
 }
 
+// z = h + z_b of a state array
+__global__ void k_refresh_z_e(double4* st, const double* __restrict__ zbv, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) st[i].w = st[i].x + zbv[i];
+}
+
 // ------------------------------------------------------------------------------------------
 // forward step
 // ------------------------------------------------------------------------------------------
@@ -1459,6 +1466,30 @@ int sw2d_assim_steps(sw2d_handle* h, double* dt, int32_t* obs_trig, int64_t capa
         if (dt) dt[j] = a->dt_seq[j];
         if (obs_trig) obs_trig[j] = a->trig[j];
     }
+    return SW2D_OK;
+}
+
+int sw2d_assim_set_start(sw2d_handle* h, const double* water_depth, const double* unit_discharge_x,
+                         const double* unit_discharge_y)
+{
+    int rc = require(h, false);
+    if (rc) return rc;
+    if (!water_depth || !unit_discharge_x || !unit_discharge_y) return fail(h, SW2D_E_ARG, "invalid arguments");
+    CK(cudaSetDevice(h->device));
+    AssimState* a = h->assim;
+    const int64_t nc = h->nc;
+    const double* src[3] = {water_depth, unit_discharge_x, unit_discharge_y};
+    double* st0 = reinterpret_cast<double*>(a->st0);
+    for (int q = 0; q < 3; q++) {
+        CK(cudaMemcpyAsync(a->stage, src[q], nc * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_gather_component<<<grid_for(nc), kBlock, 0, h->stream>>>(a->stage, h->d_cell_perm, st0, 4, q, (int)nc);
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    k_refresh_z_e<<<grid_for(nc), kBlock, 0, h->stream>>>(a->st0, h->m.zbv, (int)nc);
+    if (a->recorded && !a->ck.empty())
+        CK(cudaMemcpyAsync(a->ck[0], a->st0, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
     return SW2D_OK;
 }
 

@@ -342,6 +342,10 @@ class SpModel:
                                               max(1, total)))
         return dt[:total], tr[:total]
 
+    def assim_set_start(self, h, q, r) -> None:
+        h, q, r = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, q, r))
+        self._check(self.lib.sw2d_assim_set_start(self.handle, _p(h), _p(q), _p(r)))
+
     def assim_checkpoint(self, k: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         h, q, r = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
         self._check(self.lib.sw2d_assim_checkpoint(self.handle, int(k), _p(h), _p(q), _p(r)))
