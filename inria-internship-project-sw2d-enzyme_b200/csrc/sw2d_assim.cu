@@ -90,6 +90,7 @@ struct AssimState {
     double* d_cost = nullptr;        // cost of the observation a step ends on (replays)
     int* d_trig = nullptr;
     std::vector<double4*> ck;        // state at the start of each segment
+    std::vector<double4*> cs;        // the same states along the replay (option assim_chained_recompute)
     bool recorded = false;
     // window (get_spatial_gradient_checkpointed)
     int64_t first = 0, truncation = -1;
@@ -887,6 +888,8 @@ void free_checkpoints(AssimState* a)
 {
     for (double4* p : a->ck) cudaFree(p);
     a->ck.clear();
+    for (double4* p : a->cs) cudaFree(p);
+    a->cs.clear();
 }
 
 
@@ -1035,11 +1038,12 @@ void replay_segments(sw2d_handle* h, int64_t s0, int64_t s1)
 
 // replay_trajectory_cost: per segment the sum of its observations' costs in step order (from 0),
 // added to the total segment by segment, as ckpt_segment_E returns them
-int replay_cost(sw2d_handle* h, double* J)
+// the chains replay_trajectory_cost replays: (first segment, last segment) from each tile's
+// checkpoint, or from the one after the truncation
+std::vector<std::pair<int64_t, int64_t>> replay_runs(const AssimState* a)
 {
-    AssimState* a = h->assim;
     const int64_t K = (int64_t)a->segs.size();
-    std::vector<std::pair<int64_t, int64_t>> runs;   // (first segment, last segment) replayed chained
+    std::vector<std::pair<int64_t, int64_t>> runs;
     if (!a->tiles.empty()) {
         for (size_t ti = 0; ti < a->tiles.size(); ti++)
             runs.emplace_back(a->tiles[ti], (ti + 1 < a->tiles.size()) ? a->tiles[ti + 1] - 1 : K - 1);
@@ -1048,6 +1052,38 @@ int replay_cost(sw2d_handle* h, double* J)
         if (a->truncation >= 0 && a->truncation + 1 < K) s0 = a->truncation + 1;
         runs.emplace_back(s0, K - 1);
     }
+    return runs;
+}
+
+// The segment-start states along the replay's chains (cs[k]; for the first segment of a chain,
+// its checkpoint).  With the MUSCL-EVR scheme they differ from the dry run's checkpoints: the dry
+// run reconstructs with the previous step's dt (build_checkpoint_records calls
+// hypComputeLRStates_E before setting this->dt, swSpE_checkpoint.cpp:236-246), the replay with
+// the step's own (ckpt_segment_E, :640-641).
+int chain_states(sw2d_handle* h)
+{
+    AssimState* a = h->assim;
+    const int64_t K = (int64_t)a->segs.size(), nc = h->nc;
+    while ((int64_t)a->cs.size() < K) {
+        double4* p = nullptr;
+        CK(cudaMalloc(&p, std::max<int64_t>(1, nc) * sizeof(double4)));
+        a->cs.push_back(p);
+    }
+    for (const auto& r : replay_runs(a)) {
+        CK(cudaMemcpyAsync(h->m.st, a->ck[r.first], nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+        for (int64_t s = r.first; s <= r.second; s++) {
+            CK(cudaMemcpyAsync(a->cs[s], h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+            for (int64_t j = a->segs[s].j0; j < a->segs[s].j0 + a->segs[s].n; j++) replay_step(h, j, nullptr);
+        }
+    }
+    CK(cudaGetLastError());
+    return SW2D_OK;
+}
+
+int replay_cost(sw2d_handle* h, double* J)
+{
+    AssimState* a = h->assim;
+    const auto runs = replay_runs(a);
     for (const auto& r : runs) {
         CK(cudaMemcpyAsync(h->m.st, a->ck[r.first], h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
         replay_segments(h, r.first, r.second);
@@ -1101,14 +1137,16 @@ double norm_h(sw2d_handle* h, int* rc)
     return std::sqrt(s);
 }
 
-// Reverse of segment k (recompute from its checkpoint, then the steps backwards).
+// Reverse of segment k (recompute from its checkpoint, or from its state along the replay with
+// the option assim_chained_recompute, then the steps backwards).
 int reverse_segment(sw2d_handle* h, int64_t k)
 {
     AssimState* a = h->assim;
     const AssimSegment& sg = a->segs[k];
     const int64_t nc = h->nc;
     const bool muscl = h->p.scheme == SW2D_SCHEME_MUSCL_EVR;
-    CK(cudaMemcpyAsync(h->m.st, a->ck[k], nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    const double4* start = (h->assim_chained && k < (int64_t)a->cs.size()) ? a->cs[k] : a->ck[k];
+    CK(cudaMemcpyAsync(h->m.st, start, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
     for (int64_t j = sg.j0; j < sg.j0 + sg.n; j++) {
         CK(cudaMemcpyAsync(a->seg_st + (j - sg.j0) * nc, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice,
                            h->stream));
@@ -1350,6 +1388,7 @@ int sw2d_assim_gradient(sw2d_handle* h, const double* m, int64_t stride, double*
     CK(cudaMemsetAsync(a->g_w, 0, nc * sizeof(double), h->stream));
     CK(cudaMemsetAsync(a->gzb, 0, nc * sizeof(double), h->stream));
     if (K > 0 && (rc = seg_buffers(h))) return rc;
+    if (K > 0 && h->assim_chained && (rc = chain_states(h))) return rc;
     // tiles: tile_top[k] = the last segment of a tile (the adjoint restarts from 0 before it)
     std::vector<char> tile_top(K, 0);
     const bool tiled = !a->tiles.empty();

@@ -136,6 +136,7 @@ struct sw2d_handle {
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step
     int assim_sqrt_zero = 0;            // option "assim_sqrt_zero"
+    int assim_chained = 0;              // option "assim_chained_recompute"
     std::string err;
 };
 

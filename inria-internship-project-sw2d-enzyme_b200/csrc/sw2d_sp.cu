@@ -1299,6 +1299,11 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         // (IEEE: dy / (2 sqrt(0)), non-finite unless dy == 0, as source-transformation AD gives)
         h->assim_sqrt_zero = value ? 1 : 0;
         return SW2D_OK;
+    } else if (std::strcmp(name, "assim_chained_recompute") == 0) {
+        // where the gradient recomputes each segment: 0 from the dry run's checkpoints, as the
+        // reference does; 1 from the replay's own states (the exact gradient of the replay cost)
+        h->assim_chained = value ? 1 : 0;
+        return SW2D_OK;
     } else if (std::strcmp(name, "adjoint_edge_variant") == 0) {
         if (value < 0 || value > 4) return fail(h, SW2D_E_ARG, "adjoint_edge_variant outside 0..4");
         h->adj_edge_variant = (int)value;
