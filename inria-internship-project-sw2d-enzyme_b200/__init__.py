@@ -8,13 +8,15 @@ Modules:
   solver     -- SpModel, the host-side mirror of the reference's swSp interface
   tuning     -- launch-configuration autotuner with a JSON cache
   assimilation -- friction assimilation over the GPU adjoint (the reference's swSpE_minimize)
+  porosity   -- porosity assimilation with the reference's differentiated step (swSpE, its
+                input.solv keys, observation files, PorosityProblem and run_minimization)
   batch      -- ensembles of independent simulations advanced together (one graph launch)
   autograd   -- torch.autograd bridge to the replayed cost and its adjoint (imported on demand)
 """
-from . import build, case, mesh, workloads, capi, solver, tuning, assimilation, batch  # noqa: F401
+from . import build, case, mesh, workloads, capi, solver, tuning, assimilation, batch, porosity  # noqa: F401
 from .case import Case, read_case, write_case  # noqa: F401
 from .solver import SpModel, Sw2dError  # noqa: F401
 from .batch import Batch  # noqa: F401
 
-__all__ = ["case", "mesh", "workloads", "capi", "solver", "assimilation", "batch", "Case", "read_case", "write_case",
-           "SpModel", "Sw2dError", "Batch"]
+__all__ = ["case", "mesh", "workloads", "capi", "solver", "assimilation", "batch", "porosity", "Case", "read_case",
+           "write_case", "SpModel", "Sw2dError", "Batch"]
