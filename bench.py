@@ -61,6 +61,11 @@ def _args():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-every", type=int, default=50, help="checkpoint interval of the ensemble adjoints")
     ap.add_argument("--dip-steps", type=int, default=200)
+    ap.add_argument("--assim-cells", type=int, default=1_000_000,
+                    help="cells of the porosity-assimilation line (the reference's differentiated step; 0: skip)")
+    ap.add_argument("--assim-steps", type=int, default=2000, help="approximate steps of its trajectory")
+    ap.add_argument("--assim-only", action="store_true",
+                    help="print only the porosity-assimilation measurement (one JSON line)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint measurement (one JSON line), e.g. for profiling")
     ap.add_argument("--launch-config", default=None,
@@ -289,6 +294,120 @@ def run_adjoint(pkg, args, local_rank):
     }
 
 
+def run_assim(pkg, args, local_rank):
+    """Porosity assimilation with the reference's differentiated step (sw2d_assim_*): the gradient
+    dJ/dphi of get_spatial_gradient_checkpointed.
+    * sp_toce, the reference's own case (tests/golden/sp_toce_assim.npz: 4,800 cells, 3,157 steps,
+      41 full-field observations, 48 tiles): the GPU's dry run, replayed cost and gradient, and the
+      reference's own dry run and replayed cost on this host's CPU (its library built from its
+      sources, oracle/_ref), which a gradient costs at least.  The reference's gradient itself
+      needs Enzyme, absent here.
+    * the dam-break construction at `--assim-cells` cells (MUSCL-EVR + HLLC, phi ~ U[0.6, 1]),
+      32 gauges observed every 10 steps' worth of time, about `--assim-steps` steps, checkpoints
+      every 100: dry run, replayed cost and gradient, CUDA events on the library's stream."""
+    import numpy as np
+    import torch
+
+    from tests.conftest import GOLDEN, sp_toce_case
+    from tests.golden.make_assim_golden import decimals_to_float
+
+    def timed(model, fn):
+        stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    out = {}
+    # sp_toce
+    case, _ = sp_toce_case()
+    ax = np.load(os.path.join(GOLDEN, "sp_toce_assim.npz"))
+    cfg = json.loads(str(ax["config"]))
+    frames = decimals_to_float(ax["obs_mant"], ax["obs_exp"])
+    model = pkg.SpModel(case, device=local_rank)
+    model.assim_configure(phi_transform="none", windowed=True, window_duration=cfg["window_duration"],
+                          n_windows=int(cfg["n_windows"]), t_state_assimilation=cfg["t_state_assimilation"],
+                          cost_normalize=True)
+    model.assim_set_frames(ax["obs_times"], frames)
+    m = ax["m"]
+    stride = int(cfg["checkpoint_stride"])
+    (ns, nk), ms_rec = timed(model, lambda: model.assim_record(m, stride))
+    J, ms_rep = timed(model, lambda: model.assim_replay_cost(m))
+    ms_grads = []
+    for _ in range(3):
+        (g, info), ms = timed(model, lambda: model.assim_gradient(m, stride))
+        ms_grads.append(ms)
+    toce = {"cells": case.mesh.cell_nb, "steps": ns, "segments": nk, "tiles": info["n_tiles"],
+            "ms_record": ms_rec, "ms_replay_cost": ms_rep, "ms_per_gradient": min(ms_grads), "J": J,
+            "J_reference_same_libm": float(ax["J_pm"])}
+    try:
+        from oracle.binding import RefE, REF_E_SO
+        if os.path.exists(REF_E_SO):
+            import tempfile
+            with tempfile.TemporaryDirectory() as tmp:
+                pkg.write_case(tmp, case)
+                ref = RefE(tmp)
+                ref.set_frames(ax["obs_times"], frames)
+                ref.set_window_keys(True, cfg["window_duration"], -1, int(cfg["n_windows"]), cfg["t_state_assimilation"])
+                ref.set_options(True, 0, 1.0)
+                t0 = time.perf_counter()
+                ref.record(m, stride)
+                t1 = time.perf_counter()
+                ref.set_window()
+                Jr = ref.replay_cost(m)
+                t2 = time.perf_counter()
+                ref.close()
+            toce["reference_cpu"] = {"ms_record": 1e3 * (t1 - t0), "ms_replay_cost": 1e3 * (t2 - t1), "J": Jr,
+                                     "cores": 1, "gradient": "unavailable: the reference differentiates with Enzyme "
+                                                             "(clang-18 plugin), absent here"}
+            toce["speedup_replay_vs_reference_cpu"] = (t2 - t1) * 1e3 / ms_rep
+            toce["speedup_gradient_vs_reference_cpu_replay"] = (t2 - t1) * 1e3 / min(ms_grads)
+    except Exception as exc:  # the reference library is optional at bench time
+        toce["reference_cpu"] = {"unavailable": str(exc)}
+    out["sp_toce"] = toce
+    del model
+    # dam-break construction at scale
+    n_req = args.assim_cells
+    case = pkg.workloads.dam_break(n_cells=n_req, scheme="muscl_evr", friction="none")
+    n = case.mesh.cell_nb
+    probe = pkg.SpModel(case, device=local_rank)
+    probe.step(3)
+    dt = probe.dt
+    del probe
+    t_end = args.assim_steps * dt
+    case.opts["t_max"] = t_end
+    free0, _ = torch.cuda.mem_get_info(local_rank)
+    model = pkg.SpModel(case, device=local_rank)
+    model.assim_configure(phi_transform="none", cost_normalize=True)
+    rng = np.random.default_rng(5)
+    gauges = np.sort(rng.choice(n, size=32, replace=False))
+    times = np.arange(1, args.assim_steps // 10 + 1) * (10 * dt)
+    model.assim_set_gauges(times, gauges, np.ones(32), case.h0[gauges][None, :] * np.ones((len(times), 1)))
+    m = case.phi.copy()
+    (ns, nk), ms_rec = timed(model, lambda: model.assim_record(m, 100))
+    J, ms_rep = timed(model, lambda: model.assim_replay_cost(m))
+    grads = []
+    for _ in range(2):
+        (g, info), ms = timed(model, lambda: model.assim_gradient(m, 100))
+        grads.append(ms)
+    free1, _ = torch.cuda.mem_get_info(local_rank)
+    ms_grad = min(grads)
+    out.update({
+        "workload": f"dam break construction at {n} cells, MUSCL-EVR + HLLC with the reference's differentiated "
+                    f"step, phi ~ U[0.6, 1]; 32 gauges every 10 steps' time; {ns} steps, checkpoints every 100",
+        "metric": "porosity gradients/s", "value": 1e3 / ms_grad, "unit": "gradients/s",
+        "ms_per_gradient": ms_grad, "ms_record": ms_rec, "ms_replay_cost": ms_rep,
+        "ratio_gradient_to_replay": ms_grad / ms_rep, "cell_updates_per_s_replay": n * ns / (ms_rep / 1e3),
+        "J": J, "nonfinite_entries_set_to_zero": int(info["n_nonfinite"]),
+        "device_memory_gb": (free0 - free1) / 1e9,
+        "check": "record and replay bit for bit against the reference's own layer, gradient against its central "
+                 "differences: tests/test_gpu_assim.py",
+    })
+    return out
+
+
 def run_dip(pkg, args, local_rank):
     """The dual integral porosity forward step on the DIP feature channel at `--dip-cells`
     cells (MUSCL-EVR, HLLC, Manning, momentum dissipation, q inflow, fr outflow), graph-launched
@@ -385,6 +504,15 @@ def run_ensemble(pkg, args, local_rank):
         "device_memory_in_use_gb": (total - free) / 1e9,
         "timing": "host wall time around synchronous calls, both arms alike",
     }
+
+
+def run_assim_only(args, local_rank):
+    import torch
+
+    pkg = importlib.import_module(PKG)
+    pkg.build.build()
+    torch.cuda.set_device(local_rank)
+    print(json.dumps(run_assim(pkg, args, local_rank)))
 
 
 def run_adjoint_only(args, local_rank):
@@ -497,6 +625,7 @@ def run_ours(args, rank, world, local_rank):
         return
     adjoint = None if (args.no_adjoint or world > 1) else run_adjoint(pkg, args, local_rank)
     dip = None if (args.dip_cells <= 0 or world > 1) else run_dip(pkg, args, local_rank)
+    assim = None if (args.assim_cells <= 0 or world > 1) else run_assim(pkg, args, local_rank)
     ensemble = None if (args.ensemble_members <= 0 or world > 1) else run_ensemble(pkg, args, local_rank)
 
     steps = args.steps
@@ -536,6 +665,8 @@ def run_ours(args, rank, world, local_rank):
         line["adjoint"] = adjoint
     if dip is not None:
         line["dip"] = dip
+    if assim is not None:
+        line["assim"] = assim
     if ensemble is not None:
         line["ensemble"] = ensemble
     print(json.dumps(line))
@@ -551,6 +682,9 @@ def main():
     elif args.adjoint_only:
         if rank == 0:
             run_adjoint_only(args, local_rank)
+    elif args.assim_only:
+        if rank == 0:
+            run_assim_only(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
