@@ -279,5 +279,5 @@ def test_toce_minimization_descends(pkg, tmp_path):
     assert rows[0] == pkg.porosity.DESCENT_COLUMNS
     assert rows[1].split(",")[1] == f"{float(ax['J_pm']):.10e}"   # the log keeps 11 significant digits
     print("sp_toce descent:", [round(j, 6) for j in res["history"]])
-    assert res["J_final"] < 0.97 * res["J_init"]
+    assert res["J_final"] < 0.99 * res["J_init"]
     assert np.all((res["phi"] >= 0.0) & (res["phi"] <= 1.0))
