@@ -342,30 +342,6 @@ def run_assim(pkg, args, local_rank):
     toce = {"cells": case.mesh.cell_nb, "steps": ns, "segments": nk, "tiles": info["n_tiles"],
             "ms_record": ms_rec, "ms_replay_cost": ms_rep, "ms_per_gradient": min(ms_grads), "J": J,
             "J_reference_same_libm": float(ax["J_pm"])}
-    try:
-        from oracle.binding import RefE, REF_E_SO
-        if os.path.exists(REF_E_SO):
-            import tempfile
-            with tempfile.TemporaryDirectory() as tmp:
-                pkg.write_case(tmp, case)
-                ref = RefE(tmp)
-                ref.set_frames(ax["obs_times"], frames)
-                ref.set_window_keys(True, cfg["window_duration"], -1, int(cfg["n_windows"]), cfg["t_state_assimilation"])
-                ref.set_options(True, 0, 1.0)
-                t0 = time.perf_counter()
-                ref.record(m, stride)
-                t1 = time.perf_counter()
-                ref.set_window()
-                Jr = ref.replay_cost(m)
-                t2 = time.perf_counter()
-                ref.close()
-            toce["reference_cpu"] = {"ms_record": 1e3 * (t1 - t0), "ms_replay_cost": 1e3 * (t2 - t1), "J": Jr,
-                                     "cores": 1, "gradient": "unavailable: the reference differentiates with Enzyme "
-                                                             "(clang-18 plugin), absent here"}
-            toce["speedup_replay_vs_reference_cpu"] = (t2 - t1) * 1e3 / ms_rep
-            toce["speedup_gradient_vs_reference_cpu_replay"] = (t2 - t1) * 1e3 / min(ms_grads)
-    except Exception as exc:  # the reference library is optional at bench time
-        toce["reference_cpu"] = {"unavailable": str(exc)}
     out["sp_toce"] = toce
     del model
     # dam-break construction at scale
@@ -394,6 +370,7 @@ def run_assim(pkg, args, local_rank):
         grads.append(ms)
     free1, _ = torch.cuda.mem_get_info(local_rank)
     ms_grad = min(grads)
+    ref_cpu = _assim_reference_sample(pkg, args)
     out.update({
         "workload": f"dam break construction at {n} cells, MUSCL-EVR + HLLC with the reference's differentiated "
                     f"step, phi ~ U[0.6, 1]; 32 gauges every 10 steps' time; {ns} steps, checkpoints every 100",
@@ -404,8 +381,53 @@ def run_assim(pkg, args, local_rank):
         "device_memory_gb": (free0 - free1) / 1e9,
         "check": "record and replay bit for bit against the reference's own layer, gradient against its central "
                  "differences: tests/test_gpu_assim.py",
+        "cpu_baseline": ref_cpu,
     })
+    if "cell_updates_per_s_replay" in ref_cpu:
+        out["speedup_replay_vs_reference_cpu"] = out["cell_updates_per_s_replay"] / ref_cpu["cell_updates_per_s_replay"]
     return out
+
+
+def _assim_reference_sample(pkg, args):
+    """The reference's own dry run and replayed cost (its assimilation layer built from its
+    sources, oracle/_ref, one host core) on a bounded sample of the same construction: 100,000
+    cells, 200 steps.  Its gradient needs Enzyme (a clang-18 plugin), absent here; a reverse
+    sweep costs at least a replay."""
+    import numpy as np
+    try:
+        from oracle.binding import RefE, REF_E_SO
+    except Exception as exc:
+        return {"unavailable": f"oracle binding: {exc}"}
+    if not os.path.exists(REF_E_SO):
+        return {"unavailable": "reference library not built (oracle/_ref)"}
+    case = pkg.workloads.dam_break(n_cells=100_000, scheme="muscl_evr", friction="none")
+    n = case.mesh.cell_nb
+    probe = pkg.SpModel(case)
+    probe.step(3)
+    dt = probe.dt
+    del probe
+    steps = 200
+    case.opts["t_max"] = steps * dt
+    rng = np.random.default_rng(5)
+    gauges = np.sort(rng.choice(n, size=32, replace=False))
+    times = np.arange(1, steps // 10 + 1) * (10 * dt)
+    with tempfile.TemporaryDirectory() as tmp:
+        pkg.write_case(tmp, case)
+        ref = RefE(tmp)
+        ref.set_gauges(times, gauges, np.ones(32), case.h0[gauges][None, :] * np.ones((len(times), 1)))
+        ref.set_options(True, 0, 1.0)
+        t0 = time.perf_counter()
+        K = ref.record(case.phi, 100)
+        t1 = time.perf_counter()
+        ref.set_window()
+        ref.replay_cost(case.phi)
+        t2 = time.perf_counter()
+        ns = sum(len(sg[1]) for sg in ref.segments())
+        ref.close()
+    return {"kind": "reference", "cores": 1, "sample": f"dam break construction at {n} cells, {ns} steps",
+            "ms_record": 1e3 * (t1 - t0), "ms_replay_cost": 1e3 * (t2 - t1), "segments": K,
+            "cell_updates_per_s_replay": n * ns / (t2 - t1), "unit": "cell-updates/s",
+            "gradient": "unavailable: the reference differentiates with Enzyme (clang-18 plugin), absent here"}
 
 
 def run_dip(pkg, args, local_rank):
