@@ -54,3 +54,21 @@ def test_reverse_matches_central_differences(results, name):
     n, fail, worst = results[name]
     assert n >= 500, f"{name}: only {n} samples"
     assert fail <= max(1, int(0.002 * n)), f"{name}: {fail} of {n} samples differ (worst relative error {worst:.2e})"
+
+
+STEP_SRC = os.path.join(ROOT, "tests", "spe_step_check.cpp")
+
+
+def test_whole_steps_match_central_differences(tmp_path):
+    """tests/spe_step_check.cpp: 12 steps of the _E step on a small triangulated channel, composed
+    as the CUDA kernels compose them, and their reverse composed as the reverse kernels: the
+    gradient of a misfit with respect to porosity and the initial depth against central
+    differences (Godunov and MUSCL-EVR, 6 seeded trials x 3 directions each)."""
+    exe = str(tmp_path / "spe_step_check")
+    subprocess.run([_compiler(), "-O2", "-std=c++17", "-ffp-contract=off", "-I", CSRC, STEP_SRC, "-o", exe], check=True,
+                   capture_output=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    res = {ln.split()[0]: ln.split()[1:] for ln in out.splitlines()}
+    assert sorted(res) == ["step_godunov", "step_muscl_evr"]
+    for name, (n, fail, worst) in res.items():
+        assert int(n) >= 18 and int(fail) == 0, f"{name}: {fail} of {n} differ (worst {worst})"
