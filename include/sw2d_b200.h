@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SW2D_ABI_VERSION 2
+#define SW2D_ABI_VERSION 3
 
 /* status codes */
 #define SW2D_OK 0
@@ -49,6 +49,8 @@ extern "C" {
 #define SW2D_E_NO_DEVICE (-9)    /* no usable CUDA device                                    */
 #define SW2D_E_PHIG (-10)        /* DIP connectivity porosity < 1e-16 in a specific force:
                                     src/sw2dSolver/models/dip/swDip.cpp:1524-1528            */
+#define SW2D_E_DDP_TABLE (-11)   /* DDP: NaN elevation or volume in a porosity-table lookup, where
+                                    the reference indexes level -1 (swDdp.cpp:1090-1096, 3382-3386) */
 
 /* enumerations of the input.solv string keys (src/sw2dSolver/common/swSolverParam.h:130-153) */
 enum sw2d_scheme { SW2D_SCHEME_GODUNOV = 0, SW2D_SCHEME_MUSCL_EVR = 1 };
@@ -157,6 +159,71 @@ typedef struct sw2d_dip_fields {
 int sw2d_create_dip(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
                     const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
                     const double* r0, int device, sw2d_handle** out);
+
+/* The depth-dependent porosity (DDP) model (model_hyperb ddp, src/sw2dSolver/models/ddp/).
+ *
+ * A porosity-law record is one line of a DDP map file as swDdp::readPorosityFile reads it
+ * (swDdp.cpp:1289-1481): {law type, n, parameters...}.  Law types (swDdp.cpp:1787-1935):
+ *   -2  n couples (z_k, phi_k) used as they are;   -1  n couples re-tabulated on n_por_tab_max levels;
+ *    0  n levels z_k, phi rising linearly 0 -> 1;   1  {z_0, phi}: uniform phi from z_0;
+ *    2  {z_0, phi_0, z_1, phi_1} linear;            3  the same plus phi_2 above z_1.
+ * Elevations are relative to the cell's bottom z_b or to the edge's midpoint elevation.
+ * Record k is values[offset[k] .. offset[k+1]). */
+typedef struct sw2d_ddp_records {
+    const int64_t* offset;  /* [records + 1] */
+    const double* values;
+} sw2d_ddp_records;
+
+enum sw2d_div_corr { SW2D_DIV_CORR_NONE = 0, SW2D_DIV_CORR_LIMIT_FLUX = 1, SW2D_DIV_CORR_LIMIT_TIMESTEP = 2 };
+
+/* initial-condition columns (swDdp::setInitialConditions, swDdp.cpp:1608-1726): the level array
+ * holds "h" (depth above the cell's lowest tabulated level) unless LEVEL_Z ("z"); the x and y
+ * arrays hold unit discharges "q", "r" unless X_VELOCITY / Y_VELOCITY ("u", "v") */
+#define SW2D_DDP_IC_LEVEL_Z 1
+#define SW2D_DDP_IC_X_VELOCITY 2
+#define SW2D_DDP_IC_Y_VELOCITY 4
+
+typedef struct sw2d_ddp_fields {
+    sw2d_ddp_records cell;          /* DDP_cell_porosity_map.txt      [cell_nb records]     */
+    sw2d_ddp_records edge_int;      /* DDP_edge_int_porosity_map.txt  [edge_int_nb records] */
+    sw2d_ddp_records edge_bnd;      /* DDP_edge_bnd_porosity_map.txt  [edge_bnd_nb records] */
+    const double* edge_int_mz;      /* [edge_int_nb] edge midpoint elevation (swEdgeIntern::getZM) */
+    const double* edge_bnd_mz;      /* [edge_bnd_nb] (swEdgeBoundary::getZM)                      */
+    int64_t n_por_tab_max;          /* n_por_tab_max (default 5)                                  */
+    double h_min_ddp;               /* h_min_ddp (default 1e-3)                                   */
+    double chi_phi_max;             /* ddp_chi_phi_max (default 20)                               */
+    double chi_theta_max;           /* ddp_chi_theta_max: read by the reference, unused in its step */
+    int32_t div_corr;               /* enum sw2d_div_corr (div_corr)                              */
+    int32_t ic_columns;             /* SW2D_DDP_IC_* bits                                         */
+    int64_t n_it_div_max;           /* n_it_div_max (default 10)                                  */
+    int32_t momentum_dissipation;   /* 0 none, 1 active (model_momentum_dissipation)              */
+    int32_t pad;
+    const double* mu_1;             /* [cell_nb] cell_momentum_dissipation_map.txt; NULL when inactive */
+    const double* mu_2;
+    const double* mu_alpha;         /* degrees */
+} sw2d_ddp_fields;
+
+/* Replaces swParent::create + swDdp::init (swParent.cpp:125-173, ddp/swDdp.cpp:780-991) for
+ * model_hyperb ddp: tabulates the porosity laws as swDdp::setPorosityParameters does, checks them
+ * as swDdp::checkParameterConsistency does (phi in [0,1], an edge's phi not above its cells' at
+ * the same level), converts the initial conditions to the model's state (thetaW, thetaW*u,
+ * thetaW*v) and sets t = t_0.  fields->phi is not read; boussinesq, friction and head-loss maps
+ * are as for SP.  The step (ddp/swDdpHyp.cpp) is Godunov with the discontinuous topography only,
+ * as in the reference (scheme and topo must say so); boundary types q, h, z, fr.
+ * On a DDP handle sw2d_get_state / sw2d_set_state carry (thetaW, thetaW_velocity_x,
+ * thetaW_velocity_y), the members of swDdp (swDdp.h:199-201); sw2d_get_array adds
+ * "water_depth", "unit_discharge_x", "unit_discharge_y", "surface_elevation" (the map outputs of
+ * swDdp::storeResultMaps, swDdp.cpp:2489-2513) and "thetaG_int_hmin". */
+int sw2d_create_ddp(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                    const sw2d_ddp_fields* ddp, const sw2d_bc_table* bc, const double* ic_level, const double* ic_x,
+                    const double* ic_y, int device, sw2d_handle** out);
+
+/* The tabulated porosity law of one record, as swDdp keeps it (cell_z_tab / phiW_tab /
+ * thetaW_tab, edge_int_z_tab / phiG_int_tab / thetaG_int_tab, edge_bnd_*; swDdp.h:243-281):
+ * which = 0 cells, 1 internal edges, 2 boundary edges; record in the caller's numbering.
+ * Writes min(levels, capacity) values to each non-NULL array; returns the level count, < 0 on error. */
+int64_t sw2d_ddp_get_table(sw2d_handle* h, int which, int64_t record, double* z, double* phi, double* theta,
+                           int64_t capacity);
 
 /* Advances at most n_steps passes of the body of swSp::execute's time loop
  * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),

@@ -61,6 +61,23 @@ class Sw2dDipFields(ctypes.Structure):
                 ("mu_1", c_double_p), ("mu_2", c_double_p), ("mu_alpha", c_double_p)]
 
 
+class Sw2dDdpRecords(ctypes.Structure):
+    _fields_ = [("offset", c_int64_p), ("values", c_double_p)]
+
+
+class Sw2dDdpFields(ctypes.Structure):
+    _fields_ = [("cell", Sw2dDdpRecords), ("edge_int", Sw2dDdpRecords), ("edge_bnd", Sw2dDdpRecords),
+                ("edge_int_mz", c_double_p), ("edge_bnd_mz", c_double_p), ("n_por_tab_max", ctypes.c_int64),
+                ("h_min_ddp", ctypes.c_double), ("chi_phi_max", ctypes.c_double), ("chi_theta_max", ctypes.c_double),
+                ("div_corr", ctypes.c_int32), ("ic_columns", ctypes.c_int32), ("n_it_div_max", ctypes.c_int64),
+                ("momentum_dissipation", ctypes.c_int32), ("pad", ctypes.c_int32), ("mu_1", c_double_p),
+                ("mu_2", c_double_p), ("mu_alpha", c_double_p)]
+
+
+DIV_CORR = {"none": 0, "limit_flux": 1, "limit_timestep": 2}
+DDP_IC_LEVEL_Z, DDP_IC_X_VELOCITY, DDP_IC_Y_VELOCITY = 1, 2, 4
+
+
 class Sw2dObs(ctypes.Structure):
     _fields_ = [("n_points", ctypes.c_int64), ("cells", c_int64_p), ("w_h", c_double_p), ("w_q", c_double_p),
                 ("n_times", ctypes.c_int64), ("steps", c_int64_p), ("h_obs", c_double_p), ("q_obs", c_double_p),
@@ -108,6 +125,7 @@ class NativeInputs:
     r0: np.ndarray
     keep: List[np.ndarray]
     dip: Optional[Sw2dDipFields] = None
+    ddp: Optional[Sw2dDdpFields] = None
 
 
 def params_from_opts(opts) -> Sw2dParams:
@@ -123,8 +141,10 @@ def params_from_opts(opts) -> Sw2dParams:
         raise ValueError(f"topo_discretization {topo!r} not recognised")
     if fric not in FRICTIONS:
         raise ValueError(f"model_friction {fric!r} not handled")
-    if str(opts.get("div_corr", "none")).lower() != "none":
-        raise ValueError("div_corr other than 'none' is outside the implemented path")
+    model = str(opts.get("model_hyperb", "sp")).lower()
+    if model != "ddp" and str(opts.get("div_corr", "none")).lower() != "none":
+        raise ValueError("div_corr other than 'none' is outside the SP/DIP path (the reference's SP and DIP "
+                         "steps ignore it)")
     return Sw2dParams(
         scheme=SCHEMES[scheme], topo=TOPOS[topo], friction=FRICTIONS[fric],
         singular_head_loss=int(str(opts.get("model_singular_head_loss", "none")).lower() != "none"),
@@ -181,7 +201,43 @@ def native_inputs(case: Case) -> NativeInputs:
         diss = str(case.opts.get("model_momentum_dissipation", "none")).lower() == "active"
         dip = Sw2dDipFields(d(case.phi_g_int), d(case.phi_g_bnd), 1 if diss else 0,
                             d(mu[0]) if diss else null, d(mu[1]) if diss else null, d(mu[2]) if diss else null)
-    return NativeInputs(mesh, params, fields, bc, h0, q0, r0, keep, dip)
+    ddp = None
+    if case.is_ddp:
+        ddp = ddp_fields(case, keep)
+    return NativeInputs(mesh, params, fields, bc, h0, q0, r0, keep, dip, ddp)
+
+
+def ddp_fields(case: Case, keep: List[np.ndarray]) -> Sw2dDdpFields:
+    """input.solv DDP keys and maps -> sw2d_ddp_fields (defaults of swSolverParam.h:161-181;
+    h_min_ddp has no input.solv key in the reference and stays 1e-3)."""
+    o = case.opts
+    m = case.mesh
+
+    def recs(lr):
+        off = np.ascontiguousarray(lr.offset, dtype=np.int64)
+        val = np.ascontiguousarray(lr.values, dtype=np.float64)
+        keep.extend([off, val])
+        return Sw2dDdpRecords(off.ctypes.data_as(c_int64_p), _dp(val))
+
+    def d(a):
+        arr = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(arr)
+        return _dp(arr)
+
+    div = str(o.get("div_corr", "none")).lower()
+    if div not in DIV_CORR:
+        raise ValueError(f"div_corr {div!r} not in {sorted(DIV_CORR)}")
+    level, xcol, ycol = case.ddp_ic
+    cols = (DDP_IC_LEVEL_Z if level == "z" else 0) | (DDP_IC_X_VELOCITY if xcol == "u" else 0) | \
+           (DDP_IC_Y_VELOCITY if ycol == "v" else 0)
+    diss = str(o.get("model_momentum_dissipation", "none")).lower() == "active"
+    null = c_double_p()
+    mu = case.mu
+    return Sw2dDdpFields(recs(case.ddp_cell), recs(case.ddp_edge_int), recs(case.ddp_edge_bnd), d(m.edge_int_mz),
+                         d(m.edge_bnd_mz), int(o.get("n_por_tab_max", 5)), float(o.get("h_min_ddp", 1e-3)),
+                         float(o.get("ddp_chi_phi_max", 20.0)), float(o.get("ddp_chi_theta_max", 20.0)),
+                         DIV_CORR[div], cols, int(o.get("n_it_div_max", 10)), 1 if diss else 0, 0,
+                         d(mu[0]) if diss else null, d(mu[1]) if diss else null, d(mu[2]) if diss else null)
 
 
 _LIB = None
@@ -205,6 +261,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                     ctypes.POINTER(Sw2dBcTable), c_double_p, c_double_p, c_double_p, ctypes.c_int,
                                     ctypes.POINTER(P)]
     lib.sw2d_create_dip.restype = ctypes.c_int
+    lib.sw2d_create_ddp.argtypes = [ctypes.POINTER(Sw2dMesh), ctypes.POINTER(Sw2dParams),
+                                    ctypes.POINTER(Sw2dCellFields), ctypes.POINTER(Sw2dDdpFields),
+                                    ctypes.POINTER(Sw2dBcTable), c_double_p, c_double_p, c_double_p, ctypes.c_int,
+                                    ctypes.POINTER(P)]
+    lib.sw2d_create_ddp.restype = ctypes.c_int
+    lib.sw2d_ddp_get_table.argtypes = [P, ctypes.c_int, ctypes.c_int64, c_double_p, c_double_p, c_double_p,
+                                       ctypes.c_int64]
+    lib.sw2d_ddp_get_table.restype = ctypes.c_int64
     lib.sw2d_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
     lib.sw2d_step_n.restype = ctypes.c_int
     lib.sw2d_execute.argtypes = [P, c_int64_p]
@@ -310,7 +374,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 # every symbol include/sw2d_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_table", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",

@@ -332,6 +332,163 @@ def read_map(path: str, n_params: int, n_records: int):
 
 
 # ---------------------------------------------------------------------------------------
+# DDP porosity-law maps (DDP_cell_porosity_map.txt, DDP_edge_int/_bnd_porosity_map.txt)
+# ---------------------------------------------------------------------------------------
+# record length by law type, the count n included (swDdp::porosityLineSize, swDdp.cpp:1099-1211)
+def _law_length(law: float, n: float) -> int:
+    if law in (-2.0, -1.0):
+        return 2 * int(n) + 2
+    if law == 0.0:
+        return int(n) + 2
+    if law == 1.0:
+        return 4
+    if law == 2.0:
+        return 6
+    if law == 3.0:
+        return 7
+    raise ValueError(f"porosity law type {law!r} not in {{-2, -1, 0, 1, 2, 3}}")
+
+
+@dataclass
+class LawRecords:
+    """Porosity-law records of one DDP map: record k is ``values[offset[k]:offset[k+1]]`` =
+    {law type, n, parameters...} as swDdp::readPorosityFile reads a line (swDdp.cpp:1289-1481)."""
+
+    offset: np.ndarray   # (n_records + 1,) int64
+    values: np.ndarray   # float64
+
+    @classmethod
+    def uniform(cls, record: Sequence[float], n_records: int) -> "LawRecords":
+        rec = np.asarray(record, dtype=np.float64)
+        return cls(np.arange(n_records + 1, dtype=np.int64) * rec.size, np.tile(rec, n_records))
+
+    @classmethod
+    def from_list(cls, records: Sequence[Sequence[float]]) -> "LawRecords":
+        lens = np.array([len(r) for r in records], dtype=np.int64)
+        off = np.zeros(len(records) + 1, dtype=np.int64)
+        np.cumsum(lens, out=off[1:])
+        vals = np.concatenate([np.asarray(r, dtype=np.float64) for r in records]) if records else np.zeros(0)
+        return cls(off, vals)
+
+    @property
+    def count(self) -> int:
+        return int(self.offset.shape[0] - 1)
+
+    def record(self, k: int) -> np.ndarray:
+        return self.values[self.offset[k]:self.offset[k + 1]]
+
+    def is_uniform(self) -> bool:
+        if self.count == 0:
+            return True
+        lens = np.diff(self.offset)
+        if np.any(lens != lens[0]):
+            return False
+        return bool(np.all(self.values.reshape(self.count, -1) == self.record(0)[None, :]))
+
+
+def _law_token(v: float, k: int) -> str:
+    # law type and count are read with stringToInt: write them as integers
+    return str(int(v)) if k < 2 else repr(float(v))
+
+
+def write_porosity_laws(path: str, laws: LawRecords) -> None:
+    """Writes a DDP porosity map (the layout swDdp::readPorosityFile reads, swDdp.cpp:1289-1481):
+    ``Unif 1`` with one record when all records are equal, else ``Unif 0`` and one line per record."""
+    uniform = laws.is_uniform()
+    with open(path, "w") as fh:
+        fh.write(f"Unif\t{1 if uniform else 0}\n==== Default Param\n")
+        fh.write("law_type\tn\tparameters\n")
+        first = laws.record(0) if laws.count else np.array([1.0, 2.0, 0.0, 1.0])
+        line0 = "\t".join(_law_token(v, k) for k, v in enumerate(first.tolist()))
+        if uniform:
+            fh.write(line0 + "\n")
+            return
+        fh.write(line0 + "\n==== Distrib\n")
+        out = []
+        for k in range(laws.count):
+            out.append("\t".join(_law_token(v, j) for j, v in enumerate(laws.record(k).tolist())))
+        fh.write("\n".join(out) + "\n")
+
+
+def read_porosity_laws(path: str, n_records: int) -> LawRecords:
+    """Reads a DDP porosity map as swDdp::readPorosityFile does, with its per-line length check."""
+    with open(path) as fh:
+        lines = [ln.rstrip("\r\n") for ln in fh]
+    head = _TOKEN.findall(lines[0])
+    if len(head) != 2 or head[1] not in ("0", "1"):
+        raise ValueError(f"{path}: bad 'Unif' line")
+
+    def parse(ln: str) -> List[float]:
+        tok = _TOKEN.findall(ln)
+        vals = [float(t) for t in tok]
+        if len(vals) < 2:
+            raise ValueError(f"{path}: misformatted line {ln!r}")
+        if len(vals) != _law_length(vals[0], vals[1]):
+            raise ValueError(f"{path}: law type {vals[0]} is not compatible with {len(vals) - 1} parameters")
+        return vals
+
+    if head[1] == "1":
+        return LawRecords.uniform(parse(lines[3]), n_records)
+    body = lines[5:5 + n_records]
+    if len(body) < n_records:
+        raise ValueError(f"{path}: not enough records ({len(body)} < {n_records})")
+    return LawRecords.from_list([parse(ln) for ln in body])
+
+
+def ddp_law_table(record: Sequence[float], base: float, n_por_tab_max: int):
+    """(z_tab, phi_tab, theta_tab) of one porosity-law record, restating swDdp::setPorosityCellMap
+    (swDdp.cpp:1787-1935) and swDdp::tabulatePorosity (swDdp.cpp:2596-2645) operation for
+    operation (Python floats are binary64, evaluated in the reference's order).  Raises where the
+    reference would read outside its point list."""
+    rec = [float(v) for v in record]
+    law, ntab = rec[0], int(n_por_tab_max)
+
+    def tabulate(z, phi):
+        nv = len(z)
+        dz = (z[nv - 1] - z[0]) / float(ntab - 1)
+        zt = [z[0] + float(lv) * dz for lv in range(ntab)]
+        interp = [0.0] * ntab
+        index = 0
+        for lv in range(1, ntab):
+            while zt[lv] > z[index]:
+                index += 1
+                if index >= nv:
+                    raise ValueError("tabulated level above the last point")
+            if index == 0:
+                raise ValueError("points not increasing")
+            interp[lv] = phi[index - 1] + (phi[index] - phi[index - 1]) * (zt[lv] - z[index - 1]) / (z[index] - z[index - 1])
+        pt = [(interp[lv + 1] + interp[lv]) * 0.5 for lv in range(ntab - 1)] + [phi[nv - 1]]
+        return zt, pt
+
+    if law in (-2.0, -1.0):
+        nc = int(rec[1])
+        z = [base + rec[2 + 2 * k] for k in range(nc)]
+        phi = [rec[3 + 2 * k] for k in range(nc)]
+        zt, pt = (z, phi) if law == -2.0 else tabulate(z, phi)
+    elif law == 0.0:
+        nl = int(rec[1])
+        zt, pt = tabulate([base + rec[2 + k] for k in range(nl)], [float(k) * 1.0 / float(nl - 1) for k in range(nl)])
+    elif law == 1.0:
+        z = base + rec[2]
+        zt, pt = tabulate([z, z + 1.0], [rec[3], rec[3]])
+        pt[0] = rec[3]
+    elif law in (2.0, 3.0):
+        z0, z1 = base + rec[2], base + rec[4]
+        phi0, phi1 = rec[3], rec[5]
+        dz = (z1 - z0) / float(ntab - 1)
+        dphi = (phi1 - phi0) / float(ntab - 1)
+        zt = [z0 + float(lv) * dz for lv in range(ntab - 1)] + [z1]
+        pt = [phi0 + (float(lv) + 0.5) * dphi for lv in range(ntab - 1)] + [phi1 if law == 2.0 else rec[6]]
+    else:
+        raise ValueError(f"porosity law type {law!r} not in {{-2, -1, 0, 1, 2, 3}}")
+    theta, th = [0.0], 0.0
+    for lv in range(1, len(zt)):
+        th += (zt[lv] - zt[lv - 1]) * pt[lv - 1]
+        theta.append(th)
+    return np.array(zt), np.array(pt), np.array(theta)
+
+
+# ---------------------------------------------------------------------------------------
 # boundary time series
 # ---------------------------------------------------------------------------------------
 BC_TYPES = {"q": 0, "h": 1, "z": 2, "fr": 3, "phiWq": 4}   # phiWq: DIP only (dip/swDipHyp.cpp:88-101)
@@ -436,10 +593,21 @@ class Case:
     phi_g_int: Optional[np.ndarray] = None
     phi_g_bnd: Optional[np.ndarray] = None
     mu: Optional[np.ndarray] = None
+    # DDP (model_hyperb ddp): porosity laws of the cells, internal and boundary edges; phi is
+    # unused, h0/q0/r0 hold the initial-condition columns named by ddp_ic (h|z, q|u, r|v) and
+    # mu the dissipation map as for DIP
+    ddp_cell: Optional[LawRecords] = None
+    ddp_edge_int: Optional[LawRecords] = None
+    ddp_edge_bnd: Optional[LawRecords] = None
+    ddp_ic: Sequence[str] = ("h", "q", "r")
 
     @property
     def is_dip(self) -> bool:
         return str(self.opts.get("model_hyperb", "sp")).lower() == "dip"
+
+    @property
+    def is_ddp(self) -> bool:
+        return str(self.opts.get("model_hyperb", "sp")).lower() == "ddp"
 
 
 FRICTION_FILES = {"chezy": "friction_chezy_map.txt", "manning": "friction_manning_map.txt",
@@ -454,7 +622,11 @@ def write_case(folder: str, case: Case) -> None:
     write_geometry(os.path.join(inp, "geometry.sw2d"), case.mesh)
     write_solv(os.path.join(inp, "input.solv"), case.opts)
     ic_z = case.extra.get("ic_z") if case.extra else None
-    if ic_z is not None and not np.any(case.q0) and not np.any(case.r0):
+    if case.is_ddp:
+        # swDdp::setInitialConditions (swDdp.cpp:1608-1726) reads h|z, q|u, r|v
+        write_map(os.path.join(inp, "initial_conditions_map.txt"), list(case.ddp_ic),
+                  [_collapse(case.h0), _collapse(case.q0), _collapse(case.r0)], n)
+    elif ic_z is not None and not np.any(case.q0) and not np.any(case.r0):
         # uniform free surface at rest: "z u v" (swSp::setInitialConditions sets h = max(z - z_b, 0))
         write_map(os.path.join(inp, "initial_conditions_map.txt"), ["z", "u", "v"], [float(ic_z), 0.0, 0.0], n)
     else:
@@ -467,6 +639,15 @@ def write_case(folder: str, case: Case) -> None:
                   case.mesh.edge_int_nb)
         write_map(os.path.join(inp, "DIP_edge_bnd_porosity_map.txt"), ["DipPhiG"], [case.phi_g_bnd],
                   case.mesh.edge_bnd_nb)
+        if case.opts.get("model_momentum_dissipation", "none") != "none":
+            mu = case.mu
+            write_map(os.path.join(inp, "cell_momentum_dissipation_map.txt"), ["mu1", "mu2", "alpha"],
+                      [mu[0], mu[1], mu[2]], n)
+    elif case.is_ddp:
+        # swDdp::setPorosityParameters (swDdp.cpp:2241-2316)
+        write_porosity_laws(os.path.join(inp, "DDP_cell_porosity_map.txt"), case.ddp_cell)
+        write_porosity_laws(os.path.join(inp, "DDP_edge_bnd_porosity_map.txt"), case.ddp_edge_bnd)
+        write_porosity_laws(os.path.join(inp, "DDP_edge_int_porosity_map.txt"), case.ddp_edge_int)
         if case.opts.get("model_momentum_dissipation", "none") != "none":
             mu = case.mu
             write_map(os.path.join(inp, "cell_momentum_dissipation_map.txt"), ["mu1", "mu2", "alpha"],
@@ -498,6 +679,8 @@ def read_case(folder: str) -> Case:
     mesh = read_geometry(os.path.join(inp, "geometry.sw2d"))
     n = mesh.cell_nb
     names, ic = read_map(os.path.join(inp, "initial_conditions_map.txt"), 3, n)
+    if str(opts.get("model_hyperb", "sp")).lower() == "ddp":
+        return _read_ddp_case(inp, opts, mesh, names, ic)
     # swSp::setInitialConditions (swSp.cpp:1119-1224): h or z, then q or u, then r or v
     h = np.zeros(n)
     if "h" in names:
@@ -536,3 +719,34 @@ def read_case(folder: str) -> Case:
     bc = read_bc_series(os.path.join(inp, "hydro_boundary_time_series.txt"))
     return Case(mesh=mesh, opts=opts, h0=h, q0=q, r0=r, phi=phi[0].copy(), boussinesq=bous[0].copy(),
                 friction=fr, head_loss=hl, bc=bc, phi_g_int=pgi, phi_g_bnd=pgb, mu=mu)
+
+
+def _read_ddp_case(inp: str, opts: Dict[str, str], mesh: Mesh, names: List[str], ic: np.ndarray) -> Case:
+    """The DDP part of swDdp::init (swDdp.cpp:780-991): porosity laws, initial-condition columns
+    (kept as read: the conversion to thetaW needs the tables), Boussinesq, friction, head loss,
+    dissipation, boundary series."""
+    n = mesh.cell_nb
+    level = "z" if "z" in names else "h" if "h" in names else None
+    xcol = "u" if "u" in names else "q" if "q" in names else None
+    ycol = "v" if "v" in names else "r" if "r" in names else None
+    if level is None or xcol is None or ycol is None:
+        raise ValueError("initial conditions: DDP needs h|z, q|u and r|v columns")
+    cell = read_porosity_laws(os.path.join(inp, "DDP_cell_porosity_map.txt"), n)
+    ebnd = read_porosity_laws(os.path.join(inp, "DDP_edge_bnd_porosity_map.txt"), mesh.edge_bnd_nb)
+    eint = read_porosity_laws(os.path.join(inp, "DDP_edge_int_porosity_map.txt"), mesh.edge_int_nb)
+    mu = None
+    if opts.get("model_momentum_dissipation", "none") != "none":
+        _, mu = read_map(os.path.join(inp, "cell_momentum_dissipation_map.txt"), 3, n)
+    _, bous = read_map(os.path.join(inp, "Boussinesq_map.txt"), 1, n)
+    fr = None
+    fm = opts.get("model_friction", "none")
+    if fm != "none":
+        _, fr = read_map(os.path.join(inp, FRICTION_FILES[fm]), 3, n)
+    hl = None
+    if opts.get("model_singular_head_loss", "none") != "none":
+        _, hl = read_map(os.path.join(inp, "singular_head_loss_map.txt"), 4, n)
+    bc = read_bc_series(os.path.join(inp, "hydro_boundary_time_series.txt"))
+    return Case(mesh=mesh, opts=opts, h0=ic[names.index(level)].copy(), q0=ic[names.index(xcol)].copy(),
+                r0=ic[names.index(ycol)].copy(), phi=np.ones(n), boussinesq=bous[0].copy(), friction=fr,
+                head_loss=hl, bc=bc, mu=mu, ddp_cell=cell, ddp_edge_int=eint, ddp_edge_bnd=ebnd,
+                ddp_ic=(level, xcol, ycol))

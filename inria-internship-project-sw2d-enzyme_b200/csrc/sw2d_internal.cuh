@@ -12,6 +12,7 @@
 
 #include "../../include/sw2d_b200.h"
 #include "dip_math.cuh"
+#include "ddp_math.cuh"
 
 namespace sw2d {
 
@@ -20,6 +21,12 @@ constexpr int kBlock = 256;
 // porosity model of a handle
 constexpr int kModelSp = 0;
 constexpr int kModelDip = 1;
+constexpr int kModelDdp = 2;
+
+// divergence correction of the DDP step (div_corr: none | limit_flux | limit_timestep)
+constexpr int kDivCorrNone = 0;
+constexpr int kDivCorrFlux = 1;
+constexpr int kDivCorrTimestep = 2;
 
 // Device-resident loop control.  t and t_max decide whether a step runs; `go` and `dt` are
 // written by the CFL kernel's last block (or by the frozen-dt kernel of a replay) and read by
@@ -34,6 +41,8 @@ struct Ctrl {
     int go;
     int pad;
 };
+
+struct DdpCtrl;  // sw2d_ddp.cu
 
 struct DevMesh {
     int nc, ni, nb;
@@ -78,6 +87,25 @@ struct DevMesh {
     const double* phig;
     const double* phigb;
     const double4* mu;
+    // DDP: porosity tables (levels {z, phi, theta}) of the cells and of the internal edges in
+    // the internal numbering, record k holding levels [off[k], off[k+1]); the per-cell values
+    // derived from the current state {phiW(z), thetaW(z), pressure force Omega(z), -} (z in
+    // st.w); per-cell statics {phiW, thetaW at z_tab[0] + h_min; phiW, thetaW at z_tab[1] +
+    // h_min}; per internal edge two records {thetaG_hmin, z_tab[0], phiG, thetaG at the L cell's
+    // shallow level}, {phiG, thetaG at the R cell's shallow level, -, -}; the pre-balance state
+    // (divergence correction) and the loop control of the divergence correction
+    const ddp::Lvl* ctab;
+    const int* ctoff;
+    const ddp::Lvl* etab;
+    const int* etoff;
+    double4* dv;
+    const double4* dcs;
+    const double4* des;
+    double4* old;
+    DdpCtrl* dctl;
+    double chi_phi_max;
+    int div_corr;
+    int n_it_div_max;
     // parameters
     double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
     DryConsts dry;
@@ -104,6 +132,7 @@ inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBl
 
 struct AdjointState;  // sw2d_adjoint.cu
 struct AssimState;    // sw2d_assim.cu
+struct DdpState;      // sw2d_ddp.cu
 
 }  // namespace sw2d
 
@@ -112,7 +141,7 @@ struct sw2d_handle {
     cudaStream_t stream = nullptr;
     int64_t nc = 0, ni = 0, nb = 0;
     sw2d_params p{};
-    int model = 0;             // kModelSp or kModelDip
+    int model = 0;             // kModelSp, kModelDip or kModelDdp
     int dissipation = 0;       // DIP momentum dissipation active
     std::vector<int> cell_perm, int_perm, bnd_perm;  // [new] = caller index
     std::vector<void*> allocs;
@@ -137,6 +166,7 @@ struct sw2d_handle {
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step
     int assim_sqrt_zero = 0;            // option "assim_sqrt_zero"
     int assim_chained = 0;              // option "assim_chained_recompute"
+    sw2d::DdpState* ddp = nullptr;      // DDP model: tables, divergence-correction scratch
     std::string err;
 };
 
@@ -186,6 +216,88 @@ void launch_cfl_on(sw2d_handle* h, const DevMesh& m);
 void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance);
 // One whole time step of the handle (its four kernels, its launch variants) on its stream.
 void launch_step_on(sw2d_handle* h);
+
+// The CFL kernel with the DDP model's map-storage snap (swDdpHyp.cpp:588-600).
+void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m);
+// Friction, singular head loss and the velocity cap of one cell (swSpSourceFriction.cpp,
+// swSp.cpp:447-479; the DDP model applies the same formulas to thetaW and its momentum,
+// swDdpSourceFriction.cpp, swDdp.cpp:527-561).
+template <int kFriction, bool kHeadLoss>
+__device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt, double hh, double& qq, double& rr)
+{
+    const double hthr = smax(m.h_min, kSmallReal);
+    // friction (swSpSourceFriction.cpp:39-171)
+    if (kFriction != SW2D_FRICTION_NONE) {
+        if (hh > hthr) {
+            const double4 fr = ld(&m.fric[c]);
+            double u = qq / hh;
+            double v = rr / hh;
+            double ca = fr.z, sa = fr.w;
+            double ul = u * ca + v * sa;
+            double vl = -u * sa + v * ca;
+            double un = sqrt(u * u + v * v);
+            double f1 = friction_factor(kFriction, fr.x, hh, un, dt);
+            double f2 = friction_factor(kFriction, fr.y, hh, un, dt);
+            ul *= f1;
+            vl *= f2;
+            qq = (ul * ca - vl * sa) * hh;
+            rr = (ul * sa + vl * ca) * hh;
+        } else {
+            qq = 0.;
+            rr = 0.;
+        }
+    }
+    // singular head loss (swSpSourceFriction.cpp:174-219)
+    if (kHeadLoss) {
+        const double2 cs = ld(&m.hlb[c]);
+        double ca = cs.x, sa = cs.y;
+        double qx = qq * ca + rr * sa;
+        double qy = -qq * sa + rr * ca;
+        if (hh > hthr) {
+            const double4 hl = ld(&m.hla[c]);
+            double ax = 0, ay = 0;
+            if (hh > hl.x) {
+                ax = sqrt(qx * qx + qy * qy) * hl.y / hh;
+                ay = sqrt(qx * qx + qy * qy) * hl.z / hh;
+            }
+            qx = qx * sw2d_exp(-ax * dt);
+            qy = qy * sw2d_exp(-ay * dt);
+        } else {
+            qx = 0.;
+            qy = 0.;
+        }
+        qq = qx * ca - qy * sa;
+        rr = qx * sa + qy * ca;
+    }
+    // swSp::correctVelocity (swSp.cpp:447-479)
+    if (hh > m.h_min) {
+        double qn = sqrt(qq * qq + rr * rr);
+        double cc = sqrt(kGravity * hh);
+        double Fr = qn / cc / hh;
+        double fact = smax(qn / (hh * m.v_max), Fr / m.fr_max);
+        if (fact > 1.0) {
+            qq = qq / fact;
+            rr = rr / fact;
+        }
+    }
+}
+
+// DDP model (sw2d_ddp.cu): one step on the handle's stream; the per-cell values derived from
+// the state, recomputed after the state was set from outside; the DDP setup of sw2d_create_ddp.
+void launch_ddp_step(sw2d_handle* h);
+// phase i of a DDP step (0 none, 1 edges, 2 cfl, 3 the cell update and any divergence correction)
+void launch_ddp_phase(sw2d_handle* h, int i);
+void launch_ddp_edges(sw2d_handle* h, const DevMesh& m, int variant);
+int ddp_kernels_per_step(sw2d_handle* h);
+int64_t ddp_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity, bool* handled);
+int64_t ddp_get_table(sw2d_handle* h, int which, int64_t record, double* z, double* phi, double* theta,
+                      int64_t capacity);
+int ddp_derive(sw2d_handle* h);
+int ddp_setup(sw2d_handle* h, const sw2d_mesh* mesh, const sw2d_cell_fields* fields, const sw2d_ddp_fields* ddp,
+              const double* ic_level, const double* ic_x, const double* ic_y);
+void ddp_release(sw2d_handle* h);
+// Validates the DDP arguments before anything is allocated.
+int ddp_check(const sw2d_mesh* mesh, const sw2d_ddp_fields* ddp, std::string& why);
 
 // Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
 void adjoint_release(sw2d_handle* h);

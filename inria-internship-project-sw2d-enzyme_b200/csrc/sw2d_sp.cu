@@ -267,6 +267,9 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double min_keep(double a, double b) { return (b < a) ? b : a; }
 
+// kDdpSnap: the DDP model's form of the snap, which truncates t and t + dt to integers before
+// dividing by dt_map (swDdpHyp.cpp:588-600: `(int)t / dt_map`).
+template <bool kDdpSnap>
 __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
 {
     Ctrl* ctrl = m.ctrl;
@@ -324,8 +327,14 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
             if (wmin[w] < dt) dt = wmin[w];
         const double t = ctrl->t;
         if (m.dt_map > kSmallReal) {
-            int now = (int)(t / m.dt_map);
-            int later = (int)((t + dt) / m.dt_map);
+            int now, later;
+            if (kDdpSnap) {
+                now = (int)((double)(int)t / m.dt_map);
+                later = (int)((double)(int)(t + dt) / m.dt_map);
+            } else {
+                now = (int)(t / m.dt_map);
+                later = (int)((t + dt) / m.dt_map);
+            }
             if (later > now) dt = later * m.dt_map - t;
         }
         if ((t + dt) > ctrl->t_max) dt = ctrl->t_max - t;
@@ -391,61 +400,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
         qq = 0.;
         rr = 0.;
     }
-    const double hthr = smax(m.h_min, kSmallReal);
-    // friction (swSpSourceFriction.cpp:39-171)
-    if (kFriction != SW2D_FRICTION_NONE) {
-        if (hh > hthr) {
-            const double4 fr = ld(&m.fric[c]);
-            double u = qq / hh;
-            double v = rr / hh;
-            double ca = fr.z, sa = fr.w;
-            double ul = u * ca + v * sa;
-            double vl = -u * sa + v * ca;
-            double un = sqrt(u * u + v * v);
-            double f1 = friction_factor(kFriction, fr.x, hh, un, dt);
-            double f2 = friction_factor(kFriction, fr.y, hh, un, dt);
-            ul *= f1;
-            vl *= f2;
-            qq = (ul * ca - vl * sa) * hh;
-            rr = (ul * sa + vl * ca) * hh;
-        } else {
-            qq = 0.;
-            rr = 0.;
-        }
-    }
-    // singular head loss (swSpSourceFriction.cpp:174-219)
-    if (kHeadLoss) {
-        const double2 cs = ld(&m.hlb[c]);
-        double ca = cs.x, sa = cs.y;
-        double qx = qq * ca + rr * sa;
-        double qy = -qq * sa + rr * ca;
-        if (hh > hthr) {
-            const double4 hl = ld(&m.hla[c]);
-            double ax = 0, ay = 0;
-            if (hh > hl.x) {
-                ax = sqrt(qx * qx + qy * qy) * hl.y / hh;
-                ay = sqrt(qx * qx + qy * qy) * hl.z / hh;
-            }
-            qx = qx * sw2d_exp(-ax * dt);
-            qy = qy * sw2d_exp(-ay * dt);
-        } else {
-            qx = 0.;
-            qy = 0.;
-        }
-        qq = qx * ca - qy * sa;
-        rr = qx * sa + qy * ca;
-    }
-    // swSp::correctVelocity (swSp.cpp:447-479)
-    if (hh > m.h_min) {
-        double qn = sqrt(qq * qq + rr * rr);
-        double cc = sqrt(kGravity * hh);
-        double Fr = qn / cc / hh;
-        double fact = smax(qn / (hh * m.v_max), Fr / m.fr_max);
-        if (fact > 1.0) {
-            qq = qq / fact;
-            rr = rr / fact;
-        }
-    }
+    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr);
     // z = h + z_b of the new state, as the next step's reconstruction computes it
     // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
     m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));
@@ -553,10 +508,13 @@ int status_to_code(sw2d_handle* h, unsigned st)
 {
     if (st & kStatusNanFlux) return fail(h, SW2D_E_NAN_FLUX, "SP - mass flux is not a number on an internal interface");
     if (st & kStatusHllcConfig) return fail(h, SW2D_E_HLLC_CONFIG, "impossible flow configuration in the HLLC solver");
-    if (st & kStatusNegDepth) return fail(h, SW2D_E_NEG_DEPTH, "SP - negative water depth");
+    if (st & kStatusNegDepth)
+        return fail(h, SW2D_E_NEG_DEPTH, h->model == kModelDdp ? "DDP - negative theta" : "SP - negative water depth");
     if (st & kStatusBcType) return fail(h, SW2D_E_BC_TYPE, "boundary condition type not handled");
     if (st & kStatusBcFr) return fail(h, SW2D_E_BC_FR, "incorrect value for 'fr'-type boundary condition");
     if (st & kStatusPhiG) return fail(h, SW2D_E_PHIG, "specificForce : phiG is < small");
+    if (st & kStatusTable)
+        return fail(h, SW2D_E_DDP_TABLE, "DDP - NaN elevation or volume in a porosity-table lookup");
     if (st & kStatusUnsupported)
         return fail(h, SW2D_E_UNSUPPORTED, "cell with more neighbours than the adjoint's slope reverse handles");
     return SW2D_OK;
@@ -610,7 +568,8 @@ void launch_edges_m(sw2d_handle* h, const DevMesh& m, int v)
 
 void launch_edges(sw2d_handle* h, const DevMesh& m, int v)
 {
-    if (h->model == kModelDip) launch_edges_m<kModelDip>(h, m, v);
+    if (h->model == kModelDdp) launch_ddp_edges(h, m, v);
+    else if (h->model == kModelDip) launch_edges_m<kModelDip>(h, m, v);
     else launch_edges_m<kModelSp>(h, m, v);
 }
 
@@ -667,13 +626,17 @@ void launch_update_s(sw2d_handle* h, const DevMesh& m)
 // phase i of one step on the handle's stream: 0 slopes, 1 edges, 2 cfl, 3 update
 void launch_phase(sw2d_handle* h, int i)
 {
+    if (h->model == kModelDdp) {
+        launch_ddp_phase(h, i);
+        return;
+    }
     DevMesh& m = h->m;
     switch (i) {
         case 0:
             if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) launch_slopes(h, h->slope_variant);
             break;
         case 1: launch_edges(h, h->edge_variant); break;
-        case 2: k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); break;
+        case 2: k_cfl<false><<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); break;
         default: launch_update_s<false>(h, m); break;
     }
 }
@@ -694,7 +657,9 @@ void launch_slopes_on(sw2d_handle* h, const DevMesh& m)
 
 void launch_edges_on(sw2d_handle* h, const DevMesh& m) { launch_edges(h, m, h->edge_variant); }
 
-void launch_cfl_on(sw2d_handle* h, const DevMesh& m) { k_cfl<<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
+void launch_cfl_on(sw2d_handle* h, const DevMesh& m) { k_cfl<false><<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
+
+void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m) { k_cfl<true><<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
 
 void launch_step_on(sw2d_handle* h) { launch_step(h); }
 
@@ -746,8 +711,8 @@ int check_mesh(const sw2d_mesh* m)
 }
 
 int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
-                 const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
-                 const double* r0, int device, sw2d_handle** out);
+                 const sw2d_dip_fields* dip, const sw2d_ddp_fields* ddp, const sw2d_bc_table* bc, const double* h0,
+                 const double* q0, const double* r0, int device, sw2d_handle** out);
 
 }  // namespace
 
@@ -762,7 +727,7 @@ int sw2d_create(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cel
                 const sw2d_bc_table* bc, const double* h0, const double* q0, const double* r0, int device,
                 sw2d_handle** out)
 {
-    return create_model(mesh, params, fields, nullptr, bc, h0, q0, r0, device, out);
+    return create_model(mesh, params, fields, nullptr, nullptr, bc, h0, q0, r0, device, out);
 }
 
 int sw2d_create_dip(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
@@ -770,24 +735,51 @@ int sw2d_create_dip(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d
                     const double* r0, int device, sw2d_handle** out)
 {
     if (!dip) return fail(nullptr, SW2D_E_ARG, "DIP fields missing");
-    return create_model(mesh, params, fields, dip, bc, h0, q0, r0, device, out);
+    return create_model(mesh, params, fields, dip, nullptr, bc, h0, q0, r0, device, out);
+}
+
+int sw2d_create_ddp(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
+                    const sw2d_ddp_fields* ddp, const sw2d_bc_table* bc, const double* ic_level, const double* ic_x,
+                    const double* ic_y, int device, sw2d_handle** out)
+{
+    if (!ddp) return fail(nullptr, SW2D_E_ARG, "DDP fields missing");
+    return create_model(mesh, params, fields, nullptr, ddp, bc, ic_level, ic_x, ic_y, device, out);
+}
+
+int64_t sw2d_ddp_get_table(sw2d_handle* h, int which, int64_t record, double* z, double* phi, double* theta,
+                           int64_t capacity)
+{
+    if (!h || capacity < 0) return fail(h, SW2D_E_ARG, "invalid arguments");
+    return ddp_get_table(h, which, record, z, phi, theta, capacity);
 }
 
 }  // extern "C"
 
 namespace {
 
-// sw2d_create / sw2d_create_dip: `dip` selects the DIP model
+// sw2d_create / sw2d_create_dip / sw2d_create_ddp: `dip` selects the DIP model, `ddp` the DDP
+// model (h0, q0, r0 then hold its initial-condition columns)
 int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_cell_fields* fields,
-                 const sw2d_dip_fields* dip, const sw2d_bc_table* bc, const double* h0, const double* q0,
-                 const double* r0, int device, sw2d_handle** out)
+                 const sw2d_dip_fields* dip, const sw2d_ddp_fields* ddp, const sw2d_bc_table* bc, const double* h0,
+                 const double* q0, const double* r0, int device, sw2d_handle** out)
 {
     sw2d_handle* h = nullptr;
     if (!out) return fail(h, SW2D_E_ARG, "out is NULL");
     *out = nullptr;
     if (check_mesh(mesh) != SW2D_OK) return fail(h, SW2D_E_ARG, "invalid mesh tables");
-    if (!params || !fields || !fields->phi || !fields->boussinesq || !bc || !h0 || !q0 || !r0)
+    if (!params || !fields || (!ddp && !fields->phi) || !fields->boussinesq || !bc || !h0 || !q0 || !r0)
         return fail(h, SW2D_E_ARG, "missing parameters, porosity, Boussinesq map, boundary table or state");
+    if (ddp) {
+        // swDdp::hypComputeLRStates and hypComputeFluxes (swDdpHyp.cpp:434-458,496-516): Godunov
+        // and the discontinuous topography only
+        if (params->scheme != SW2D_SCHEME_GODUNOV)
+            return fail(h, SW2D_E_UNSUPPORTED, "the DDP model runs the Godunov scheme only (swDdpHyp.cpp:506-510)");
+        if (params->topo != SW2D_TOPO_DISCONTINUOUS)
+            return fail(h, SW2D_E_UNSUPPORTED, "the DDP model runs the discontinuous topography only (swDdpHyp.cpp:454-458)");
+        std::string why;
+        int rc0 = ddp_check(mesh, ddp, why);
+        if (rc0) return fail(h, rc0, why);
+    }
     if (params->variant != SW2D_VARIANT_NATIVE)
         return fail(h, SW2D_E_UNSUPPORTED, "only the native SP variant is implemented");
     if (params->scheme != SW2D_SCHEME_GODUNOV && params->scheme != SW2D_SCHEME_MUSCL_EVR)
@@ -810,7 +802,8 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     // swSp::checkParameterConsistency (swSp.cpp:33-335), the checks on this path
     for (int64_t c = 0; c < mesh->cell_nb; c++) {
         if (!(fields->boussinesq[c] >= 1.0)) return fail(h, SW2D_E_ARG, "boussinesq coeff. should be >= 1");
-        if ((fields->phi[c] < 0.0) || (fields->phi[c] > 1.0)) return fail(h, SW2D_E_ARG, "porosity should belong to [0,1]");
+        if (!ddp && ((fields->phi[c] < 0.0) || (fields->phi[c] > 1.0)))
+            return fail(h, SW2D_E_ARG, "porosity should belong to [0,1]");
     }
     // swDip::checkParameterConsistency (dip/swDip.cpp:121-240): phiG in [0,1], not above phiW
     if (dip) {
@@ -838,8 +831,8 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     h = new sw2d_handle();
     h->device = device;
     h->p = *params;
-    h->model = dip ? kModelDip : kModelSp;
-    h->dissipation = (dip && dip->momentum_dissipation) ? 1 : 0;
+    h->model = dip ? kModelDip : ddp ? kModelDdp : kModelSp;
+    h->dissipation = ((dip && dip->momentum_dissipation) || (ddp && ddp->momentum_dissipation)) ? 1 : 0;
     h->nc = mesh->cell_nb;
     h->ni = mesh->edge_int_nb;
     h->nb = mesh->edge_bnd_nb;
@@ -939,7 +932,9 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
         const int o = h->cell_perm[i];
         const double zb = mesh->cell_z_b[o];
         st[i] = make_double4(h0[o], q0[o], r0[o], h0[o] + zb);
-        cst[i] = make_double4(zb, fields->boussinesq[o], fields->phi[o], mesh->cell_area[o]);
+        // DDP: the SP coefficient w / area / phi with phi = 1 is the DDP factor w / area
+        // (swDdp.cpp:430-466); the DDP set-up then stores the lowest table level in .z
+        cst[i] = make_double4(zb, fields->boussinesq[o], ddp ? 1.0 : fields->phi[o], mesh->cell_area[o]);
         cxy[i] = make_double2(mesh->cell_x[o], mesh->cell_y[o]);
         zbv[i] = zb;
         area[i] = mesh->cell_area[o];
@@ -1073,7 +1068,7 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     m.lmax = nullptr;
     m.lmaxb = nullptr;
     m.h_min = params->h_min;
-    m.phi_min = params->phi_min;
+    m.phi_min = ddp ? 0.0 : params->phi_min;
     m.cfl_max = params->cfl_max;
     m.dt_max = params->dt_max;
     m.dt_map = params->dt_map;
@@ -1101,6 +1096,12 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     k_edge_coefficients<<<grid_for(ni + nb), kBlock, 0, h->stream>>>(m, coef_d, bgeo_d);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return bail(fail(h, SW2D_E_CUDA, "initialisation kernels failed"));
+    if (ddp) {
+        if ((rc = ddp_setup(h, mesh, fields, ddp, h0, q0, r0))) return bail(rc);
+        CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if ((rc = status_to_code(h, h->ctrl_host->status))) return bail(rc);
+    }
     *out = h;
     return SW2D_OK;
 }
@@ -1289,8 +1290,9 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
             if (!rc) rc = dev_alloc(h, h->nb, &h->bflux_buf);
             if (rc) return rc;
         }
-        h->m.flux = value ? h->flux_buf : nullptr;
-        h->m.bflux = value ? h->bflux_buf : nullptr;
+        const bool keep = h->model == kModelDdp && h->m.div_corr == kDivCorrFlux;  // the correction scales them
+        h->m.flux = (value || keep) ? h->flux_buf : nullptr;
+        h->m.bflux = (value || keep) ? h->bflux_buf : nullptr;
     } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
         h->adj_flush_branch = value ? 1 : 0;
         return SW2D_OK;
@@ -1334,6 +1336,7 @@ int sw2d_set_state_device(sw2d_handle* h, const double* dh, const double* dq, co
     CK(cudaSetDevice(h->device));
     k_gather_state<<<grid_for(h->nc), kBlock, 0, h->stream>>>(dh, dq, dr, h->d_cell_perm, h->m.cst, h->m.st, (int)h->nc);
     CK(cudaGetLastError());
+    if (h->model == kModelDdp) return ddp_derive(h);  // z and the cell-table values of the new state
     return SW2D_OK;
 }
 
@@ -1391,6 +1394,11 @@ int sw2d_set_time(sw2d_handle* h, double t, double dt)
 int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity)
 {
     if (!h || !name || !out) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (h->model == kModelDdp) {
+        bool handled = false;
+        const int64_t r = ddp_get_array(h, name, out, capacity, &handled);
+        if (handled) return r;
+    }
     struct Entry {
         const char* n;
         const double* p;
@@ -1541,6 +1549,7 @@ void* sw2d_get_stream(sw2d_handle* h) { return h ? (void*)h->stream : nullptr; }
 int sw2d_kernels_per_step(sw2d_handle* h)
 {
     if (!h) return 0;
+    if (h->model == kModelDdp) return ddp_kernels_per_step(h);
     return h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3;
 }
 
@@ -1578,6 +1587,7 @@ int sw2d_destroy(sw2d_handle* h)
     if (h->graph) cudaGraphExecDestroy(h->graph);
     adjoint_release(h);
     assim_release(h);
+    ddp_release(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -37,8 +37,10 @@ class Sw2dError(RuntimeError):
 
 
 class SpModel:
-    """SW2D porosity model (single porosity, or dual integral porosity when the case says
-    model_hyperb dip) running on one GPU."""
+    """SW2D porosity model running on one GPU: single porosity, dual integral porosity when the
+    case says model_hyperb dip, depth-dependent porosity when it says ddp (then ``state()`` is
+    the model's own (thetaW, thetaW u, thetaW v), and ``array("water_depth")`` etc. give the map
+    outputs)."""
 
     def __init__(self, case: Case, device: int = 0):
         self.lib = capi.load_library()
@@ -49,7 +51,11 @@ class SpModel:
         self._in = capi.native_inputs(case)
         i = self._in
         handle = ctypes.c_void_p()
-        if i.dip is not None:  # model_hyperb dip: swDip
+        if i.ddp is not None:  # model_hyperb ddp: swDdp (h0/q0/r0 are the initial-condition columns)
+            st = self.lib.sw2d_create_ddp(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
+                                          ctypes.byref(i.ddp), ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0),
+                                          capi._dp(i.r0), int(device), ctypes.byref(handle))
+        elif i.dip is not None:  # model_hyperb dip: swDip
             st = self.lib.sw2d_create_dip(ctypes.byref(i.mesh), ctypes.byref(i.params), ctypes.byref(i.fields),
                                           ctypes.byref(i.dip), ctypes.byref(i.bc), capi._dp(i.h0), capi._dp(i.q0),
                                           capi._dp(i.r0), int(device), ctypes.byref(handle))
@@ -64,8 +70,9 @@ class SpModel:
     @classmethod
     def from_folder(cls, folder: str, device: int = 0) -> "SpModel":
         case = read_case(folder)
-        if str(case.opts.get("model_hyperb", "sp")).lower() not in ("sp", "dip"):
-            raise Sw2dError(-8, f"model_hyperb {case.opts.get('model_hyperb')!r}: only 'sp' and 'dip' are implemented")
+        if str(case.opts.get("model_hyperb", "sp")).lower() not in ("sp", "dip", "ddp"):
+            raise Sw2dError(-8, f"model_hyperb {case.opts.get('model_hyperb')!r}: only 'sp', 'dip' and 'ddp' are "
+                                "implemented")
         return cls(case, device)
 
     def _check(self, st: int) -> None:
@@ -81,6 +88,17 @@ class SpModel:
         done = ctypes.c_int64(0)
         self._check(self.lib.sw2d_execute(self.handle, ctypes.byref(done)))
         return int(done.value)
+
+    def ddp_table(self, which: str, record: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Tabulated porosity law (z, phi, theta) of a DDP cell ("cell"), internal edge ("edge_int")
+        or boundary edge ("edge_bnd"), as swDdp keeps it (cell_z_tab / phiW_tab / thetaW_tab ...)."""
+        k = {"cell": 0, "edge_int": 1, "edge_bnd": 2}[which]
+        n = self.lib.sw2d_ddp_get_table(self.handle, k, int(record), None, None, None, 0)
+        if n < 0:
+            self._check(int(n))
+        z, phi, theta = np.empty(n), np.empty(n), np.empty(n)
+        self.lib.sw2d_ddp_get_table(self.handle, k, int(record), _p(z), _p(phi), _p(theta), n)
+        return z, phi, theta
 
     def state(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         h, q, r = (np.empty(self.n) for _ in range(3))

@@ -12,7 +12,9 @@ The reference ships no benchmark suite; these constructions stand in for it:
   seed 5), MUSCL-EVR + HLLC, walls;
 * ``channel_features``: a small case exercising every other branch of the path (blending
   topography, Strickler or Chezy friction, singular head loss, 'q' inflow and 'fr'/'h'/'z'
-  outflow time series).
+  outflow time series);
+* ``dip_channel`` / ``ddp_channel``: the feature channel as a dual integral porosity or a
+  depth-dependent porosity (DDP) case.
 """
 from __future__ import annotations
 
@@ -21,7 +23,7 @@ from typing import Dict, Optional
 
 import numpy as np
 
-from .case import BoundarySeries, Case
+from .case import BoundarySeries, Case, LawRecords, ddp_law_table
 from .mesh import jittered_triangle_mesh
 
 
@@ -193,3 +195,122 @@ def dip_channel(n_cells: int = 3000, scheme: str = "muscl_evr", topo: str = "dis
     return Case(mesh=mesh, opts=opts, h0=base.h0, q0=base.q0, r0=base.r0, phi=phiW, boussinesq=base.boussinesq,
                 friction=base.friction, head_loss=None, bc=bc, extra={"name": "dip_channel"},
                 phi_g_int=phi_g_int, phi_g_bnd=phi_g_bnd, mu=mu)
+
+
+def _ddp_cell_record(rng, kind: str, ntab: int):
+    """One cell porosity-law record (elevations relative to the cell bottom)."""
+    z0 = 0.0 if rng.uniform() < 0.7 else float(rng.uniform(0.0, 0.04))
+    if kind == "3":    # linear up to z1, then an open level above (an overtopped wall)
+        return [3, 5, z0, rng.uniform(0.3, 0.7), z0 + rng.uniform(0.15, 0.5), rng.uniform(0.5, 0.9), rng.uniform(0.8, 1.0)]
+    if kind == "2":
+        return [2, 4, z0, rng.uniform(0.4, 0.8), z0 + rng.uniform(0.2, 0.7), rng.uniform(0.6, 1.0)]
+    if kind == "1":
+        return [1, 2, z0, rng.uniform(0.5, 1.0)]
+    if kind == "-1":
+        k = int(rng.integers(3, 5))
+        zs = z0 + np.concatenate([[0.0], np.cumsum(rng.uniform(0.05, 0.3, k - 1))])
+        ph = rng.uniform(0.3, 1.0, k)
+        return [-1, k] + [v for pair in zip(zs.tolist(), ph.tolist()) for v in pair]
+    if kind == "-2":   # pre-tabulated: more levels than n_por_tab_max
+        k = ntab + 1
+        zs = z0 + np.concatenate([[0.0], np.cumsum(rng.uniform(0.05, 0.2, k - 1))])
+        ph = np.sort(rng.uniform(0.3, 1.0, k))
+        return [-2, k] + [v for pair in zip(zs.tolist(), ph.tolist()) for v in pair]
+    if kind == "0":    # levels only: phi rising from 0 to 1
+        k = int(rng.integers(3, 5))
+        zs = z0 + np.concatenate([[0.0], np.cumsum(rng.uniform(0.05, 0.3, k - 1))])
+        return [0, k] + zs.tolist()
+    raise ValueError(kind)
+
+
+def _ddp_edge_record(rng, pmax: float, nlev: int, ntab: int):
+    """An edge record whose tabulated porosities stay below pmax at every level (the reference
+    requires phiG <= phiW level by level, swDdp.cpp:180-213) with at most nlev levels."""
+    z0 = 0.0 if rng.uniform() < 0.7 else float(rng.uniform(0.0, 0.04))
+    u = rng.uniform()
+    if u < 0.5 and nlev >= ntab:
+        return [3, 5, z0, pmax * rng.uniform(0.3, 1.0), z0 + rng.uniform(0.15, 0.5), pmax * rng.uniform(0.5, 1.0),
+                pmax * rng.uniform(0.7, 1.0)]
+    if u < 0.75 and nlev >= ntab:
+        return [1, 2, z0, pmax * rng.uniform(0.4, 1.0)]
+    if u < 0.9 and nlev >= ntab:
+        return [2, 4, z0, pmax * rng.uniform(0.4, 1.0), z0 + rng.uniform(0.2, 0.6), pmax * rng.uniform(0.4, 1.0)]
+    k = 2
+    return [-2, k, z0, pmax * rng.uniform(0.3, 1.0), z0 + rng.uniform(0.1, 0.4), pmax * rng.uniform(0.3, 1.0)]
+
+
+def ddp_channel(n_cells: int = 3000, friction: str = "manning", inflow_q: float = 0.5, outflow: str = "fr",
+                head_loss: bool = False, dissipation: bool = False, div_corr: str = "none", n_it_div_max: int = 10,
+                laws: str = "mixed", n_por_tab_max: int = 5, ic: str = "hqr", h_floor: float = 0.0,
+                moving: bool = False, boussinesq: float = 1.0, t_max: float = 40.0, seed: int = 21) -> Case:
+    """The feature channel as a depth-dependent porosity (DDP) case, Godunov with the
+    discontinuous topography (the only path the reference's DDP step runs).  Cells get seeded
+    porosity laws: laws="mixed" draws every law type (3: linear with an open top level, 2
+    linear, 1 uniform, -1 re-tabulated couples, -2 pre-tabulated couples, 0 levels), "linear"
+    only types 3, 2 and 1 (what the large benchmark case uses).  Edge laws stay below their
+    cells' tabulated porosity at every level.  The initial state: depth max(h_floor, 0.45 - z_b)
+    above the lowest level, a discharge of 0.05 m2/s where wet when moving; ic names the
+    initial-condition columns ("hqr", "zuv", ...)."""
+    base = channel_features(n_cells=n_cells, scheme="godunov", topo="discontinuous", friction=friction,
+                            outflow=outflow, head_loss=head_loss, boussinesq=boussinesq, t_max=t_max, seed=seed,
+                            h_floor=h_floor)
+    mesh = base.mesh
+    n = mesh.cell_nb
+    rng = np.random.default_rng(seed + 100)
+    if laws == "mixed":
+        kinds = rng.choice(["3", "2", "1", "-1", "-2", "0"], size=n, p=[0.45, 0.2, 0.15, 0.1, 0.05, 0.05])
+    else:
+        kinds = rng.choice(["3", "2", "1"], size=n, p=[0.5, 0.3, 0.2])
+    cell_recs, pmin, nlev = [], np.empty(n), np.empty(n, dtype=np.int64)
+    for c in range(n):
+        while True:
+            rec = _ddp_cell_record(rng, str(kinds[c]), n_por_tab_max)
+            try:
+                zt, pt, _ = ddp_law_table(rec, float(mesh.cell_z_b[c]), n_por_tab_max)
+                break
+            except ValueError:   # a draw the reference cannot tabulate: draw again
+                continue
+        cell_recs.append(rec)
+        pmin[c] = float(np.min(pt))
+        nlev[c] = zt.size
+    def edge(pmax, nl, base):
+        while True:
+            rec = _ddp_edge_record(rng, pmax, nl, n_por_tab_max)
+            try:
+                ddp_law_table(rec, base, n_por_tab_max)
+                return rec
+            except ValueError:
+                continue
+
+    L, R = mesh.edge_int_cells[:, 0], mesh.edge_int_cells[:, 1]
+    eint = [edge(0.9 * min(pmin[a], pmin[b]), int(min(nlev[a], nlev[b])), float(mz))
+            for a, b, mz in zip(L.tolist(), R.tolist(), mesh.edge_int_mz.tolist())]
+    ebnd = [edge(0.9 * pmin[c], int(nlev[c]), float(mz))
+            for c, mz in zip(mesh.edge_bnd_cell.tolist(), mesh.edge_bnd_mz.tolist())]
+    opts = dict(base.opts)
+    opts.update({"model_hyperb": "ddp", "n_por_tab_max": n_por_tab_max, "div_corr": div_corr,
+                 "n_it_div_max": n_it_div_max, "ddp_chi_phi_max": 20.0})
+    mu = None
+    if dissipation:
+        opts["model_momentum_dissipation"] = "active"
+        mu = np.stack([rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 90.0, n)])
+    level = base.h0.copy()
+    z_tab0 = np.array([float(mesh.cell_z_b[c]) + float(cell_recs[c][2]) for c in range(n)])
+    wet = level > 0.0
+    qx = np.where(wet, 0.05, 0.0) if moving else np.zeros(n)
+    qy = np.where(wet, 0.01, 0.0) if moving else np.zeros(n)
+    if ic[0] == "z":
+        level = level + z_tab0
+    if ic[1] == "u":
+        qx = np.where(wet, qx / np.maximum(base.h0, 1e-3), 0.0)
+    if ic[2] == "v":
+        qy = np.where(wet, qy / np.maximum(base.h0, 1e-3), 0.0)
+    bc = base.bc
+    values = np.array(bc.values, copy=True)
+    values[1] = values[1] * (inflow_q / 0.5)
+    bc = BoundarySeries(codes=bc.codes, types=list(bc.types), times=bc.times, values=values)
+    return Case(mesh=mesh, opts=opts, h0=level, q0=qx, r0=qy, phi=np.ones(n), boussinesq=base.boussinesq,
+                friction=base.friction, head_loss=base.head_loss, bc=bc, mu=mu,
+                extra={"name": "ddp_channel"}, ddp_cell=LawRecords.from_list(cell_recs),
+                ddp_edge_int=LawRecords.from_list(eint), ddp_edge_bnd=LawRecords.from_list(ebnd),
+                ddp_ic=(ic[0], ic[1], ic[2]))

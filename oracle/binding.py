@@ -121,8 +121,9 @@ class SpOracle:
 
 
 class RefSolver:
-    """The reference's native SP solver (built from its own sources) on a case folder.
-    ``portable_math`` loads the build linked with the portable exp/log of the CUDA build."""
+    """The reference's native SP, DIP or DDP solver (built from its own sources) on a case
+    folder.  ``portable_math`` loads the build linked with the portable exp/log of the CUDA
+    build.  For a DDP case ``state()`` is (thetaW, thetaW u, thetaW v)."""
 
     def __init__(self, folder: str, quiet: bool = True, portable_math: bool = False):
         so = REF_PM_SO if portable_math else REF_SO
@@ -145,6 +146,8 @@ class RefSolver:
         lib.sw2dref_get_array.argtypes = [_P, ctypes.c_char_p, _D]
         lib.sw2dref_get_array.restype = ctypes.c_int
         lib.sw2dref_slopes.argtypes = [_P, _D, _D]
+        lib.sw2dref_ddp_table.argtypes = [_P, ctypes.c_int, ctypes.c_long, _D, _D, _D, ctypes.c_long]
+        lib.sw2dref_ddp_table.restype = ctypes.c_long
         self.lib = lib
         self.h = lib.sw2dref_open(folder.encode(), 1 if quiet else 0)
         if not self.h:
@@ -186,6 +189,15 @@ class RefSolver:
         sx, sy = np.empty(self.n), np.empty(self.n)
         self.lib.sw2dref_slopes(self.h, sx, sy)
         return sx, sy
+
+    def ddp_table(self, which: str, record: int):
+        """(z, phi, theta) levels of a DDP cell / internal edge / boundary edge table."""
+        k = {"cell": 0, "edge_int": 1, "edge_bnd": 2}[which]
+        buf = [np.empty(4096) for _ in range(3)]
+        n = self.lib.sw2dref_ddp_table(self.h, k, int(record), buf[0], buf[1], buf[2], 4096)
+        if n < 0:
+            raise KeyError(f"{which}[{record}]")
+        return tuple(b[:n].copy() for b in buf)
 
 
 class RefE:

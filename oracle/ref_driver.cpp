@@ -1,5 +1,5 @@
-// Test harness around the reference's own native SP and DIP solvers (compiled from the reference
-// sources by oracle/Makefile).  It is a checker, never part of the product.
+// Test harness around the reference's own native SP, DIP and DDP solvers (compiled from the
+// reference sources by oracle/Makefile).  It is a checker, never part of the product.
 //
 // The reference only runs a whole simulation (`swSp::execute`, src/sw2dSolver/models/sp/swSp.cpp:482-670;
 // `swDip::execute`, models/dip/swDip.cpp, the same loop).  This subclass template reaches the
@@ -14,6 +14,7 @@
 //   sw2dref_run(handle)                the reference's own execute() (whole loop, with storage)
 //   sw2dref_get/set_state, sw2dref_get_array, sw2dref_time, sw2dref_dt, sizes
 
+#include <algorithm>
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -21,12 +22,14 @@
 #include <string>
 #include <vector>
 
+#include "../common/param.h"
 #include "../common/swFile.h"
 #include "../common/swIO.h"
 #include "../common/swLog.h"
 #include "../common/swMessage.h"
 #include "../common/geometry/swMesh.h"
 #include "common/swSolverParam.h"
+#include "models/ddp/swDdp.h"
 #include "models/dip/swDip.h"
 #include "models/sp/swSp.h"
 
@@ -52,6 +55,7 @@ public:
     virtual double timeStep() const = 0;
     virtual double tMax() const = 0;
     virtual bool run() = 0;
+    virtual long table(int which, long record, double* z, double* phi, double* theta, long cap) = 0;
 };
 
 template <class M>
@@ -84,10 +88,17 @@ public:
 
     void beginTime() override { this->t = this->t_0; }
 
+    static constexpr bool kDdp = std::is_same<M, swDdp>::value;
+
     // Limited free-surface slopes exactly as the MUSCL-EVR reconstruction computes them
-    // (sp/swSpHypMusclEvr.cpp:126-139), for kernel-level checks.
+    // (sp/swSpHypMusclEvr.cpp:126-139), for kernel-level checks (SP and DIP).
     void slopes(double* sx, double* sy) override
     {
+        if constexpr (kDdp) {
+            (void)sx;
+            (void)sy;
+            return;
+        } else {
         std::vector<double> z_cell(this->cell_nb), dzx(this->cell_nb), dzy(this->cell_nb);
         for (size_t i = 0; i < this->cell_nb; i++) z_cell[i] = this->water_depth[i] + this->cell_z_b[i];
         this->computeMusclSlopes(this->cell_centre_x, this->cell_centre_y, this->cell_neigh_cell_idx,
@@ -95,6 +106,28 @@ public:
                            this->edge_int_celL_idx, this->edge_int_celR_idx, z_cell, dzx, dzy);
         std::memcpy(sx, dzx.data(), this->cell_nb * sizeof(double));
         std::memcpy(sy, dzy.data(), this->cell_nb * sizeof(double));
+        }
+    }
+
+    // DDP porosity tables (swDdp.h:243-281): which 0 cells, 1 internal edges, 2 boundary edges
+    long table(int which, long record, double* z, double* phi, double* theta, long cap) override
+    {
+        if constexpr (kDdp) {
+            const std::vector<std::vector<double>>* tz = which == 0 ? &this->cell_z_tab : which == 1 ? &this->edge_int_z_tab : &this->edge_bnd_z_tab;
+            const std::vector<std::vector<double>>* tp = which == 0 ? &this->phiW_tab : which == 1 ? &this->phiG_int_tab : &this->phiG_bnd_tab;
+            const std::vector<std::vector<double>>* tt = which == 0 ? &this->thetaW_tab : which == 1 ? &this->thetaG_int_tab : &this->thetaG_bnd_tab;
+            if (record < 0 || (size_t)record >= tz->size()) return -1;
+            const long n = (long)(*tz)[record].size();
+            for (long l = 0; l < n && l < cap; l++) {
+                z[l] = (*tz)[record][l];
+                phi[l] = (*tp)[record][l];
+                theta[l] = (*tt)[record][l];
+            }
+            return n;
+        } else {
+            (void)which; (void)record; (void)z; (void)phi; (void)theta; (void)cap;
+            return -1;
+        }
     }
 
     int getArray(const std::string& name, double* out) override
@@ -104,9 +137,48 @@ public:
             for (size_t i = 0; i < v.size(); i++) out[i] = v[i][side];
             return (int)v.size();
         };
-        if (name == "h") return put(this->water_depth);
-        if (name == "q") return put(this->unit_discharge_x);
-        if (name == "r") return put(this->unit_discharge_y);
+        if constexpr (kDdp) {
+            // state (swDdp.h:199-201), Riemann states, tables' derived values
+            if (name == "h" || name == "theta") return put(this->thetaW);
+            if (name == "q" || name == "theta_u") return put(this->thetaW_velocity_x);
+            if (name == "r" || name == "theta_v") return put(this->thetaW_velocity_y);
+            if (name == "theta_riemann_L") return put2(this->theta_riemann_int, 0);
+            if (name == "theta_riemann_R") return put2(this->theta_riemann_int, 1);
+            if (name == "theta_u_riemann_L") return put2(this->theta_u_riemann_int, 0);
+            if (name == "theta_u_riemann_R") return put2(this->theta_u_riemann_int, 1);
+            if (name == "theta_v_riemann_L") return put2(this->theta_v_riemann_int, 0);
+            if (name == "theta_v_riemann_R") return put2(this->theta_v_riemann_int, 1);
+            if (name == "thetaG_int_hmin") return put(this->thetaG_int_hmin);
+            if (name == "z_riemann_bnd") return put(this->z_riemann_bnd);
+            if (name == "surface_elevation" || name == "water_depth" || name == "unit_discharge_x" ||
+                name == "unit_discharge_y") {
+                // swDdp::storeResultMaps (swDdp.cpp:2489-2513)
+                for (size_t n = 0; n < this->cell_nb; n++) {
+                    double theta = this->thetaW[n];
+                    double z = this->zOfThetaW(n, theta);
+                    double h = std::max(0.0, z - this->cell_z_tab[n][0]);
+                    double u = 0.0, v = 0.0;
+                    if (theta > small_real) {
+                        u = this->thetaW_velocity_x[n] / theta;
+                        v = this->thetaW_velocity_y[n] / theta;
+                    }
+                    out[n] = name == "surface_elevation" ? z : name == "water_depth" ? h : name == "unit_discharge_x" ? u * h : v * h;
+                }
+                return (int)this->cell_nb;
+            }
+        } else {
+            if (name == "h") return put(this->water_depth);
+            if (name == "q") return put(this->unit_discharge_x);
+            if (name == "r") return put(this->unit_discharge_y);
+            if (name == "q_riemann_L") return put2(this->q_riemann_int, 0);
+            if (name == "q_riemann_R") return put2(this->q_riemann_int, 1);
+            if (name == "r_riemann_L") return put2(this->r_riemann_int, 0);
+            if (name == "r_riemann_R") return put2(this->r_riemann_int, 1);
+            if (name == "phi") {
+                if constexpr (std::is_same<M, swDip>::value) return put(this->phiW);
+                else return put(this->phi);
+            }
+        }
         if (name == "F1_int") return put(this->F1_int);
         if (name == "F2_int") return put(this->F2_int);
         if (name == "F3_int") return put(this->F3_int);
@@ -120,18 +192,10 @@ public:
         if (name == "lambda_max_bnd") return put(this->lambda_max_bnd);
         if (name == "z_riemann_L") return put2(this->z_riemann_int, 0);
         if (name == "z_riemann_R") return put2(this->z_riemann_int, 1);
-        if (name == "q_riemann_L") return put2(this->q_riemann_int, 0);
-        if (name == "q_riemann_R") return put2(this->q_riemann_int, 1);
-        if (name == "r_riemann_L") return put2(this->r_riemann_int, 0);
-        if (name == "r_riemann_R") return put2(this->r_riemann_int, 1);
         if (name == "lambda_minus_L") return put2(this->lambda_minus_int, 0);
         if (name == "lambda_minus_R") return put2(this->lambda_minus_int, 1);
         if (name == "lambda_plus_L") return put2(this->lambda_plus_int, 0);
         if (name == "lambda_plus_R") return put2(this->lambda_plus_int, 1);
-        if (name == "phi") {
-            if constexpr (std::is_same<M, swDip>::value) return put(this->phiW);
-            else return put(this->phi);
-        }
         if constexpr (std::is_same<M, swDip>::value) {
             if (name == "phiG_int") return put(this->phiG_int);
             if (name == "phiG_bnd") return put(this->phiG_bnd);
@@ -145,9 +209,15 @@ public:
 
     void setState(const double* h, const double* q, const double* r) override
     {
-        std::memcpy(this->water_depth.data(), h, this->cell_nb * sizeof(double));
-        std::memcpy(this->unit_discharge_x.data(), q, this->cell_nb * sizeof(double));
-        std::memcpy(this->unit_discharge_y.data(), r, this->cell_nb * sizeof(double));
+        if constexpr (kDdp) {
+            std::memcpy(this->thetaW.data(), h, this->cell_nb * sizeof(double));
+            std::memcpy(this->thetaW_velocity_x.data(), q, this->cell_nb * sizeof(double));
+            std::memcpy(this->thetaW_velocity_y.data(), r, this->cell_nb * sizeof(double));
+        } else {
+            std::memcpy(this->water_depth.data(), h, this->cell_nb * sizeof(double));
+            std::memcpy(this->unit_discharge_x.data(), q, this->cell_nb * sizeof(double));
+            std::memcpy(this->unit_discharge_y.data(), r, this->cell_nb * sizeof(double));
+        }
     }
 
     size_t nCells() const override { return this->cell_nb; }
@@ -177,7 +247,7 @@ struct QuietErr
 
 extern "C" {
 
-// Mirrors src/sw2dSolver/main.cpp:76-163 for an SP or DIP case (model_hyperb sp | dip).
+// Mirrors src/sw2dSolver/main.cpp:76-163 for an SP, DIP or DDP case (model_hyperb sp | dip | ddp).
 void* sw2dref_open(const char* folder, int quiet)
 {
     QuietErr q(quiet != 0);
@@ -189,11 +259,12 @@ void* sw2dref_open(const char* folder, int quiet)
     swSolverParam* param = new swSolverParam(hd->io);
     if (param->readParameters() != EXIT_SUCCESS) return nullptr;
     const std::string hyp = param->getModelHyp();
-    if (hyp != "sp" && hyp != "dip") return nullptr;
+    if (hyp != "sp" && hyp != "dip" && hyp != "ddp") return nullptr;
     swMesh* mesh = new swMesh(hd->io);
     if (mesh->build() != EXIT_SUCCESS) return nullptr;
     if (param->getHotstart() == false) hd->io->createEmptyOutputFolder(true);
-    if (hyp == "dip") hd->model = new Ref<swDip>();
+    if (hyp == "ddp") hd->model = new Ref<swDdp>();
+    else if (hyp == "dip") hd->model = new Ref<swDip>();
     else hd->model = new Ref<swSp>();
     swParent* p = hd->model->parent();
     p->setIOPointer(hd->io);
@@ -248,6 +319,11 @@ void sw2dref_set_state(void* h, const double* hh, const double* q, const double*
 int sw2dref_get_array(void* h, const char* name, double* out)
 {
     return static_cast<Handle*>(h)->model->getArray(name, out);
+}
+
+long sw2dref_ddp_table(void* h, int which, long record, double* z, double* phi, double* theta, long cap)
+{
+    return static_cast<Handle*>(h)->model->table(which, record, z, phi, theta, cap);
 }
 
 void sw2dref_slopes(void* h, double* sx, double* sy)

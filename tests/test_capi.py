@@ -26,7 +26,7 @@ def test_library_exports_declared_symbols():
     missing = [n for n in sorted(declared) if not hasattr(lib, n)]
     assert not missing, missing
     assert set(pkg.capi.EXPORTED) == declared
-    assert lib.sw2d_abi_version() == 2
+    assert lib.sw2d_abi_version() == 3
 
 
 def test_params_from_input_solv_keys():
