@@ -148,6 +148,8 @@ class RefSolver:
         lib.sw2dref_slopes.argtypes = [_P, _D, _D]
         lib.sw2dref_ddp_table.argtypes = [_P, ctypes.c_int, ctypes.c_long, _D, _D, _D, ctypes.c_long]
         lib.sw2dref_ddp_table.restype = ctypes.c_long
+        lib.sw2dref_failed.argtypes = [_P]
+        lib.sw2dref_failed.restype = ctypes.c_int
         self.lib = lib
         self.h = lib.sw2dref_open(folder.encode(), 1 if quiet else 0)
         if not self.h:
@@ -161,6 +163,11 @@ class RefSolver:
 
     def run(self) -> int:
         return self.lib.sw2dref_run(self.h)
+
+    @property
+    def failed(self) -> bool:
+        """True once a step failed where the reference's execute() stops with EXIT_FAILURE."""
+        return bool(self.lib.sw2dref_failed(self.h))
 
     def state(self):
         h, q, r = (np.empty(self.n) for _ in range(3))

@@ -56,6 +56,7 @@ public:
     virtual double tMax() const = 0;
     virtual bool run() = 0;
     virtual long table(int which, long record, double* z, double* phi, double* theta, long cap) = 0;
+    bool failed = false;  // the reference's execute() would have stopped with EXIT_FAILURE
 };
 
 template <class M>
@@ -66,11 +67,19 @@ public:
     bool run() override { return this->execute(); }
 
     // One pass of the body of swSp::execute's time loop (sp/swSp.cpp:522-589), storage left out.
+    // Where execute() returns EXIT_FAILURE (a failing hypCompute: NaN flux, impossible HLLC
+    // configuration, negative depth with detection) the pass stops there and `failed` is set.
     bool stepOnce() override
     {
-        if (!(this->t < this->t_max)) return false;
+        if (failed || !(this->t < this->t_max)) return false;
         this->computeBC(this->t);
-        this->hypCompute(this->div_corr_option, this->n_it_div_max, this->num_scheme, this->dt);
+        auto hyp = [&]() { return this->hypCompute(this->div_corr_option, this->n_it_div_max, this->num_scheme, this->dt); };
+        if constexpr (std::is_void<decltype(hyp())>::value) {
+            hyp();  // SP and DIP report their failures through the result of the step itself
+        } else if (hyp() != EXIT_SUCCESS) {
+            failed = true;
+            return false;
+        }
         if (this->model_momentum_diffusion != "none") this->parabComputeExplicit();
         if (this->model_friction != "none") this->sourceFriction(this->model_friction, this->dt);
         if (this->model_singular_head_loss != "none") this->sourceSingularHeadLoss(this->dt);
@@ -295,6 +304,8 @@ int sw2dref_run(void* h)
     Handle* hd = static_cast<Handle*>(h);
     return hd->model->run() == EXIT_SUCCESS ? 0 : 1;
 }
+
+int sw2dref_failed(void* h) { return static_cast<Handle*>(h)->model->failed ? 1 : 0; }
 
 double sw2dref_time(void* h) { return static_cast<Handle*>(h)->model->time(); }
 double sw2dref_dt(void* h) { return static_cast<Handle*>(h)->model->timeStep(); }

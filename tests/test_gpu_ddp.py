@@ -66,7 +66,19 @@ def test_ddp_matches_live_reference(pkg, tmp_path, name):
     for a, b in zip(model.state(), ref.state()):  # the initial-condition conversion
         assert _bits_equal(a, b)
     for chunk in (1, 1, 5, 40, 150):
-        assert model.step(chunk) == ref.step(chunk)
+        done = ref.step(chunk)
+        if ref.failed:
+            # the reference's execute() stops inside the step after `done` (a NaN mass flux,
+            # swDdpHyp.cpp:460-483, before the balance): the model reports the same step
+            assert model.step(done) == done
+            assert model.t == ref.t
+            for a, b in zip(model.state(), ref.state()):
+                assert _bits_equal(a, b)
+            with pytest.raises(pkg.solver.Sw2dError) as e:
+                model.step(1)
+            assert e.value.code == -3
+            return
+        assert model.step(chunk) == done
         assert model.t == ref.t and model.dt == ref.dt, (model.t, ref.t, model.dt, ref.dt)
         for k, (a, b) in enumerate(zip(model.state(), ref.state())):
             assert _bits_equal(a, b), (chunk, k, np.flatnonzero(a.view(np.int64) != b.view(np.int64))[:5])
