@@ -12,7 +12,8 @@ h/q/r...) and from the same reference objects linked with the portable exp/log o
 build (oracle/_ref/libsw2d_ref_pm.so, fields ..._pm).  ``libm_stable`` records whether the two
 agree within 1e-10 (relative, infinity norm; discharges scaled by max(|q|max, h_max sqrt(g h_max))).
 
-The dip_* cases are dual integral porosity cases (the reference's swDip).
+The dip_* cases are dual integral porosity cases (the reference's swDip), the ddp_* cases
+depth-dependent porosity cases (swDdp; their state is thetaW, thetaW u, thetaW v).
 
 Run here (the reference tree must be present):  python tests/golden/make_golden.py [name ...]
 """
@@ -53,8 +54,16 @@ CASES = {
                                                              "outflow": "h", "dissipation": False}),
     "dip_muscl_blend_chezy_q_z_b11": ("dip_channel", {"n_cells": 2000, "topo": "blending", "friction": "chezy",
                                                        "outflow": "z", "boussinesq": 1.1}),
+    # depth-dependent porosity (model_hyperb ddp)
+    "ddp_mixed_manning_fr": ("ddp_channel", {"n_cells": 2000}),
+    "ddp_linear_strickler_h_hl_diss": ("ddp_channel", {"n_cells": 2000, "friction": "strickler", "outflow": "h",
+                                                        "head_loss": True, "dissipation": True, "moving": True,
+                                                        "laws": "linear", "seed": 51}),
+    "ddp_mixed_chezy_z_limit_flux": ("ddp_channel", {"n_cells": 2000, "friction": "chezy", "outflow": "z",
+                                                      "div_corr": "limit_flux", "n_it_div_max": 4, "seed": 53}),
 }
 DIP_BUILDERS = {"dip_channel"}
+DDP_BUILDERS = {"ddp_channel"}
 NATIVE_KEYS = ["model_hyperb", "model_friction", "model_singular_head_loss", "num_scheme", "topo_discretization",
                "t_max", "dt_max", "dt_map", "dt_time_series", "h_min", "fr_max", "store_flag"]
 
@@ -74,6 +83,14 @@ def case_digest(case) -> str:
     for a in (case.friction, case.head_loss, case.phi_g_int, case.phi_g_bnd, case.mu):
         if a is not None:
             h.update(np.ascontiguousarray(a).tobytes())
+    for laws in (case.ddp_cell, case.ddp_edge_int, case.ddp_edge_bnd):
+        if laws is not None:
+            h.update(np.ascontiguousarray(laws.offset).tobytes())
+            h.update(np.ascontiguousarray(laws.values).tobytes())
+    if case.ddp_cell is not None:
+        h.update(np.ascontiguousarray(m.edge_int_mz).tobytes())
+        h.update(np.ascontiguousarray(m.edge_bnd_mz).tobytes())
+        h.update("".join(case.ddp_ic).encode())
     h.update(json.dumps(case.opts, sort_keys=True, default=str).encode())
     return h.hexdigest()
 

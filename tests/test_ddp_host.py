@@ -237,3 +237,58 @@ def test_host_steps_match_reference(hostlib, tmp_path, name):
             assert np.array_equal(ref.array(nm).view(np.uint64), got.view(np.uint64)), (name, k, nm)
     th, _, _ = ref.state()
     assert np.any(th > 0)
+
+
+def _ddp_golden_names():
+    from tests.conftest import golden_names
+    return [n for n in golden_names() if n.startswith("ddp_")]
+
+
+@pytest.mark.parametrize("name", _ddp_golden_names())
+def test_host_steps_match_golden(hostlib, name):
+    """The host composition against the fixtures the reference (portable exp/log) made: needs
+    no reference at run time."""
+    from tests.conftest import golden_case
+    case, fx = golden_case(name)
+    host = HostModel(hostlib, case)
+    # the reference's initial state: thetaW from the initial-condition columns
+    # (swDdp::setInitialConditions, restated here with the tabulated laws)
+    m = case.mesh
+    ntab = int(case.opts.get("n_por_tab_max", 5))
+    th, tu, tv = np.zeros(m.cell_nb), np.zeros(m.cell_nb), np.zeros(m.cell_nb)
+    for c in range(m.cell_nb):
+        z, p, t = case_mod.ddp_law_table(case.ddp_cell.record(c), float(m.cell_z_b[c]), ntab)
+        level = case.h0[c] if case.ddp_ic[0] == "z" else case.h0[c] + z[0]
+        th[c] = _theta_of_z(z, p, t, level)
+        zz = _z_of_theta(z, p, t, th[c])
+        hq = max(1e-16, zz - z[0])
+        tu[c] = th[c] * case.q0[c] if case.ddp_ic[1] == "u" else th[c] * case.q0[c] / hq
+        tv[c] = th[c] * case.r0[c] if case.ddp_ic[2] == "v" else th[c] * case.r0[c] / hq
+    host.set_state(th, tu, tv)
+    assert host.step(int(fx["steps_pm"])) == int(fx["steps_pm"])
+    assert host.t[0] == float(fx["t_pm"]) and host.dt[0] == float(fx["dt_pm"])
+    for got, key in ((host.theta, "h_pm"), (host.tu, "q_pm"), (host.tv, "r_pm")):
+        assert np.array_equal(got.view(np.uint64), np.asarray(fx[key]).view(np.uint64)), key
+
+
+def _theta_of_z(z, p, t, zz):
+    # thetaWOfZ (swDdp.cpp:2708-2736)
+    if zz <= z[0]:
+        return 0.0
+    lv = 0
+    while lv < z.size and zz > z[lv]:
+        lv += 1
+    th = float(t[lv - 1])
+    if zz > z[lv - 1]:
+        th += (zz - float(z[lv - 1])) * float(p[lv - 1])
+    return th
+
+
+def _z_of_theta(z, p, t, th):
+    # zOfThetaW (swDdp.cpp:3368-3388)
+    if th <= 0:
+        return float(z[0])
+    lv = 0
+    while lv < t.size and th > t[lv]:
+        lv += 1
+    return float(z[lv - 1]) + (th - float(t[lv - 1])) / float(p[lv - 1])

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from tests.conftest import golden_case, golden_names, load_pkg, sp_toce_case
-from tests.golden.make_golden import DIP_BUILDERS
+from tests.golden.make_golden import DDP_BUILDERS, DIP_BUILDERS
 
 oracle_binding = pytest.importorskip("oracle.binding")
 
@@ -30,13 +30,14 @@ def _bits_equal(a, b):
 def test_oracle_matches_reference_golden(name, portable):
     """The oracle with the host libm against the reference linked with glibc, and the oracle
     with the portable exp/log against the reference objects linked with them.  The C oracle
-    restates the SP step; the DIP fixtures are pinned to the live reference instead (the
-    reference re-run here must reproduce them bit for bit)."""
+    restates the SP step; the DIP and DDP fixtures are pinned to the live reference instead (the
+    reference re-run here must reproduce them bit for bit; the DDP host composition of
+    tests/test_ddp_host.py is checked against them too)."""
     case, fx = golden_case(name)
     sfx = "_pm" if portable else ""
-    if str(fx["builder"]) in DIP_BUILDERS:
+    if str(fx["builder"]) in DIP_BUILDERS | DDP_BUILDERS:
         if not os.path.isdir(os.path.join(oracle_binding.REFERENCE_SRC, "src")):
-            pytest.skip("DIP fixtures are pinned to the live reference, absent on this machine")
+            pytest.skip("DIP and DDP fixtures are pinned to the live reference, absent on this machine")
         import tempfile
         folder = tempfile.mkdtemp(prefix="sw2d_dip_")
         load_pkg().write_case(folder, case)
