@@ -61,6 +61,11 @@ def _args():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-every", type=int, default=50, help="checkpoint interval of the ensemble adjoints")
     ap.add_argument("--dip-steps", type=int, default=200)
+    ap.add_argument("--ddp-cells", type=int, default=4_000_000, help="cells of the DDP forward line (0: skip)")
+    ap.add_argument("--ddp-steps", type=int, default=200)
+    ap.add_argument("--ddp-cpu-cells", type=int, default=50_000, help="cells of the DDP reference sample")
+    ap.add_argument("--ddp-cpu-steps", type=int, default=30)
+    ap.add_argument("--ddp-only", action="store_true", help="run only the DDP forward line")
     ap.add_argument("--assim-cells", type=int, default=1_000_000,
                     help="cells of the porosity-assimilation line (the reference's differentiated step; 0: skip)")
     ap.add_argument("--assim-steps", type=int, default=2000, help="approximate steps of its trajectory")
@@ -454,6 +459,101 @@ def run_dip(pkg, args, local_rank):
             "unit": "cell-updates/s", "steps": done, "ms_per_step": ms / done, "launch_config": tune["report"]}
 
 
+def ddp_algo_bytes(nc: int, ni: int, nb: int, ntab: int) -> int:
+    """Compulsory HBM traffic of one DDP step with this library's layout: every input read once,
+    every output written once.  Cells: state {theta, theta u, theta v, z} read and written (64),
+    the derived {phiW, thetaW, Omega force} read and written (64), statics cst and dcs (64), CSR
+    offsets (12), area (8), table levels {z, phi, theta} (24 per level).  Internal edges: L/R,
+    normal, length, coefficients, slots, statics (2 records), table offset (132), table levels
+    (24 per level).  Boundary edges: cell, geometry, series index, slot (44).  Balance slots:
+    {a, b, c} + CFL share written by the edge kernel and read by the CFL and update kernels
+    (2 x 40 per slot; 2 slots per internal edge, 1 per boundary edge)."""
+    cells = nc * (64 + 64 + 64 + 12 + 8 + 24 * ntab)
+    edges = ni * (132 + 24 * ntab) + nb * 44
+    slots = (2 * ni + nb) * 2 * 40
+    return cells + edges + slots
+
+
+def _ddp_reference_sample(pkg, args):
+    """The reference's own swDdp (built from its sources) on a bounded sample of the same
+    construction: `--ddp-cpu-cells` cells, `--ddp-cpu-steps` steps, one host core."""
+    from oracle.binding import RefSolver, reference_available
+    if not reference_available():
+        return {"unavailable": "reference solver library oracle/_ref not built"}
+    case = pkg.workloads.ddp_channel(n_cells=args.ddp_cpu_cells, laws="linear", friction="manning", outflow="fr",
+                                     t_max=1.0e9, seed=61)
+    tmp = tempfile.mkdtemp(prefix="sw2d_ddp_ref_")
+    try:
+        pkg.write_case(tmp, case)
+        ref = RefSolver(tmp)
+        ref.step(2)
+        t0 = time.perf_counter()
+        done = ref.step(args.ddp_cpu_steps)
+        t1 = time.perf_counter()
+        n = ref.n
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"kind": "reference", "cores": 1, "value": n * done / (t1 - t0), "unit": "cell-updates/s",
+            "sample": f"the same construction at {n} cells, {done} steps of swDdp's loop body, {_cpu_model()}"}
+
+
+def run_ddp(pkg, args, local_rank):
+    """The depth-dependent porosity (DDP) forward step on the DDP feature channel at
+    `--ddp-cells` cells: porosity laws of types 3 (linear with an open top level), 2 and 1 on 5
+    levels per cell and per edge, Godunov + DDP HLLC (the only path of the reference's DDP
+    step), Manning, q inflow, fr outflow; graph-launched steps timed with CUDA events on the
+    library's stream, the phase shares from sw2d_phase_times."""
+    import numpy as np
+    import torch
+
+    case = pkg.workloads.ddp_channel(n_cells=args.ddp_cells, laws="linear", friction="manning", outflow="fr",
+                                     t_max=1.0e9, seed=61)
+    model = pkg.SpModel(case, device=local_rank)
+    tune = pkg.tuning.autotune(model, iters=3, device=local_rank, cache_path=None)
+    stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
+    model.step(5)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done = model.step(args.ddp_steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    phases = model.phase_times(10)
+    th = model.state()[0]
+    if not np.all(np.isfinite(th)):
+        raise RuntimeError("non-finite DDP state")
+    m = case.mesh
+    n = m.cell_nb
+    step_ms = ms / done
+    algo = ddp_algo_bytes(n, m.edge_int_nb, m.edge_bnd_nb, 5)
+    achieved = algo / (step_ms / 1e3) / 1e9
+    peak, peak_kind = _measured_peak()
+    tot = sum(phases.values())
+    line = {"workload": f"DDP feature channel at {n} cells, porosity laws 3/2/1 on 5 levels, Godunov + DDP HLLC, "
+                        f"Manning, q inflow, fr outflow", "metric": "DDP cell-updates/s", "value": n * done / (ms / 1e3),
+            "unit": "cell-updates/s", "steps": done, "ms_per_step": step_ms, "dtype": "f64",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "scope": f"whole step; algorithmic bytes {algo / n:.0f} B per cell-update x {n} cells "
+                                  f"(bench.ddp_algo_bytes) / device time per step",
+                         "kernels": {k: {"ms": v, "share": v / tot if tot > 0 else None} for k, v in phases.items()}},
+            "gpu_launches": done * model.kernels_per_step, "launch_config": tune["report"]}
+    if local_rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = _ddp_reference_sample(pkg, args)
+    return line
+
+
+def run_ddp_only(args, local_rank):
+    pkg = importlib.import_module(PKG)
+    pkg.build.build()
+    import torch
+    torch.cuda.set_device(local_rank)
+    line = run_ddp(pkg, args, local_rank)
+    line["clocks"] = None
+    print(json.dumps(line))
+
+
 def run_ensemble(pkg, args, local_rank):
     """Batched ensemble: `--ensemble-members` independent SP solves, sizes log-uniform in
     [5k, 200k] cells (seeded), alternately the dam-break and the Gaussian-bump constructions,
@@ -647,6 +747,7 @@ def run_ours(args, rank, world, local_rank):
         return
     adjoint = None if (args.no_adjoint or world > 1) else run_adjoint(pkg, args, local_rank)
     dip = None if (args.dip_cells <= 0 or world > 1) else run_dip(pkg, args, local_rank)
+    ddp = None if (args.ddp_cells <= 0 or world > 1) else run_ddp(pkg, args, local_rank)
     assim = None if (args.assim_cells <= 0 or world > 1) else run_assim(pkg, args, local_rank)
     ensemble = None if (args.ensemble_members <= 0 or world > 1) else run_ensemble(pkg, args, local_rank)
 
@@ -687,6 +788,8 @@ def run_ours(args, rank, world, local_rank):
         line["adjoint"] = adjoint
     if dip is not None:
         line["dip"] = dip
+    if ddp is not None:
+        line["ddp"] = ddp
     if assim is not None:
         line["assim"] = assim
     if ensemble is not None:
@@ -707,6 +810,9 @@ def main():
     elif args.assim_only:
         if rank == 0:
             run_assim_only(args, local_rank)
+    elif args.ddp_only:
+        if rank == 0:
+            run_ddp_only(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

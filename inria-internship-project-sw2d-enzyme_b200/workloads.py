@@ -258,35 +258,14 @@ def ddp_channel(n_cells: int = 3000, friction: str = "manning", inflow_q: float 
     n = mesh.cell_nb
     rng = np.random.default_rng(seed + 100)
     if laws == "mixed":
-        kinds = rng.choice(["3", "2", "1", "-1", "-2", "0"], size=n, p=[0.45, 0.2, 0.15, 0.1, 0.05, 0.05])
+        cell_laws, eint_laws, ebnd_laws, z_tab0 = _ddp_mixed_laws(mesh, rng, n_por_tab_max)
+    elif laws == "linear":
+        cell_laws, eint_laws, ebnd_laws, z_tab0 = _ddp_linear_laws(mesh, rng)
+        _check_uniform_law_levels(cell_laws, mesh.cell_z_b, n_por_tab_max)
+        _check_uniform_law_levels(eint_laws, mesh.edge_int_mz, n_por_tab_max)
+        _check_uniform_law_levels(ebnd_laws, mesh.edge_bnd_mz, n_por_tab_max)
     else:
-        kinds = rng.choice(["3", "2", "1"], size=n, p=[0.5, 0.3, 0.2])
-    cell_recs, pmin, nlev = [], np.empty(n), np.empty(n, dtype=np.int64)
-    for c in range(n):
-        while True:
-            rec = _ddp_cell_record(rng, str(kinds[c]), n_por_tab_max)
-            try:
-                zt, pt, _ = ddp_law_table(rec, float(mesh.cell_z_b[c]), n_por_tab_max)
-                break
-            except ValueError:   # a draw the reference cannot tabulate: draw again
-                continue
-        cell_recs.append(rec)
-        pmin[c] = float(np.min(pt))
-        nlev[c] = zt.size
-    def edge(pmax, nl, base):
-        while True:
-            rec = _ddp_edge_record(rng, pmax, nl, n_por_tab_max)
-            try:
-                ddp_law_table(rec, base, n_por_tab_max)
-                return rec
-            except ValueError:
-                continue
-
-    L, R = mesh.edge_int_cells[:, 0], mesh.edge_int_cells[:, 1]
-    eint = [edge(0.9 * min(pmin[a], pmin[b]), int(min(nlev[a], nlev[b])), float(mz))
-            for a, b, mz in zip(L.tolist(), R.tolist(), mesh.edge_int_mz.tolist())]
-    ebnd = [edge(0.9 * pmin[c], int(nlev[c]), float(mz))
-            for c, mz in zip(mesh.edge_bnd_cell.tolist(), mesh.edge_bnd_mz.tolist())]
+        raise ValueError(f"laws {laws!r} not in {{'mixed', 'linear'}}")
     opts = dict(base.opts)
     opts.update({"model_hyperb": "ddp", "n_por_tab_max": n_por_tab_max, "div_corr": div_corr,
                  "n_it_div_max": n_it_div_max, "ddp_chi_phi_max": 20.0})
@@ -295,7 +274,6 @@ def ddp_channel(n_cells: int = 3000, friction: str = "manning", inflow_q: float 
         opts["model_momentum_dissipation"] = "active"
         mu = np.stack([rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 0.5, n), rng.uniform(0.0, 90.0, n)])
     level = base.h0.copy()
-    z_tab0 = np.array([float(mesh.cell_z_b[c]) + float(cell_recs[c][2]) for c in range(n)])
     wet = level > 0.0
     qx = np.where(wet, 0.05, 0.0) if moving else np.zeros(n)
     qy = np.where(wet, 0.01, 0.0) if moving else np.zeros(n)
@@ -311,6 +289,108 @@ def ddp_channel(n_cells: int = 3000, friction: str = "manning", inflow_q: float 
     bc = BoundarySeries(codes=bc.codes, types=list(bc.types), times=bc.times, values=values)
     return Case(mesh=mesh, opts=opts, h0=level, q0=qx, r0=qy, phi=np.ones(n), boussinesq=base.boussinesq,
                 friction=base.friction, head_loss=base.head_loss, bc=bc, mu=mu,
-                extra={"name": "ddp_channel"}, ddp_cell=LawRecords.from_list(cell_recs),
-                ddp_edge_int=LawRecords.from_list(eint), ddp_edge_bnd=LawRecords.from_list(ebnd),
+                extra={"name": "ddp_channel"}, ddp_cell=cell_laws, ddp_edge_int=eint_laws, ddp_edge_bnd=ebnd_laws,
                 ddp_ic=(ic[0], ic[1], ic[2]))
+
+
+def _ddp_mixed_laws(mesh, rng, ntab: int):
+    """Every law type, record by record (small cases)."""
+    n = mesh.cell_nb
+    kinds = rng.choice(["3", "2", "1", "-1", "-2", "0"], size=n, p=[0.45, 0.2, 0.15, 0.1, 0.05, 0.05])
+    cell_recs, pmin, nlev = [], np.empty(n), np.empty(n, dtype=np.int64)
+    for c in range(n):
+        while True:
+            rec = _ddp_cell_record(rng, str(kinds[c]), ntab)
+            try:
+                zt, pt, _ = ddp_law_table(rec, float(mesh.cell_z_b[c]), ntab)
+                break
+            except ValueError:   # a draw the reference cannot tabulate: draw again
+                continue
+        cell_recs.append(rec)
+        pmin[c] = float(np.min(pt))
+        nlev[c] = zt.size
+
+    def edge(pmax, nl, base):
+        while True:
+            rec = _ddp_edge_record(rng, pmax, nl, ntab)
+            try:
+                ddp_law_table(rec, base, ntab)
+                return rec
+            except ValueError:
+                continue
+
+    L, R = mesh.edge_int_cells[:, 0], mesh.edge_int_cells[:, 1]
+    eint = [edge(0.9 * min(pmin[a], pmin[b]), int(min(nlev[a], nlev[b])), float(mz))
+            for a, b, mz in zip(L.tolist(), R.tolist(), mesh.edge_int_mz.tolist())]
+    ebnd = [edge(0.9 * pmin[c], int(nlev[c]), float(mz))
+            for c, mz in zip(mesh.edge_bnd_cell.tolist(), mesh.edge_bnd_mz.tolist())]
+    z_tab0 = np.array([float(mesh.cell_z_b[c]) + float(cell_recs[c][2]) for c in range(n)])
+    return LawRecords.from_list(cell_recs), LawRecords.from_list(eint), LawRecords.from_list(ebnd), z_tab0
+
+
+def _records(kind: np.ndarray, columns: Dict[int, np.ndarray]) -> LawRecords:
+    """Records of law types 3 (7 values), 2 (6) and 1 (4), built array-wise: columns[t] holds
+    the (count_t, length_t) rows of type t in record order."""
+    length = np.where(kind == 3, 7, np.where(kind == 2, 6, 4)).astype(np.int64)
+    off = np.zeros(kind.size + 1, dtype=np.int64)
+    np.cumsum(length, out=off[1:])
+    vals = np.empty(int(off[-1]))
+    for t, rows in columns.items():
+        idx = np.flatnonzero(kind == t)
+        if idx.size:
+            cols = np.arange(rows.shape[1])
+            vals[(off[idx][:, None] + cols[None, :]).reshape(-1)] = rows.reshape(-1)
+    return LawRecords(off, vals)
+
+
+def _linear_rows(kind, rng, pmax=None):
+    """Rows of law types 3 / 2 / 1 ({law, n, z0, phi0, z1, phi1[, phi2]} / {1, 2, z0, phi}); with
+    pmax the porosities are scaled below it (edges)."""
+    m = kind.size
+    z0 = np.where(rng.uniform(size=m) < 0.7, 0.0, rng.uniform(0.0, 0.04, m))
+    s = np.ones(m) if pmax is None else pmax
+    p0 = rng.uniform(0.3, 0.7, m) * (1.0 if pmax is None else 1.0)
+    dz3 = rng.uniform(0.15, 0.5, m)
+    p1 = rng.uniform(0.5, 0.9, m)
+    p2 = rng.uniform(0.8, 1.0, m)
+    if pmax is not None:
+        p0, p1, p2 = s * rng.uniform(0.3, 1.0, m), s * rng.uniform(0.5, 1.0, m), s * rng.uniform(0.7, 1.0, m)
+    q0 = rng.uniform(0.4, 0.8, m) if pmax is None else s * rng.uniform(0.4, 1.0, m)
+    q1 = rng.uniform(0.6, 1.0, m) if pmax is None else s * rng.uniform(0.4, 1.0, m)
+    dz2 = rng.uniform(0.2, 0.7, m)
+    u = rng.uniform(0.5, 1.0, m) if pmax is None else s * rng.uniform(0.4, 1.0, m)
+    rows = {3: np.stack([np.full(m, 3.0), np.full(m, 5.0), z0, p0, z0 + dz3, p1, p2], axis=1),
+            2: np.stack([np.full(m, 2.0), np.full(m, 4.0), z0, q0, z0 + dz2, q1], axis=1),
+            1: np.stack([np.full(m, 1.0), np.full(m, 2.0), z0, u], axis=1)}
+    sel = {t: rows[t][kind == t] for t in (3, 2, 1)}
+    # smallest tabulated porosity of each record (the tables interpolate between these values)
+    pmin = np.where(kind == 3, np.minimum(np.minimum(p0, p1), p2), np.where(kind == 2, np.minimum(q0, q1), u))
+    return sel, pmin, z0
+
+
+def _ddp_linear_laws(mesh, rng):
+    """Law types 3, 2 and 1 only, array-wise (large cases)."""
+    n = mesh.cell_nb
+    kind = rng.choice(np.array([3, 2, 1]), size=n, p=[0.5, 0.3, 0.2])
+    rows, pmin, z0 = _linear_rows(kind, rng)
+    cell = _records(kind, rows)
+    L, R = mesh.edge_int_cells[:, 0], mesh.edge_int_cells[:, 1]
+    ki = rng.choice(np.array([3, 2, 1]), size=mesh.edge_int_nb, p=[0.5, 0.25, 0.25])
+    ri, _, _ = _linear_rows(ki, rng, pmax=0.9 * np.minimum(pmin[L], pmin[R]))
+    kb = rng.choice(np.array([3, 2, 1]), size=mesh.edge_bnd_nb, p=[0.5, 0.25, 0.25])
+    rb, _, _ = _linear_rows(kb, rng, pmax=0.9 * pmin[mesh.edge_bnd_cell])
+    return cell, _records(ki, ri), _records(kb, rb), mesh.cell_z_b + z0
+
+
+def _check_uniform_law_levels(laws: LawRecords, base: np.ndarray, ntab: int) -> None:
+    """Law type 1 re-tabulates {z, z + 1}: its top level z + (ntab - 1) dz must not exceed z + 1
+    after rounding, or the reference reads past its point list (swDdp.cpp:2616-2620)."""
+    first = laws.values[laws.offset[:-1]]
+    idx = np.flatnonzero(first == 1.0)
+    if idx.size == 0:
+        return
+    z = base[idx] + laws.values[laws.offset[idx] + 2]
+    z1 = z + 1.0
+    dz = (z1 - z) / float(ntab - 1)
+    if np.any(z + float(ntab - 1) * dz > z1):
+        raise ValueError(f"n_por_tab_max = {ntab}: a uniform law's top level rounds above its last point")
