@@ -463,13 +463,13 @@ def ddp_algo_bytes(nc: int, ni: int, nb: int, ntab: int) -> int:
     """Compulsory HBM traffic of one DDP step with this library's layout: every input read once,
     every output written once.  Cells: state {theta, theta u, theta v, z} read and written (64),
     the derived {phiW, thetaW, Omega force} read and written (64), statics cst and dcs (64), CSR
-    offsets (12), area (8), table levels {z, phi, theta} (24 per level).  Internal edges: L/R,
-    normal, length, coefficients, slots, statics (2 records), table offset (132), table levels
-    (24 per level).  Boundary edges: cell, geometry, series index, slot (44).  Balance slots:
-    {a, b, c} + CFL share written by the edge kernel and read by the CFL and update kernels
-    (2 x 40 per slot; 2 slots per internal edge, 1 per boundary edge)."""
-    cells = nc * (64 + 64 + 64 + 12 + 8 + 24 * ntab)
-    edges = ni * (132 + 24 * ntab) + nb * 44
+    offsets (12), area (8), table levels {z, phi} (16 per level; theta is rebuilt from them).
+    Internal edges: L/R, normal, length, coefficients, slots, statics (2 records), table offset
+    (132), table levels (16 per level).  Boundary edges: cell, geometry, series index, slot (44).
+    Balance slots: {a, b, c} + CFL share written by the edge kernel and read by the CFL and
+    update kernels (2 x 40 per slot; 2 slots per internal edge, 1 per boundary edge)."""
+    cells = nc * (64 + 64 + 64 + 12 + 8 + 16 * ntab)
+    edges = ni * (132 + 16 * ntab) + nb * 44
     slots = (2 * ni + nb) * 2 * 40
     return cells + edges + slots
 

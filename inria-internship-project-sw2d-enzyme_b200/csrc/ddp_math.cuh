@@ -21,9 +21,17 @@ constexpr unsigned kStatusTable = 128u;  // NaN elevation or volume in a porosit
 
 namespace ddp {
 
-// one level of a porosity table: {z_k, phi_k, theta_k}
-struct alignas(32) Lvl {
-    double z, phi, theta, pad;
+// one level of a porosity table as it is stored: {z_k, phi_k}.  The cumulated volume
+// theta_k = theta_(k-1) + (z_k - z_(k-1)) phi_(k-1), theta_0 = 0, is rebuilt while a lookup walks
+// the levels, by the recurrence that builds the reference's thetaW_tab (swDdp.cpp:1921-1929),
+// so it has the same bits and the table keeps 16 bytes per level.
+struct alignas(16) Lvl {
+    double z, phi;
+};
+
+// a level with its cumulated volume
+struct LvlT {
+    double z, phi, theta;
 };
 
 struct PhiTheta {
@@ -32,59 +40,168 @@ struct PhiTheta {
 
 SW2D_HD double quiet_nan() { return __builtin_nan(""); }
 
-// phiWOfZ / phiGIntOfZ (swDdp.cpp:1049-1097) and thetaWOfZ / thetaGIntOfZ (swDdp.cpp:2678-2736)
-// at the same elevation: both run the same scan, so one scan gives both.
-SW2D_HD PhiTheta phi_theta(const Lvl* t, int n, double z, unsigned& bad)
+SW2D_HD Lvl load_level(const Lvl* p)
 {
-    if (z <= t[0].z) return {0.0, 0.0};
-    int l = 0;
-    while ((l < n) && (z > t[l].z)) ++l;
-    if (l == 0) {
-        bad |= kStatusTable;
-        return {quiet_nan(), quiet_nan()};
-    }
-    const Lvl a = t[l - 1];
-    double theta = a.theta;
-    if (z > a.z) theta += (z - a.z) * a.phi;
-    return {a.phi, theta};
+#if defined(__CUDA_ARCH__)
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    return Lvl{a.x, a.y};
+#else
+    return *p;
+#endif
 }
 
-// swDdp::zOfThetaW (swDdp.cpp:3368-3388)
+// Visits the n levels of a table in order with their cumulated volumes.  Every level is
+// visited (no early exit, so the loads do not wait on the comparisons): the reference's scans
+// stop at the first failing comparison, which the visitors below reproduce with a flag.
+template <class F>
+SW2D_HD void for_levels(const Lvl* t, int n, F&& f)
+{
+    double theta = 0.0;
+    Lvl prev{0.0, 0.0};
+    for (int k = 0; k < n; k++) {
+        const Lvl lv = load_level(t + k);
+        if (k > 0) theta += (lv.z - prev.z) * prev.phi;
+        f(k, LvlT{lv.z, lv.phi, theta});
+        prev = lv;
+    }
+}
+
+// One pass over a table answering phiWOfZ / thetaWOfZ (equally phiGIntOfZ / thetaGIntOfZ;
+// swDdp.cpp:1049-1097, 2678-2736) at the NQ elevations zq and the pressure-force integral
+// pressureForceOmegaOfZ / pressureForceGammaOfZ (swDdp.cpp:1214-1273) at the NP elevations zp,
+// each with the reference's own scan semantics and summation order:
+//   phi, theta at z: 0 at or below z_0; else level l - 1 where l counts the leading levels with
+//     z > z_k (the scan stops at the first that fails), theta = theta_(l-1) + (z - z_(l-1)) phi_(l-1);
+//   force at z: when z > z_0, sum over the leading levels k >= 1 with z >= z_k of
+//     phi_(k-1) (z - (z_(k-1) + z_k) / 2) (z_k - z_(k-1)), then phi_l max(0, z - z_l)^2 / 2 at
+//     the last such level l; times g.
+template <int NQ, int NP>
+SW2D_HD void table_pass(const Lvl* t, int n, const double* zq, PhiTheta* pq, const double* zp, double* pp,
+                        unsigned& bad)
+{
+    const double z0 = load_level(t).z;
+    bool run[NQ > 0 ? NQ : 1];
+    bool hit[NQ > 0 ? NQ : 1];
+    LvlT a[NQ > 0 ? NQ : 1];
+    bool prun[NP > 0 ? NP : 1];
+    bool started[NP > 0 ? NP : 1];
+    double acc[NP > 0 ? NP : 1];
+    LvlT cur[NP > 0 ? NP : 1];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        run[q] = true;
+        hit[q] = false;
+        a[q] = LvlT{0, 0, 0};
+    }
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+        started[p] = zp[p] > z0;
+        prun[p] = started[p];
+        acc[p] = 0;
+        cur[p] = LvlT{0, 0, 0};
+    }
+    LvlT prev{0, 0, 0};
+    for_levels(t, n, [&](int k, const LvlT& lv) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            if (run[q]) {
+                if (zq[q] > lv.z) {
+                    hit[q] = true;
+                    a[q] = lv;
+                } else {
+                    run[q] = false;
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            if (k == 0) {
+                cur[p] = lv;
+            } else if (prun[p] && zp[p] >= lv.z) {
+                const double dz1 = zp[p] - (prev.z + lv.z) / 2.;
+                const double dz2 = lv.z - prev.z;
+                acc[p] += prev.phi * dz1 * dz2;
+                cur[p] = lv;
+            } else {
+                prun[p] = false;
+            }
+        }
+        prev = lv;
+    });
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        if (zq[q] <= z0) {
+            pq[q] = PhiTheta{0.0, 0.0};
+        } else if (!hit[q]) {
+            bad |= kStatusTable;
+            pq[q] = PhiTheta{quiet_nan(), quiet_nan()};
+        } else {
+            double theta = a[q].theta;
+            if (zq[q] > a[q].z) theta += (zq[q] - a[q].z) * a[q].phi;
+            pq[q] = PhiTheta{a[q].phi, theta};
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+        double v = 0;
+        if (started[p]) {
+            v = acc[p];
+            const double dz1 = smax(0., zp[p] - cur[p].z);
+            v += cur[p].phi * dz1 * dz1 / 2.;
+        }
+        v *= kGravity;
+        pp[p] = v;
+    }
+}
+
+// phiWOfZ and thetaWOfZ at one elevation
+SW2D_HD PhiTheta phi_theta(const Lvl* t, int n, double z, unsigned& bad)
+{
+    const double zq[1] = {z};
+    PhiTheta pq[1];
+    const double zp[1] = {0.0};
+    double pp[1];
+    table_pass<1, 0>(t, n, zq, pq, zp, pp, bad);
+    return pq[0];
+}
+
+// pressureForceOmegaOfZ / pressureForceGammaOfZ at one elevation
+SW2D_HD double pressure_force(const Lvl* t, int n, double z)
+{
+    unsigned bad = 0;
+    const double zq[1] = {0.0};
+    PhiTheta pq[1];
+    const double zp[1] = {z};
+    double pp[1];
+    table_pass<0, 1>(t, n, zq, pq, zp, pp, bad);
+    return pp[0];
+}
+
+// swDdp::zOfThetaW (swDdp.cpp:3368-3388): theta_0 ... scanned while theta > theta_k
 SW2D_HD double z_of_theta(const Lvl* t, int n, double theta, unsigned& bad)
 {
-    if (theta <= 0) return t[0].z;
-    int l = 0;
-    while ((l < n) && (theta > t[l].theta)) ++l;
-    if (l == 0) {
+    bool run = true, hit = false;
+    LvlT a{0, 0, 0};
+    double z0 = 0;
+    for_levels(t, n, [&](int k, const LvlT& lv) {
+        if (k == 0) z0 = lv.z;
+        if (run) {
+            if (theta > lv.theta) {
+                hit = true;
+                a = lv;
+            } else {
+                run = false;
+            }
+        }
+    });
+    if (theta <= 0) return z0;
+    if (!hit) {
         bad |= kStatusTable;
         return quiet_nan();
     }
-    const Lvl a = t[l - 1];
     double z = a.z;
     z += (theta - a.theta) / a.phi;
     return z;
-}
-
-// swDdp::pressureForceOmegaOfZ / pressureForceGammaOfZ (swDdp.cpp:1214-1273): g times the
-// integral of phi(zeta) (z - zeta) over the wetted levels.
-SW2D_HD double pressure_force(const Lvl* t, int n, double z)
-{
-    double p = 0;
-    if (z > t[0].z) {
-        int l = 0;
-        while ((l < n - 1) && (z >= t[l + 1].z)) {
-            const double z1 = t[l].z;
-            const double z2 = t[l + 1].z;
-            const double dz1 = z - (z1 + z2) / 2.;
-            const double dz2 = z2 - z1;
-            p += t[l].phi * dz1 * dz2;
-            ++l;
-        }
-        const double dz1 = smax(0., z - t[l].z);
-        p += t[l].phi * dz1 * dz1 / 2.;
-    }
-    p *= kGravity;
-    return p;
 }
 
 // swDdp::pressureWaveCelerity (swDdp.cpp:1276-1286)
@@ -111,15 +228,17 @@ SW2D_HD double spec_force(double theta_velocity, double velocity, double pressur
 // One side of an internal edge in swDdp::hypGodunovComputeLRStates (swDdpHypGodunov.cpp:59-149):
 // the rotated momentum (zeroed on a shallow side that has an interface) and the wave speeds
 // lambda-/+ with x_phi = phiW/phiG and x_theta = thetaW/thetaG.  `omega` and `gamma` are the
-// cell's and the edge's tables at the side's elevation, `omega_min` and `gamma_min` at the
-// reference's shallow-side elevation (cell_z_tab[L][0] + h_min on the left, cell_z_tab[R][1] +
-// h_min on the right, as swDdpHypGodunov.cpp:84,130 write them).
+// cell's and the edge's tables at the side's elevation; `shallow(omega_min, gamma_min)` gives
+// them at the reference's shallow-side elevation (cell_z_tab[L][0] + h_min on the left,
+// cell_z_tab[R][1] + h_min on the right, as swDdpHypGodunov.cpp:84,130 write them), asked for
+// only on a shallow side that has an interface.
 struct Side {
     double tu, tv, lm, lp;
 };
 
+template <class MinF>
 SW2D_HD Side lr_side(double theta, double thu, double thv, double z, double z_tab0, double b, double nx, double ny,
-                     PhiTheta omega, PhiTheta gamma, PhiTheta omega_min, PhiTheta gamma_min, double h_min)
+                     PhiTheta omega, PhiTheta gamma, MinF&& shallow, double h_min)
 {
     const double h = smax(z - z_tab0, 0.);
     Side s;
@@ -132,6 +251,8 @@ SW2D_HD Side lr_side(double theta, double thu, double thv, double z, double z_ta
         if (h < h_min) {
             s.tu = 0.;
             s.tv = 0.;
+            PhiTheta omega_min, gamma_min;
+            shallow(omega_min, gamma_min);  // the tables at the shallow-side level
             phi_omega = omega_min.phi;
             phi_gamma = gamma_min.phi;
             theta_omega = omega_min.theta;

@@ -20,8 +20,9 @@
 // predicated on the device), and k_ddp_finish does the rest.  Every kernel reads the loop
 // control on the device, so a CUDA graph of many steps runs without the host.
 //
-// Tables live in HBM as levels {z, phi, theta} (32 bytes each), cells and internal edges in the
-// internal numbering with CSR offsets; boundary-edge tables are read and checked but the step
+// Tables live in HBM as levels {z, phi} (16 bytes each; the cumulated volume is rebuilt on the
+// fly by the recurrence that built it), cells and internal edges in the internal numbering with
+// CSR offsets; boundary-edge tables are read and checked but the step
 // never uses them (swDdpHyp.cpp:38-48 and swDdpHypGodunov.cpp:39-42 force phiG = phiW there).
 // Balance slots, their order and their persistence are the SP step's (sw2d_sp.cu): the DDP
 // edge factors are w / area (swDdp.cpp:399-489), the SP ones with phi = 1.
@@ -98,9 +99,11 @@ __device__ __forceinline__ double derive_cell(const DevMesh& m, int c, double th
     const int o = ld(&m.ctoff[c]), n = ld(&m.ctoff[c + 1]) - o;
     const Lvl* t = m.ctab + o;
     const double z = ddp::z_of_theta(t, n, th, bad);
-    const PhiTheta pt = ddp::phi_theta(t, n, z, bad);
-    const double p = ddp::pressure_force(t, n, z);
-    m.dv[c] = make_double4(pt.phi, pt.theta, p, 0.0);
+    const double zq[1] = {z};
+    PhiTheta pt[1];
+    double p[1];
+    ddp::table_pass<1, 1>(t, n, zq, pt, zq, p, bad);
+    m.dv[c] = make_double4(pt[0].phi, pt[0].theta, p[0], 0.0);
     return z;
 }
 
@@ -156,23 +159,39 @@ __global__ void __launch_bounds__(kB, kMinB) k_ddp_edges(DevMesh m)
         const int a = lr.x, b = lr.y;
         const double2 n = ld(&m.nxy[e]);
         const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);   // {theta, theta u, theta v, z}
-        const double4 va = ld(&m.dv[a]), vb = ld(&m.dv[b]);   // {phiW, thetaW, force Omega, -} at z
-        const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]); // {z_b, boussinesq, z_tab[0], area}
-        const double4 ma = ld(&m.dcs[a]), mb = ld(&m.dcs[b]);
-        const double4 e0 = ld(&m.des[2 * e]), e1 = ld(&m.des[2 * e + 1]);
+        const double2 va = ld(reinterpret_cast<const double2*>(&m.dv[a]));  // {phiW, thetaW} at z
+        const double2 vb = ld(reinterpret_cast<const double2*>(&m.dv[b]));
+        const double2 ca = ld(reinterpret_cast<const double2*>(&m.cst[a]));  // {z_b, boussinesq}
+        const double2 cb = ld(reinterpret_cast<const double2*>(&m.cst[b]));
+        const double ta0 = ld(&m.cst[a].z), tb0 = ld(&m.cst[b].z);  // lowest table levels
         const int eo = ld(&m.etoff[e]), en = ld(&m.etoff[e + 1]) - eo;
         const Lvl* et = m.etab + eo;
-        const PhiTheta gL = ddp::phi_theta(et, en, sa.w, bad);
-        const PhiTheta gR = ddp::phi_theta(et, en, sb.w, bad);
+        // the edge's table at both sides' levels: phiG, thetaG and the pressure force on the edge
+        const double zs[2] = {sa.w, sb.w};
+        PhiTheta gs[2];
+        double fg[2];
+        ddp::table_pass<2, 2>(et, en, zs, gs, zs, fg, bad);
         const PhiTheta oL{va.x, va.y}, oR{vb.x, vb.y};
-        const ddp::Side SL = ddp::lr_side(sa.x, sa.y, sa.z, sa.w, ca.z, ca.y, n.x, n.y, oL, gL, PhiTheta{ma.x, ma.y},
-                                          PhiTheta{e0.z, e0.w}, m.h_min);
-        const ddp::Side SR = ddp::lr_side(sb.x, sb.y, sb.z, sb.w, cb.z, cb.y, n.x, n.y, oR, gR, PhiTheta{mb.z, mb.w},
-                                          PhiTheta{e1.x, e1.y}, m.h_min);
+        const ddp::Side SL = ddp::lr_side(
+            sa.x, sa.y, sa.z, sa.w, ta0, ca.y, n.x, n.y, oL, gs[0],
+            [&](PhiTheta& om, PhiTheta& gm) {
+                const double4 ma = ld(&m.dcs[a]), e0 = ld(&m.des[2 * e]);
+                om = PhiTheta{ma.x, ma.y};
+                gm = PhiTheta{e0.z, e0.w};
+            },
+            m.h_min);
+        const ddp::Side SR = ddp::lr_side(
+            sb.x, sb.y, sb.z, sb.w, tb0, cb.y, n.x, n.y, oR, gs[1],
+            [&](PhiTheta& om, PhiTheta& gm) {
+                const double4 mb = ld(&m.dcs[b]), e1 = ld(&m.des[2 * e + 1]);
+                om = PhiTheta{mb.z, mb.w};
+                gm = PhiTheta{e1.x, e1.y};
+            },
+            m.h_min);
         const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
         if (m.lmax) m.lmax[e] = lm;
         const double lw = lm * ld(&m.len[e]);
-        const bool wetL = sa.w - ca.z > m.h_min, wetR = sb.w - cb.z > m.h_min;
+        const bool wetL = sa.w - ta0 > m.h_min, wetR = sb.w - tb0 > m.h_min;
         const int2 sl = ld(&m.eslot[e]);
         m.slot_w[sl.x] = wetL ? lw : 0.0;
         m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
@@ -197,16 +216,17 @@ __global__ void __launch_bounds__(kB, kMinB) k_ddp_edges(DevMesh m)
             }
             in.omega_L = oL;
             in.omega_R = oR;
-            in.gamma_L = gL;
-            in.gamma_R = gR;
+            in.gamma_L = gs[0];
+            in.gamma_R = gs[1];
             const int ao = ld(&m.ctoff[a]), an = ld(&m.ctoff[a + 1]) - ao;
             const int bo = ld(&m.ctoff[b]), bn = ld(&m.ctoff[b + 1]) - bo;
             in.theta_RL = ddp::phi_theta(m.ctab + bo, bn, sa.w, bad).theta;
             in.theta_LR = ddp::phi_theta(m.ctab + ao, an, sb.w, bad).theta;
-            in.force_omega_L = va.z;
-            in.force_omega_R = vb.z;
-            in.force_gamma_L = ddp::pressure_force(et, en, sa.w);
-            in.force_gamma_R = ddp::pressure_force(et, en, sb.w);
+            in.force_omega_L = ld(&m.dv[a].z);
+            in.force_omega_R = ld(&m.dv[b].z);
+            in.force_gamma_L = fg[0];
+            in.force_gamma_R = fg[1];
+            const double2 e0 = ld(reinterpret_cast<const double2*>(&m.des[2 * e]));
             in.theta_gamma_hmin = e0.x;
             in.z_gamma_min = e0.y;
             const ddp::Flux f = ddp::hllc(in, m.h_min, m.chi_phi_max);
@@ -312,7 +332,7 @@ __device__ __forceinline__ void finish_cell(const DevMesh& m, int c, double dt, 
 
 // k_ddp_update: the whole cell update when no divergence correction is selected
 template <int kF, bool kHL, bool kDissip>
-__global__ void __launch_bounds__(kBlock, 4) k_ddp_update(DevMesh m)
+__global__ void __launch_bounds__(kBlock, 3) k_ddp_update(DevMesh m)
 {
     Ctrl* ctrl = m.ctrl;
     if (!ctrl->go) return;
@@ -618,7 +638,7 @@ __global__ void k_lf_next(DevMesh m)
 // k_ddp_finish: after a divergence correction (time-step limitation: re-weights the state when
 // some cell dries, swDdpHyp.cpp:756-766), the rest of the step with the final dt
 template <int kF, bool kHL, bool kTs>
-__global__ void __launch_bounds__(kBlock, 4) k_ddp_finish(DevMesh m)
+__global__ void __launch_bounds__(kBlock, 3) k_ddp_finish(DevMesh m)
 {
     Ctrl* ctrl = m.ctrl;
     if (!ctrl->go) return;
@@ -754,7 +774,7 @@ __global__ void k_scatter_field(const double* __restrict__ src, int stride, int 
 struct Variant {
     int block, minb;
 };
-constexpr Variant kDdpVariants[] = {{256, 3}, {256, 2}, {256, 4}, {128, 4}, {128, 8}, {512, 1}};
+constexpr Variant kDdpVariants[] = {{256, 2}, {128, 4}, {256, 3}, {192, 3}, {128, 5}, {512, 1}};
 
 template <int V>
 void launch_edges_v(sw2d_handle* h, const DevMesh& m)
@@ -981,7 +1001,7 @@ std::vector<Lvl> levels_in_order(const DdpTables& t, const std::vector<int>& per
     lv.reserve(t.z.size());
     for (size_t i = 0; i < perm.size(); i++) {
         const int64_t o = perm[i];
-        for (int64_t k = t.off[o]; k < t.off[o + 1]; k++) lv.push_back(Lvl{t.z[k], t.phi[k], t.theta[k], 0.0});
+        for (int64_t k = t.off[o]; k < t.off[o + 1]; k++) lv.push_back(Lvl{t.z[k], t.phi[k]});
         off[i + 1] = (int)lv.size();
     }
     return lv;
@@ -1001,6 +1021,13 @@ void launch_ddp_edges(sw2d_handle* h, const DevMesh& m, int v)
         case 5: launch_edges_v<5>(h, m); break;
         default: launch_edges_v<0>(h, m); break;
     }
+}
+
+void ddp_variant(int v, int* block, int* minb)
+{
+    const Variant x = kDdpVariants[(v >= 0 && v < 6) ? v : 0];
+    *block = x.block;
+    *minb = x.minb;
 }
 
 void launch_ddp_phase(sw2d_handle* h, int i)
@@ -1072,7 +1099,7 @@ int ddp_setup(sw2d_handle* h, const sw2d_mesh* mesh, const sw2d_cell_fields* fie
     (void)fields;
     DdpState* d = new DdpState();
     h->ddp = d;
-    h->edge_variant = 1;  // {256, 2}: the DDP edge kernel's registers without spills
+    h->edge_variant = 0;  // {256, 2}: the DDP edge kernel's registers without spills
     d->div_corr = ddp->div_corr;
     d->n_it_div_max = (int)ddp->n_it_div_max;
     const int64_t nc = h->nc, ni = h->ni, nb = h->nb;

@@ -288,6 +288,8 @@ void launch_ddp_step(sw2d_handle* h);
 // phase i of a DDP step (0 none, 1 edges, 2 cfl, 3 the cell update and any divergence correction)
 void launch_ddp_phase(sw2d_handle* h, int i);
 void launch_ddp_edges(sw2d_handle* h, const DevMesh& m, int variant);
+// {threads per block, minimum resident blocks} of the DDP edge kernel's launch variant v
+void ddp_variant(int v, int* block, int* minb);
 int ddp_kernels_per_step(sw2d_handle* h);
 int64_t ddp_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity, bool* handled);
 int64_t ddp_get_table(sw2d_handle* h, int which, int64_t record, double* z, double* phi, double* theta,

@@ -1220,11 +1220,16 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
         }
         launch_slopes(h, h->slope_variant);
     }
+    auto label = [&](int v) {
+        int b = kVariants[v].block, mb = kVariants[v].minb;
+        if (h->model == kModelDdp) ddp_variant(v, &b, &mb);
+        return std::to_string(b) + "x" + std::to_string(mb);
+    };
     double best = 1e300;
     for (int v = 0; v < kNumVariants; v++) {
         double ms = time_it([&] { launch_edges(h, v); });
-        rep += "k_edges/" + std::to_string(kVariants[v].block) + "x" + std::to_string(kVariants[v].minb) + "=" +
-               std::to_string(ms) + "ms ";
+        rep += std::string(h->model == kModelDdp ? "k_ddp_edges/" : "k_edges/") + label(v) + "=" + std::to_string(ms) +
+               "ms ";
         if (ms < best) {
             best = ms;
             h->edge_variant = v;
@@ -1239,8 +1244,8 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
         h->graph = nullptr;
     }
     rep += "chosen k_slopes/" + std::to_string(kVariants[h->slope_variant].block) + "x" +
-           std::to_string(kVariants[h->slope_variant].minb) + " k_edges/" +
-           std::to_string(kVariants[h->edge_variant].block) + "x" + std::to_string(kVariants[h->edge_variant].minb);
+           std::to_string(kVariants[h->slope_variant].minb) + (h->model == kModelDdp ? " k_ddp_edges/" : " k_edges/") +
+           label(h->edge_variant);
     if (report && capacity > 0) {
         std::strncpy(report, rep.c_str(), (size_t)capacity - 1);
         report[capacity - 1] = '\0';

@@ -62,10 +62,10 @@ Tabs make_tabs(const HostCase& c)
     Tabs t;
     t.cell.resize(c.nc);
     for (int64_t i = 0; i < c.nc; i++)
-        for (int64_t k = c.ctoff[i]; k < c.ctoff[i + 1]; k++) t.cell[i].push_back(Lvl{c.cz[k], c.cphi[k], c.ctheta[k], 0});
+        for (int64_t k = c.ctoff[i]; k < c.ctoff[i + 1]; k++) t.cell[i].push_back(Lvl{c.cz[k], c.cphi[k]});
     t.eint.resize(c.ni);
     for (int64_t i = 0; i < c.ni; i++)
-        for (int64_t k = c.etoff[i]; k < c.etoff[i + 1]; k++) t.eint[i].push_back(Lvl{c.ez[k], c.ephi[k], c.etheta[k], 0});
+        for (int64_t k = c.etoff[i]; k < c.etoff[i + 1]; k++) t.eint[i].push_back(Lvl{c.ez[k], c.ephi[k]});
     return t;
 }
 
@@ -110,9 +110,19 @@ int one_step(const HostCase& c, const Tabs& T, HostState& s)
         const auto& tb = T.cell[b];
         const auto& te = T.eint[e];
         SL[e] = ddp::lr_side(s.theta[a], s.tu[a], s.tv[a], z[a], ta[0].z, c.bous[a], c.nx[e], c.ny[e], pt(ta, z[a], bad),
-                             pt(te, z[a], bad), pt(ta, ta[0].z + c.h_min, bad), pt(te, ta[0].z + c.h_min, bad), c.h_min);
+                             pt(te, z[a], bad),
+                             [&](PhiTheta& om, PhiTheta& gm) {
+                                 om = pt(ta, ta[0].z + c.h_min, bad);
+                                 gm = pt(te, ta[0].z + c.h_min, bad);
+                             },
+                             c.h_min);
         SR[e] = ddp::lr_side(s.theta[b], s.tu[b], s.tv[b], z[b], tb[0].z, c.bous[b], c.nx[e], c.ny[e], pt(tb, z[b], bad),
-                             pt(te, z[b], bad), pt(tb, tb[1].z + c.h_min, bad), pt(te, tb[1].z + c.h_min, bad), c.h_min);
+                             pt(te, z[b], bad),
+                             [&](PhiTheta& om, PhiTheta& gm) {
+                                 om = pt(tb, tb[1].z + c.h_min, bad);
+                                 gm = pt(te, tb[1].z + c.h_min, bad);
+                             },
+                             c.h_min);
         s.lmi[e] = max4(std::fabs(SL[e].lm), std::fabs(SL[e].lp), std::fabs(SR[e].lm), std::fabs(SR[e].lp));
     }
     // ---- time step (swDdpHyp.cpp:522-636)
@@ -397,7 +407,7 @@ extern "C" int ddp_host_steps(const HostCase* c, HostState* s, int n)
 extern "C" double ddp_host_z_of_theta(const double* z, const double* phi, const double* theta, int n, double th)
 {
     std::vector<Lvl> t(n);
-    for (int i = 0; i < n; i++) t[i] = Lvl{z[i], phi[i], theta[i], 0};
+    for (int i = 0; i < n; i++) t[i] = Lvl{z[i], phi[i]};
     unsigned bad = 0;
     return ddp::z_of_theta(t.data(), n, th, bad);
 }
