@@ -225,6 +225,27 @@ int sw2d_create_ddp(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d
 int64_t sw2d_ddp_get_table(sw2d_handle* h, int which, int64_t record, double* z, double* phi, double* theta,
                            int64_t capacity);
 
+/* Case folders.  sw2d_load_case replaces sw2dSolver's main up to init (src/sw2dSolver/main.cpp:
+ * 99-163): it reads input/input.solv (swSolverParam::readInputFile), input/geometry.sw2d version 2
+ * (swMesh::readGeometryFileV2), the initial conditions, the porosity maps of the model that
+ * model_hyperb names (sp, dip or ddp), the Boussinesq, friction, singular head loss and
+ * momentum dissipation maps and the boundary time series, with the reference's readers' formats
+ * and checks, and creates that model on `device`.  The two-step form reads first
+ * (sw2d_case_read, no GPU needed), lets the caller inspect what was read (sw2d_case_array: the
+ * mesh tables and fields by their sw2d_mesh / sw2d_cell_fields names, "h0"/"q0"/"r0", "bc_*",
+ * "ddp_*_offset"/"_values"; sw2d_case_info: {cells, internal edges, boundary edges, model 0 sp /
+ * 1 dip / 2 ddp, DDP initial-condition columns}; sw2d_case_option: an input.solv value), then
+ * creates.  Errors of the reading return SW2D_E_ARG with the text in sw2d_case_last_error(). */
+typedef struct sw2d_case sw2d_case;
+int sw2d_load_case(const char* folder, int device, sw2d_handle** out);
+int sw2d_case_read(const char* folder, sw2d_case** out);
+int64_t sw2d_case_array(const sw2d_case* c, const char* name, double* out, int64_t capacity);
+int sw2d_case_info(const sw2d_case* c, int64_t* sizes /* [5] */);
+const char* sw2d_case_option(const sw2d_case* c, const char* key);
+int sw2d_case_create(const sw2d_case* c, int device, sw2d_handle** out);
+void sw2d_case_free(sw2d_case* c);
+const char* sw2d_case_last_error(void);
+
 /* Advances at most n_steps passes of the body of swSp::execute's time loop
  * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),
  * stopping once t >= t_max.  The loop runs on the device (CUDA graph); the host does not

@@ -269,6 +269,22 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_ddp_get_table.argtypes = [P, ctypes.c_int, ctypes.c_int64, c_double_p, c_double_p, c_double_p,
                                        ctypes.c_int64]
     lib.sw2d_ddp_get_table.restype = ctypes.c_int64
+    lib.sw2d_load_case.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(P)]
+    lib.sw2d_load_case.restype = ctypes.c_int
+    lib.sw2d_case_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(P)]
+    lib.sw2d_case_read.restype = ctypes.c_int
+    lib.sw2d_case_array.argtypes = [P, ctypes.c_char_p, c_double_p, ctypes.c_int64]
+    lib.sw2d_case_array.restype = ctypes.c_int64
+    lib.sw2d_case_info.argtypes = [P, c_int64_p]
+    lib.sw2d_case_info.restype = ctypes.c_int
+    lib.sw2d_case_option.argtypes = [P, ctypes.c_char_p]
+    lib.sw2d_case_option.restype = ctypes.c_char_p
+    lib.sw2d_case_create.argtypes = [P, ctypes.c_int, ctypes.POINTER(P)]
+    lib.sw2d_case_create.restype = ctypes.c_int
+    lib.sw2d_case_free.argtypes = [P]
+    lib.sw2d_case_free.restype = None
+    lib.sw2d_case_last_error.argtypes = []
+    lib.sw2d_case_last_error.restype = ctypes.c_char_p
     lib.sw2d_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
     lib.sw2d_step_n.restype = ctypes.c_int
     lib.sw2d_execute.argtypes = [P, c_int64_p]
@@ -374,7 +390,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 # every symbol include/sw2d_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_table", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_table", "sw2d_load_case",
+            "sw2d_case_read", "sw2d_case_array", "sw2d_case_info", "sw2d_case_option", "sw2d_case_create",
+            "sw2d_case_free", "sw2d_case_last_error", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",
@@ -386,3 +404,44 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_batch_destroy", "sw2d_batch_last_error", "sw2d_assim_configure", "sw2d_assim_set_observations",
             "sw2d_assim_record", "sw2d_assim_replay_cost", "sw2d_assim_gradient", "sw2d_assim_segments",
             "sw2d_assim_steps", "sw2d_assim_checkpoint", "sw2d_assim_set_start"]
+
+
+class CaseFolder:
+    """A case folder read by the library's own loader (sw2d_case_read): the tables and fields as
+    the C ABI will hand them to the model, for inspection; ``create(device)`` builds the model."""
+
+    def __init__(self, folder: str):
+        self.lib = load_library()
+        self.ptr = ctypes.c_void_p()
+        st = self.lib.sw2d_case_read(folder.encode(), ctypes.byref(self.ptr))
+        if st != 0:
+            raise ValueError(f"sw2d_case_read: {self.lib.sw2d_case_last_error().decode()}")
+        info = np.zeros(5, dtype=np.int64)
+        self.lib.sw2d_case_info(self.ptr, info.ctypes.data_as(c_int64_p))
+        self.cell_nb, self.edge_int_nb, self.edge_bnd_nb, self.model, self.ic_columns = (int(v) for v in info)
+
+    def array(self, name: str) -> np.ndarray:
+        cap = 8 * max(self.cell_nb, self.edge_int_nb, self.edge_bnd_nb, 1) + 1024
+        while True:
+            out = np.empty(cap)
+            k = self.lib.sw2d_case_array(self.ptr, name.encode(), _dp(out), cap)
+            if k >= 0:
+                return out[:k].copy()
+            if cap > 1 << 31:
+                raise KeyError(name)
+            cap *= 4
+
+    def option(self, key: str) -> Optional[str]:
+        v = self.lib.sw2d_case_option(self.ptr, key.encode())
+        return None if v is None else v.decode()
+
+    def close(self) -> None:
+        if self.ptr:
+            self.lib.sw2d_case_free(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

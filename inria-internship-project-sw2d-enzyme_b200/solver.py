@@ -75,6 +75,24 @@ class SpModel:
                                 "implemented")
         return cls(case, device)
 
+    @classmethod
+    def load(cls, folder: str, device: int = 0) -> "SpModel":
+        """The model a case folder names, read and created by the library itself
+        (sw2d_load_case: the C++ readers of input.solv, geometry.sw2d and the maps)."""
+        self = cls.__new__(cls)
+        self.lib = capi.load_library()
+        self.case = None
+        cf = capi.CaseFolder(folder)
+        self.n, self.ni, self.nb = cf.cell_nb, cf.edge_int_nb, cf.edge_bnd_nb
+        handle = ctypes.c_void_p()
+        st = self.lib.sw2d_case_create(cf.ptr, int(device), ctypes.byref(handle))
+        cf.close()
+        if st != 0:
+            msg = self.lib.sw2d_last_error(None).decode() or self.lib.sw2d_case_last_error().decode()
+            raise Sw2dError(st, msg)
+        self.handle = handle
+        return self
+
     def _check(self, st: int) -> None:
         if st != 0:
             raise Sw2dError(st, self.lib.sw2d_last_error(self.handle).decode())
