@@ -246,6 +246,28 @@ int sw2d_case_create(const sw2d_case* c, int device, sw2d_handle** out);
 void sw2d_case_free(sw2d_case* c);
 const char* sw2d_case_last_error(void);
 
+/* Learned momentum-exchange closure (the DIP/DDP dissipation site): an MLP of 10 features ->
+ * 64 -> 64 -> 2 outputs with GELU, BF16 operands and FP32 accumulation on the tensor cores
+ * (tcgen05).  params: sw2d_mlp_param_count() floats, W1 [64 x 10], b1 [64], W2 [64 x 64], b2 [64],
+ * W3 [2 x 64], b3 [2] (row-major, out x in).  norm: feature means [10], feature standard
+ * deviations [10], output means [2], output standard deviations [2]: the network sees
+ * (x - mean) / std and its outputs are scaled back by y * std + mean.  Host buffers throughout. */
+typedef struct sw2d_mlp sw2d_mlp;
+int sw2d_mlp_param_count(void);
+int sw2d_mlp_create(int device, const float* params, const float* norm, sw2d_mlp** out);
+int sw2d_mlp_destroy(sw2d_mlp* m);
+const char* sw2d_mlp_last_error(sw2d_mlp* m);
+int sw2d_mlp_get_params(sw2d_mlp* m, float* params);
+/* outputs [n x 2] of raw features [n x 10]; `layers` (may be NULL) receives Z1, H1, Z2, H2
+ * ([n x 64] each: pre-activations and activations of the two hidden layers) */
+int sw2d_mlp_infer(sw2d_mlp* m, const float* features, int64_t n, float* outputs, float* layers);
+/* mean squared error of the normalised outputs against targets [n x 2] and its gradient with
+ * respect to the parameters ([sw2d_mlp_param_count()] floats, may be NULL) */
+int sw2d_mlp_loss_grad(sw2d_mlp* m, const float* features, const float* targets, int64_t n, double* loss,
+                       float* grad);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the gradient of the last sw2d_mlp_loss_grad */
+int sw2d_mlp_adam_step(sw2d_mlp* m, float lr);
+
 /* Advances at most n_steps passes of the body of swSp::execute's time loop
  * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),
  * stopping once t >= t_max.  The loop runs on the device (CUDA graph); the host does not

@@ -285,6 +285,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_case_free.restype = None
     lib.sw2d_case_last_error.argtypes = []
     lib.sw2d_case_last_error.restype = ctypes.c_char_p
+    c_float_p = ctypes.POINTER(ctypes.c_float)
+    lib.sw2d_mlp_param_count.argtypes = []
+    lib.sw2d_mlp_param_count.restype = ctypes.c_int
+    lib.sw2d_mlp_create.argtypes = [ctypes.c_int, c_float_p, c_float_p, ctypes.POINTER(P)]
+    lib.sw2d_mlp_create.restype = ctypes.c_int
+    lib.sw2d_mlp_destroy.argtypes = [P]
+    lib.sw2d_mlp_destroy.restype = ctypes.c_int
+    lib.sw2d_mlp_last_error.argtypes = [P]
+    lib.sw2d_mlp_last_error.restype = ctypes.c_char_p
+    lib.sw2d_mlp_get_params.argtypes = [P, c_float_p]
+    lib.sw2d_mlp_get_params.restype = ctypes.c_int
+    lib.sw2d_mlp_infer.argtypes = [P, c_float_p, ctypes.c_int64, c_float_p, c_float_p]
+    lib.sw2d_mlp_infer.restype = ctypes.c_int
+    lib.sw2d_mlp_loss_grad.argtypes = [P, c_float_p, c_float_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                                       c_float_p]
+    lib.sw2d_mlp_loss_grad.restype = ctypes.c_int
+    lib.sw2d_mlp_adam_step.argtypes = [P, ctypes.c_float]
+    lib.sw2d_mlp_adam_step.restype = ctypes.c_int
     lib.sw2d_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
     lib.sw2d_step_n.restype = ctypes.c_int
     lib.sw2d_execute.argtypes = [P, c_int64_p]
@@ -392,7 +410,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 # every symbol include/sw2d_b200.h declares (checked by the CPU test suite)
 EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_table", "sw2d_load_case",
             "sw2d_case_read", "sw2d_case_array", "sw2d_case_info", "sw2d_case_option", "sw2d_case_create",
-            "sw2d_case_free", "sw2d_case_last_error", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+            "sw2d_case_free", "sw2d_case_last_error", "sw2d_mlp_param_count", "sw2d_mlp_create",
+            "sw2d_mlp_destroy", "sw2d_mlp_last_error", "sw2d_mlp_get_params", "sw2d_mlp_infer",
+            "sw2d_mlp_loss_grad", "sw2d_mlp_adam_step", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",

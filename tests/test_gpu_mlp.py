@@ -1,0 +1,73 @@
+"""The closure MLP on the tensor cores (csrc/sw2d_mlp.cu, tcgen05 BF16 GEMMs with FP32
+accumulation in TMEM) against the FP64 reference with the same BF16 roundings
+(closure.reference_forward / reference_loss_grad): the first layer's pre-activations, the
+outputs, the loss and the parameter gradient; training with Adam reduces the loss and is
+deterministic."""
+import numpy as np
+import pytest
+
+from tests.conftest import load_pkg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def C():
+    p = load_pkg()
+    p.build.build()
+    return p.closure
+
+
+def _setup(seed, n):
+    rng = np.random.default_rng(seed)
+    norm = np.concatenate([rng.normal(0, 1, 10), rng.uniform(0.5, 2, 10), rng.normal(0, 1, 2),
+                           rng.uniform(0.5, 2, 2)]).astype(np.float32)
+    x = (rng.normal(0, 1.5, (n, 10)) * norm[10:20] + norm[:10]).astype(np.float32)
+    return rng, norm, x
+
+
+def test_forward_matches_fp64(C):
+    rng, norm, x = _setup(1, 1000)          # not a multiple of 128: the padded tail
+    p = C.init_params(2)
+    p[640:704] = rng.normal(0, 0.2, 64)
+    net = C.MLP(p, norm)
+    y, lay = net.infer(x, layers=True)
+    ref = C.reference_forward(p, norm, x)
+    # first GEMM + bias: exact products of BF16 operands summed in FP32
+    z1 = lay[0].astype(np.float64)
+    assert np.max(np.abs(z1 - ref["z1"])) <= 1e-5 * (1.0 + np.max(np.abs(ref["z1"])))
+    z2 = lay[2].astype(np.float64)
+    assert np.max(np.abs(z2 - ref["z2"])) <= 2e-2 * (1.0 + np.max(np.abs(ref["z2"])))
+    assert np.max(np.abs(y - ref["y"])) <= 2e-2 * (1.0 + np.max(np.abs(ref["y"])))
+
+
+def test_gradient_matches_fp64(C):
+    rng, norm, x = _setup(4, 4096)
+    t = rng.normal(0, 1, (4096, 2)).astype(np.float32) * norm[22:24] + norm[20:22]
+    p = C.init_params(6)
+    net = C.MLP(p, norm)
+    loss, g = net.loss_grad(x, t)
+    rloss, rg = C.reference_loss_grad(p, norm, x, t)
+    assert abs(loss - rloss) <= 1e-3 * abs(rloss)
+    k = 0
+    for name, shape in C.SHAPES:
+        nk = int(np.prod(shape))
+        a, b = g[k:k + nk].astype(np.float64), rg[k:k + nk]
+        assert np.linalg.norm(a - b) <= 2e-2 * np.linalg.norm(b) + 1e-7, name
+        k += nk
+
+
+def test_training_reduces_loss_and_is_deterministic(C):
+    rng = np.random.default_rng(7)
+    x = rng.uniform(-2, 2, (16384, 10)).astype(np.float32)
+    t = np.stack([np.sin(x[:, 0]) + 0.5 * x[:, 1] * x[:, 2], np.tanh(x[:, 3]) - 0.3 * x[:, 4] ** 2], 1)
+    t = t.astype(np.float32)
+    norm = np.concatenate([x.mean(0), x.std(0), t.mean(0), t.std(0)]).astype(np.float32)
+    runs = []
+    for _ in range(2):
+        net = C.MLP(C.init_params(8), norm)
+        hist = net.train(x, t, epochs=12, batch=2048, lr=3e-3, seed=9)
+        runs.append((hist, net.params))
+    hist = runs[0][0]
+    assert hist[-1] < 0.05 * hist[0], hist
+    assert np.array_equal(runs[0][1].view(np.int32), runs[1][1].view(np.int32))
