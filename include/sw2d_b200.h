@@ -268,6 +268,21 @@ int sw2d_mlp_loss_grad(sw2d_mlp* m, const float* features, const float* targets,
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the gradient of the last sw2d_mlp_loss_grad */
 int sw2d_mlp_adam_step(sw2d_mlp* m, float lr);
 
+/* Attaches a closure network to a DIP model (net NULL detaches).  Every step then adds the
+ * network's momentum correction to the cells whose ten features lie within [hull_lo, hull_hi]
+ * (per feature) and applies the model's plain momentum-dissipation closure (its mu map,
+ * model_momentum_dissipation) to the step's increments elsewhere; the plain closure inside the
+ * cell update is off meanwhile.  Features, from the state at the start of the step (h0, q0, r0)
+ * and after the update (h, q, r): h0, q0, r0, h - h0, q - q0, r - r0, phiW, the smallest phiG of
+ * the cell's internal edges, dt, sqrt(q0^2 + r0^2) / max(h0, 1e-3).  Outputs: the corrections
+ * of q and r, added times `scale`.  The network must live on the model's device and outlive
+ * the attachment. */
+int sw2d_set_closure(sw2d_handle* h, sw2d_mlp* net, const float* hull_lo, const float* hull_hi, float scale);
+
+/* Replaces the end time t_max of the run (swSp member t_max): the time step is clipped to it,
+ * so a run can be brought exactly to any time. */
+int sw2d_set_t_max(sw2d_handle* h, double t_max);
+
 /* Advances at most n_steps passes of the body of swSp::execute's time loop
  * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),
  * stopping once t >= t_max.  The loop runs on the device (CUDA graph); the host does not

@@ -133,6 +133,7 @@ inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBl
 struct AdjointState;  // sw2d_adjoint.cu
 struct AssimState;    // sw2d_assim.cu
 struct DdpState;      // sw2d_ddp.cu
+struct ClosureState;  // sw2d_mlp.cu
 
 }  // namespace sw2d
 
@@ -167,6 +168,7 @@ struct sw2d_handle {
     int assim_sqrt_zero = 0;            // option "assim_sqrt_zero"
     int assim_chained = 0;              // option "assim_chained_recompute"
     sw2d::DdpState* ddp = nullptr;      // DDP model: tables, divergence-correction scratch
+    sw2d::ClosureState* closure = nullptr;  // learned momentum-exchange closure (sw2d_set_closure)
     std::string err;
 };
 
@@ -300,6 +302,12 @@ int ddp_setup(sw2d_handle* h, const sw2d_mesh* mesh, const sw2d_cell_fields* fie
 void ddp_release(sw2d_handle* h);
 // Validates the DDP arguments before anything is allocated.
 int ddp_check(const sw2d_mesh* mesh, const sw2d_ddp_fields* ddp, std::string& why);
+
+// The learned closure around a step (sw2d_mlp.cu): the state at the step's start, then the
+// network's correction after the update; and its release.
+void closure_begin(sw2d_handle* h);
+void closure_end(sw2d_handle* h);
+void closure_release(sw2d_handle* h);
 
 // Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
 void adjoint_release(sw2d_handle* h);

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/sw2d_b200.h"
+#include "sw2d_internal.cuh"
 #include "umma.cuh"
 
 namespace {
@@ -356,15 +357,17 @@ __global__ void k_adam(float* p, float* m1, float* m2, const float* __restrict__
 }
 
 int gemm(sw2d_mlp* m, int mode, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
-         const float* bias, float* out, int ldo, __nv_bfloat16* act, int ldact, const float* pre, int n_valid)
+         const float* bias, float* out, int ldo, __nv_bfloat16* act, int ldact, const float* pre, int n_valid,
+         cudaStream_t stream = nullptr)
 {
+    if (!stream) stream = m->stream;
     if (N % 16 || N > kMaxN || K % 16 || K <= 0 || M <= 0 || (lda % 8) || (ldb % 8))
         return mlp_fail(m, SW2D_E_ARG, "gemm: shape outside the kernel's contract");
     GemmArgs g{A, B, M, N, K, lda, ldb, bias, out, act, pre, ldo, ldact, n_valid, tmem_cols_for(N), m->status};
     const unsigned grid = (unsigned)((M + kTileM - 1) / kTileM);
-    if (mode == kEpiStore) k_umma_gemm<kEpiStore><<<grid, 128, 0, m->stream>>>(g);
-    else if (mode == kEpiGelu) k_umma_gemm<kEpiGelu><<<grid, 128, 0, m->stream>>>(g);
-    else k_umma_gemm<kEpiGeluGrad><<<grid, 128, 0, m->stream>>>(g);
+    if (mode == kEpiStore) k_umma_gemm<kEpiStore><<<grid, 128, 0, stream>>>(g);
+    else if (mode == kEpiGelu) k_umma_gemm<kEpiGelu><<<grid, 128, 0, stream>>>(g);
+    else k_umma_gemm<kEpiGeluGrad><<<grid, 128, 0, stream>>>(g);
     MCK(cudaGetLastError());
     return SW2D_OK;
 }
@@ -604,5 +607,220 @@ int sw2d_mlp_adam_step(sw2d_mlp* m, float lr)
 }
 
 int sw2d_mlp_param_count(void) { return sw2d::kNParams; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// The closure inside a model's step.  With a network attached (sw2d_set_closure), each step
+// keeps the state it starts from; after the cell update the features of every cell are formed
+// from that state and the updated one, the network runs on the handle's stream (three GEMM
+// launches), and the momentum correction it outputs is added where the cell's features lie in
+// the training hull.  Elsewhere the model's plain momentum-dissipation closure (the DIP mu
+// tensor, dip/swDipHyp.cpp:295-324) is applied to the step's increments when the model has
+// one; the plain closure inside the update is switched off while a network is attached.
+// ------------------------------------------------------------------------------------------
+namespace sw2d {
+
+struct ClosureState {
+    sw2d_mlp* net = nullptr;
+    int64_t npad = 0;
+    float lo[kIn], hi[kIn];
+    float scale = 1.0f;  // factor on the network's correction
+    double4* old = nullptr;
+    float* phig_min = nullptr;
+    __nv_bfloat16 *x = nullptr, *h1 = nullptr, *h2 = nullptr;
+    float *z1 = nullptr, *z2 = nullptr, *y = nullptr;
+    unsigned char* inside = nullptr;
+    std::vector<void*> allocs;
+};
+
+// the ten features of a cell from the state at the start of the step (a) and after the update
+// (b): depth, unit discharges, their increments, storage porosity, the smallest connectivity
+// porosity of the cell's internal edges, dt and the speed at the start
+SW2D_HD void closure_features(double4 a, double4 b, double phiw, double phig_min, double dt, double* f)
+{
+    f[0] = a.x;
+    f[1] = a.y;
+    f[2] = a.z;
+    f[3] = b.x - a.x;
+    f[4] = b.y - a.y;
+    f[5] = b.z - a.z;
+    f[6] = phiw;
+    f[7] = phig_min;
+    f[8] = dt;
+    f[9] = sqrt(a.y * a.y + a.z * a.z) / fmax(a.x, 1e-3);
+}
+
+}  // namespace sw2d
+
+namespace {
+
+using namespace sw2d;
+
+struct ClosureNorm {
+    float xmean[kIn], xstd[kIn], lo[kIn], hi[kIn], ymean[kOut], ystd[kOut], scale;
+};
+
+__global__ void k_closure_phig_min(DevMesh m, float* out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int k0 = m.coff[c].x, k1 = m.coff[c + 1].x;
+    double g = 1.0;
+    for (int k = k0; k < k1; k++) g = fmin(g, m.phig[m.cint[k].x >> 1]);
+    out[c] = (float)g;
+}
+
+__global__ void k_closure_features(DevMesh m, const double4* __restrict__ old, const float* __restrict__ phig_min,
+                                   ClosureNorm cn, int64_t npad, __nv_bfloat16* x, unsigned char* inside)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npad) return;
+    if (i >= m.nc) {
+        for (int k = 0; k < kInPad; k++) x[i * kInPad + k] = __float2bfloat16_rn(0.0f);
+        return;
+    }
+    double f[kIn];
+    closure_features(old[i], m.st[i], m.cst[i].z, phig_min[i], m.ctrl->dt, f);
+    bool in = true;
+    for (int k = 0; k < kInPad; k++) {
+        float v = 0.0f;
+        if (k < kIn) {
+            const float fk = (float)f[k];
+            in = in && (fk >= cn.lo[k]) && (fk <= cn.hi[k]);
+            v = (fk - cn.xmean[k]) / cn.xstd[k];
+        }
+        x[i * kInPad + k] = __float2bfloat16_rn(v);
+    }
+    inside[i] = in ? 1 : 0;
+}
+
+__global__ void k_closure_apply(DevMesh m, const double4* __restrict__ old, const float* __restrict__ y,
+                                const unsigned char* __restrict__ inside, ClosureNorm cn, int dissip)
+{
+    if (!m.ctrl->go) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nc) return;
+    double4 s = m.st[i];
+    if (inside[i]) {
+        s.y += (double)(cn.scale * (y[(size_t)i * kOutPad + 0] * cn.ystd[0] + cn.ymean[0]));
+        s.z += (double)(cn.scale * (y[(size_t)i * kOutPad + 1] * cn.ystd[1] + cn.ymean[1]));
+    } else if (dissip) {
+        const double4 mu = m.mu[i];
+        const double4 a = old[i];
+        double q = s.y, r = s.z;
+        momentum_dissipation(mu.x, mu.y, mu.z, mu.w, a.x, a.y, a.z, s.x, q, r);
+        s.y = q;
+        s.z = r;
+    } else {
+        return;
+    }
+    m.st[i] = s;
+}
+
+ClosureNorm closure_norm(const ClosureState* c)
+{
+    ClosureNorm cn;
+    const sw2d_mlp* n = c->net;
+    std::memcpy(cn.xmean, n->xmean, sizeof(cn.xmean));
+    std::memcpy(cn.xstd, n->xstd, sizeof(cn.xstd));
+    std::memcpy(cn.lo, c->lo, sizeof(cn.lo));
+    std::memcpy(cn.hi, c->hi, sizeof(cn.hi));
+    std::memcpy(cn.ymean, n->ymean, sizeof(cn.ymean));
+    std::memcpy(cn.ystd, n->ystd, sizeof(cn.ystd));
+    cn.scale = c->scale;
+    return cn;
+}
+
+void closure_free(ClosureState* c)
+{
+    if (!c) return;
+    for (void* p : c->allocs) cudaFree(p);
+    delete c;
+}
+
+}  // namespace
+
+namespace sw2d {
+
+void closure_begin(sw2d_handle* h)
+{
+    cudaMemcpyAsync(h->closure->old, h->m.st, (size_t)h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream);
+}
+
+void closure_end(sw2d_handle* h)
+{
+    ClosureState* c = h->closure;
+    sw2d_mlp* net = c->net;
+    const ClosureNorm cn = closure_norm(c);
+    const int64_t npad = c->npad;
+    k_closure_features<<<(unsigned)((npad + 255) / 256), 256, 0, h->stream>>>(h->m, c->old, c->phig_min, cn, npad, c->x,
+                                                                             c->inside);
+    gemm(net, kEpiGelu, c->x, kInPad, net->w1, kInPad, (int)npad, kHid, kInPad, net->b1, c->z1, kHid, c->h1, kHid,
+         nullptr, kHid, h->stream);
+    gemm(net, kEpiGelu, c->h1, kHid, net->w2, kHid, (int)npad, kHid, kHid, net->b2, c->z2, kHid, c->h2, kHid, nullptr,
+         kHid, h->stream);
+    gemm(net, kEpiStore, c->h2, kHid, net->w3, kHid, (int)npad, kOutPad, kHid, net->b3, c->y, kOutPad, nullptr, 0,
+         nullptr, kOutPad, h->stream);
+    k_closure_apply<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, c->old, c->y, c->inside, cn,
+                                                              h->dissipation && h->m.mu ? 1 : 0);
+}
+
+void closure_release(sw2d_handle* h)
+{
+    closure_free(h->closure);
+    h->closure = nullptr;
+}
+
+}  // namespace sw2d
+
+using sw2d::fail;
+using sw2d::grid_for;
+using sw2d::kBlock;
+using sw2d::kModelDip;
+
+extern "C" {
+
+int sw2d_set_closure(sw2d_handle* h, sw2d_mlp* net, const float* hull_lo, const float* hull_hi, float scale)
+{
+    using namespace sw2d;
+    if (!h) return SW2D_E_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    closure_release(h);
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    if (!net) return SW2D_OK;
+    if (h->model != sw2d::kModelDip) return fail(h, SW2D_E_UNSUPPORTED, "the learned closure runs on the DIP model");
+    if (net->device != h->device) return fail(h, SW2D_E_ARG, "network and model on different devices");
+    if (!hull_lo || !hull_hi) return fail(h, SW2D_E_ARG, "training hull missing");
+    ClosureState* c = new ClosureState();
+    c->net = net;
+    c->npad = (h->nc + kTileM - 1) / kTileM * kTileM;
+    std::memcpy(c->lo, hull_lo, sizeof(c->lo));
+    std::memcpy(c->hi, hull_hi, sizeof(c->hi));
+    c->scale = scale;
+    auto al = [&](size_t bytes, void** p) {
+        if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) return false;
+        c->allocs.push_back(*p);
+        return cudaMemset(*p, 0, std::max<size_t>(bytes, 16)) == cudaSuccess;
+    };
+    const size_t np = (size_t)c->npad;
+    bool ok = al((size_t)h->nc * sizeof(double4), (void**)&c->old) && al(np * sizeof(float), (void**)&c->phig_min) &&
+              al(np * kInPad * 2, (void**)&c->x) && al(np * kHid * 2, (void**)&c->h1) &&
+              al(np * kHid * 2, (void**)&c->h2) && al(np * kHid * 4, (void**)&c->z1) &&
+              al(np * kHid * 4, (void**)&c->z2) && al(np * kOutPad * 4, (void**)&c->y) && al(np, (void**)&c->inside);
+    if (!ok) {
+        closure_free(c);
+        return fail(h, SW2D_E_CUDA, "closure buffers");
+    }
+    h->closure = c;
+    k_closure_phig_min<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, c->phig_min);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
 
 }  // extern "C"

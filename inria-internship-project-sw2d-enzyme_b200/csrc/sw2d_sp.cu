@@ -619,7 +619,9 @@ void launch_update_d(sw2d_handle* h, const DevMesh& m)
 template <bool kStoreB>
 void launch_update_s(sw2d_handle* h, const DevMesh& m)
 {
-    if (!kStoreB && h->dissipation) launch_update_d<false, true>(h, m);
+    // a learned closure replaces the plain dissipation inside the update (it applies the plain
+    // closure itself where its inputs leave the training hull)
+    if (!kStoreB && h->dissipation && !h->closure) launch_update_d<false, true>(h, m);
     else launch_update_d<kStoreB, false>(h, m);
 }
 
@@ -643,7 +645,9 @@ void launch_phase(sw2d_handle* h, int i)
 
 void launch_step(sw2d_handle* h)
 {
+    if (h->closure) closure_begin(h);
     for (int i = 0; i < 4; i++) launch_phase(h, i);
+    if (h->closure) closure_end(h);
 }
 
 }  // namespace
@@ -1372,6 +1376,18 @@ int sw2d_set_state(sw2d_handle* h, const double* wd, const double* qx, const dou
     return SW2D_OK;
 }
 
+int sw2d_set_t_max(sw2d_handle* h, double t_max)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->ctrl_host->t_max = t_max;
+    CK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
 int sw2d_get_time(sw2d_handle* h, double* t, double* dt)
 {
     if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
@@ -1593,6 +1609,7 @@ int sw2d_destroy(sw2d_handle* h)
     adjoint_release(h);
     assim_release(h);
     ddp_release(h);
+    closure_release(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -29,6 +29,15 @@ def jittered_triangle_mesh(nx: int, ny: int, lx: float, ly: float, x0: float = 0
     ``z_fn(x, y)`` gives the node elevations (default 0); ``bc_code_fn(mx, my)`` the negative
     boundary code of each boundary edge from its midpoint (default -1 everywhere).
     """
+    x, y, z, tri = jittered_triangles(nx, ny, lx, ly, x0, y0, jitter, seed, z_fn)
+    return mesh_from_triangles(x, y, z, tri, bc_code_fn)
+
+
+def jittered_triangles(nx: int, ny: int, lx: float, ly: float, x0: float = 0.0, y0: float = 0.0,
+                       jitter: float = 0.2, seed: int = 1,
+                       z_fn: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None):
+    """Nodes (x, y, z) and triangles of jittered_triangle_mesh: the triangles of quad q of the
+    grid (row-major, q = j nx + i) are rows 2q and 2q + 1."""
     rng = np.random.default_rng(seed)
     dx, dy = lx / nx, ly / ny
     ii, jj = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1))
@@ -64,7 +73,7 @@ def jittered_triangle_mesh(nx: int, ny: int, lx: float, ly: float, x0: float = 0
     tri = np.empty((2 * qi.size, 3), dtype=np.int64)
     tri[0::2] = t0
     tri[1::2] = t1
-    return mesh_from_triangles(x, y, z, tri, bc_code_fn)
+    return x, y, z, tri
 
 
 def mesh_from_triangles(x: np.ndarray, y: np.ndarray, z: np.ndarray, tri: np.ndarray,

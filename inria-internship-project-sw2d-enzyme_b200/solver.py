@@ -150,6 +150,24 @@ class SpModel:
     def set_time(self, t: float, dt: float) -> None:
         self._check(self.lib.sw2d_set_time(self.handle, float(t), float(dt)))
 
+    def set_t_max(self, t_max: float) -> None:
+        """Moves the run's end time (the time step is clipped to it)."""
+        self._check(self.lib.sw2d_set_t_max(self.handle, float(t_max)))
+
+    def set_closure(self, net, hull_lo=None, hull_hi=None, scale: float = 1.0) -> None:
+        """Attaches a closure.MLP (None detaches) with its training hull [lo, hi] per feature; the
+        network's correction is applied times `scale`."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        if net is None:
+            self._check(self.lib.sw2d_set_closure(self.handle, None, None, None, 1.0))
+            self._closure = None
+            return
+        lo = np.ascontiguousarray(hull_lo, dtype=np.float32)
+        hi = np.ascontiguousarray(hull_hi, dtype=np.float32)
+        self._check(self.lib.sw2d_set_closure(self.handle, net.h, lo.ctypes.data_as(fp), hi.ctypes.data_as(fp),
+                                              float(scale)))
+        self._closure = net  # keep the network alive while attached
+
     def array(self, name: str) -> np.ndarray:
         out = np.empty(max(self.n, self.ni, self.nb, 1))
         k = self.lib.sw2d_get_array(self.handle, name.encode(), out.ctypes.data_as(capi.c_double_p), out.size)
