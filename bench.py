@@ -66,6 +66,10 @@ def _args():
     ap.add_argument("--ddp-cpu-cells", type=int, default=50_000, help="cells of the DDP reference sample")
     ap.add_argument("--ddp-cpu-steps", type=int, default=30)
     ap.add_argument("--ddp-only", action="store_true", help="run only the DDP forward line")
+    ap.add_argument("--closure-cells", type=int, default=4_000_000,
+                    help="cells of the DIP run that times the learned closure")
+    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure line")
+    ap.add_argument("--closure-only", action="store_true", help="run only the learned-closure line")
     ap.add_argument("--assim-cells", type=int, default=1_000_000,
                     help="cells of the porosity-assimilation line (the reference's differentiated step; 0: skip)")
     ap.add_argument("--assim-steps", type=int, default=2000, help="approximate steps of its trajectory")
@@ -544,6 +548,86 @@ def run_ddp(pkg, args, local_rank):
     return line
 
 
+def run_closure(pkg, args, local_rank):
+    """The learned momentum-exchange closure.  (1) Cost inside the step: the DIP channel
+    (Godunov, Manning, momentum dissipation as the fallback) timed with and without a network
+    attached (random weights, a hull that admits every cell), CUDA events on the library's
+    stream, with the fused inference kernel (default) and with the five-launch path; the three
+    layers' FLOPs and the compulsory bytes per step over the closure's time.  (2) The pipeline
+    on a building layout (400 m x 200 m, buildings 5-30 m at 30 % cover, fine 1 m triangles,
+    coarse 8 m DIP cells): sample generation from the solver's own runs, training on the tensor
+    cores, and the coarse run's error against the fine run averaged onto it."""
+    import numpy as np
+    import torch
+
+    C = pkg.closure
+    case = pkg.workloads.dip_channel(n_cells=args.closure_cells, scheme="godunov", t_max=1.0e9)
+    model = pkg.SpModel(case, device=local_rank)
+    stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
+
+    def timed(steps):
+        model.step(3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        done = model.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / done
+
+    base_ms = timed(100)
+    norm = np.concatenate([np.zeros(10), np.ones(10), np.zeros(2), np.full(2, 1e-6)]).astype(np.float32)
+    net = C.MLP(C.init_params(1), norm, device=local_rank)
+    model.set_closure(net, np.full(10, -1e30, np.float32), np.full(10, 1e30, np.float32))
+    clos_ms = timed(100)
+    model.set_option("closure_fused", 0)
+    unfused_ms = timed(100)
+    n = case.mesh.cell_nb
+    npad = (n + 127) // 128 * 128
+    flops = 2.0 * npad * (16 * 64 + 64 * 64 + 64 * 16)
+    model.close()
+    net.close()
+    peak = None
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        peak = float(json.load(open(p)).get("bf16_tflops", 0.0)) or None
+    t0 = time.perf_counter()
+    fine, coarse, av = C.urban_cases(lx=400.0, ly=200.0, dx_fine=1.0, coarse_factor=8, seed=1)
+    X, Y, T = C.generate_samples(fine, coarse, av, t_start=5.0, n_samples=150, spacing=0.3, device=local_rank)
+    t1 = time.perf_counter()
+    net, lo, hi, hist = C.train_closure(X, Y, epochs=40, batch=4096, lr=2e-3, device=local_rank)
+    t2 = time.perf_counter()
+    ev = C.evaluate(fine, coarse, av, 10.0, 30.0, net=net, hull=(lo, hi), mu=0.3, device=local_rank,
+                    scales=(0.5, 1.0))
+    t3 = time.perf_counter()
+    closure_ms = clos_ms - base_ms
+    # compulsory bytes of the closure per cell: the state copy at the step's start (32 B read,
+    # 32 B written), then the fused kernel's reads of both states, phiW and the edge minimum of
+    # phiG (32 + 32 + 8 + 4 B) and the state written back (32 B)
+    closure_bytes = n * (64 + 76 + 32)
+    return {"workload": f"DIP channel at {n} cells (Godunov, Manning) with the closure network attached",
+            "ms_per_step_without": base_ms, "ms_per_step_with": clos_ms, "closure_ms_per_step": closure_ms,
+            "closure_ms_per_step_five_launches": unfused_ms - base_ms,
+            "closure_compulsory_bytes_per_step": closure_bytes,
+            "closure_gbs_over_closure_time": closure_bytes / (closure_ms * 1e-3) / 1e9 if closure_ms > 0 else None,
+            "gemm_flops_per_step": flops,
+            "tensor_tflops_over_closure_time": flops / (closure_ms * 1e-3) / 1e12 if closure_ms > 0 else None,
+            "bf16_peak_tflops": peak,
+            "pipeline": {"layout": "400 m x 200 m, buildings 5-30 m at 30 % cover", "fine_cells": fine.mesh.cell_nb,
+                         "coarse_cells": coarse.mesh.cell_nb, "samples": int(X.shape[0]),
+                         "s_generate": t1 - t0, "s_train": t2 - t1, "s_evaluate": t3 - t2,
+                         "train_loss_first_last": [hist[0], hist[-1]],
+                         "coarse_error_vs_fine_h_q": ev}}
+
+
+def run_closure_only(args, local_rank):
+    pkg = importlib.import_module(PKG)
+    pkg.build.build()
+    import torch
+    torch.cuda.set_device(local_rank)
+    print(json.dumps(run_closure(pkg, args, local_rank)))
+
+
 def run_ddp_only(args, local_rank):
     pkg = importlib.import_module(PKG)
     pkg.build.build()
@@ -750,6 +834,7 @@ def run_ours(args, rank, world, local_rank):
     ddp = None if (args.ddp_cells <= 0 or world > 1) else run_ddp(pkg, args, local_rank)
     assim = None if (args.assim_cells <= 0 or world > 1) else run_assim(pkg, args, local_rank)
     ensemble = None if (args.ensemble_members <= 0 or world > 1) else run_ensemble(pkg, args, local_rank)
+    closure = None if (args.no_closure or world > 1) else run_closure(pkg, args, local_rank)
 
     steps = args.steps
     value = n * steps * world / (ms / 1e3)
@@ -794,6 +879,8 @@ def run_ours(args, rank, world, local_rank):
         line["assim"] = assim
     if ensemble is not None:
         line["ensemble"] = ensemble
+    if closure is not None:
+        line["closure"] = closure
     print(json.dumps(line))
 
 
@@ -813,6 +900,9 @@ def main():
     elif args.ddp_only:
         if rank == 0:
             run_ddp_only(args, local_rank)
+    elif args.closure_only:
+        if rank == 0:
+            run_closure_only(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

@@ -308,6 +308,8 @@ int ddp_check(const sw2d_mesh* mesh, const sw2d_ddp_fields* ddp, std::string& wh
 void closure_begin(sw2d_handle* h);
 void closure_end(sw2d_handle* h);
 void closure_release(sw2d_handle* h);
+void closure_set_fused(sw2d_handle* h, int fused);
+int closure_kernels(const sw2d_handle* h);  // kernel launches the closure adds to a step
 
 // Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
 void adjoint_release(sw2d_handle* h);

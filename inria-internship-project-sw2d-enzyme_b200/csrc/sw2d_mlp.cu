@@ -613,9 +613,9 @@ int sw2d_mlp_param_count(void) { return sw2d::kNParams; }
 // ------------------------------------------------------------------------------------------
 // The closure inside a model's step.  With a network attached (sw2d_set_closure), each step
 // keeps the state it starts from; after the cell update the features of every cell are formed
-// from that state and the updated one, the network runs on the handle's stream (three GEMM
-// launches), and the momentum correction it outputs is added where the cell's features lie in
-// the training hull.  Elsewhere the model's plain momentum-dissipation closure (the DIP mu
+// from that state and the updated one, the network runs on the handle's stream (one fused
+// kernel, or features, three GEMM launches and an apply kernel), and the momentum correction it
+// outputs is added where the cell's features lie in the training hull.  Elsewhere the model's plain momentum-dissipation closure (the DIP mu
 // tensor, dip/swDipHyp.cpp:295-324) is applied to the step's increments when the model has
 // one; the plain closure inside the update is switched off while a network is attached.
 // ------------------------------------------------------------------------------------------
@@ -626,6 +626,7 @@ struct ClosureState {
     int64_t npad = 0;
     float lo[kIn], hi[kIn];
     float scale = 1.0f;  // factor on the network's correction
+    int fused = 1;       // one fused kernel per step (0: features, three GEMM launches, apply)
     double4* old = nullptr;
     float* phig_min = nullptr;
     __nv_bfloat16 *x = nullptr, *h1 = nullptr, *h2 = nullptr;
@@ -718,6 +719,174 @@ __global__ void k_closure_apply(DevMesh m, const double4* __restrict__ old, cons
     m.st[i] = s;
 }
 
+// The whole closure of a step in one kernel: per tile of 128 cells the features go to shared
+// memory as the first layer's A operand, and each layer is an MMA into TMEM whose epilogue
+// (bias, GELU, BF16) writes the next layer's A operand back to shared memory; the last
+// epilogue applies the correction (or the plain closure out of the hull) to the state.  The
+// weights are staged once per CTA; CTAs loop over tiles.  The three accumulators share TMEM
+// columns [0, 64): each layer's MMA is issued after every lane has read the previous one out.
+// The MMAs, their order and the epilogue arithmetic are those of the five-launch path.
+__global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4* __restrict__ old,
+                                                       const float* __restrict__ phig_min, ClosureNorm cn,
+                                                       const __nv_bfloat16* __restrict__ w1,
+                                                       const __nv_bfloat16* __restrict__ w2,
+                                                       const __nv_bfloat16* __restrict__ w3, const float* __restrict__ b1,
+                                                       const float* __restrict__ b2, const float* __restrict__ b3,
+                                                       int dissip, unsigned* status)
+{
+    __shared__ __align__(1024) uint16_t sX[kTileM * kInPad];
+    __shared__ __align__(1024) uint16_t sH[kTileM * kHid];
+    __shared__ __align__(1024) uint16_t sW1[kHid * kInPad];
+    __shared__ __align__(1024) uint16_t sW2[kHid * kHid];
+    __shared__ __align__(1024) uint16_t sW3[kOutPad * kHid];
+    __shared__ float sb1[kHid], sb2[kHid], sb3[kOutPad];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_holder;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t ncols = 64;
+    if (warp == 0) {
+        tmem_alloc(&tmem_holder, ncols);
+        tmem_relinquish();
+    }
+    if (tid == 0) mbar_init(&bar, 1);
+    // weights in the K-major core-matrix layout, biases
+    for (int i = tid; i < kHid * (kInPad / 8); i += 128) {
+        const int n = i / (kInPad / 8), c = i % (kInPad / 8);
+        *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sW1) + core_offset(n, c * 8, kInPad)) =
+            *reinterpret_cast<const uint4*>(w1 + n * kInPad + c * 8);
+    }
+    for (int i = tid; i < kHid * (kHid / 8); i += 128) {
+        const int n = i / (kHid / 8), c = i % (kHid / 8);
+        *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sW2) + core_offset(n, c * 8, kHid)) =
+            *reinterpret_cast<const uint4*>(w2 + n * kHid + c * 8);
+    }
+    for (int i = tid; i < kOutPad * (kHid / 8); i += 128) {
+        const int n = i / (kHid / 8), c = i % (kHid / 8);
+        *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sW3) + core_offset(n, c * 8, kHid)) =
+            *reinterpret_cast<const uint4*>(w3 + n * kHid + c * 8);
+    }
+    if (tid < kHid) {
+        sb1[tid] = b1[tid];
+        sb2[tid] = b2[tid];
+    }
+    if (tid < kOutPad) sb3[tid] = b3[tid];
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmem_holder;
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+    const uint32_t id64 = idesc_bf16_f32(kTileM, kHid), id16 = idesc_bf16_f32(kTileM, kOutPad);
+    const uint32_t aX = smem_u32(sX), aH = smem_u32(sH), aW1 = smem_u32(sW1), aW2 = smem_u32(sW2),
+                   aW3 = smem_u32(sW3);
+    const bool go = m.ctrl->go != 0;
+    const double dt = m.ctrl->dt;
+    uint32_t phase = 0;
+    bool ok = true;
+    const int ntiles = (m.nc + kTileM - 1) / kTileM;
+    for (int tile = blockIdx.x; tile < ntiles && go; tile += gridDim.x) {
+        const int row = tid;  // the tile row of this thread: its TMEM lane
+        const int c = tile * kTileM + row;
+        const bool valid = c < m.nc;
+        double4 a = make_double4(0, 0, 0, 0), b = make_double4(0, 0, 0, 0);
+        bool in = false;
+        {
+            float xv[kInPad];
+            for (int k = 0; k < kInPad; k++) xv[k] = 0.0f;
+            if (valid) {
+                a = old[c];
+                b = m.st[c];
+                double f[kIn];
+                closure_features(a, b, m.cst[c].z, phig_min[c], dt, f);
+                in = true;
+                for (int k = 0; k < kIn; k++) {
+                    const float fk = (float)f[k];
+                    in = in && (fk >= cn.lo[k]) && (fk <= cn.hi[k]);
+                    xv[k] = (fk - cn.xmean[k]) / cn.xstd[k];
+                }
+            }
+            for (int cc = 0; cc < kInPad / 8; cc++) {
+                __align__(16) __nv_bfloat16 v[8];
+                for (int j = 0; j < 8; j++) v[j] = __float2bfloat16_rn(xv[cc * 8 + j]);
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sX) + core_offset(row, cc * 8, kInPad)) =
+                    *reinterpret_cast<const uint4*>(v);
+            }
+        }
+        // layer 1: one MMA of K = 16
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after_sync();
+            mma_bf16(tmem, smem_desc(aX, kInPad), smem_desc(aW1, kInPad), id64, 0u);
+            mma_commit(&bar);
+        }
+        if (!mbar_wait(&bar, phase, kWaitPolls)) {
+            ok = false;
+            mbar_wait(&bar, phase, kWaitPolls);
+        }
+        phase ^= 1u;
+        fence_after_sync();
+        // hidden layers' epilogues, each followed by the next layer's four MMAs of K = 16
+        for (int layer = 0; layer < 2; layer++) {
+            const float* bias = layer == 0 ? sb1 : sb2;
+            for (int c0 = 0; c0 < kHid; c0 += 16) {
+                uint32_t v[16];
+                tmem_ld16(lane_base + (uint32_t)c0, v);
+                tmem_wait_ld();
+                __align__(16) __nv_bfloat16 hv[16];
+                for (int j = 0; j < 16; j++) hv[j] = __float2bfloat16_rn(gelu(__uint_as_float(v[j]) + bias[c0 + j]));
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(row, c0, kHid)) =
+                    *reinterpret_cast<const uint4*>(hv);
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(row, c0 + 8, kHid)) =
+                    *reinterpret_cast<const uint4*>(hv + 8);
+            }
+            fence_before_sync();
+            fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                fence_after_sync();
+                const uint32_t bw = layer == 0 ? aW2 : aW3;
+                const uint32_t id = layer == 0 ? id64 : id16;
+                for (int s2 = 0; s2 < kHid / 16; s2++)
+                    mma_bf16(tmem, smem_desc(aH + 256u * s2, kHid), smem_desc(bw + 256u * s2, kHid), id,
+                             s2 > 0 ? 1u : 0u);
+                mma_commit(&bar);
+            }
+            if (!mbar_wait(&bar, phase, kWaitPolls)) {
+                ok = false;
+                mbar_wait(&bar, phase, kWaitPolls);
+            }
+            phase ^= 1u;
+            fence_after_sync();
+        }
+        // output layer: the correction, or the plain closure outside the hull
+        uint32_t v[16];
+        tmem_ld16(lane_base, v);
+        tmem_wait_ld();
+        if (valid && ok) {
+            double4 s = b;
+            if (in) {
+                s.y += (double)(cn.scale * ((__uint_as_float(v[0]) + sb3[0]) * cn.ystd[0] + cn.ymean[0]));
+                s.z += (double)(cn.scale * ((__uint_as_float(v[1]) + sb3[1]) * cn.ystd[1] + cn.ymean[1]));
+                m.st[c] = s;
+            } else if (dissip) {
+                const double4 mu = m.mu[c];
+                double q = s.y, r = s.z;
+                momentum_dissipation(mu.x, mu.y, mu.z, mu.w, a.x, a.y, a.z, s.x, q, r);
+                s.y = q;
+                s.z = r;
+                m.st[c] = s;
+            }
+        }
+        fence_before_sync();
+        ok = __syncthreads_and(ok);  // every lane read out before the next tile's MMAs overwrite TMEM
+        if (!ok) break;
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+    if (!ok && tid == 0) atomicOr(status, kStatusTimeout);
+}
+
 ClosureNorm closure_norm(const ClosureState* c)
 {
     ClosureNorm cn;
@@ -754,6 +923,16 @@ void closure_end(sw2d_handle* h)
     sw2d_mlp* net = c->net;
     const ClosureNorm cn = closure_norm(c);
     const int64_t npad = c->npad;
+    if (c->fused) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        const int ntiles = (int)(npad / kTileM);
+        const unsigned grid = (unsigned)std::max(1, std::min(ntiles, 6 * sms));
+        k_closure_fused<<<grid, 128, 0, h->stream>>>(h->m, c->old, c->phig_min, cn, net->w1, net->w2, net->w3,
+                                                     net->b1, net->b2, net->b3, h->dissipation && h->m.mu ? 1 : 0,
+                                                     net->status);
+        return;
+    }
     k_closure_features<<<(unsigned)((npad + 255) / 256), 256, 0, h->stream>>>(h->m, c->old, c->phig_min, cn, npad, c->x,
                                                                              c->inside);
     gemm(net, kEpiGelu, c->x, kInPad, net->w1, kInPad, (int)npad, kHid, kInPad, net->b1, c->z1, kHid, c->h1, kHid,
@@ -765,6 +944,9 @@ void closure_end(sw2d_handle* h)
     k_closure_apply<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, c->old, c->y, c->inside, cn,
                                                               h->dissipation && h->m.mu ? 1 : 0);
 }
+
+void closure_set_fused(sw2d_handle* h, int fused) { h->closure->fused = fused; }
+int closure_kernels(const sw2d_handle* h) { return h->closure->fused ? 1 : 5; }
 
 void closure_release(sw2d_handle* h)
 {

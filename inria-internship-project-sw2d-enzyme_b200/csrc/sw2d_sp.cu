@@ -1315,6 +1315,11 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         // reference does; 1 from the replay's own states (the exact gradient of the replay cost)
         h->assim_chained = value ? 1 : 0;
         return SW2D_OK;
+    } else if (std::strcmp(name, "closure_fused") == 0) {
+        // the learned closure as one fused kernel (1, default) or as features, three GEMM
+        // launches and the apply kernel (0); both give the same numbers
+        if (!h->closure) return fail(h, SW2D_E_ARG, "no closure attached");
+        closure_set_fused(h, value ? 1 : 0);
     } else if (std::strcmp(name, "adjoint_edge_variant") == 0) {
         if (value < 0 || value > 4) return fail(h, SW2D_E_ARG, "adjoint_edge_variant outside 0..4");
         h->adj_edge_variant = (int)value;
@@ -1571,7 +1576,7 @@ int sw2d_kernels_per_step(sw2d_handle* h)
 {
     if (!h) return 0;
     if (h->model == kModelDdp) return ddp_kernels_per_step(h);
-    return h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3;
+    return (h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3) + (h->closure ? closure_kernels(h) : 0);
 }
 
 int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n)

@@ -101,3 +101,48 @@ def test_pipeline_runs_and_trains(pkg, urban):
     res = C.evaluate(fine, coarse, av, 5.0, 12.0, net=net, hull=(lo, hi), mu=0.3)
     for key in ("none", "plain_mu", "learned"):
         assert np.all(np.isfinite(res[key]))
+
+
+def test_fused_kernel_matches_the_gemm_path_and_the_reference(pkg, urban):
+    """The in-step inference as one fused kernel (features, three tensor-core layers through
+    shared memory and TMEM, apply) gives the same state bit for bit as the five-launch path
+    (features, three GEMM launches, apply), and its correction matches the FP64 forward with the
+    kernels' BF16 roundings."""
+    C = pkg.closure
+    _, coarse, _ = urban
+    m0 = pkg.SpModel(coarse)
+    m0.step(30)
+    s0 = m0.state()
+    t0 = m0.t
+    plain = pkg.SpModel(coarse)
+    plain.set_state(*s0)
+    plain.set_time(t0, 0.0)
+    plain.step(1)
+    s1, dt = plain.state(), plain.dt
+    f = C.features(s0, s1, coarse.phi, C.phig_min_of(coarse), dt)
+    norm = np.concatenate([f.mean(0), np.maximum(f.std(0), 1e-6), np.zeros(2), np.full(2, 1e-3)]).astype(np.float32)
+    p = C.init_params(seed=5)
+    net = C.MLP(p, norm)
+    runs = []
+    for fused in (1, 0):
+        m = pkg.SpModel(coarse)
+        m.set_state(*s0)
+        m.set_time(t0, 0.0)
+        m.set_closure(net, *_wide_hull())
+        m.set_option("closure_fused", fused)
+        assert m.kernels_per_step == plain.kernels_per_step + (1 if fused else 5)
+        m.step(1)
+        one = m.state()
+        m.step(20)
+        runs.append((one, m.state(), m.t))
+    for a, b in zip(runs[0][0] + runs[0][1], runs[1][0] + runs[1][1]):
+        assert np.array_equal(a, b)
+    assert runs[0][2] == runs[1][2]
+    # the first step's correction against the FP64 forward (an FP32-accumulation difference can
+    # move a BF16 rounding of a hidden activation: a tolerance of 1 % of the largest correction)
+    y = C.reference_forward(p, norm, f)["y"]
+    h, q, r = runs[0][0]
+    assert np.array_equal(h, s1[0])
+    for got, want in ((q - s1[1], y[:, 0]), (r - s1[2], y[:, 1])):
+        assert np.abs(want).max() > 0
+        assert np.max(np.abs(got - want)) <= 1e-2 * np.abs(want).max()
