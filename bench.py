@@ -550,13 +550,14 @@ def run_ddp(pkg, args, local_rank):
 
 def run_closure(pkg, args, local_rank):
     """The learned momentum-exchange closure.  (1) Cost inside the step: the DIP channel
-    (Godunov, Manning, momentum dissipation as the fallback) timed with and without a network
-    attached (random weights, a hull that admits every cell), CUDA events on the library's
-    stream, with the fused inference kernel (default) and with the five-launch path; the three
-    layers' FLOPs and the compulsory bytes per step over the closure's time.  (2) The pipeline
-    on a building layout (400 m x 200 m, buildings 5-30 m at 30 % cover, fine 1 m triangles,
-    coarse 8 m DIP cells): sample generation from the solver's own runs, training on the tensor
-    cores, and the coarse run's error against the fine run averaged onto it."""
+    (Godunov, Manning, momentum dissipation) timed with the plain closure and with a network
+    attached in its place (random weights, a hull that admits every cell: the network runs for
+    every cell inside the cell-update kernel), CUDA events on the library's stream; the three
+    layers' FLOPs per step over the added time.  (2) The pipeline on building layouts
+    (400 m x 200 m, buildings 5-30 m at 30 % cover, fine 1 m triangles, coarse 8 m DIP cells):
+    on-trajectory samples with nudging targets from three layouts, training on the tensor
+    cores, and on two unseen layouts the coarse runs' errors against the fine run averaged onto
+    them: without closure, with the plain closure (mu 0.1, 0.3), with the learned one."""
     import numpy as np
     import torch
 
@@ -580,11 +581,9 @@ def run_closure(pkg, args, local_rank):
     net = C.MLP(C.init_params(1), norm, device=local_rank)
     model.set_closure(net, np.full(10, -1e30, np.float32), np.full(10, 1e30, np.float32))
     clos_ms = timed(100)
-    model.set_option("closure_fused", 0)
-    unfused_ms = timed(100)
+    kps = model.kernels_per_step
     n = case.mesh.cell_nb
-    npad = (n + 127) // 128 * 128
-    flops = 2.0 * npad * (16 * 64 + 64 * 64 + 64 * 16)
+    flops = 2.0 * n * (16 * 64 + 64 * 64 + 64 * 16)
     model.close()
     net.close()
     peak = None
@@ -592,30 +591,27 @@ def run_closure(pkg, args, local_rank):
     if os.path.exists(p):
         peak = float(json.load(open(p)).get("bf16_tflops", 0.0)) or None
     t0 = time.perf_counter()
-    fine, coarse, av = C.urban_cases(lx=400.0, ly=200.0, dx_fine=1.0, coarse_factor=8, seed=1)
-    X, Y, T = C.generate_samples(fine, coarse, av, t_start=5.0, n_samples=150, spacing=0.3, device=local_rank)
+    lay = {s: C.urban_cases(lx=400.0, ly=200.0, dx_fine=1.0, coarse_factor=8, seed=s) for s in (1, 2, 3, 7, 8)}
     t1 = time.perf_counter()
-    net, lo, hi, hist = C.train_closure(X, Y, epochs=40, batch=4096, lr=2e-3, device=local_rank)
+    net, lo, hi, hist, n_samples = C.train_on_layouts([lay[1], lay[2], lay[3]], tau=16.0, epochs=12,
+                                                      device=local_rank)
     t2 = time.perf_counter()
-    ev = C.evaluate(fine, coarse, av, 10.0, 30.0, net=net, hull=(lo, hi), mu=0.3, device=local_rank,
-                    scales=(0.5, 1.0))
+    ev = {f"layout{s}_{a:g}-{b:g}s": C.evaluate(*lay[s], a, b, net=net, hull=(lo, hi), device=local_rank)
+          for s in (7, 8) for a, b in ((10.0, 30.0), (20.0, 45.0))}
     t3 = time.perf_counter()
-    closure_ms = clos_ms - base_ms
-    # compulsory bytes of the closure per cell: the state copy at the step's start (32 B read,
-    # 32 B written), then the fused kernel's reads of both states, phiW and the edge minimum of
-    # phiG (32 + 32 + 8 + 4 B) and the state written back (32 B)
-    closure_bytes = n * (64 + 76 + 32)
-    return {"workload": f"DIP channel at {n} cells (Godunov, Manning) with the closure network attached",
-            "ms_per_step_without": base_ms, "ms_per_step_with": clos_ms, "closure_ms_per_step": closure_ms,
-            "closure_ms_per_step_five_launches": unfused_ms - base_ms,
-            "closure_compulsory_bytes_per_step": closure_bytes,
-            "closure_gbs_over_closure_time": closure_bytes / (closure_ms * 1e-3) / 1e9 if closure_ms > 0 else None,
-            "gemm_flops_per_step": flops,
-            "tensor_tflops_over_closure_time": flops / (closure_ms * 1e-3) / 1e12 if closure_ms > 0 else None,
+    net.close()
+    added = clos_ms - base_ms
+    return {"workload": f"DIP channel at {n} cells (Godunov, Manning, momentum dissipation); the network in place "
+                        f"of the plain closure for every cell",
+            "ms_per_step_plain_closure": base_ms, "ms_per_step_learned_closure": clos_ms,
+            "added_ms_per_step": added, "kernels_per_step": kps,
+            "network_flops_per_step": flops,
+            "tensor_tflops_over_added_time": flops / (added * 1e-3) / 1e12 if added > 0 else None,
             "bf16_peak_tflops": peak,
-            "pipeline": {"layout": "400 m x 200 m, buildings 5-30 m at 30 % cover", "fine_cells": fine.mesh.cell_nb,
-                         "coarse_cells": coarse.mesh.cell_nb, "samples": int(X.shape[0]),
-                         "s_generate": t1 - t0, "s_train": t2 - t1, "s_evaluate": t3 - t2,
+            "pipeline": {"layouts": "400 m x 200 m, buildings 5-30 m at 30 % cover, seeds 1-3 train, 7-8 judged",
+                         "fine_cells": lay[1][0].mesh.cell_nb, "coarse_cells": lay[1][1].mesh.cell_nb,
+                         "samples": n_samples, "tau_s": 16.0,
+                         "s_layouts": t1 - t0, "s_collect_and_train": t2 - t1, "s_evaluate": t3 - t2,
                          "train_loss_first_last": [hist[0], hist[-1]],
                          "coarse_error_vs_fine_h_q": ev}}
 

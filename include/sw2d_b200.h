@@ -268,16 +268,25 @@ int sw2d_mlp_loss_grad(sw2d_mlp* m, const float* features, const float* targets,
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the gradient of the last sw2d_mlp_loss_grad */
 int sw2d_mlp_adam_step(sw2d_mlp* m, float lr);
 
-/* Attaches a closure network to a DIP model (net NULL detaches).  Every step then adds the
- * network's momentum correction to the cells whose ten features lie within [hull_lo, hull_hi]
- * (per feature) and applies the model's plain momentum-dissipation closure (its mu map,
- * model_momentum_dissipation) to the step's increments elsewhere; the plain closure inside the
- * cell update is off meanwhile.  Features, from the state at the start of the step (h0, q0, r0)
- * and after the update (h, q, r): h0, q0, r0, h - h0, q - q0, r - r0, phiW, the smallest phiG of
- * the cell's internal edges, dt, sqrt(q0^2 + r0^2) / max(h0, 1e-3).  Outputs: the corrections
- * of q and r, added times `scale`.  The network must live on the model's device and outlive
- * the attachment. */
+/* Attaches a closure network to a DIP model (net NULL detaches).  The network then stands in
+ * for the momentum-dissipation closure of the DIP balance (dip/swDipHyp.cpp:295-324): in every
+ * step, after the flux balance and before the round-off flush and the sources, the cells whose
+ * ten features lie within [hull_lo, hull_hi] (per feature) get the network's momentum
+ * correction, and the others the plain closure (the model's mu map, when
+ * model_momentum_dissipation is active), exactly as without a network.  Features, from the
+ * state at the start of the step (h0, q0, r0) and after the flux balance (h, q, r): h0, q0, r0,
+ * h - h0, q - q0, r - r0, phiW, the smallest phiG of the cell's internal edges, dt,
+ * sqrt(q0^2 + r0^2) / max(h0, 1e-3).  Outputs: the corrections of q and r, added times `scale`.
+ * The network runs inside the cell-update kernel (tensor cores): the step has no more launches.
+ * The network must live on the model's device and outlive the attachment.  Option
+ * "closure_record" (sw2d_set_option) keeps each step's features and outputs for
+ * sw2d_closure_record. */
 int sw2d_set_closure(sw2d_handle* h, sw2d_mlp* net, const float* hull_lo, const float* hull_hi, float scale);
+/* The features and network outputs of every cell in the last step taken with "closure_record"
+ * on, in the caller's cell order: [n_cells x 12] floats (the ten features, then the two outputs
+ * in physical units before `scale` and the hull test).  Returns the number of floats written or
+ * a negative status.  No counterpart in the reference (training-data capture). */
+int64_t sw2d_closure_record(sw2d_handle* h, float* out, int64_t capacity);
 
 /* Replaces the end time t_max of the run (swSp member t_max): the time step is clipped to it,
  * so a run can be brought exactly to any time. */

@@ -331,7 +331,8 @@ def phig_min_of(case) -> np.ndarray:
 
 def features(s0, s1, phiw, phig_min, dt) -> np.ndarray:
     """The ten closure features (float32) of every cell from the state at the start of a step
-    (s0 = h, q, r) and after its update (s1), as the step's closure kernel forms them."""
+    (s0 = h, q, r) and after its flux balance (s1), as the step's update kernel forms them
+    (the kernel's own record, SpModel.closure_record, is what the generators below use)."""
     h0, q0, r0 = (np.asarray(a, dtype=np.float64) for a in s0)
     h1, q1, r1 = (np.asarray(a, dtype=np.float64) for a in s1)
     f = np.stack([h0, q0, r0, h1 - h0, q1 - q0, r1 - r0, np.asarray(phiw, np.float64), np.asarray(phig_min, np.float64),
@@ -339,21 +340,34 @@ def features(s0, s1, phiw, phig_min, dt) -> np.ndarray:
     return f.astype(np.float32)
 
 
+def recorder(device: int = 0) -> "MLP":
+    """A network whose outputs are zero: attached with an empty hull it only records features."""
+    n = np.concatenate([np.zeros(N_IN), np.ones(N_IN), np.zeros(N_OUT), np.ones(N_OUT)])
+    return MLP(np.zeros_like(init_params()), n, device)
+
+
+EMPTY_HULL = (np.ones(N_IN, np.float32), np.zeros(N_IN, np.float32))
+
+
+def _in_hull(f, hull):
+    return np.all((f >= hull[0]) & (f <= hull[1]), 1)
+
+
 def generate_samples(fine, coarse, av, t_start: float, n_samples: int, spacing: float, device: int = 0,
-                     min_depth: float = 1e-3, horizon: int = 1):
-    """Training pairs from the solver itself.  The fine run (buildings resolved) is brought to
-    t_start, then for each sample: its state averaged onto the coarse cells is one coarse DIP step
-    (without closure) from that state; the fine run is brought to exactly the same end time
-    (t_max clip) and averaged again.  Features: closure.features of the coarse step; targets: the
-    averaged fine unit discharges minus the coarse step's.  With horizon > 1 the coarse run
-    makes that many steps and the target is the mismatch at their end divided by the number of
-    steps (a per-step correction fitted over a short rollout).  Cells with fluid and depth above
-    min_depth only.  Returns (X [n x 10], Y [n x 2], times)."""
+                     min_depth: float = 1e-3):
+    """One-step training pairs.  The fine run (buildings resolved) is brought to t_start, then
+    for each sample: its state averaged onto the coarse cells is one coarse DIP step (without
+    correction; features from the update kernel's record); the fine run is brought to exactly
+    the same end time (t_max clip) and averaged again.  Targets: the averaged fine unit
+    discharges minus the coarse step's.  Cells with fluid and depth above min_depth only.
+    Returns (X [n x 10], Y [n x 2], times)."""
     from .solver import SpModel
 
     fm = SpModel(fine, device)
     cm = SpModel(coarse, device)
-    pmin = phig_min_of(coarse)
+    rec = recorder(device)
+    cm.set_closure(rec, *EMPTY_HULL)
+    cm.set_option("closure_record", 1)
     wet_cells = av.fluid_area > 0
     X, Y, T = [], [], []
     fm.set_t_max(t_start)
@@ -365,18 +379,14 @@ def generate_samples(fine, coarse, av, t_start: float, n_samples: int, spacing: 
         cm.set_time(t, 0.0)
         cm.set_t_max(1.0e9)
         cm.step(1)
+        f = cm.closure_record()[:, :N_IN]
         s1 = cm.state()
-        dt = cm.dt
-        f = features(s0, s1, coarse.phi, pmin, dt)
-        if horizon > 1:
-            cm.step(horizon - 1)
-        sk = cm.state()
         fm.set_t_max(cm.t)
         fm.execute()
         st = tuple(av.average(a) for a in fm.state())
         keep = wet_cells & (s0[0] > min_depth)
         X.append(f[keep])
-        Y.append((np.stack([st[1] - sk[1], st[2] - sk[2]], 1)[keep] / horizon).astype(np.float32))
+        Y.append(np.stack([st[1] - s1[1], st[2] - s1[2]], 1)[keep].astype(np.float32))
         T.append(t)
         t = fm.t
         fm.set_t_max(t + spacing)
@@ -384,7 +394,59 @@ def generate_samples(fine, coarse, av, t_start: float, n_samples: int, spacing: 
         t = fm.t
     fm.close()
     cm.close()
+    rec.close()
     return np.concatenate(X), np.concatenate(Y), np.array(T)
+
+
+def generate_trajectory_samples(fine, coarse, av, starts, window: float, tau: float, every: int = 4,
+                                net=None, hull=None, device: int = 0, min_depth: float = 1e-3):
+    """On-trajectory training pairs with nudging targets.  From each start time the coarse model
+    runs freely from the averaged fine state for `window` seconds, with the network `net`
+    attached (its hull, plain closure outside) or with none; every `every`-th step samples each
+    cell: the features the update kernel formed, and as target the correction that would have
+    moved the step's result a fraction dt / tau of the way to the fine run averaged at the same
+    time: Y = c + (fine - coarse) dt / tau, c the correction applied in that step (zero without
+    a network).  The coarse model thus learns, from its own states, the local mean of its error
+    relative to the fine run; tau sets how fast it is corrected.  Returns (X, Y)."""
+    from .solver import SpModel
+
+    own = net is None
+    if own:
+        net, hull = recorder(device), EMPTY_HULL
+    wet_cells = av.fluid_area > 0
+    X, Y = [], []
+    for ts in starts:
+        fm = SpModel(fine, device)
+        fm.set_t_max(ts)
+        fm.execute()
+        cm = SpModel(coarse, device)
+        cm.set_state(*(av.average(a) for a in fm.state()))
+        cm.set_time(fm.t, 0.0)
+        cm.set_t_max(1.0e9)
+        cm.set_closure(net, hull[0], hull[1])
+        cm.set_option("closure_record", 1)
+        t_end = fm.t + window
+        while cm.t < t_end:
+            if every > 1:
+                cm.step(every - 1)
+            h_before = cm.state()[0]
+            cm.step(1)
+            r = cm.closure_record()
+            f, y = r[:, :N_IN], r[:, N_IN:].astype(np.float64)
+            c = np.where(_in_hull(f, hull)[:, None], y, 0.0)
+            s1 = cm.state()
+            fm.set_t_max(cm.t)
+            fm.execute()
+            fa = tuple(av.average(a) for a in fm.state())
+            keep = wet_cells & (h_before > min_depth)
+            g = cm.dt / tau
+            X.append(f[keep])
+            Y.append((c + np.stack([fa[1] - s1[1], fa[2] - s1[2]], 1) * g)[keep].astype(np.float32))
+        fm.close()
+        cm.close()
+    if own:
+        net.close()
+    return np.concatenate(X), np.concatenate(Y)
 
 
 def train_closure(X, Y, epochs: int = 30, batch: int = 4096, lr: float = 2e-3, seed: int = 0, device: int = 0,
@@ -398,12 +460,25 @@ def train_closure(X, Y, epochs: int = 30, batch: int = 4096, lr: float = 2e-3, s
     return net, X.min(0) - hull_margin * span, X.max(0) + hull_margin * span, hist
 
 
-def evaluate(fine, coarse, av, t0: float, t1: float, net=None, hull=None, mu: float = 0.3, device: int = 0,
+def train_on_layouts(layouts, tau: float = 16.0, starts=(4.0, 14.0, 24.0), window: float = 10.0, every: int = 8,
+                     epochs: int = 20, batch: int = 8192, lr: float = 2e-3, seed: int = 0, device: int = 0):
+    """The closure's training protocol: on-trajectory samples with nudging targets
+    (generate_trajectory_samples) from every (fine, coarse, averager) layout, then Adam on the
+    tensor cores.  Returns (net, hull_lo, hull_hi, loss history, number of samples)."""
+    D = [generate_trajectory_samples(*lay, starts=starts, window=window, tau=tau, every=every, device=device)
+         for lay in layouts]
+    X = np.concatenate([d[0] for d in D])
+    Y = np.concatenate([d[1] for d in D])
+    net, lo, hi, hist = train_closure(X, Y, epochs=epochs, batch=batch, lr=lr, seed=seed, device=device)
+    return net, lo, hi, hist, int(X.shape[0])
+
+
+def evaluate(fine, coarse, av, t0: float, t1: float, net=None, hull=None, mus=(0.1, 0.3), device: int = 0,
              scales=(1.0,)):
     """Coarse DIP runs from the fine state averaged at t0 to t1 with (a) no closure, (b) the plain
-    closure (uniform mu tensor), (c) the learned closure with the plain one as fallback; each is
-    judged against the fine run averaged at t1.  Returns {run: (relative L2 error of h, of
-    (q, r))} over the cells with fluid."""
+    closure (uniform mu tensor, for each value in mus), (c) the learned closure with the plain one
+    (mus[0]) as fallback out of its hull; each is judged against the fine run averaged at t1.
+    Returns {run: (relative L2 error of h, of (q, r))} over the cells with fluid."""
     import copy
     from .solver import SpModel
 
@@ -417,9 +492,12 @@ def evaluate(fine, coarse, av, t0: float, t1: float, net=None, hull=None, mu: fl
     fm.close()
     wet = av.fluid_area > 0
     n = coarse.mesh.cell_nb
-    with_mu = copy.copy(coarse)
-    with_mu.opts = dict(coarse.opts, model_momentum_dissipation="active")
-    with_mu.mu = np.stack([np.full(n, mu), np.full(n, mu), np.zeros(n)])
+
+    def with_mu(mu):
+        c = copy.copy(coarse)
+        c.opts = dict(coarse.opts, model_momentum_dissipation="active")
+        c.mu = np.stack([np.full(n, mu), np.full(n, mu), np.zeros(n)])
+        return c
 
     def run(case, attach, scale=1.0):
         cm = SpModel(case, device)
@@ -436,8 +514,10 @@ def evaluate(fine, coarse, av, t0: float, t1: float, net=None, hull=None, mu: fl
         tq = np.concatenate([truth[1][wet], truth[2][wet]])
         return float(eh), float(np.linalg.norm(dq) / max(np.linalg.norm(tq), 1e-30))
 
-    res = {"none": run(coarse, False), "plain_mu": run(with_mu, False)}
+    res = {"none": run(coarse, False)}
+    for mu in mus:
+        res[f"plain_mu{mu:g}"] = run(with_mu(mu), False)
     if net is not None:
         for sc in scales:
-            res["learned" if sc == 1.0 else f"learned_x{sc:g}"] = run(with_mu, True, sc)
+            res["learned" if sc == 1.0 else f"learned_x{sc:g}"] = run(with_mu(mus[0]), True, sc)
     return res

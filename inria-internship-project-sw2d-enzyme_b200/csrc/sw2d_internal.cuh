@@ -303,13 +303,12 @@ void ddp_release(sw2d_handle* h);
 // Validates the DDP arguments before anything is allocated.
 int ddp_check(const sw2d_mesh* mesh, const sw2d_ddp_fields* ddp, std::string& why);
 
-// The learned closure around a step (sw2d_mlp.cu): the state at the step's start, then the
-// network's correction after the update; and its release.
-void closure_begin(sw2d_handle* h);
-void closure_end(sw2d_handle* h);
+// The learned closure (sw2d_mlp.cu): the DIP cell update with the network at the closure site,
+// the release, and the feature record switch.
+void closure_update(sw2d_handle* h, const DevMesh& m);
 void closure_release(sw2d_handle* h);
-void closure_set_fused(sw2d_handle* h, int fused);
-int closure_kernels(const sw2d_handle* h);  // kernel launches the closure adds to a step
+int closure_record(sw2d_handle* h, int on);
+int closure_set_ctas(sw2d_handle* h, int per_sm);  // resident CTAs per SM of the update (0: all that fit)
 
 // Releases the adjoint buffers of the handle (sw2d_adjoint.cu).
 void adjoint_release(sw2d_handle* h);

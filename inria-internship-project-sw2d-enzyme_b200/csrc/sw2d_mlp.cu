@@ -54,18 +54,34 @@ struct GemmArgs {
     unsigned* status;
 };
 
-__device__ __forceinline__ float gelu(float x)
+// GELU in its tanh form, 0.5 x (1 + tanh(k0 (x + k1 x^3))), with the hardware tanh
+// (tanh.approx.f32, relative error about 2^-11: below the BF16 rounding the activation gets
+// next) and explicit FMAs, so that training and inference share one activation whatever the
+// file's contraction flags
+__device__ __forceinline__ float tanh_hw(float u)
 {
-    const float k0 = 0.7978845608028654f, k1 = 0.044715f;
-    return 0.5f * x * (1.0f + tanhf(k0 * (x + k1 * x * x * x)));
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return t;
 }
 
+constexpr float kGeluK0 = 0.7978845608028654f, kGeluK1 = 0.044715f;
+
+__device__ __forceinline__ float gelu(float x)
+{
+    const float u = x * __fmaf_rn(kGeluK0 * kGeluK1, x * x, kGeluK0);
+    const float hx = 0.5f * x;
+    return __fmaf_rn(hx, tanh_hw(u), hx);
+}
+
+// d/dx of gelu: 0.5 (1 + t) + 0.5 x (1 - t^2) k0 (1 + 3 k1 x^2), t = tanh(k0 (x + k1 x^3))
 __device__ __forceinline__ float gelu_grad(float x)
 {
-    const float k0 = 0.7978845608028654f, k1 = 0.044715f;
-    const float u = k0 * (x + k1 * x * x * x);
-    const float t = tanhf(u);
-    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * k0 * (1.0f + 3.0f * k1 * x * x);
+    const float x2 = x * x;
+    const float t = tanh_hw(x * __fmaf_rn(kGeluK0 * kGeluK1, x2, kGeluK0));
+    const float du = __fmaf_rn(3.0f * kGeluK0 * kGeluK1, x2, kGeluK0);
+    const float sech2 = __fmaf_rn(-t, t, 1.0f);
+    return __fmaf_rn(0.5f * x * sech2, du, __fmaf_rn(0.5f, t, 0.5f));
 }
 
 template <int kMode>
@@ -611,33 +627,32 @@ int sw2d_mlp_param_count(void) { return sw2d::kNParams; }
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------
-// The closure inside a model's step.  With a network attached (sw2d_set_closure), each step
-// keeps the state it starts from; after the cell update the features of every cell are formed
-// from that state and the updated one, the network runs on the handle's stream (one fused
-// kernel, or features, three GEMM launches and an apply kernel), and the momentum correction it
-// outputs is added where the cell's features lie in the training hull.  Elsewhere the model's plain momentum-dissipation closure (the DIP mu
-// tensor, dip/swDipHyp.cpp:295-324) is applied to the step's increments when the model has
-// one; the plain closure inside the update is switched off while a network is attached.
+// The closure inside a model's step.  With a network attached (sw2d_set_closure), the DIP cell
+// update runs as k_update_closure: per tile of 128 cells it forms the flux balance of every
+// cell as the plain update does, then the ten features of the cell from the state at the step's
+// start and the balanced one, runs the network on the tensor cores and adds the momentum
+// correction it outputs where the features lie in the training hull, at the place where the
+// plain momentum-dissipation closure acts (dip/swDipHyp.cpp:295-324, before the round-off
+// flush and the sources).  Elsewhere the plain closure is applied as the update applies it when
+// the model has one.  No launch is added to the step.
 // ------------------------------------------------------------------------------------------
 namespace sw2d {
 
 struct ClosureState {
     sw2d_mlp* net = nullptr;
-    int64_t npad = 0;
     float lo[kIn], hi[kIn];
     float scale = 1.0f;  // factor on the network's correction
-    int fused = 1;       // one fused kernel per step (0: features, three GEMM launches, apply)
-    double4* old = nullptr;
     float* phig_min = nullptr;
-    __nv_bfloat16 *x = nullptr, *h1 = nullptr, *h2 = nullptr;
-    float *z1 = nullptr, *z2 = nullptr, *y = nullptr;
-    unsigned char* inside = nullptr;
+    float* rec = nullptr;  // [nc x 12] features and outputs of the last step, or null
+    unsigned grid = 0;     // persistent grid of the update kernel
+    int sms = 0, per_sm_max = 1;  // SMs, resident CTAs per SM the kernel's resources allow
+    int64_t ntiles = 0;
     std::vector<void*> allocs;
 };
 
-// the ten features of a cell from the state at the start of the step (a) and after the update
-// (b): depth, unit discharges, their increments, storage porosity, the smallest connectivity
-// porosity of the cell's internal edges, dt and the speed at the start
+// the ten features of a cell from the state at the start of the step (a) and after the flux
+// balance (b): depth, unit discharges, their increments, storage porosity, the smallest
+// connectivity porosity of the cell's internal edges, dt and the speed at the start
 SW2D_HD void closure_features(double4 a, double4 b, double phiw, double phig_min, double dt, double* f)
 {
     f[0] = a.x;
@@ -658,8 +673,20 @@ namespace {
 
 using namespace sw2d;
 
+constexpr int kRec = kIn + kOut;  // floats per cell in the feature record
+
 struct ClosureNorm {
     float xmean[kIn], xstd[kIn], lo[kIn], hi[kIn], ymean[kOut], ystd[kOut], scale;
+};
+
+struct ClosureArgs {
+    const float* phig_min;
+    ClosureNorm cn;
+    const __nv_bfloat16 *w1, *w2, *w3;
+    const float *b1, *b2, *b3;
+    float* rec;
+    int dissip;
+    unsigned* status;
 };
 
 __global__ void k_closure_phig_min(DevMesh m, float* out)
@@ -672,67 +699,18 @@ __global__ void k_closure_phig_min(DevMesh m, float* out)
     out[c] = (float)g;
 }
 
-__global__ void k_closure_features(DevMesh m, const double4* __restrict__ old, const float* __restrict__ phig_min,
-                                   ClosureNorm cn, int64_t npad, __nv_bfloat16* x, unsigned char* inside)
-{
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npad) return;
-    if (i >= m.nc) {
-        for (int k = 0; k < kInPad; k++) x[i * kInPad + k] = __float2bfloat16_rn(0.0f);
-        return;
-    }
-    double f[kIn];
-    closure_features(old[i], m.st[i], m.cst[i].z, phig_min[i], m.ctrl->dt, f);
-    bool in = true;
-    for (int k = 0; k < kInPad; k++) {
-        float v = 0.0f;
-        if (k < kIn) {
-            const float fk = (float)f[k];
-            in = in && (fk >= cn.lo[k]) && (fk <= cn.hi[k]);
-            v = (fk - cn.xmean[k]) / cn.xstd[k];
-        }
-        x[i * kInPad + k] = __float2bfloat16_rn(v);
-    }
-    inside[i] = in ? 1 : 0;
-}
-
-__global__ void k_closure_apply(DevMesh m, const double4* __restrict__ old, const float* __restrict__ y,
-                                const unsigned char* __restrict__ inside, ClosureNorm cn, int dissip)
-{
-    if (!m.ctrl->go) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.nc) return;
-    double4 s = m.st[i];
-    if (inside[i]) {
-        s.y += (double)(cn.scale * (y[(size_t)i * kOutPad + 0] * cn.ystd[0] + cn.ymean[0]));
-        s.z += (double)(cn.scale * (y[(size_t)i * kOutPad + 1] * cn.ystd[1] + cn.ymean[1]));
-    } else if (dissip) {
-        const double4 mu = m.mu[i];
-        const double4 a = old[i];
-        double q = s.y, r = s.z;
-        momentum_dissipation(mu.x, mu.y, mu.z, mu.w, a.x, a.y, a.z, s.x, q, r);
-        s.y = q;
-        s.z = r;
-    } else {
-        return;
-    }
-    m.st[i] = s;
-}
-
-// The whole closure of a step in one kernel: per tile of 128 cells the features go to shared
-// memory as the first layer's A operand, and each layer is an MMA into TMEM whose epilogue
-// (bias, GELU, BF16) writes the next layer's A operand back to shared memory; the last
-// epilogue applies the correction (or the plain closure out of the hull) to the state.  The
-// weights are staged once per CTA; CTAs loop over tiles.  The three accumulators share TMEM
-// columns [0, 64): each layer's MMA is issued after every lane has read the previous one out.
-// The MMAs, their order and the epilogue arithmetic are those of the five-launch path.
-__global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4* __restrict__ old,
-                                                       const float* __restrict__ phig_min, ClosureNorm cn,
-                                                       const __nv_bfloat16* __restrict__ w1,
-                                                       const __nv_bfloat16* __restrict__ w2,
-                                                       const __nv_bfloat16* __restrict__ w3, const float* __restrict__ b1,
-                                                       const float* __restrict__ b2, const float* __restrict__ b3,
-                                                       int dissip, unsigned* status)
+// The DIP cell update with the network at the closure site, persistent over tiles of 128 cells
+// (thread i of the CTA owns cell i of the tile, which is TMEM lane i).  Per tile: the flux
+// balance (as k_update: swSpHyp.cpp:214-273), the features as the first layer's BF16 A operand
+// in shared memory, then per layer one round of MMAs into TMEM whose epilogue (bias, GELU,
+// BF16) writes the next layer's A operand back to shared memory; the three accumulators share
+// TMEM columns [0, 64), each layer's MMAs issued after every lane has read the previous one
+// out.  Then the correction (in the hull) or the plain closure, the round-off flush, the
+// negative-depth rule, friction and head loss, and the new state.  The weights are staged once
+// per CTA.  The MMAs, their order and the epilogue arithmetic are those of the GEMM kernel, so
+// the outputs equal sw2d_mlp_infer's on the same features bit for bit.
+template <int kFriction, bool kHeadLoss>
+__global__ void __launch_bounds__(128) k_update_closure(DevMesh m, ClosureArgs a)
 {
     __shared__ __align__(1024) uint16_t sX[kTileM * kInPad];
     __shared__ __align__(1024) uint16_t sH[kTileM * kHid];
@@ -742,7 +720,14 @@ __global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4*
     __shared__ float sb1[kHid], sb2[kHid], sb3[kOutPad];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_holder;
+    Ctrl* ctrl = m.ctrl;
+    if (!ctrl->go) return;  // uniform over the grid: nothing allocated yet
+    const double dt = ctrl->dt;
     const int tid = threadIdx.x, warp = tid >> 5;
+    if (blockIdx.x == 0 && tid == 0) {
+        ctrl->t = ctrl->t + dt;  // swSp.cpp:592; no other thread of this kernel reads t
+        ctrl->steps += 1;
+    }
     const uint32_t ncols = 64;
     if (warp == 0) {
         tmem_alloc(&tmem_holder, ncols);
@@ -753,23 +738,23 @@ __global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4*
     for (int i = tid; i < kHid * (kInPad / 8); i += 128) {
         const int n = i / (kInPad / 8), c = i % (kInPad / 8);
         *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sW1) + core_offset(n, c * 8, kInPad)) =
-            *reinterpret_cast<const uint4*>(w1 + n * kInPad + c * 8);
+            *reinterpret_cast<const uint4*>(a.w1 + n * kInPad + c * 8);
     }
     for (int i = tid; i < kHid * (kHid / 8); i += 128) {
         const int n = i / (kHid / 8), c = i % (kHid / 8);
         *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sW2) + core_offset(n, c * 8, kHid)) =
-            *reinterpret_cast<const uint4*>(w2 + n * kHid + c * 8);
+            *reinterpret_cast<const uint4*>(a.w2 + n * kHid + c * 8);
     }
     for (int i = tid; i < kOutPad * (kHid / 8); i += 128) {
         const int n = i / (kHid / 8), c = i % (kHid / 8);
         *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sW3) + core_offset(n, c * 8, kHid)) =
-            *reinterpret_cast<const uint4*>(w3 + n * kHid + c * 8);
+            *reinterpret_cast<const uint4*>(a.w3 + n * kHid + c * 8);
     }
     if (tid < kHid) {
-        sb1[tid] = b1[tid];
-        sb2[tid] = b2[tid];
+        sb1[tid] = a.b1[tid];
+        sb2[tid] = a.b2[tid];
     }
-    if (tid < kOutPad) sb3[tid] = b3[tid];
+    if (tid < kOutPad) sb3[tid] = a.b3[tid];
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
@@ -778,37 +763,50 @@ __global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4*
     const uint32_t id64 = idesc_bf16_f32(kTileM, kHid), id16 = idesc_bf16_f32(kTileM, kOutPad);
     const uint32_t aX = smem_u32(sX), aH = smem_u32(sH), aW1 = smem_u32(sW1), aW2 = smem_u32(sW2),
                    aW3 = smem_u32(sW3);
-    const bool go = m.ctrl->go != 0;
-    const double dt = m.ctrl->dt;
+    const ClosureNorm& cn = a.cn;
     uint32_t phase = 0;
     bool ok = true;
     const int ntiles = (m.nc + kTileM - 1) / kTileM;
-    for (int tile = blockIdx.x; tile < ntiles && go; tile += gridDim.x) {
-        const int row = tid;  // the tile row of this thread: its TMEM lane
-        const int c = tile * kTileM + row;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int c = tile * kTileM + tid;
         const bool valid = c < m.nc;
-        double4 a = make_double4(0, 0, 0, 0), b = make_double4(0, 0, 0, 0);
+        double4 s0 = make_double4(0, 0, 0, 0);
+        double hh = 0, qq = 0, rr = 0;
         bool in = false;
+        float f32[kIn];
         {
             float xv[kInPad];
             for (int k = 0; k < kInPad; k++) xv[k] = 0.0f;
             if (valid) {
-                a = old[c];
-                b = m.st[c];
+                s0 = m.st[c];
+                hh = s0.x;
+                qq = s0.y;
+                rr = s0.z;
+                // hypComputeBalance (swSpHyp.cpp:214-273), the slots in the reference's order
+                const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
+                for (int k = k0; k < k1; k++) {
+                    const double4 v = m.slot[k];
+                    hh += v.x * dt;
+                    qq += v.y * dt;
+                    rr += v.z * dt;
+                }
                 double f[kIn];
-                closure_features(a, b, m.cst[c].z, phig_min[c], dt, f);
+                closure_features(s0, make_double4(hh, qq, rr, 0.0), ld(&m.cst[c].z), a.phig_min[c], dt, f);
                 in = true;
                 for (int k = 0; k < kIn; k++) {
-                    const float fk = (float)f[k];
-                    in = in && (fk >= cn.lo[k]) && (fk <= cn.hi[k]);
-                    xv[k] = (fk - cn.xmean[k]) / cn.xstd[k];
+                    f32[k] = (float)f[k];
+                    in = in && (f32[k] >= cn.lo[k]) && (f32[k] <= cn.hi[k]);
+                    xv[k] = (f32[k] - cn.xmean[k]) / cn.xstd[k];
                 }
             }
             for (int cc = 0; cc < kInPad / 8; cc++) {
-                __align__(16) __nv_bfloat16 v[8];
-                for (int j = 0; j < 8; j++) v[j] = __float2bfloat16_rn(xv[cc * 8 + j]);
-                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sX) + core_offset(row, cc * 8, kInPad)) =
-                    *reinterpret_cast<const uint4*>(v);
+                uint32_t pk[4];
+                for (int j = 0; j < 4; j++) {
+                    const __nv_bfloat162 pr = __floats2bfloat162_rn(xv[cc * 8 + 2 * j], xv[cc * 8 + 2 * j + 1]);
+                    pk[j] = *reinterpret_cast<const uint32_t*>(&pr);
+                }
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sX) + core_offset(tid, cc * 8, kInPad)) =
+                    make_uint4(pk[0], pk[1], pk[2], pk[3]);
             }
         }
         // layer 1: one MMA of K = 16
@@ -825,19 +823,23 @@ __global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4*
         }
         phase ^= 1u;
         fence_after_sync();
-        // hidden layers' epilogues, each followed by the next layer's four MMAs of K = 16
+        // the hidden layers' epilogues, each followed by the next layer's four MMAs of K = 16
         for (int layer = 0; layer < 2; layer++) {
             const float* bias = layer == 0 ? sb1 : sb2;
             for (int c0 = 0; c0 < kHid; c0 += 16) {
                 uint32_t v[16];
                 tmem_ld16(lane_base + (uint32_t)c0, v);
                 tmem_wait_ld();
-                __align__(16) __nv_bfloat16 hv[16];
-                for (int j = 0; j < 16; j++) hv[j] = __float2bfloat16_rn(gelu(__uint_as_float(v[j]) + bias[c0 + j]));
-                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(row, c0, kHid)) =
-                    *reinterpret_cast<const uint4*>(hv);
-                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(row, c0 + 8, kHid)) =
-                    *reinterpret_cast<const uint4*>(hv + 8);
+                uint32_t hv[8];  // bf16 pairs
+                for (int j = 0; j < 8; j++) {
+                    const __nv_bfloat162 pr = __floats2bfloat162_rn(gelu(__uint_as_float(v[2 * j]) + bias[c0 + 2 * j]),
+                                                                    gelu(__uint_as_float(v[2 * j + 1]) + bias[c0 + 2 * j + 1]));
+                    hv[j] = *reinterpret_cast<const uint32_t*>(&pr);
+                }
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0, kHid)) =
+                    make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0 + 8, kHid)) =
+                    make_uint4(hv[4], hv[5], hv[6], hv[7]);
             }
             fence_before_sync();
             fence_proxy_async();
@@ -858,24 +860,39 @@ __global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4*
             phase ^= 1u;
             fence_after_sync();
         }
-        // output layer: the correction, or the plain closure outside the hull
         uint32_t v[16];
         tmem_ld16(lane_base, v);
         tmem_wait_ld();
         if (valid && ok) {
-            double4 s = b;
-            if (in) {
-                s.y += (double)(cn.scale * ((__uint_as_float(v[0]) + sb3[0]) * cn.ystd[0] + cn.ymean[0]));
-                s.z += (double)(cn.scale * ((__uint_as_float(v[1]) + sb3[1]) * cn.ystd[1] + cn.ymean[1]));
-                m.st[c] = s;
-            } else if (dissip) {
-                const double4 mu = m.mu[c];
-                double q = s.y, r = s.z;
-                momentum_dissipation(mu.x, mu.y, mu.z, mu.w, a.x, a.y, a.z, s.x, q, r);
-                s.y = q;
-                s.z = r;
-                m.st[c] = s;
+            // the network's outputs in physical units, as sw2d_mlp_infer gives them
+            const float y0 = (__uint_as_float(v[0]) + sb3[0]) * cn.ystd[0] + cn.ymean[0];
+            const float y1 = (__uint_as_float(v[1]) + sb3[1]) * cn.ystd[1] + cn.ymean[1];
+            if (a.rec) {
+                float* r = a.rec + (size_t)c * kRec;
+                for (int k = 0; k < kIn; k++) r[k] = f32[k];
+                r[kIn] = y0;
+                r[kIn + 1] = y1;
             }
+            if (in) {
+                qq += (double)(cn.scale * y0);
+                rr += (double)(cn.scale * y1);
+            } else if (a.dissip) {  // the plain closure (dip/swDipHyp.cpp:295-324)
+                const double4 mu = ld(&m.mu[c]);
+                momentum_dissipation(mu.x, mu.y, mu.z, mu.w, s0.x, s0.y, s0.z, hh, qq, rr);
+            }
+            if (fabs(hh) < kSmallReal) hh = 0.;
+            if (fabs(qq) < kSmallReal) qq = 0.;
+            if (fabs(rr) < kSmallReal) rr = 0.;
+            // negative depth (swSpHyp.cpp:182-210)
+            if (m.neg_detect) {
+                if (hh < 0) atomicOr(&ctrl->status, kStatusNegDepth);
+            } else if (hh < 0.) {
+                hh = 0.;
+                qq = 0.;
+                rr = 0.;
+            }
+            cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr);
+            m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));
         }
         fence_before_sync();
         ok = __syncthreads_and(ok);  // every lane read out before the next tile's MMAs overwrite TMEM
@@ -884,7 +901,27 @@ __global__ void __launch_bounds__(128) k_closure_fused(DevMesh m, const double4*
     fence_before_sync();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, ncols);
-    if (!ok && tid == 0) atomicOr(status, kStatusTimeout);
+    if (!ok && tid == 0) atomicOr(a.status, kStatusTimeout);
+}
+
+// the largest shared-memory carveout for every instance, so that the resident CTAs the
+// occupancy query counts on fit
+template <int kF>
+cudaError_t closure_carveout()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_update_closure<kF, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_update_closure<kF, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+
+template <int kF>
+void launch_closure_f(sw2d_handle* h, const DevMesh& m, const ClosureArgs& a, unsigned g)
+{
+    if (h->p.singular_head_loss) k_update_closure<kF, true><<<g, 128, 0, h->stream>>>(m, a);
+    else k_update_closure<kF, false><<<g, 128, 0, h->stream>>>(m, a);
 }
 
 ClosureNorm closure_norm(const ClosureState* c)
@@ -912,46 +949,58 @@ void closure_free(ClosureState* c)
 
 namespace sw2d {
 
-void closure_begin(sw2d_handle* h)
-{
-    cudaMemcpyAsync(h->closure->old, h->m.st, (size_t)h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream);
-}
-
-void closure_end(sw2d_handle* h)
+void closure_update(sw2d_handle* h, const DevMesh& m)
 {
     ClosureState* c = h->closure;
     sw2d_mlp* net = c->net;
-    const ClosureNorm cn = closure_norm(c);
-    const int64_t npad = c->npad;
-    if (c->fused) {
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-        const int ntiles = (int)(npad / kTileM);
-        const unsigned grid = (unsigned)std::max(1, std::min(ntiles, 6 * sms));
-        k_closure_fused<<<grid, 128, 0, h->stream>>>(h->m, c->old, c->phig_min, cn, net->w1, net->w2, net->w3,
-                                                     net->b1, net->b2, net->b3, h->dissipation && h->m.mu ? 1 : 0,
-                                                     net->status);
-        return;
+    ClosureArgs a;
+    a.phig_min = c->phig_min;
+    a.cn = closure_norm(c);
+    a.w1 = net->w1;
+    a.w2 = net->w2;
+    a.w3 = net->w3;
+    a.b1 = net->b1;
+    a.b2 = net->b2;
+    a.b3 = net->b3;
+    a.rec = c->rec;
+    a.dissip = h->dissipation && m.mu ? 1 : 0;
+    a.status = net->status;
+    switch (h->p.friction) {
+        case SW2D_FRICTION_CHEZY: launch_closure_f<SW2D_FRICTION_CHEZY>(h, m, a, c->grid); break;
+        case SW2D_FRICTION_MANNING: launch_closure_f<SW2D_FRICTION_MANNING>(h, m, a, c->grid); break;
+        case SW2D_FRICTION_STRICKLER: launch_closure_f<SW2D_FRICTION_STRICKLER>(h, m, a, c->grid); break;
+        default: launch_closure_f<SW2D_FRICTION_NONE>(h, m, a, c->grid); break;
     }
-    k_closure_features<<<(unsigned)((npad + 255) / 256), 256, 0, h->stream>>>(h->m, c->old, c->phig_min, cn, npad, c->x,
-                                                                             c->inside);
-    gemm(net, kEpiGelu, c->x, kInPad, net->w1, kInPad, (int)npad, kHid, kInPad, net->b1, c->z1, kHid, c->h1, kHid,
-         nullptr, kHid, h->stream);
-    gemm(net, kEpiGelu, c->h1, kHid, net->w2, kHid, (int)npad, kHid, kHid, net->b2, c->z2, kHid, c->h2, kHid, nullptr,
-         kHid, h->stream);
-    gemm(net, kEpiStore, c->h2, kHid, net->w3, kHid, (int)npad, kOutPad, kHid, net->b3, c->y, kOutPad, nullptr, 0,
-         nullptr, kOutPad, h->stream);
-    k_closure_apply<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, c->old, c->y, c->inside, cn,
-                                                              h->dissipation && h->m.mu ? 1 : 0);
 }
-
-void closure_set_fused(sw2d_handle* h, int fused) { h->closure->fused = fused; }
-int closure_kernels(const sw2d_handle* h) { return h->closure->fused ? 1 : 5; }
 
 void closure_release(sw2d_handle* h)
 {
     closure_free(h->closure);
     h->closure = nullptr;
+}
+
+int closure_set_ctas(sw2d_handle* h, int per_sm)
+{
+    ClosureState* c = h->closure;
+    const int k = per_sm <= 0 ? c->per_sm_max : std::min(per_sm, c->per_sm_max);
+    c->grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(c->ntiles, (int64_t)k * c->sms));
+    return SW2D_OK;
+}
+
+int closure_record(sw2d_handle* h, int on)
+{
+    ClosureState* c = h->closure;
+    if (on && !c->rec) {
+        void* p = nullptr;
+        const size_t bytes = (size_t)std::max<int64_t>(h->nc, 1) * kRec * sizeof(float);
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return fail(h, SW2D_E_CUDA, "closure record buffer");
+        c->allocs.push_back(p);
+        if (cudaMemset(p, 0, bytes) != cudaSuccess) return fail(h, SW2D_E_CUDA, "closure record buffer");
+        c->rec = static_cast<float*>(p);
+    } else if (!on) {
+        c->rec = nullptr;  // the buffer stays allocated until the closure is detached
+    }
+    return SW2D_OK;
 }
 
 }  // namespace sw2d
@@ -980,29 +1029,63 @@ int sw2d_set_closure(sw2d_handle* h, sw2d_mlp* net, const float* hull_lo, const 
     if (!hull_lo || !hull_hi) return fail(h, SW2D_E_ARG, "training hull missing");
     ClosureState* c = new ClosureState();
     c->net = net;
-    c->npad = (h->nc + kTileM - 1) / kTileM * kTileM;
     std::memcpy(c->lo, hull_lo, sizeof(c->lo));
     std::memcpy(c->hi, hull_hi, sizeof(c->hi));
     c->scale = scale;
-    auto al = [&](size_t bytes, void** p) {
-        if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) return false;
-        c->allocs.push_back(*p);
-        return cudaMemset(*p, 0, std::max<size_t>(bytes, 16)) == cudaSuccess;
-    };
-    const size_t np = (size_t)c->npad;
-    bool ok = al((size_t)h->nc * sizeof(double4), (void**)&c->old) && al(np * sizeof(float), (void**)&c->phig_min) &&
-              al(np * kInPad * 2, (void**)&c->x) && al(np * kHid * 2, (void**)&c->h1) &&
-              al(np * kHid * 2, (void**)&c->h2) && al(np * kHid * 4, (void**)&c->z1) &&
-              al(np * kHid * 4, (void**)&c->z2) && al(np * kOutPad * 4, (void**)&c->y) && al(np, (void**)&c->inside);
-    if (!ok) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, (size_t)std::max<int64_t>(h->nc, 1) * sizeof(float)) != cudaSuccess) {
         closure_free(c);
         return fail(h, SW2D_E_CUDA, "closure buffers");
     }
+    c->allocs.push_back(p);
+    c->phig_min = static_cast<float*>(p);
+    // persistent grid: every CTA resident at once (each holds 64 TMEM columns of the SM's 512)
+    // resident CTAs per SM from the kernel's registers and shared memory (1 KB of it reserved per
+    // CTA), at most 8: 8 x 64 TMEM columns fill the SM's 512
+    cudaError_t e = closure_carveout<SW2D_FRICTION_NONE>();
+    if (e == cudaSuccess) e = closure_carveout<SW2D_FRICTION_CHEZY>();
+    if (e == cudaSuccess) e = closure_carveout<SW2D_FRICTION_MANNING>();
+    if (e == cudaSuccess) e = closure_carveout<SW2D_FRICTION_STRICKLER>();
+    cudaFuncAttributes fa;
+    cudaDeviceProp prop;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_update_closure<SW2D_FRICTION_MANNING, true>);
+    if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, h->device);
+    if (e != cudaSuccess) {
+        closure_free(c);
+        return fail(h, SW2D_E_CUDA, std::string("closure launch set-up: ") + cudaGetErrorString(e));
+    }
+    c->sms = prop.multiProcessorCount;
+    const int by_regs = prop.regsPerMultiprocessor / std::max(1, ((fa.numRegs * 32 + 255) / 256 * 256) * 4);
+    const int by_smem = (int)(prop.sharedMemPerMultiprocessor / (fa.sharedSizeBytes + 1024));
+    const int by_threads = prop.maxThreadsPerMultiProcessor / 128;
+    c->per_sm_max = std::max(1, std::min(std::min(by_regs, by_smem), std::min(by_threads, 8)));
+    c->ntiles = (h->nc + kTileM - 1) / kTileM;
     h->closure = c;
+    closure_set_ctas(h, 0);
     k_closure_phig_min<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, c->phig_min);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     return SW2D_OK;
+}
+
+// Features and network outputs of every cell in the last step taken with recording on
+// (sw2d_set_option "closure_record"), in the caller's cell order: [n_cells x 12] floats, the
+// ten features then the two outputs in physical units (before the scale factor and the hull
+// test).  Returns the number of floats written.
+int64_t sw2d_closure_record(sw2d_handle* h, float* out, int64_t capacity)
+{
+    using namespace sw2d;
+    if (!h || !out) return SW2D_E_ARG;
+    if (!h->closure || !h->closure->rec) return fail(h, SW2D_E_ARG, "closure recording is off");
+    const int64_t n = h->nc * kRec;
+    if (capacity < n) return fail(h, SW2D_E_ARG, "output buffer too small");
+    CK(cudaSetDevice(h->device));
+    std::vector<float> buf((size_t)n);
+    CK(cudaMemcpyAsync(buf.data(), h->closure->rec, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t i = 0; i < h->nc; i++)
+        std::memcpy(out + (int64_t)h->cell_perm[i] * kRec, buf.data() + i * kRec, kRec * sizeof(float));
+    return n;
 }
 
 }  // extern "C"

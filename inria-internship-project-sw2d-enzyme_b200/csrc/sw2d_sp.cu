@@ -619,9 +619,10 @@ void launch_update_d(sw2d_handle* h, const DevMesh& m)
 template <bool kStoreB>
 void launch_update_s(sw2d_handle* h, const DevMesh& m)
 {
-    // a learned closure replaces the plain dissipation inside the update (it applies the plain
-    // closure itself where its inputs leave the training hull)
-    if (!kStoreB && h->dissipation && !h->closure) launch_update_d<false, true>(h, m);
+    // with a learned closure attached the update runs the network at the closure site (and the
+    // plain closure where the features leave the training hull)
+    if (!kStoreB && h->closure) closure_update(h, m);
+    else if (!kStoreB && h->dissipation) launch_update_d<false, true>(h, m);
     else launch_update_d<kStoreB, false>(h, m);
 }
 
@@ -645,9 +646,7 @@ void launch_phase(sw2d_handle* h, int i)
 
 void launch_step(sw2d_handle* h)
 {
-    if (h->closure) closure_begin(h);
     for (int i = 0; i < 4; i++) launch_phase(h, i);
-    if (h->closure) closure_end(h);
 }
 
 }  // namespace
@@ -1139,16 +1138,19 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
 int sw2d_execute(sw2d_handle* h, int64_t* steps_done)
 {
     if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
-    int64_t total = 0;
+    // passes of growing length (32 .. 1024 steps): a run that ends after a few steps does not
+    // pay for a thousand launches that find the run over
+    int64_t total = 0, chunk = 32;
     for (;;) {
         int64_t k = 0;
-        int st = sw2d_step_n(h, 1024, &k);
+        int st = sw2d_step_n(h, chunk, &k);
         total += k;
         if (st) {
             if (steps_done) *steps_done = total;
             return st;
         }
-        if (k < 1024) break;
+        if (k < chunk) break;
+        chunk = std::min<int64_t>(2 * chunk, 1024);
     }
     if (steps_done) *steps_done = total;
     return SW2D_OK;
@@ -1315,11 +1317,17 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         // reference does; 1 from the replay's own states (the exact gradient of the replay cost)
         h->assim_chained = value ? 1 : 0;
         return SW2D_OK;
-    } else if (std::strcmp(name, "closure_fused") == 0) {
-        // the learned closure as one fused kernel (1, default) or as features, three GEMM
-        // launches and the apply kernel (0); both give the same numbers
+    } else if (std::strcmp(name, "closure_record") == 0) {
+        // keep each step's closure features and network outputs (sw2d_closure_record)
         if (!h->closure) return fail(h, SW2D_E_ARG, "no closure attached");
-        closure_set_fused(h, value ? 1 : 0);
+        const int rc = closure_record(h, value ? 1 : 0);
+        if (rc) return rc;
+    } else if (std::strcmp(name, "closure_ctas_per_sm") == 0) {
+        // launch shape of the closure's update kernel: CTAs per SM of its persistent grid (0:
+        // as many as the kernel's registers and shared memory let reside)
+        if (!h->closure) return fail(h, SW2D_E_ARG, "no closure attached");
+        if (value < 0 || value > 8) return fail(h, SW2D_E_ARG, "closure_ctas_per_sm outside 0..8");
+        closure_set_ctas(h, (int)value);
     } else if (std::strcmp(name, "adjoint_edge_variant") == 0) {
         if (value < 0 || value > 4) return fail(h, SW2D_E_ARG, "adjoint_edge_variant outside 0..4");
         h->adj_edge_variant = (int)value;
@@ -1576,7 +1584,7 @@ int sw2d_kernels_per_step(sw2d_handle* h)
 {
     if (!h) return 0;
     if (h->model == kModelDdp) return ddp_kernels_per_step(h);
-    return (h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3) + (h->closure ? closure_kernels(h) : 0);
+    return h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3;
 }
 
 int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n)

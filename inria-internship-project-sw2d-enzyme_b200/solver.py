@@ -168,6 +168,15 @@ class SpModel:
                                               float(scale)))
         self._closure = net  # keep the network alive while attached
 
+    def closure_record(self) -> np.ndarray:
+        """[n x 12] float32: the ten closure features and the network's two outputs of every cell
+        in the last step taken with option "closure_record" on (caller's cell order)."""
+        out = np.empty((self.n, 12), dtype=np.float32)
+        k = self.lib.sw2d_closure_record(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), out.size)
+        if k < 0:
+            self._check(int(k))
+        return out
+
     def array(self, name: str) -> np.ndarray:
         out = np.empty(max(self.n, self.ni, self.nb, 1))
         k = self.lib.sw2d_get_array(self.handle, name.encode(), out.ctypes.data_as(capi.c_double_p), out.size)
