@@ -51,6 +51,7 @@ extern "C" {
                                     src/sw2dSolver/models/dip/swDip.cpp:1524-1528            */
 #define SW2D_E_DDP_TABLE (-11)   /* DDP: NaN elevation or volume in a porosity-table lookup, where
                                     the reference indexes level -1 (swDdp.cpp:1090-1096, 3382-3386) */
+#define SW2D_E_IO (-12)          /* writing the result file failed (the reference: logFatal)     */
 
 /* enumerations of the input.solv string keys (src/sw2dSolver/common/swSolverParam.h:130-153) */
 enum sw2d_scheme { SW2D_SCHEME_GODUNOV = 0, SW2D_SCHEME_MUSCL_EVR = 1 };
@@ -291,6 +292,29 @@ int64_t sw2d_closure_record(sw2d_handle* h, float* out, int64_t capacity);
 /* Replaces the end time t_max of the run (swSp member t_max): the time step is clipped to it,
  * so a run can be brought exactly to any time. */
 int sw2d_set_t_max(sw2d_handle* h, double t_max);
+
+/* ---- binary map file (ResultHydro.bin) -------------------------------------------------------
+ * The reference's output_format bin: swIO::initBinFileMapDecimal (src/common/swIO.cpp:311-645)
+ * writes the header, swIO::fillBinFileMapDecimal (:285-309) one frame per stored map, with the
+ * values of storeResultMaps (sp/swSp.cpp:1514-1605, dip/swDip.cpp:1657-1750,
+ * ddp/swDdp.cpp:2440-2555) at the times of swParent::checkStore (swParent.cpp:46-69).
+ * Header: the geometry file's part from its start to the node-to-cell lists, the variable count
+ * (u64), "bottom_elevation" and the names of map_storage_mode (u64 length + bytes), t_0, t_max,
+ * dt_map.  Frame: t, then per cell (caller's numbering) z_b and the mode's values (f64).
+ * mode: map_storage_mode default (h, qx, qy, |q|), all (15 values; not for DDP) or none. */
+enum sw2d_result_mode { SW2D_RESULT_DEFAULT = 0, SW2D_RESULT_ALL = 1, SW2D_RESULT_NONE = 2 };
+/* Writes the header alone (host only; model 0 SP, 1 DIP, 2 DDP). */
+int sw2d_result_header(const char* path, const char* geometry_path, int model, int mode, double t_0, double t_max,
+                       double dt_map);
+/* Creates `path` with the header (t_0 and dt_map of the model, its current t_max) and attaches
+ * it: sw2d_execute then appends the run's first frame (once), a frame after every step that
+ * ends on a storage time, and a frame at its end, as swSp::execute does (swSp.cpp:501-632);
+ * sw2d_step_n appends the frames of its steps.  Frames are copied from the device while the
+ * next steps run and written by a thread of the library; sw2d_execute returns once its frames
+ * are on file. */
+int sw2d_result_open(sw2d_handle* h, const char* path, const char* geometry_path, int mode);
+/* Waits for every frame to reach the file, closes and detaches it. */
+int sw2d_result_close(sw2d_handle* h);
 
 /* Advances at most n_steps passes of the body of swSp::execute's time loop
  * (swSp.cpp:522-589: hypCompute, friction, singular head loss, correctVelocity, t += dt),

@@ -24,6 +24,8 @@ c_int32_p = ctypes.POINTER(ctypes.c_int32)
 
 SCHEMES = {"godunov": 0, "muscl_evr": 1}
 TOPOS = {"discontinuous": 0, "blending": 1}
+# map_storage_mode -> enum sw2d_result_mode
+RESULT_MODES = {"default": 0, "all": 1, "none": 2}
 FRICTIONS = {"none": 0, "chezy": 1, "manning": 2, "strickler": 3}
 
 
@@ -305,6 +307,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_mlp_adam_step.restype = ctypes.c_int
     lib.sw2d_set_closure.argtypes = [P, P, c_float_p, c_float_p, ctypes.c_float]
     lib.sw2d_set_closure.restype = ctypes.c_int
+    lib.sw2d_result_header.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double]
+    lib.sw2d_result_header.restype = ctypes.c_int
+    lib.sw2d_result_open.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+    lib.sw2d_result_open.restype = ctypes.c_int
+    lib.sw2d_result_close.argtypes = [P]
+    lib.sw2d_result_close.restype = ctypes.c_int
     lib.sw2d_closure_record.argtypes = [P, c_float_p, ctypes.c_int64]
     lib.sw2d_closure_record.restype = ctypes.c_int64
     lib.sw2d_set_t_max.argtypes = [P, ctypes.c_double]
@@ -418,7 +427,8 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_case_read", "sw2d_case_array", "sw2d_case_info", "sw2d_case_option", "sw2d_case_create",
             "sw2d_case_free", "sw2d_case_last_error", "sw2d_mlp_param_count", "sw2d_mlp_create",
             "sw2d_mlp_destroy", "sw2d_mlp_last_error", "sw2d_mlp_get_params", "sw2d_mlp_infer",
-            "sw2d_mlp_loss_grad", "sw2d_mlp_adam_step", "sw2d_set_closure", "sw2d_closure_record", "sw2d_set_t_max", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+            "sw2d_mlp_loss_grad", "sw2d_mlp_adam_step", "sw2d_set_closure", "sw2d_closure_record", "sw2d_set_t_max",
+            "sw2d_result_header", "sw2d_result_open", "sw2d_result_close", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name",

@@ -100,6 +100,7 @@ int sw2d_batch_create(sw2d_handle* const* members, int n_members, sw2d_batch** o
     *out = nullptr;
     for (int i = 0; i < n_members; i++) {
         if (!members[i]) return bfail(b, SW2D_E_ARG, "NULL member handle");
+        if (members[i]->result) return bfail(b, SW2D_E_ARG, "a member has a result file attached");
         if (members[i]->device != members[0]->device)
             return bfail(b, SW2D_E_ARG, "batch members must share one device");
         for (int j = 0; j < i; j++)

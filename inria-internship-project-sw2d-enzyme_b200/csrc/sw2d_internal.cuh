@@ -39,10 +39,11 @@ struct Ctrl {
     unsigned int status;
     unsigned int blocks_done;
     int go;
-    int pad;
+    int store_map;  // DDP: the step ends on a storage time (swDdpHyp.cpp:590-609)
 };
 
-struct DdpCtrl;  // sw2d_ddp.cu
+struct DdpCtrl;       // sw2d_ddp.cu
+struct ResultWriter;  // sw2d_result.cu
 
 struct DevMesh {
     int nc, ni, nb;
@@ -168,6 +169,7 @@ struct sw2d_handle {
     int assim_sqrt_zero = 0;            // option "assim_sqrt_zero"
     int assim_chained = 0;              // option "assim_chained_recompute"
     sw2d::DdpState* ddp = nullptr;      // DDP model: tables, divergence-correction scratch
+    sw2d::ResultWriter* result = nullptr;   // binary map file (sw2d_result_open)
     sw2d::ClosureState* closure = nullptr;  // learned momentum-exchange closure (sw2d_set_closure)
     std::string err;
 };
@@ -302,6 +304,18 @@ int ddp_setup(sw2d_handle* h, const sw2d_mesh* mesh, const sw2d_cell_fields* fie
 void ddp_release(sw2d_handle* h);
 // Validates the DDP arguments before anything is allocated.
 int ddp_check(const sw2d_mesh* mesh, const sw2d_ddp_fields* ddp, std::string& why);
+
+// The binary map file (sw2d_result.cu): the frame kernels after a step, the steps per chunk
+// while a file is attached, the wait for frames in flight, the hand-over of stored frames to
+// the writer thread (stream synchronised), a frame of the current state, whether the run's
+// first frame is stored, the release.
+void result_after_step(sw2d_handle* h);
+int result_chunk(const sw2d_handle* h);
+int result_wait(sw2d_handle* h, long long in_flight);
+int result_drain(sw2d_handle* h);
+int result_force(sw2d_handle* h);
+bool result_started(const sw2d_handle* h);
+void result_release(sw2d_handle* h);
 
 // The learned closure (sw2d_mlp.cu): the DIP cell update with the network at the closure site,
 // the release, and the feature record switch.

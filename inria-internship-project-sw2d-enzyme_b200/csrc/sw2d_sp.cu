@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
         for (int w = 0; w < kBlock / 32; w++)
             if (wmin[w] < dt) dt = wmin[w];
         const double t = ctrl->t;
+        int store = m.dt_map <= -kSmallReal ? 1 : 0;
         if (m.dt_map > kSmallReal) {
             int now, later;
             if (kDdpSnap) {
@@ -335,9 +336,13 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
                 now = (int)(t / m.dt_map);
                 later = (int)((t + dt) / m.dt_map);
             }
-            if (later > now) dt = later * m.dt_map - t;
+            if (later > now) {
+                dt = later * m.dt_map - t;
+                store = 1;
+            }
         }
         if ((t + dt) > ctrl->t_max) dt = ctrl->t_max - t;
+        ctrl->store_map = store;
         ctrl->dt = dt;
         ctrl->go = 1;
         ctrl->blocks_done = 0;
@@ -647,6 +652,7 @@ void launch_phase(sw2d_handle* h, int i)
 void launch_step(sw2d_handle* h)
 {
     for (int i = 0; i < 4; i++) launch_phase(h, i);
+    if (h->result) result_after_step(h);
 }
 
 }  // namespace
@@ -1120,6 +1126,31 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
     CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     const long long before = h->ctrl_host->steps;
+    if (h->result) {
+        // chunks of at most half the frame ring, each drained to the writer thread; before a
+        // chunk, the frames of the chunk before last are on file
+        const int chunk = result_chunk(h);
+        int64_t left = n_steps;
+        while (left > 0) {
+            const int64_t k = std::min<int64_t>(left, chunk);
+            int rc = result_wait(h, chunk);
+            if (rc) return rc;
+            if (k == chunk) {
+                if ((rc = ensure_graph(h, chunk))) return rc;
+                CK(cudaGraphLaunch(h->graph, h->stream));
+            } else {
+                for (int64_t i = 0; i < k; i++) launch_step(h);
+            }
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            if ((rc = result_drain(h))) return rc;
+            left -= k;
+            if (h->ctrl_host->status || h->ctrl_host->steps - before < n_steps - left) break;
+        }
+        if (steps_done) *steps_done = h->ctrl_host->steps - before;
+        return status_to_code(h, h->ctrl_host->status);
+    }
     const int chunk = 32;
     const int64_t full = n_steps / chunk, rem = n_steps % chunk;
     if (full > 0) {
@@ -1138,6 +1169,12 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
 int sw2d_execute(sw2d_handle* h, int64_t* steps_done)
 {
     if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    // with a map file attached: the run's first map (swSp.cpp:504), once
+    if (h->result && !result_started(h)) {
+        CK(cudaSetDevice(h->device));
+        const int rc = result_force(h);
+        if (rc) return rc;
+    }
     // passes of growing length (32 .. 1024 steps): a run that ends after a few steps does not
     // pay for a thousand launches that find the run over
     int64_t total = 0, chunk = 32;
@@ -1151,6 +1188,14 @@ int sw2d_execute(sw2d_handle* h, int64_t* steps_done)
         }
         if (k < chunk) break;
         chunk = std::min<int64_t>(2 * chunk, 1024);
+    }
+    if (h->result) {  // the map after the loop (swSp.cpp:630), then every frame on file
+        int rc = result_force(h);
+        if (!rc) rc = result_wait(h, 0);
+        if (rc) {
+            if (steps_done) *steps_done = total;
+            return rc;
+        }
     }
     if (steps_done) *steps_done = total;
     return SW2D_OK;
@@ -1623,6 +1668,7 @@ int sw2d_destroy(sw2d_handle* h)
     assim_release(h);
     ddp_release(h);
     closure_release(h);
+    result_release(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);

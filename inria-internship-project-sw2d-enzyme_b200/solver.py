@@ -17,12 +17,13 @@ the CUDA library or a GPU the constructor raises.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional, Tuple
 
 import numpy as np
 
 from . import capi
-from .case import Case, read_case
+from .case import Case, read_case, read_solv
 
 
 def _p(a: Optional[np.ndarray]):
@@ -76,9 +77,11 @@ class SpModel:
         return cls(case, device)
 
     @classmethod
-    def load(cls, folder: str, device: int = 0) -> "SpModel":
+    def load(cls, folder: str, device: int = 0, results: bool = False) -> "SpModel":
         """The model a case folder names, read and created by the library itself
-        (sw2d_load_case: the C++ readers of input.solv, geometry.sw2d and the maps)."""
+        (sw2d_load_case: the C++ readers of input.solv, geometry.sw2d and the maps).  With
+        results=True and output_format bin or all, output/ResultHydro.bin is opened with the
+        folder's store_flag (the reference's map_storage_mode), as its init does."""
         self = cls.__new__(cls)
         self.lib = capi.load_library()
         self.case = None
@@ -91,7 +94,25 @@ class SpModel:
             msg = self.lib.sw2d_last_error(None).decode() or self.lib.sw2d_case_last_error().decode()
             raise Sw2dError(st, msg)
         self.handle = handle
+        if results:
+            opts = read_solv(os.path.join(folder, "input", "input.solv"))
+            if str(opts.get("output_format", "all")).lower() in ("bin", "all"):
+                out = os.path.join(folder, "output")
+                os.makedirs(out, exist_ok=True)
+                self.result_open(os.path.join(out, "ResultHydro.bin"), os.path.join(folder, "input", "geometry.sw2d"),
+                                 str(opts.get("store_flag", "default")).lower())
         return self
+
+    def result_open(self, path: str, geometry_path: str, mode: str = "default") -> None:
+        """Creates the binary map file (ResultHydro.bin layout) and attaches it: execute() then
+        appends the run's maps (first, every storage time, last)."""
+        if mode not in capi.RESULT_MODES:
+            raise ValueError(f"map_storage_mode {mode!r}")
+        self._check(self.lib.sw2d_result_open(self.handle, path.encode(), geometry_path.encode(),
+                                              capi.RESULT_MODES[mode]))
+
+    def result_close(self) -> None:
+        self._check(self.lib.sw2d_result_close(self.handle))
 
     def _check(self, st: int) -> None:
         if st != 0:
