@@ -302,6 +302,39 @@ int sw2d_set_t_max(sw2d_handle* h, double t_max);
  * (u64), "bottom_elevation" and the names of map_storage_mode (u64 length + bytes), t_0, t_max,
  * dt_map.  Frame: t, then per cell (caller's numbering) z_b and the mode's values (f64).
  * mode: map_storage_mode default (h, qx, qy, |q|), all (15 values; not for DDP) or none. */
+/* ---- porosity mapper (sw2dPorosityMapper, footprint input) -------------------------------------
+ * The geometry of swPorosityMapperPipeline::cellPorosity / edgePorosity
+ * (src/sw2dPorosityMapper/swPorosityMapperPipeline.cpp:31-90, 256-388) and of the swGeometry
+ * polygon routines they call (src/common/swGeometry.cpp), on the GPU: for every cell
+ * 1 - (area inside building footprints) / area, for every edge 1 - (length inside them) / length,
+ * at each level h of `levels` (a building counts at h when its height exceeds h; with
+ * `height` NULL every building counts at every level, as for SP and DIP).  Outputs are
+ * [element x n_levels].  Cells of up to 8 nodes, buildings of up to 64 vertices. */
+typedef struct sw2d_map_mesh {
+    int64_t cell_nb, node_nb, edge_int_nb, edge_bnd_nb;
+    const double* node_x;
+    const double* node_y;
+    const int64_t* cell_node_offsets; /* [cell_nb + 1] */
+    const int64_t* cell_nodes;        /* node indices of each cell */
+    const double* cell_area;
+    const int64_t* edge_int_nodes;    /* [edge_int_nb x 2] (node_beg, node_end) */
+    const double* edge_int_length;
+    const int64_t* edge_bnd_nodes;    /* [edge_bnd_nb x 2] */
+    const double* edge_bnd_length;
+} sw2d_map_mesh;
+typedef struct sw2d_buildings {
+    int64_t n;
+    const int64_t* offsets; /* [n + 1] into x, y */
+    const double* x;
+    const double* y;
+    const double* height;   /* [n] or NULL */
+} sw2d_buildings;
+/* edge_int_phi / edge_bnd_phi may be NULL (cells only).  Errors: SW2D_E_ARG with the text in
+ * sw2d_map_last_error(). */
+int sw2d_map_porosity(int device, const sw2d_map_mesh* mesh, const sw2d_buildings* buildings, const double* levels,
+                      int n_levels, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi);
+const char* sw2d_map_last_error(void);
+
 enum sw2d_result_mode { SW2D_RESULT_DEFAULT = 0, SW2D_RESULT_ALL = 1, SW2D_RESULT_NONE = 2 };
 /* Writes the header alone (host only; model 0 SP, 1 DIP, 2 DDP). */
 int sw2d_result_header(const char* path, const char* geometry_path, int model, int mode, double t_0, double t_max,

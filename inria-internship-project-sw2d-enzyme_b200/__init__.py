@@ -13,7 +13,7 @@ Modules:
   batch      -- ensembles of independent simulations advanced together (one graph launch)
   autograd   -- torch.autograd bridge to the replayed cost and its adjoint (imported on demand)
 """
-from . import build, case, mesh, workloads, capi, solver, tuning, assimilation, batch, porosity, closure  # noqa: F401
+from . import build, case, mesh, workloads, capi, solver, tuning, assimilation, batch, porosity, closure, porosity_mapper  # noqa: F401
 from .case import Case, read_case, write_case  # noqa: F401
 from .solver import SpModel, Sw2dError  # noqa: F401
 from .batch import Batch  # noqa: F401

@@ -22,6 +22,7 @@ REF_SO = os.path.join(HERE, "_ref", "libsw2d_ref.so")
 REF_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_pm.so")
 REF_BIN = os.path.join(HERE, "_ref", "sw2dSolver")
 REF_BIN_PM = os.path.join(HERE, "_ref", "sw2dSolver_pm")
+REF_MAPPER = os.path.join(HERE, "_ref", "sw2dPorosityMapper")
 REF_E_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e.so")
 REF_E_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e_pm.so")
 REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "/root/reference")
