@@ -70,6 +70,8 @@ def _args():
                     help="cells of the DIP run that times the learned closure")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure line")
     ap.add_argument("--closure-only", action="store_true", help="run only the learned-closure line")
+    ap.add_argument("--closure-no-pipeline", action="store_true",
+                    help="time the closure inside the step only (no data generation, training or judging)")
     ap.add_argument("--assim-cells", type=int, default=1_000_000,
                     help="cells of the porosity-assimilation line (the reference's differentiated step; 0: skip)")
     ap.add_argument("--assim-steps", type=int, default=2000, help="approximate steps of its trajectory")
@@ -590,6 +592,16 @@ def run_closure(pkg, args, local_rank):
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         peak = float(json.load(open(p)).get("bf16_tflops", 0.0)) or None
+    added = clos_ms - base_ms
+    line = {"workload": f"DIP channel at {n} cells (Godunov, Manning, momentum dissipation); the network in place "
+                        f"of the plain closure for every cell",
+            "ms_per_step_plain_closure": base_ms, "ms_per_step_learned_closure": clos_ms,
+            "added_ms_per_step": added, "kernels_per_step": kps,
+            "network_flops_per_step": flops,
+            "tensor_tflops_over_added_time": flops / (added * 1e-3) / 1e12 if added > 0 else None,
+            "bf16_peak_tflops": peak}
+    if args.closure_no_pipeline:
+        return line
     t0 = time.perf_counter()
     lay = {s: C.urban_cases(lx=400.0, ly=200.0, dx_fine=1.0, coarse_factor=8, seed=s) for s in (1, 2, 3, 7, 8)}
     t1 = time.perf_counter()
@@ -600,14 +612,7 @@ def run_closure(pkg, args, local_rank):
           for s in (7, 8) for a, b in ((10.0, 30.0), (20.0, 45.0))}
     t3 = time.perf_counter()
     net.close()
-    added = clos_ms - base_ms
-    return {"workload": f"DIP channel at {n} cells (Godunov, Manning, momentum dissipation); the network in place "
-                        f"of the plain closure for every cell",
-            "ms_per_step_plain_closure": base_ms, "ms_per_step_learned_closure": clos_ms,
-            "added_ms_per_step": added, "kernels_per_step": kps,
-            "network_flops_per_step": flops,
-            "tensor_tflops_over_added_time": flops / (added * 1e-3) / 1e12 if added > 0 else None,
-            "bf16_peak_tflops": peak,
+    return {**line,
             "pipeline": {"layouts": "400 m x 200 m, buildings 5-30 m at 30 % cover, seeds 1-3 train, 7-8 judged",
                          "fine_cells": lay[1][0].mesh.cell_nb, "coarse_cells": lay[1][1].mesh.cell_nb,
                          "samples": n_samples, "tau_s": 16.0,
