@@ -333,6 +333,18 @@ typedef struct sw2d_buildings {
  * sw2d_map_last_error(). */
 int sw2d_map_porosity(int device, const sw2d_map_mesh* mesh, const sw2d_buildings* buildings, const double* levels,
                       int n_levels, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi);
+/* The raster input (swRasterBuildings, src/sw2dPorosityMapper/swRasterBuildings.cpp): building
+ * heights on a grid of pixel centres x [nx] and y [ny], both ascending, height [ny x nx] (row j at
+ * y[j]); a pixel counts at level h when its height exceeds h.  A cell or an edge outside the
+ * raster is an error, as in the reference. */
+typedef struct sw2d_raster {
+    int64_t nx, ny;
+    const double* x;
+    const double* y;
+    const double* height;
+} sw2d_raster;
+int sw2d_map_porosity_raster(int device, const sw2d_map_mesh* mesh, const sw2d_raster* raster, const double* levels,
+                             int n_levels, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi);
 const char* sw2d_map_last_error(void);
 
 enum sw2d_result_mode { SW2D_RESULT_DEFAULT = 0, SW2D_RESULT_ALL = 1, SW2D_RESULT_NONE = 2 };

@@ -314,6 +314,130 @@ __global__ void k_edge_porosity(int ne, const int2* __restrict__ enodes, const d
     out[(size_t)e * nl + l] = 1 - built / len[e];
 }
 
+// ---- raster input (swRasterBuildings, src/sw2dPorosityMapper/swRasterBuildings.cpp): a grid of
+// building heights, pixel centres xc [nx] and yc [ny] ascending, heights b [ny x nx]
+struct Raster {
+    int nx, ny;
+    const double* xc;
+    const double* yc;
+    const double* b;
+    double dx, dy;
+};
+
+// getIndexX / getIndexY (:268-331): the pixel holding x (y); the y test of the first pixel uses
+// yc[1], as the reference does.  Outside the raster (the reference stops) sets `bad`.
+__device__ int index_x(const Raster& r, double x, bool& bad)
+{
+    if (x < r.xc[0] - r.dx / 2 || x > r.xc[r.nx - 1] + r.dx / 2) bad = true;
+    if (x < r.xc[0] + r.dx / 2) return 0;
+    int i = 0;
+    while ((i < r.nx - 1) && (x > r.xc[i + 1] - r.dx / 2)) i++;
+    return i;
+}
+__device__ int index_y(const Raster& r, double y, bool& bad)
+{
+    if (y < r.yc[0] - r.dy / 2 || y > r.yc[r.ny - 1] + r.dy / 2) bad = true;
+    if (y < r.yc[1] + r.dy / 2) return 0;
+    int i = 0;
+    while ((i < r.ny - 1) && (y > r.yc[i + 1] - r.dy / 2)) i++;
+    return i;
+}
+
+// the pixel (i, j) as the reference builds it (corners in the order x-, x+, x-, x+ / y-, y-,
+// y+, y+), sorted
+__device__ void pixel(const Raster& r, int i, int j, double* x, double* y)
+{
+    x[0] = r.xc[i] - r.dx / 2;
+    x[1] = r.xc[i] + r.dx / 2;
+    x[2] = r.xc[i] - r.dx / 2;
+    x[3] = r.xc[i] + r.dx / 2;
+    y[0] = r.yc[j] - r.dy / 2;
+    y[1] = r.yc[j] - r.dy / 2;
+    y[2] = r.yc[j] + r.dy / 2;
+    y[3] = r.yc[j] + r.dy / 2;
+    sort_vertices(x, y, 4);
+}
+
+// cellPorosity, raster branch (:64-87): the pixels of the cell's bounding box taller than h
+__global__ void k_cell_porosity_raster(int nc, const int* __restrict__ coff, const int* __restrict__ cnodes,
+                                       const double* __restrict__ nx, const double* __restrict__ ny,
+                                       const double* __restrict__ area, Raster r, const double* __restrict__ levels,
+                                       int nl, double* out, unsigned* status)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nc * nl) return;
+    const int c = (int)(t / nl), l = (int)(t % nl);
+    const double level = levels[l];
+    const int o = coff[c], n = coff[c + 1] - o;
+    bool overflow = n > kMaxCellVerts || n < 3;
+    double cx[kMaxCellVerts], cy[kMaxCellVerts];
+    double built = 0;
+    if (!overflow) {
+        double x0 = nx[cnodes[o]], y0 = ny[cnodes[o]], x1 = x0, y1 = y0;  // getBoundingBox (:147-181)
+        for (int k = 0; k < n; k++) {
+            cx[k] = nx[cnodes[o + k]];
+            cy[k] = ny[cnodes[o + k]];
+            if (cx[k] < x0) x0 = cx[k];
+            if (cy[k] < y0) y0 = cy[k];
+            if (cx[k] > x1) x1 = cx[k];
+            if (cy[k] > y1) y1 = cy[k];
+        }
+        int i0 = index_x(r, x0, overflow), j0 = index_y(r, y0, overflow);
+        int i1 = index_x(r, x1, overflow) + 1, j1 = index_y(r, y1, overflow) + 1;
+        if (i1 > r.nx - 1) i1 -= 1;
+        if (j1 > r.ny - 1) j1 -= 1;
+        sort_vertices(cx, cy, n);
+        double px[4], py[4];
+        for (int i = i0; i <= i1 && !overflow; i++)
+            for (int j = j0; j <= j1 && !overflow; j++) {
+                if (!(r.b[(size_t)j * r.nx + i] > level)) continue;
+                pixel(r, i, j, px, py);
+                built += intersection_area(cx, cy, n, px, py, 4, overflow);
+            }
+    }
+    if (overflow) atomicOr(status, 1u);
+    out[(size_t)c * nl + l] = 1 - built / area[c];
+}
+
+// edgePorosity, raster branch (:283-318): a pixel side shared by two built pixels along the
+// edge counts half in each
+__global__ void k_edge_porosity_raster(int ne, const int2* __restrict__ enodes, const double* __restrict__ nx,
+                                       const double* __restrict__ ny, const double* __restrict__ len, Raster r,
+                                       const double* __restrict__ levels, int nl, double* out, unsigned* status)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ne * nl) return;
+    const int e = (int)(t / nl), l = (int)(t % nl);
+    const double level = levels[l];
+    const int2 en = enodes[e];
+    const double x0 = nx[en.x], y0 = ny[en.x], x1 = nx[en.y], y1 = ny[en.y];
+    bool overflow = false;
+    // getBoundingBox of an edge (:183-240)
+    const double mnx = dmin(x0, x1), mny = dmin(y0, y1), mxx = dmax(x0, x1), mxy = dmax(y0, y1);
+    const int i0 = index_x(r, mnx, overflow), j0 = index_y(r, mny, overflow);
+    int i1 = index_x(r, mxx, overflow) + 1, j1 = index_y(r, mxy, overflow) + 1;
+    if (mxx == r.xc[0] - r.dx / 2) i1 -= 1;
+    if (mxy == r.yc[0] - r.dy / 2) j1 -= 1;
+    if (i1 > r.nx - 1) i1 -= 1;
+    if (j1 > r.ny - 1) j1 -= 1;
+    const bool horizontal = (y0 == y1) && (y0 == r.yc[j1] - r.dy / 2) && j0 != j1;
+    const bool vertical = (x0 == x1) && (x0 == r.xc[i1] - r.dx / 2) && i0 != i1;
+    double built = 0;
+    double px[4], py[4];
+    for (int i = i0; i <= i1 && !overflow; i++)
+        for (int j = j0; j <= j1 && !overflow; j++) {
+            if (!(r.b[(size_t)j * r.nx + i] > level)) continue;
+            pixel(r, i, j, px, py);
+            double li = length_in_polygon(px, py, 4, x0, y0, x1, y1, overflow);
+            if ((horizontal && (r.b[(size_t)j0 * r.nx + i] > level) && (r.b[(size_t)j1 * r.nx + i] > level)) ||
+                (vertical && (r.b[(size_t)j * r.nx + i0] > level) && (r.b[(size_t)j * r.nx + i1] > level)))
+                li /= 2;
+            built += li;
+        }
+    if (overflow) atomicOr(status, 1u);
+    out[(size_t)e * nl + l] = 1 - built / len[e];
+}
+
 struct DevBuf {
     std::vector<void*> p;
     ~DevBuf()
@@ -342,29 +466,33 @@ int map_fail(int code, const std::string& msg)
     return code;
 }
 
-}  // namespace
+// The mesh on the device and the outputs, shared by both inputs.
+struct MeshDev {
+    DevBuf d;
+    int nc = 0, nl = 0, ni = 0, nb = 0;
+    int *coff = nullptr, *cn = nullptr;
+    int2 *ei = nullptr, *eb = nullptr;
+    double *nx = nullptr, *ny = nullptr, *area = nullptr, *il = nullptr, *bl = nullptr, *lev = nullptr;
+    double *cell = nullptr, *eint = nullptr, *ebnd = nullptr;
+    unsigned* status = nullptr;
+};
 
-extern "C" {
-
-const char* sw2d_map_last_error(void) { return g_map_error.c_str(); }
-
-int sw2d_map_porosity(int device, const sw2d_map_mesh* mesh, const sw2d_buildings* blds, const double* levels,
-                      int n_levels, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi)
+int mesh_setup(int device, const sw2d_map_mesh* mesh, const double* levels, int n_levels, bool want_int,
+               bool want_bnd, MeshDev& md)
 {
-    g_map_error.clear();
-    if (!mesh || !blds || !levels || n_levels < 1 || !cell_phi) return map_fail(SW2D_E_ARG, "invalid arguments");
-    if (mesh->cell_nb <= 0 || mesh->node_nb <= 0 || mesh->cell_nb >= (1LL << 30) || mesh->node_nb >= (1LL << 31))
+    if (!mesh || !levels || n_levels < 1) return map_fail(SW2D_E_ARG, "invalid arguments");
+    if (mesh->cell_nb <= 0 || mesh->node_nb <= 0 || mesh->cell_nb >= (1LL << 30) || mesh->node_nb >= (1LL << 31) ||
+        mesh->edge_int_nb < 0 || mesh->edge_bnd_nb < 0 || mesh->edge_int_nb >= (1LL << 30) ||
+        mesh->edge_bnd_nb >= (1LL << 30))
         return map_fail(SW2D_E_ARG, "mesh sizes");
     if (!mesh->node_x || !mesh->node_y || !mesh->cell_node_offsets || !mesh->cell_nodes || !mesh->cell_area)
         return map_fail(SW2D_E_ARG, "mesh arrays missing");
-    if ((edge_int_phi && (!mesh->edge_int_nodes || !mesh->edge_int_length)) ||
-        (edge_bnd_phi && (!mesh->edge_bnd_nodes || !mesh->edge_bnd_length)))
+    if ((want_int && (!mesh->edge_int_nodes || !mesh->edge_int_length)) ||
+        (want_bnd && (!mesh->edge_bnd_nodes || !mesh->edge_bnd_length)))
         return map_fail(SW2D_E_ARG, "edge arrays missing");
-    if (blds->n < 0 || (blds->n > 0 && (!blds->offsets || !blds->x || !blds->y)))
-        return map_fail(SW2D_E_ARG, "building arrays missing");
-    const int64_t nc = mesh->cell_nb, nn = mesh->node_nb, nl = n_levels;
+    const int64_t nc = mesh->cell_nb, nn = mesh->node_nb;
     // host-side checks and conversions: offsets and node indices in range
-    std::vector<int> coff(nc + 1), cn((size_t)mesh->cell_node_offsets[nc]);
+    std::vector<int> coff(nc + 1), cn((size_t)std::max<int64_t>(0, mesh->cell_node_offsets[nc]));
     for (int64_t c = 0; c <= nc; c++) {
         const int64_t v = mesh->cell_node_offsets[c];
         if (v < 0 || (c > 0 && v < mesh->cell_node_offsets[c - 1])) return map_fail(SW2D_E_ARG, "cell node offsets");
@@ -384,14 +512,75 @@ int sw2d_map_porosity(int device, const sw2d_map_mesh* mesh, const sw2d_building
         return true;
     };
     std::vector<int2> ei, eb;
-    if (edge_int_phi && !edges(mesh->edge_int_nb, mesh->edge_int_nodes, ei))
+    if (want_int && !edges(mesh->edge_int_nb, mesh->edge_int_nodes, ei))
         return map_fail(SW2D_E_ARG, "internal edge node index out of range");
-    if (edge_bnd_phi && !edges(mesh->edge_bnd_nb, mesh->edge_bnd_nodes, eb))
+    if (want_bnd && !edges(mesh->edge_bnd_nb, mesh->edge_bnd_nodes, eb))
         return map_fail(SW2D_E_ARG, "boundary edge node index out of range");
+    if (cudaSetDevice(device) != cudaSuccess) return map_fail(SW2D_E_NO_DEVICE, "cudaSetDevice failed");
+    md.nc = (int)nc;
+    md.nl = n_levels;
+    md.ni = want_int ? (int)mesh->edge_int_nb : 0;
+    md.nb = want_bnd ? (int)mesh->edge_bnd_nb : 0;
+    DevBuf& d = md.d;
+    cudaError_t e = d.up(coff.data(), coff.size(), &md.coff);
+    if (e == cudaSuccess) e = d.up(cn.data(), cn.size(), &md.cn);
+    if (e == cudaSuccess) e = d.up(mesh->node_x, (size_t)nn, &md.nx);
+    if (e == cudaSuccess) e = d.up(mesh->node_y, (size_t)nn, &md.ny);
+    if (e == cudaSuccess) e = d.up(mesh->cell_area, (size_t)nc, &md.area);
+    if (e == cudaSuccess) e = d.up(levels, (size_t)n_levels, &md.lev);
+    if (e == cudaSuccess) e = d.up((const double*)nullptr, (size_t)nc * n_levels, &md.cell);
+    if (e == cudaSuccess) e = d.up((const unsigned*)nullptr, 1, &md.status);
+    if (e == cudaSuccess && want_int) {
+        e = d.up(ei.data(), ei.size(), &md.ei);
+        if (e == cudaSuccess) e = d.up(mesh->edge_int_length, (size_t)mesh->edge_int_nb, &md.il);
+        if (e == cudaSuccess) e = d.up((const double*)nullptr, (size_t)mesh->edge_int_nb * n_levels, &md.eint);
+    }
+    if (e == cudaSuccess && want_bnd) {
+        e = d.up(eb.data(), eb.size(), &md.eb);
+        if (e == cudaSuccess) e = d.up(mesh->edge_bnd_length, (size_t)mesh->edge_bnd_nb, &md.bl);
+        if (e == cudaSuccess) e = d.up((const double*)nullptr, (size_t)mesh->edge_bnd_nb * n_levels, &md.ebnd);
+    }
+    if (e != cudaSuccess) return map_fail(SW2D_E_CUDA, std::string("mapper buffers: ") + cudaGetErrorString(e));
+    return SW2D_OK;
+}
+
+int mesh_finish(MeshDev& md, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi, const char* limits)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    unsigned st = 0;
+    const size_t nl = (size_t)md.nl;
+    if (e == cudaSuccess) e = cudaMemcpy(&st, md.status, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(cell_phi, md.cell, (size_t)md.nc * nl * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && md.eint && md.ni > 0)
+        e = cudaMemcpy(edge_int_phi, md.eint, (size_t)md.ni * nl * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && md.ebnd && md.nb > 0)
+        e = cudaMemcpy(edge_bnd_phi, md.ebnd, (size_t)md.nb * nl * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return map_fail(SW2D_E_CUDA, std::string("mapper kernels: ") + cudaGetErrorString(e));
+    if (st) return map_fail(SW2D_E_ARG, limits);
+    return SW2D_OK;
+}
+
+constexpr int kMapBlock = 128;
+unsigned map_blocks(int64_t n) { return (unsigned)((n + kMapBlock - 1) / kMapBlock); }
+
+}  // namespace
+
+extern "C" {
+
+const char* sw2d_map_last_error(void) { return g_map_error.c_str(); }
+
+int sw2d_map_porosity(int device, const sw2d_map_mesh* mesh, const sw2d_buildings* blds, const double* levels,
+                      int n_levels, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi)
+{
+    g_map_error.clear();
+    if (!blds || !cell_phi) return map_fail(SW2D_E_ARG, "invalid arguments");
+    if (blds->n < 0 || (blds->n > 0 && (!blds->offsets || !blds->x || !blds->y)))
+        return map_fail(SW2D_E_ARG, "building arrays missing");
     const int64_t nb = blds->n;
     std::vector<int> boff(nb + 1);
     std::vector<double4> bbox(nb);
-    for (int64_t k = 0; k <= nb; k++) boff[k] = (int)blds->offsets[k];
+    for (int64_t k = 0; k <= nb; k++) boff[k] = nb ? (int)blds->offsets[k] : 0;
     for (int64_t k = 0; k < nb; k++) {
         const int64_t o = blds->offsets[k], e = blds->offsets[k + 1];
         if (e - o < 1 || e - o > kMaxBldVerts) return map_fail(SW2D_E_ARG, "a building has 0 or more than 64 vertices");
@@ -401,63 +590,61 @@ int sw2d_map_porosity(int device, const sw2d_map_mesh* mesh, const sw2d_building
                              std::max(b.w, blds->y[i]));
         bbox[k] = b;
     }
-    if (cudaSetDevice(device) != cudaSuccess) return map_fail(SW2D_E_NO_DEVICE, "cudaSetDevice failed");
-    DevBuf d;
-    int *d_coff = nullptr, *d_cn = nullptr, *d_boff = nullptr;
-    int2 *d_ei = nullptr, *d_eb = nullptr;
-    double *d_nx = nullptr, *d_ny = nullptr, *d_area = nullptr, *d_bx = nullptr, *d_by = nullptr, *d_bh = nullptr;
-    double *d_lev = nullptr, *d_il = nullptr, *d_bl = nullptr, *d_cell = nullptr, *d_int = nullptr, *d_bnd = nullptr;
+    MeshDev md;
+    int rc = mesh_setup(device, mesh, levels, n_levels, edge_int_phi != nullptr, edge_bnd_phi != nullptr, md);
+    if (rc) return rc;
+    int* d_boff = nullptr;
+    double *d_bx = nullptr, *d_by = nullptr, *d_bh = nullptr;
     double4* d_bb = nullptr;
-    unsigned* d_status = nullptr;
     const size_t nbv = nb ? (size_t)blds->offsets[nb] : 0;
-    cudaError_t e = d.up(coff.data(), coff.size(), &d_coff);
-    if (e == cudaSuccess) e = d.up(cn.data(), cn.size(), &d_cn);
-    if (e == cudaSuccess) e = d.up(mesh->node_x, (size_t)nn, &d_nx);
-    if (e == cudaSuccess) e = d.up(mesh->node_y, (size_t)nn, &d_ny);
-    if (e == cudaSuccess) e = d.up(mesh->cell_area, (size_t)nc, &d_area);
-    if (e == cudaSuccess) e = d.up(boff.data(), boff.size(), &d_boff);
-    if (e == cudaSuccess) e = d.up(blds->x, nbv, &d_bx);
-    if (e == cudaSuccess) e = d.up(blds->y, nbv, &d_by);
-    if (e == cudaSuccess && blds->height) e = d.up(blds->height, (size_t)nb, &d_bh);
-    if (e == cudaSuccess) e = d.up(bbox.data(), bbox.size(), &d_bb);
-    if (e == cudaSuccess) e = d.up(levels, (size_t)nl, &d_lev);
-    if (e == cudaSuccess) e = d.up((const double*)nullptr, (size_t)nc * nl, &d_cell);
-    if (e == cudaSuccess) e = d.up((const unsigned*)nullptr, 1, &d_status);
-    if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(unsigned));
-    if (e == cudaSuccess && edge_int_phi) {
-        e = d.up(ei.data(), ei.size(), &d_ei);
-        if (e == cudaSuccess) e = d.up(mesh->edge_int_length, (size_t)mesh->edge_int_nb, &d_il);
-        if (e == cudaSuccess) e = d.up((const double*)nullptr, (size_t)mesh->edge_int_nb * nl, &d_int);
-    }
-    if (e == cudaSuccess && edge_bnd_phi) {
-        e = d.up(eb.data(), eb.size(), &d_eb);
-        if (e == cudaSuccess) e = d.up(mesh->edge_bnd_length, (size_t)mesh->edge_bnd_nb, &d_bl);
-        if (e == cudaSuccess) e = d.up((const double*)nullptr, (size_t)mesh->edge_bnd_nb * nl, &d_bnd);
-    }
+    cudaError_t e = md.d.up(boff.data(), boff.size(), &d_boff);
+    if (e == cudaSuccess) e = md.d.up(blds->x, nbv, &d_bx);
+    if (e == cudaSuccess) e = md.d.up(blds->y, nbv, &d_by);
+    if (e == cudaSuccess && blds->height) e = md.d.up(blds->height, (size_t)nb, &d_bh);
+    if (e == cudaSuccess) e = md.d.up(bbox.data(), bbox.size(), &d_bb);
     if (e != cudaSuccess) return map_fail(SW2D_E_CUDA, std::string("mapper buffers: ") + cudaGetErrorString(e));
     Blds b{(int)nb, d_boff, d_bx, d_by, d_bh, d_bb};
-    const int T = 128;
-    auto blocks = [&](int64_t n) { return (unsigned)((n + T - 1) / T); };
-    k_cell_porosity<<<blocks(nc * nl), T>>>((int)nc, d_coff, d_cn, d_nx, d_ny, d_area, b, d_lev, (int)nl, d_cell,
-                                            d_status);
-    if (edge_int_phi && mesh->edge_int_nb > 0)
-        k_edge_porosity<<<blocks(mesh->edge_int_nb * nl), T>>>((int)mesh->edge_int_nb, d_ei, d_nx, d_ny, d_il, b, d_lev,
-                                                               (int)nl, d_int, d_status);
-    if (edge_bnd_phi && mesh->edge_bnd_nb > 0)
-        k_edge_porosity<<<blocks(mesh->edge_bnd_nb * nl), T>>>((int)mesh->edge_bnd_nb, d_eb, d_nx, d_ny, d_bl, b, d_lev,
-                                                               (int)nl, d_bnd, d_status);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    unsigned st = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&st, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(cell_phi, d_cell, (size_t)nc * nl * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && edge_int_phi && mesh->edge_int_nb > 0)
-        e = cudaMemcpy(edge_int_phi, d_int, (size_t)mesh->edge_int_nb * nl * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && edge_bnd_phi && mesh->edge_bnd_nb > 0)
-        e = cudaMemcpy(edge_bnd_phi, d_bnd, (size_t)mesh->edge_bnd_nb * nl * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return map_fail(SW2D_E_CUDA, std::string("mapper kernels: ") + cudaGetErrorString(e));
-    if (st) return map_fail(SW2D_E_ARG, "a cell with more than 8 nodes or an intersection of more than 96 points");
-    return SW2D_OK;
+    k_cell_porosity<<<map_blocks((int64_t)md.nc * md.nl), kMapBlock>>>(md.nc, md.coff, md.cn, md.nx, md.ny, md.area, b,
+                                                                      md.lev, md.nl, md.cell, md.status);
+    if (md.ni > 0)
+        k_edge_porosity<<<map_blocks((int64_t)md.ni * md.nl), kMapBlock>>>(md.ni, md.ei, md.nx, md.ny, md.il, b, md.lev,
+                                                                          md.nl, md.eint, md.status);
+    if (md.nb > 0)
+        k_edge_porosity<<<map_blocks((int64_t)md.nb * md.nl), kMapBlock>>>(md.nb, md.eb, md.nx, md.ny, md.bl, b, md.lev,
+                                                                          md.nl, md.ebnd, md.status);
+    return mesh_finish(md, cell_phi, edge_int_phi, edge_bnd_phi,
+                       "a cell with more than 8 nodes or an intersection of more than 96 points");
+}
+
+int sw2d_map_porosity_raster(int device, const sw2d_map_mesh* mesh, const sw2d_raster* raster, const double* levels,
+                             int n_levels, double* cell_phi, double* edge_int_phi, double* edge_bnd_phi)
+{
+    g_map_error.clear();
+    if (!raster || !cell_phi || !raster->x || !raster->y || !raster->height)
+        return map_fail(SW2D_E_ARG, "invalid arguments");
+    if (raster->nx < 2 || raster->ny < 2 || raster->nx * raster->ny >= (1LL << 31))
+        return map_fail(SW2D_E_ARG, "the raster needs at least 2 x 2 pixels");
+    MeshDev md;
+    int rc = mesh_setup(device, mesh, levels, n_levels, edge_int_phi != nullptr, edge_bnd_phi != nullptr, md);
+    if (rc) return rc;
+    double *d_x = nullptr, *d_y = nullptr, *d_b = nullptr;
+    cudaError_t e = md.d.up(raster->x, (size_t)raster->nx, &d_x);
+    if (e == cudaSuccess) e = md.d.up(raster->y, (size_t)raster->ny, &d_y);
+    if (e == cudaSuccess) e = md.d.up(raster->height, (size_t)(raster->nx * raster->ny), &d_b);
+    if (e != cudaSuccess) return map_fail(SW2D_E_CUDA, std::string("mapper buffers: ") + cudaGetErrorString(e));
+    // swRasterBuildings::build (:124-125): the pixel sizes from the first two centres
+    Raster r{(int)raster->nx, (int)raster->ny, d_x, d_y, d_b, raster->x[1] - raster->x[0], raster->y[1] - raster->y[0]};
+    k_cell_porosity_raster<<<map_blocks((int64_t)md.nc * md.nl), kMapBlock>>>(md.nc, md.coff, md.cn, md.nx, md.ny,
+                                                                             md.area, r, md.lev, md.nl, md.cell,
+                                                                             md.status);
+    if (md.ni > 0)
+        k_edge_porosity_raster<<<map_blocks((int64_t)md.ni * md.nl), kMapBlock>>>(md.ni, md.ei, md.nx, md.ny, md.il, r,
+                                                                                 md.lev, md.nl, md.eint, md.status);
+    if (md.nb > 0)
+        k_edge_porosity_raster<<<map_blocks((int64_t)md.nb * md.nl), kMapBlock>>>(md.nb, md.eb, md.nx, md.ny, md.bl, r,
+                                                                                 md.lev, md.nl, md.ebnd, md.status);
+    return mesh_finish(md, cell_phi, edge_int_phi, edge_bnd_phi,
+                       "a cell with more than 8 nodes, or a cell or an edge outside the raster");
 }
 
 }  // extern "C"

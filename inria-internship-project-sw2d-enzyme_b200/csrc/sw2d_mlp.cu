@@ -1,6 +1,8 @@
 // sw2d_mlp.cu — the learned momentum-exchange closure: an MLP of 10 inputs -> 64 -> 64 -> 2
 // (GELU) whose inference and training run on the 5th-generation tensor cores (tcgen05, BF16
-// operands, FP32 accumulators in TMEM) through one hand-written GEMM kernel.
+// operands, FP32 accumulators in TMEM): one hand-written GEMM kernel for training and
+// stand-alone inference, and the DIP cell-update kernel with the network inside
+// (k_update_closure, further down) for the closure in a model's step.
 //
 // k_umma_gemm computes, for a tile of 128 rows per CTA, D = A * B^T with A [M x K] and B [N x K]
 // (bf16, row-major, K contiguous), K looped in chunks of 64 through shared memory (K-major

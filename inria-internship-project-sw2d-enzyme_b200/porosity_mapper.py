@@ -1,9 +1,10 @@
-"""The porosity mapper (the reference's sw2dPorosityMapper, footprint input) with its geometry on
-the GPU (C ABI sw2d_map_porosity).
+"""The porosity mapper (the reference's sw2dPorosityMapper, footprint and raster inputs) with its
+geometry on the GPU (C ABI sw2d_map_porosity, sw2d_map_porosity_raster).
 
 ``map_folder(folder)`` does what the reference's mapper program does on a case folder: it reads
-``primary_files/input.pmap`` (model sp / dip / ddp, input footprint),
-``primary_files/buildings.txt`` and ``input/geometry.sw2d``, computes the storage porosity of
+``primary_files/input.pmap`` (model sp / dip / ddp, input footprint or raster),
+``primary_files/buildings.txt`` (footprints, or a raster of building heights) and
+``input/geometry.sw2d``, computes the storage porosity of
 every cell and the connectivity porosity of every edge, and writes the model's porosity maps
 into ``input/`` in the reference's text layout (swPorosityMapperPipeline::writeSp / writeDip /
 writeDdp, src/sw2dPorosityMapper/swPorosityMapperPipeline.cpp:537-822; numbers as an
@@ -28,6 +29,11 @@ class _MapMesh(ctypes.Structure):
                 ("cell_area", ctypes.c_void_p), ("edge_int_nodes", ctypes.c_void_p),
                 ("edge_int_length", ctypes.c_void_p), ("edge_bnd_nodes", ctypes.c_void_p),
                 ("edge_bnd_length", ctypes.c_void_p)]
+
+
+class _Raster(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p),
+                ("height", ctypes.c_void_p)]
 
 
 class _Buildings(ctypes.Structure):
@@ -78,6 +84,46 @@ def write_buildings(path: str, xs, ys, heights=None) -> None:
         fh.write("x y ... -height\n" + "\n".join(rows))
 
 
+def read_raster(path: str) -> Tuple[np.ndarray, np.ndarray, np.ndarray, List[float]]:
+    """A building raster as swRasterBuildings::build reads it (:35-128): a header line, then one
+    pixel per line, x y height, row by row from the top (y descending, x ascending within a
+    row).  Returns (x centres, y centres ascending, heights [ny x nx], the distinct heights
+    ascending).  As with the reference's reader, a last line without a newline is not read."""
+    with open(path) as fh:
+        text = fh.read()
+    # after the header; the last element of the split is empty after a final newline, or the
+    # last line, which the reference's loop reads at end of file and does not use
+    lines = text.split("\n")[1:-1]
+    rows, xs, ys = [], [], []
+    y0 = None
+    for ln in lines:
+        x, y, b = (float(t) for t in ln.split()[:3])
+        if y0 is None:
+            y0 = y
+            rows.append([b])
+            xs.append(x)
+            ys.append(y)
+        elif y != ys[-1]:
+            rows.append([b])
+            ys.append(y)
+        else:
+            rows[-1].append(b)
+            if y == y0:
+                xs.append(x)
+    heights = np.array(rows[::-1], dtype=np.float64)
+    topo = sorted(set(float(v) for v in heights.reshape(-1)))
+    return np.array(xs), np.array(ys[::-1]), heights, topo
+
+
+def write_raster(path: str, x: np.ndarray, y: np.ndarray, heights: np.ndarray) -> None:
+    """A building raster for the reference mapper (top row first), ending with a newline."""
+    out = ["x y height"]
+    for j in range(len(y) - 1, -1, -1):
+        out.extend(f"{float(x[i])!r} {float(y[j])!r} {float(heights[j, i])!r}" for i in range(len(x)))
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+
+
 def _cell_nodes(mesh) -> Tuple[np.ndarray, np.ndarray]:
     flat = None if mesh.cell_nodes_flat is None else np.asarray(mesh.cell_nodes_flat, dtype=np.int64)
     if flat is not None and flat.ndim == 2:  # one node count for every cell
@@ -121,6 +167,37 @@ def map_porosity(mesh, xs, ys, heights, levels, device: int = 0, edges: bool = T
                                nl, dp(cell), dp(eint), dp(ebnd))
     if st != 0:
         raise RuntimeError(f"sw2d_map_porosity failed ({st}): {lib.sw2d_map_last_error().decode()}")
+    return {"cell": cell, "edge_int": eint, "edge_bnd": ebnd, "levels": lev}
+
+
+def map_porosity_raster(mesh, x, y, heights, levels, device: int = 0, edges: bool = True) -> Dict[str, np.ndarray]:
+    """Porosities [element x level] from a building raster (pixel centres x, y ascending,
+    heights [ny x nx])."""
+    lib = capi.load_library()
+    off, cn = _cell_nodes(mesh)
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    nl = len(levels)
+    nc, ni, nb = mesh.cell_nb, mesh.edge_int_nb, mesh.edge_bnd_nb
+    mm = _MapMesh(nc, int(np.asarray(mesh.node_x).size), ni, nb, arr(mesh.node_x, np.float64),
+                  arr(mesh.node_y, np.float64), arr(off, np.int64), arr(cn, np.int64), arr(mesh.cell_area, np.float64),
+                  arr(mesh.edge_int_nodes, np.int64), arr(mesh.edge_int_length, np.float64),
+                  arr(mesh.edge_bnd_nodes, np.int64), arr(mesh.edge_bnd_length, np.float64))
+    ra = _Raster(len(x), len(y), arr(x, np.float64), arr(y, np.float64), arr(heights, np.float64))
+    lev = np.ascontiguousarray(levels, dtype=np.float64)
+    cell = np.empty((nc, nl))
+    eint = np.empty((ni, nl)) if edges else None
+    ebnd = np.empty((nb, nl)) if edges else None
+    dp = lambda a: a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+    st = lib.sw2d_map_porosity_raster(int(device), ctypes.byref(mm), ctypes.byref(ra),
+                                      lev.ctypes.data_as(ctypes.c_void_p), nl, dp(cell), dp(eint), dp(ebnd))
+    if st != 0:
+        raise RuntimeError(f"sw2d_map_porosity_raster failed ({st}): {lib.sw2d_map_last_error().decode()}")
     return {"cell": cell, "edge_int": eint, "edge_bnd": ebnd, "levels": lev}
 
 
@@ -186,10 +263,16 @@ def map_folder(folder: str, device: int = 0) -> Dict[str, np.ndarray]:
     model, kind = prm.get("model"), prm.get("input")
     if model not in ("sp", "dip", "ddp"):
         raise ValueError(f"model {model!r}")
-    if kind != "footprint":
-        raise NotImplementedError("the raster input of the mapper is not built; footprint only")
-    xs, ys, heights, topo = read_buildings(os.path.join(folder, "primary_files", "buildings.txt"))
+    if kind not in ("footprint", "raster"):
+        raise ValueError(f"input {kind!r}")
     mesh = read_geometry(os.path.join(folder, "input", "geometry.sw2d"))
+    if kind == "raster":
+        x, y, hgt, topo = read_raster(os.path.join(folder, "primary_files", "buildings.txt"))
+        levels = topo if model == "ddp" else [0.0]
+        res = map_porosity_raster(mesh, x, y, hgt, levels, device, edges=(model != "sp"))
+        write_maps(folder, model, res, topo)
+        return res
+    xs, ys, heights, topo = read_buildings(os.path.join(folder, "primary_files", "buildings.txt"))
     if model == "ddp":
         if heights is None:
             raise ValueError("the DDP mapping needs a height for every building")

@@ -1,7 +1,8 @@
 """The porosity mapper on the GPU (porosity_mapper.map_folder over sw2d_map_porosity) against
 the reference's mapper program on the same case folder: every map file byte for byte (values
 printed with 6 significant digits, as the reference prints them), for SP, DIP and DDP, on
-hand-placed footprints and on a seeded building layout; and the arrays against the reference's
+hand-placed footprints, on a seeded building layout and on a raster of block buildings; and the
+arrays against the reference's
 values to 5e-6."""
 import os
 import shutil
@@ -11,19 +12,22 @@ import numpy as np
 import pytest
 
 from tests.conftest import load_pkg
-from tests.test_mapper import FILES, _values, mapper_case, needs_mapper, run_reference_mapper
+from tests.test_mapper import FILES, _values, mapper_case, needs_mapper, raster_case, run_reference_mapper
 
 pytestmark = pytest.mark.gpu
 PKG = load_pkg()
 
 
 @needs_mapper
-@pytest.mark.parametrize("urban", [False, True], ids=["footprints", "layout"])
+@pytest.mark.parametrize("urban", [False, True, "raster"], ids=["footprints", "layout", "raster"])
 @pytest.mark.parametrize("model", ["sp", "dip", "ddp"])
 def test_maps_equal_the_reference_mappers(tmp_path, model, urban):
     PKG.build.build()
     ref_folder = str(tmp_path / "ref")
-    mapper_case(ref_folder, model, n_cells=6000 if urban else 900, urban=urban)
+    if urban == "raster":
+        raster_case(ref_folder, model)
+    else:
+        mapper_case(ref_folder, model, n_cells=6000 if urban else 900, urban=urban)
     t0 = time.perf_counter()
     ref = run_reference_mapper(ref_folder)
     t_ref = time.perf_counter() - t0

@@ -22,6 +22,28 @@ FILES = {"sp": ["SP_cell_porosity_map.txt"],
          "ddp": ["DDP_cell_porosity_map.txt", "DDP_edge_bnd_porosity_map.txt", "DDP_edge_int_porosity_map.txt"]}
 
 
+def raster_case(folder, model, seed=5):
+    """The dam-break channel (100 m x 20 m) under a 1 m raster of block buildings of heights 0, 3
+    and 6 m (blocks of 2-6 pixels), with the raster input."""
+    case = PKG.workloads.dam_break(n_cells=900, seed_mesh=seed, seed_phi=seed + 1)
+    x = np.arange(100) + 0.5
+    y = np.arange(20) + 0.5
+    rng = np.random.default_rng(seed)
+    hgt = np.zeros((20, 100))
+    for _ in range(40):
+        i, j = rng.integers(0, 96), rng.integers(0, 17)
+        hgt[j:j + rng.integers(2, 5), i:i + rng.integers(2, 7)] = rng.choice([3.0, 6.0])
+    PKG.write_case(folder, case)
+    for fn in os.listdir(os.path.join(folder, "input")):
+        if fn.endswith("porosity_map.txt"):
+            os.remove(os.path.join(folder, "input", fn))
+    os.makedirs(os.path.join(folder, "primary_files"), exist_ok=True)
+    M.write_raster(os.path.join(folder, "primary_files", "buildings.txt"), x, y, hgt)
+    with open(os.path.join(folder, "primary_files", "input.pmap"), "w") as fh:
+        fh.write(f"model {model}\ninput raster\n")
+    return case, x, y, hgt
+
+
 def mapper_case(folder, model, n_cells=900, seed=31, urban=False):
     """A case folder with buildings: three hand-placed footprints (rectangles and a triangle,
     one across many cells) on the dam-break channel, or (urban=True) a seeded building layout."""
@@ -79,11 +101,19 @@ def test_buildings_reader(tmp_path):
     assert topo == [0.0, 3.0, 4.5, 6.0]
 
 
+def test_raster_reader(tmp_path):
+    _, x, y, hgt = raster_case(str(tmp_path / "c"), "ddp")
+    rx, ry, rh, topo = M.read_raster(str(tmp_path / "c" / "primary_files" / "buildings.txt"))
+    assert np.array_equal(rx, x) and np.array_equal(ry, y) and np.array_equal(rh, hgt)
+    assert topo == [0.0, 3.0, 6.0]
+
+
 @needs_mapper
+@pytest.mark.parametrize("raster", [False, True], ids=["footprint", "raster"])
 @pytest.mark.parametrize("model", ["sp", "dip", "ddp"])
-def test_writer_reproduces_the_reference_files(tmp_path, model):
+def test_writer_reproduces_the_reference_files(tmp_path, model, raster):
     folder = str(tmp_path / "c")
-    mapper_case(folder, model)
+    (raster_case if raster else mapper_case)(folder, model)
     ref = run_reference_mapper(folder)
     assert sorted(ref) == sorted(FILES[model])
     ddp = model == "ddp"
@@ -92,7 +122,7 @@ def test_writer_reproduces_the_reference_files(tmp_path, model):
         res[key], t = _values(ref[fn], ddp)
         topo = t or topo
     if ddp:
-        assert topo == [0.0, 3.0, 4.5, 6.0]
+        assert topo == ([0.0, 3.0, 6.0] if raster else [0.0, 3.0, 4.5, 6.0])
     out = str(tmp_path / "o")
     os.makedirs(os.path.join(out, "input"))
     M.write_maps(out, model, res, topo)
