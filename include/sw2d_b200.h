@@ -301,7 +301,7 @@ int sw2d_set_t_max(sw2d_handle* h, double t_max);
  * Header: the geometry file's part from its start to the node-to-cell lists, the variable count
  * (u64), "bottom_elevation" and the names of map_storage_mode (u64 length + bytes), t_0, t_max,
  * dt_map.  Frame: t, then per cell (caller's numbering) z_b and the mode's values (f64).
- * mode: map_storage_mode default (h, qx, qy, |q|), all (15 values; not for DDP) or none. */
+ * mode: map_storage_mode default (h, qx, qy, |q|), all (15 values) or none. */
 /* ---- porosity mapper (sw2dPorosityMapper, footprint input) -------------------------------------
  * The geometry of swPorosityMapperPipeline::cellPorosity / edgePorosity
  * (src/sw2dPorosityMapper/swPorosityMapperPipeline.cpp:31-90, 256-388) and of the swGeometry

@@ -89,6 +89,24 @@ __device__ __forceinline__ void frame_values(const DevMesh& m, int c, int mode, 
         v[2] = u * h;
         v[3] = w * h;
         v[4] = h * sqrt(u * u + w * w);
+        if (mode == SW2D_RESULT_ALL) {  // swDdp.cpp:2500-2530
+            const double z = s.w;
+            const double vn = sqrt(u * u + w * w);
+            unsigned bad = 0;
+            const int o = m.ctoff[c], n = m.ctoff[c + 1] - o;
+            const double phi = ddp::phi_theta(m.ctab + o, n, z, bad).phi;  // phiWOfZ
+            v[5] = z;
+            v[6] = u;
+            v[7] = w;
+            v[8] = vn;
+            v[9] = vn / ddp::celerity(s.x, phi);
+            v[10] = h + 0.5 * vn * vn / kGravity;
+            v[11] = z + 0.5 * vn * vn / kGravity;
+            v[12] = s.x;
+            v[13] = u * s.x;
+            v[14] = w * s.x;
+            v[15] = vn * s.x;
+        }
         return;
     }
     const double h = s.x, qx = s.y, qy = s.z, zb = cs.x;
@@ -192,8 +210,13 @@ const std::vector<std::string>& var_names(int model, int mode)
                                                  "phi_by_unit_discharge_y", "phi_by_unit_discharge_norm"};
     static const std::vector<std::string> ddp_def = {"water_depth", "unit_discharge_x", "unit_discharge_y",
                                                      "unit_disch_norm"};
+    static const std::vector<std::string> ddp_all = {"water_depth", "unit_discharge_x", "unit_discharge_y",
+                                                     "unit_disc_norm", "surface_elevation", "velocity_x",
+                                                     "velocity_y", "velocity_norm", "froude", "specific_head",
+                                                     "total_head", "phi_by_wat_depth", "phi_by_disc_x",
+                                                     "phi_by_disc_y", "phi_by_disc_norm"};
     if (mode == SW2D_RESULT_NONE) return none;
-    if (model == kModelDdp) return ddp_def;
+    if (model == kModelDdp) return mode == SW2D_RESULT_ALL ? ddp_all : ddp_def;
     return mode == SW2D_RESULT_ALL ? all : def;
 }
 
@@ -417,7 +440,6 @@ int sw2d_result_header(const char* path, const char* geometry_path, int model, i
                        double dt_map)
 {
     if (!path || !geometry_path || model < 0 || model > 2 || mode < 0 || mode > 2) return SW2D_E_ARG;
-    if (model == kModelDdp && mode == SW2D_RESULT_ALL) return SW2D_E_UNSUPPORTED;
     std::string why;
     return write_header(path, geometry_path, model, mode, t_0, t_max, dt_map, why, nullptr);
 }
@@ -426,8 +448,6 @@ int sw2d_result_open(sw2d_handle* h, const char* path, const char* geometry_path
 {
     if (!h) return SW2D_E_ARG;
     if (!path || !geometry_path || mode < 0 || mode > 2) return fail(h, SW2D_E_ARG, "invalid arguments");
-    if (h->model == kModelDdp && mode == SW2D_RESULT_ALL)
-        return fail(h, SW2D_E_UNSUPPORTED, "map_storage_mode 'all' is not written for DDP");
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     result_release(h);

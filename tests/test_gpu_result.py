@@ -17,7 +17,7 @@ PKG = load_pkg()
 @needs_cli
 @pytest.mark.parametrize("kind,mode,dt_map", [("sp", "default", "0.1"), ("sp", "all", "-1"), ("sp", "none", "0.1"),
                                               ("dip", "default", "0.05"), ("dip", "all", "0.1"),
-                                              ("ddp", "default", "0.1")])
+                                              ("ddp", "default", "0.1"), ("ddp", "all", "-1")])
 def test_file_equals_the_reference_solvers(tmp_path, kind, mode, dt_map):
     PKG.build.build()
     case = result_case(kind, mode, dt_map=dt_map)

@@ -60,7 +60,7 @@ def run_reference(folder, case):
 
 @needs_cli
 @pytest.mark.parametrize("kind,mode", [("sp", "default"), ("sp", "all"), ("sp", "none"), ("dip", "default"),
-                                       ("dip", "all"), ("ddp", "default")])
+                                       ("dip", "all"), ("ddp", "default"), ("ddp", "all")])
 def test_header_is_the_reference_files_prefix(tmp_path, kind, mode):
     case = result_case(kind, mode)
     data, geo = run_reference(str(tmp_path / "case"), case)
@@ -74,8 +74,10 @@ def test_header_is_the_reference_files_prefix(tmp_path, kind, mode):
     assert data[:len(head)] == head
     names, times_cfg, times, frames = read_result(data, geo, case.mesh.cell_nb)
     expect = list(NAMES[mode])
-    if kind == "ddp":  # swDdp::init's name for the discharge norm (swDdp.cpp:794-797)
-        expect[4] = "unit_disch_norm"
+    if kind == "ddp":  # swDdp::init's names (swDdp.cpp:794-805)
+        expect[4] = "unit_disch_norm" if mode == "default" else "unit_disc_norm"
+        if mode == "all":
+            expect[12:] = ["phi_by_wat_depth", "phi_by_disc_x", "phi_by_disc_y", "phi_by_disc_norm"]
     assert names == expect
     assert times_cfg == (0.0, 0.5, 0.1)
     if mode == "none":
@@ -99,5 +101,5 @@ def test_header_rejects_bad_arguments(tmp_path):
     lib = PKG.capi.load_library()
     assert lib.sw2d_result_header(str(tmp_path / "x.bin").encode(), b"/nonexistent/geometry.sw2d", 0, 0, 0.0, 1.0,
                                   1.0) == -1
-    assert lib.sw2d_result_header(str(tmp_path / "x.bin").encode(), b"g", 2, 1, 0.0, 1.0, 1.0) == -8
+    assert lib.sw2d_result_header(str(tmp_path / "x.bin").encode(), b"g", 0, 3, 0.0, 1.0, 1.0) == -1
     assert lib.sw2d_result_header(str(tmp_path / "x.bin").encode(), b"g", 3, 0, 0.0, 1.0, 1.0) == -1
