@@ -569,7 +569,7 @@ def run_closure(pkg, args, local_rank):
     stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
 
     def timed(steps):
-        model.step(3)
+        model.step(40)  # warm-up, including the capture of the step graph
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)

@@ -86,6 +86,49 @@ __device__ __forceinline__ float gelu_grad(float x)
     return __fmaf_rn(0.5f * x * sech2, du, __fmaf_rn(0.5f, t, 0.5f));
 }
 
+// Two GELUs at once in packed FP32 (sm_100 add / mul / fma .rn.f32x2): per lane the same IEEE
+// operations, in the same order, as gelu() above, so the results are the same bit for bit,
+// with about half the FP32 instructions.
+__device__ __forceinline__ unsigned long long pack2(float a, float b)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& a, float& b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// gelu(z0 + b0), gelu(z1 + b1)
+__device__ __forceinline__ void gelu_bias2(float z0, float z1, float b0, float b1, float& g0, float& g1)
+{
+    const unsigned long long x = add2(pack2(z0, z1), pack2(b0, b1));
+    const unsigned long long p = fma2(pack2(kGeluK0 * kGeluK1, kGeluK0 * kGeluK1), mul2(x, x), pack2(kGeluK0, kGeluK0));
+    float u0, u1;
+    unpack2(mul2(x, p), u0, u1);
+    const unsigned long long hx = mul2(pack2(0.5f, 0.5f), x);
+    unpack2(fma2(hx, pack2(tanh_hw(u0), tanh_hw(u1)), hx), g0, g1);
+}
+
 template <int kMode>
 __global__ void __launch_bounds__(128) k_umma_gemm(GemmArgs g)
 {
@@ -834,8 +877,10 @@ __global__ void __launch_bounds__(128) k_update_closure(DevMesh m, ClosureArgs a
                 tmem_wait_ld();
                 uint32_t hv[8];  // bf16 pairs
                 for (int j = 0; j < 8; j++) {
-                    const __nv_bfloat162 pr = __floats2bfloat162_rn(gelu(__uint_as_float(v[2 * j]) + bias[c0 + 2 * j]),
-                                                                    gelu(__uint_as_float(v[2 * j + 1]) + bias[c0 + 2 * j + 1]));
+                    float g0, g1;
+                    gelu_bias2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]), bias[c0 + 2 * j],
+                               bias[c0 + 2 * j + 1], g0, g1);
+                    const __nv_bfloat162 pr = __floats2bfloat162_rn(g0, g1);
                     hv[j] = *reinterpret_cast<const uint32_t*>(&pr);
                 }
                 *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0, kHid)) =
