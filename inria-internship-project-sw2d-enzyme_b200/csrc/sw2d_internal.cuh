@@ -144,6 +144,7 @@ struct sw2d_handle {
     int64_t nc = 0, ni = 0, nb = 0;
     sw2d_params p{};
     int model = 0;             // kModelSp, kModelDip or kModelDdp
+    int sms = 0;               // the device's SM count (0 until first needed)
     int dissipation = 0;       // DIP momentum dissipation active
     std::vector<int> cell_perm, int_perm, bnd_perm;  // [new] = caller index
     std::vector<void*> allocs;

@@ -267,6 +267,17 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double min_keep(double a, double b) { return (b < a) ? b : a; }
 
+// k_cfl's grid: 8 blocks of kBlock threads per SM (a full SM), at most one block per kBlock cells
+unsigned cfl_grid(sw2d_handle* h, int nc)
+{
+    if (!h->sms) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess || sms <= 0) sms = 148;
+        h->sms = sms;
+    }
+    return std::min<unsigned>(grid_for(nc), (unsigned)(8 * h->sms));
+}
+
 // kDdpSnap: the DDP model's form of the snap, which truncates t and t + dt to integers before
 // dividing by dt_map (swDdpHyp.cpp:588-600: `(int)t / dt_map`).
 template <bool kDdpSnap>
@@ -277,9 +288,12 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
         if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->go = 0;
         return;
     }
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    // grid-stride over the cells (the grid is a few blocks per SM, see cfl_grid), several cells
+    // per thread in flight; the minimum does not depend on the order it is taken in
     double best = m.dt_max;
-    if (c < m.nc) {
+    const int stride = gridDim.x * blockDim.x;
+#pragma unroll 4
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m.nc; c += stride) {
         const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
         double sw = 0.0;
         if (k1 - k0 <= kUnroll) {
@@ -644,7 +658,7 @@ void launch_phase(sw2d_handle* h, int i)
             if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) launch_slopes(h, h->slope_variant);
             break;
         case 1: launch_edges(h, h->edge_variant); break;
-        case 2: k_cfl<false><<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); break;
+        case 2: k_cfl<false><<<cfl_grid(h, m.nc), kBlock, 0, h->stream>>>(m); break;
         default: launch_update_s<false>(h, m); break;
     }
 }
@@ -666,9 +680,9 @@ void launch_slopes_on(sw2d_handle* h, const DevMesh& m)
 
 void launch_edges_on(sw2d_handle* h, const DevMesh& m) { launch_edges(h, m, h->edge_variant); }
 
-void launch_cfl_on(sw2d_handle* h, const DevMesh& m) { k_cfl<false><<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
+void launch_cfl_on(sw2d_handle* h, const DevMesh& m) { k_cfl<false><<<cfl_grid(h, m.nc), kBlock, 0, h->stream>>>(m); }
 
-void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m) { k_cfl<true><<<grid_for(m.nc), kBlock, 0, h->stream>>>(m); }
+void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m) { k_cfl<true><<<cfl_grid(h, m.nc), kBlock, 0, h->stream>>>(m); }
 
 void launch_step_on(sw2d_handle* h) { launch_step(h); }
 
