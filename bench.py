@@ -70,6 +70,9 @@ def _args():
                     help="cells of the DIP run that times the learned closure")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure line")
     ap.add_argument("--closure-only", action="store_true", help="run only the learned-closure line")
+    ap.add_argument("--result-cells", type=int, default=500_000,
+                    help="cells of the ResultHydro.bin line (0: skip)")
+    ap.add_argument("--result-only", action="store_true", help="run only the ResultHydro.bin line")
     ap.add_argument("--closure-no-pipeline", action="store_true",
                     help="time the closure inside the step only (no data generation, training or judging)")
     ap.add_argument("--assim-cells", type=int, default=1_000_000,
@@ -621,6 +624,75 @@ def run_closure(pkg, args, local_rank):
                          "coarse_error_vs_fine_h_q": ev}}
 
 
+def run_result(pkg, args, local_rank):
+    """The binary map file written during a run: the Gaussian-bump construction at
+    `--result-cells` cells, 200 graph-launched steps with a map every 20 steps' time (dt_map),
+    without and with ResultHydro.bin attached (frames copied from the device on a side stream
+    and written by the library's thread while the next steps run).  Host wall time around the
+    steps and, with the file, until the last frame is on file."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    folder = tempfile.mkdtemp(prefix="sw2d_result_")
+    try:
+        case = pkg.workloads.gaussian_bumps(n_cells=args.result_cells)
+        probe = pkg.SpModel(case, device=local_rank)
+        probe.step(5)
+        dt = probe.dt
+        probe.close()
+        # a power of two near 20 steps' time: the snapped times are then multiples of it
+        # exactly, which checkStore's test needs
+        import math
+        case.opts = dict(case.opts, dt_map=repr(2.0 ** round(math.log2(20 * dt))), t_max="1e9")
+        pkg.write_case(folder, case)
+        geo = os.path.join(folder, "input", "geometry.sw2d")
+
+        def run(with_file):
+            m = pkg.SpModel(case, device=local_rank)
+            m.step(40)
+            torch.cuda.synchronize()
+            path = os.path.join(folder, "ResultHydro.bin")
+            if with_file:
+                m.result_open(path, geo, "default")
+            t0 = time.perf_counter()
+            done = m.step(200)
+            if with_file:
+                m.result_close()
+            torch.cuda.synchronize()
+            el = time.perf_counter() - t0
+            size = os.path.getsize(path) if with_file else 0
+            m.close()
+            return el, done, size
+
+        t_plain, n_plain, _ = run(False)
+        t_file, n_file, size = run(True)
+        with open(geo, "rb") as fh:
+            geo_bytes = len(fh.read())
+        n = case.mesh.cell_nb
+        frame = 8 + 8 * 5 * n
+        frames = (size - geo_bytes) // frame if size > geo_bytes else 0
+        return {"workload": f"SP Gaussian bumps at {n} cells, 200 steps, a map every {case.opts['dt_map']} s "
+                            f"(about 20 steps), store_flag default",
+                "ms_per_step_without_file": 1e3 * t_plain / max(n_plain, 1),
+                "ms_per_step_with_file": 1e3 * t_file / max(n_file, 1),
+                "frames": int(frames), "frame_mb": frame / 1e6, "file_mb": size / 1e6,
+                "frame_gb_per_s_over_run": frames * frame / t_file / 1e9,
+                "overhead": (t_file / max(n_file, 1)) / (t_plain / max(n_plain, 1)) - 1.0,
+                "timing": "host wall time; with the file, until every frame is on file"}
+    finally:
+        shutil.rmtree(folder, ignore_errors=True)
+
+
+def run_result_only(args, local_rank):
+    pkg = importlib.import_module(PKG)
+    pkg.build.build()
+    import torch
+    torch.cuda.set_device(local_rank)
+    print(json.dumps(run_result(pkg, args, local_rank)))
+
+
 def run_closure_only(args, local_rank):
     pkg = importlib.import_module(PKG)
     pkg.build.build()
@@ -836,6 +908,7 @@ def run_ours(args, rank, world, local_rank):
     assim = None if (args.assim_cells <= 0 or world > 1) else run_assim(pkg, args, local_rank)
     ensemble = None if (args.ensemble_members <= 0 or world > 1) else run_ensemble(pkg, args, local_rank)
     closure = None if (args.no_closure or world > 1) else run_closure(pkg, args, local_rank)
+    result = None if (args.result_cells <= 0 or world > 1) else run_result(pkg, args, local_rank)
 
     steps = args.steps
     value = n * steps * world / (ms / 1e3)
@@ -882,6 +955,8 @@ def run_ours(args, rank, world, local_rank):
         line["ensemble"] = ensemble
     if closure is not None:
         line["closure"] = closure
+    if result is not None:
+        line["result_file"] = result
     print(json.dumps(line))
 
 
@@ -904,6 +979,9 @@ def main():
     elif args.closure_only:
         if rank == 0:
             run_closure_only(args, local_rank)
+    elif args.result_only:
+        if rank == 0:
+            run_result_only(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
