@@ -67,7 +67,7 @@ def sp_toce_case():
     return case, fx
 
 
-# north_star: results within 1e-10 relative of the reference in h, hu, hv
+# parity bar of the floating-point comparisons: within 1e-10 relative of the reference in h, hu, hv
 REL_TOL = 1e-10
 
 
