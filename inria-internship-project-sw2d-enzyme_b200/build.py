@@ -45,24 +45,47 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return OUT
-    os.makedirs(LIBDIR, exist_ok=True)
-    cmd = [_nvcc()] + NVCC_FLAGS
-    hc = _host_compiler()
+def _compile(src: str, obj: str, hc) -> subprocess.CompletedProcess:
+    cmd = [_nvcc()] + [f for f in NVCC_FLAGS if f != "-shared"] + ["-c"]
     if hc:
         cmd += ["-ccbin", hc]
-    cmd += ["-o", OUT + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+    cmd += ["-o", obj + ".tmp", src]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode == 0:
+        os.replace(obj + ".tmp", obj)
+    return res
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object in lib/obj (in parallel, one nvcc per source) and links
+    the shared library; the -Xptxas -v report of all sources goes to lib/ptxas.log."""
+    if not force and up_to_date():
+        return OUT
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    hc = _host_compiler()
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    objs = [os.path.join(objdir, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda so: _compile(so[0], so[1], hc), zip(srcs, objs)))
+    log = "".join(r.stderr for r in results)
+    if any(r.returncode != 0 for r in results):
+        sys.stderr.write("".join(r.stdout + r.stderr for r in results if r.returncode != 0))
+        raise RuntimeError("nvcc failed")
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared"]
+    if hc:
+        cmd += ["-ccbin", hc]
+    cmd += ["-o", OUT + ".tmp"] + objs
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed")
+        raise RuntimeError("nvcc link failed")
     if verbose:
-        sys.stderr.write(res.stderr)
+        sys.stderr.write(log)
     os.replace(OUT + ".tmp", OUT)
     with open(os.path.join(LIBDIR, "ptxas.log"), "w") as fh:
-        fh.write(res.stderr)
+        fh.write(log)
     return OUT
 
 

@@ -25,7 +25,8 @@ REF_BIN_PM = os.path.join(HERE, "_ref", "sw2dSolver_pm")
 REF_MAPPER = os.path.join(HERE, "_ref", "sw2dPorosityMapper")
 REF_E_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e.so")
 REF_E_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e_pm.so")
-REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "/root/reference")
+# root of the reference's source tree (the environment variable SW2D_REFERENCE; empty when unset)
+REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "")
 
 _pkg = importlib.import_module("inria-internship-project-sw2d-enzyme_b200")
 capi = _pkg.capi

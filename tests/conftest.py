@@ -20,6 +20,23 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 
 
+def reference_missing():
+    """Why the reference's source tree is unavailable to a test ("" when it is available): its
+    root comes from the environment variable SW2D_REFERENCE."""
+    root = os.environ.get("SW2D_REFERENCE", "")
+    if not root:
+        return "SW2D_REFERENCE is not set (root of the reference's source tree)"
+    if not os.path.isdir(root):
+        return f"SW2D_REFERENCE={root} is not a directory"
+    return ""
+
+
+def reference_case(name):
+    """Folder of the reference's functional case `name` under SW2D_REFERENCE ("" when unset)."""
+    root = os.environ.get("SW2D_REFERENCE", "")
+    return os.path.join(root, "configue_fonctionels", name) if root else ""
+
+
 def load_pkg():
     return importlib.import_module(PKG_NAME)
 

@@ -37,7 +37,8 @@ sys.path.insert(0, ROOT)
 
 from oracle.binding import RefE, REFERENCE_SRC  # noqa: E402
 
-CASE = os.path.join(REFERENCE_SRC, "configue_fonctionels", "sp_toce")
+# the reference's functional case (under SW2D_REFERENCE; "" when unset: main() then stops)
+CASE = os.path.join(REFERENCE_SRC, "configue_fonctionels", "sp_toce") if REFERENCE_SRC else ""
 OUT = os.path.join(ROOT, "tests", "golden", "sp_toce_assim.npz")
 EPS = (1e-6, 1e-7, 1e-8)
 
@@ -84,6 +85,8 @@ def decimals_to_float(mant, expo):
 
 
 def main():
+    if not CASE:
+        raise SystemExit("make_assim_golden.py: set SW2D_REFERENCE to the reference's source tree")
     ref = RefE(CASE, portable_math=True)
     cfg = ref.config()
     times, frames = ref.load_observations()

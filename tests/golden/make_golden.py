@@ -143,7 +143,10 @@ def main(only=None):
 
         if only and "sp_toce" not in only:
             return
-        src = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
+        root = os.environ.get("SW2D_REFERENCE", "")
+        if not root:
+            raise SystemExit("make_golden.py: set SW2D_REFERENCE to the reference's source tree")
+        src = os.path.join(root, "configue_fonctionels", "sp_toce")
         folder = os.path.join(tmp, "sp_toce")
         shutil.copytree(src, folder)
         solv = os.path.join(folder, "input", "input.solv")

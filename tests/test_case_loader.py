@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from tests.conftest import load_pkg
+from tests.conftest import load_pkg, reference_case, reference_missing
 
 PKG = load_pkg()
 
@@ -87,9 +87,9 @@ def test_loader_reads_what_the_python_readers_read(tmp_path, name):
 
 
 def test_loader_reads_sp_toce():
-    src = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
+    src = reference_case("sp_toce")
     if not os.path.isdir(src):
-        pytest.skip("the reference's functional case is not on this machine")
+        pytest.skip(reference_missing() or "the reference's functional case sp_toce is missing")
     _check(src)
 
 

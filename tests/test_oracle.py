@@ -36,8 +36,8 @@ def test_oracle_matches_reference_golden(name, portable):
     case, fx = golden_case(name)
     sfx = "_pm" if portable else ""
     if str(fx["builder"]) in DIP_BUILDERS | DDP_BUILDERS:
-        if not os.path.isdir(os.path.join(oracle_binding.REFERENCE_SRC, "src")):
-            pytest.skip("DIP and DDP fixtures are pinned to the live reference, absent on this machine")
+        if not oracle_binding.reference_available():
+            pytest.skip("DIP and DDP fixtures are pinned to the live reference, whose library (oracle/_ref) is not built")
         import tempfile
         folder = tempfile.mkdtemp(prefix="sw2d_dip_")
         load_pkg().write_case(folder, case)
@@ -70,8 +70,8 @@ def test_oracle_matches_reference_sp_toce(portable):
     assert _bits_equal(r, fx["r_end" + sfx])
 
 
-needs_ref = pytest.mark.skipif(not os.path.isdir(os.path.join(oracle_binding.REFERENCE_SRC, "src")),
-                               reason="reference sources not present on this machine")
+needs_ref = pytest.mark.skipif(not oracle_binding.reference_available(),
+                               reason="the reference solver library (oracle/_ref) is not built")
 
 
 @needs_ref

@@ -16,16 +16,16 @@ import os
 import numpy as np
 import pytest
 
-from tests.conftest import GOLDEN
+from tests.conftest import GOLDEN, reference_case, reference_missing
 
-CASE = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
+CASE = reference_case("sp_toce")
 DESCENT_LOG_J_INIT = 3.1042911536e+00   # descent_log_reference_-75.8pct.csv, iteration 1, J_total
 
 
 def _ref(pm):
     from oracle.binding import RefE, REF_E_SO, REF_E_PM_SO
     if not os.path.isdir(CASE) or not os.path.exists(REF_E_PM_SO if pm else REF_E_SO):
-        pytest.skip("reference sources or the reference assimilation library are absent")
+        pytest.skip(reference_missing() or "the reference assimilation library (oracle/_ref) is not built")
     return RefE(CASE, portable_math=pm)
 
 

@@ -8,15 +8,15 @@ import os
 import numpy as np
 import pytest
 
-from tests.conftest import load_pkg
+from tests.conftest import load_pkg, reference_case, reference_missing
 
-CASE = os.path.join(os.environ.get("SW2D_REFERENCE", "/root/reference"), "configue_fonctionels", "sp_toce")
+CASE = reference_case("sp_toce")
 
 
 def _ref():
     from oracle.binding import RefE, REF_E_SO
     if not os.path.isdir(CASE) or not os.path.exists(REF_E_SO):
-        pytest.skip("reference sources or the reference assimilation library are absent")
+        pytest.skip(reference_missing() or "the reference assimilation library (oracle/_ref) is not built")
     return RefE(CASE)
 
 
