@@ -62,7 +62,7 @@ struct AdjointState {
     double* d_t_seq = nullptr;
     // checkpoints k = 0 .. n_ck-1 at step k*every, and the end of the trajectory
     double4* ck_st = nullptr;            // (n_ck + 1) * nc
-    double4* ck_slot = nullptr;          // (n_ck + 1) * nslot
+    Slot* ck_slot = nullptr;             // (n_ck + 1) * nslot
     Ctrl* ck_ctrl = nullptr;             // n_ck + 1
     bool ck_valid = false;
     // one segment of recomputed steps
@@ -429,7 +429,7 @@ int ck_save(sw2d_handle* h, int64_t k)
 {
     AdjointState* a = h->adj;
     CK(cudaMemcpyAsync(a->ck_st + k * h->nc, h->m.st, h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(a->ck_slot + k * a->nslot, h->m.slot, a->nslot * sizeof(double4), cudaMemcpyDeviceToDevice,
+    CK(cudaMemcpyAsync(a->ck_slot + k * a->nslot, h->m.slot, a->nslot * sizeof(Slot), cudaMemcpyDeviceToDevice,
                        h->stream));
     CK(cudaMemcpyAsync(a->ck_ctrl + k, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, h->stream));
     return SW2D_OK;
@@ -439,7 +439,7 @@ int ck_load(sw2d_handle* h, int64_t k)
 {
     AdjointState* a = h->adj;
     CK(cudaMemcpyAsync(h->m.st, a->ck_st + k * h->nc, h->nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->m.slot, a->ck_slot + k * a->nslot, a->nslot * sizeof(double4), cudaMemcpyDeviceToDevice,
+    CK(cudaMemcpyAsync(h->m.slot, a->ck_slot + k * a->nslot, a->nslot * sizeof(Slot), cudaMemcpyDeviceToDevice,
                        h->stream));
     CK(cudaMemcpyAsync(h->ctrl, a->ck_ctrl + k, sizeof(Ctrl), cudaMemcpyDeviceToDevice, h->stream));
     return SW2D_OK;

@@ -64,6 +64,7 @@ struct AssimState {
     bool configured = false;
     double t0 = 0.0;                 // start of the trajectory
     double4* st0 = nullptr;          // nc: the state at the start (swSpE::save_initial_state)
+    double4* slot4 = nullptr;        // nslot: balance slots of the differentiated step
     // control
     double* d_m = nullptr;           // nc (internal numbering)
     double* d_phi = nullptr;         // nc: phi = T(m)
@@ -241,14 +242,14 @@ __global__ void __launch_bounds__(kBlock) k_e_edges(DevMesh m, EView v)
             const double c = cf.x;
             const double f1 = -c, f2F2 = -c * nx, f2F3 = +c * ny, f2S2 = +c * nx;
             const double f3F2 = -c * ny, f3F3 = -c * nx, f3S2 = +c * ny;
-            m.slot[sl.x] = make_double4(f.f1, f2F2 * f.f2 + f2S2 * f.sl + f2F3 * f.f3,
+            m.slot4[sl.x] = make_double4(f.f1, f2F2 * f.f2 + f2S2 * f.sl + f2F3 * f.f3,
                                         f3F2 * f.f2 + f3S2 * f.sl + f3F3 * f.f3, f1);
         }
         {
             const double c = cf.y;
             const double f1 = +c, f2F2 = +c * nx, f2F3 = -c * ny, f2S2 = +c * nx;
             const double f3F2 = +c * ny, f3F3 = +c * nx, f3S2 = +c * ny;
-            m.slot[sl.y] = make_double4(f.f1, f2F2 * f.f2 + f2S2 * f.sr + f2F3 * f.f3,
+            m.slot4[sl.y] = make_double4(f.f1, f2F2 * f.f2 + f2S2 * f.sr + f2F3 * f.f3,
                                         f3F2 * f.f2 + f3S2 * f.sr + f3F3 * f.f3, f1);
         }
     } else if (i < m.ni + m.nb) {
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(kBlock) k_e_edges(DevMesh m, EView v)
         const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
         const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
         const double s2 = 0.0;  // source_right of hypBoundaryFlux_E (swSpE_hyp.cpp:167)
-        m.slot[sb] = make_double4(fa * F.f1, f2F2 * F.f2 + f2S2 * s2 + f2F3 * F.f3,
+        m.slot4[sb] = make_double4(fa * F.f1, f2F2 * F.f2 + f2S2 * s2 + f2F3 * F.f3,
                                   f3F2 * F.f2 + f3S2 * s2 + f3F3 * F.f3, 1.0);
     }
 }
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(kBlock) k_e_update(DevMesh m, const double* __
         double4 v[kEUnroll];
 #pragma unroll
         for (int i = 0; i < kEUnroll; i++)
-            if (i < k1 - k0) v[i] = m.slot[k0 + i];
+            if (i < k1 - k0) v[i] = m.slot4[k0 + i];
 #pragma unroll
         for (int i = 0; i < kEUnroll; i++)
             if (i < k1 - k0) {
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(kBlock) k_e_update(DevMesh m, const double* __
             }
     } else {
         for (int k = k0; k < k1; k++) {
-            const double4 v = m.slot[k];
+            const double4 v = m.slot4[k];
             hh += v.w * (v.x * dt);
             qq += v.y * dt;
             rr += v.z * dt;
@@ -682,6 +683,7 @@ DevMesh view_with(sw2d_handle* h, Ctrl* ctrl)
 {
     DevMesh m = h->m;
     m.ctrl = ctrl;
+    m.slot4 = h->assim ? h->assim->slot4 : nullptr;
     return m;
 }
 
@@ -708,7 +710,7 @@ int fixed_buffers(sw2d_handle* h)
         (rc = adj_alloc(h, L, nc, &a->g_k1)) || (rc = adj_alloc(h, L, nc, &a->g_k2)) ||
         (rc = adj_alloc(h, L, nc, &a->g_w)) || (rc = adj_alloc(h, L, kCostBlocks, &a->d_part)) ||
         (rc = adj_alloc(h, L, 8, &a->d_out)) || (rc = adj_alloc(h, L, 4, &a->d_count)) ||
-        (rc = adj_alloc(h, L, 3 * nc, &a->stage)))
+        (rc = adj_alloc(h, L, 3 * nc, &a->stage)) || (rc = adj_alloc(h, L, a->nslot, &a->slot4)))
         return rc;
     Ctrl on{};
     on.t = 0.0;

@@ -117,13 +117,13 @@ __device__ __forceinline__ void put_int_slots(const DevMesh& m, int e, double nx
         const double c = cf.x;
         const double a1 = -c, f2F2 = -c * nx, f2F3 = +c * ny, f2S2 = +c * nx;
         const double f3F2 = -c * ny, f3F3 = -c * nx, f3S2 = +c * ny;
-        m.slot[sl.x] = make_double4(a1 * f1, f2F2 * f2 + f2S2 * sL + f2F3 * f3, f3F2 * f2 + f3S2 * sL + f3F3 * f3, 0.0);
+        m.slot[sl.x] = make_slot(a1 * f1, f2F2 * f2 + f2S2 * sL + f2F3 * f3, f3F2 * f2 + f3S2 * sL + f3F3 * f3);
     }
     {
         const double c = cf.y;
         const double a1 = +c, f2F2 = +c * nx, f2F3 = -c * ny, f2S2 = +c * nx;
         const double f3F2 = +c * ny, f3F3 = +c * nx, f3S2 = +c * ny;
-        m.slot[sl.y] = make_double4(a1 * f1, f2F2 * f2 + f2S2 * sR + f2F3 * f3, f3F2 * f2 + f3S2 * sR + f3F3 * f3, 0.0);
+        m.slot[sl.y] = make_slot(a1 * f1, f2F2 * f2 + f2S2 * sR + f2F3 * f3, f3F2 * f2 + f3S2 * sR + f3F3 * f3);
     }
 }
 
@@ -134,7 +134,7 @@ __device__ __forceinline__ void put_bnd_slot(const DevMesh& m, double4 g, int sb
     const double cf = g.w, nx = g.x, ny = g.y;
     const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
     const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
-    m.slot[sb] = make_double4(fa * f1, f2F2 * f2 + f2S2 * s2 + f2F3 * f3, f3F2 * f2 + f3S2 * s2 + f3F3 * f3, 0.0);
+    m.slot[sb] = make_slot(fa * f1, f2F2 * f2 + f2S2 * s2 + f2F3 * f3, f3F2 * f2 + f3S2 * s2 + f3F3 * f3);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -290,23 +290,23 @@ __device__ __forceinline__ void slot_balance(const DevMesh& m, int c, double dt,
 {
     const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
     if (k1 - k0 <= kUnroll) {
-        double4 v[kUnroll];
+        Slot v[kUnroll];
 #pragma unroll
         for (int i = 0; i < kUnroll; i++)
             if (i < k1 - k0) v[i] = m.slot[k0 + i];
 #pragma unroll
         for (int i = 0; i < kUnroll; i++)
             if (i < k1 - k0) {
-                hh += v[i].x * dt;
-                qq += v[i].y * dt;
-                rr += v[i].z * dt;
+                hh += v[i].a * dt;
+                qq += v[i].b * dt;
+                rr += v[i].c * dt;
             }
     } else {
         for (int k = k0; k < k1; k++) {
-            const double4 v = m.slot[k];
-            hh += v.x * dt;
-            qq += v.y * dt;
-            rr += v.z * dt;
+            const Slot v = m.slot[k];
+            hh += v.a * dt;
+            qq += v.b * dt;
+            rr += v.c * dt;
         }
     }
 }
@@ -620,10 +620,10 @@ __global__ void __launch_bounds__(kBlock) k_lf_recompute(DevMesh m)
     const int2 a = ld(&m.coff[c]), b = ld(&m.coff[c + 1]);
     if (b.x - a.x <= 0) return;  // no internal edge
     const double dt = m.ctrl->dt;
-    const double4 v = m.slot[b.y - 1];
+    const Slot v = m.slot[b.y - 1];
     const double4 o = m.old[c];
     const double4 s = m.st[c];
-    m.st[c] = make_double4(o.x + v.x * dt, o.y + v.y * dt, o.z + v.z * dt, s.w);
+    m.st[c] = make_double4(o.x + v.a * dt, o.y + v.b * dt, o.z + v.c * dt, s.w);
 }
 
 __global__ void k_lf_next(DevMesh m)

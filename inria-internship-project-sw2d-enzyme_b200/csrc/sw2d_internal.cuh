@@ -42,6 +42,21 @@ struct Ctrl {
     int store_map;  // DDP: the step ends on a storage time (swDdpHyp.cpp:590-609)
 };
 
+// One balance slot: the dt-free contributions {a, b, c} of one edge to one cell's h, q and r
+// (hypComputeBalance, swSpHyp.cpp:221-263: h += a dt, q += b dt, r += c dt).
+struct Slot {
+    double a, b, c;
+};
+
+__host__ __device__ __forceinline__ Slot make_slot(double a, double b, double c)
+{
+    Slot s;
+    s.a = a;
+    s.b = b;
+    s.c = c;
+    return s;
+}
+
 struct DdpCtrl;       // sw2d_ddp.cu
 struct ResultWriter;  // sw2d_result.cu
 
@@ -59,7 +74,8 @@ struct DevMesh {
     const double* area;
     const int2* coff;        // [nc+1] {first internal-neighbour entry, first balance slot}
     const int2* cint;        // {edge*2 + side, neighbour} (MUSCL slopes)
-    double4* slot;           // balance slots {a, b, c, -}
+    Slot* slot;              // balance slots {a, b, c}
+    double4* slot4;          // balance slots of the differentiated step {f1 F1, b, c, f1} (sw2d_assim.cu)
     double* slot_w;          // CFL contribution of the slot
     double4* bal;            // post-balance state {h, q, r, -} (written only by the recording update)
     // internal edges
@@ -241,8 +257,9 @@ __device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt,
             double ul = u * ca + v * sa;
             double vl = -u * sa + v * ca;
             double un = sqrt(u * u + v * v);
+            // isotropic friction (equal coefficients): the same factor, computed once
             double f1 = friction_factor(kFriction, fr.x, hh, un, dt);
-            double f2 = friction_factor(kFriction, fr.y, hh, un, dt);
+            double f2 = (fr.y == fr.x) ? f1 : friction_factor(kFriction, fr.y, hh, un, dt);
             ul *= f1;
             vl *= f2;
             qq = (ul * ca - vl * sa) * hh;

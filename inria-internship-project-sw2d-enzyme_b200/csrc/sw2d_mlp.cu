@@ -830,10 +830,10 @@ __global__ void __launch_bounds__(128) k_update_closure(DevMesh m, ClosureArgs a
                 // hypComputeBalance (swSpHyp.cpp:214-273), the slots in the reference's order
                 const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
                 for (int k = k0; k < k1; k++) {
-                    const double4 v = m.slot[k];
-                    hh += v.x * dt;
-                    qq += v.y * dt;
-                    rr += v.z * dt;
+                    const Slot v = m.slot[k];
+                    hh += v.a * dt;
+                    qq += v.b * dt;
+                    rr += v.c * dt;
                 }
                 double f[kIn];
                 closure_features(s0, make_double4(hh, qq, rr, 0.0), ld(&m.cst[c].z), a.phig_min[c], dt, f);

@@ -218,15 +218,15 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
                 const double c = cf.x;
                 const double f1 = -c, f2F2 = -c * nx, f2F3 = +c * ny, f2S2 = +c * nx;
                 const double f3F2 = -c * ny, f3F3 = -c * nx, f3S2 = +c * ny;
-                m.slot[sl.x] = make_double4(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sl + f2F3 * f.f3,
-                                            f3F2 * f.f2 + f3S2 * f.sl + f3F3 * f.f3, 0.0);
+                m.slot[sl.x] = make_slot(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sl + f2F3 * f.f3,
+                                         f3F2 * f.f2 + f3S2 * f.sl + f3F3 * f.f3);
             }
             {
                 const double c = cf.y;
                 const double f1 = +c, f2F2 = +c * nx, f2F3 = -c * ny, f2S2 = +c * nx;
                 const double f3F2 = +c * ny, f3F3 = +c * nx, f3S2 = +c * ny;
-                m.slot[sl.y] = make_double4(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sr + f2F3 * f.f3,
-                                            f3F2 * f.f2 + f3S2 * f.sr + f3F3 * f.f3, 0.0);
+                m.slot[sl.y] = make_slot(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sr + f2F3 * f.f3,
+                                         f3F2 * f.f2 + f3S2 * f.sr + f3F3 * f.f3);
             }
         }
     } else if (i < m.ni + m.nb) {
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
         const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
         const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
         const double s2 = 0.0;  // boundary geometric source: never set by hypBoundaryFlux
-        m.slot[sb] = make_double4(fa * f1, f2F2 * f2 + f2S2 * s2 + f2F3 * f3, f3F2 * f2 + f3S2 * s2 + f3F3 * f3, 0.0);
+        m.slot[sb] = make_slot(fa * f1, f2F2 * f2 + f2S2 * s2 + f2F3 * f3, f3F2 * f2 + f3S2 * s2 + f3F3 * f3);
     }
     if (bad) atomicOr(&m.ctrl->status, bad);
 }
@@ -384,23 +384,23 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
     // over the cell's slots, in the reference's order
     const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
     if (k1 - k0 <= kUnroll) {
-        double4 v[kUnroll];
+        Slot v[kUnroll];
 #pragma unroll
         for (int i = 0; i < kUnroll; i++)
             if (i < k1 - k0) v[i] = m.slot[k0 + i];
 #pragma unroll
         for (int i = 0; i < kUnroll; i++)
             if (i < k1 - k0) {
-                hh += v[i].x * dt;
-                qq += v[i].y * dt;
-                rr += v[i].z * dt;
+                hh += v[i].a * dt;
+                qq += v[i].b * dt;
+                rr += v[i].c * dt;
             }
     } else {
         for (int k = k0; k < k1; k++) {
-            const double4 v = m.slot[k];
-            hh += v.x * dt;
-            qq += v.y * dt;
-            rr += v.z * dt;
+            const Slot v = m.slot[k];
+            hh += v.a * dt;
+            qq += v.b * dt;
+            rr += v.c * dt;
         }
     }
     if (kDissip) {  // DIP momentum dissipation, before the round-off flush (dip/swDipHyp.cpp:295-324)
