@@ -33,6 +33,47 @@ def jittered_triangle_mesh(nx: int, ny: int, lx: float, ly: float, x0: float = 0
     return mesh_from_triangles(x, y, z, tri, bc_code_fn)
 
 
+def delaunay_triangle_mesh(n_cells: int, lx: float, ly: float, x0: float = 0.0, y0: float = 0.0,
+                           jitter: float = 0.3, seed: int = 1, permute: bool = True,
+                           z_fn: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None,
+                           bc_code_fn: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None) -> Mesh:
+    """Seeded jittered-Delaunay triangulation of [x0, x0+lx] x [y0, y0+ly] with about n_cells
+    triangles.
+
+    Nodes: a grid of cell-centred points (spacing d with lx*ly / d^2 ~ n_cells / 2), each moved
+    by a seeded uniform jitter of +-jitter*d in x and y, plus points every d along the four sides
+    (corners included).  Triangles: the Delaunay triangulation of those nodes
+    (scipy.spatial.Delaunay, i.e. Qhull).  Cell degrees vary (1 to 3 internal neighbours), and
+    with ``permute`` the triangles are listed in a seeded random order, so the cell and edge
+    numbering a solver receives carries no locality of its own.
+    """
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    d = float(np.sqrt(lx * ly / max(n_cells / 2.0, 1.0)))
+    nx = max(2, int(round(lx / d)))
+    ny = max(2, int(round(ly / d)))
+    dx, dy = lx / nx, ly / ny
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny))
+    xi = x0 + (ii.reshape(-1) + 0.5) * dx + rng.uniform(-jitter, jitter, ii.size) * dx
+    yi = y0 + (jj.reshape(-1) + 0.5) * dy + rng.uniform(-jitter, jitter, jj.size) * dy
+    bx = x0 + np.arange(nx + 1) * dx
+    by = y0 + np.arange(1, ny) * dy
+    xb = np.concatenate([bx, bx, np.full(by.size, x0), np.full(by.size, x0 + lx)])
+    yb = np.concatenate([np.full(bx.size, y0), np.full(bx.size, y0 + ly), by, by])
+    x = np.concatenate([xb, xi])
+    y = np.concatenate([yb, yi])
+    tri = Delaunay(np.stack([x, y], 1)).simplices.astype(np.int64)
+    # drop slivers of zero area (collinear boundary nodes)
+    px, py = x[tri], y[tri]
+    area2 = (px[:, 1] - px[:, 0]) * (py[:, 2] - py[:, 0]) - (px[:, 2] - px[:, 0]) * (py[:, 1] - py[:, 0])
+    tri = tri[np.abs(area2) > 1e-12 * dx * dy]
+    if permute:
+        tri = tri[np.random.default_rng(seed + 1_000_003).permutation(tri.shape[0])]
+    z = z_fn(x, y) if z_fn is not None else np.zeros_like(x)
+    return mesh_from_triangles(x, y, np.asarray(z, dtype=np.float64), tri, bc_code_fn)
+
+
 def jittered_triangles(nx: int, ny: int, lx: float, ly: float, x0: float = 0.0, y0: float = 0.0,
                        jitter: float = 0.2, seed: int = 1,
                        z_fn: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None):

@@ -24,7 +24,7 @@ from typing import Dict, Optional
 import numpy as np
 
 from .case import BoundarySeries, Case, LawRecords, ddp_law_table
-from .mesh import jittered_triangle_mesh
+from .mesh import delaunay_triangle_mesh, jittered_triangle_mesh
 
 
 def _grid_for(n_cells: int, aspect: float):
@@ -41,10 +41,25 @@ def _wall_series(codes):
                           values=np.zeros((len(codes), 2)))
 
 
+def _mesh(kind: str, n_cells: int, lx: float, ly: float, seed: int, z_fn=None, bc_code_fn=None):
+    """kind "grid": jittered_triangle_mesh (row-major numbering, every interior cell of degree 3);
+    kind "delaunay": delaunay_triangle_mesh (seeded jittered-Delaunay, cells in a seeded random
+    order)."""
+    if kind == "delaunay":
+        return delaunay_triangle_mesh(n_cells, lx, ly, seed=seed, z_fn=z_fn, bc_code_fn=bc_code_fn)
+    if kind != "grid":
+        raise ValueError(f"mesh kind {kind!r}: 'grid' or 'delaunay'")
+    nx, ny = _grid_for(n_cells, lx / ly)
+    return jittered_triangle_mesh(nx, ny, lx, ly, seed=seed, z_fn=z_fn, bc_code_fn=bc_code_fn)
+
+
 def dam_break(n_cells: int = 20000, scheme: str = "muscl_evr", friction: str = "manning",
-              t_max: float = 1.0e6, seed_mesh: int = 1, seed_phi: int = 2) -> Case:
+              t_max: float = 1.0e6, seed_mesh: int = 1, seed_phi: int = 2, mesh: str = "grid") -> Case:
+    """The plain SP dam break; ``mesh="delaunay"`` is the benchmark configuration's seeded
+    jittered-Delaunay mesh (randomly numbered)."""
+    kind = mesh
     nx, ny = _grid_for(n_cells, 5.0)
-    mesh = jittered_triangle_mesh(nx, ny, 100.0, 20.0, seed=seed_mesh)
+    mesh = _mesh(kind, n_cells, 100.0, 20.0, seed_mesh)
     n = mesh.cell_nb
     h0 = np.where(mesh.cell_x < 50.0, 1.0, 0.1)
     rng = np.random.default_rng(seed_phi)
@@ -58,7 +73,7 @@ def dam_break(n_cells: int = 20000, scheme: str = "muscl_evr", friction: str = "
                        np.zeros(n)])
     return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
                 boussinesq=np.ones(n), friction=fr, bc=_wall_series(mesh.bc_codes()),
-                extra={"name": "dam_break", "nx": nx, "ny": ny})
+                extra={"name": "dam_break", "nx": nx, "ny": ny, "mesh": kind})
 
 
 def _smooth_field(x, y, lx, ly, seed, coarse=24):
@@ -78,7 +93,14 @@ def _smooth_field(x, y, lx, ly, seed, coarse=24):
 
 
 def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: float = 1.0e6,
-                   seed_mesh: int = 1, seed_bed: int = 3, seed_phi: int = 4, seed_n: int = 5) -> Case:
+                   seed_mesh: int = 1, seed_bed: int = 3, seed_phi: int = 4, seed_n: int = 5, mesh: str = "grid",
+                   initial: str = "lake") -> Case:
+    """The large SP forward solve.  ``initial="lake"``: h = max(0, 2 - z_b), the configuration's
+    initial state (a lake at rest between dry bumps: most of the domain is dry and the wet part
+    does not move).  ``initial="dam"``: the same bed under a dam break, free surface 3.5 m for
+    x < 1000 m and 2.2 m beyond, water at rest: a moving, mostly wet flow with wet/dry fronts
+    around the bumps.  ``mesh="delaunay"``: the seeded jittered-Delaunay mesh."""
+    kind = mesh
     L = 2000.0
     rng = np.random.default_rng(seed_bed)
     amp = rng.uniform(0.0, 3.0, 50)
@@ -93,9 +115,15 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
         return z
 
     nx, ny = _grid_for(n_cells, 1.0)
-    mesh = jittered_triangle_mesh(nx, ny, L, L, seed=seed_mesh, z_fn=bed)
+    mesh = _mesh(kind, n_cells, L, L, seed_mesh, z_fn=bed)
     n = mesh.cell_nb
-    h0 = np.where(2.0 - mesh.cell_z_b < 0.0, 0.0, 2.0 - mesh.cell_z_b)   # std::max(z - z_b, 0.0)
+    if initial == "lake":
+        zs = np.full(n, 2.0)
+    elif initial == "dam":
+        zs = np.where(mesh.cell_x < 0.5 * L, 3.5, 2.2)
+    else:
+        raise ValueError(f"initial {initial!r}: 'lake' or 'dam'")
+    h0 = np.where(zs - mesh.cell_z_b < 0.0, 0.0, zs - mesh.cell_z_b)   # std::max(z - z_b, 0.0)
     phi = 0.3 + 0.7 * _smooth_field(mesh.cell_x, mesh.cell_y, L, L, seed_phi)
     rng_n = np.random.default_rng(seed_n)
     man = np.exp(np.log(0.03) + 0.3 * rng_n.standard_normal(n))
@@ -104,7 +132,8 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
             "h_min": 1e-5, "t_max": t_max, "store_flag": "none", "output_format": "txt"}
     return Case(mesh=mesh, opts=opts, h0=h0, q0=np.zeros(n), r0=np.zeros(n), phi=phi,
                 boussinesq=np.ones(n), friction=np.stack([man, man, np.zeros(n)]),
-                bc=_wall_series(mesh.bc_codes()), extra={"name": "gaussian_bumps", "nx": nx, "ny": ny, "ic_z": 2.0})
+                bc=_wall_series(mesh.bc_codes()),
+                extra={"name": "gaussian_bumps", "nx": nx, "ny": ny, "ic_z": 2.0, "mesh": kind, "initial": initial})
 
 
 def channel_features(n_cells: int = 3000, scheme: str = "godunov", topo: str = "blending",
