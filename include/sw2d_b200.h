@@ -390,19 +390,33 @@ int sw2d_set_time(sw2d_handle* h, double t, double dt);
 /* Per-edge intermediate arrays of the last step, in the caller's edge numbering, for
  * kernel-level checks: name is one of "F1_int","F2_int","F3_int","s2L_int","s2R_int",
  * "F1_bnd","F2_bnd","F3_bnd","s2R_bnd","lambda_max_int","lambda_max_bnd",
- * "slope_x","slope_y" (per cell).  Returns the element count written, or < 0. */
+ * "slope_x","slope_y" (per cell).  The fused step keeps the slopes only while the option
+ * "record_fluxes" or "record_wave_speeds" is on (SW2D_E_ARG otherwise).  Returns the element
+ * count written, or < 0. */
 int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity);
 
 /* Device time of each phase of the step, averaged over n_steps steps that this call runs
  * (they advance the simulation).  The analogue of the reference's per-phase clock() totals
  * (LRStates / TimeStep / Fluxes / Balance + sources, swSp.cpp:491-501,645-667): the phases are
- * the kernels "k_slopes", "k_edges", "k_cfl", "k_update" (sw2d_phase_name).  Launches each
- * kernel separately with CUDA events on the handle's stream.  Returns the number of phases
- * written to ms (milliseconds), or < 0. */
+ * the step's kernels, named by sw2d_phase_label: "k_flux", "k_update" for the fused step of the
+ * SP and DIP models (LRStates + TimeStep + Fluxes, then Balance + sources), "k_slopes",
+ * "k_edges", "k_cfl", "k_update" for the four-kernel step (option "fused_step" 0) and the DDP
+ * model.  Launches each kernel separately with CUDA events on the handle's stream.  Returns the
+ * number of phases written to ms (milliseconds), or < 0. */
 int sw2d_phase_times(sw2d_handle* h, int64_t n_steps, double* ms, int capacity);
+/* Name of phase i of this handle's step (sw2d_phase_times). */
+const char* sw2d_phase_label(sw2d_handle* h, int i);
+/* Phase names of the four-kernel step ("k_slopes", "k_edges", "k_cfl", "k_update"). */
 const char* sw2d_phase_name(int i);
 
-/* Run-time options.  "record_wave_speeds" (0/1): also keep lambda_max per edge for
+/* Run-time options.  "fused_step" (0/1): 1 (the default for the SP and DIP models) runs each
+ * time step as two kernels, k_flux (per tile of consecutive cells staged with their two rings
+ * of neighbours in shared memory: slopes, Riemann states, fluxes, balance terms, CFL bound and
+ * the grid's dt) and k_update; 0 runs the four-kernel step (k_slopes, k_edges, k_cfl, k_update).
+ * Both give the same bits.  "tile_cells" (32..8192): cells per tile of the fused step (512 by
+ * default, or the environment variable SW2D_TILE_CELLS read when the handle is created); the
+ * tiles are rebuilt.  "flux_variant": the launch variant of k_flux (sw2d_autotune picks it).
+ * "record_wave_speeds" (0/1): also keep lambda_max per edge for
  * sw2d_get_array("lambda_max_int"/"lambda_max_bnd") (the reference's lambda_max_int/_bnd
  * members, swSp.h:201-203); off by default since the step itself only needs lambda_max * length.
  * "record_fluxes" (0/1): keep F1, F2, F3, s2L, s2R per edge for sw2d_get_array.
@@ -412,6 +426,9 @@ const char* sw2d_phase_name(int i);
  * on the flush).  1: as the branch taken (zero derivative for flushed values), which is what
  * differentiating the reference's code line by line gives. */
 int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value);
+/* Current value of "fused_step", "flux_variant", "tile_cells" (0 without tiles),
+ * "record_fluxes" or "record_wave_speeds".  No counterpart in the reference. */
+int sw2d_get_option(sw2d_handle* h, const char* name, int64_t* value);
 
 /* Launch-configuration autotuner (no counterpart in the reference): times every
  * {threads per block, register cap} variant of the slope and edge kernels `iters` times on the

@@ -57,6 +57,27 @@ __host__ __device__ __forceinline__ Slot make_slot(double a, double b, double c)
     return s;
 }
 
+// One tile of the fused step (sw2d_tile.cu): cells [c0, c0 + nt) of the internal numbering,
+// nh1 cells one edge away and nh2 two edges away (halo[hoff ..]); internal edges with a cell in
+// the tile: the owned range [e0, e0 + ne_own) (lower cell in the tile) and nx_flux incoming edges,
+// then nx_slope edges that only the ring-1 slopes need (xe[xoff ..]); per tile edge the local
+// {L, R} indices (eloc[loff ..]); the neighbour lists of the tile and ring-1 cells (scsr[soff ..],
+// offsets soffs[so_off ..]); boundary edges [b0, b1); first balance slot s0.
+struct TileInfo {
+    int c0, nt, nh1, nh2, hoff, e0, ne_own, xoff, nx_flux, nx_slope, loff, soff, so_off, b0, b1, s0;
+};
+
+struct TileMesh {
+    int ntiles = 0, tile_cells = 0;
+    int nl_max = 0, nf_max = 0, ns_max = 0;  // largest staged cell set, tile + ring 1, slot range
+    const TileInfo* info = nullptr;
+    const int* halo = nullptr;
+    const int* xe = nullptr;
+    const ushort2* eloc = nullptr;
+    const unsigned* scsr = nullptr;        // local neighbour | tile edge << 16 | side << 31
+    const unsigned short* soffs = nullptr;
+};
+
 struct DdpCtrl;       // sw2d_ddp.cu
 struct ResultWriter;  // sw2d_result.cu
 
@@ -188,6 +209,12 @@ struct sw2d_handle {
     sw2d::DdpState* ddp = nullptr;      // DDP model: tables, divergence-correction scratch
     sw2d::ResultWriter* result = nullptr;   // binary map file (sw2d_result_open)
     sw2d::ClosureState* closure = nullptr;  // learned momentum-exchange closure (sw2d_set_closure)
+    sw2d::TileMesh tiles{};             // tiles of the fused step (SP and DIP models)
+    std::vector<void*> tile_allocs;     // device arrays of the tiles
+    std::vector<int2> h_coff, h_cint, h_lr;  // host tables the tiles are built from
+    std::vector<int> h_bcell;
+    int fused = 0;                      // step as the two kernels k_flux + k_update (option "fused_step")
+    int flux_variant = 0;               // launch variant of k_flux (sw2d_autotune)
     std::string err;
 };
 
@@ -237,6 +264,15 @@ void launch_cfl_on(sw2d_handle* h, const DevMesh& m);
 void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance);
 // One whole time step of the handle (its four kernels, its launch variants) on its stream.
 void launch_step_on(sw2d_handle* h);
+
+// The fused step's flux kernel (sw2d_tile.cu) on the handle's stream with launch variant v; with
+// attr_only only its shared-memory attribute is set (before a graph capture).  The tiles are
+// built by tiles_build from the internal-numbering tables.
+cudaError_t launch_flux(sw2d_handle* h, const DevMesh& m, int v, bool attr_only);
+int flux_variants();
+std::string flux_variant_label(int v);
+int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector<int2>& cint,
+                const std::vector<int2>& lr, const std::vector<int>& bcell, int tile_cells, std::string& why);
 
 // The CFL kernel with the DDP model's map-storage snap (swDdpHyp.cpp:588-600).
 void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m);

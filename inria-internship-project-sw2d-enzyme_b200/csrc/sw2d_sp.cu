@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <mutex>
@@ -543,6 +544,8 @@ int status_to_code(sw2d_handle* h, unsigned st)
 
 namespace {
 
+constexpr int kDefaultTileCells = 512;  // cells per tile of the fused step
+
 // Launch variants {threads per block, minimum resident blocks per SM (register cap)} of the
 // two heaviest kernels; sw2d_autotune times them on the live state and keeps the fastest.
 struct Variant {
@@ -645,7 +648,11 @@ void launch_update_s(sw2d_handle* h, const DevMesh& m)
     else launch_update_d<kStoreB, false>(h, m);
 }
 
-// phase i of one step on the handle's stream: 0 slopes, 1 edges, 2 cfl, 3 update
+// kernels of one step: the fused step's k_flux and k_update, or the four-kernel step
+int n_phases(const sw2d_handle* h) { return h->fused ? 2 : 4; }
+
+// phase i of one step on the handle's stream: fused step 0 flux, 1 update; four-kernel step (and
+// DDP) 0 slopes, 1 edges, 2 cfl, 3 update
 void launch_phase(sw2d_handle* h, int i)
 {
     if (h->model == kModelDdp) {
@@ -653,6 +660,11 @@ void launch_phase(sw2d_handle* h, int i)
         return;
     }
     DevMesh& m = h->m;
+    if (h->fused) {
+        if (i == 0) launch_flux(h, m, h->flux_variant, false);
+        else launch_update_s<false>(h, m);
+        return;
+    }
     switch (i) {
         case 0:
             if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) launch_slopes(h, h->slope_variant);
@@ -665,8 +677,18 @@ void launch_phase(sw2d_handle* h, int i)
 
 void launch_step(sw2d_handle* h)
 {
-    for (int i = 0; i < 4; i++) launch_phase(h, i);
+    for (int i = 0; i < n_phases(h); i++) launch_phase(h, i);
     if (h->result) result_after_step(h);
+}
+
+// host-side set-up a step's launches need before they are captured in a graph
+int prepare_step(sw2d_handle* h)
+{
+    if (h->fused) {
+        const cudaError_t e = launch_flux(h, h->m, h->flux_variant, true);
+        if (e != cudaSuccess) return fail(h, SW2D_E_CUDA, std::string("k_flux attributes: ") + cudaGetErrorString(e));
+    }
+    return SW2D_OK;
 }
 
 }  // namespace
@@ -703,6 +725,8 @@ int ensure_graph(sw2d_handle* h, int steps)
         cudaGraphExecDestroy(h->graph);
         h->graph = nullptr;
     }
+    const int rc = prepare_step(h);
+    if (rc) return rc;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < steps; i++) launch_step(h);
@@ -1083,7 +1107,7 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     m.coef = coef_d;
     // persistent balance slots start at zero, like the reference's resized flux vectors
     if ((rc = dev_alloc(h, nslot, &m.slot)) || (rc = dev_alloc(h, nslot, &m.slot_w)) ||
-        (rc = dev_alloc(h, nc, &m.slope)) || (rc = dev_alloc(h, grid_for(nc) + 1, &m.part)) ||
+        (rc = dev_alloc(h, nc, &m.slope)) || (rc = dev_alloc(h, nc / 32 + grid_for(nc) + 2, &m.part)) ||
         (rc = dev_alloc(h, 3 * nc, &h->stage)))
         return bail(rc);
     m.flux = nullptr;
@@ -1119,6 +1143,19 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     k_edge_coefficients<<<grid_for(ni + nb), kBlock, 0, h->stream>>>(m, coef_d, bgeo_d);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return bail(fail(h, SW2D_E_CUDA, "initialisation kernels failed"));
+    if (!ddp) {
+        // tiles of the fused step; a mesh whose tiles do not fit (16-bit local indices, shared
+        // memory) keeps the four-kernel step
+        std::string why;
+        int tc = kDefaultTileCells;
+        if (const char* env = std::getenv("SW2D_TILE_CELLS")) tc = std::atoi(env);
+        h->h_coff = coff;
+        h->h_cint = cint;
+        h->h_lr = lr;
+        h->h_bcell = bcell;
+        if (tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, tc, why) == SW2D_OK) h->fused = 1;
+        h->err.clear();
+    }
     if (ddp) {
         if ((rc = ddp_setup(h, mesh, fields, ddp, h0, q0, r0))) return bail(rc);
         CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
@@ -1153,6 +1190,7 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
                 if ((rc = ensure_graph(h, chunk))) return rc;
                 CK(cudaGraphLaunch(h->graph, h->stream));
             } else {
+                if ((rc = prepare_step(h))) return rc;
                 for (int64_t i = 0; i < k; i++) launch_step(h);
             }
             CK(cudaGetLastError());
@@ -1171,6 +1209,10 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
         int st = ensure_graph(h, chunk);
         if (st) return st;
         for (int64_t i = 0; i < full; i++) CK(cudaGraphLaunch(h->graph, h->stream));
+    }
+    if (rem > 0) {
+        int st = prepare_step(h);
+        if (st) return st;
     }
     for (int64_t i = 0; i < rem; i++) launch_step(h);
     CK(cudaGetLastError());
@@ -1218,12 +1260,16 @@ int sw2d_execute(sw2d_handle* h, int64_t* steps_done)
 int sw2d_phase_times(sw2d_handle* h, int64_t n_steps, double* ms, int capacity)
 {
     if (!h || !ms || n_steps <= 0) return fail(h, SW2D_E_ARG, "invalid arguments");
-    const int nph = 4;
-    if (capacity < nph) return fail(h, SW2D_E_ARG, "capacity < 4");
+    const int nph = (h->model == kModelDdp) ? 4 : n_phases(h);
+    if (capacity < nph) return fail(h, SW2D_E_ARG, "capacity below the number of phases");
     CK(cudaSetDevice(h->device));
-    cudaEvent_t ev[nph + 1];
+    {
+        const int rc = prepare_step(h);
+        if (rc) return rc;
+    }
+    cudaEvent_t ev[4 + 1];
     for (int i = 0; i <= nph; i++) CK(cudaEventCreate(&ev[i]));
-    double acc[nph] = {0, 0, 0, 0};
+    double acc[4] = {0, 0, 0, 0};
     for (int64_t s = 0; s < n_steps; s++) {
         for (int i = 0; i < nph; i++) {
             cudaEventRecord(ev[i], h->stream);
@@ -1252,6 +1298,13 @@ const char* sw2d_phase_name(int i)
     return (i >= 0 && i < 4) ? names[i] : "";
 }
 
+const char* sw2d_phase_label(sw2d_handle* h, int i)
+{
+    static const char* fused[] = {"k_flux", "k_update"};
+    if (h && h->model != kModelDdp && h->fused) return (i >= 0 && i < 2) ? fused[i] : "";
+    return sw2d_phase_name(i);
+}
+
 int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
 {
     if (!h || iters <= 0) return fail(h, SW2D_E_ARG, "invalid arguments");
@@ -1270,8 +1323,36 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
         cudaEventElapsedTime(&ms, e0, e1);
         return (double)ms / iters;
     };
-    // k_slopes and k_edges recompute the same outputs from the same state every time they run
-    // (slopes, balance slots, CFL contributions), so timing them does not advance the run.
+    // k_flux, k_slopes and k_edges recompute the same outputs from the same state every time they
+    // run (slopes, balance slots, CFL contributions, the pending dt), so timing them does not
+    // advance the run.
+    if (h->fused) {
+        double best = 1e300;
+        for (int v = 0; v < flux_variants(); v++) {
+            if (launch_flux(h, h->m, v, true) != cudaSuccess) continue;
+            double ms = time_it([&] { launch_flux(h, h->m, v, false); });
+            rep += "k_flux/" + flux_variant_label(v) + "=" + std::to_string(ms) + "ms ";
+            if (ms < best) {
+                best = ms;
+                h->flux_variant = v;
+            }
+        }
+        launch_flux(h, h->m, h->flux_variant, false);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->graph) {
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+        }
+        rep += "chosen k_flux/" + flux_variant_label(h->flux_variant) + " tile " + std::to_string(h->tiles.tile_cells);
+        if (report && capacity > 0) {
+            std::strncpy(report, rep.c_str(), (size_t)capacity - 1);
+            report[capacity - 1] = '\0';
+        }
+        return SW2D_OK;
+    }
     if (h->p.scheme == SW2D_SCHEME_MUSCL_EVR) {
         double best = 1e300;
         for (int v = 0; v < kNumVariants; v++) {
@@ -1387,6 +1468,24 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         if (!h->closure) return fail(h, SW2D_E_ARG, "no closure attached");
         if (value < 0 || value > 8) return fail(h, SW2D_E_ARG, "closure_ctas_per_sm outside 0..8");
         closure_set_ctas(h, (int)value);
+    } else if (std::strcmp(name, "fused_step") == 0) {
+        // 1: the step as k_flux + k_update (the default for the SP and DIP models); 0: the
+        // four-kernel step k_slopes, k_edges, k_cfl, k_update (the same results)
+        if (value && !h->tiles.ntiles) return fail(h, SW2D_E_UNSUPPORTED, "this handle has no tiles (DDP model)");
+        h->fused = value ? 1 : 0;
+    } else if (std::strcmp(name, "tile_cells") == 0) {
+        // cells per tile of the fused step (32..8192): the tiles are rebuilt
+        if (h->model == kModelDdp) return fail(h, SW2D_E_UNSUPPORTED, "the DDP model has no tiles");
+        CK(cudaStreamSynchronize(h->stream));
+        std::string why;
+        const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, (int)value, why);
+        if (rc) {
+            if (!h->tiles.ntiles) h->fused = 0;  // the previous tiles are kept unless they were released
+            return fail(h, rc, "tile_cells: " + (why.empty() ? h->err : why));
+        }
+    } else if (std::strcmp(name, "flux_variant") == 0) {
+        if (value < 0 || value >= flux_variants()) return fail(h, SW2D_E_ARG, "flux_variant outside the variants");
+        h->flux_variant = (int)value;
     } else if (std::strcmp(name, "adjoint_edge_variant") == 0) {
         if (value < 0 || value > 4) return fail(h, SW2D_E_ARG, "adjoint_edge_variant outside 0..4");
         h->adj_edge_variant = (int)value;
@@ -1399,6 +1498,18 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         h->graph = nullptr;
     }
     CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
+int sw2d_get_option(sw2d_handle* h, const char* name, int64_t* value)
+{
+    if (!h || !name || !value) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (std::strcmp(name, "fused_step") == 0) *value = h->fused;
+    else if (std::strcmp(name, "flux_variant") == 0) *value = h->flux_variant;
+    else if (std::strcmp(name, "tile_cells") == 0) *value = h->tiles.tile_cells;
+    else if (std::strcmp(name, "record_fluxes") == 0) *value = h->m.flux != nullptr;
+    else if (std::strcmp(name, "record_wave_speeds") == 0) *value = h->m.lmax != nullptr;
+    else return fail(h, SW2D_E_ARG, std::string("option not readable: ") + name);
     return SW2D_OK;
 }
 
@@ -1492,6 +1603,10 @@ int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t ca
         const int64_t r = ddp_get_array(h, name, out, capacity, &handled);
         if (handled) return r;
     }
+    if (h->fused && !h->m.flux && !h->m.lmax &&
+        (std::strcmp(name, "slope_x") == 0 || std::strcmp(name, "slope_y") == 0))
+        return fail(h, SW2D_E_ARG, "the fused step keeps the slopes only with the option record_fluxes or "
+                                   "record_wave_speeds on");
     struct Entry {
         const char* n;
         const double* p;
@@ -1643,6 +1758,7 @@ int sw2d_kernels_per_step(sw2d_handle* h)
 {
     if (!h) return 0;
     if (h->model == kModelDdp) return ddp_kernels_per_step(h);
+    if (h->fused) return 2;
     return h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3;
 }
 
@@ -1684,6 +1800,7 @@ int sw2d_destroy(sw2d_handle* h)
     closure_release(h);
     result_release(h);
     for (void* p : h->allocs) cudaFree(p);
+    for (void* p : h->tile_allocs) cudaFree(p);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -46,6 +46,7 @@ class SpModel:
     def __init__(self, case: Case, device: int = 0):
         self.lib = capi.load_library()
         self.case = case
+        self.device = int(device)
         self.n = case.mesh.cell_nb
         self.ni = case.mesh.edge_int_nb
         self.nb = case.mesh.edge_bnd_nb
@@ -216,7 +217,12 @@ class SpModel:
         k = self.lib.sw2d_phase_times(self.handle, int(n_steps), ms.ctypes.data_as(capi.c_double_p), ms.size)
         if k < 0:
             self._check(int(k))
-        return {self.lib.sw2d_phase_name(i).decode(): float(ms[i]) for i in range(k)}
+        return {self.lib.sw2d_phase_label(self.handle, i).decode(): float(ms[i]) for i in range(k)}
+
+    def get_option(self, name: str) -> int:
+        v = ctypes.c_int64(0)
+        self._check(self.lib.sw2d_get_option(self.handle, name.encode(), ctypes.byref(v)))
+        return int(v.value)
 
     def set_option(self, name: str, value: int) -> None:
         self._check(self.lib.sw2d_set_option(self.handle, name.encode(), int(value)))

@@ -1,9 +1,10 @@
 """Launch-configuration autotuner with a persistent JSON cache.
 
 ``autotune(model)`` asks the library (sw2d_autotune) to time every {threads per block,
-register cap} variant of the slope and edge kernels on the model's current state and keeps
-the fastest; the choice is stored in a JSON file keyed by GPU, scheme, options and mesh size
-(power-of-two bucket), and reused by later runs without timing again.
+register cap} variant of the step's heaviest kernels on the model's current state (k_flux for
+the fused step; k_slopes and k_edges for the four-kernel step) and keeps the fastest; the
+choice is stored in a JSON file keyed by GPU, scheme, options, step kind, tile size and mesh
+size (power-of-two bucket), and reused by later runs without timing again.
 """
 from __future__ import annotations
 
@@ -29,7 +30,8 @@ def _key(model, device: int) -> str:
     bucket = int(math.log2(max(1, model.n)))
     return "|".join([_device_name(device), str(o.get("model_hyperb", "sp")), str(o.get("num_scheme", "godunov")),
                      str(o.get("topo_discretization", "discontinuous")), str(o.get("model_friction", "none")),
-                     str(o.get("model_singular_head_loss", "none")), f"2^{bucket}"])
+                     str(o.get("model_singular_head_loss", "none")), f"2^{bucket}",
+                     f"fused{model.get_option('fused_step')}", f"tile{model.get_option('tile_cells')}"])
 
 
 def _load(path: str) -> Dict[str, dict]:
@@ -47,12 +49,15 @@ def autotune(model, iters: int = 10, device: int = 0, cache_path: Optional[str] 
     if not force and key in db:
         e = db[key]
         model._check(model.lib.sw2d_set_launch_config(model.handle, int(e["slopes"]), int(e["edges"])))
+        if "flux" in e and model.get_option("fused_step"):
+            model.set_option("flux_variant", int(e["flux"]))
         return {**e, "cached": True}
     buf = ctypes.create_string_buffer(4096)
     model._check(model.lib.sw2d_autotune(model.handle, int(iters), buf, len(buf)))
     sv, ev = ctypes.c_int(), ctypes.c_int()
     model._check(model.lib.sw2d_get_launch_config(model.handle, ctypes.byref(sv), ctypes.byref(ev)))
-    entry = {"slopes": sv.value, "edges": ev.value, "report": buf.value.decode()}
+    entry = {"slopes": sv.value, "edges": ev.value, "flux": model.get_option("flux_variant"),
+             "report": buf.value.decode()}
     if cache_path:
         db[key] = entry
         try:

@@ -97,9 +97,9 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
                    initial: str = "lake") -> Case:
     """The large SP forward solve.  ``initial="lake"``: h = max(0, 2 - z_b), the configuration's
     initial state (a lake at rest between dry bumps: most of the domain is dry and the wet part
-    does not move).  ``initial="dam"``: the same bed under a dam break, free surface 3.5 m for
-    x < 1000 m and 2.2 m beyond, water at rest: a moving, mostly wet flow with wet/dry fronts
-    around the bumps.  ``mesh="delaunay"``: the seeded jittered-Delaunay mesh."""
+    does not move).  ``initial="dam"``: the same bed under a dam break, free surface 5.0 m for
+    x < 1000 m and 3.5 m beyond, water at rest: a moving flow over about 80 % of the cells, with
+    wet/dry fronts around the tallest bumps.  ``mesh="delaunay"``: the seeded jittered-Delaunay mesh."""
     kind = mesh
     L = 2000.0
     rng = np.random.default_rng(seed_bed)
@@ -120,7 +120,7 @@ def gaussian_bumps(n_cells: int = 4_000_000, scheme: str = "muscl_evr", t_max: f
     if initial == "lake":
         zs = np.full(n, 2.0)
     elif initial == "dam":
-        zs = np.where(mesh.cell_x < 0.5 * L, 3.5, 2.2)
+        zs = np.where(mesh.cell_x < 0.5 * L, 5.0, 3.5)
     else:
         raise ValueError(f"initial {initial!r}: 'lake' or 'dam'")
     h0 = np.where(zs - mesh.cell_z_b < 0.0, 0.0, zs - mesh.cell_z_b)   # std::max(z - z_b, 0.0)

@@ -162,3 +162,54 @@ def test_gpu_full_size_properties(pkg):
     again.step(3)
     for x, y in zip(again.state(), got):
         assert np.array_equal(x.view(np.int64), y.view(np.int64))
+
+
+def test_gpu_c1_dam_break_delaunay_1000_steps(pkg, tmp_path):
+    """The plain SP dam break configuration at its stated size: ~20k cells of a seeded
+    jittered-Delaunay mesh in a randomly permuted numbering, flat bed, h = 1.0 / 0.1 m, phi ~
+    U[0.6, 1], Manning n = 0.03, MUSCL-EVR + the reference's limiter + HLLC, CFL 0.9, walls,
+    1000 steps.  Against the reference's own solver run here on the same case folder: bit for bit
+    with the reference linked with the portable exp/log, within 1e-10 relative of the reference
+    linked with glibc (a dam break on a flat bed is insensitive to the last bit of exp/log)."""
+    case = pkg.workloads.dam_break(n_cells=20000, mesh="delaunay")
+    assert 19000 <= case.mesh.cell_nb <= 21000
+    if not oracle_binding.reference_available():
+        pytest.skip("the reference solver library (oracle/_ref) is not built")
+    folder = str(tmp_path / "c1")
+    pkg.write_case(folder, case)
+    model = pkg.SpModel(case)
+    assert model.step(1000) == 1000
+    got = model.state()
+    ref_pm = oracle_binding.RefSolver(folder, portable_math=True)
+    assert ref_pm.step(1000) == 1000
+    assert model.t == ref_pm.t
+    assert_state_close(got, ref_pm.state(), True, "C1 vs reference(portable libm)")
+    ref = oracle_binding.RefSolver(folder)
+    assert ref.step(1000) == 1000
+    assert_state_close(got, ref.state(), False, "C1 vs reference(glibc)")
+    assert got[0].min() >= 0.0 and np.all(np.isfinite(got[0]))
+
+
+@pytest.mark.parametrize("n_cells,steps", [(1_000_000, 200), (4_000_000, 200)])
+def test_gpu_c2_moving_bumps_vs_oracle(pkg, n_cells, steps):
+    """The large SP forward solve's bed under a dam break (free surface 5.0 m for x < 1 km, 3.5 m
+    beyond, at rest): a moving, mostly wet flow with wet/dry fronts around the bumps, on the
+    jittered-Delaunay mesh, `steps` steps bit for bit against the CPU oracle, with the stored
+    volume sum(phi A h) conserved to round-off (closed basin)."""
+    case = pkg.workloads.gaussian_bumps(n_cells=n_cells, mesh="delaunay", initial="dam")
+    model = pkg.SpModel(case)
+    w = case.phi * case.mesh.cell_area
+    h0 = model.state()[0]
+    wet0 = float(np.mean(h0 > 1e-5))
+    assert wet0 > 0.75, f"the moving case should be mostly wet ({wet0:.2f})"
+    v0 = float(np.sum(w * h0))
+    assert model.step(steps) == steps
+    got = model.state()
+    o = oracle_binding.SpOracle(case, portable_math=True)
+    assert o.step(steps) == steps
+    assert model.time == (o.t, o.dt)
+    assert_state_close(got, o.state(), True, f"moving bumps {n_cells} cells, {steps} steps")
+    moved = float(np.mean(np.abs(got[1]) + np.abs(got[2]) > 1e-6))
+    assert moved > 0.1, f"the flow should be moving ({moved:.2f} of the cells)"
+    v1 = float(np.sum(w * got[0]))
+    assert abs(v1 - v0) / v0 < 1e-11, f"stored volume drifted by {abs(v1 - v0) / v0:.2e}"
