@@ -48,6 +48,11 @@ def _args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=4_000_000)
+    ap.add_argument("--mesh", choices=["delaunay", "grid"], default="delaunay",
+                    help="seeded jittered-Delaunay mesh in a random numbering (the configuration's), or the "
+                         "jittered grid split into triangles")
+    ap.add_argument("--wet-steps", type=int, default=100,
+                    help="timed steps of the moving (dam-break) variant of the workload (0: skip)")
     ap.add_argument("--e2e-chunk", type=int, default=50, help="time steps per state upload/download in e2e")
     ap.add_argument("--cpu-steps", type=int, default=150, help="timed steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -90,6 +95,7 @@ def _args():
 def _config(args, world):
     return {"workload": f"SP gaussian-bumps forward solve, {args.cells} cells (2 km x 2 km), MUSCL-EVR + HLLC, "
                         "Manning, FP64", "cells": args.cells, "scheme": "muscl_evr", "friction": "manning",
+            "mesh": args.mesh,
             "global_cells": args.cells * world, "parallelism": f"replicas{world}" if world > 1 else "single",
             "l2": "inputs larger than L2 (state + mesh tables ~0.9 GB per replica)"}
 
@@ -243,6 +249,40 @@ def _traffic_per_step():
         except ValueError:
             return None
     return None
+
+
+def run_wet(pkg, args, local_rank):
+    """The same bed, mesh and parameters under a dam break (free surface 5.0 m for x < 1 km,
+    3.5 m beyond, at rest): a moving flow over most of the domain, with wet/dry fronts, timed like
+    the headline (graph-launched steps, CUDA events on the library's stream) after 20 steps of
+    motion."""
+    import numpy as np
+    import torch
+
+    case = pkg.workloads.gaussian_bumps(n_cells=args.cells, mesh=args.mesh, initial="dam")
+    model = pkg.SpModel(case, device=local_rank)
+    tune = pkg.tuning.autotune(model, iters=3, device=local_rank, cache_path=None)
+    stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
+    model.step(20)
+    phases = model.phase_times(5)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done = model.step(args.wet_steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    n = case.mesh.cell_nb
+    h = model.state()[0]
+    step_ms = ms / max(done, 1)
+    peak, peak_kind = _measured_peak()
+    achieved = ALGO_BYTES_PER_CELL_UPDATE * n / (step_ms / 1e3) / 1e9
+    return {"workload": f"gaussian-bumps bed under a dam break, {n} cells, MUSCL-EVR + HLLC, Manning, FP64",
+            "metric": METRIC, "value": n * done / (ms / 1e3), "unit": UNIT, "steps": done, "ms_per_step": step_ms,
+            "wet_fraction_initial": float(np.mean(case.h0 > float(case.opts["h_min"]))),
+            "wet_fraction_after": float(np.mean(h > float(case.opts["h_min"]))),
+            "roofline_frac": achieved / peak, "peak_kind": peak_kind, "phases_ms": phases,
+            "launch_config": tune["report"]}
 
 
 def run_adjoint(pkg, args, local_rank):
@@ -828,10 +868,11 @@ def run_ours(args, rank, world, local_rank):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
-    case = pkg.workloads.gaussian_bumps(n_cells=args.cells)
+    case = pkg.workloads.gaussian_bumps(n_cells=args.cells, mesh=args.mesh)
     model = pkg.SpModel(case, device=local_rank)
     stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
     n = case.mesh.cell_nb
+    dry_fraction = float(np.mean(case.h0 <= float(case.opts["h_min"])))
 
     def barrier():
         if dist is not None:
@@ -902,6 +943,8 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank != 0:
         return
+    del model
+    wet = None if (args.wet_steps <= 0 or world > 1) else run_wet(pkg, args, local_rank)
     adjoint = None if (args.no_adjoint or world > 1) else run_adjoint(pkg, args, local_rank)
     dip = None if (args.dip_cells <= 0 or world > 1) else run_dip(pkg, args, local_rank)
     ddp = None if (args.ddp_cells <= 0 or world > 1) else run_ddp(pkg, args, local_rank)
@@ -927,7 +970,8 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Gaussian-bump bed, smooth porosity field, lognormal Manning n)",
-        "config": _config(args, world),
+        "config": {**_config(args, world), "dry_fraction": dry_fraction,
+                   "initial_state": "lake at rest h = max(0, 2 - z_b): dry cells and still water"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * n / chunk,
                 "d2h_bytes_per_step": (3 * 8 * n + 2 * 48) / chunk,
                 "note": f"sw2d_set_state + sw2d_step_n({chunk}) + sw2d_get_state from pinned host buffers per chunk"},
@@ -943,6 +987,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if wet is not None:
+        line["wet"] = wet
     if adjoint is not None:
         line["adjoint"] = adjoint
     if dip is not None:
