@@ -448,12 +448,17 @@ int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n);
  * arrays in host memory).  For callers that must not allocate device memory once their run has
  * started: it stages the array in a fixed buffer compiled into the library (2^20 doubles =
  * 8 MiB, held by every GPU that loads the library until the process exits) instead of a
- * buffer allocated per call.  Arrays longer than 2^20 values are rejected with SW2D_E_ARG and
- * a message naming the limit (use sw2d_get_array for them).  The first call on a device looks
- * up the buffer's device address (cudaGetSymbolAddress) for that device; make that first call
- * before any stream capture.  All calls share the one buffer: calls that overlap on the GPU
- * (from several threads or handles on the same device) race; this call returns only after its
- * copy has completed. */
+ * buffer allocated per call.  It serves the same names as sw2d_get_array, the DDP model's map
+ * outputs ("water_depth", "unit_discharge_x", "unit_discharge_y", "surface_elevation",
+ * "thetaG_int_hmin") included.  Arrays longer than 2^20 values are rejected with SW2D_E_ARG and
+ * a message naming the limit (use sw2d_get_array for them).  The buffer's device address is
+ * looked up (cudaGetSymbolAddress) once per device, by sw2d_create, sw2d_create_dip and
+ * sw2d_create_ddp when they make a handle on that device, so this call itself does no set-up
+ * for a handle made by them; the address stays cached for the life of the process, so after
+ * cudaDeviceReset (or anything else that destroys the device's primary context) this entry
+ * point must not be used again in that process.  All calls share the one buffer: calls that
+ * overlap on the GPU (from several threads or handles on the same device) race; this call
+ * returns only after its copy has completed. */
 int64_t sw2d_get_array_noalloc(sw2d_handle* h, const char* name, double* out, int64_t capacity);
 
 /* ---- Adjoint: gradient of an observation misfit along a recorded trajectory ----------------

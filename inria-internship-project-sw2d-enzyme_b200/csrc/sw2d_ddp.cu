@@ -760,6 +760,23 @@ __global__ void k_ddp_outputs(DevMesh m, double* out)
     out[3 * m.nc + c] = s.w;
 }
 
+// one storeResultMaps output of k_ddp_outputs (0 h, 1 q, 2 r, 3 z) per cell, written straight to
+// the caller's numbering: out[perm[c]]
+__global__ void k_ddp_output_field(DevMesh m, int which, const int* __restrict__ perm, double* out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const double4 s = m.st[c];
+    const double4 cs = m.cst[c];
+    const double h = smax(0.0, s.w - cs.z);
+    double u = 0.0, v = 0.0;
+    if (s.x > kSmallReal) {
+        u = s.y / s.x;
+        v = s.z / s.x;
+    }
+    out[perm[c]] = which == 0 ? h : which == 1 ? u * h : which == 2 ? v * h : s.w;
+}
+
 // out[perm[i]] = src[i * stride + offset]
 __global__ void k_scatter_field(const double* __restrict__ src, int stride, int offset, const int* __restrict__ perm,
                                 double* out, int n)
@@ -1274,6 +1291,39 @@ int64_t ddp_get_array(sw2d_handle* h, const char* name, double* out, int64_t cap
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, stage, len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return len;
+}
+
+// ddp_get_array through a device staging buffer the caller supplies (stage_cap doubles), with no
+// allocation; arrays longer than stage_cap are rejected.
+int64_t ddp_get_array_staged(sw2d_handle* h, const char* name, double* out, int64_t capacity, double* stage,
+                             int64_t stage_cap, bool* handled)
+{
+    *handled = false;
+    static const char* names[] = {"water_depth", "unit_discharge_x", "unit_discharge_y", "surface_elevation"};
+    int which = -1;
+    for (int i = 0; i < 4; i++)
+        if (std::strcmp(name, names[i]) == 0) which = i;
+    const bool hmin = std::strcmp(name, "thetaG_int_hmin") == 0;
+    if (which < 0 && !hmin) return 0;
+    *handled = true;
+    const int64_t len = hmin ? h->ni : h->nc;
+    if (capacity < len) return fail(h, SW2D_E_ARG, "output buffer too small");
+    if (len > stage_cap)
+        return fail(h, SW2D_E_ARG, std::string("sw2d_get_array_noalloc: ") + name + " has " + std::to_string(len) +
+                                       " values, more than the fixed staging array holds (" +
+                                       std::to_string(stage_cap) + "); use sw2d_get_array");
+    CK(cudaSetDevice(h->device));
+    if (len > 0) {
+        if (hmin)
+            k_scatter_field<<<grid_for(h->ni), kBlock, 0, h->stream>>>(reinterpret_cast<const double*>(h->m.des), 8, 0,
+                                                                        h->d_int_perm, stage, (int)h->ni);
+        else
+            k_ddp_output_field<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, which, h->d_cell_perm, stage);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, stage, len * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
     CK(cudaStreamSynchronize(h->stream));
     return len;
 }

@@ -350,6 +350,11 @@ void launch_ddp_edges(sw2d_handle* h, const DevMesh& m, int variant);
 void ddp_variant(int v, int* block, int* minb);
 int ddp_kernels_per_step(sw2d_handle* h);
 int64_t ddp_get_array(sw2d_handle* h, const char* name, double* out, int64_t capacity, bool* handled);
+int64_t ddp_get_array_staged(sw2d_handle* h, const char* name, double* out, int64_t capacity, double* stage,
+                             int64_t stage_cap, bool* handled);
+// Looks up the device address of the no-allocation staging array on the handle's device (done
+// by the create functions, so that sw2d_get_array_noalloc itself never needs to).
+int noalloc_prepare(sw2d_handle* h);
 int64_t ddp_get_table(sw2d_handle* h, int which, int64_t record, double* z, double* phi, double* theta,
                       int64_t capacity);
 int ddp_derive(sw2d_handle* h);

@@ -1143,6 +1143,7 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     k_edge_coefficients<<<grid_for(ni + nb), kBlock, 0, h->stream>>>(m, coef_d, bgeo_d);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return bail(fail(h, SW2D_E_CUDA, "initialisation kernels failed"));
+    if ((rc = noalloc_prepare(h))) return bail(rc);
     if (!ddp) {
         // tiles of the fused step; a mesh whose tiles do not fit (16-bit local indices, shared
         // memory) keeps the four-kernel step
@@ -1690,9 +1691,36 @@ int noalloc_stage(sw2d_handle* h, int device, double** out)
 
 }  // namespace
 
+}  // extern "C"
+
+namespace sw2d {
+
+int noalloc_prepare(sw2d_handle* h)
+{
+    double* stage = nullptr;
+    return noalloc_stage(h, h->device, &stage);
+}
+
+}  // namespace sw2d
+
+extern "C" {
+
 int64_t sw2d_get_array_noalloc(sw2d_handle* h, const char* name, double* out, int64_t capacity)
 {
     if (!h || !name || !out) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (h->model == kModelDdp) {  // the DDP model's map outputs, computed straight into the staging array
+        CK(cudaSetDevice(h->device));
+        double* stage = nullptr;
+        const int st = noalloc_stage(h, h->device, &stage);
+        if (st) return st;
+        bool handled = false;
+        const int64_t r = ddp_get_array_staged(h, name, out, capacity, stage, kNoAllocMaxDoubles, &handled);
+        if (handled) return r;
+    }
+    if (h->fused && !h->m.flux && !h->m.lmax &&
+        (std::strcmp(name, "slope_x") == 0 || std::strcmp(name, "slope_y") == 0))
+        return fail(h, SW2D_E_ARG, "the fused step keeps the slopes only with the option record_fluxes or "
+                                   "record_wave_speeds on");
     struct Entry {
         const char* n;
         const double* p;
