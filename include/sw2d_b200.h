@@ -676,6 +676,14 @@ int sw2d_assim_steps(sw2d_handle* h, double* dt, int32_t* obs_trig, int64_t capa
  * trajectory, its first checkpoint too (time steps, boundary values and triggers stay frozen). */
 int sw2d_assim_set_start(sw2d_handle* h, const double* water_depth, const double* unit_discharge_x,
                          const double* unit_discharge_y);
+/* The states the reference's gen-ref-e mode writes (swSpE::generate_references_E,
+ * assim/swSpE_checkpoint.cpp:470-515, with storeReferenceMap at each observation trigger,
+ * :360-375): the recorded trajectory replayed at control m from its start state, and for each
+ * observation k that a step lands on, the state after that step, caller numbering, at
+ * [k * n_cells].  n_written receives the number of observations a step landed on; the rows of
+ * the others are left as they were.  Needs a recorded trajectory (sw2d_assim_record). */
+int sw2d_assim_trigger_states(sw2d_handle* h, const double* m, double* water_depth, double* unit_discharge_x,
+                              double* unit_discharge_y, int64_t n_obs_capacity, int64_t* n_written);
 /* Checkpoint k (the state at the start of segment k), caller numbering. */
 int sw2d_assim_checkpoint(sw2d_handle* h, int64_t k, double* water_depth, double* unit_discharge_x,
                           double* unit_discharge_y);

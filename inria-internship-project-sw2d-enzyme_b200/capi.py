@@ -428,6 +428,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_assim_set_start.restype = ctypes.c_int
     lib.sw2d_assim_checkpoint.argtypes = [P, ctypes.c_int64, c_double_p, c_double_p, c_double_p]
     lib.sw2d_assim_checkpoint.restype = ctypes.c_int
+    lib.sw2d_assim_trigger_states.argtypes = [P, c_double_p, c_double_p, c_double_p, c_double_p, ctypes.c_int64,
+                                              ctypes.POINTER(ctypes.c_int64)]
+    lib.sw2d_assim_trigger_states.restype = ctypes.c_int
     _LIB = lib
     return lib
 
@@ -450,7 +453,7 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_batch_create", "sw2d_batch_step_n", "sw2d_batch_adjoint", "sw2d_batch_size",
             "sw2d_batch_destroy", "sw2d_batch_last_error", "sw2d_assim_configure", "sw2d_assim_set_observations",
             "sw2d_assim_record", "sw2d_assim_replay_cost", "sw2d_assim_gradient", "sw2d_assim_segments",
-            "sw2d_assim_steps", "sw2d_assim_checkpoint", "sw2d_assim_set_start"]
+            "sw2d_assim_steps", "sw2d_assim_checkpoint", "sw2d_assim_set_start", "sw2d_assim_trigger_states"]
 
 
 class CaseFolder:

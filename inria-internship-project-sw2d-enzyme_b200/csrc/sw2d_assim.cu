@@ -1534,6 +1534,41 @@ int sw2d_assim_set_start(sw2d_handle* h, const double* water_depth, const double
     return SW2D_OK;
 }
 
+int sw2d_assim_trigger_states(sw2d_handle* h, const double* m, double* water_depth, double* unit_discharge_x,
+                              double* unit_discharge_y, int64_t n_obs_capacity, int64_t* n_written)
+{
+    int rc = require(h, true);
+    if (rc) return rc;
+    if (!m || !water_depth || !unit_discharge_x || !unit_discharge_y || n_obs_capacity < 0)
+        return fail(h, SW2D_E_ARG, "invalid arguments");
+    AssimState* a = h->assim;
+    if (n_obs_capacity < a->n_obs) return fail(h, SW2D_E_ARG, "capacity below the number of observations");
+    CK(cudaSetDevice(h->device));
+    if ((rc = set_control(h, m, false))) return rc;
+    const int64_t nc = h->nc;
+    // the recorded trajectory from its start state (swSpE::reset_to_start), step by step with the
+    // frozen dt and boundary times; the state after a step that lands on observation k is what
+    // storeReferenceMap writes at that time (swSpE_checkpoint.cpp:360-375)
+    CK(cudaMemcpyAsync(h->m.st, a->st0, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    int64_t written = 0;
+    for (const AssimSegment& sg : a->segs)
+        for (int64_t j = sg.j0; j < sg.j0 + sg.n; j++) {
+            replay_step(h, j, nullptr);
+            const int k = a->trig[j];
+            if (k < 0 || k >= a->n_obs) continue;
+            const double* src = reinterpret_cast<const double*>(h->m.st);
+            if ((rc = scatter(h, src, 4, 0, water_depth + k * nc)) ||
+                (rc = scatter(h, src, 4, 1, unit_discharge_x + k * nc)) ||
+                (rc = scatter(h, src, 4, 2, unit_discharge_y + k * nc)))
+                return rc;
+            written++;
+        }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    if (n_written) *n_written = written;
+    return SW2D_OK;
+}
+
 int sw2d_assim_checkpoint(sw2d_handle* h, int64_t k, double* water_depth, double* unit_discharge_x,
                           double* unit_discharge_y)
 {

@@ -196,6 +196,46 @@ def load_map(path: str, n_cells: int) -> np.ndarray:
     return out
 
 
+def result_file_name(prefix: str, t: float) -> str:
+    """swIO::computeFileNameFromTime (src/common/swIO.cpp:51-87): prefix + DDDDdHHhMMmSSsmmm.txt,
+    the digits taken the way the reference computes them (truncations of float quotients, the
+    milliseconds rounded with +0.499999)."""
+    nb_d = int(t / 86400.)
+    nb_d_e3 = int(nb_d / 1000.)
+    nb_d_e2 = int((nb_d - 1000. * nb_d_e3) / 100.)
+    nb_d_e1 = int((nb_d - 1000. * nb_d_e3 - 100. * nb_d_e2) / 10.)
+    nb_d_e0 = int(nb_d - 1000. * nb_d_e3 - 100. * nb_d_e2 - 10. * nb_d_e1)
+    nb_h = int((t - float(np.float32(nb_d)) * 86400.) / 3600.)
+    nb_h_e1 = int(nb_h / 10.)
+    nb_h_e0 = int(nb_h - 10. * nb_h_e1)
+    nb_m = int((t - nb_d * 86400. - nb_h * 3600.) / 60.)
+    nb_m_e1 = int(nb_m / 10.)
+    nb_m_e0 = int(nb_m - 10. * nb_m_e1)
+    nb_s = int(t - 86400. * nb_d - 3600. * nb_h - 60. * nb_m)
+    nb_s_e1 = int(nb_s / 10.)
+    nb_s_e0 = int(nb_s - 10. * nb_s_e1)
+    nb_mill = int((t - int(t)) * 1000. + 0.499999)
+    nb_mill_e2 = int(nb_mill / 100.)
+    nb_mill_e1 = int((nb_mill - 100 * nb_mill_e2) / 10.)
+    nb_mill_e0 = int(nb_mill - 100 * nb_mill_e2 - 10 * nb_mill_e1)
+    return (f"{prefix}{nb_d_e3}{nb_d_e2}{nb_d_e1}{nb_d_e0}d{nb_h_e1}{nb_h_e0}h{nb_m_e1}{nb_m_e0}m"
+            f"{nb_s_e1}{nb_s_e0}s{nb_mill_e2}{nb_mill_e1}{nb_mill_e0}.txt")
+
+
+def write_map_decimal(path: str, names: Sequence[str], cols: Sequence[np.ndarray], precision: int) -> None:
+    """swIO::createTxtFileMapDecimal (src/common/swIO.cpp:182-222): a header of the names, each
+    padded with spaces to precision + 7 characters and followed by a tab, then one line per cell
+    of the values in scientific notation with `precision` digits, each followed by a tab."""
+    width = precision + 7
+    lines = ["".join(nm + " " * max(0, width - len(nm)) + "\t" for nm in names)]
+    fmt = f"{{:.{precision}e}}\t"
+    arrs = [np.asarray(c, dtype=np.float64) for c in cols]
+    for i in range(arrs[0].size):
+        lines.append("".join(fmt.format(float(a[i])) for a in arrs))
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+
+
 def resolve_weight(spec: str, folder: str, n_cells: int) -> np.ndarray:
     """swSpE::resolve_cost_weight (assim/swSpE_core.cpp:268-298): a number (uniform weight) or a
     map path relative to the case folder; an unreadable map gives weight 1."""
@@ -300,6 +340,66 @@ class SpE:
         g, info = self.model.assim_gradient(phi_map, stride or self.cfg.checkpoint_stride)
         self.diag = info
         return g
+
+    def observation_grid(self) -> np.ndarray:
+        """The observation times generate_references_E synthesises (swSpE_checkpoint.cpp:482-496):
+        the multiples of dt_map_ad in [t_state_assimilation, t_max] (1e-16 slack at both ends)."""
+        c = self.cfg
+        dt_ref = float(c.dt_map_ad)
+        if not dt_ref > 1e-16:
+            raise ValueError(f"generate_references_E: invalid dt_map_ad ({dt_ref})")
+        t_max = float(self.model.case.opts["t_max"])
+        k0 = max(0, int(math.ceil((c.t_state_assimilation - 1e-16) / dt_ref)))
+        times = []
+        k = k0
+        while True:
+            tt = float(k) * dt_ref
+            if tt > t_max + 1e-16:
+                break
+            if tt >= c.t_state_assimilation - 1e-16:
+                times.append(tt)
+            k += 1
+        if not times:
+            raise ValueError(f"generate_references_E: no observation time in [{c.t_state_assimilation}, {t_max}] "
+                             f"(dt_map_ad = {dt_ref})")
+        return np.array(times)
+
+    def generate_references_E(self, phi_map, out_dir: str, stride: Optional[int] = None) -> List[str]:
+        """The reference's gen-ref-e mode (swSpE::generate_references_E,
+        assim/swSpE_checkpoint.cpp:470-515): the _E forward (the dry run at control phi_map) on the
+        synthesised observation grid, and at every observation it lands on, the state written as
+        storeReferenceMap does (swSpE_core.cpp:300-340): out_dir/ResultHydro_p<time>.txt with the
+        columns x, y, zb, water_depth, unit_discharge_x, unit_discharge_y, unit_discharge_norm, in
+        n_decimal-digit scientific notation.  Returns the files written.  Replaying the same _E
+        trajectory at phi_map against these maps then gives J = 0 up to their printed digits."""
+        times = self.observation_grid()
+        n = self.n
+        self.set_frames(times, np.zeros((times.size, n)))
+        m = np.ascontiguousarray(phi_map, dtype=np.float64)
+        self.model.assim_record(m, stride or self.cfg.checkpoint_stride)
+        h, q, r, landed = self.model.assim_trigger_states(m, times.size)
+        dt, trig = self.model.assim_steps()
+        # the time after each step, accumulated as the engine does (t_{j+1} = t_j + dt_j)
+        t = float(self.model.assim_segments()[0][0]) if dt.size else 0.0
+        t_after = np.empty(dt.size)
+        for j in range(dt.size):
+            t = t + float(dt[j])
+            t_after[j] = t
+        mesh = self.model.case.mesh
+        digits = int(self.model.case.opts.get("n_decimal", 10))
+        os.makedirs(out_dir, exist_ok=True)
+        written = []
+        for j in np.nonzero(trig >= 0)[0]:
+            k = int(trig[j])
+            if k >= times.size:
+                continue
+            path = os.path.join(out_dir, result_file_name("ResultHydro_p", float(t_after[j])))
+            cols = [mesh.cell_x, mesh.cell_y, mesh.cell_z_b, h[k], q[k], r[k], np.sqrt(q[k] * q[k] + r[k] * r[k])]
+            write_map_decimal(path, ["x", "y", "zb", "water_depth", "unit_discharge_x", "unit_discharge_y",
+                                     "unit_discharge_norm"], cols, digits)
+            written.append(path)
+        self.diag["gen_ref_e"] = {"observations": int(times.size), "written": len(written), "landed": landed}
+        return written
 
     # ---- swSpE::phi_correct / dphi_dm / m_from_phi (assim/swSpE.h:59-107)
     def phi_correct(self, m) -> np.ndarray:
@@ -481,6 +581,48 @@ class PorosityProblem:
             self._csv = None
 
 
+def free_cells(spe: SpE, phi_start) -> np.ndarray:
+    """The cells the minimisation moves (swSpE::run_minimization, assim/swSpE_minimize.cpp:604-668).
+
+    * mask_dry_cells: a native forward run (swSp::execute) of the case to t_max with the
+      first-guess porosity; cells still dry at its end (h <= 1e-4) never see water, their
+      porosity has no observable effect and stays at the first guess.  Otherwise every cell.
+    * porosity_free_zone_map ("cell_id,value" or SW2D map, path relative to the case folder):
+      of those, only the cells whose value is below 0.5.  An unreadable map leaves the set as
+      it is (the reference logs an error and carries on); an empty zone is reported."""
+    cfg = spe.cfg
+    n = spe.n
+    if cfg.mask_dry_cells:
+        import dataclasses
+
+        case = dataclasses.replace(spe.model.case, phi=np.ascontiguousarray(phi_start, dtype=np.float64))
+        fwd = SpModel(case, device=getattr(spe.model, "device", 0))
+        try:
+            fwd.execute()
+            h_end = fwd.state()[0]
+        finally:
+            fwd.close()
+        free = np.nonzero(h_end > 1e-4)[0]
+        spe.diag["mask_dry_cells"] = {"fixed": int(n - free.size), "free": int(free.size)}
+    else:
+        free = np.arange(n)
+    if cfg.porosity_free_zone_map:
+        path = cfg.porosity_free_zone_map
+        if spe.folder and not os.path.isabs(path):
+            path = os.path.join(spe.folder, path)
+        try:
+            zone = load_map(path, n)
+        except (OSError, ValueError) as exc:
+            spe.diag["zone_map_error"] = f"{path}: {exc}; zonation ignored"
+        else:
+            before = free.size
+            free = free[zone[free] < 0.5]
+            spe.diag["porosity_free_zone_map"] = {"free_in_zone": int(free.size), "free_before": int(before)}
+            if free.size == 0:
+                spe.diag["zone_map_error"] = f"{path}: empty zone (no cell with value < 0.5)"
+    return free
+
+
 def run_minimization(spe: SpE, phi_start, max_it: Optional[int] = None, alpha_reg: Optional[float] = None,
                      descent_dir: Optional[str] = None, free=None, phi_ref=None) -> Dict[str, object]:
     """swSpE::run_minimization (assim/swSpE_minimize.cpp:582-1073) with minimize_algo "lbfgsb"
@@ -490,6 +632,8 @@ def run_minimization(spe: SpE, phi_start, max_it: Optional[int] = None, alpha_re
     cfg = spe.cfg
     max_it = cfg.max_it if max_it is None else max_it
     alpha = cfg.alpha_reg if alpha_reg is None else alpha_reg
+    if free is None:
+        free = free_cells(spe, phi_start)
     prob = PorosityProblem(spe, phi_start, free=free, zonation=cfg.zonation, alpha_reg=alpha, phi_ref=phi_ref,
                            descent_dir=descent_dir)
     theta = prob.theta_start()

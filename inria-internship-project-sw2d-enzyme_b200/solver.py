@@ -436,6 +436,17 @@ class SpModel:
         h, q, r = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, q, r))
         self._check(self.lib.sw2d_assim_set_start(self.handle, _p(h), _p(q), _p(r)))
 
+    def assim_trigger_states(self, m, n_obs: int):
+        """The recorded trajectory replayed at control m: the state after each step that lands on
+        an observation, as arrays [n_obs, n_cells] (h, qx, qy), and the number of observations
+        landed on."""
+        mm = np.ascontiguousarray(m, dtype=np.float64)
+        h, q, r = (np.full((n_obs, self.n), np.nan) for _ in range(3))
+        k = ctypes.c_int64(0)
+        self._check(self.lib.sw2d_assim_trigger_states(self.handle, _p(mm), _p(h), _p(q), _p(r), int(n_obs),
+                                                       ctypes.byref(k)))
+        return h, q, r, int(k.value)
+
     def assim_checkpoint(self, k: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         h, q, r = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
         self._check(self.lib.sw2d_assim_checkpoint(self.handle, int(k), _p(h), _p(q), _p(r)))

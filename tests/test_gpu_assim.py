@@ -281,3 +281,28 @@ def test_toce_minimization_descends(pkg, tmp_path):
     print("sp_toce descent:", [round(j, 6) for j in res["history"]])
     assert res["J_final"] < 0.99 * res["J_init"]
     assert np.all((res["phi"] >= 0.0) & (res["phi"] <= 1.0))
+
+
+def test_toce_gen_ref_e_reproduces_the_reference_observations(pkg, tmp_path):
+    """The reference's gen-ref-e mode (swSpE::generate_references_E) on sp_toce, with the case's
+    truth porosity (input/SP_cell_porosity_map.txt, its porosity_ref_map, kept in the sp_toce
+    fixture as the case's porosity): the 41 observation maps reference/ResultHydro_p*.txt that the
+    case ships (made by that mode) are reproduced digit for digit in water_depth,
+    unit_discharge_x and unit_discharge_y, at the same times (file names)."""
+    from tests.golden.make_assim_golden import frames_as_decimals
+    case, fx = sp_toce_case()
+    ax = np.load(os.path.join(GOLDEN, "sp_toce_assim.npz"))
+    c = json.loads(str(ax["config"]))
+    cfg = pkg.porosity.AssimConfig(dt_map_ad=c["dt_map_ad"], t_state_assimilation=c["t_state_assimilation"],
+                                   checkpoint_stride=int(c["checkpoint_stride"]), windowed_assimilation=True,
+                                   assimilation_window_duration=c["window_duration"],
+                                   n_assimilation_windows=int(c["n_windows"]), cost_normalize=True)
+    spe = pkg.porosity.SpE(pkg.SpModel(case), cfg)
+    files = spe.generate_references_E(fx["phi"], str(tmp_path))
+    names = [os.path.basename(f) for f in files]
+    assert len(files) == 41 and names[0] == "ResultHydro_p0000d00h00m10s000.txt" \
+        and names[-1] == "ResultHydro_p0000d00h00m30s000.txt", names[:3] + names[-3:]
+    mant, expo = frames_as_decimals(sorted(files))
+    same = (mant == ax["obs_mant"]) & ((expo == ax["obs_exp"]) | (mant == 0))
+    nbad = int(np.count_nonzero(~same))
+    assert nbad == 0, f"{nbad} of {same.size} printed values differ from the reference's observation maps"

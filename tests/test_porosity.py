@@ -113,3 +113,39 @@ def test_porosity_problem_gradient(transform):
     fd = (prob.grad(theta + e * d)[0] - prob.grad(theta - e * d)[0]) / (2 * e)
     assert abs(fd - g @ d) <= 1e-6 * max(1.0, abs(fd))
     assert abs(prob.func(theta) - J) < 1e-12
+
+
+def test_free_cells_zone_map(tmp_path):
+    """porosity_free_zone_map (assim/swSpE_minimize.cpp:648-668): of the cells the dry mask leaves
+    free (here all), only those whose zone value is below 0.5; an unreadable map leaves the set
+    unchanged and is reported; an empty zone is reported."""
+    from types import SimpleNamespace
+    pkg = load_pkg()
+    por = pkg.porosity
+    n = 6
+    (tmp_path / "zone.csv").write_text("cell_id,value\n" + "".join(f"{i},{v}\n" for i, v in
+                                                                 enumerate([0, 1, 0.2, 0.7, 0.49, 1])))
+    cfg = por.AssimConfig(porosity_free_zone_map="zone.csv")
+    spe = SimpleNamespace(cfg=cfg, n=n, folder=str(tmp_path), diag={})
+    assert por.free_cells(spe, np.ones(n)).tolist() == [0, 2, 4]
+    assert spe.diag["porosity_free_zone_map"] == {"free_in_zone": 3, "free_before": 6}
+    spe = SimpleNamespace(cfg=por.AssimConfig(porosity_free_zone_map="missing.csv"), n=n, folder=str(tmp_path), diag={})
+    assert por.free_cells(spe, np.ones(n)).tolist() == list(range(n)) and "zone_map_error" in spe.diag
+    (tmp_path / "none.csv").write_text("".join(f"{i},1\n" for i in range(n)))
+    spe = SimpleNamespace(cfg=por.AssimConfig(porosity_free_zone_map="none.csv"), n=n, folder=str(tmp_path), diag={})
+    assert por.free_cells(spe, np.ones(n)).size == 0 and "empty zone" in spe.diag["zone_map_error"]
+
+
+def test_reference_map_file_name_and_format(tmp_path):
+    """swIO::computeFileNameFromTime and createTxtFileMapDecimal, restated: the names and layout of
+    the observation maps the reference's gen-ref-e mode writes (reference/ResultHydro_p*.txt)."""
+    por = load_pkg().porosity
+    assert por.result_file_name("ResultHydro_p", 10.0) == "ResultHydro_p0000d00h00m10s000.txt"
+    assert por.result_file_name("ResultHydro_p", 29.5) == "ResultHydro_p0000d00h00m29s500.txt"
+    assert por.result_file_name("ResultHydro_p", 90061.25) == "ResultHydro_p0001d01h01m01s250.txt"
+    path = str(tmp_path / "m.txt")
+    por.write_map_decimal(path, ["x", "unit_discharge_norm"], [np.array([7.006166665, -0.0]), np.array([1e-7, 2.5])], 10)
+    lines = open(path).read().split("\n")
+    assert lines[0] == "x" + " " * 16 + "\t" + "unit_discharge_norm\t"
+    assert lines[1] == "7.0061666650e+00\t1.0000000000e-07\t"
+    assert lines[2] == "-0.0000000000e+00\t2.5000000000e+00\t"
