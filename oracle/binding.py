@@ -25,6 +25,7 @@ REF_BIN_PM = os.path.join(HERE, "_ref", "sw2dSolver_pm")
 REF_MAPPER = os.path.join(HERE, "_ref", "sw2dPorosityMapper")
 REF_E_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e.so")
 REF_E_PM_SO = os.path.join(HERE, "_ref", "libsw2d_ref_e_pm.so")
+B200_BINDING_SO = os.path.join(HERE, "_ref", "libsw2d_b200_binding.so")
 # root of the reference's source tree (the environment variable SW2D_REFERENCE; empty when unset)
 REFERENCE_SRC = os.environ.get("SW2D_REFERENCE", "")
 
@@ -354,4 +355,49 @@ class RefE:
     def close(self) -> None:
         if self.h:
             self.lib.sw2dref_e_close(self.h)
+            self.h = None
+
+
+class B200Binding:
+    """The reference-side binding of INTEGRATION.md (oracle/b200_binding.cpp, compiled against the
+    reference's headers and objects): the reference reads the case folder with its own swSp and
+    the model class swSpB200 runs the time loop on the GPU through the C ABI."""
+
+    def __init__(self, folder: str, device: int = 0):
+        if not os.path.exists(B200_BINDING_SO):
+            raise RuntimeError(f"binding library not built ({B200_BINDING_SO})")
+        lib = ctypes.CDLL(B200_BINDING_SO)
+        lib.b200_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        lib.b200_open.restype = _P
+        lib.b200_execute.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
+        lib.b200_execute.restype = ctypes.c_int
+        lib.b200_cell_nb.argtypes = [_P]
+        lib.b200_cell_nb.restype = ctypes.c_long
+        lib.b200_state.argtypes = [_P, _D, _D, _D]
+        lib.b200_error.argtypes = [_P]
+        lib.b200_error.restype = ctypes.c_char_p
+        lib.b200_close.argtypes = [_P]
+        self.lib = lib
+        self.h = lib.b200_open(folder.encode(), int(device))
+        if not self.h:
+            raise RuntimeError(f"binding failed to open {folder}")
+        err = lib.b200_error(self.h).decode()
+        if err:
+            raise RuntimeError(f"binding init: {err}")
+        self.n = lib.b200_cell_nb(self.h)
+
+    def execute(self) -> int:
+        steps = ctypes.c_int64(0)
+        if self.lib.b200_execute(self.h, ctypes.byref(steps)) != 0:
+            raise RuntimeError(f"binding execute: {self.lib.b200_error(self.h).decode()}")
+        return int(steps.value)
+
+    def state(self):
+        h, q, r = (np.empty(self.n) for _ in range(3))
+        self.lib.b200_state(self.h, h, q, r)
+        return h, q, r
+
+    def close(self):
+        if self.h:
+            self.lib.b200_close(self.h)
             self.h = None
