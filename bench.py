@@ -943,6 +943,7 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank != 0:
         return
+    kps = model.kernels_per_step
     del model
     wet = None if (args.wet_steps <= 0 or world > 1) else run_wet(pkg, args, local_rank)
     adjoint = None if (args.no_adjoint or world > 1) else run_adjoint(pkg, args, local_rank)
@@ -962,7 +963,6 @@ def run_ours(args, rank, world, local_rank):
     algo_bytes = ALGO_BYTES_PER_CELL_UPDATE * n
     achieved = algo_bytes / (step_ms / 1e3) / 1e9
     traffic = _traffic_per_step()
-    kps = model.kernels_per_step
     tot_phase = sum(phases.values())
     kernels = {k2: {"ms": v, "share": v / tot_phase if tot_phase > 0 else None} for k2, v in phases.items()}
     dominant = max(phases, key=phases.get)

@@ -61,7 +61,7 @@ def _same(a, b):
     return np.array_equal(np.asarray(a).view(np.int64), np.asarray(b).view(np.int64))
 
 
-@pytest.mark.parametrize("tile", [32, 97, None, 2048])
+@pytest.mark.parametrize("tile", [32, 97, None, 1024])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_fused_matches_four_kernel_step(pkg, name, tile):
     kind, kwargs = CASES[name]
@@ -105,6 +105,9 @@ def test_fused_phase_labels_and_switch(pkg):
         m.set_option("tile_cells", 5)
     assert m.kernels_per_step == 2 and m.step(3) == 3   # the previous tiles are kept
     assert m.get_option("tile_cells") == 512
+    with pytest.raises(pkg.Sw2dError, match="shared-memory"):
+        m.set_option("tile_cells", 4096)                  # a stage beyond 200 KB is refused
+    assert m.get_option("tile_cells") == 512 and m.step(2) == 2
 
 
 def test_fused_autotune_keeps_results(pkg):
