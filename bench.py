@@ -87,6 +87,8 @@ def _args():
                     help="print only the porosity-assimilation measurement (one JSON line)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint measurement (one JSON line), e.g. for profiling")
+    ap.add_argument("--flux-variant", type=int, default=None,
+                    help="launch variant of the fused step's k_flux instead of autotuning (profiling runs)")
     ap.add_argument("--launch-config", default=None,
                     help="'S,E': slope and edge kernel launch variants instead of autotuning (profiling runs)")
     return ap.parse_args()
@@ -880,7 +882,10 @@ def run_ours(args, rank, world, local_rank):
 
     # launch-configuration autotune on the live state (no step taken), then warm-up (also
     # builds the CUDA graph)
-    if args.launch_config:
+    if args.flux_variant is not None:
+        model.set_option("flux_variant", args.flux_variant)
+        tune = {"report": f"fixed k_flux variant {args.flux_variant}"}
+    elif args.launch_config:
         sv, ev = (int(v) for v in args.launch_config.split(","))
         model._check(model.lib.sw2d_set_launch_config(model.handle, sv, ev))
         tune = {"report": f"fixed variants slopes={sv} edges={ev}"}

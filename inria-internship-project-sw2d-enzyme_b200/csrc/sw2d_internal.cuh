@@ -148,6 +148,7 @@ struct DevMesh {
     double h_min, phi_min, cfl_max, dt_max, dt_map, v_max, fr_max;
     DryConsts dry;
     int neg_detect;
+    int rev_update;  // the cell update walks its blocks from the last cells to the first
     // dt reduction scratch
     double* part;
     Ctrl* ctrl;

@@ -373,7 +373,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
     Ctrl* ctrl = m.ctrl;
     if (!ctrl->go) return;
     const double dt = ctrl->dt;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    // with rev_update the blocks take the cells from the end: the flux kernel finishes on the last
+    // tiles, whose slots and states are then still in L2
+    const int blk = m.rev_update ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    const int c = blk * blockDim.x + threadIdx.x;
     if (c == 0) {
         ctrl->t = ctrl->t + dt;  // swSp.cpp:592; no other thread of this kernel reads t
         ctrl->steps += 1;
@@ -1484,6 +1487,9 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
             if (!h->tiles.ntiles) h->fused = 0;  // the previous tiles are kept unless they were released
             return fail(h, rc, "tile_cells: " + (why.empty() ? h->err : why));
         }
+    } else if (std::strcmp(name, "update_reverse") == 0) {
+        // block order of the cell update: 1 from the last cells to the first (the same results)
+        h->m.rev_update = value ? 1 : 0;
     } else if (std::strcmp(name, "flux_variant") == 0) {
         if (value < 0 || value >= flux_variants()) return fail(h, SW2D_E_ARG, "flux_variant outside the variants");
         h->flux_variant = (int)value;
@@ -1507,6 +1513,7 @@ int sw2d_get_option(sw2d_handle* h, const char* name, int64_t* value)
     if (!h || !name || !value) return fail(h, SW2D_E_ARG, "invalid arguments");
     if (std::strcmp(name, "fused_step") == 0) *value = h->fused;
     else if (std::strcmp(name, "flux_variant") == 0) *value = h->flux_variant;
+    else if (std::strcmp(name, "update_reverse") == 0) *value = h->m.rev_update;
     else if (std::strcmp(name, "tile_cells") == 0) *value = h->tiles.tile_cells;
     else if (std::strcmp(name, "record_fluxes") == 0) *value = h->m.flux != nullptr;
     else if (std::strcmp(name, "record_wave_speeds") == 0) *value = h->m.lmax != nullptr;
