@@ -62,20 +62,25 @@ __host__ __device__ __forceinline__ Slot make_slot(double a, double b, double c)
 // the tile: the owned range [e0, e0 + ne_own) (lower cell in the tile) and nx_flux incoming edges,
 // then nx_slope edges that only the ring-1 slopes need (xe[xoff ..]); per tile edge the local
 // {L, R} indices (eloc[loff ..]); the neighbour lists of the tile and ring-1 cells (scsr[soff ..],
-// offsets soffs[so_off ..]); boundary edges [b0, b1); first balance slot s0.
+// offsets soffs[so_off ..], nent entries); boundary edges [b0, b1); first balance slot s0.
 struct TileInfo {
-    int c0, nt, nh1, nh2, hoff, e0, ne_own, xoff, nx_flux, nx_slope, loff, soff, so_off, b0, b1, s0;
+    int c0, nt, nh1, nh2, hoff, e0, ne_own, xoff, nx_flux, nx_slope, loff, soff, so_off, b0, b1, s0, nent;
 };
 
 struct TileMesh {
     int ntiles = 0, tile_cells = 0;
-    int nl_max = 0, nf_max = 0, ns_max = 0;  // largest staged cell set, tile + ring 1, slot range
+    // the largest tile: staged cells, tile + ring-1 cells, tile cells, slot range, flux edges, all
+    // tile edges, neighbour-list entries
+    int nl_max = 0, nf_max = 0, nt_max = 0, ns_max = 0, ne_max = 0, na_max = 0, nent_max = 0;
+    // byte offsets of the stage's sections in shared memory and its size (sw2d_tile.cu)
+    int o_st = 0, o_cst = 0, o_xy = 0, o_sl = 0, o_coff = 0, o_lam = 0, o_en = 0, o_ecf = 0, o_elen = 0, o_esl = 0,
+        o_epg = 0, o_em = 0, o_ell = 0, o_ent = 0, o_so = 0, smem = 0;
     const TileInfo* info = nullptr;
     const int* halo = nullptr;
     const int* xe = nullptr;
     const ushort2* eloc = nullptr;
     const unsigned* scsr = nullptr;        // local neighbour | tile edge << 16 | side << 31
-    const unsigned short* soffs = nullptr;
+    const unsigned* soffs = nullptr;
 };
 
 struct DdpCtrl;       // sw2d_ddp.cu

@@ -48,23 +48,66 @@ using namespace sw2d;
 
 namespace {
 
-// Staged cell records in shared memory: A = {h, q, r, z_b}, B = {b, phi, sx, sy} for the tile
-// and ring-1 cells, C = {z, cx, cy, -} for every staged cell (MUSCL-EVR only).
-struct StageView {
-    double4* A;
-    double4* B;
-    double4* C;
-    double* lam;  // CFL contribution of each of the tile's slots
+// Asynchronous global -> shared copies (cp.async, sm_80+): every copy of a tile is issued before
+// the first is waited for, so the loads of a tile are in flight together.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cpa16(void* s, const void* g)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cpa8(void* s, const void* g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cpa4(void* s, const void* g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// A tile's stage in shared memory, in the global records' own layouts (byte offsets computed on
+// the host, TileMesh::o_*): per staged cell its state {h, q, r, z} and centroid {x, y}; per tile
+// and ring-1 cell its statics {z_b, b, phi, area} and limited slope {sx, sy}; per tile cell its
+// slot offsets; per tile slot the CFL contribution; per flux edge {nx, ny}, {coefL, coefR},
+// length, {slot L, slot R} (and phiG for DIP); per tile edge {mx, my} and the local {L, R}; the
+// neighbour lists of the tile and ring-1 cells.
+struct Stage {
+    double4* st;
+    double4* cst;
+    double2* xy;
+    double2* sl;
+    int2* coff;
+    double* lam;
+    double2* en;
+    double2* ecf;
+    double* elen;
+    int2* esl;
+    double* epg;
+    double2* em;
+    ushort2* ell;
+    unsigned* ent;
+    unsigned* so;
 };
 
-__device__ __forceinline__ StageView stage_view(const TileMesh& tm, bool muscl)
+__device__ __forceinline__ Stage stage_of(const TileMesh& tm)
 {
-    extern __shared__ double4 smem4[];
-    StageView v;
-    v.A = smem4;
-    v.B = v.A + tm.nf_max;
-    v.C = v.B + tm.nf_max;
-    v.lam = reinterpret_cast<double*>(v.C + (muscl ? tm.nl_max : 0));
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Stage v;
+    v.st = reinterpret_cast<double4*>(smem_raw + tm.o_st);
+    v.cst = reinterpret_cast<double4*>(smem_raw + tm.o_cst);
+    v.xy = reinterpret_cast<double2*>(smem_raw + tm.o_xy);
+    v.sl = reinterpret_cast<double2*>(smem_raw + tm.o_sl);
+    v.coff = reinterpret_cast<int2*>(smem_raw + tm.o_coff);
+    v.lam = reinterpret_cast<double*>(smem_raw + tm.o_lam);
+    v.en = reinterpret_cast<double2*>(smem_raw + tm.o_en);
+    v.ecf = reinterpret_cast<double2*>(smem_raw + tm.o_ecf);
+    v.elen = reinterpret_cast<double*>(smem_raw + tm.o_elen);
+    v.esl = reinterpret_cast<int2*>(smem_raw + tm.o_esl);
+    v.epg = reinterpret_cast<double*>(smem_raw + tm.o_epg);
+    v.em = reinterpret_cast<double2*>(smem_raw + tm.o_em);
+    v.ell = reinterpret_cast<ushort2*>(smem_raw + tm.o_ell);
+    v.ent = reinterpret_cast<unsigned*>(smem_raw + tm.o_ent);
+    v.so = reinterpret_cast<unsigned*>(smem_raw + tm.o_so);
     return v;
 }
 
@@ -72,34 +115,33 @@ __device__ __forceinline__ StageView stage_view(const TileMesh& tm, bool muscl)
 // side << 31), the same two passes as k_slopes: the gradient over the neighbours in the
 // reference's order (divided by the weight sum; none with a single neighbour), then the limiter
 // edge by edge in the same order
-__device__ __forceinline__ double2 tile_slope(const DevMesh& m, const TileMesh& tm, int e0, int ne_own, int xoff,
-                                              const unsigned* __restrict__ ent, int cnt, double4 cc, const double4* C)
+__device__ __forceinline__ double2 tile_slope(const Stage& sv, int k0, int k1, double zc, double xc, double yc)
 {
-    const double zc = cc.x, xc = cc.y, yc = cc.z;
+    const int cnt = k1 - k0;
     double sx = 0.0, sy = 0.0, wsum = 0.0;
     if (cnt > 1) {
-        for (int k = 0; k < cnt; k++) {
-            const int j = (int)(ld(&ent[k]) & 0xffffu);
-            const double4 cj = C[j];
-            const double dx = cj.y - xc;
-            const double dy = cj.z - yc;
+        for (int k = k0; k < k1; k++) {
+            const int j = (int)(sv.ent[k] & 0xffffu);
+            const double2 xj = sv.xy[j];
+            const double zj = sv.st[j].w;
+            const double dx = xj.x - xc;
+            const double dy = xj.y - yc;
             const double dist = sqrt(dx * dx + dy * dy);
             const double w = 1.0 / dist;
-            sx += (cj.x - zc) * dx / dist / dist * w;
-            sy += (cj.x - zc) * dy / dist / dist * w;
+            sx += (zj - zc) * dx / dist / dist * w;
+            sy += (zj - zc) * dy / dist / dist * w;
             wsum += w;
         }
         sx /= wsum;
         sy /= wsum;
     }
-    for (int k = 0; k < cnt; k++) {
-        const unsigned en = ld(&ent[k]);
+    for (int k = k0; k < k1; k++) {
+        const unsigned en = sv.ent[k];
         const int j = (int)(en & 0xffffu);
         const int te = (int)((en >> 16) & 0x7fffu);
         const bool is_r = (en >> 31) != 0;
-        const int e = (te < ne_own) ? e0 + te : ld(&tm.xe[xoff + te - ne_own]);
-        const double2 mp = ld(&m.mxy[e]);
-        const double zj = C[j].x;
+        const double2 mp = sv.em[te];
+        const double zj = sv.st[j].w;
         const double zL = is_r ? zj : zc;
         const double zR = is_r ? zc : zj;
         const double fmx = smax(zL, zR);
@@ -133,40 +175,56 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
         if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->go = 0;
         return;
     }
-    const StageView sv = stage_view(tm, kMuscl);
+    const Stage sv = stage_of(tm);
 
-    // ---- stage the tile (contiguous) and its rings (gathered)
+    // ---- stage the tile (contiguous), its rings (gathered) and its edges, all copies in flight
     {
         const int c0 = TI(c0), nt = TI(nt), hoff = TI(hoff);
         const int nf = nt + TI(nh1), nl = kMuscl ? nf + TI(nh2) : nf;
         for (int l = threadIdx.x; l < nl; l += kThreads) {
             const int g = (l < nt) ? c0 + l : ld(&tm.halo[hoff + l - nt]);
-            const double4 s = ld(&m.st[g]);
-            if (kMuscl) {
-                const double2 xy = ld(&m.cxy[g]);
-                sv.C[l] = make_double4(s.w, xy.x, xy.y, 0.0);
-            }
+            const double2* sg = reinterpret_cast<const double2*>(m.st + g);
+            cpa16(reinterpret_cast<double2*>(sv.st + l), sg);
+            cpa16(reinterpret_cast<double2*>(sv.st + l) + 1, sg + 1);
+            if (kMuscl) cpa16(sv.xy + l, m.cxy + g);
             if (l < nf) {
-                const double4 c = ld(&m.cst[g]);
-                sv.A[l] = make_double4(s.x, s.y, s.z, c.x);
-                sv.B[l] = make_double4(c.y, c.z, 0.0, 0.0);
+                const double2* cg = reinterpret_cast<const double2*>(m.cst + g);
+                cpa16(reinterpret_cast<double2*>(sv.cst + l), cg);
+                cpa16(reinterpret_cast<double2*>(sv.cst + l) + 1, cg + 1);
             }
         }
+        for (int l = threadIdx.x; l <= nt; l += kThreads) cpa8(sv.coff + l, m.coff + c0 + l);
+        const int e0 = TI(e0), ne_own = TI(ne_own), xoff = TI(xoff), loff = TI(loff);
+        const int nflux = ne_own + TI(nx_flux), nall = kMuscl ? nflux + TI(nx_slope) : nflux;
+        for (int j = threadIdx.x; j < nall; j += kThreads) {
+            const int e = (j < ne_own) ? e0 + j : ld(&tm.xe[xoff + j - ne_own]);
+            cpa4(sv.ell + j, tm.eloc + loff + j);
+            if (kMuscl) cpa16(sv.em + j, m.mxy + e);
+            if (j < nflux) {
+                cpa16(sv.en + j, m.nxy + e);
+                cpa16(sv.ecf + j, m.coef + e);
+                cpa8(sv.elen + j, m.len + e);
+                cpa8(sv.esl + j, m.eslot + e);
+                if (kDip) cpa8(sv.epg + j, m.phig + e);
+            }
+        }
+        if (kMuscl) {
+            const int soff = TI(soff), so_off = TI(so_off), nent = TI(nent);
+            for (int k = threadIdx.x; k < nent; k += kThreads) cpa4(sv.ent + k, tm.scsr + soff + k);
+            for (int l = threadIdx.x; l <= nf; l += kThreads) cpa4(sv.so + l, tm.soffs + so_off + l);
+        }
+        cpa_wait_all();
     }
     __syncthreads();
 
     // ---- slopes of the tile and ring-1 cells (computeMusclSlopes)
     if (kMuscl) {
         const int c0 = TI(c0), nt = TI(nt), nf = nt + TI(nh1);
-        const int e0 = TI(e0), ne_own = TI(ne_own), xoff = TI(xoff);
-        const unsigned short* so = tm.soffs + TI(so_off);
-        const unsigned* ent = tm.scsr + TI(soff);
         const bool keep = m.flux != nullptr || m.lmax != nullptr;
         for (int l = threadIdx.x; l < nf; l += kThreads) {
-            const int k0 = ld(&so[l]), k1 = ld(&so[l + 1]);
-            const double2 g = tile_slope(m, tm, e0, ne_own, xoff, ent + k0, k1 - k0, sv.C[l], sv.C);
-            sv.B[l].z = g.x;
-            sv.B[l].w = g.y;
+            const double2 xy = sv.xy[l];
+            const double2 g = tile_slope(sv, (int)sv.so[l], (int)sv.so[l + 1], sv.st[l].w, xy.x, xy.y);
+            sv.sl[l] = g;
             if (keep && l < nt) m.slope[c0 + l] = g;
         }
         __syncthreads();
@@ -176,55 +234,58 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
     unsigned bad = 0;
     {
         const double dtp = ctrl->dt;
-        const int nt = TI(nt), e0 = TI(e0), ne_own = TI(ne_own), xoff = TI(xoff), loff = TI(loff), s0 = TI(s0);
+        const int nt = TI(nt), s0 = TI(s0);
+        const int ne_own = TI(ne_own);
         const int nflux = ne_own + TI(nx_flux);
+        const bool rec = m.flux != nullptr || m.lmax != nullptr;
         for (int j = threadIdx.x; j < nflux; j += kThreads) {
-            const int e = (j < ne_own) ? e0 + j : ld(&tm.xe[xoff + j - ne_own]);
-            const ushort2 ll = ld(&tm.eloc[loff + j]);
+            const ushort2 ll = sv.ell[j];
             const int a = ll.x, b = ll.y;
-            const double2 n = ld(&m.nxy[e]);
-            const double4 Aa = sv.A[a], Ab = sv.A[b];
-            const double4 Ba = sv.B[a], Bb = sv.B[b];
+            const double2 n = sv.en[j];
+            const double4 Sa = sv.st[a], Sb = sv.st[b];
+            const double4 Ka = sv.cst[a], Kb = sv.cst[b];
             SideState SL, SR;
             double phiG = 0.0, xL = 1.0, xR = 1.0;
             if (kDip) {
-                phiG = ld(&m.phig[e]);
-                xL = dip_x(Ba.y, phiG);
-                xR = dip_x(Bb.y, phiG);
+                phiG = sv.epg[j];
+                xL = dip_x(Ka.z, phiG);
+                xR = dip_x(Kb.z, phiG);
             }
             if (!kMuscl) {
                 if (kDip) {
-                    SL = godunov_side_dip(Aa.x, Aa.y, Aa.z, Aa.w, Ba.x, xL, n.x, n.y);
-                    SR = godunov_side_dip(Ab.x, Ab.y, Ab.z, Ab.w, Bb.x, xR, n.x, n.y);
+                    SL = godunov_side_dip(Sa.x, Sa.y, Sa.z, Ka.x, Ka.y, xL, n.x, n.y);
+                    SR = godunov_side_dip(Sb.x, Sb.y, Sb.z, Kb.x, Kb.y, xR, n.x, n.y);
                 } else {
-                    SL = godunov_side(Aa.x, Aa.y, Aa.z, Aa.w, Ba.x, n.x, n.y);
-                    SR = godunov_side(Ab.x, Ab.y, Ab.z, Ab.w, Bb.x, n.x, n.y);
+                    SL = godunov_side(Sa.x, Sa.y, Sa.z, Ka.x, Ka.y, n.x, n.y);
+                    SR = godunov_side(Sb.x, Sb.y, Sb.z, Kb.x, Kb.y, n.x, n.y);
                 }
             } else {
-                const double2 mp = ld(&m.mxy[e]);
-                const double4 Ca = sv.C[a], Cb = sv.C[b];
-                const double dax = mp.x - Ca.y, day = mp.y - Ca.z;
-                const double dbx = mp.x - Cb.y, dby = mp.y - Cb.z;
+                const double2 mp = sv.em[j];
+                const double2 ca = sv.xy[a], cb = sv.xy[b];
+                const double2 ga = sv.sl[a], gb = sv.sl[b];
+                const double dax = mp.x - ca.x, day = mp.y - ca.y;
+                const double dbx = mp.x - cb.x, dby = mp.y - cb.y;
                 if (kDip) {
-                    SL = evr_side_dip(true, Aa.x, Aa.y, Aa.z, Aa.w, Ba.x, xL, Ca.x, Ba.z, Ba.w, dax, day, n.x, n.y, dtp);
-                    SR = evr_side_dip(false, Ab.x, Ab.y, Ab.z, Ab.w, Bb.x, xR, Cb.x, Bb.z, Bb.w, dbx, dby, n.x, n.y, dtp);
+                    SL = evr_side_dip(true, Sa.x, Sa.y, Sa.z, Ka.x, Ka.y, xL, Sa.w, ga.x, ga.y, dax, day, n.x, n.y, dtp);
+                    SR = evr_side_dip(false, Sb.x, Sb.y, Sb.z, Kb.x, Kb.y, xR, Sb.w, gb.x, gb.y, dbx, dby, n.x, n.y, dtp);
                 } else {
-                    SL = evr_side(true, Aa.x, Aa.y, Aa.z, Aa.w, Ba.x, Ca.x, Ba.z, Ba.w, dax, day, n.x, n.y, dtp, m.dry);
-                    SR = evr_side(false, Ab.x, Ab.y, Ab.z, Ab.w, Bb.x, Cb.x, Bb.z, Bb.w, dbx, dby, n.x, n.y, dtp, m.dry);
+                    SL = evr_side(true, Sa.x, Sa.y, Sa.z, Ka.x, Ka.y, Sa.w, ga.x, ga.y, dax, day, n.x, n.y, dtp, m.dry);
+                    SR = evr_side(false, Sb.x, Sb.y, Sb.z, Kb.x, Kb.y, Sb.w, gb.x, gb.y, dbx, dby, n.x, n.y, dtp, m.dry);
                 }
             }
             const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
+            const int e = rec ? ((j < ne_own) ? TI(e0) + j : ld(&tm.xe[TI(xoff) + j - ne_own])) : 0;
             if (m.lmax) m.lmax[e] = lm;
-            const double lw = lm * ld(&m.len[e]);
-            const bool wetL = Aa.x > m.h_min, wetR = Ab.x > m.h_min;
-            const int2 sl = ld(&m.eslot[e]);
+            const double lw = lm * sv.elen[j];
+            const bool wetL = Sa.x > m.h_min, wetR = Sb.x > m.h_min;
+            const int2 sl = sv.esl[j];
             const bool ownL = a < nt, ownR = b < nt;
             if (ownL) sv.lam[sl.x - s0] = wetL ? lw : 0.0;
             if (ownR) sv.lam[sl.y - s0] = (wetL || wetR) ? lw : 0.0;
-            const double hL = SL.z - Aa.w, hR = SR.z - Ab.w;
+            const double hL = SL.z - Ka.x, hR = SR.z - Kb.x;
             if ((hL > m.h_min) || (hR > m.h_min)) {
-                EdgeFlux f = kDip ? hllc_dip(kBlending, Ba.x, Bb.x, phiG, Ba.y, Bb.y, Aa.w, Ab.w, SL, SR, m.h_min, m.phi_min)
-                                  : hllc(kBlending, Ba.x, Bb.x, Ba.y, Bb.y, Aa.w, Ab.w, SL, SR, m.h_min, m.phi_min);
+                EdgeFlux f = kDip ? hllc_dip(kBlending, Ka.y, Kb.y, phiG, Ka.z, Kb.z, Ka.x, Kb.x, SL, SR, m.h_min, m.phi_min)
+                                  : hllc(kBlending, Ka.y, Kb.y, Ka.z, Kb.z, Ka.x, Kb.x, SL, SR, m.h_min, m.phi_min);
                 bad |= f.bad;
                 if (isnan(f.f1)) bad |= kStatusNanFlux;
                 if (m.flux) {
@@ -233,7 +294,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
                     fp[1] = make_double2(f.f3, f.sl);
                     fp[2] = make_double2(f.sr, 0.0);
                 }
-                const double2 cf = ld(&m.coef[e]);
+                const double2 cf = sv.ecf[j];
                 const double nx = n.x, ny = n.y;
                 if (ownL) {
                     const double c = cf.x;
@@ -261,20 +322,20 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
             const int e = b0 + j;
             const int l = ld(&m.bcell[e]) - c0;
             const double4 g = ld(&m.bgeo[e]);
-            const double4 Al = sv.A[l], Bl = sv.B[l];
+            const double4 Sl = sv.st[l], Kl = sv.cst[l];
             const double phiGb = kDip ? ld(&m.phigb[e]) : 0.0;
-            SideState S = kDip ? godunov_side_dip(Al.x, Al.y, Al.z, Al.w, Bl.x, dip_x(Bl.y, phiGb), g.x, g.y)
-                               : godunov_side(Al.x, Al.y, Al.z, Al.w, Bl.x, g.x, g.y);
+            SideState S = kDip ? godunov_side_dip(Sl.x, Sl.y, Sl.z, Kl.x, Kl.y, dip_x(Kl.z, phiGb), g.x, g.y)
+                               : godunov_side(Sl.x, Sl.y, Sl.z, Kl.x, Kl.y, g.x, g.y);
             const double lm = kMuscl ? smax(fabs(S.lm), fabs(S.lp)) : smax(fabs(S.lp), fabs(S.lm));
             if (m.lmaxb) m.lmaxb[e] = lm;
             const int sbi = ld(&m.bslot[e]);
-            sv.lam[sbi - s0] = (Al.x > m.h_min) ? lm * g.z : 0.0;
+            sv.lam[sbi - s0] = (Sl.x > m.h_min) ? lm * g.z : 0.0;
             const int k = ld(&m.bbc[e]);
             const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
             const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, tnow);
             double f1, f2, f3;
-            bad |= kDip ? boundary_flux_dip(Bl.x, phiGb, Bl.y, Al.w, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3)
-                        : boundary_flux(Bl.x, Bl.y, Al.w, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
+            bad |= kDip ? boundary_flux_dip(Kl.y, phiGb, Kl.z, Kl.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3)
+                        : boundary_flux(Kl.y, Kl.z, Kl.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
             if (m.bflux) m.bflux[e] = make_double4(f1, f2, f3, 0.0);
             const double cf = g.w, nx = g.x, ny = g.y;
             const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
@@ -289,13 +350,12 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
     // ---- swept length and CFL bound of the tile's cells (hypComputeTimeStep)
     double best = m.dt_max;
     {
-        const int c0 = TI(c0), nt = TI(nt), s0 = TI(s0);
+        const int nt = TI(nt), s0 = TI(s0);
         for (int l = threadIdx.x; l < nt; l += kThreads) {
-            const int c = c0 + l;
-            const int k0 = ld(&m.coff[c].y) - s0, k1 = ld(&m.coff[c + 1].y) - s0;
+            const int k0 = sv.coff[l].y - s0, k1 = sv.coff[l + 1].y - s0;
             double sw = 0.0;
             for (int k = k0; k < k1; k++) sw += sv.lam[k];
-            const double x = m.cfl_max * (ld(&m.area[c]) / smax(sw, kSmallReal));
+            const double x = m.cfl_max * (sv.cst[l].w / smax(sw, kSmallReal));
             if (x < best) best = x;
         }
     }
@@ -353,15 +413,37 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
 struct FluxVariant {
     int threads, minb;
 };
-constexpr FluxVariant kFluxVariants[] = {{256, 2}, {256, 3}, {128, 4}, {128, 6}, {512, 1}, {384, 2}};
+constexpr FluxVariant kFluxVariants[] = {{256, 2}, {256, 3}, {192, 3}, {160, 4}, {320, 2}, {384, 2}};
 constexpr int kNumFluxVariants = sizeof(kFluxVariants) / sizeof(kFluxVariants[0]);
 
-size_t flux_smem(const TileMesh& tm, bool muscl)
+// The stage's byte layout (every section 16-byte aligned) for the largest tile; returns its size.
+size_t stage_layout(TileMesh& tm, bool muscl, bool dip)
 {
-    size_t n = 2 * 4 * (size_t)tm.nf_max + (size_t)tm.ns_max;
-    if (muscl) n += 4 * (size_t)tm.nl_max;
-    return n * sizeof(double);
+    size_t o = 0;
+    auto sec = [&](int* off, size_t bytes) {
+        *off = (int)o;
+        o += (bytes + 15) & ~(size_t)15;
+    };
+    sec(&tm.o_st, 32 * (size_t)tm.nl_max);
+    sec(&tm.o_cst, 32 * (size_t)tm.nf_max);
+    sec(&tm.o_xy, muscl ? 16 * (size_t)tm.nl_max : 0);
+    sec(&tm.o_sl, muscl ? 16 * (size_t)tm.nf_max : 0);
+    sec(&tm.o_coff, 8 * ((size_t)tm.nt_max + 1));
+    sec(&tm.o_lam, 8 * (size_t)tm.ns_max);
+    sec(&tm.o_en, 16 * (size_t)tm.ne_max);
+    sec(&tm.o_ecf, 16 * (size_t)tm.ne_max);
+    sec(&tm.o_elen, 8 * (size_t)tm.ne_max);
+    sec(&tm.o_esl, 8 * (size_t)tm.ne_max);
+    sec(&tm.o_epg, dip ? 8 * (size_t)tm.ne_max : 0);
+    sec(&tm.o_em, muscl ? 16 * (size_t)tm.na_max : 0);
+    sec(&tm.o_ell, 4 * (size_t)tm.na_max);
+    sec(&tm.o_ent, muscl ? 4 * (size_t)tm.nent_max : 0);
+    sec(&tm.o_so, muscl ? 4 * ((size_t)tm.nf_max + 1) : 0);
+    tm.smem = (int)o;
+    return o;
 }
+
+size_t flux_smem(const TileMesh& tm, bool) { return (size_t)tm.smem; }
 
 template <int kScheme, bool kBlending, int kModel, int V>
 cudaError_t launch_flux_v(sw2d_handle* h, const DevMesh& m, bool attr_only)
@@ -449,10 +531,10 @@ int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector
     std::vector<int> halo, xe;
     std::vector<ushort2> eloc;
     std::vector<unsigned> scsr;
-    std::vector<unsigned short> soffs;
+    std::vector<unsigned> soffs;
     halo.reserve((size_t)nc / 2);
     std::vector<int> cstamp(nc, -1), clid(nc, 0), estamp(ni, -1), elid(ni, 0);
-    int nl_max = 0, nf_max = 0, ns_max = 0;
+    int nl_max = 0, nf_max = 0, ns_max = 0, ne_max = 0, na_max = 0, nent_max = 0, nt_max = 0;
     std::vector<int> h1, h2, xin, xsl;
     for (int t = 0; t < ntiles; t++) {
         TileInfo& ti = info[t];
@@ -533,10 +615,11 @@ int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector
         for (int e : xsl) eloc.push_back(make_ushort2((unsigned short)lid(lr[e].x), (unsigned short)lid(lr[e].y)));
         ti.soff = (int)scsr.size();
         ti.so_off = (int)soffs.size();
+        ti.nent = 0;
         if (muscl) {
             int cnt = 0;
             for (int l = 0; l < nf; l++) {
-                soffs.push_back((unsigned short)cnt);
+                soffs.push_back((unsigned)cnt);
                 const int g = l < nt ? c0 + l : h1[l - nt];
                 for (int k = coff[g].x; k < coff[g + 1].x; k++) {
                     const int e = cint[k].x >> 1, side = cint[k].x & 1;
@@ -548,21 +631,30 @@ int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector
                     return SW2D_E_UNSUPPORTED;
                 }
             }
-            soffs.push_back((unsigned short)cnt);
+            soffs.push_back((unsigned)cnt);
+            ti.nent = cnt;
         }
         ti.b0 = bfirst[c0];
         ti.b1 = bfirst[c1];
         ti.s0 = coff[c0].y;
         nl_max = std::max(nl_max, nl);
         nf_max = std::max(nf_max, nf);
+        nt_max = std::max(nt_max, nt);
         ns_max = std::max(ns_max, coff[c1].y - coff[c0].y);
+        ne_max = std::max(ne_max, ne_own + nx_flux);
+        na_max = std::max(na_max, nedges);
+        nent_max = std::max(nent_max, ti.nent);
     }
     TileMesh& tm = h->tiles;
     TileMesh probe;
     probe.nl_max = nl_max;
     probe.nf_max = nf_max;
+    probe.nt_max = nt_max;
     probe.ns_max = ns_max;
-    const size_t smem = flux_smem(probe, muscl);
+    probe.ne_max = ne_max;
+    probe.na_max = na_max;
+    probe.nent_max = nent_max;
+    const size_t smem = stage_layout(probe, muscl, h->model == kModelDip);
     if (smem > 200 * 1024) {
         why = "a tile's shared-memory stage exceeds 200 KB";
         return SW2D_E_UNSUPPORTED;
@@ -570,12 +662,9 @@ int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector
     // replace the previous tiles' arrays
     for (void* p : h->tile_allocs) cudaFree(p);
     h->tile_allocs.clear();
-    tm = TileMesh{};
+    tm = probe;
     tm.ntiles = ntiles;
     tm.tile_cells = tile_cells;
-    tm.nl_max = nl_max;
-    tm.nf_max = nf_max;
-    tm.ns_max = ns_max;
     auto up = [&](const auto& vec, auto** dst) -> int {
         using T = typename std::remove_reference<decltype(vec)>::type::value_type;
         void* p = nullptr;
@@ -592,7 +681,7 @@ int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector
     int *d_halo = nullptr, *d_xe = nullptr;
     ushort2* d_eloc = nullptr;
     unsigned* d_scsr = nullptr;
-    unsigned short* d_soffs = nullptr;
+    unsigned* d_soffs = nullptr;
     int rc = up(info, &d_info);
     if (!rc) rc = up(halo, &d_halo);
     if (!rc) rc = up(xe, &d_xe);
