@@ -119,6 +119,60 @@ __device__ __forceinline__ double2 tile_slope(const Stage& sv, int k0, int k1, d
 {
     const int cnt = k1 - k0;
     double sx = 0.0, sy = 0.0, wsum = 0.0;
+    if (cnt == 3) {
+        // triangles: the three neighbours' terms are independent until they are summed, in the
+        // same order as below
+        unsigned en[3];
+        double zj[3];
+        double2 xj[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            en[i] = sv.ent[k0 + i];
+            const int j = (int)(en[i] & 0xffffu);
+            xj[i] = sv.xy[j];
+            zj[i] = sv.st[j].w;
+        }
+        double tx[3], ty[3], w[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const double dx = xj[i].x - xc;
+            const double dy = xj[i].y - yc;
+            const double dist = sqrt(dx * dx + dy * dy);
+            w[i] = 1.0 / dist;
+            tx[i] = (zj[i] - zc) * dx / dist / dist * w[i];
+            ty[i] = (zj[i] - zc) * dy / dist / dist * w[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            sx += tx[i];
+            sy += ty[i];
+            wsum += w[i];
+        }
+        sx /= wsum;
+        sy /= wsum;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const int te = (int)((en[i] >> 16) & 0x7fffu);
+            const bool is_r = (en[i] >> 31) != 0;
+            const double2 mp = sv.em[te];
+            const double zL = is_r ? zj[i] : zc;
+            const double zR = is_r ? zc : zj[i];
+            const double fmx = smax(zL, zR);
+            const double fmn = smin(zL, zR);
+            const double rec = zc + (mp.x - xc) * sx + (mp.y - yc) * sy;
+            if (rec < fmn) {
+                const double fac = (fmn - zc) / (rec - zc);
+                sx *= fac;
+                sy *= fac;
+            }
+            if (rec > fmx) {
+                const double fac = (fmx - zc) / (rec - zc);
+                sx *= fac;
+                sy *= fac;
+            }
+        }
+        return make_double2(sx, sy);
+    }
     if (cnt > 1) {
         for (int k = k0; k < k1; k++) {
             const int j = (int)(sv.ent[k] & 0xffffu);
