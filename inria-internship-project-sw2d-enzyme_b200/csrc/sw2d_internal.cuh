@@ -40,7 +40,23 @@ struct Ctrl {
     unsigned int blocks_done;
     int go;
     int store_map;  // DDP: the step ends on a storage time (swDdpHyp.cpp:590-609)
+    // the fused step's running minimum of the CFL bounds, as an order-preserving integer key of
+    // the double (kDminEmpty between steps)
+    unsigned long long dmin;
 };
+
+constexpr unsigned long long kDminEmpty = ~0ull;
+
+// Order-preserving map of a non-NaN double onto unsigned 64-bit integers (and back): a < b as
+// doubles iff key(a) < key(b) as integers, so an integer atomicMin takes the double minimum.
+__host__ __device__ __forceinline__ unsigned long long dmin_key(unsigned long long bits)
+{
+    return (bits >> 63) ? ~bits : (bits | 0x8000000000000000ull);
+}
+__host__ __device__ __forceinline__ unsigned long long dmin_bits(unsigned long long key)
+{
+    return (key >> 63) ? (key & 0x7fffffffffffffffull) : ~key;
+}
 
 // One balance slot: the dt-free contributions {a, b, c} of one edge to one cell's h, q and r
 // (hypComputeBalance, swSpHyp.cpp:221-263: h += a dt, q += b dt, r += c dt).

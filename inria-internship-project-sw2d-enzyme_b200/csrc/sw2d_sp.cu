@@ -1139,6 +1139,7 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
     Ctrl c0{};
     c0.t = params->t_0;
     c0.dt = 0.0;  // swSp.h:155
+    c0.dmin = kDminEmpty;
     c0.t_max = params->t_max;
     *h->ctrl_host = c0;
     if (cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)

@@ -413,51 +413,41 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
             if (x < best) best = x;
         }
     }
-    // warp -> block minimum, then the grid minimum in the last CTA done
+    // warp -> block minimum; the grid minimum by an integer atomicMin on the order-preserving key
+    // (the minimum does not depend on the order it is taken in; no candidate is NaN: a NaN bound
+    // never replaces best); dt_map snap and t_max clip in the last CTA done
     for (int off = 16; off > 0; off >>= 1) best = min_keep_t(best, __shfl_down_sync(0xffffffffu, best, off));
     __shared__ double wmin[kThreads / 32];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) wmin[wid] = best;
     __syncthreads();
-    if (wid == 0) {
-        best = (lane < kThreads / 32) ? wmin[lane] : m.dt_max;
-        for (int off = 16; off > 0; off >>= 1) best = min_keep_t(best, __shfl_down_sync(0xffffffffu, best, off));
-        if (lane == 0) {
-            m.part[blockIdx.x] = best;
-            __threadfence();
-            const unsigned done = atomicAdd(&ctrl->blocks_done, 1u);
-            last = (done == gridDim.x - 1);
-        }
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    double b2 = m.dt_max;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) b2 = min_keep_t(b2, ((volatile double*)m.part)[i]);
-    for (int off = 16; off > 0; off >>= 1) b2 = min_keep_t(b2, __shfl_down_sync(0xffffffffu, b2, off));
-    __syncthreads();
-    if (lane == 0) wmin[wid] = b2;
-    __syncthreads();
     if (threadIdx.x == 0) {
-        double dt = m.dt_max;
-        for (int w = 0; w < kThreads / 32; w++)
-            if (wmin[w] < dt) dt = wmin[w];
-        const double t = ctrl->t;
-        int store = m.dt_map <= -kSmallReal ? 1 : 0;
-        if (m.dt_map > kSmallReal) {
-            const int now = (int)(t / m.dt_map);
-            const int later = (int)((t + dt) / m.dt_map);
-            if (later > now) {
-                dt = later * m.dt_map - t;
-                store = 1;
+        for (int w = 1; w < kThreads / 32; w++) best = min_keep_t(best, wmin[w]);
+        atomicMin(&ctrl->dmin, dmin_key((unsigned long long)__double_as_longlong(best)));
+        __threadfence();
+        const unsigned done = atomicAdd(&ctrl->blocks_done, 1u);
+        last = (done == gridDim.x - 1);
+        if (last) {
+            __threadfence();
+            const unsigned long long key = atomicExch(&ctrl->dmin, kDminEmpty);
+            double dt = __longlong_as_double((long long)dmin_bits(key));
+            const double t = ctrl->t;
+            int store = m.dt_map <= -kSmallReal ? 1 : 0;
+            if (m.dt_map > kSmallReal) {
+                const int now = (int)(t / m.dt_map);
+                const int later = (int)((t + dt) / m.dt_map);
+                if (later > now) {
+                    dt = later * m.dt_map - t;
+                    store = 1;
+                }
             }
+            if ((t + dt) > ctrl->t_max) dt = ctrl->t_max - t;
+            ctrl->store_map = store;
+            ctrl->dt = dt;
+            ctrl->go = 1;
+            ctrl->blocks_done = 0;
         }
-        if ((t + dt) > ctrl->t_max) dt = ctrl->t_max - t;
-        ctrl->store_map = store;
-        ctrl->dt = dt;
-        ctrl->go = 1;
-        ctrl->blocks_done = 0;
     }
 }
 
@@ -467,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
 struct FluxVariant {
     int threads, minb;
 };
-constexpr FluxVariant kFluxVariants[] = {{256, 2}, {256, 3}, {192, 3}, {160, 4}, {320, 2}, {384, 2}};
+constexpr FluxVariant kFluxVariants[] = {{256, 2}, {256, 3}, {192, 3}, {320, 2}, {256, 4}, {128, 8}};
 constexpr int kNumFluxVariants = sizeof(kFluxVariants) / sizeof(kFluxVariants[0]);
 
 // The stage's byte layout (every section 16-byte aligned) for the largest tile; returns its size.
