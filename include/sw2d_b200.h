@@ -268,6 +268,12 @@ int sw2d_mlp_loss_grad(sw2d_mlp* m, const float* features, const float* targets,
                        float* grad);
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the gradient of the last sw2d_mlp_loss_grad */
 int sw2d_mlp_adam_step(sw2d_mlp* m, float lr);
+/* Poll limit of the first wait on each tensor-core chunk in this network's GEMMs (no counterpart
+ * in the reference): a wait that runs out sets the status, waits once more with the full limit
+ * for the MMA in flight, frees the kernel's TMEM and returns; the call then fails with
+ * SW2D_E_CUDA ("tensor-core wait ran out") and the network stays usable.  polls < 0 restores the
+ * default (2^26 polls, seconds); 0 makes every first wait give up at once (tests of that path). */
+int sw2d_mlp_set_wait_polls(sw2d_mlp* m, int64_t polls);
 
 /* Attaches a closure network to a DIP model (net NULL detaches).  The network then stands in
  * for the momentum-dissipation closure of the DIP balance (dip/swDipHyp.cpp:295-324): in every

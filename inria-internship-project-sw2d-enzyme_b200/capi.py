@@ -305,6 +305,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_mlp_loss_grad.restype = ctypes.c_int
     lib.sw2d_mlp_adam_step.argtypes = [P, ctypes.c_float]
     lib.sw2d_mlp_adam_step.restype = ctypes.c_int
+    lib.sw2d_mlp_set_wait_polls.argtypes = [P, ctypes.c_int64]
+    lib.sw2d_mlp_set_wait_polls.restype = ctypes.c_int
     lib.sw2d_set_closure.argtypes = [P, P, c_float_p, c_float_p, ctypes.c_float]
     lib.sw2d_set_closure.restype = ctypes.c_int
     lib.sw2d_map_porosity.argtypes = [ctypes.c_int, P, P, P, ctypes.c_int, P, P, P]
@@ -440,7 +442,7 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_case_read", "sw2d_case_array", "sw2d_case_info", "sw2d_case_option", "sw2d_case_create",
             "sw2d_case_free", "sw2d_case_last_error", "sw2d_mlp_param_count", "sw2d_mlp_create",
             "sw2d_mlp_destroy", "sw2d_mlp_last_error", "sw2d_mlp_get_params", "sw2d_mlp_infer",
-            "sw2d_mlp_loss_grad", "sw2d_mlp_adam_step", "sw2d_set_closure", "sw2d_closure_record", "sw2d_set_t_max",
+            "sw2d_mlp_loss_grad", "sw2d_mlp_adam_step", "sw2d_mlp_set_wait_polls", "sw2d_set_closure", "sw2d_closure_record", "sw2d_set_t_max",
             "sw2d_result_header", "sw2d_result_open", "sw2d_result_close", "sw2d_map_porosity", "sw2d_map_porosity_raster",
             "sw2d_map_last_error", "sw2d_step_n", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",

@@ -147,6 +147,10 @@ class MLP:
     def adam_step(self, lr: float) -> None:
         self._check(self.lib.sw2d_mlp_adam_step(self.h, float(lr)))
 
+    def set_wait_polls(self, polls: int) -> None:
+        """Poll limit of the first tensor-core wait of each chunk (< 0: the default)."""
+        self._check(self.lib.sw2d_mlp_set_wait_polls(self.h, int(polls)))
+
     def train(self, x, t, epochs: int = 10, batch: int = 4096, lr: float = 2e-3, seed: int = 0):
         """Mini-batch Adam over seeded shuffles; returns the per-epoch mean losses."""
         rng = np.random.default_rng(seed)

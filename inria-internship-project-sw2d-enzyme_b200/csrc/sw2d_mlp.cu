@@ -54,6 +54,7 @@ struct GemmArgs {
     int n_valid;             // columns written (<= N)
     uint32_t tmem_cols;      // power of two >= max(32, N)
     unsigned* status;
+    long long first_wait;    // polls of a chunk's first wait on the tensor core (the drain wait: kWaitPolls)
 };
 
 // GELU in its tanh form, 0.5 x (1 + tanh(k0 (x + k1 x^3))), with the hardware tanh
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(128) k_umma_gemm(GemmArgs g)
                          (k0 > 0 || s > 0) ? 1u : 0u);
             mma_commit(&bar);
         }
-        if (!mbar_wait(&bar, phase, kWaitPolls)) {
+        if (!mbar_wait(&bar, phase, g.first_wait)) {
             ok = false;
             mbar_wait(&bar, phase, kWaitPolls);  // the MMA still in flight: give it time once more
         }
@@ -258,6 +259,7 @@ struct sw2d_mlp {
     std::vector<void*> allocs;
     std::string err;
     unsigned* status = nullptr;
+    long long first_wait = kWaitPolls;  // sw2d_mlp_set_wait_polls
     // fp32 master parameters, Adam moments, gradients
     float *p = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr;
     // bf16 operand copies: W1 [64 x 16] (inputs padded), W2 [64 x 64], W3 [16 x 64] (outputs padded),
@@ -424,7 +426,8 @@ int gemm(sw2d_mlp* m, int mode, const __nv_bfloat16* A, int lda, const __nv_bflo
     if (!stream) stream = m->stream;
     if (N % 16 || N > kMaxN || K % 16 || K <= 0 || M <= 0 || (lda % 8) || (ldb % 8))
         return mlp_fail(m, SW2D_E_ARG, "gemm: shape outside the kernel's contract");
-    GemmArgs g{A, B, M, N, K, lda, ldb, bias, out, act, pre, ldo, ldact, n_valid, tmem_cols_for(N), m->status};
+    GemmArgs g{A, B, M, N, K, lda, ldb, bias, out, act, pre, ldo, ldact, n_valid, tmem_cols_for(N), m->status,
+               m->first_wait};
     const unsigned grid = (unsigned)((M + kTileM - 1) / kTileM);
     if (mode == kEpiStore) k_umma_gemm<kEpiStore><<<grid, 128, 0, stream>>>(g);
     else if (mode == kEpiGelu) k_umma_gemm<kEpiGelu><<<grid, 128, 0, stream>>>(g);
@@ -537,6 +540,13 @@ int sw2d_mlp_destroy(sw2d_mlp* m)
 
 const char* sw2d_mlp_last_error(sw2d_mlp* m) { return m ? m->err.c_str() : ""; }
 
+int sw2d_mlp_set_wait_polls(sw2d_mlp* m, int64_t polls)
+{
+    if (!m) return SW2D_E_ARG;
+    m->first_wait = polls < 0 ? kWaitPolls : (long long)polls;
+    return SW2D_OK;
+}
+
 int sw2d_mlp_get_params(sw2d_mlp* m, float* params)
 {
     using namespace sw2d;
@@ -576,7 +586,11 @@ int sw2d_mlp_infer(sw2d_mlp* m, const float* features, int64_t n, float* outputs
     MCK(cudaStreamSynchronize(m->stream));
     unsigned st = 0;
     MCK(cudaMemcpy(&st, m->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (st) return mlp_fail(m, SW2D_E_CUDA, "tensor-core wait ran out");
+    if (st) {
+        // reported once: the kernel that ran out freed its TMEM, and the object stays usable
+        MCK(cudaMemset(m->status, 0, sizeof(unsigned)));
+        return mlp_fail(m, SW2D_E_CUDA, "tensor-core wait ran out");
+    }
     for (int64_t i = 0; i < n; i++)
         for (int k = 0; k < kOut; k++) outputs[i * kOut + k] = y[i * kOutPad + k] * m->ystd[k] + m->ymean[k];
     return SW2D_OK;
@@ -642,7 +656,11 @@ int sw2d_mlp_loss_grad(sw2d_mlp* m, const float* features, const float* targets,
     MCK(cudaStreamSynchronize(m->stream));
     unsigned st = 0;
     MCK(cudaMemcpy(&st, m->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (st) return mlp_fail(m, SW2D_E_CUDA, "tensor-core wait ran out");
+    if (st) {
+        // reported once: the kernel that ran out freed its TMEM, and the object stays usable
+        MCK(cudaMemset(m->status, 0, sizeof(unsigned)));
+        return mlp_fail(m, SW2D_E_CUDA, "tensor-core wait ran out");
+    }
     double s = 0.0;
     for (float v : part) s += v;
     if (loss) *loss = s / (double)(n * kOut);

@@ -71,3 +71,22 @@ def test_training_reduces_loss_and_is_deterministic(C):
     hist = runs[0][0]
     assert hist[-1] < 0.05 * hist[0], hist
     assert np.array_equal(runs[0][1].view(np.int32), runs[1][1].view(np.int32))
+
+
+def test_tensor_core_wait_that_runs_out(C):
+    """A first wait on the tensor core that gives up at once (poll limit 0): the GEMM kernel sets
+    the status, waits once more with the full limit for the MMA in flight, frees its TMEM and
+    returns; the call fails with "tensor-core wait ran out".  Back to the default limit, the same
+    network gives the same outputs as before, twice (its TMEM was released and the status was
+    cleared after being reported)."""
+    rng, norm, x = _setup(9, 700)
+    net = C.MLP(C.init_params(3), norm)
+    y0 = net.infer(x)
+    net.set_wait_polls(0)
+    for _ in range(2):
+        with pytest.raises(RuntimeError, match="tensor-core wait ran out"):
+            net.infer(x)
+    net.set_wait_polls(-1)
+    for _ in range(2):
+        y1 = net.infer(x)
+        assert np.array_equal(y0.view(np.int32), y1.view(np.int32))
