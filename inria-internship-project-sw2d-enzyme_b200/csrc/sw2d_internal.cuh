@@ -85,6 +85,7 @@ struct TileInfo {
 
 struct TileMesh {
     int ntiles = 0, tile_cells = 0;
+    int slopes_in = 1;  // MUSCL-EVR: 1 slopes computed by k_flux (ring 2 staged); 0 read from k_slopes' output
     // the largest tile: staged cells, tile + ring-1 cells, tile cells, slot range, flux edges, all
     // tile edges, neighbour-list entries
     int nl_max = 0, nf_max = 0, nt_max = 0, ns_max = 0, ne_max = 0, na_max = 0, nent_max = 0;
@@ -236,6 +237,7 @@ struct sw2d_handle {
     std::vector<int2> h_coff, h_cint, h_lr;  // host tables the tiles are built from
     std::vector<int> h_bcell;
     int fused = 0;                      // step as the two kernels k_flux + k_update (option "fused_step")
+    int fused_slopes = 1;               // MUSCL-EVR: slopes inside k_flux (1) or by k_slopes first (0)
     int flux_variant = 0;               // launch variant of k_flux (sw2d_autotune)
     std::string err;
 };

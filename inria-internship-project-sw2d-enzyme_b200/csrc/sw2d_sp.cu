@@ -651,8 +651,10 @@ void launch_update_s(sw2d_handle* h, const DevMesh& m)
     else launch_update_d<kStoreB, false>(h, m);
 }
 
-// kernels of one step: the fused step's k_flux and k_update, or the four-kernel step
-int n_phases(const sw2d_handle* h) { return h->fused ? 2 : 4; }
+// kernels of one step: the fused step's k_flux and k_update (with k_slopes first when the
+// MUSCL-EVR slopes are not computed inside k_flux), or the four-kernel step
+bool slopes_first(const sw2d_handle* h) { return h->p.scheme == SW2D_SCHEME_MUSCL_EVR && !h->tiles.slopes_in; }
+int n_phases(const sw2d_handle* h) { return h->fused ? (slopes_first(h) ? 3 : 2) : 4; }
 
 // phase i of one step on the handle's stream: fused step 0 flux, 1 update; four-kernel step (and
 // DDP) 0 slopes, 1 edges, 2 cfl, 3 update
@@ -664,6 +666,12 @@ void launch_phase(sw2d_handle* h, int i)
     }
     DevMesh& m = h->m;
     if (h->fused) {
+        if (slopes_first(h)) {
+            if (i == 0) launch_slopes(h, h->slope_variant);
+            else if (i == 1) launch_flux(h, m, h->flux_variant, false);
+            else launch_update_s<false>(h, m);
+            return;
+        }
         if (i == 0) launch_flux(h, m, h->flux_variant, false);
         else launch_update_s<false>(h, m);
         return;
@@ -1306,7 +1314,11 @@ const char* sw2d_phase_name(int i)
 const char* sw2d_phase_label(sw2d_handle* h, int i)
 {
     static const char* fused[] = {"k_flux", "k_update"};
-    if (h && h->model != kModelDdp && h->fused) return (i >= 0 && i < 2) ? fused[i] : "";
+    static const char* fused3[] = {"k_slopes", "k_flux", "k_update"};
+    if (h && h->model != kModelDdp && h->fused) {
+        if (slopes_first(h)) return (i >= 0 && i < 3) ? fused3[i] : "";
+        return (i >= 0 && i < 2) ? fused[i] : "";
+    }
     return sw2d_phase_name(i);
 }
 
@@ -1332,6 +1344,19 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
     // run (slopes, balance slots, CFL contributions, the pending dt), so timing them does not
     // advance the run.
     if (h->fused) {
+        if (slopes_first(h)) {
+            double bs = 1e300;
+            for (int v = 0; v < kNumVariants; v++) {
+                double ms = time_it([&] { launch_slopes(h, v); });
+                rep += "k_slopes/" + std::to_string(kVariants[v].block) + "x" + std::to_string(kVariants[v].minb) + "=" +
+                       std::to_string(ms) + "ms ";
+                if (ms < bs) {
+                    bs = ms;
+                    h->slope_variant = v;
+                }
+            }
+            launch_slopes(h, h->slope_variant);
+        }
         double best = 1e300;
         for (int v = 0; v < flux_variants(); v++) {
             if (launch_flux(h, h->m, v, true) != cudaSuccess) continue;
@@ -1488,6 +1513,20 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
             if (!h->tiles.ntiles) h->fused = 0;  // the previous tiles are kept unless they were released
             return fail(h, rc, "tile_cells: " + (why.empty() ? h->err : why));
         }
+    } else if (std::strcmp(name, "fused_slopes") == 0) {
+        // MUSCL-EVR fused step: 1 the slopes inside k_flux (ring 2 staged), 0 k_slopes first and
+        // k_flux reading its output (the same results); the tiles are rebuilt
+        if (h->model == kModelDdp) return fail(h, SW2D_E_UNSUPPORTED, "the DDP model has no tiles");
+        CK(cudaStreamSynchronize(h->stream));
+        const int prev = h->fused_slopes;
+        h->fused_slopes = value ? 1 : 0;
+        std::string why;
+        const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, h->tiles.tile_cells, why);
+        if (rc) {
+            h->fused_slopes = prev;
+            if (!h->tiles.ntiles) h->fused = 0;
+            return fail(h, rc, "fused_slopes: " + (why.empty() ? h->err : why));
+        }
     } else if (std::strcmp(name, "update_reverse") == 0) {
         // block order of the cell update: 1 from the last cells to the first (the same results)
         h->m.rev_update = value ? 1 : 0;
@@ -1515,6 +1554,7 @@ int sw2d_get_option(sw2d_handle* h, const char* name, int64_t* value)
     if (std::strcmp(name, "fused_step") == 0) *value = h->fused;
     else if (std::strcmp(name, "flux_variant") == 0) *value = h->flux_variant;
     else if (std::strcmp(name, "update_reverse") == 0) *value = h->m.rev_update;
+    else if (std::strcmp(name, "fused_slopes") == 0) *value = h->fused_slopes;
     else if (std::strcmp(name, "tile_cells") == 0) *value = h->tiles.tile_cells;
     else if (std::strcmp(name, "record_fluxes") == 0) *value = h->m.flux != nullptr;
     else if (std::strcmp(name, "record_wave_speeds") == 0) *value = h->m.lmax != nullptr;
@@ -1612,7 +1652,7 @@ int64_t sw2d_get_array(sw2d_handle* h, const char* name, double* out, int64_t ca
         const int64_t r = ddp_get_array(h, name, out, capacity, &handled);
         if (handled) return r;
     }
-    if (h->fused && !h->m.flux && !h->m.lmax &&
+    if (h->fused && h->tiles.slopes_in && h->p.scheme == SW2D_SCHEME_MUSCL_EVR && !h->m.flux && !h->m.lmax &&
         (std::strcmp(name, "slope_x") == 0 || std::strcmp(name, "slope_y") == 0))
         return fail(h, SW2D_E_ARG, "the fused step keeps the slopes only with the option record_fluxes or "
                                    "record_wave_speeds on");
@@ -1725,7 +1765,7 @@ int64_t sw2d_get_array_noalloc(sw2d_handle* h, const char* name, double* out, in
         const int64_t r = ddp_get_array_staged(h, name, out, capacity, stage, kNoAllocMaxDoubles, &handled);
         if (handled) return r;
     }
-    if (h->fused && !h->m.flux && !h->m.lmax &&
+    if (h->fused && h->tiles.slopes_in && h->p.scheme == SW2D_SCHEME_MUSCL_EVR && !h->m.flux && !h->m.lmax &&
         (std::strcmp(name, "slope_x") == 0 || std::strcmp(name, "slope_y") == 0))
         return fail(h, SW2D_E_ARG, "the fused step keeps the slopes only with the option record_fluxes or "
                                    "record_wave_speeds on");
@@ -1794,7 +1834,7 @@ int sw2d_kernels_per_step(sw2d_handle* h)
 {
     if (!h) return 0;
     if (h->model == kModelDdp) return ddp_kernels_per_step(h);
-    if (h->fused) return 2;
+    if (h->fused) return n_phases(h);
     return h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? 4 : 3;
 }
 

@@ -234,7 +234,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
     // ---- stage the tile (contiguous), its rings (gathered) and its edges, all copies in flight
     {
         const int c0 = TI(c0), nt = TI(nt), hoff = TI(hoff);
-        const int nf = nt + TI(nh1), nl = kMuscl ? nf + TI(nh2) : nf;
+        const bool own_slopes = kMuscl && tm.slopes_in;
+        const int nf = nt + TI(nh1), nl = own_slopes ? nf + TI(nh2) : nf;
         for (int l = threadIdx.x; l < nl; l += kThreads) {
             const int g = (l < nt) ? c0 + l : ld(&tm.halo[hoff + l - nt]);
             const double2* sg = reinterpret_cast<const double2*>(m.st + g);
@@ -245,11 +246,12 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
                 const double2* cg = reinterpret_cast<const double2*>(m.cst + g);
                 cpa16(reinterpret_cast<double2*>(sv.cst + l), cg);
                 cpa16(reinterpret_cast<double2*>(sv.cst + l) + 1, cg + 1);
+                if (kMuscl && !own_slopes) cpa16(sv.sl + l, m.slope + g);
             }
         }
         for (int l = threadIdx.x; l <= nt; l += kThreads) cpa8(sv.coff + l, m.coff + c0 + l);
         const int e0 = TI(e0), ne_own = TI(ne_own), xoff = TI(xoff), loff = TI(loff);
-        const int nflux = ne_own + TI(nx_flux), nall = kMuscl ? nflux + TI(nx_slope) : nflux;
+        const int nflux = ne_own + TI(nx_flux), nall = own_slopes ? nflux + TI(nx_slope) : nflux;
         for (int j = threadIdx.x; j < nall; j += kThreads) {
             const int e = (j < ne_own) ? e0 + j : ld(&tm.xe[xoff + j - ne_own]);
             cpa4(sv.ell + j, tm.eloc + loff + j);
@@ -262,7 +264,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
                 if (kDip) cpa8(sv.epg + j, m.phig + e);
             }
         }
-        if (kMuscl) {
+        if (own_slopes) {
             const int soff = TI(soff), so_off = TI(so_off), nent = TI(nent);
             for (int k = threadIdx.x; k < nent; k += kThreads) cpa4(sv.ent + k, tm.scsr + soff + k);
             for (int l = threadIdx.x; l <= nf; l += kThreads) cpa4(sv.so + l, tm.soffs + so_off + l);
@@ -271,8 +273,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_flux(DevMesh m, TileMesh tm
     }
     __syncthreads();
 
-    // ---- slopes of the tile and ring-1 cells (computeMusclSlopes)
-    if (kMuscl) {
+    // ---- slopes of the tile and ring-1 cells (computeMusclSlopes), unless k_slopes computed them
+    if (kMuscl && tm.slopes_in) {
         const int c0 = TI(c0), nt = TI(nt), nf = nt + TI(nh1);
         const bool keep = m.flux != nullptr || m.lmax != nullptr;
         for (int l = threadIdx.x; l < nf; l += kThreads) {
@@ -461,17 +463,18 @@ constexpr FluxVariant kFluxVariants[] = {{256, 2}, {256, 3}, {192, 3}, {320, 2},
 constexpr int kNumFluxVariants = sizeof(kFluxVariants) / sizeof(kFluxVariants[0]);
 
 // The stage's byte layout (every section 16-byte aligned) for the largest tile; returns its size.
-size_t stage_layout(TileMesh& tm, bool muscl, bool dip)
+size_t stage_layout(TileMesh& tm, bool muscl, bool slopes_read, bool dip)
 {
     size_t o = 0;
     auto sec = [&](int* off, size_t bytes) {
         *off = (int)o;
         o += (bytes + 15) & ~(size_t)15;
     };
+    const bool evr = muscl || slopes_read;
     sec(&tm.o_st, 32 * (size_t)tm.nl_max);
     sec(&tm.o_cst, 32 * (size_t)tm.nf_max);
-    sec(&tm.o_xy, muscl ? 16 * (size_t)tm.nl_max : 0);
-    sec(&tm.o_sl, muscl ? 16 * (size_t)tm.nf_max : 0);
+    sec(&tm.o_xy, evr ? 16 * (size_t)tm.nl_max : 0);
+    sec(&tm.o_sl, evr ? 16 * (size_t)tm.nf_max : 0);
     sec(&tm.o_coff, 8 * ((size_t)tm.nt_max + 1));
     sec(&tm.o_lam, 8 * (size_t)tm.ns_max);
     sec(&tm.o_en, 16 * (size_t)tm.ne_max);
@@ -479,7 +482,7 @@ size_t stage_layout(TileMesh& tm, bool muscl, bool dip)
     sec(&tm.o_elen, 8 * (size_t)tm.ne_max);
     sec(&tm.o_esl, 8 * (size_t)tm.ne_max);
     sec(&tm.o_epg, dip ? 8 * (size_t)tm.ne_max : 0);
-    sec(&tm.o_em, muscl ? 16 * (size_t)tm.na_max : 0);
+    sec(&tm.o_em, evr ? 16 * (size_t)tm.na_max : 0);
     sec(&tm.o_ell, 4 * (size_t)tm.na_max);
     sec(&tm.o_ent, muscl ? 4 * (size_t)tm.nent_max : 0);
     sec(&tm.o_so, muscl ? 4 * ((size_t)tm.nf_max + 1) : 0);
@@ -551,7 +554,9 @@ cudaError_t launch_flux(sw2d_handle* h, const DevMesh& m, int v, bool attr_only)
 int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector<int2>& cint,
                 const std::vector<int2>& lr, const std::vector<int>& bcell, int tile_cells, std::string& why)
 {
-    const bool muscl = h->p.scheme == SW2D_SCHEME_MUSCL_EVR;
+    // ring 2, the ring-1 slope edges and the neighbour lists serve the slopes k_flux computes
+    const bool muscl = h->p.scheme == SW2D_SCHEME_MUSCL_EVR && h->fused_slopes;
+    const bool slopes_read = h->p.scheme == SW2D_SCHEME_MUSCL_EVR && !h->fused_slopes;
     const int nc = (int)h->nc, ni = (int)h->ni, nb = (int)h->nb;
     if (tile_cells < 32 || tile_cells > 8192) {
         why = "tile size outside 32..8192 cells";
@@ -698,7 +703,8 @@ int tiles_build(sw2d_handle* h, const std::vector<int2>& coff, const std::vector
     probe.ne_max = ne_max;
     probe.na_max = na_max;
     probe.nent_max = nent_max;
-    const size_t smem = stage_layout(probe, muscl, h->model == kModelDip);
+    probe.slopes_in = muscl ? 1 : 0;
+    const size_t smem = stage_layout(probe, muscl, slopes_read, h->model == kModelDip);
     if (smem > 200 * 1024) {
         why = "a tile's shared-memory stage exceeds 200 KB";
         return SW2D_E_UNSUPPORTED;

@@ -43,9 +43,12 @@ def pkg():
     return p
 
 
-def _pair(pkg, case, tile):
+def _pair(pkg, case, tile, slopes_in=1):
     fused = pkg.SpModel(case)
-    assert fused.kernels_per_step == 2, "the SP and DIP models step as two kernels by default"
+    assert fused.get_option("fused_step") == 1
+    fused.set_option("fused_slopes", slopes_in)
+    muscl = case.opts["num_scheme"] == "muscl_evr"
+    assert fused.kernels_per_step == (3 if muscl and not slopes_in else 2)
     if tile is not None:
         fused.set_option("tile_cells", tile)
     four = pkg.SpModel(case)
@@ -61,12 +64,14 @@ def _same(a, b):
     return np.array_equal(np.asarray(a).view(np.int64), np.asarray(b).view(np.int64))
 
 
-@pytest.mark.parametrize("tile", [32, 97, 320, None])
+@pytest.mark.parametrize("tile,slopes_in", [(32, 1), (97, 1), (320, 1), (None, 1), (97, 0), (None, 0)])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_fused_matches_four_kernel_step(pkg, name, tile):
+def test_fused_matches_four_kernel_step(pkg, name, tile, slopes_in):
     kind, kwargs = CASES[name]
     case = getattr(pkg.workloads, kind)(**kwargs)
-    fused, four = _pair(pkg, case, tile)
+    if not slopes_in and case.opts["num_scheme"] != "muscl_evr":
+        pytest.skip("slopes exist only in the MUSCL-EVR scheme")
+    fused, four = _pair(pkg, case, tile, slopes_in)
     names = list(ARRAYS)
     if case.opts["num_scheme"] == "muscl_evr":
         names += ["slope_x", "slope_y"]
@@ -96,6 +101,9 @@ def test_fused_phase_labels_and_switch(pkg):
     m = pkg.SpModel(case)
     ph = m.phase_times(3)
     assert list(ph) == ["k_flux", "k_update"]
+    m.set_option("fused_slopes", 0)
+    assert list(m.phase_times(3)) == ["k_slopes", "k_flux", "k_update"] and m.kernels_per_step == 3
+    m.set_option("fused_slopes", 1)
     m.set_option("fused_step", 0)
     ph = m.phase_times(3)
     assert list(ph) == ["k_slopes", "k_edges", "k_cfl", "k_update"]
