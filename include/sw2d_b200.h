@@ -437,11 +437,22 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value);
 int sw2d_get_option(sw2d_handle* h, const char* name, int64_t* value);
 
 /* Launch-configuration autotuner (no counterpart in the reference): times every
- * {threads per block, register cap} variant of the slope and edge kernels `iters` times on the
- * current state (those kernels recompute the same outputs from the same state, so the run does
- * not advance), keeps the fastest and writes a one-line report.  The chosen variants can be
- * read back and set again (sw2d_get/set_launch_config) so that a caller can persist them. */
+ * {threads per block, register cap} variant of the kernels of the handle's current step form
+ * (k_slopes and k_edges, or k_flux) `iters` times on the current state, keeps the fastest and
+ * writes a one-line report.  Those kernels recompute the same outputs from the same state; the
+ * control block (time, dt, pending dt) is saved before and put back after, so the run continues
+ * with the same bits as without the call.  The chosen variants can be read back and set again
+ * (sw2d_get/set_launch_config, the "flux_variant" option) so that a caller can persist them. */
 int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity);
+/* Step-form autotuner (no counterpart in the reference): times, on the current state, the
+ * four-kernel step and the fused step at each of the n_tile_sizes tile sizes (192, 256, 320, 384,
+ * 512 cells when n_tile_sizes is 0), for MUSCL-EVR with the slopes inside k_flux and with
+ * k_slopes first, each at its fastest launch variant (k_update, the same in every form, is left
+ * out of the sums); then sets the fastest form ("fused_step", "fused_slopes", "tile_cells",
+ * "flux_variant" and the launch config can be read back to persist it).  The run continues with
+ * the same bits, as for sw2d_autotune.  DDP handles: sw2d_autotune. */
+int sw2d_autotune_step(sw2d_handle* h, int iters, const int* tile_sizes, int n_tile_sizes, char* report,
+                       int capacity);
 int sw2d_get_launch_config(sw2d_handle* h, int* slopes_variant, int* edges_variant);
 int sw2d_set_launch_config(sw2d_handle* h, int slopes_variant, int edges_variant);
 

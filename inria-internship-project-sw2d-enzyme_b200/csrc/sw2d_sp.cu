@@ -1330,6 +1330,18 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     std::string rep;
+    // The timed kernels recompute their outputs (slopes, balance slots, CFL contributions) from the
+    // state, but k_flux and k_cfl also write the pending dt into the control block, which the
+    // MUSCL-EVR reconstruction of the next step reads as the previous dt: the block is saved here
+    // and put back once the timings are done, so the run continues as if nothing had been timed.
+    Ctrl saved;
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(&saved, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    auto restore = [&]() -> int {
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaMemcpy(h->ctrl, &saved, sizeof(Ctrl), cudaMemcpyHostToDevice));
+        return SW2D_OK;
+    };
     auto time_it = [&](auto&& launch) {
         launch();  // warm
         cudaEventRecord(e0, h->stream);
@@ -1340,9 +1352,6 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
         cudaEventElapsedTime(&ms, e0, e1);
         return (double)ms / iters;
     };
-    // k_flux, k_slopes and k_edges recompute the same outputs from the same state every time they
-    // run (slopes, balance slots, CFL contributions, the pending dt), so timing them does not
-    // advance the run.
     if (h->fused) {
         if (slopes_first(h)) {
             double bs = 1e300;
@@ -1367,11 +1376,10 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
                 h->flux_variant = v;
             }
         }
-        launch_flux(h, h->m, h->flux_variant, false);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(h->stream));
+        if (const int rc = restore()) return rc;
         if (h->graph) {
             cudaGraphExecDestroy(h->graph);
             h->graph = nullptr;
@@ -1414,7 +1422,7 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(h->stream));
+    if (const int rc = restore()) return rc;
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
         h->graph = nullptr;
@@ -1422,6 +1430,134 @@ int sw2d_autotune(sw2d_handle* h, int iters, char* report, int capacity)
     rep += "chosen k_slopes/" + std::to_string(kVariants[h->slope_variant].block) + "x" +
            std::to_string(kVariants[h->slope_variant].minb) + (h->model == kModelDdp ? " k_ddp_edges/" : " k_edges/") +
            label(h->edge_variant);
+    if (report && capacity > 0) {
+        std::strncpy(report, rep.c_str(), (size_t)capacity - 1);
+        report[capacity - 1] = '\0';
+    }
+    return SW2D_OK;
+}
+
+int sw2d_autotune_step(sw2d_handle* h, int iters, const int* tile_sizes, int n_tile_sizes, char* report,
+                       int capacity)
+{
+    if (!h || iters <= 0 || n_tile_sizes < 0 || (n_tile_sizes && !tile_sizes))
+        return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (h->model == kModelDdp || !h->tiles.ntiles) return sw2d_autotune(h, iters, report, capacity);
+    CK(cudaSetDevice(h->device));
+    static const int kDefaultTiles[] = {192, 256, 320, 384, 512};
+    if (!n_tile_sizes) {
+        tile_sizes = kDefaultTiles;
+        n_tile_sizes = (int)(sizeof(kDefaultTiles) / sizeof(int));
+    }
+    // the timed kernels write the pending dt (read as the previous dt by the next MUSCL-EVR step):
+    // the control block is put back at the end, as in sw2d_autotune
+    Ctrl saved;
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(&saved, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time_it = [&](auto&& launch) {
+        launch();  // warm
+        cudaEventRecord(e0, h->stream);
+        for (int i = 0; i < iters; i++) launch();
+        cudaEventRecord(e1, h->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return (double)ms / iters;
+    };
+    const bool muscl = h->p.scheme == SW2D_SCHEME_MUSCL_EVR;
+    std::string rep;
+    // k_slopes at its fastest launch variant (shared by the four-kernel step and the fused step
+    // that computes the slopes first)
+    double t_slopes = 0.0;
+    int slope_v = h->slope_variant;
+    if (muscl) {
+        t_slopes = 1e300;
+        for (int v = 0; v < kNumVariants; v++) {
+            const double ms = time_it([&] { launch_slopes(h, v); });
+            if (ms < t_slopes) {
+                t_slopes = ms;
+                slope_v = v;
+            }
+        }
+        launch_slopes(h, slope_v);  // the slopes k_flux reads when it does not compute them
+    }
+    // four-kernel step: k_slopes + k_edges + k_cfl (k_update is the same in every form)
+    double t_edges = 1e300;
+    int edge_v = h->edge_variant;
+    for (int v = 0; v < kNumVariants; v++) {
+        const double ms = time_it([&] { launch_edges(h, v); });
+        if (ms < t_edges) {
+            t_edges = ms;
+            edge_v = v;
+        }
+    }
+    const double t_cfl = time_it([&] { k_cfl<false><<<cfl_grid(h, h->m.nc), kBlock, 0, h->stream>>>(h->m); });
+    const double t_four = t_slopes + t_edges + t_cfl;
+    rep += "four-kernel=" + std::to_string(t_four) + "ms ";
+    // fused forms: for MUSCL-EVR both places of the slopes, every tile size
+    struct Best {
+        double ms;
+        int fused, fused_slopes, tile, flux_v;
+    } best{t_four, 0, h->fused_slopes, h->tiles.tile_cells, h->flux_variant};
+    const int prev_fs = h->fused_slopes, prev_tile = h->tiles.tile_cells;
+    for (int fs = muscl ? 0 : h->fused_slopes; fs <= (muscl ? 1 : h->fused_slopes); fs++) {
+        h->fused_slopes = fs;
+        for (int k = 0; k < n_tile_sizes; k++) {
+            std::string why;
+            if (tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, tile_sizes[k], why)) {
+                rep += "tile " + std::to_string(tile_sizes[k]) + " refused ";
+                continue;
+            }
+            const double pre = slopes_first(h) ? t_slopes : 0.0;
+            double bf = 1e300;
+            int bv = 0;
+            for (int v = 0; v < flux_variants(); v++) {
+                if (launch_flux(h, h->m, v, true) != cudaSuccess) continue;
+                const double ms = time_it([&] { launch_flux(h, h->m, v, false); });
+                if (ms < bf) {
+                    bf = ms;
+                    bv = v;
+                }
+            }
+            rep += std::string(muscl ? (fs ? "fused" : "fused/slopes-first") : "fused") + "/tile" +
+                   std::to_string(tile_sizes[k]) + "/" + flux_variant_label(bv) + "=" + std::to_string(pre + bf) +
+                   "ms ";
+            if (pre + bf < best.ms) best = {pre + bf, 1, fs, tile_sizes[k], bv};
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    // the chosen form (tiles rebuilt for it; the previous tiles when the four-kernel step wins)
+    h->fused_slopes = best.fused ? best.fused_slopes : prev_fs;
+    {
+        std::string why;
+        const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, best.fused ? best.tile : prev_tile, why);
+        if (rc) {
+            h->fused = 0;
+            return fail(h, rc, "autotune_step: " + (why.empty() ? h->err : why));
+        }
+    }
+    h->fused = best.fused;
+    h->slope_variant = slope_v;
+    h->edge_variant = edge_v;
+    h->flux_variant = best.flux_v;
+    CK(cudaMemcpy(h->ctrl, &saved, sizeof(Ctrl), cudaMemcpyHostToDevice));
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    if (best.fused)
+        rep += "chosen fused" + std::string(muscl ? (best.fused_slopes ? "" : "/slopes-first") : "") + " tile " +
+               std::to_string(best.tile) + " k_flux/" + flux_variant_label(best.flux_v);
+    else
+        rep += "chosen four-kernel k_slopes/" + std::to_string(kVariants[slope_v].block) + "x" +
+               std::to_string(kVariants[slope_v].minb) + " k_edges/" + std::to_string(kVariants[edge_v].block) + "x" +
+               std::to_string(kVariants[edge_v].minb);
     if (report && capacity > 0) {
         std::strncpy(report, rep.c_str(), (size_t)capacity - 1);
         report[capacity - 1] = '\0';

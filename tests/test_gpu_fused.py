@@ -124,10 +124,45 @@ def test_fused_autotune_keeps_results(pkg):
     a = pkg.SpModel(case)
     b = pkg.SpModel(case)
     a.step(5)
-    b.step(5)
+    b.step(4)
+    dt4 = b.dt
+    b.step(1)
+    # the MUSCL-EVR step reads the previous dt: the case must have one that changes
+    assert b.dt != dt4
     rep = pkg.tuning.autotune(a, iters=2, cache_path=None)
     assert "k_flux/" in rep["report"]
     assert a.step(50) == b.step(50)
     for x, y in zip(a.state(), b.state()):
         assert _same(x, y)
     assert a.time == b.time
+
+
+@pytest.mark.parametrize("scheme", ["muscl_evr", "godunov"])
+def test_autotune_step_keeps_results(pkg, scheme, tmp_path):
+    """sw2d_autotune_step times the four-kernel step and the fused step at several tile sizes
+    (and both places of the MUSCL-EVR slopes) on the live state, then sets the fastest form; the
+    run continues with the same bits, and the cached choice is applied to a new model."""
+    case = pkg.workloads.gaussian_bumps(n_cells=20000, mesh="delaunay", initial="dam", scheme=scheme)
+    a = pkg.SpModel(case)
+    b = pkg.SpModel(case)
+    a.step(5)
+    b.step(5)
+    cache = str(tmp_path / "tune.json")
+    rep = pkg.tuning.autotune_step(a, iters=2, tile_sizes=(97, 256), cache_path=cache)
+    assert "four-kernel=" in rep["report"] and "tile97" in rep["report"] and "chosen" in rep["report"]
+    if scheme == "muscl_evr":
+        assert "slopes-first/tile256" in rep["report"]
+    assert rep["fused"] == a.get_option("fused_step")
+    if rep["fused"]:
+        assert a.get_option("tile_cells") == rep["tile"] and a.get_option("flux_variant") == rep["flux"]
+    assert a.step(50) == b.step(50)
+    for x, y in zip(a.state(), b.state()):
+        assert _same(x, y)
+    assert a.time == b.time
+    c = pkg.SpModel(case)
+    again = pkg.tuning.autotune_step(c, iters=2, tile_sizes=(97, 256), cache_path=cache)
+    assert again["cached"] and c.get_option("fused_step") == rep["fused"]
+    c.step(5)
+    assert c.step(50) == 50
+    for x, y in zip(c.state(), b.state()):
+        assert _same(x, y)
