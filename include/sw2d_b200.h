@@ -372,6 +372,11 @@ int sw2d_result_close(sw2d_handle* h);
  * stopping once t >= t_max.  The loop runs on the device (CUDA graph); the host does not
  * synchronise between steps.  *steps_done receives the number of steps taken (may be NULL). */
 int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done);
+/* Captures and instantiates the CUDA graph sw2d_step_n launches (32 steps, or the result file's
+ * chunk), without taking a step, so that a timed run does not include the capture; the graph is
+ * captured again after an option or launch configuration changes.  No counterpart in the
+ * reference. */
+int sw2d_prepare_steps(sw2d_handle* h);
 
 /* Replaces swSp::execute (swSp.cpp:482-670) without result storage: runs until t >= t_max. */
 int sw2d_execute(sw2d_handle* h, int64_t* steps_done);
@@ -415,13 +420,17 @@ const char* sw2d_phase_label(sw2d_handle* h, int i);
 /* Phase names of the four-kernel step ("k_slopes", "k_edges", "k_cfl", "k_update"). */
 const char* sw2d_phase_name(int i);
 
-/* Run-time options.  "fused_step" (0/1): 1 (the default for the SP and DIP models) runs each
- * time step as two kernels, k_flux (per tile of consecutive cells staged with their two rings
- * of neighbours in shared memory: slopes, Riemann states, fluxes, balance terms, CFL bound and
- * the grid's dt) and k_update; 0 runs the four-kernel step (k_slopes, k_edges, k_cfl, k_update).
- * Both give the same bits.  "tile_cells" (32..8192): cells per tile of the fused step (512 by
+/* Run-time options.  "fused_step" (0/1): 1 runs each time step as k_flux (per tile of
+ * consecutive cells staged with their neighbours in shared memory: Riemann states, fluxes,
+ * balance terms, CFL bound and the grid's dt) and k_update, with k_slopes first for MUSCL-EVR
+ * unless "fused_slopes" is 1 (then k_flux also stages the second ring of neighbours and computes
+ * the slopes itself); 0 runs the four-kernel step (k_slopes, k_edges, k_cfl, k_update).  Every
+ * form gives the same bits.  Defaults: 1 for Godunov, 0 for MUSCL-EVR (the faster forms on
+ * B200; sw2d_autotune_step measures them).  "fused_slopes" (0/1, default 0): see above; the
+ * tiles are rebuilt.  "tile_cells" (32..8192): cells per tile of the fused step (384 by
  * default, or the environment variable SW2D_TILE_CELLS read when the handle is created); the
  * tiles are rebuilt.  "flux_variant": the launch variant of k_flux (sw2d_autotune picks it).
+ * "update_reverse" (0/1): k_update takes its blocks from the last cells to the first.
  * "record_wave_speeds" (0/1): also keep lambda_max per edge for
  * sw2d_get_array("lambda_max_int"/"lambda_max_bnd") (the reference's lambda_max_int/_bnd
  * members, swSp.h:201-203); off by default since the step itself only needs lambda_max * length.

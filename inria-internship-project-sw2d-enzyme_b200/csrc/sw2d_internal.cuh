@@ -237,7 +237,7 @@ struct sw2d_handle {
     std::vector<int2> h_coff, h_cint, h_lr;  // host tables the tiles are built from
     std::vector<int> h_bcell;
     int fused = 0;                      // step as the two kernels k_flux + k_update (option "fused_step")
-    int fused_slopes = 1;               // MUSCL-EVR: slopes inside k_flux (1) or by k_slopes first (0)
+    int fused_slopes = 0;               // MUSCL-EVR: slopes inside k_flux (1) or by k_slopes first (0)
     int flux_variant = 0;               // launch variant of k_flux (sw2d_autotune)
     std::string err;
 };

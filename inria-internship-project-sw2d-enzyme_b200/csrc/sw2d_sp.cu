@@ -547,7 +547,7 @@ int status_to_code(sw2d_handle* h, unsigned st)
 
 namespace {
 
-constexpr int kDefaultTileCells = 512;  // cells per tile of the fused step
+constexpr int kDefaultTileCells = 384;  // cells per tile of the fused step
 
 // Launch variants {threads per block, minimum resident blocks per SM (register cap)} of the
 // two heaviest kernels; sw2d_autotune times them on the live state and keeps the fastest.
@@ -728,6 +728,9 @@ void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance)
 }  // namespace sw2d
 
 namespace {
+
+// steps per launch of the captured step graph (sw2d_step_n without a result file)
+constexpr int kGraphSteps = 32;
 
 int ensure_graph(sw2d_handle* h, int steps)
 {
@@ -1157,8 +1160,11 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
         return bail(fail(h, SW2D_E_CUDA, "initialisation kernels failed"));
     if ((rc = noalloc_prepare(h))) return bail(rc);
     if (!ddp) {
-        // tiles of the fused step; a mesh whose tiles do not fit (16-bit local indices, shared
-        // memory) keeps the four-kernel step
+        // tiles of the fused step.  The fused step is the default for Godunov, whose k_flux does
+        // the work of k_edges and k_cfl in less time; MUSCL-EVR keeps the four-kernel step, which
+        // is the faster form there (its k_edges and k_slopes beat the tile kernel on B200: the
+        // step is bound by FP64 instruction latency, and staging adds instructions).  A mesh
+        // whose tiles do not fit (16-bit local indices, shared memory) keeps the four-kernel step.
         std::string why;
         int tc = kDefaultTileCells;
         if (const char* env = std::getenv("SW2D_TILE_CELLS")) tc = std::atoi(env);
@@ -1166,7 +1172,8 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
         h->h_cint = cint;
         h->h_lr = lr;
         h->h_bcell = bcell;
-        if (tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, tc, why) == SW2D_OK) h->fused = 1;
+        if (tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, tc, why) == SW2D_OK)
+            h->fused = h->p.scheme == SW2D_SCHEME_GODUNOV ? 1 : 0;
         h->err.clear();
     }
     if (ddp) {
@@ -1216,7 +1223,7 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
         if (steps_done) *steps_done = h->ctrl_host->steps - before;
         return status_to_code(h, h->ctrl_host->status);
     }
-    const int chunk = 32;
+    const int chunk = kGraphSteps;
     const int64_t full = n_steps / chunk, rem = n_steps % chunk;
     if (full > 0) {
         int st = ensure_graph(h, chunk);
@@ -1233,6 +1240,16 @@ int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done)
     CK(cudaStreamSynchronize(h->stream));
     if (steps_done) *steps_done = h->ctrl_host->steps - before;
     return status_to_code(h, h->ctrl_host->status);
+}
+
+int sw2d_prepare_steps(sw2d_handle* h)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    CK(cudaSetDevice(h->device));
+    const int rc = ensure_graph(h, h->result ? result_chunk(h) : kGraphSteps);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
 }
 
 int sw2d_execute(sw2d_handle* h, int64_t* steps_done)

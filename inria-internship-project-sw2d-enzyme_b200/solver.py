@@ -124,6 +124,11 @@ class SpModel:
         self._check(self.lib.sw2d_step_n(self.handle, int(n), ctypes.byref(done)))
         return int(done.value)
 
+    def prepare(self) -> None:
+        """Captures the step graph that ``step`` launches (no step taken), so that a timed run
+        does not include the capture."""
+        self._check(self.lib.sw2d_prepare_steps(self.handle))
+
     def execute(self) -> int:
         done = ctypes.c_int64(0)
         self._check(self.lib.sw2d_execute(self.handle, ctypes.byref(done)))

@@ -45,9 +45,11 @@ def pkg():
 
 def _pair(pkg, case, tile, slopes_in=1):
     fused = pkg.SpModel(case)
-    assert fused.get_option("fused_step") == 1
-    fused.set_option("fused_slopes", slopes_in)
     muscl = case.opts["num_scheme"] == "muscl_evr"
+    # the default form: fused for Godunov, the four-kernel step for MUSCL-EVR
+    assert fused.get_option("fused_step") == (0 if muscl else 1)
+    fused.set_option("fused_step", 1)
+    fused.set_option("fused_slopes", slopes_in)
     assert fused.kernels_per_step == (3 if muscl and not slopes_in else 2)
     if tile is not None:
         fused.set_option("tile_cells", tile)
@@ -99,6 +101,10 @@ def test_fused_matches_oracle_on_delaunay_mesh(pkg):
 def test_fused_phase_labels_and_switch(pkg):
     case = pkg.workloads.dam_break(n_cells=2000)
     m = pkg.SpModel(case)
+    assert list(m.phase_times(3)) == ["k_slopes", "k_edges", "k_cfl", "k_update"]   # MUSCL-EVR default
+    m.set_option("fused_step", 1)
+    assert list(m.phase_times(3)) == ["k_slopes", "k_flux", "k_update"]            # slopes first by default
+    m.set_option("fused_slopes", 1)
     ph = m.phase_times(3)
     assert list(ph) == ["k_flux", "k_update"]
     m.set_option("fused_slopes", 0)
@@ -112,10 +118,10 @@ def test_fused_phase_labels_and_switch(pkg):
     with pytest.raises(pkg.Sw2dError):
         m.set_option("tile_cells", 5)
     assert m.kernels_per_step == 2 and m.step(3) == 3   # the previous tiles are kept
-    assert m.get_option("tile_cells") == 512
+    assert m.get_option("tile_cells") == 384
     with pytest.raises(pkg.Sw2dError, match="shared-memory"):
         m.set_option("tile_cells", 4096)                  # a stage beyond 200 KB is refused
-    assert m.get_option("tile_cells") == 512 and m.step(2) == 2
+    assert m.get_option("tile_cells") == 384 and m.step(2) == 2
 
 
 def test_fused_autotune_keeps_results(pkg):
