@@ -425,8 +425,8 @@ const char* sw2d_phase_name(int i);
  * balance terms, CFL bound and the grid's dt) and k_update, with k_slopes first for MUSCL-EVR
  * unless "fused_slopes" is 1 (then k_flux also stages the second ring of neighbours and computes
  * the slopes itself); 0 runs the four-kernel step (k_slopes, k_edges, k_cfl, k_update).  Every
- * form gives the same bits.  Defaults: 1 for Godunov, 0 for MUSCL-EVR (the faster forms on
- * B200; sw2d_autotune_step measures them).  "fused_slopes" (0/1, default 0): see above; the
+ * form gives the same bits.  Default 0, the faster form on B200 for both schemes
+ * (sw2d_autotune_step measures them on the caller's mesh and state).  "fused_slopes" (0/1, default 0): see above; the
  * tiles are rebuilt.  "tile_cells" (32..8192): cells per tile of the fused step (384 by
  * default, or the environment variable SW2D_TILE_CELLS read when the handle is created); the
  * tiles are rebuilt.  "flux_variant": the launch variant of k_flux (sw2d_autotune picks it).
@@ -469,6 +469,10 @@ int sw2d_set_launch_config(sw2d_handle* h, int slopes_variant, int edges_variant
  * (no counterpart in the reference, which calls the host libm's exp/log), 2: CUDA's exp,
  * 3: CUDA's log, on n host values; for the tests of the elementary functions. */
 int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n);
+/* Evaluates q[i] = a[i] / b[i] on device `device` for n host values: fn = 0 by the IEEE
+ * division, 1 by the division from a shared reciprocal that the slope kernels use (the same
+ * bits); for the tests.  No counterpart in the reference. */
+int sw2d_eval_div(int device, int fn, const double* a, const double* b, double* q, int64_t n);
 
 /* sw2d_get_array without any allocation.  No counterpart in the reference (which keeps these
  * arrays in host memory).  For callers that must not allocate device memory once their run has

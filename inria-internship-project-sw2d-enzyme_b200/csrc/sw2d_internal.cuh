@@ -235,6 +235,7 @@ struct sw2d_handle {
     sw2d::TileMesh tiles{};             // tiles of the fused step (SP and DIP models)
     std::vector<void*> tile_allocs;     // device arrays of the tiles
     std::vector<int2> h_coff, h_cint, h_lr;  // host tables the tiles are built from
+    int tile_default = 384;                  // tile size of the first build (SW2D_TILE_CELLS)
     std::vector<int> h_bcell;
     int fused = 0;                      // step as the two kernels k_flux + k_update (option "fused_step")
     int fused_slopes = 0;               // MUSCL-EVR: slopes inside k_flux (1) or by k_slopes first (0)

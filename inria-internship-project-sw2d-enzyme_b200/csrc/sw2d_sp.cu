@@ -90,8 +90,9 @@ __device__ __forceinline__ void grad_term(double zc, double zj, double2 xy, doub
     double dy = xj.y - xy.y;
     double dist = sqrt(dx * dx + dy * dy);
     double w = 1.0 / dist;
-    sx += (zj - zc) * dx / dist / dist * w;
-    sy += (zj - zc) * dy / dist / dist * w;
+    // (zj - zc) dx / dist / dist * w with both quotients from the reciprocal w (the same bits)
+    sx += div_rcp(div_rcp((zj - zc) * dx, dist, w), dist, w) * w;
+    sy += div_rcp(div_rcp((zj - zc) * dy, dist, w), dist, w) * w;
     wsum += w;
 }
 
@@ -489,6 +490,13 @@ __global__ void k_eval_math(int fn, const double* __restrict__ x, double* y, lon
          : fn == 4 ? sw2d_cbrt(v) : cbrt(v);
 }
 
+__global__ void k_eval_div(int fn, const double* __restrict__ a, const double* __restrict__ b, double* q, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = a[i], d = b[i];
+    q[i] = fn == 0 ? x / d : div_rcp(x, d, 1.0 / d);
+}
 
 // Hilbert index of (x, y) on a 2^16 x 2^16 grid (the classic rotate-and-flip walk).
 uint64_t hilbert_d(uint32_t x, uint32_t y)
@@ -1160,20 +1168,19 @@ int create_model(const sw2d_mesh* mesh, const sw2d_params* params, const sw2d_ce
         return bail(fail(h, SW2D_E_CUDA, "initialisation kernels failed"));
     if ((rc = noalloc_prepare(h))) return bail(rc);
     if (!ddp) {
-        // tiles of the fused step.  The fused step is the default for Godunov, whose k_flux does
-        // the work of k_edges and k_cfl in less time; MUSCL-EVR keeps the four-kernel step, which
-        // is the faster form there (its k_edges and k_slopes beat the tile kernel on B200: the
-        // step is bound by FP64 instruction latency, and staging adds instructions).  A mesh
-        // whose tiles do not fit (16-bit local indices, shared memory) keeps the four-kernel step.
-        std::string why;
-        int tc = kDefaultTileCells;
-        if (const char* env = std::getenv("SW2D_TILE_CELLS")) tc = std::atoi(env);
+        // tables for the tiles of the fused step, which is an option ("fused_step"; the tiles
+        // are built when it is first switched on).  The four-kernel step is the default, being
+        // the faster form on B200 for both schemes: the step is bound by the latency of its FP64
+        // instructions, not by HBM, and k_edges and k_slopes reach their operands through L1 at
+        // a higher occupancy than the tile kernel, whose staging and barriers add instructions
+        // and whose cross-tile edges are computed twice.
+        h->tile_default = kDefaultTileCells;
+        if (const char* env = std::getenv("SW2D_TILE_CELLS")) h->tile_default = std::atoi(env);
         h->h_coff = coff;
         h->h_cint = cint;
         h->h_lr = lr;
         h->h_bcell = bcell;
-        if (tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, tc, why) == SW2D_OK)
-            h->fused = h->p.scheme == SW2D_SCHEME_GODUNOV ? 1 : 0;
+        h->fused = 0;
         h->err.clear();
     }
     if (ddp) {
@@ -1459,7 +1466,7 @@ int sw2d_autotune_step(sw2d_handle* h, int iters, const int* tile_sizes, int n_t
 {
     if (!h || iters <= 0 || n_tile_sizes < 0 || (n_tile_sizes && !tile_sizes))
         return fail(h, SW2D_E_ARG, "invalid arguments");
-    if (h->model == kModelDdp || !h->tiles.ntiles) return sw2d_autotune(h, iters, report, capacity);
+    if (h->model == kModelDdp) return sw2d_autotune(h, iters, report, capacity);
     CK(cudaSetDevice(h->device));
     static const int kDefaultTiles[] = {192, 256, 320, 384, 512};
     if (!n_tile_sizes) {
@@ -1549,9 +1556,10 @@ int sw2d_autotune_step(sw2d_handle* h, int iters, const int* tile_sizes, int n_t
     cudaEventDestroy(e1);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
-    // the chosen form (tiles rebuilt for it; the previous tiles when the four-kernel step wins)
+    // the chosen form (tiles rebuilt for it; the previous tiles, if any, when the four-kernel
+    // step wins)
     h->fused_slopes = best.fused ? best.fused_slopes : prev_fs;
-    {
+    if (best.fused || prev_tile > 0) {
         std::string why;
         const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, best.fused ? best.tile : prev_tile, why);
         if (rc) {
@@ -1652,9 +1660,16 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         if (value < 0 || value > 8) return fail(h, SW2D_E_ARG, "closure_ctas_per_sm outside 0..8");
         closure_set_ctas(h, (int)value);
     } else if (std::strcmp(name, "fused_step") == 0) {
-        // 1: the step as k_flux + k_update (the default for the SP and DIP models); 0: the
-        // four-kernel step k_slopes, k_edges, k_cfl, k_update (the same results)
-        if (value && !h->tiles.ntiles) return fail(h, SW2D_E_UNSUPPORTED, "this handle has no tiles (DDP model)");
+        // 1: the step as [k_slopes +] k_flux + k_update; 0 (the default): the four-kernel step
+        // k_slopes, k_edges, k_cfl, k_update (the same results).  The tiles are built the first
+        // time the fused step is switched on.
+        if (value && !h->tiles.ntiles) {
+            if (h->model == kModelDdp) return fail(h, SW2D_E_UNSUPPORTED, "the DDP model has no fused step");
+            CK(cudaStreamSynchronize(h->stream));
+            std::string why;
+            const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, h->tile_default, why);
+            if (rc) return fail(h, rc, "fused_step: " + (why.empty() ? h->err : why));
+        }
         h->fused = value ? 1 : 0;
     } else if (std::strcmp(name, "tile_cells") == 0) {
         // cells per tile of the fused step (32..8192): the tiles are rebuilt
@@ -2013,6 +2028,30 @@ int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n)
     if (e == cudaSuccess) e = cudaMemcpy(y, dy, n * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(dx);
     cudaFree(dy);
+    if (e != cudaSuccess) return fail(h, SW2D_E_CUDA, cudaGetErrorString(e));
+    return SW2D_OK;
+}
+
+int sw2d_eval_div(int device, int fn, const double* a, const double* b, double* q, int64_t n)
+{
+    sw2d_handle* h = nullptr;
+    if (!a || !b || !q || n < 0 || fn < 0 || fn > 1) return fail(h, SW2D_E_ARG, "invalid arguments");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(h, SW2D_E_NO_DEVICE, "no usable CUDA device");
+    CK(cudaSetDevice(device));
+    double* d = nullptr;
+    const size_t bytes = std::max<int64_t>(1, n) * sizeof(double);
+    CK(cudaMalloc(&d, 3 * bytes));
+    double *da = d, *db = d + std::max<int64_t>(1, n), *dq = d + 2 * std::max<int64_t>(1, n);
+    cudaError_t e = cudaMemcpy(da, a, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(db, b, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n > 0) {
+        k_eval_div<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock>>>(fn, da, db, dq, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(q, dq, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
     if (e != cudaSuccess) return fail(h, SW2D_E_CUDA, cudaGetErrorString(e));
     return SW2D_OK;
 }

@@ -46,8 +46,7 @@ def pkg():
 def _pair(pkg, case, tile, slopes_in=1):
     fused = pkg.SpModel(case)
     muscl = case.opts["num_scheme"] == "muscl_evr"
-    # the default form: fused for Godunov, the four-kernel step for MUSCL-EVR
-    assert fused.get_option("fused_step") == (0 if muscl else 1)
+    assert fused.get_option("fused_step") == 0   # the four-kernel step is the default form
     fused.set_option("fused_step", 1)
     fused.set_option("fused_slopes", slopes_in)
     assert fused.kernels_per_step == (3 if muscl and not slopes_in else 2)
@@ -126,15 +125,16 @@ def test_fused_phase_labels_and_switch(pkg):
 
 def test_fused_autotune_keeps_results(pkg):
     """sw2d_autotune times every k_flux launch variant on the live state; the run is unchanged."""
-    case = pkg.workloads.gaussian_bumps(n_cells=20000, mesh="delaunay", initial="dam")
+    # a channel whose dt changes from step to step (the MUSCL-EVR step reads the previous dt)
+    case = pkg.workloads.channel_features(n_cells=20000, scheme="muscl_evr")
     a = pkg.SpModel(case)
     b = pkg.SpModel(case)
-    a.step(5)
-    b.step(4)
-    dt4 = b.dt
+    a.set_option("fused_step", 1)
+    a.step(25)
+    b.step(24)
+    dt_before = b.dt
     b.step(1)
-    # the MUSCL-EVR step reads the previous dt: the case must have one that changes
-    assert b.dt != dt4
+    assert b.dt != dt_before
     rep = pkg.tuning.autotune(a, iters=2, cache_path=None)
     assert "k_flux/" in rep["report"]
     assert a.step(50) == b.step(50)
@@ -148,11 +148,14 @@ def test_autotune_step_keeps_results(pkg, scheme, tmp_path):
     """sw2d_autotune_step times the four-kernel step and the fused step at several tile sizes
     (and both places of the MUSCL-EVR slopes) on the live state, then sets the fastest form; the
     run continues with the same bits, and the cached choice is applied to a new model."""
-    case = pkg.workloads.gaussian_bumps(n_cells=20000, mesh="delaunay", initial="dam", scheme=scheme)
+    case = pkg.workloads.channel_features(n_cells=20000, scheme=scheme)   # dt changes every step
     a = pkg.SpModel(case)
     b = pkg.SpModel(case)
-    a.step(5)
-    b.step(5)
+    a.step(25)
+    b.step(24)
+    dt_before = b.dt
+    b.step(1)
+    assert b.dt != dt_before
     cache = str(tmp_path / "tune.json")
     rep = pkg.tuning.autotune_step(a, iters=2, tile_sizes=(97, 256), cache_path=cache)
     assert "four-kernel=" in rep["report"] and "tile97" in rep["report"] and "chosen" in rep["report"]
@@ -168,7 +171,7 @@ def test_autotune_step_keeps_results(pkg, scheme, tmp_path):
     c = pkg.SpModel(case)
     again = pkg.tuning.autotune_step(c, iters=2, tile_sizes=(97, 256), cache_path=cache)
     assert again["cached"] and c.get_option("fused_step") == rep["fused"]
-    c.step(5)
+    c.step(25)
     assert c.step(50) == 50
     for x, y in zip(c.state(), b.state()):
         assert _same(x, y)
