@@ -469,10 +469,6 @@ int sw2d_set_launch_config(sw2d_handle* h, int slopes_variant, int edges_variant
  * (no counterpart in the reference, which calls the host libm's exp/log), 2: CUDA's exp,
  * 3: CUDA's log, on n host values; for the tests of the elementary functions. */
 int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n);
-/* Evaluates q[i] = a[i] / b[i] on device `device` for n host values: fn = 0 by the IEEE
- * division, 1 by the division from a shared reciprocal that the slope kernels use (the same
- * bits); for the tests.  No counterpart in the reference. */
-int sw2d_eval_div(int device, int fn, const double* a, const double* b, double* q, int64_t n);
 
 /* sw2d_get_array without any allocation.  No counterpart in the reference (which keeps these
  * arrays in host memory).  For callers that must not allocate device memory once their run has

@@ -366,8 +366,6 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_set_option.restype = ctypes.c_int
     lib.sw2d_eval_math.argtypes = [ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, ctypes.c_int64]
     lib.sw2d_eval_math.restype = ctypes.c_int
-    lib.sw2d_eval_div.argtypes = [ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, c_double_p, ctypes.c_int64]
-    lib.sw2d_eval_div.restype = ctypes.c_int
     lib.sw2d_autotune.argtypes = [P, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     lib.sw2d_autotune.restype = ctypes.c_int
     lib.sw2d_autotune_step.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_char_p,
@@ -455,7 +453,7 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name", "sw2d_phase_label", "sw2d_get_option",
-            "sw2d_set_option", "sw2d_eval_math", "sw2d_eval_div", "sw2d_autotune", "sw2d_autotune_step", "sw2d_get_launch_config",
+            "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_autotune_step", "sw2d_get_launch_config",
             "sw2d_set_launch_config", "sw2d_get_array_noalloc", "sw2d_record", "sw2d_rerecord", "sw2d_trajectory_info",
             "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
             "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint", "sw2d_adjoint_nonfinite",

@@ -711,8 +711,8 @@ SW2D_HD void slopes_fwd_t(double zc, int n, const SlopeNbr* nb, double& sx, doub
             if (k < n) {
                 const double dist = sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
                 const double w = 1.0 / dist;
-                sx += div_rcp(div_rcp((nb[k].zj - zc) * nb[k].dx, dist, w), dist, w) * w;
-                sy += div_rcp(div_rcp((nb[k].zj - zc) * nb[k].dy, dist, w), dist, w) * w;
+                sx += (nb[k].zj - zc) * nb[k].dx / dist / dist * w;
+                sy += (nb[k].zj - zc) * nb[k].dy / dist / dist * w;
                 wsum += w;
             }
         }
@@ -792,8 +792,7 @@ SW2D_HD void slopes_rev_t(double zc, int n, const SlopeNbr* nb, double sxb, doub
             if (k < n) {
                 const double dist = sqrt(nb[k].dx * nb[k].dx + nb[k].dy * nb[k].dy);
                 const double w = 1.0 / dist;
-                const double t_bar = Sx_bar * (div_rcp(div_rcp(nb[k].dx, dist, w), dist, w) * w) +
-                                     Sy_bar * (div_rcp(div_rcp(nb[k].dy, dist, w), dist, w) * w);
+                const double t_bar = Sx_bar * (nb[k].dx / dist / dist * w) + Sy_bar * (nb[k].dy / dist / dist * w);
                 zj_bar[k] += t_bar;
                 zc_bar -= t_bar;
             }

@@ -27,7 +27,6 @@ namespace sw2d {
 
 using std::fabs;
 using std::sqrt;
-using std::fma;
 
 constexpr double kSmallReal = 1e-16;  // src/common/param.h:2
 constexpr double kGravity = 9.81;     // src/common/param.h:3
@@ -90,25 +89,6 @@ SW2D_HD bool warp_all(bool p)
 }
 
 SW2D_HD double sqrt_z(double x) { return warp_all(x == 0.0) ? x : sqrt(x); }
-
-// a / b, correctly rounded (the same bits as IEEE division), for a divisor b whose correctly
-// rounded reciprocal y = RN(1 / b) is at hand (computed once by an IEEE division and shared by
-// several quotients).  Published method: q0 = RN(a y) is within a few ulps of a / b; one
-// correction q1 = RN(q0 + RN(a - b q0) y) makes it faithful, and a second one is then the
-// correctly rounded quotient by Markstein's theorem (P. Markstein, "Computation of elementary
-// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; J.-M. Muller
-// et al., Handbook of Floating-Point Arithmetic, 2nd ed., section 4.9), each residual taken
-// exactly by a fused multiply-add.  The theorem needs no underflow or overflow: zero numerators
-// (a y has the sign of a / b), quotients outside [2^-900, 2^900] and non-finite values take the
-// IEEE division instead.  Precondition: 2^-60 < b < 2^60 (mesh distances).
-SW2D_HD double div_rcp(double a, double b, double y)
-{
-    const double q0 = a * y;
-    const double aq = fabs(q0);
-    if (!(aq > 0x1p-900 && aq < 0x1p+900)) return (a == 0.0) ? q0 : a / b;
-    const double q1 = fma(fma(-q0, b, a), y, q0);
-    return fma(fma(-q1, b, a), y, q1);
-}
 
 SW2D_HD double div_z(double x, double d) { return warp_all(x == 0.0) ? x : x / d; }  // d > 0
 

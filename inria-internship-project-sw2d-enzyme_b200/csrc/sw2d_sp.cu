@@ -90,9 +90,8 @@ __device__ __forceinline__ void grad_term(double zc, double zj, double2 xy, doub
     double dy = xj.y - xy.y;
     double dist = sqrt(dx * dx + dy * dy);
     double w = 1.0 / dist;
-    // (zj - zc) dx / dist / dist * w with both quotients from the reciprocal w (the same bits)
-    sx += div_rcp(div_rcp((zj - zc) * dx, dist, w), dist, w) * w;
-    sy += div_rcp(div_rcp((zj - zc) * dy, dist, w), dist, w) * w;
+    sx += (zj - zc) * dx / dist / dist * w;
+    sy += (zj - zc) * dy / dist / dist * w;
     wsum += w;
 }
 
@@ -488,14 +487,6 @@ __global__ void k_eval_math(int fn, const double* __restrict__ x, double* y, lon
     const double v = x[i];
     y[i] = fn == 0 ? sw2d_exp(v) : fn == 1 ? sw2d_log(v) : fn == 2 ? exp(v) : fn == 3 ? log(v)
          : fn == 4 ? sw2d_cbrt(v) : cbrt(v);
-}
-
-__global__ void k_eval_div(int fn, const double* __restrict__ a, const double* __restrict__ b, double* q, long long n)
-{
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double x = a[i], d = b[i];
-    q[i] = fn == 0 ? x / d : div_rcp(x, d, 1.0 / d);
 }
 
 // Hilbert index of (x, y) on a 2^16 x 2^16 grid (the classic rotate-and-flip walk).
@@ -1689,7 +1680,8 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
         const int prev = h->fused_slopes;
         h->fused_slopes = value ? 1 : 0;
         std::string why;
-        const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, h->tiles.tile_cells, why);
+        const int tc = h->tiles.ntiles ? h->tiles.tile_cells : h->tile_default;
+        const int rc = tiles_build(h, h->h_coff, h->h_cint, h->h_lr, h->h_bcell, tc, why);
         if (rc) {
             h->fused_slopes = prev;
             if (!h->tiles.ntiles) h->fused = 0;
@@ -2028,30 +2020,6 @@ int sw2d_eval_math(int device, int fn, const double* x, double* y, int64_t n)
     if (e == cudaSuccess) e = cudaMemcpy(y, dy, n * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(dx);
     cudaFree(dy);
-    if (e != cudaSuccess) return fail(h, SW2D_E_CUDA, cudaGetErrorString(e));
-    return SW2D_OK;
-}
-
-int sw2d_eval_div(int device, int fn, const double* a, const double* b, double* q, int64_t n)
-{
-    sw2d_handle* h = nullptr;
-    if (!a || !b || !q || n < 0 || fn < 0 || fn > 1) return fail(h, SW2D_E_ARG, "invalid arguments");
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
-        return fail(h, SW2D_E_NO_DEVICE, "no usable CUDA device");
-    CK(cudaSetDevice(device));
-    double* d = nullptr;
-    const size_t bytes = std::max<int64_t>(1, n) * sizeof(double);
-    CK(cudaMalloc(&d, 3 * bytes));
-    double *da = d, *db = d + std::max<int64_t>(1, n), *dq = d + 2 * std::max<int64_t>(1, n);
-    cudaError_t e = cudaMemcpy(da, a, n * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(db, b, n * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && n > 0) {
-        k_eval_div<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock>>>(fn, da, db, dq, n);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaMemcpy(q, dq, n * sizeof(double), cudaMemcpyDeviceToHost);
-    cudaFree(d);
     if (e != cudaSuccess) return fail(h, SW2D_E_CUDA, cudaGetErrorString(e));
     return SW2D_OK;
 }

@@ -139,8 +139,8 @@ __device__ __forceinline__ double2 tile_slope(const Stage& sv, int k0, int k1, d
             const double dy = xj[i].y - yc;
             const double dist = sqrt(dx * dx + dy * dy);
             w[i] = 1.0 / dist;
-            tx[i] = div_rcp(div_rcp((zj[i] - zc) * dx, dist, w[i]), dist, w[i]) * w[i];
-            ty[i] = div_rcp(div_rcp((zj[i] - zc) * dy, dist, w[i]), dist, w[i]) * w[i];
+            tx[i] = (zj[i] - zc) * dx / dist / dist * w[i];
+            ty[i] = (zj[i] - zc) * dy / dist / dist * w[i];
         }
 #pragma unroll
         for (int i = 0; i < 3; i++) {
@@ -182,8 +182,8 @@ __device__ __forceinline__ double2 tile_slope(const Stage& sv, int k0, int k1, d
             const double dy = xj.y - yc;
             const double dist = sqrt(dx * dx + dy * dy);
             const double w = 1.0 / dist;
-            sx += div_rcp(div_rcp((zj - zc) * dx, dist, w), dist, w) * w;
-            sy += div_rcp(div_rcp((zj - zc) * dy, dist, w), dist, w) * w;
+            sx += (zj - zc) * dx / dist / dist * w;
+            sy += (zj - zc) * dy / dist / dist * w;
             wsum += w;
         }
         sx /= wsum;

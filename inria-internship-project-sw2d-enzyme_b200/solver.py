@@ -483,22 +483,6 @@ def eval_math(fn: str, x, device: int = 0) -> np.ndarray:
     return y
 
 
-def eval_div(a, b, shared_reciprocal: bool, device: int = 0) -> np.ndarray:
-    """Device quotients a / b: by the IEEE division, or (shared_reciprocal) by the division from
-    the correctly rounded reciprocal of b that the slope kernels use."""
-    lib = capi.load_library()
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    b = np.ascontiguousarray(b, dtype=np.float64)
-    if a.shape != b.shape:
-        raise ValueError("a and b differ in shape")
-    q = np.empty_like(a)
-    st = lib.sw2d_eval_div(int(device), 1 if shared_reciprocal else 0, a.ctypes.data_as(capi.c_double_p),
-                           b.ctypes.data_as(capi.c_double_p), q.ctypes.data_as(capi.c_double_p), a.size)
-    if st != 0:
-        raise Sw2dError(st, lib.sw2d_last_error(None).decode())
-    return q
-
-
 def run_case(folder: str, device: int = 0, n_steps: Optional[int] = None):
     """`sw2dSolver <folder>` without result storage: returns (model, steps taken)."""
     model = SpModel.from_folder(folder, device)
