@@ -592,7 +592,13 @@ int sw2d_adjoint_nonfinite(sw2d_handle* h, int64_t* counts);
  * so one launch advances the whole ensemble and small members run side by side.  Each member
  * keeps its own CFL time steps, t_max and status; its results are bit for bit those of the
  * member run alone.  The batch captures the members' options and launch variants when it first
- * steps; change them before that. */
+ * steps; change them before that.
+ *
+ * When every member is an SP model of one scheme and topography discretisation (without a
+ * learned closure), the batch runs by default as ONE persistent kernel over a work queue of
+ * (step, phase, member, tile) items: CTAs take items in order from an atomic ticket counter;
+ * an item waits (bounded) for the phase it depends on to be complete for its member; each member
+ * keeps its own last-tile-done dt reduction.  The same bits as the member run alone. */
 typedef struct sw2d_batch sw2d_batch;
 
 int sw2d_batch_create(sw2d_handle* const* members, int n_members, sw2d_batch** out);
@@ -606,6 +612,23 @@ int sw2d_batch_step_n(sw2d_batch* b, int64_t n_steps, int64_t* steps_done);
  * concurrently from n_threads host threads (<= 0: 16): J[i] and grads[i] (grads may be NULL). */
 int sw2d_batch_adjoint(sw2d_batch* b, double* J, const sw2d_gradient* grads, int n_threads);
 
+/* Form of the batch's step: mode 0 the graph of per-member stream branches, 1 the work queue
+ * (SW2D_E_UNSUPPORTED when the members do not qualify).  For mode 1: the launch variant
+ * (threads per CTA x CTAs per SM, see sw2d_batch_autotune's report) and the cells (edges) per
+ * tile of an item; values < 0 (variant) or <= 0 (tiles) keep the current ones.  No counterpart
+ * in the reference. */
+int sw2d_batch_configure(sw2d_batch* b, int mode, int variant, int cells_per_tile, int edges_per_tile);
+int sw2d_batch_get_config(sw2d_batch* b, int* mode, int* variant, int* cells_per_tile, int* edges_per_tile);
+/* Times the work queue for `steps` steps at every launch variant and each of the n_tile_sizes
+ * tile sizes (512, 1024, 2048, 4096 when 0), with CUDA events on the batch's stream, on the
+ * members' current states (saved before and put back after every trial, so the run continues
+ * with the same bits), then sets the fastest and writes a one-line report. */
+int sw2d_batch_autotune(sw2d_batch* b, int steps, const int* tile_sizes, int n_tile_sizes, char* report, int capacity);
+/* Poll limit of the work queue's waits (< 0: the default, about a second).  A wait that runs out
+ * ends the launch with SW2D_E_CUDA ("a wait ... ran out"); the members' states are then partial. */
+int sw2d_batch_set_wait_polls(sw2d_batch* b, int64_t polls);
+/* The batch's stream (a cudaStream_t): the work queue runs on it. */
+void* sw2d_batch_stream(sw2d_batch* b);
 int sw2d_batch_size(sw2d_batch* b);
 int sw2d_batch_destroy(sw2d_batch* b);   /* the member handles stay valid */
 const char* sw2d_batch_last_error(sw2d_batch* b);

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
-SOURCES = ["sw2d_sp.cu", "sw2d_tile.cu", "sw2d_adjoint.cu", "sw2d_batch.cu", "sw2d_assim.cu", "sw2d_ddp.cu", "sw2d_case.cpp", "sw2d_mlp.cu",
+SOURCES = ["sw2d_sp.cu", "sw2d_tile.cu", "sw2d_queue.cu", "sw2d_adjoint.cu", "sw2d_batch.cu", "sw2d_assim.cu", "sw2d_ddp.cu", "sw2d_case.cpp", "sw2d_mlp.cu",
            "sw2d_result.cu", "sw2d_mapper.cu"]
 HEADERS = ["sw2d_internal.cuh", "sp_math.cuh", "dip_math.cuh", "sp_adjoint.cuh", "portable_math.h", "adjoint_common.cuh",
            "spe_math.cuh", "ddp_math.cuh", "umma.cuh"]

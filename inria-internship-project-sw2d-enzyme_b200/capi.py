@@ -409,6 +409,17 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_batch_step_n.restype = ctypes.c_int
     lib.sw2d_batch_adjoint.argtypes = [P, c_double_p, ctypes.POINTER(Sw2dGradient), ctypes.c_int]
     lib.sw2d_batch_adjoint.restype = ctypes.c_int
+    lib.sw2d_batch_configure.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.sw2d_batch_configure.restype = ctypes.c_int
+    c_int_p = ctypes.POINTER(ctypes.c_int)
+    lib.sw2d_batch_get_config.argtypes = [P, c_int_p, c_int_p, c_int_p, c_int_p]
+    lib.sw2d_batch_get_config.restype = ctypes.c_int
+    lib.sw2d_batch_autotune.argtypes = [P, ctypes.c_int, c_int_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    lib.sw2d_batch_autotune.restype = ctypes.c_int
+    lib.sw2d_batch_set_wait_polls.argtypes = [P, ctypes.c_int64]
+    lib.sw2d_batch_set_wait_polls.restype = ctypes.c_int
+    lib.sw2d_batch_stream.argtypes = [P]
+    lib.sw2d_batch_stream.restype = ctypes.c_void_p
     lib.sw2d_batch_size.argtypes = [P]
     lib.sw2d_batch_size.restype = ctypes.c_int
     lib.sw2d_batch_destroy.argtypes = [P]
@@ -458,6 +469,8 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
             "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint", "sw2d_adjoint_nonfinite",
             "sw2d_batch_create", "sw2d_batch_step_n", "sw2d_batch_adjoint", "sw2d_batch_size",
+            "sw2d_batch_configure", "sw2d_batch_get_config", "sw2d_batch_autotune", "sw2d_batch_set_wait_polls",
+            "sw2d_batch_stream",
             "sw2d_batch_destroy", "sw2d_batch_last_error", "sw2d_assim_configure", "sw2d_assim_set_observations",
             "sw2d_assim_record", "sw2d_assim_replay_cost", "sw2d_assim_gradient", "sw2d_assim_segments",
             "sw2d_assim_steps", "sw2d_assim_checkpoint", "sw2d_assim_set_start", "sw2d_assim_trigger_states"]

@@ -290,6 +290,20 @@ void launch_update_on(sw2d_handle* h, const DevMesh& m, bool store_balance);
 // One whole time step of the handle (its four kernels, its launch variants) on its stream.
 void launch_step_on(sw2d_handle* h);
 
+// ensemble work queue (sw2d_queue.cu): one persistent kernel over (step, phase, member, tile)
+struct QueueState;
+int queue_eligible(sw2d_handle* const* members, int n, std::string& why);
+int queue_build(QueueState*& q, sw2d_handle* const* members, int n, int variant, int cells_per_tile, int edges_per_tile,
+                std::string& why);
+int queue_launch(QueueState* q, int steps, cudaStream_t stream);
+unsigned queue_read_status(QueueState* q);
+void queue_clear_status(QueueState* q);
+void queue_release(QueueState* q);
+int queue_variants();
+std::string queue_variant_label(int v);
+void queue_set_polls(QueueState* q, long long polls);
+int queue_grid(const QueueState* q);
+
 // The fused step's flux kernel (sw2d_tile.cu) on the handle's stream with launch variant v; with
 // attr_only only its shared-memory attribute is set (before a graph capture).  The tiles are
 // built by tiles_build from the internal-numbering tables.

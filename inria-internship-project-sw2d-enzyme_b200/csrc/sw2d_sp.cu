@@ -46,6 +46,7 @@
 #include <string>
 #include <vector>
 
+#include "sp_phases.cuh"
 #include "sw2d_internal.cuh"
 
 using namespace sw2d;
@@ -53,209 +54,26 @@ using namespace sw2d;
 namespace {
 
 
-// ------------------------------------------------------------------------------------------
-// k_slopes: swSp::computeMusclSlopes (swSpHypMusclEvr.cpp:11-115) per cell.  Step 1 sums the
-// neighbour contributions in increasing internal-edge order; step 2 applies, edge after edge
-// in the same order, the under/overshoot rescaling of this cell's slope (that rescaling only
-// reads this cell's slope, so the reference's global edge loop decomposes exactly per cell).
-// Cells with up to kUnroll neighbours issue all their neighbour loads up front.
-// ------------------------------------------------------------------------------------------
-constexpr int kUnroll = 4;        // balance slots handled without a loop (cell degree)
-constexpr int kUnrollSlopes = 3;  // neighbours gathered up front in k_slopes (triangles)
-
-__device__ __forceinline__ void limit_slope(double zc, double zj, bool is_r, double2 mp, double2 xy, double& sx,
-                                            double& sy)
-{
-    const double zL = is_r ? zj : zc;
-    const double zR = is_r ? zc : zj;
-    const double fmx = smax(zL, zR);
-    const double fmn = smin(zL, zR);
-    const double rec = zc + (mp.x - xy.x) * sx + (mp.y - xy.y) * sy;
-    if (rec < fmn) {
-        double fac = (fmn - zc) / (rec - zc);
-        sx *= fac;
-        sy *= fac;
-    }
-    if (rec > fmx) {
-        double fac = (fmx - zc) / (rec - zc);
-        sx *= fac;
-        sy *= fac;
-    }
-}
-
-__device__ __forceinline__ void grad_term(double zc, double zj, double2 xy, double2 xj, double& sx, double& sy,
-                                          double& wsum)
-{
-    double dx = xj.x - xy.x;
-    double dy = xj.y - xy.y;
-    double dist = sqrt(dx * dx + dy * dy);
-    double w = 1.0 / dist;
-    sx += (zj - zc) * dx / dist / dist * w;
-    sy += (zj - zc) * dy / dist / dist * w;
-    wsum += w;
-}
-
+// k_slopes: the limited slopes of one cell per thread (slopes_cell, sp_phases.cuh)
 template <int kB, int kMinB>
 __global__ void __launch_bounds__(kB, kMinB) k_slopes(DevMesh m)
 {
     if (!step_active(m.ctrl)) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
-    const double zc = ld(&m.st[c].w);
-    const double2 xy = ld(&m.cxy[c]);
-    const int k0 = ld(&m.coff[c].x), k1 = ld(&m.coff[c + 1].x);
-    const int cnt = k1 - k0;
-    double sx = 0.0, sy = 0.0, wsum = 0.0;
-    if (cnt <= kUnrollSlopes) {
-        int2 en[kUnrollSlopes];
-        double zj[kUnrollSlopes];
-        double2 xj[kUnrollSlopes];
-#pragma unroll
-        for (int i = 0; i < kUnrollSlopes; i++)
-            if (i < cnt) en[i] = ld(&m.cint[k0 + i]);
-#pragma unroll
-        for (int i = 0; i < kUnrollSlopes; i++)
-            if (i < cnt) {
-                zj[i] = ld(&m.st[en[i].y].w);
-                xj[i] = ld(&m.cxy[en[i].y]);
-            }
-        if (cnt > 1) {
-#pragma unroll
-            for (int i = 0; i < kUnrollSlopes; i++)
-                if (i < cnt) grad_term(zc, zj[i], xy, xj[i], sx, sy, wsum);
-            sx /= wsum;
-            sy /= wsum;
-        }
-#pragma unroll
-        for (int i = 0; i < kUnrollSlopes; i++)
-            if (i < cnt) limit_slope(zc, zj[i], en[i].x & 1, ld(&m.mxy[en[i].x >> 1]), xy, sx, sy);
-    } else {
-        for (int k = k0; k < k1; k++) {
-            const int j = ld(&m.cint[k]).y;
-            grad_term(zc, ld(&m.st[j].w), xy, ld(&m.cxy[j]), sx, sy, wsum);
-        }
-        sx /= wsum;
-        sy /= wsum;
-        for (int k = k0; k < k1; k++) {
-            const int2 en = ld(&m.cint[k]);
-            limit_slope(zc, ld(&m.st[en.y].w), en.x & 1, ld(&m.mxy[en.x >> 1]), xy, sx, sy);
-        }
-    }
-    m.slope[c] = make_double2(sx, sy);
+    slopes_cell<LdNc>(m, c);
 }
 
-// ------------------------------------------------------------------------------------------
-// k_edges: one thread per internal edge, then one per boundary edge.  Writes the balance
-// terms {a, b, c} of the edge into the slots of its cells (when the flux is computed) and,
-// every step, the CFL contributions lambda_max * length that hypComputeTimeStep adds
-// (swSpHyp.cpp:437-477: the L cell counts it when it is wet; the R cell when L or R is wet,
-// because the reference carries `lambda` over from the L test).
-// ------------------------------------------------------------------------------------------
+// k_edges: one thread per internal edge, then one per boundary edge (edge_internal and
+// edge_boundary, sp_phases.cuh)
 template <int kScheme, bool kBlending, int kModel, int kB, int kMinB>
 __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
 {
-    constexpr bool kDip = kModel == kModelDip;
     if (!step_active(m.ctrl)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned bad = 0;
-    if (i < m.ni) {
-        const int e = i;
-        const int2 lr = ld(&m.lr[e]);
-        const int a = lr.x, b = lr.y;
-        const double2 n = ld(&m.nxy[e]);
-        const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
-        const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
-        SideState SL, SR;
-        double phiG = 0.0, xL = 1.0, xR = 1.0;
-        if (kDip) {
-            phiG = ld(&m.phig[e]);
-            xL = dip_x(ca.z, phiG);
-            xR = dip_x(cb.z, phiG);
-        }
-        if (kScheme == SW2D_SCHEME_GODUNOV) {
-            if (kDip) {
-                SL = godunov_side_dip(sa.x, sa.y, sa.z, ca.x, ca.y, xL, n.x, n.y);
-                SR = godunov_side_dip(sb.x, sb.y, sb.z, cb.x, cb.y, xR, n.x, n.y);
-            } else {
-                SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
-                SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
-            }
-        } else {
-            const double dtp = m.ctrl->dt;
-            const double4 d = ld(&m.emc[e]);  // midpoint - centroid of L and R
-            const double2 ga = ld(&m.slope[a]), gb = ld(&m.slope[b]);
-            if (kDip) {
-                SL = evr_side_dip(true, sa.x, sa.y, sa.z, ca.x, ca.y, xL, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp);
-                SR = evr_side_dip(false, sb.x, sb.y, sb.z, cb.x, cb.y, xR, sb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp);
-            } else {
-                SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp, m.dry);
-                SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp, m.dry);
-            }
-        }
-        const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
-        if (m.lmax) m.lmax[e] = lm;
-        const double lw = lm * ld(&m.len[e]);
-        const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;
-        const int2 sl = ld(&m.eslot[e]);
-        m.slot_w[sl.x] = wetL ? lw : 0.0;
-        m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
-        const double hL = SL.z - ca.x, hR = SR.z - cb.x;
-        if ((hL > m.h_min) || (hR > m.h_min)) {
-            EdgeFlux f = kDip ? hllc_dip(kBlending, ca.y, cb.y, phiG, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min)
-                              : hllc(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min);
-            bad |= f.bad;
-            if (isnan(f.f1)) bad |= kStatusNanFlux;
-            if (m.flux) {
-                double2* fp = m.flux + 3 * (size_t)e;
-                fp[0] = make_double2(f.f1, f.f2);
-                fp[1] = make_double2(f.f3, f.sl);
-                fp[2] = make_double2(f.sr, 0.0);
-            }
-            // factors of swSp::computeEdgeFactors (swSp.cpp:398-427) and the dt-free products of
-            // hypComputeBalance (swSpHyp.cpp:237-262)
-            const double2 cf = ld(&m.coef[e]);
-            const double nx = n.x, ny = n.y;
-            {
-                const double c = cf.x;
-                const double f1 = -c, f2F2 = -c * nx, f2F3 = +c * ny, f2S2 = +c * nx;
-                const double f3F2 = -c * ny, f3F3 = -c * nx, f3S2 = +c * ny;
-                m.slot[sl.x] = make_slot(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sl + f2F3 * f.f3,
-                                         f3F2 * f.f2 + f3S2 * f.sl + f3F3 * f.f3);
-            }
-            {
-                const double c = cf.y;
-                const double f1 = +c, f2F2 = +c * nx, f2F3 = -c * ny, f2S2 = +c * nx;
-                const double f3F2 = +c * ny, f3F3 = +c * nx, f3S2 = +c * ny;
-                m.slot[sl.y] = make_slot(f1 * f.f1, f2F2 * f.f2 + f2S2 * f.sr + f2F3 * f.f3,
-                                         f3F2 * f.f2 + f3S2 * f.sr + f3F3 * f.f3);
-            }
-        }
-    } else if (i < m.ni + m.nb) {
-        const int e = i - m.ni;
-        const int c = ld(&m.bcell[e]);
-        const double4 s = ld(&m.st[c]);
-        const double4 cs = ld(&m.cst[c]);
-        const double4 g = ld(&m.bgeo[e]);
-        const double phiGb = kDip ? ld(&m.phigb[e]) : 0.0;
-        SideState S = kDip ? godunov_side_dip(s.x, s.y, s.z, cs.x, cs.y, dip_x(cs.z, phiGb), g.x, g.y)
-                           : godunov_side(s.x, s.y, s.z, cs.x, cs.y, g.x, g.y);
-        const double lm = (kScheme == SW2D_SCHEME_GODUNOV) ? smax(fabs(S.lp), fabs(S.lm)) : smax(fabs(S.lm), fabs(S.lp));
-        if (m.lmaxb) m.lmaxb[e] = lm;
-        const int sb = ld(&m.bslot[e]);
-        m.slot_w[sb] = (s.x > m.h_min) ? lm * g.z : 0.0;
-        const int k = ld(&m.bbc[e]);
-        const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
-        const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, m.ctrl->t);
-        double f1, f2, f3;
-        bad |= kDip ? boundary_flux_dip(cs.y, phiGb, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3)
-                    : boundary_flux(cs.y, cs.z, cs.x, S, ld(&m.bctype[k]), v, m.h_min, &f1, &f2, &f3);
-        if (m.bflux) m.bflux[e] = make_double4(f1, f2, f3, 0.0);
-        const double cf = g.w, nx = g.x, ny = g.y;
-        const double fa = +cf, f2F2 = +cf * nx, f2F3 = -cf * ny, f2S2 = +cf * nx;
-        const double f3F2 = +cf * ny, f3F3 = +cf * nx, f3S2 = +cf * ny;
-        const double s2 = 0.0;  // boundary geometric source: never set by hypBoundaryFlux
-        m.slot[sb] = make_slot(fa * f1, f2F2 * f2 + f2S2 * s2 + f2F3 * f3, f3F2 * f2 + f3S2 * s2 + f3F3 * f3);
-    }
+    if (i < m.ni) bad = edge_internal<kScheme, kBlending, kModel, LdNc>(m, i);
+    else if (i < m.ni + m.nb) bad = edge_boundary<kScheme, kModel, LdNc>(m, i - m.ni);
     if (bad) atomicOr(&m.ctrl->status, bad);
 }
 
@@ -266,7 +84,6 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges(DevMesh m)
 // and the t_max clip, all on the device.  A skipped contribution is stored as 0, and adding
 // +0 to the (non-negative) sum changes no bit, so the sum is the reference's.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ double min_keep(double a, double b) { return (b < a) ? b : a; }
 
 // k_cfl's grid: 8 blocks of kBlock threads per SM (a full SM), at most one block per kBlock cells
 unsigned cfl_grid(sw2d_handle* h, int nc)
@@ -295,19 +112,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
     const int stride = gridDim.x * blockDim.x;
 #pragma unroll 4
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m.nc; c += stride) {
-        const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
-        double sw = 0.0;
-        if (k1 - k0 <= kUnroll) {
-            double w[kUnroll];
-#pragma unroll
-            for (int i = 0; i < kUnroll; i++) w[i] = (i < k1 - k0) ? ld(&m.slot_w[k0 + i]) : 0.0;
-#pragma unroll
-            for (int i = 0; i < kUnroll; i++)
-                if (i < k1 - k0) sw += w[i];
-        } else {
-            for (int k = k0; k < k1; k++) sw += ld(&m.slot_w[k]);
-        }
-        double x = m.cfl_max * (ld(&m.area[c]) / smax(sw, kSmallReal));
+        const double x = cfl_cell<LdNc>(m, c);
         if (x < best) best = x;
     }
     // warp then block minimum (NaN candidates never win: comparisons with NaN are false)
@@ -340,26 +145,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(DevMesh m)
         double dt = m.dt_max;
         for (int w = 0; w < kBlock / 32; w++)
             if (wmin[w] < dt) dt = wmin[w];
-        const double t = ctrl->t;
-        int store = m.dt_map <= -kSmallReal ? 1 : 0;
-        if (m.dt_map > kSmallReal) {
-            int now, later;
-            if (kDdpSnap) {
-                now = (int)((double)(int)t / m.dt_map);
-                later = (int)((double)(int)(t + dt) / m.dt_map);
-            } else {
-                now = (int)(t / m.dt_map);
-                later = (int)((t + dt) / m.dt_map);
-            }
-            if (later > now) {
-                dt = later * m.dt_map - t;
-                store = 1;
-            }
-        }
-        if ((t + dt) > ctrl->t_max) dt = ctrl->t_max - t;
-        ctrl->store_map = store;
-        ctrl->dt = dt;
-        ctrl->go = 1;
+        dt_finalize<kDdpSnap>(m, ctrl, dt);
         ctrl->blocks_done = 0;
     }
 }
@@ -382,51 +168,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(DevMesh m)
         ctrl->steps += 1;
     }
     if (c >= m.nc) return;
-    const double4 s0 = m.st[c];
-    double hh = s0.x, qq = s0.y, rr = s0.z;
-    // hypComputeBalance (swSpHyp.cpp:214-273): h += (factor*F1)*dt, q += (...)*dt, r += (...)*dt
-    // over the cell's slots, in the reference's order
-    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
-    if (k1 - k0 <= kUnroll) {
-        Slot v[kUnroll];
-#pragma unroll
-        for (int i = 0; i < kUnroll; i++)
-            if (i < k1 - k0) v[i] = m.slot[k0 + i];
-#pragma unroll
-        for (int i = 0; i < kUnroll; i++)
-            if (i < k1 - k0) {
-                hh += v[i].a * dt;
-                qq += v[i].b * dt;
-                rr += v[i].c * dt;
-            }
-    } else {
-        for (int k = k0; k < k1; k++) {
-            const Slot v = m.slot[k];
-            hh += v.a * dt;
-            qq += v.b * dt;
-            rr += v.c * dt;
-        }
-    }
-    if (kDissip) {  // DIP momentum dissipation, before the round-off flush (dip/swDipHyp.cpp:295-324)
-        const double4 mu = ld(&m.mu[c]);
-        momentum_dissipation(mu.x, mu.y, mu.z, mu.w, s0.x, s0.y, s0.z, hh, qq, rr);
-    }
-    if (kStoreB) m.bal[c] = make_double4(hh, qq, rr, 0.0);  // for the reverse sweep
-    if (fabs(hh) < kSmallReal) hh = 0.;
-    if (fabs(qq) < kSmallReal) qq = 0.;
-    if (fabs(rr) < kSmallReal) rr = 0.;
-    // negative depth (swSpHyp.cpp:182-210)
-    if (m.neg_detect) {
-        if (hh < 0) atomicOr(&ctrl->status, kStatusNegDepth);
-    } else if (hh < 0.) {
-        hh = 0.;
-        qq = 0.;
-        rr = 0.;
-    }
-    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr);
-    // z = h + z_b of the new state, as the next step's reconstruction computes it
-    // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
-    m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));
+    update_cell<kFriction, kHeadLoss, kStoreB, kDissip, LdNc>(m, c, dt);
 }
 
 // swSp::computeEdgeFactors coefficient w / area / phi (swSp.cpp:364-368, 397-405)
