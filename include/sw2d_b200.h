@@ -439,7 +439,9 @@ const char* sw2d_phase_name(int i);
  * |x| < 1e-16 -> 0 after the balance (swSpHyp.cpp:197-199, assim/swSpE_hyp.cpp:390-392).  0 (the
  * default): as the identity, which is what finite differences see (a state at rest sits exactly
  * on the flush).  1: as the branch taken (zero derivative for flushed values), which is what
- * differentiating the reference's code line by line gives. */
+ * differentiating the reference's code line by line gives.
+ * "adjoint_keep_nonfinite" (0/1): 1 hands back sw2d_adjoint's non-finite gradient entries as
+ * they are (still counted by sw2d_adjoint_nonfinite) instead of zeroing them, to locate them. */
 int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value);
 /* Current value of "fused_step", "flux_variant", "tile_cells" (0 without tiles),
  * "record_fluxes" or "record_wave_speeds".  No counterpart in the reference. */

@@ -201,10 +201,11 @@ __global__ void __launch_bounds__(kBlock) k_nbr_rev(DevMesh m, const int* __rest
 // friction_2): the reference's final clean-up of its gradient (assim/swSpE_checkpoint.cpp:
 // 1196-1207).  Near-dry cells carry the 1/max(h, 1e-16) factors of the wave speeds and
 // velocities; over long windows their adjoint can overflow, in the reference as here.
-__device__ __forceinline__ void clean(double& v, unsigned long long* count)
+// keep = true counts them without zeroing (the option "adjoint_keep_nonfinite", to locate them).
+__device__ __forceinline__ void clean(double& v, unsigned long long* count, bool keep = false)
 {
     if (!isfinite(v)) {
-        v = 0.0;
+        if (!keep) v = 0.0;
         atomicAdd(count, 1ull);
     }
 }

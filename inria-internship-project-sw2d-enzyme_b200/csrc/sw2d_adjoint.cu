@@ -367,19 +367,19 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
 }
 
 __global__ void k_sanitize(double4* lam, double* gzb, double* gk1, double* gk2, unsigned long long* counts, int n,
-                           int with_friction)
+                           int with_friction, int keep)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     double4 l = lam[c];
-    clean(l.x, counts + 0);
-    clean(l.y, counts + 1);
-    clean(l.z, counts + 2);
+    clean(l.x, counts + 0, keep);
+    clean(l.y, counts + 1, keep);
+    clean(l.z, counts + 2, keep);
     lam[c] = l;
-    clean(gzb[c], counts + 3);
+    clean(gzb[c], counts + 3, keep);
     if (with_friction) {
-        clean(gk1[c], counts + 4);
-        clean(gk2[c], counts + 5);
+        clean(gk1[c], counts + 4, keep);
+        clean(gk2[c], counts + 5, keep);
     }
 }
 
@@ -693,7 +693,7 @@ int reverse_sweep(sw2d_handle* h)
     }
     CK(cudaMemsetAsync(a->d_nonfinite, 0, 6 * sizeof(unsigned long long), h->stream));
     k_sanitize<<<gc, kBlock, 0, h->stream>>>(a->lam, a->g_zb, a->g_k1, a->g_k2, a->d_nonfinite, (int)nc,
-                                              h->p.friction != SW2D_FRICTION_NONE);
+                                              h->p.friction != SW2D_FRICTION_NONE, h->adj_keep_nonfinite);
     unsigned long long cnt[6];
     CK(cudaMemcpyAsync(cnt, a->d_nonfinite, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
     if ((rc = ck_load(h, a->n_ck))) return rc;

@@ -225,6 +225,7 @@ struct sw2d_handle {
     int slope_variant = 2;
     sw2d::AdjointState* adj = nullptr;  // recorded trajectory, checkpoints and adjoint buffers
     int adj_flush_branch = 0;           // option "adjoint_flush_branch"
+    int adj_keep_nonfinite = 0;         // option "adjoint_keep_nonfinite"
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step
     int assim_sqrt_zero = 0;            // option "assim_sqrt_zero"

@@ -1371,6 +1371,11 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
     } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
         h->adj_flush_branch = value ? 1 : 0;
         return SW2D_OK;
+    } else if (std::strcmp(name, "adjoint_keep_nonfinite") == 0) {
+        // 1: sw2d_adjoint counts its non-finite gradient entries but hands them back as they are
+        // (to locate them) instead of zeroing them as the reference does
+        h->adj_keep_nonfinite = value ? 1 : 0;
+        return SW2D_OK;
     } else if (std::strcmp(name, "assim_sqrt_zero") == 0) {
         // reverse of sqrt at 0 in the assimilation sweep: 0 (subgradient 0, default) or 1
         // (IEEE: dy / (2 sqrt(0)), non-finite unless dy == 0, as source-transformation AD gives)

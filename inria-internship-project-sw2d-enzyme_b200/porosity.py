@@ -648,8 +648,13 @@ def run_minimization(spe: SpE, phi_start, max_it: Optional[int] = None, alpha_re
             return J, g
 
         bounds = [(cfg.phi_lower_bound, cfg.phi_upper_bound)] * prob.size() if algo == "lbfgsb" else None
+        # the reference's LBFGSpp settings: m corrections (lbfgsb_m), at most lbfgsb_max_linesearch
+        # line-search trials, convergence at a projected gradient below lbfgsb_epsilon
+        opts = {"maxiter": max_it}
+        if algo == "lbfgsb":
+            opts.update(maxcor=int(cfg.lbfgsb_m), maxls=int(cfg.lbfgsb_max_linesearch), gtol=float(cfg.lbfgsb_epsilon))
         res = minimize(fg, theta, jac=True, method="L-BFGS-B" if algo == "lbfgsb" else "BFGS", bounds=bounds,
-                       options={"maxiter": max_it})
+                       options=opts)
         theta = res.x
     elif algo == "gd":
         project = cfg.phi_transform in ("none", "clamp")

@@ -146,7 +146,7 @@ def test_queue_autotune_keeps_results(pkg):
     batch = pkg.Batch(members)
     batch.step(25)
     rep = batch.autotune(steps=3, tile_sizes=(128, 512))
-    assert rep.count("tile128") == 5 and "chosen" in rep
+    assert rep.count("/tile128=") == 5 and "chosen" in rep
     batch.step(40)
     for m in alone:
         m.step(65)
