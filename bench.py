@@ -760,11 +760,14 @@ def run_ensemble(pkg, args, local_rank):
     """Batched ensemble: `--ensemble-members` independent SP solves, sizes log-uniform in
     [5k, 200k] cells (seeded), alternately the dam-break and the Gaussian-bump constructions,
     MUSCL-EVR + HLLC, Manning n perturbed by +-20 % (smooth field, per member).  Forward:
-    `--ensemble-steps` steps of every member as one batch (one graph launch per 32-step chunk,
-    members on concurrent stream branches) against the same members stepped one after another
-    (each with its own graph).  Adjoint: each member records its trajectory and observes 16
-    gauges every 10 steps; the members' gradients run concurrently (batch) and one after
-    another.  Host wall time around synchronous calls (both arms alike)."""
+    `--ensemble-steps` steps of every member in three forms, each timed with CUDA events on the
+    device: the work queue (one persistent kernel over (step, phase, member, tile) items, its
+    launch variant and tile size autotuned first), the graph of per-member stream branches, and
+    the members one after another (each with its own step graph; the sum of the members' device
+    times).  Every form continues from the same states (saved and restored), and the queue's and
+    the branches' results are checked bit for bit against the sequential ones.  Adjoint: each
+    member records its trajectory and observes 16 gauges every 10 steps; the members' gradients
+    run concurrently (batch, host threads) and one after another (host wall time)."""
     import numpy as np
     import torch
 
@@ -784,20 +787,56 @@ def run_ensemble(pkg, args, local_rank):
         m.set_param("friction", n1 * (1.0 + 0.2 * f))
         models.append(m)
     cells = int(sum(m.n for m in models))
-    batch = pkg.Batch(models)
     K = args.ensemble_steps
+    batch = pkg.Batch(models)
     batch.step(3)
     for m in models:
-        m.step(3)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    done = batch.step(K)
-    t_batch = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    done_seq = [m.step(K) for m in models]
-    t_seq = time.perf_counter() - t0
-    if int(np.sum(done)) != M * K or sum(done_seq) != M * K:
+        m.save_point()
+
+    def reset():
+        for m in models:
+            m.restore_point()
+
+    bstream = torch.cuda.ExternalStream(batch.stream, device=local_rank)
+
+    def timed_batch():
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(bstream)
+        done = batch.step(K)
+        e1.record(bstream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, done
+
+    tune = batch.autotune(steps=4)
+    reset()
+    batch.step(32)       # warm-up (graph capture), then back to the start
+    reset()
+    t_queue, done_q = timed_batch()
+    end_q = [m.state() for m in models]
+    reset()
+    batch.configure(pkg.Batch.BRANCHES)
+    batch.step(32)
+    reset()
+    t_branch, done_b = timed_batch()
+    end_b = [m.state() for m in models]
+    # sequential: each member alone with its own step graph, device time per member summed
+    reset()
+    t_seq, done_seq = 0.0, []
+    for m in models:
+        m.prepare()
+        s = torch.cuda.ExternalStream(m.stream, device=local_rank)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        done_seq.append(m.step(K))
+        e1.record(s)
+        e1.synchronize()
+        t_seq += e0.elapsed_time(e1) / 1e3
+    end_s = [m.state() for m in models]
+    if int(np.sum(done_q)) != M * K or int(np.sum(done_b)) != M * K or sum(done_seq) != M * K:
         raise RuntimeError("ensemble: a member stopped early")
+    same = lambda A, B: all(np.array_equal(x.view(np.int64), y.view(np.int64)) for a, b in zip(A, B) for x, y in zip(a, b))
     # adjoints: record, observe, then concurrent vs sequential gradients
     for m in models:
         m.record(K, args.ensemble_every)
@@ -808,25 +847,33 @@ def run_ensemble(pkg, args, local_rank):
     t0 = time.perf_counter()
     res = batch.adjoint(n_threads=16)
     t_adj_batch = time.perf_counter() - t0
-    nonfinite = sum(sum(m.adjoint_nonfinite().values()) for m in models)
+    nonfinite = [int(sum(m.adjoint_nonfinite().values())) for m in models]
     t0 = time.perf_counter()
     res_seq = [m.adjoint() for m in models]
     t_adj_seq = time.perf_counter() - t0
-    same = all(a[0] == b[0] and all(np.array_equal(a[1][k], b[1][k]) for k in a[1]) for a, b in zip(res, res_seq))
+    same_adj = all(a[0] == b[0] and all(np.array_equal(a[1][k], b[1][k]) for k in a[1]) for a, b in zip(res, res_seq))
     free, total = torch.cuda.mem_get_info(local_rank)
     batch.close()
     return {
         "workload": f"{M} SP members, {int(sizes.min())}-{int(sizes.max())} cells (log-uniform, {cells} in all), "
                     f"dam break / Gaussian bumps, MUSCL-EVR + HLLC, Manning n +-20 %, {K} steps each",
         "metric": "ensemble cell-updates/s", "unit": "cell-updates/s",
-        "value": cells * K / t_batch, "sequential_value": cells * K / t_seq, "speedup": t_seq / t_batch,
-        "s_batched": t_batch, "s_sequential": t_seq,
+        "value": cells * K / t_queue,
+        "arms_device_s": {"work_queue": t_queue, "stream_branches": t_branch, "sequential": t_seq},
+        "arms_value": {"work_queue": cells * K / t_queue, "stream_branches": cells * K / t_branch,
+                       "sequential": cells * K / t_seq},
+        "speedup_queue_over_sequential": t_seq / t_queue, "speedup_queue_over_branches": t_branch / t_queue,
+        "bitwise_same_as_sequential": {"work_queue": bool(same(end_q, end_s)), "stream_branches": bool(same(end_b, end_s))},
+        "queue_tuning": tune,
         "adjoint": {"gradients_per_s": M / t_adj_batch, "sequential_gradients_per_s": M / t_adj_seq,
                     "speedup": t_adj_seq / t_adj_batch, "s_batched": t_adj_batch, "s_sequential": t_adj_seq,
-                    "checkpoint_every": args.ensemble_every, "bitwise_same_as_sequential": bool(same),
-                    "nonfinite_entries_set_to_zero": int(nonfinite)},
+                    "checkpoint_every": args.ensemble_every, "bitwise_same_as_sequential": bool(same_adj),
+                    "timing": "host wall time (the adjoints run from host threads)",
+                    "nonfinite_entries_set_to_zero": int(sum(nonfinite)),
+                    "nonfinite_per_member": {str(i): c for i, c in enumerate(nonfinite) if c}},
         "device_memory_in_use_gb": (total - free) / 1e9,
-        "timing": "host wall time around synchronous calls, both arms alike",
+        "timing": "forward: CUDA events on the device (queue and branches on the batch's stream; sequential: "
+                  "sum of the members' own device times)",
     }
 
 

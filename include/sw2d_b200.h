@@ -372,6 +372,12 @@ int sw2d_result_close(sw2d_handle* h);
  * stopping once t >= t_max.  The loop runs on the device (CUDA graph); the host does not
  * synchronise between steps.  *steps_done receives the number of steps taken (may be NULL). */
 int sw2d_step_n(sw2d_handle* h, int64_t n_steps, int64_t* steps_done);
+/* Saves the run's point on the device (state, the balance slots that carry the fluxes of edges
+ * left dry from step to step, time, dt and step count); sw2d_restore_point returns the run to
+ * it, so that the steps that follow give the same bits as from the saved point.  One point per
+ * handle (saving again replaces it).  SP and DIP models.  No counterpart in the reference. */
+int sw2d_save_point(sw2d_handle* h);
+int sw2d_restore_point(sw2d_handle* h);
 /* Captures and instantiates the CUDA graph sw2d_step_n launches (32 steps, or the result file's
  * chunk), without taking a step, so that a timed run does not include the capture; the graph is
  * captured again after an option or launch configuration changes.  No counterpart in the

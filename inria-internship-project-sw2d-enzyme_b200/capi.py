@@ -328,6 +328,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_set_t_max.restype = ctypes.c_int
     lib.sw2d_step_n.argtypes = [P, ctypes.c_int64, c_int64_p]
     lib.sw2d_step_n.restype = ctypes.c_int
+    lib.sw2d_save_point.argtypes = [P]
+    lib.sw2d_save_point.restype = ctypes.c_int
+    lib.sw2d_restore_point.argtypes = [P]
+    lib.sw2d_restore_point.restype = ctypes.c_int
     lib.sw2d_prepare_steps.argtypes = [P]
     lib.sw2d_prepare_steps.restype = ctypes.c_int
     lib.sw2d_execute.argtypes = [P, c_int64_p]
@@ -460,7 +464,7 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_mlp_destroy", "sw2d_mlp_last_error", "sw2d_mlp_get_params", "sw2d_mlp_infer",
             "sw2d_mlp_loss_grad", "sw2d_mlp_adam_step", "sw2d_mlp_set_wait_polls", "sw2d_set_closure", "sw2d_closure_record", "sw2d_set_t_max",
             "sw2d_result_header", "sw2d_result_open", "sw2d_result_close", "sw2d_map_porosity", "sw2d_map_porosity_raster",
-            "sw2d_map_last_error", "sw2d_step_n", "sw2d_prepare_steps", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
+            "sw2d_map_last_error", "sw2d_step_n", "sw2d_prepare_steps", "sw2d_save_point", "sw2d_restore_point", "sw2d_execute", "sw2d_get_state", "sw2d_set_state",
             "sw2d_get_state_device", "sw2d_set_state_device", "sw2d_get_time", "sw2d_set_time",
             "sw2d_get_array", "sw2d_get_cell_permutation", "sw2d_get_stream", "sw2d_kernels_per_step",
             "sw2d_destroy", "sw2d_last_error", "sw2d_abi_version", "sw2d_phase_times", "sw2d_phase_name", "sw2d_phase_label", "sw2d_get_option",

@@ -1515,6 +1515,46 @@ int sw2d_set_state(sw2d_handle* h, const double* wd, const double* qx, const dou
     return SW2D_OK;
 }
 
+// bytes of a saved point: the state records, the balance slots (they keep the fluxes of edges
+// left dry from one step to the next) and the control block
+static size_t point_bytes(const sw2d_handle* h, size_t* st, size_t* sl)
+{
+    *st = (size_t)h->nc * sizeof(double4);
+    *sl = (size_t)h->h_coff.back().y * sizeof(Slot);
+    return *st + *sl + sizeof(Ctrl);
+}
+
+int sw2d_save_point(sw2d_handle* h)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    if (h->model == kModelDdp) return fail(h, SW2D_E_UNSUPPORTED, "save_point: the DDP model keeps more state");
+    CK(cudaSetDevice(h->device));
+    size_t st, sl;
+    const size_t bytes = point_bytes(h, &st, &sl);
+    if (!h->saved_point) CK(cudaMalloc(&h->saved_point, bytes));
+    char* d = static_cast<char*>(h->saved_point);
+    CK(cudaMemcpyAsync(d, h->m.st, st, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(d + st, h->m.slot, sl, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(d + st + sl, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
+int sw2d_restore_point(sw2d_handle* h)
+{
+    if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
+    if (!h->saved_point) return fail(h, SW2D_E_ARG, "restore_point: no point saved");
+    CK(cudaSetDevice(h->device));
+    size_t st, sl;
+    point_bytes(h, &st, &sl);
+    const char* d = static_cast<const char*>(h->saved_point);
+    CK(cudaMemcpyAsync(h->m.st, d, st, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->m.slot, d + st, sl, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->ctrl, d + st + sl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SW2D_OK;
+}
+
 int sw2d_set_t_max(sw2d_handle* h, double t_max)
 {
     if (!h) return fail(h, SW2D_E_ARG, "invalid handle");
@@ -1784,6 +1824,7 @@ int sw2d_destroy(sw2d_handle* h)
     result_release(h);
     for (void* p : h->allocs) cudaFree(p);
     for (void* p : h->tile_allocs) cudaFree(p);
+    if (h->saved_point) cudaFree(h->saved_point);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

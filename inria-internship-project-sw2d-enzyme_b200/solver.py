@@ -124,6 +124,14 @@ class SpModel:
         self._check(self.lib.sw2d_step_n(self.handle, int(n), ctypes.byref(done)))
         return int(done.value)
 
+    def save_point(self) -> None:
+        """Saves the run's point on the device (state, balance slots, time); restore_point
+        returns to it with the same bits as from the saved point."""
+        self._check(self.lib.sw2d_save_point(self.handle))
+
+    def restore_point(self) -> None:
+        self._check(self.lib.sw2d_restore_point(self.handle))
+
     def prepare(self) -> None:
         """Captures the step graph that ``step`` launches (no step taken), so that a timed run
         does not include the capture."""

@@ -171,3 +171,20 @@ def test_queue_wait_that_runs_out(pkg):
     for m in alone:
         m.step(40)
     _same_as_alone(alone, members)
+
+
+def test_save_and_restore_point(pkg):
+    """sw2d_save_point / sw2d_restore_point: the steps after a restore give the bits of the steps
+    after the save (the balance slots, which keep the fluxes of edges left dry, are restored with
+    the state and the time)."""
+    case = pkg.workloads.gaussian_bumps(n_cells=20000, mesh="delaunay", initial="dam")
+    m = pkg.SpModel(case)
+    m.step(10)
+    m.save_point()
+    m.step(37)
+    first, t_first = m.state(), m.time
+    m.step(5)
+    m.restore_point()
+    assert m.step(37) == 37 and m.time == t_first
+    for x, y in zip(first, m.state()):
+        assert _bits_equal(x, y)
