@@ -591,6 +591,13 @@ int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad);
  * 1/max(h, 1e-16) factors of the wave speeds and velocities, and over long windows their
  * adjoint can overflow. */
 int sw2d_adjoint_nonfinite(sw2d_handle* h, int64_t* counts);
+/* With the option "adjoint_trace" on, the last sw2d_adjoint's state adjoint after each reverse
+ * step j (trajectory order): entries with a non-finite component, the largest finite |adjoint of
+ * h| and of q or r, and the first cell (caller numbering; -1 for none) holding a non-finite one.
+ * Arrays of `capacity` values, any may be NULL; returns the trajectory's step count.  No
+ * counterpart in the reference. */
+int sw2d_adjoint_trace(sw2d_handle* h, int64_t* nonfinite, double* max_h, double* max_qr, int64_t* first_cell,
+                       int64_t capacity);
 
 /* ---- Ensembles ---------------------------------------------------------------------------------
  * The reference runs one simulation per process; its assimilation evaluates line-search trial

@@ -406,6 +406,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.sw2d_adjoint.restype = ctypes.c_int
     lib.sw2d_adjoint_nonfinite.argtypes = [P, c_int64_p]
     lib.sw2d_adjoint_nonfinite.restype = ctypes.c_int
+    lib.sw2d_adjoint_trace.argtypes = [P, c_int64_p, c_double_p, c_double_p, c_int64_p, ctypes.c_int64]
+    lib.sw2d_adjoint_trace.restype = ctypes.c_int
     # ensembles
     lib.sw2d_batch_create.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P)]
     lib.sw2d_batch_create.restype = ctypes.c_int
@@ -471,7 +473,7 @@ EXPORTED = ["sw2d_create", "sw2d_create_dip", "sw2d_create_ddp", "sw2d_ddp_get_t
             "sw2d_set_option", "sw2d_eval_math", "sw2d_autotune", "sw2d_autotune_step", "sw2d_get_launch_config",
             "sw2d_set_launch_config", "sw2d_get_array_noalloc", "sw2d_record", "sw2d_rerecord", "sw2d_trajectory_info",
             "sw2d_get_trajectory_dt", "sw2d_set_trajectory_start", "sw2d_set_param", "sw2d_get_param",
-            "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint", "sw2d_adjoint_nonfinite",
+            "sw2d_set_observations", "sw2d_replay_cost", "sw2d_replay_sample", "sw2d_adjoint", "sw2d_adjoint_nonfinite", "sw2d_adjoint_trace",
             "sw2d_batch_create", "sw2d_batch_step_n", "sw2d_batch_adjoint", "sw2d_batch_size",
             "sw2d_batch_configure", "sw2d_batch_get_config", "sw2d_batch_autotune", "sw2d_batch_set_wait_polls",
             "sw2d_batch_stream",

@@ -12,9 +12,12 @@
 //
 // The load policy L says how a body reads the arrays that the step itself writes (states,
 // slopes, balance slots, CFL contributions, the control block).  LdNc: the step kernels, where
-// those arrays were written by an earlier kernel, through the read-only path.  LdL2: the work-
-// queue kernel, where other CTAs of the same launch wrote them, through L2 (L1 is not coherent
-// between SMs); the arithmetic is the same.
+// those arrays were written by an earlier kernel, through the read-only path.  LdL2: through L2
+// only.  LdCo: plain (coherent, L1-cached) loads, for the work-queue kernel, where other CTAs of
+// the same launch wrote the arrays: each item starts after a gpu-scope acquire of the counter
+// its prerequisites released, followed by a CTA barrier, and the memory model then orders its
+// plain loads after those writes (the read-only path gives no such guarantee).  The arithmetic
+// is the same under every policy.
 #pragma once
 
 #include "sw2d_internal.cuh"
@@ -54,6 +57,14 @@ struct LdL2 {
     template <class T>
     static __device__ __forceinline__ T own(const T* p) { return ldl2(p); }
     static __device__ __forceinline__ double ctl(const double* p) { return __ldcg(p); }
+};
+
+struct LdCo {
+    template <class T>
+    static __device__ __forceinline__ T in(const T* p) { return *p; }
+    template <class T>
+    static __device__ __forceinline__ T own(const T* p) { return *p; }
+    static __device__ __forceinline__ double ctl(const double* p) { return *p; }
 };
 
 // ------------------------------------------------------------------------------------------

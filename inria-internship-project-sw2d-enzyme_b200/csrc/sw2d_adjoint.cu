@@ -85,6 +85,11 @@ struct AdjointState {
     double* stage = nullptr;             // nc doubles for parameter transfers
     unsigned long long* d_nonfinite = nullptr;  // 6 counters of the last gradient's clean-up
     int64_t nonfinite[6] = {0, 0, 0, 0, 0, 0};
+    // option "adjoint_trace": per reverse step j, after its kernels, {non-finite entries of the
+    // state adjoint, bits of max |adjoint of h|, bits of max |adjoint of q, r|, first cell with a
+    // non-finite entry}
+    unsigned long long* d_trace = nullptr;
+    int64_t trace_steps = 0;
     // observations
     int64_t n_pts = 0, n_obs = 0;
     int normalize = 0;
@@ -366,6 +371,22 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
     gzb[c] += zbb;
 }
 
+// one reverse step of the trace: non-finite entries of the state adjoint (count, first cell)
+// and the largest finite magnitudes (order-preserving bits of non-negative doubles)
+__global__ void k_trace(const double4* __restrict__ lam, int n, unsigned long long* out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double4 l = lam[c];
+    if (!isfinite(l.x) || !isfinite(l.y) || !isfinite(l.z)) {
+        atomicAdd(out, 1ull);
+        atomicMin(out + 3, (unsigned long long)c);
+        return;
+    }
+    atomicMax(out + 1, (unsigned long long)__double_as_longlong(fabs(l.x)));
+    atomicMax(out + 2, (unsigned long long)__double_as_longlong(fmax(fabs(l.y), fabs(l.z))));
+}
+
 __global__ void k_sanitize(double4* lam, double* gzb, double* gk1, double* gk2, unsigned long long* counts, int n,
                            int with_friction, int keep)
 {
@@ -640,6 +661,21 @@ int reverse_sweep(sw2d_handle* h)
     CK(cudaMemsetAsync(a->g_k2, 0, nc * sizeof(double), h->stream));
     const unsigned gc = grid_for(nc);
     int rc = SW2D_OK;
+    if (h->adj_trace) {
+        if (a->trace_steps != a->n_steps) {
+            cudaFree(a->d_trace);
+            a->d_trace = nullptr;
+            CK(cudaMalloc(&a->d_trace, 4 * a->n_steps * sizeof(unsigned long long)));
+            a->trace_steps = a->n_steps;
+        }
+        std::vector<unsigned long long> init(4 * a->n_steps, 0ull);
+        for (int64_t j = 0; j < a->n_steps; j++) init[4 * j + 3] = ~0ull;
+        CK(cudaMemcpy(a->d_trace, init.data(), init.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    } else if (a->d_trace) {
+        cudaFree(a->d_trace);
+        a->d_trace = nullptr;
+        a->trace_steps = 0;
+    }
     for (int64_t s = a->n_ck - 1; s >= 0; s--) {
         const int64_t j0 = s * a->every, j1 = std::min(a->n_steps, j0 + a->every);
         if ((rc = ck_load(h, s))) return rc;
@@ -683,6 +719,8 @@ int reverse_sweep(sw2d_handle* h)
                 k_cells_rev<SW2D_SCHEME_GODUNOV><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
                                                                                 a->sgb, dtp);
             }
+            if (a->d_trace && j < a->trace_steps)
+                k_trace<<<gc, kBlock, 0, h->stream>>>(a->lam, (int)nc, a->d_trace + 4 * j);
         }
         CK(cudaGetLastError());
     }
@@ -775,6 +813,7 @@ namespace sw2d {
 void adjoint_release(sw2d_handle* h)
 {
     if (!h || !h->adj) return;
+    cudaFree(h->adj->d_trace);
     free_list(h->adj->traj_allocs);
     free_list(h->adj->obs_allocs);
     free_list(h->adj->fixed_allocs);
@@ -1080,6 +1119,25 @@ int sw2d_adjoint(sw2d_handle* h, double* J, const sw2d_gradient* grad)
         }
     }
     return SW2D_OK;
+}
+
+int sw2d_adjoint_trace(sw2d_handle* h, int64_t* nonfinite, double* max_h, double* max_qr, int64_t* first_cell,
+                       int64_t capacity)
+{
+    if (!h || capacity < 0) return fail(h, SW2D_E_ARG, "invalid arguments");
+    if (!h->adj || !h->adj->d_trace) return fail(h, SW2D_E_ARG, "no traced gradient (option adjoint_trace)");
+    AdjointState* a = h->adj;
+    const int64_t n = std::min(capacity, a->trace_steps);
+    std::vector<unsigned long long> t(4 * a->trace_steps);
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpy(t.data(), a->d_trace, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (int64_t j = 0; j < n; j++) {
+        if (nonfinite) nonfinite[j] = (int64_t)t[4 * j];
+        if (max_h) max_h[j] = __builtin_bit_cast(double, t[4 * j + 1]);
+        if (max_qr) max_qr[j] = __builtin_bit_cast(double, t[4 * j + 2]);
+        if (first_cell) first_cell[j] = t[4 * j + 3] == ~0ull ? -1 : h->cell_perm[t[4 * j + 3]];
+    }
+    return (int)std::min<int64_t>(a->trace_steps, INT32_MAX);
 }
 
 int sw2d_adjoint_nonfinite(sw2d_handle* h, int64_t* counts)

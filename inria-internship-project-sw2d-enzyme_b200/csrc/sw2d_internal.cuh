@@ -226,6 +226,7 @@ struct sw2d_handle {
     sw2d::AdjointState* adj = nullptr;  // recorded trajectory, checkpoints and adjoint buffers
     int adj_flush_branch = 0;           // option "adjoint_flush_branch"
     int adj_keep_nonfinite = 0;         // option "adjoint_keep_nonfinite"
+    int adj_trace = 0;                  // option "adjoint_trace"
     void* saved_point = nullptr;        // sw2d_save_point: state, balance slots, control block
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step

@@ -19,6 +19,11 @@
 // the launch wrote the data), so every member's results are bit for bit those of the member run
 // alone.  A wait that runs out sets the queue's status word; every CTA then leaves the queue,
 // and the host reports the error.
+//
+// Memory ordering: an item's thread 0 takes the counter of its prerequisite with a gpu-scope
+// acquire load and the CTA then passes a barrier; a finished item passes a barrier, and its
+// thread 0 fences (gpu scope) and increments its counter.  That release/acquire chain orders
+// every write of a prerequisite before every plain load of the item that depends on it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,6 +38,10 @@ namespace sw2d {
 namespace {
 
 constexpr int kPhaseSlopes = 0, kPhaseEdges = 1, kPhaseCfl = 2, kPhaseUpdate = 3;
+
+// how the phases read what other CTAs of the launch wrote (sp_phases.cuh): plain loads after
+// the item's acquire and barrier
+using LdQ = LdCo;
 constexpr unsigned kQueueTimeout = 1u;
 
 struct QMember {
@@ -92,7 +101,7 @@ __device__ bool wait_at_least(const QArgs& q, const unsigned* p, unsigned target
 // item, not per element.
 __device__ __noinline__ void q_slopes(const DevMesh& m, int c0, int c1, int stride)
 {
-    for (int c = c0; c < c1; c += stride) slopes_cell<LdL2>(m, c);
+    for (int c = c0; c < c1; c += stride) slopes_cell<LdQ>(m, c);
 }
 
 template <int kScheme, bool kBlending>
@@ -100,15 +109,15 @@ __device__ __noinline__ unsigned q_edges(const DevMesh& m, int i0, int i1, int s
 {
     unsigned bad = 0;
     for (int i = i0; i < i1; i += stride)
-        bad |= (i < m.ni) ? edge_internal<kScheme, kBlending, kModelSp, LdL2>(m, i)
-                          : edge_boundary<kScheme, kModelSp, LdL2>(m, i - m.ni);
+        bad |= (i < m.ni) ? edge_internal<kScheme, kBlending, kModelSp, LdQ>(m, i)
+                          : edge_boundary<kScheme, kModelSp, LdQ>(m, i - m.ni);
     return bad;
 }
 
 __device__ __noinline__ double q_cfl(const DevMesh& m, int c0, int c1, int stride, double best)
 {
     for (int c = c0; c < c1; c += stride) {
-        const double x = cfl_cell<LdL2>(m, c);
+        const double x = cfl_cell<LdQ>(m, c);
         if (x < best) best = x;
     }
     return best;
@@ -117,7 +126,7 @@ __device__ __noinline__ double q_cfl(const DevMesh& m, int c0, int c1, int strid
 template <int kFriction, bool kHeadLoss>
 __device__ __noinline__ void q_update(const DevMesh& m, int c0, int c1, int stride, double dt)
 {
-    for (int c = c0; c < c1; c += stride) update_cell<kFriction, kHeadLoss, false, false, LdL2>(m, c, dt);
+    for (int c = c0; c < c1; c += stride) update_cell<kFriction, kHeadLoss, false, false, LdQ>(m, c, dt);
 }
 
 template <int kFriction>
@@ -216,7 +225,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_queue(QArgs q)
                 // the member's last CFL tile of step s: publish its dt (or stop the member)
                 __threadfence();
                 const unsigned long long key = atomicExch(&q.dmin[mi], kDminEmpty);
-                if (active(ctrl)) dt_finalize<false, LdL2>(m, ctrl, __longlong_as_double((long long)dmin_bits(key)));
+                if (active(ctrl)) dt_finalize<false, LdQ>(m, ctrl, __longlong_as_double((long long)dmin_bits(key)));
                 else ctrl->go = 0;
                 __threadfence();
                 atomicExch(&sy->dt_ready, s + 1);

@@ -1371,6 +1371,11 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
     } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
         h->adj_flush_branch = value ? 1 : 0;
         return SW2D_OK;
+    } else if (std::strcmp(name, "adjoint_trace") == 0) {
+        // 1: sw2d_adjoint records, after each reverse step, the non-finite entries and the largest
+        // magnitudes of the state adjoint (sw2d_adjoint_trace)
+        h->adj_trace = value ? 1 : 0;
+        return SW2D_OK;
     } else if (std::strcmp(name, "adjoint_keep_nonfinite") == 0) {
         // 1: sw2d_adjoint counts its non-finite gradient entries but hands them back as they are
         // (to locate them) instead of zeroing them as the reference does

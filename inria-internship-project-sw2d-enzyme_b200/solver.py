@@ -357,6 +357,19 @@ class SpModel:
         self._check(self.lib.sw2d_adjoint_nonfinite(self.handle, c.ctypes.data_as(capi.c_int64_p)))
         return dict(zip(self.GRADIENTS, (int(v) for v in c)))
 
+    def adjoint_trace(self) -> dict:
+        """With the option "adjoint_trace": the last gradient's state adjoint after each reverse
+        step (trajectory order): non-finite entries, largest finite |adjoint| of h and of q/r, and
+        the first cell holding a non-finite entry (-1: none)."""
+        n = int(self.lib.sw2d_adjoint_trace(self.handle, None, None, None, None, 0))
+        if n < 0:
+            self._check(n)
+        nf, fc = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        mh, mq = np.zeros(n), np.zeros(n)
+        self._check(min(0, self.lib.sw2d_adjoint_trace(self.handle, nf.ctypes.data_as(capi.c_int64_p), _p(mh), _p(mq),
+                                                       fc.ctypes.data_as(capi.c_int64_p), n)))
+        return {"nonfinite": nf, "max_h": mh, "max_qr": mq, "first_cell": fc}
+
     # ---- porosity assimilation with the reference's differentiated step (sw2d_assim_*) ----
     PHI_TRANSFORMS = {"none": 0, "clamp": 1, "tanh": 2, "normalize": 3}
 
