@@ -60,6 +60,8 @@ def _args():
     ap.add_argument("--adjoint-cells", type=int, default=1_000_000, help="cells of the adjoint workload")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--adjoint-every", type=int, default=100, help="checkpoint interval of the adjoint")
+    ap.add_argument("--adjoint-store-states", type=int, default=1,
+                    help="1: the segment recompute keeps each step's slopes and Riemann states for the reverse")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--dip-cells", type=int, default=4_000_000, help="cells of the DIP forward line (0: skip)")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the ensemble line (0: skip)")
@@ -302,6 +304,7 @@ def run_adjoint(pkg, args, local_rank):
     free0, total = torch.cuda.mem_get_info(local_rank)
     model = pkg.SpModel(case, device=local_rank)
     pkg.tuning.autotune(model, iters=3, device=local_rank, cache_path=None)
+    model.set_option("adjoint_store_states", args.adjoint_store_states)
     stream = torch.cuda.ExternalStream(model.stream, device=local_rank)
     n = case.mesh.cell_nb
 

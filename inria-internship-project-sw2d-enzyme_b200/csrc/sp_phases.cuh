@@ -201,6 +201,14 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
     }
     const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
     if (m.lmax) m.lmax[e] = lm;
+    if (m.rstate) {
+        double2* p = m.rstate + 5 * (size_t)e;
+        p[0] = make_double2(SL.z, SL.q);
+        p[1] = make_double2(SL.r, SL.lm);
+        p[2] = make_double2(SL.lp, SR.z);
+        p[3] = make_double2(SR.q, SR.r);
+        p[4] = make_double2(SR.lm, SR.lp);
+    }
     const double lw = lm * ld(&m.len[e]);
     const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;
     const int2 sl = ld(&m.eslot[e]);

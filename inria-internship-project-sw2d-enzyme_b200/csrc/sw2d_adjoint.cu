@@ -68,6 +68,8 @@ struct AdjointState {
     // one segment of recomputed steps
     double4* seg_st = nullptr;           // (every + 1) * nc
     double4* seg_bal = nullptr;          // every * nc
+    double2* seg_slope = nullptr;        // every * nc: each step's MUSCL-EVR slopes
+    double2* seg_rs = nullptr;           // every * ni * 5: each step's Riemann states (when memory allows)
     // adjoint buffers
     double4* lam = nullptr;              // nc: adjoint of the state {h, q, r, -}
     double4* sig = nullptr;              // nslot: adjoint of the balance slots {a, b, c, -}
@@ -225,9 +227,11 @@ __device__ __forceinline__ void slot_rev(const SlotFactors& f, const double4& s,
     Sb += f.f2S2 * s.y + f.f3S2 * s.z;
 }
 
-template <int kScheme, bool kBlending, int kB, int kMinB>
+// kStored: the two Riemann states of the step come from the segment's forward recompute
+// (rs, 5 x double2 per edge) instead of being rebuilt here
+template <int kScheme, bool kBlending, int kB, int kMinB, bool kStored>
 __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig, double4* ctb, double2* cts, double t,
-                                                         double dtp)
+                                                         double dtp, const double2* __restrict__ rs)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m.ni) {
@@ -235,13 +239,27 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig
         const int2 lr = ld(&m.lr[e]);
         const int a = lr.x, b = lr.y;
         const double2 n = ld(&m.nxy[e]);
-        const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
         const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
         SideState SL, SR;
-        if (kScheme == SW2D_SCHEME_GODUNOV) {
+        if (kStored) {
+            const double2* p = rs + 5 * (size_t)e;
+            const double2 r0 = ld(p), r1 = ld(p + 1), r2 = ld(p + 2), r3 = ld(p + 3), r4 = ld(p + 4);
+            SL.z = r0.x;
+            SL.q = r0.y;
+            SL.r = r1.x;
+            SL.lm = r1.y;
+            SL.lp = r2.x;
+            SR.z = r2.y;
+            SR.q = r3.x;
+            SR.r = r3.y;
+            SR.lm = r4.x;
+            SR.lp = r4.y;
+        } else if (kScheme == SW2D_SCHEME_GODUNOV) {
+            const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
             SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
             SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
         } else {
+            const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
             const double4 d = ld(&m.emc[e]);
             const double2 ga = m.slope[a], gb = m.slope[b];
             SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp, m.dry);
@@ -575,35 +593,41 @@ constexpr RevVariant kRevVariants[] = {{128, 3}, {256, 1}, {256, 2}, {128, 4}, {
 constexpr int kNumRevVariants = sizeof(kRevVariants) / sizeof(kRevVariants[0]);
 
 template <int kScheme, bool kBlending, int V>
-void launch_edges_rev_v(sw2d_handle* h, const DevMesh& m, double t, double dtp)
+void launch_edges_rev_v(sw2d_handle* h, const DevMesh& m, double t, double dtp, const double2* rs)
 {
     constexpr int B = kRevVariants[V].block, M = kRevVariants[V].minb;
     AdjointState* a = h->adj;
     const unsigned n = (unsigned)(m.ni + m.nb);
-    k_edges_rev<kScheme, kBlending, B, M><<<(n + B - 1) / B, B, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t, dtp);
+    if (rs)
+        k_edges_rev<kScheme, kBlending, B, M, true><<<(n + B - 1) / B, B, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t,
+                                                                                          dtp, rs);
+    else
+        k_edges_rev<kScheme, kBlending, B, M, false><<<(n + B - 1) / B, B, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t,
+                                                                                           dtp, rs);
 }
 
 template <int kScheme, bool kBlending>
-void launch_edges_rev_s(sw2d_handle* h, const DevMesh& m, double t, double dtp)
+void launch_edges_rev_s(sw2d_handle* h, const DevMesh& m, double t, double dtp, const double2* rs)
 {
     switch (h->adj_edge_variant) {
-        case 1: launch_edges_rev_v<kScheme, kBlending, 1>(h, m, t, dtp); break;
-        case 2: launch_edges_rev_v<kScheme, kBlending, 2>(h, m, t, dtp); break;
-        case 3: launch_edges_rev_v<kScheme, kBlending, 3>(h, m, t, dtp); break;
-        case 4: launch_edges_rev_v<kScheme, kBlending, 4>(h, m, t, dtp); break;
-        default: launch_edges_rev_v<kScheme, kBlending, 0>(h, m, t, dtp); break;
+        case 1: launch_edges_rev_v<kScheme, kBlending, 1>(h, m, t, dtp, rs); break;
+        case 2: launch_edges_rev_v<kScheme, kBlending, 2>(h, m, t, dtp, rs); break;
+        case 3: launch_edges_rev_v<kScheme, kBlending, 3>(h, m, t, dtp, rs); break;
+        case 4: launch_edges_rev_v<kScheme, kBlending, 4>(h, m, t, dtp, rs); break;
+        default: launch_edges_rev_v<kScheme, kBlending, 0>(h, m, t, dtp, rs); break;
     }
 }
 
-void launch_edges_rev(sw2d_handle* h, const DevMesh& m, double t, double dtp)
+// rs: the step's stored Riemann states, or nullptr to rebuild them
+void launch_edges_rev(sw2d_handle* h, const DevMesh& m, double t, double dtp, const double2* rs)
 {
     const bool bl = h->p.topo == SW2D_TOPO_BLENDING;
     if (h->p.scheme == SW2D_SCHEME_GODUNOV) {
-        if (bl) launch_edges_rev_s<SW2D_SCHEME_GODUNOV, true>(h, m, t, dtp);
-        else launch_edges_rev_s<SW2D_SCHEME_GODUNOV, false>(h, m, t, dtp);
+        if (bl) launch_edges_rev_s<SW2D_SCHEME_GODUNOV, true>(h, m, t, dtp, rs);
+        else launch_edges_rev_s<SW2D_SCHEME_GODUNOV, false>(h, m, t, dtp, rs);
     } else {
-        if (bl) launch_edges_rev_s<SW2D_SCHEME_MUSCL_EVR, true>(h, m, t, dtp);
-        else launch_edges_rev_s<SW2D_SCHEME_MUSCL_EVR, false>(h, m, t, dtp);
+        if (bl) launch_edges_rev_s<SW2D_SCHEME_MUSCL_EVR, true>(h, m, t, dtp, rs);
+        else launch_edges_rev_s<SW2D_SCHEME_MUSCL_EVR, false>(h, m, t, dtp, rs);
     }
 }
 
@@ -685,6 +709,8 @@ int reverse_sweep(sw2d_handle* h)
             CK(cudaMemcpyAsync(stj, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
             DevMesh mj = h->m;
             mj.bal = a->seg_bal + (j - j0) * nc;
+            if (a->seg_slope) mj.slope = a->seg_slope + (j - j0) * nc;
+            if (a->seg_rs) mj.rstate = a->seg_rs + (j - j0) * 5 * h->ni;
             launch_slopes_on(h, mj);
             launch_edges_on(h, mj);
             k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
@@ -704,11 +730,16 @@ int reverse_sweep(sw2d_handle* h)
             DevMesh mr = h->m;
             mr.st = a->seg_st + (j - j0) * nc;
             if (muscl) {
-                DevMesh ms = mr;
-                ms.ctrl = a->ctrl_rev;  // always active: recompute the slopes of step j
-                launch_slopes_on(h, ms);
+                if (a->seg_slope) {
+                    mr.slope = a->seg_slope + (j - j0) * nc;  // kept by the segment's recompute
+                } else {
+                    DevMesh ms = mr;
+                    ms.ctrl = a->ctrl_rev;  // always active: recompute the slopes of step j
+                    launch_slopes_on(h, ms);
+                }
             }
-            launch_edges_rev(h, mr, a->t_seq[j], j > 0 ? a->dt_seq[j - 1] : a->dt_before);
+            launch_edges_rev(h, mr, a->t_seq[j], j > 0 ? a->dt_seq[j - 1] : a->dt_before,
+                             a->seg_rs ? a->seg_rs + (j - j0) * 5 * h->ni : nullptr);
             const double dtp = j > 0 ? a->dt_seq[j - 1] : a->dt_before;
             if (muscl) {
                 k_cells_rev<SW2D_SCHEME_MUSCL_EVR><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
@@ -761,6 +792,20 @@ int alloc_trajectory(sw2d_handle* h, int64_t n_steps, int64_t every)
         free_list(a->traj_allocs);
         a->n_steps = 0;
         return rc;
+    }
+    // each step's slopes and Riemann states, kept by the segment's forward recompute for the
+    // reverse steps, when they fit in half of the free device memory (else rebuilt there)
+    a->seg_slope = nullptr;
+    a->seg_rs = nullptr;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const size_t sl_b = h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? (size_t)seg * nc * sizeof(double2) : 0;
+        const size_t rs_b = (size_t)seg * h->ni * 5 * sizeof(double2);
+        if (h->adj_store_states && sl_b + rs_b < free_b / 2) {
+            if (sl_b && adj_alloc(h, L, seg * nc, &a->seg_slope)) a->seg_slope = nullptr;
+            if (h->ni && adj_alloc(h, L, seg * h->ni * 5, &a->seg_rs)) a->seg_rs = nullptr;
+            h->err.clear();
+        }
     }
     a->n_requested = n_steps;
     return SW2D_OK;

@@ -130,6 +130,8 @@ struct DevMesh {
     const double* len;
     const double2* coef;     // {coefL, coefR}
     double2* flux;           // optional copy: 3 x double2 per edge {F1,F2},{F3,S2L},{S2R,-} (tests)
+    double2* rstate;         // optional: the two Riemann states per edge, 5 x double2 (the adjoint's
+                             // segment recompute keeps them for k_edges_rev)
     double* lmax;            // optional copy of lambda_max (tests)
     // boundary edges
     const int* bcell;
@@ -227,6 +229,7 @@ struct sw2d_handle {
     int adj_flush_branch = 0;           // option "adjoint_flush_branch"
     int adj_keep_nonfinite = 0;         // option "adjoint_keep_nonfinite"
     int adj_trace = 0;                  // option "adjoint_trace"
+    int adj_store_states = 1;           // option "adjoint_store_states"
     void* saved_point = nullptr;        // sw2d_save_point: state, balance slots, control block
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step

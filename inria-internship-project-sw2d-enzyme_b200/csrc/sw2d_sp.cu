@@ -1371,6 +1371,12 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
     } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
         h->adj_flush_branch = value ? 1 : 0;
         return SW2D_OK;
+    } else if (std::strcmp(name, "adjoint_store_states") == 0) {
+        // 1 (default): the adjoint's segment recompute keeps each step's slopes and Riemann
+        // states for the reverse steps when they fit in half of the free device memory; 0:
+        // the reverse steps rebuild them (the same bits).  Takes effect at the next sw2d_record.
+        h->adj_store_states = value ? 1 : 0;
+        return SW2D_OK;
     } else if (std::strcmp(name, "adjoint_trace") == 0) {
         // 1: sw2d_adjoint records, after each reverse step, the non-finite entries and the largest
         // magnitudes of the state adjoint (sw2d_adjoint_trace)
