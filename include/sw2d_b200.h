@@ -645,7 +645,7 @@ int sw2d_batch_adjoint(sw2d_batch* b, double* J, const sw2d_gradient* grads, int
 int sw2d_batch_configure(sw2d_batch* b, int mode, int variant, int cells_per_tile, int edges_per_tile);
 int sw2d_batch_get_config(sw2d_batch* b, int* mode, int* variant, int* cells_per_tile, int* edges_per_tile);
 /* Times the work queue for `steps` steps at every launch variant and each of the n_tile_sizes
- * tile sizes (512, 1024, 2048, 4096 when 0), with CUDA events on the batch's stream, on the
+ * tile sizes (1024 to 16384 cells when 0), with CUDA events on the batch's stream, on the
  * members' current states (saved before and put back after every trial, so the run continues
  * with the same bits), then sets the fastest and writes a one-line report. */
 int sw2d_batch_autotune(sw2d_batch* b, int steps, const int* tile_sizes, int n_tile_sizes, char* report, int capacity);

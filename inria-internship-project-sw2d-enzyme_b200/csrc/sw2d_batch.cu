@@ -42,7 +42,7 @@ struct sw2d_batch {
     // work-queue form
     sw2d::QueueState* queue = nullptr;
     int mode = 0;  // SW2D_BATCH_BRANCHES or SW2D_BATCH_QUEUE
-    int q_variant = 0, q_cells = 1024, q_edges = 1024;
+    int q_variant = 3, q_cells = 4096, q_edges = 4096;  // 128 threads x 6 CTAs per SM, the C4 ensemble's best
     cudaGraphExec_t qgraph = nullptr;
     int qgraph_steps = 0;
     std::string err;
@@ -310,10 +310,10 @@ int sw2d_batch_autotune(sw2d_batch* b, int steps, const int* tile_sizes, int n_t
     std::string why;
     if (!queue_eligible(b->members.data(), (int)b->members.size(), why)) return bfail(b, SW2D_E_UNSUPPORTED, "work queue: " + why);
     BCK(cudaSetDevice(b->device));
-    static const int kTiles[] = {512, 1024, 2048, 4096};
+    static const int kTiles[] = {1024, 2048, 4096, 8192, 16384};
     if (!n_tile_sizes) {
         tile_sizes = kTiles;
-        n_tile_sizes = 4;
+        n_tile_sizes = (int)(sizeof(kTiles) / sizeof(int));
     }
     const size_t M = b->members.size();
     // the members' states, balance slots (which carry the fluxes of edges left dry) and control
