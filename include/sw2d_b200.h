@@ -448,12 +448,6 @@ const char* sw2d_phase_name(int i);
  * differentiating the reference's code line by line gives.
  * "adjoint_keep_nonfinite" (0/1): 1 hands back sw2d_adjoint's non-finite gradient entries as
  * they are (still counted by sw2d_adjoint_nonfinite) instead of zeroing them, to locate them.
- * "adjoint_flat_slopes" (0/1): MUSCL-EVR reverse of the limited slope where the free surface of
- * a cell and of all its neighbours is exactly level (a lake at rest), which puts every limiter
- * test on its kink: 0 (default) the branch taken, the unlimited gradient, as Enzyme
- * differentiates the reference; its linearisation grows about threefold per step over a lake at
- * rest, and long windows overflow; 1 a zero derivative there, what the limiter gives for any
- * perturbation that does not move the neighbourhood as a plane.
  * "adjoint_store_states" (0/1, default 1): the segment recompute keeps each step's slopes and
  * Riemann states for the reverse steps when they fit in half of the free device memory.
  * "adjoint_trace" (0/1): record the state adjoint's magnitude per reverse step

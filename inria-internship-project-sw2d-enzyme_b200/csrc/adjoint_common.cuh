@@ -156,16 +156,8 @@ __device__ __forceinline__ double slope_rev_cell(const DevMesh& m, int e0, int c
 
 // Reverse of each cell's slope limiter (MUSCL-EVR): the cell's own z contribution is applied
 // here, the neighbours' go to znb (one value per internal-neighbour entry).
-//
-// flat_zero: where the free surface of the cell and of all its neighbours is exactly level (a
-// lake at rest), the slope is 0 and every limiter test sits on its kink (the reconstruction
-// equals the neighbours' values).  The branch taken there is the unlimited gradient, whose
-// linearisation over many steps grows (the reverse dynamics of the unlimited second-order
-// reconstruction); any perturbation that does not move the neighbourhood as a plane is clipped
-// by the limiter instead.  flat_zero = 1 gives the slope there a zero derivative, the one-sided
-// derivative in those directions; 0 keeps the branch taken (the reference's Enzyme convention).
 __global__ void __launch_bounds__(kBlock) k_limiter_rev(DevMesh m, const double2* __restrict__ sgb, double4* lam,
-                                                        double* gzb, double* znb, int flat_zero)
+                                                        double* gzb, double* znb)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
@@ -177,14 +169,6 @@ __global__ void __launch_bounds__(kBlock) k_limiter_rev(DevMesh m, const double2
         return;
     }
     const double zc = m.st[c].w;
-    if (flat_zero) {
-        bool level = true;
-        for (int i = e0; i < e1; i++) level = level && (m.st[ld(&m.cint[i]).y].w == zc);
-        if (level) {
-            for (int i = e0; i < e1; i++) znb[i] = 0.0;
-            return;
-        }
-    }
     const double2 xy = ld(&m.cxy[c]);
     double zcb = 0.0;
     if (cnt <= 3) zcb = slope_rev_cell<3>(m, e0, cnt, zc, xy, b.x, b.y, znb);

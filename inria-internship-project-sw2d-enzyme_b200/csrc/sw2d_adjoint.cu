@@ -744,7 +744,7 @@ int reverse_sweep(sw2d_handle* h)
             if (muscl) {
                 k_cells_rev<SW2D_SCHEME_MUSCL_EVR><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
                                                                                   a->sgb, dtp);
-                k_limiter_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->sgb, a->lam, a->g_zb, a->znb, h->adj_flat_slopes);
+                k_limiter_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->sgb, a->lam, a->g_zb, a->znb);
                 k_nbr_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->mirror, a->znb, a->lam, a->g_zb);
             } else {
                 k_cells_rev<SW2D_SCHEME_GODUNOV><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,

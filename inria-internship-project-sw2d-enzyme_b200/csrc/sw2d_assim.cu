@@ -1175,7 +1175,7 @@ int reverse_segment(sw2d_handle* h, int64_t k)
         if (gc > 0) {
             if (muscl) {
                 k_e_cells_rev<true><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_phi, a->sgb);
-                k_limiter_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->sgb, a->lam, a->gzb, a->znb, 0);
+                k_limiter_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->sgb, a->lam, a->gzb, a->znb);
                 k_nbr_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->mirror, a->znb, a->lam, a->gzb);
             } else {
                 k_e_cells_rev<false><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_phi, a->sgb);

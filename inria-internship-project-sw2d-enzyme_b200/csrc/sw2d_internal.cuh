@@ -230,7 +230,6 @@ struct sw2d_handle {
     int adj_keep_nonfinite = 0;         // option "adjoint_keep_nonfinite"
     int adj_trace = 0;                  // option "adjoint_trace"
     int adj_store_states = 1;           // option "adjoint_store_states"
-    int adj_flat_slopes = 0;            // option "adjoint_flat_slopes"
     void* saved_point = nullptr;        // sw2d_save_point: state, balance slots, control block
     int adj_edge_variant = 0;           // option "adjoint_edge_variant"
     sw2d::AssimState* assim = nullptr;  // porosity assimilation with the differentiated step

@@ -1371,13 +1371,6 @@ int sw2d_set_option(sw2d_handle* h, const char* name, int64_t value)
     } else if (std::strcmp(name, "adjoint_flush_branch") == 0) {
         h->adj_flush_branch = value ? 1 : 0;
         return SW2D_OK;
-    } else if (std::strcmp(name, "adjoint_flat_slopes") == 0) {
-        // MUSCL-EVR reverse of the slope where the free surface of a cell and of all its
-        // neighbours is exactly level: 0 the branch taken (the unlimited gradient, the
-        // reference's Enzyme convention), 1 a zero derivative (what the limiter gives for any
-        // perturbation that does not move the neighbourhood as a plane)
-        h->adj_flat_slopes = value ? 1 : 0;
-        return SW2D_OK;
     } else if (std::strcmp(name, "adjoint_store_states") == 0) {
         // 1 (default): the adjoint's segment recompute keeps each step's slopes and Riemann
         // states for the reverse steps when they fit in half of the free device memory; 0:
