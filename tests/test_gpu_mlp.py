@@ -27,18 +27,39 @@ def _setup(seed, n):
 
 
 def test_forward_matches_fp64(C):
+    """Layer by layer against FP64 with the kernels' BF16 roundings.  Each GEMM is checked on the
+    kernel's own inputs (its BF16 activations), so only the FP32 accumulation differs: a wrong
+    accumulation order or a dropped K-chunk shows as an error far above 1e-5.  The activations
+    (GELU with the hardware tanh, relative error about 2^-11) are within one BF16 unit of the
+    FP64 GELU of the kernel's pre-activations, and almost always equal to it.  End to end, the
+    outputs are within 1e-3 (norm-wise) of the all-FP64 forward with the same roundings."""
     rng, norm, x = _setup(1, 1000)          # not a multiple of 128: the padded tail
     p = C.init_params(2)
     p[640:704] = rng.normal(0, 0.2, 64)
     net = C.MLP(p, norm)
     y, lay = net.infer(x, layers=True)
     ref = C.reference_forward(p, norm, x)
+    w = C.unpack(p)
+    z1, h1, z2, h2 = (lay[k].astype(np.float64) for k in range(4))
     # first GEMM + bias: exact products of BF16 operands summed in FP32
-    z1 = lay[0].astype(np.float64)
     assert np.max(np.abs(z1 - ref["z1"])) <= 1e-5 * (1.0 + np.max(np.abs(ref["z1"])))
-    z2 = lay[2].astype(np.float64)
-    assert np.max(np.abs(z2 - ref["z2"])) <= 2e-2 * (1.0 + np.max(np.abs(ref["z2"])))
-    assert np.max(np.abs(y - ref["y"])) <= 2e-2 * (1.0 + np.max(np.abs(ref["y"])))
+    # activations: one BF16 unit at most from the FP64 GELU of the kernel's own pre-activations
+    for z, h in ((z1, h1), (z2, h2)):
+        g = C.bf16(C.gelu(z))
+        ulp = np.maximum(np.abs(g), 1e-30) * 2.0 ** -7
+        assert np.all(np.abs(h - g) <= ulp + 1e-30)
+        assert np.mean(h == g) >= 0.99
+    # second and third GEMMs on the kernel's activations
+    z2_k = h1 @ C.bf16(w["W2"]).T + w["b2"]
+    assert np.max(np.abs(z2 - z2_k)) <= 1e-5 * (1.0 + np.max(np.abs(z2_k)))
+    ym, ys = norm[20:22].astype(np.float64), norm[22:24].astype(np.float64)
+    y_k = (h2 @ C.bf16(w["W3"]).T + w["b3"]) * ys + ym
+    assert np.max(np.abs(y - y_k)) <= 1e-5 * (1.0 + np.max(np.abs(y_k)))
+    # end to end against the all-FP64 forward
+    err_z2 = np.linalg.norm(z2 - ref["z2"]) / np.linalg.norm(ref["z2"])
+    err_y = np.linalg.norm(y - ref["y"]) / np.linalg.norm(ref["y"] - ym)
+    print(f"forward: z2 norm-wise {err_z2:.2e}, y norm-wise {err_y:.2e}")
+    assert err_z2 <= 1e-3 and err_y <= 1e-3
 
 
 def test_gradient_matches_fp64(C):
@@ -48,13 +69,19 @@ def test_gradient_matches_fp64(C):
     net = C.MLP(p, norm)
     loss, g = net.loss_grad(x, t)
     rloss, rg = C.reference_loss_grad(p, norm, x, t)
-    assert abs(loss - rloss) <= 1e-3 * abs(rloss)
+    assert abs(loss - rloss) <= 1e-4 * abs(rloss)
     k = 0
+    errs = {}
     for name, shape in C.SHAPES:
         nk = int(np.prod(shape))
         a, b = g[k:k + nk].astype(np.float64), rg[k:k + nk]
-        assert np.linalg.norm(a - b) <= 2e-2 * np.linalg.norm(b) + 1e-7, name
+        errs[name] = float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
         k += nk
+    print("gradient norm-wise errors:", {n: f"{e:.2e}" for n, e in errs.items()})
+    # the backward layers differ from FP64 only by the hardware tanh in GELU' and the BF16
+    # roundings of dZ2, dZ1 that it flips
+    for name, e in errs.items():
+        assert e <= 1e-3, (name, e)
 
 
 def test_training_reduces_loss_and_is_deterministic(C):
