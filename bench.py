@@ -246,7 +246,7 @@ def _measured_peak():
 
 
 def _traffic_per_step():
-    p = os.path.join(ROOT, "profiles", "sp_step_traffic_gaussian_bumps_4M.json")
+    p = os.path.join(ROOT, "profiles", "sp_step_traffic_gaussian_bumps_1M.json")
     if os.path.exists(p):
         try:
             return json.load(open(p))
