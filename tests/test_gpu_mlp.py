@@ -43,12 +43,14 @@ def test_forward_matches_fp64(C):
     z1, h1, z2, h2 = (lay[k].astype(np.float64) for k in range(4))
     # first GEMM + bias: exact products of BF16 operands summed in FP32
     assert np.max(np.abs(z1 - ref["z1"])) <= 1e-5 * (1.0 + np.max(np.abs(ref["z1"])))
-    # activations: one BF16 unit at most from the FP64 GELU of the kernel's own pre-activations
+    # activations against the FP64 GELU of the kernel's own pre-activations: the hardware tanh's
+    # error (about 2^-11 relative to tanh) moves 0.5 z (1 + t) by up to 0.5 |z| 2^-11, which for
+    # very negative z is large next to the activation itself; beyond that, one BF16 unit
     for z, h in ((z1, h1), (z2, h2)):
         g = C.bf16(C.gelu(z))
-        ulp = np.maximum(np.abs(g), 1e-30) * 2.0 ** -7
-        assert np.all(np.abs(h - g) <= ulp + 1e-30)
-        assert np.mean(h == g) >= 0.99
+        tol = np.abs(g) * 2.0 ** -7 + np.abs(z) * 2.0 ** -11
+        assert np.all(np.abs(h - g) <= tol)
+        assert np.mean(h == g) >= 0.95
     # second and third GEMMs on the kernel's activations
     z2_k = h1 @ C.bf16(w["W2"]).T + w["b2"]
     assert np.max(np.abs(z2 - z2_k)) <= 1e-5 * (1.0 + np.max(np.abs(z2_k)))
