@@ -872,50 +872,17 @@ __global__ void __launch_bounds__(128) k_update_closure(DevMesh m, ClosureArgs a
                     make_uint4(pk[0], pk[1], pk[2], pk[3]);
             }
         }
-        // layer 1: one MMA of K = 16
+        // the network runs only for tiles with a cell inside the training hull (or while the
+        // closure's inputs and outputs are recorded): elsewhere its outputs are not used
         fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            fence_after_sync();
-            mma_bf16(tmem, smem_desc(aX, kInPad), smem_desc(aW1, kInPad), id64, 0u);
-            mma_commit(&bar);
-        }
-        if (!mbar_wait(&bar, phase, kWaitPolls)) {
-            ok = false;
-            mbar_wait(&bar, phase, kWaitPolls);
-        }
-        phase ^= 1u;
-        fence_after_sync();
-        // the hidden layers' epilogues, each followed by the next layer's four MMAs of K = 16
-        for (int layer = 0; layer < 2; layer++) {
-            const float* bias = layer == 0 ? sb1 : sb2;
-            for (int c0 = 0; c0 < kHid; c0 += 16) {
-                uint32_t v[16];
-                tmem_ld16(lane_base + (uint32_t)c0, v);
-                tmem_wait_ld();
-                uint32_t hv[8];  // bf16 pairs
-                for (int j = 0; j < 8; j++) {
-                    float g0, g1;
-                    gelu_bias2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]), bias[c0 + 2 * j],
-                               bias[c0 + 2 * j + 1], g0, g1);
-                    const __nv_bfloat162 pr = __floats2bfloat162_rn(g0, g1);
-                    hv[j] = *reinterpret_cast<const uint32_t*>(&pr);
-                }
-                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0, kHid)) =
-                    make_uint4(hv[0], hv[1], hv[2], hv[3]);
-                *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0 + 8, kHid)) =
-                    make_uint4(hv[4], hv[5], hv[6], hv[7]);
-            }
-            fence_before_sync();
-            fence_proxy_async();
-            __syncthreads();
+        const bool net = __syncthreads_or((int)(valid && in)) != 0 || a.rec != nullptr;
+        uint32_t v[16];
+        for (int j = 0; j < 16; j++) v[j] = 0u;
+        if (net) {
+            // layer 1: one MMA of K = 16
             if (tid == 0) {
                 fence_after_sync();
-                const uint32_t bw = layer == 0 ? aW2 : aW3;
-                const uint32_t id = layer == 0 ? id64 : id16;
-                for (int s2 = 0; s2 < kHid / 16; s2++)
-                    mma_bf16(tmem, smem_desc(aH + 256u * s2, kHid), smem_desc(bw + 256u * s2, kHid), id,
-                             s2 > 0 ? 1u : 0u);
+                mma_bf16(tmem, smem_desc(aX, kInPad), smem_desc(aW1, kInPad), id64, 0u);
                 mma_commit(&bar);
             }
             if (!mbar_wait(&bar, phase, kWaitPolls)) {
@@ -924,10 +891,48 @@ __global__ void __launch_bounds__(128) k_update_closure(DevMesh m, ClosureArgs a
             }
             phase ^= 1u;
             fence_after_sync();
+            // the hidden layers' epilogues, each followed by the next layer's four MMAs of K = 16
+            for (int layer = 0; layer < 2; layer++) {
+                const float* bias = layer == 0 ? sb1 : sb2;
+                for (int c0 = 0; c0 < kHid; c0 += 16) {
+                    uint32_t v[16];
+                    tmem_ld16(lane_base + (uint32_t)c0, v);
+                    tmem_wait_ld();
+                    uint32_t hv[8];  // bf16 pairs
+                    for (int j = 0; j < 8; j++) {
+                        float g0, g1;
+                        gelu_bias2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]), bias[c0 + 2 * j],
+                                   bias[c0 + 2 * j + 1], g0, g1);
+                        const __nv_bfloat162 pr = __floats2bfloat162_rn(g0, g1);
+                        hv[j] = *reinterpret_cast<const uint32_t*>(&pr);
+                    }
+                    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0, kHid)) =
+                        make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sH) + core_offset(tid, c0 + 8, kHid)) =
+                        make_uint4(hv[4], hv[5], hv[6], hv[7]);
+                }
+                fence_before_sync();
+                fence_proxy_async();
+                __syncthreads();
+                if (tid == 0) {
+                    fence_after_sync();
+                    const uint32_t bw = layer == 0 ? aW2 : aW3;
+                    const uint32_t id = layer == 0 ? id64 : id16;
+                    for (int s2 = 0; s2 < kHid / 16; s2++)
+                        mma_bf16(tmem, smem_desc(aH + 256u * s2, kHid), smem_desc(bw + 256u * s2, kHid), id,
+                                 s2 > 0 ? 1u : 0u);
+                    mma_commit(&bar);
+                }
+                if (!mbar_wait(&bar, phase, kWaitPolls)) {
+                    ok = false;
+                    mbar_wait(&bar, phase, kWaitPolls);
+                }
+                phase ^= 1u;
+                fence_after_sync();
+            }
+            tmem_ld16(lane_base, v);
+            tmem_wait_ld();
         }
-        uint32_t v[16];
-        tmem_ld16(lane_base, v);
-        tmem_wait_ld();
         if (valid && ok) {
             // the network's outputs in physical units, as sw2d_mlp_infer gives them
             const float y0 = (__uint_as_float(v[0]) + sb3[0]) * cn.ystd[0] + cn.ymean[0];
