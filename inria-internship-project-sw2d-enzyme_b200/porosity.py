@@ -374,7 +374,7 @@ class SpE:
         trajectory at phi_map against these maps then gives J = 0 up to their printed digits."""
         times = self.observation_grid()
         n = self.n
-        self.set_frames(times, np.zeros((times.size, n)))
+        self.set_frames(times, np.zeros((times.size, 3, n)))
         m = np.ascontiguousarray(phi_map, dtype=np.float64)
         self.model.assim_record(m, stride or self.cfg.checkpoint_stride)
         h, q, r, landed = self.model.assim_trigger_states(m, times.size)
