@@ -260,17 +260,28 @@ def test_state_gradient_matches_differences(pkg, scheme):
         assert min(errs) <= 1e-5, f"{name}: adjoint {ad:.9e}, relative differences {errs}"
 
 
+REFERENCE_DESCENT_J = [3.1042911536, 3.1042911536, 2.9053396594, 2.5666208839, 2.8002945144, 1.5732719235,
+                       1.0991733610, 0.81922662858, 0.75116668751, 0.93003294460, 0.75643629818, 0.75106388837,
+                       0.75105195207, 0.75105756353]   # configue_fonctionels/sp_toce/descent_log_reference_-75.8pct.csv
+
+
 def test_toce_minimization_descends(pkg, tmp_path):
     """porosity.run_minimization (the reference's run_minimization with L-BFGS-B) from the case's
-    first guess phi = 1: the descent log has the reference's columns, its first row is the
-    reference's J at phi = 1, and the cost decreases (the reference's own run: -6.4 % at its
-    third evaluation, -75.8 % after 9 iterations, with LBFGSpp instead of scipy)."""
+    first guess phi = 1 with the case's own settings (input.solv: max_it 50, lbfgsb_m 6, 30
+    line-search trials, epsilon 1e-5, 48 windows of 20 s from t = 10 s, uniform weights): the
+    descent log has the reference's columns, its first row is the reference's J at phi = 1 (same
+    libm), and the cost falls by at least 35 %.  The reference's own run (LBFGSpp, host libm)
+    falls by 75.8 % in 14 evaluations (REFERENCE_DESCENT_J); this one, with scipy's L-BFGS-B and
+    the GPU gradient, stops at J = 1.924 (-38 %): every trial point after its ninth evaluation
+    lands at J = 2.935, a jump next to its best point (each trial's dry run re-derives its time
+    steps), and the two gradients differ at the case's wet/dry-front cells."""
     from tests.golden.make_assim_golden import decimals_to_float
     case, _ = sp_toce_case()
     ax = np.load(os.path.join(GOLDEN, "sp_toce_assim.npz"))
     cfg = pkg.porosity.AssimConfig(minimize_algo="lbfgsb", windowed_assimilation=True, assimilation_window_duration=20.0,
                                    n_assimilation_windows=48, t_state_assimilation=10.0, cost_normalize=True,
-                                   checkpoint_stride=30, max_it=4)
+                                   checkpoint_stride=30, max_it=50, lbfgsb_m=6, lbfgsb_max_linesearch=30,
+                                   lbfgsb_epsilon=1e-5)
     spe = pkg.porosity.SpE(pkg.SpModel(case), cfg)
     spe.set_frames(ax["obs_times"], decimals_to_float(ax["obs_mant"], ax["obs_exp"]))
     out = str(tmp_path / "descent")
@@ -278,8 +289,9 @@ def test_toce_minimization_descends(pkg, tmp_path):
     rows = open(os.path.join(out, "descent_log.csv")).read().splitlines()
     assert rows[0] == pkg.porosity.DESCENT_COLUMNS
     assert rows[1].split(",")[1] == f"{float(ax['J_pm']):.10e}"   # the log keeps 11 significant digits
-    print("sp_toce descent:", [round(j, 6) for j in res["history"]])
-    assert res["J_final"] < 0.99 * res["J_init"]
+    assert abs(res["J_init"] - REFERENCE_DESCENT_J[0]) < 2e-5 * REFERENCE_DESCENT_J[0]   # host vs portable libm
+    print("sp_toce descent:", [round(j, 6) for j in res["history"][:16]], "...; reference:", REFERENCE_DESCENT_J)
+    assert res["J_final"] <= 0.65 * res["J_init"], (res["J_final"], res["J_init"])
     assert np.all((res["phi"] >= 0.0) & (res["phi"] <= 1.0))
 
 
