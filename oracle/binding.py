@@ -253,6 +253,10 @@ class RefE:
         lib.sw2dref_e_time.argtypes = [_P]
         lib.sw2dref_e_time.restype = ctypes.c_double
         lib.sw2dref_e_close.argtypes = [_P]
+        lib.sw2dref_e_folder.argtypes = [_P]
+        lib.sw2dref_e_folder.restype = ctypes.c_char_p
+        lib.sw2dref_e_generate_references.argtypes = [_P, _D, L, ctypes.c_int]
+        lib.sw2dref_e_generate_references.restype = L
         self.lib = lib
         self.h = lib.sw2dref_e_open(folder.encode(), 1 if quiet else 0)
         if not self.h:
@@ -263,6 +267,16 @@ class RefE:
     CONFIG = ("checkpoint_stride", "windowed", "window_duration", "window_steps", "n_windows",
               "t_state_assimilation", "cost_normalize", "phi_transform", "lambda_tanh", "dt_map_ad",
               "mask_wall_gradient", "alpha_reg", "t_0", "t_max")
+
+    def generate_references(self, phi, stride: int, quiet: bool = True):
+        """The reference's gen-ref-e mode (generate_references_E) at porosity phi: the maps it
+        writes (into this handle's temporary folder), sorted by name."""
+        n = self.lib.sw2dref_e_generate_references(self.h, np.ascontiguousarray(phi, dtype=np.float64), int(stride),
+                                                   1 if quiet else 0)
+        if n < 0:
+            raise RuntimeError("the reference's generate_references_E failed")
+        folder = os.path.join(self.lib.sw2dref_e_folder(self.h).decode(), "reference")
+        return sorted(os.path.join(folder, f) for f in os.listdir(folder) if f.startswith("ResultHydro_p"))
 
     def config(self) -> dict:
         out = np.zeros(len(self.CONFIG))

@@ -26,6 +26,10 @@
 //   sw2dref_e_set_window(...)          the assimilation window and tiles (restated below from
 //                                      get_spatial_gradient_checkpointed, which cannot run)
 //   sw2dref_e_replay_cost(m)           replay_trajectory_cost (leaves the replayed end state)
+//   sw2dref_e_generate_references(m)   the gen-ref-e mode, generate_references_E
+//                                      (assim/swSpE_checkpoint.cpp:470-515), writing its maps
+//                                      into the handle's own temporary folder
+//                                      (sw2dref_e_folder(h)/reference), never the case's
 #include <unistd.h>
 
 #include <cstdlib>
@@ -434,6 +438,26 @@ void sw2dref_e_get_state(void* h, double* hh, double* q, double* r)
 }
 
 double sw2dref_e_time(void* h) { return static_cast<HandleE*>(h)->m->t; }
+
+const char* sw2dref_e_folder(void* h) { return static_cast<HandleE*>(h)->tmp.c_str(); }
+
+// The reference's gen-ref-e mode on phi_map.  Its begin_reference_generation empties and
+// recreates <case>/reference: the temporary folder's `reference` entry, a link to the case's own
+// folder for load_observations, is first replaced by an empty directory of its own.  Returns the
+// number of maps written, or -1.
+long sw2dref_e_generate_references(void* h, const double* phi_map, long stride, int quiet)
+{
+    QuietOut qo(quiet != 0);
+    HandleE* hd = static_cast<HandleE*>(h);
+    const fs::path ref = fs::path(hd->tmp) / "reference";
+    std::error_code ec;
+    if (fs::is_symlink(fs::symlink_status(ref, ec))) fs::remove(ref, ec);
+    if (fs::exists(fs::symlink_status(ref, ec)) && fs::is_symlink(fs::symlink_status(ref, ec))) return -1;
+    fs::create_directories(ref, ec);
+    std::vector<double> mm(phi_map, phi_map + hd->m->cell_nb);
+    if (!hd->m->generate_references_E(mm.data(), (size_t)stride)) return -1;
+    return (long)hd->m->n_ref_written;
+}
 
 void sw2dref_e_close(void* h)
 {

@@ -9,10 +9,12 @@ Bars:
   flag libm_stable; the wetting/drying channel cases move by 1e-6..1e-1 when only the
   reference's libm changes, which no implementation can undercut).
 """
+import os
+
 import numpy as np
 import pytest
 
-from tests.conftest import assert_state_close, golden_case, golden_names, load_pkg, sp_toce_case
+from tests.conftest import GOLDEN, assert_state_close, golden_case, golden_names, load_pkg, sp_toce_case
 
 pytestmark = pytest.mark.gpu
 
@@ -202,28 +204,43 @@ def test_gpu_c1_dam_break_delaunay_1000_steps(pkg, tmp_path, friction):
     assert got[0].min() >= 0.0 and np.all(np.isfinite(got[0]))
 
 
-@pytest.mark.parametrize("n_cells,steps", [(1_000_000, 200), (4_000_000, 200)])
-def test_gpu_c2_moving_bumps_vs_oracle(pkg, n_cells, steps):
+@pytest.mark.parametrize("n_cells", [1_000_000, 4_000_000])
+def test_gpu_c2_moving_bumps_vs_oracle(pkg, n_cells):
     """The large SP forward solve's bed under a dam break (free surface 5.0 m for x < 1 km, 3.5 m
     beyond, at rest): a moving, mostly wet flow with wet/dry fronts around the bumps, on the
-    jittered-Delaunay mesh, `steps` steps bit for bit against the CPU oracle, with the stored
-    volume sum(phi A h) conserved to round-off (closed basin)."""
+    jittered-Delaunay mesh, 200 steps bit for bit against the CPU oracle.  The oracle takes
+    minutes at these sizes, so tests/golden/make_c2_digest.py ran it once and kept the SHA-256 of
+    its final (h, q, r) bits, its t and dt, and a digest of the inputs (which this test checks
+    first).  The stored volume sum(phi A h) of the closed basin changes only by round-off and by
+    the reference's negative-depth clamp at the wet/dry fronts (h < 0 -> 0, swSpHyp.cpp:197-209)."""
+    import hashlib
+    import json
+    fx = json.load(open(os.path.join(GOLDEN, "c2_moving_digest.json")))[str(n_cells)]
     case = pkg.workloads.gaussian_bumps(n_cells=n_cells, mesh="delaunay", initial="dam")
+    m = case.mesh
+    d = hashlib.sha256()
+    for a in (m.cell_x, m.cell_y, m.cell_z_b, m.cell_area, m.edge_int_cells, m.edge_int_nx, m.edge_int_ny,
+              m.edge_int_length, m.edge_bnd_cell, case.h0, case.q0, case.r0, case.phi, case.friction):
+        d.update(np.ascontiguousarray(a).tobytes())
+    assert d.hexdigest() == fx["inputs_sha256"], "the case's inputs are not the ones the oracle ran"
     model = pkg.SpModel(case)
     w = case.phi * case.mesh.cell_area
     h0 = model.state()[0]
     wet0 = float(np.mean(h0 > 1e-5))
     assert wet0 > 0.75, f"the moving case should be mostly wet ({wet0:.2f})"
     v0 = float(np.sum(w * h0))
+    steps = int(fx["steps"])
     assert model.step(steps) == steps
     got = model.state()
-    o = oracle_binding.SpOracle(case, portable_math=True)
-    assert o.step(steps) == steps
-    assert model.time == (o.t, o.dt)
-    assert_state_close(got, o.state(), True, f"moving bumps {n_cells} cells, {steps} steps")
+    assert model.time == (float(fx["t"]), float(fx["dt"]))
+    d = hashlib.sha256()
+    for a in got:
+        d.update(np.ascontiguousarray(a, np.float64).tobytes())
+    assert d.hexdigest() == fx["state_sha256"], f"moving bumps {n_cells} cells: state bits differ from the oracle's"
     moved = float(np.mean(np.abs(got[1]) + np.abs(got[2]) > 1e-6))
     # the dam line at x = 1 km: after 200 steps (about 10 s) the bores have run about 70 m each way
     # over the 2 km basin, so a band of about 1.5 % of the cells moves
     assert moved > 0.01, f"the flow should be moving ({moved:.3f} of the cells)"
     v1 = float(np.sum(w * got[0]))
-    assert abs(v1 - v0) / v0 < 1e-11, f"stored volume drifted by {abs(v1 - v0) / v0:.2e}"
+    # measured 2.1e-9 (1M cells) and 1.2e-10 (4M cells) relative, the oracle's bits included
+    assert abs(v1 - v0) / v0 < 1e-8, f"stored volume drifted by {abs(v1 - v0) / v0:.2e}"

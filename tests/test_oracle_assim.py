@@ -62,3 +62,32 @@ def test_fixture_matches_reference():
     assert J == float(ax["J_pm"])
     # the portable libm moves this chaotic run's cost by a few 1e-6 relative
     assert abs(J - DESCENT_LOG_J_INIT) / DESCENT_LOG_J_INIT < 2e-5
+
+
+def test_reference_gen_ref_e_reproduces_the_shipped_maps():
+    """The reference's gen-ref-e mode (generate_references_E) at the case's porosity_ref_map,
+    linked with the host libm, writes the case's shipped reference/ResultHydro_p*.txt digit for
+    digit: those maps are this mode's output.  Linked with the portable exp/log/cbrt instead, it
+    gives the maps whose digests tests/golden/sp_toce_genref_pm.json keeps (the GPU's _E step
+    uses the portable functions and is compared with those, tests/test_gpu_assim.py)."""
+    import glob
+    from tests.golden.make_assim_golden import frames_as_decimals
+    from tests.golden.make_genref_digest import frame_digests
+    shipped = sorted(glob.glob(os.path.join(CASE, "reference", "ResultHydro_p*.txt")))
+    ms, es = frames_as_decimals(shipped)
+    fx = json.load(open(os.path.join(GOLDEN, "sp_toce_genref_pm.json")))
+    for pm in (False, True):
+        ref = _ref(pm)
+        try:
+            phi = ref.load_phi_map(os.path.join(CASE, "input", "SP_cell_porosity_map.txt"))
+            files = ref.generate_references(phi, int(ref.config()["checkpoint_stride"]))
+            assert [os.path.basename(f) for f in files] == [os.path.basename(f) for f in shipped]
+            if pm:
+                assert frame_digests(files) == fx["sha256"]
+                assert [os.path.basename(f) for f in files] == fx["names"]
+            else:
+                mant, expo = frames_as_decimals(files)
+                same = (mant == ms) & ((expo == es) | (mant == 0))
+                assert same.all(), f"{np.count_nonzero(~same)} printed values differ from the shipped maps"
+        finally:
+            ref.close()
