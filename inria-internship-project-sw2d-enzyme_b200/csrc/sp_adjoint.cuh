@@ -86,15 +86,16 @@ SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, do
     const double c = sqrt(kGravity * hr);
     const double X = (b - 1.0) * b * u * u + c * c;
     const double root = sqrt(X);
-    // reverse
+    // reverse (the derivative terms multiply by the reciprocals of the two denominators)
+    const double rd2 = 1.0 / d2, rhd = 1.0 / hd;
     const double bu_bar = sb.lm + sb.lp;
     const double root_bar = sb.lp - sb.lm;
     const double X_bar = dsqrt_bar(root, root_bar);
     const double u_bar = bu_bar * b + X_bar * (b - 1.0) * b * 2.0 * u;
     const double c_bar = X_bar * 2.0 * c;
     double hr_bar = dsqrt_bar(c, c_bar) * kGravity;
-    const double sq_bar = sb.q + u_bar / d2;
-    if (!(hr < kSmallReal)) hr_bar += -u_bar * u / d2;
+    const double sq_bar = sb.q + u_bar * rd2;
+    if (!(hr < kSmallReal)) hr_bar += -u_bar * u * rd2;
     hr_bar += sb.z;                               // z = hr + z_b
     double zb_bar = sb.z;
     hr_bar += sq_bar * ul;
@@ -126,9 +127,9 @@ SW2D_HD void evr_side_rev(bool left, double h, double q, double r, double zb, do
     const double X1_bar = dsqrt_bar(root1, root1_bar);
     ul_bar += X1_bar * (b - 1.0) * b * 2.0 * ul;
     const double cl_bar = X1_bar * 2.0 * cl;
-    const double ql_bar = ul_bar / hd;
-    const double rl_bar = vl_bar / hd;
-    double hd_bar = -ul_bar * ul / hd - vl_bar * vl / hd + dsqrt_bar(cl, cl_bar) * kGravity;
+    const double ql_bar = ul_bar * rhd;
+    const double rl_bar = vl_bar * rhd;
+    double hd_bar = -ul_bar * ul * rhd - vl_bar * vl * rhd + dsqrt_bar(cl, cl_bar) * kGravity;
     if (kSmallReal < h) cb.h += hd_bar;
     cb.q += ql_bar * nx - rl_bar * ny;
     cb.r += ql_bar * ny + rl_bar * nx;
@@ -215,23 +216,25 @@ SW2D_HD void hllc_rev(bool blending, double bL, double bR, double phiL, double p
         const double f2 = N2 / den;
         const double dvL = smax(hL, kSmallReal), dvR = smax(hR, kSmallReal);
         const double vL = L.r / dvL, vR = R.r / dvR;
-        // ---- reverse
+        // ---- reverse.  The derivative terms divide by the reciprocal of each denominator, taken
+        // once (the forward values above, which decide the branches, keep the forward's divisions)
+        const double rden = 1.0 / den, rdvL = 1.0 / dvL, rdvR = 1.0 / dvR, rduL = 1.0 / duL, rduR = 1.0 / duR;
         double f1_bar = fb.f1, L1_bar = 0, L2_bar = 0, den_bar = 0;
         double Lq_bar = 0, Rq_bar = 0, Lz_bar = 0, Rz_bar = 0, Lr_bar = 0, Rr_bar = 0;
         double uL_bar = 0, uR_bar = 0;
         if (f1 >= 0) {
             f1_bar += fb.f3 * bL * vL;
             const double vL_bar = fb.f3 * bL * f1;
-            Lr_bar += vL_bar / dvL;
-            if (!(hL < kSmallReal)) hL_bar += -vL_bar * vL / dvL;
+            Lr_bar += vL_bar * rdvL;
+            if (!(hL < kSmallReal)) hL_bar += -vL_bar * vL * rdvL;
         } else {
             f1_bar += fb.f3 * bR * vR;
             const double vR_bar = fb.f3 * bR * f1;
-            Rr_bar += vR_bar / dvR;
-            if (!(hR < kSmallReal)) hR_bar += -vR_bar * vR / dvR;
+            Rr_bar += vR_bar * rdvR;
+            if (!(hR < kSmallReal)) hR_bar += -vR_bar * vR * rdvR;
         }
-        const double N2_bar = fb.f2 / den;
-        den_bar += -fb.f2 * f2 / den;
+        const double N2_bar = fb.f2 * rden;
+        den_bar += -fb.f2 * f2 * rden;
         L2_bar += N2_bar * (FL + sl) + N2_bar * L1 * P;
         const double FL_bar = N2_bar * L2;
         double sl_bar = fb.sl + N2_bar * L2;
@@ -248,8 +251,8 @@ SW2D_HD void hllc_rev(bool blending, double bL, double bR, double phiL, double p
         L1_bar += -sl_bar * s2;
         double s2_bar = -sl_bar * L1 + sr_bar * L2;
         L2_bar += sr_bar * s2;
-        const double s2a_bar = s2_bar * kGravity / den;
-        den_bar += -s2_bar * s2 / den;
+        const double s2a_bar = s2_bar * kGravity * rden;
+        den_bar += -s2_bar * s2 * rden;
         double fact_bar = 0.0, alpha_bar = 0.0;
         if (blending) {
             alpha_bar += s2a_bar * (s2h - s2z);
@@ -272,8 +275,8 @@ SW2D_HD void hllc_rev(bool blending, double bL, double bR, double phiL, double p
             // f1 = alpha F1h + (1 - alpha) F1z
             alpha_bar += f1_bar * (F1h - F1z);
             const double F1h_bar = f1_bar * alpha, F1z_bar = f1_bar * (1.0 - alpha);
-            const double Nh_bar = F1h_bar * phiLR / den, Nz_bar = F1z_bar * phiLR / den;
-            den_bar += -F1h_bar * F1h / den - F1z_bar * F1z / den;
+            const double Nh_bar = F1h_bar * phiLR * rden, Nz_bar = F1z_bar * phiLR * rden;
+            den_bar += -F1h_bar * F1h * rden - F1z_bar * F1z * rden;
             const double Ns_bar = Nh_bar + Nz_bar;  // the shared part L2 qL - L1 qR
             L2_bar += Ns_bar * L.q + Nh_bar * L1 * (hR - hL) + Nz_bar * L1 * (R.z - L.z);
             L1_bar += -Ns_bar * R.q + Nh_bar * L2 * (hR - hL) + Nz_bar * L2 * (R.z - L.z);
@@ -297,8 +300,8 @@ SW2D_HD void hllc_rev(bool blending, double bL, double bR, double phiL, double p
             fact_bar += s2a_bar * (L.z - R.z);
             Lz_bar += s2a_bar * fact;
             Rz_bar -= s2a_bar * fact;
-            const double N1_bar = f1_bar * phiLR / den;
-            den_bar += -f1_bar * f1 / den;
+            const double N1_bar = f1_bar * phiLR * rden;
+            den_bar += -f1_bar * f1 * rden;
             L2_bar += N1_bar * (L.q + L1 * (R.z - L.z));
             L1_bar += N1_bar * (-R.q + L2 * (R.z - L.z));
             Lq_bar += N1_bar * L2;
@@ -323,10 +326,10 @@ SW2D_HD void hllc_rev(bool blending, double bL, double bR, double phiL, double p
         } else {
             Lb.lp += L2_bar;
         }
-        Lq_bar += uL_bar / duL;
-        if (duL_h) hL_bar += -uL_bar * uL / duL;
-        Rq_bar += uR_bar / duR;
-        if (duR_h) hR_bar += -uR_bar * uR / duR;
+        Lq_bar += uL_bar * rduL;
+        if (duL_h) hL_bar += -uL_bar * uL * rduL;
+        Rq_bar += uR_bar * rduR;
+        if (duR_h) hR_bar += -uR_bar * uR * rduR;
         Lb.q += Lq_bar;
         Rb.q += Rq_bar;
         Lb.r += Lr_bar;
