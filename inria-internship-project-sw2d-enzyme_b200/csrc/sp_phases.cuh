@@ -202,12 +202,15 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
     const double lm = max4(fabs(SL.lm), fabs(SL.lp), fabs(SR.lm), fabs(SR.lp));
     if (m.lmax) m.lmax[e] = lm;
     if (m.rstate) {
-        double2* p = m.rstate + 5 * (size_t)e;
+        // five planes of ni double2 each, so that a warp's stores and the reverse's loads are
+        // contiguous
+        const size_t ni = (size_t)m.ni;
+        double2* p = m.rstate + e;
         p[0] = make_double2(SL.z, SL.q);
-        p[1] = make_double2(SL.r, SL.lm);
-        p[2] = make_double2(SL.lp, SR.z);
-        p[3] = make_double2(SR.q, SR.r);
-        p[4] = make_double2(SR.lm, SR.lp);
+        p[ni] = make_double2(SL.r, SL.lm);
+        p[2 * ni] = make_double2(SL.lp, SR.z);
+        p[3 * ni] = make_double2(SR.q, SR.r);
+        p[4 * ni] = make_double2(SR.lm, SR.lp);
     }
     const double lw = lm * ld(&m.len[e]);
     const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;

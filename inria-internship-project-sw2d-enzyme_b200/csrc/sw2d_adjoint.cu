@@ -70,6 +70,7 @@ struct AdjointState {
     double4* seg_bal = nullptr;          // every * nc
     double2* seg_slope = nullptr;        // every * nc: each step's MUSCL-EVR slopes
     double2* seg_rs = nullptr;           // every * ni * 5: each step's Riemann states (when memory allows)
+    double2* eside = nullptr;            // 3 * ni: {z_b}, {b}, {phi} of each internal edge's (L, R) cells
     // adjoint buffers
     double4* lam = nullptr;              // nc: adjoint of the state {h, q, r, -}
     double4* sig = nullptr;              // nslot: adjoint of the balance slots {a, b, c, -}
@@ -151,6 +152,20 @@ __global__ void k_sample(const double4* __restrict__ st, const int* __restrict__
 // reverse kernels
 // ------------------------------------------------------------------------------------------
 
+// The side table of k_edges_rev: per internal edge, {z_b}, {b}, {phi} of its (L, R) cells, in
+// three planes of ni double2 (rebuilt at each reverse sweep from the current cell constants)
+__global__ void k_edge_sides(DevMesh m, double2* eside)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.ni) return;
+    const size_t ni = (size_t)m.ni;
+    const int2 lr = ld(&m.lr[e]);
+    const double4 ca = ld(&m.cst[lr.x]), cb = ld(&m.cst[lr.y]);
+    eside[e] = make_double2(ca.x, cb.x);
+    eside[ni + e] = make_double2(ca.y, cb.y);
+    eside[2 * ni + e] = make_double2(ca.z, cb.z);
+}
+
 // Reverse of k_update for one step: lam holds the adjoint of the state after the step and
 // becomes the adjoint of the state before it (balance part); the slots' adjoints gain
 // dt * (adjoint of the post-balance state); friction-coefficient gradients accumulate.
@@ -227,23 +242,64 @@ __device__ __forceinline__ void slot_rev(const SlotFactors& f, const double4& s,
     Sb += f.f2S2 * s.y + f.f3S2 * s.z;
 }
 
+// Loads issued where they stand: a volatile asm is neither sunk below the dry-edge test nor
+// reordered against the other volatile asms, so every load of an edge is in flight before the
+// first one is used.  ld_now reads data no kernel writes meanwhile; the slot adjoints, which
+// this kernel resets after reading, go through ld_sig / st_sig (coherent path).
+__device__ __forceinline__ double2 ld_now(const double2* p)
+{
+    double2 v;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int2 ld_now(const int2* p)
+{
+    int2 v;
+    asm volatile("ld.global.nc.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double4 ld_sig(const double4* p)
+{
+    double4 v;
+    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    asm volatile("ld.global.f64 %0, [%1+16];" : "=d"(v.z) : "l"(p));
+    v.w = 0.0;
+    return v;
+}
+__device__ __forceinline__ void st_sig_zero(double4* p)
+{
+    asm volatile("st.global.v2.f64 [%0], {%1, %2};\n\tst.global.v2.f64 [%0+16], {%1, %2};" ::"l"(p), "d"(0.0),
+                 "d"(0.0));
+}
+
 // kStored: the two Riemann states of the step come from the segment's forward recompute
-// (rs, 5 x double2 per edge) instead of being rebuilt here
+// (rs, 5 planes of ni double2) and the constants of the two cells from the side table (eside,
+// 3 planes of ni double2: {z_b}, {b}, {phi} of (L, R)), so that no load of an internal edge
+// depends on another one but the two slot adjoints (on the edge's slots); otherwise the states
+// are rebuilt here from the cells.
 template <int kScheme, bool kBlending, int kB, int kMinB, bool kStored>
 __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig, double4* ctb, double2* cts, double t,
-                                                         double dtp, const double2* __restrict__ rs)
+                                                         double dtp, const double2* __restrict__ rs,
+                                                         const double2* __restrict__ eside)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m.ni) {
         const int e = i;
-        const int2 lr = ld(&m.lr[e]);
-        const int a = lr.x, b = lr.y;
-        const double2 n = ld(&m.nxy[e]);
-        const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
         SideState SL, SR;
+        double zbL, zbR, bL, bR, phL, phR;
+        int2 sl;
+        double2 n, cf;
+        double4 sa, sb;
         if (kStored) {
-            const double2* p = rs + 5 * (size_t)e;
-            const double2 r0 = ld(p), r1 = ld(p + 1), r2 = ld(p + 2), r3 = ld(p + 3), r4 = ld(p + 4);
+            const size_t ni = (size_t)m.ni;
+            sl = ld_now(&m.eslot[e]);
+            const double2 r0 = ld_now(rs + e), r1 = ld_now(rs + ni + e), r2 = ld_now(rs + 2 * ni + e);
+            const double2 r3 = ld_now(rs + 3 * ni + e), r4 = ld_now(rs + 4 * ni + e);
+            const double2 z = ld_now(eside + e), bb = ld_now(eside + ni + e), ph = ld_now(eside + 2 * ni + e);
+            n = ld_now(&m.nxy[e]);
+            cf = ld_now(&m.coef[e]);
+            sa = ld_sig(&sig[sl.x]);
+            sb = ld_sig(&sig[sl.y]);
             SL.z = r0.x;
             SL.q = r0.y;
             SL.r = r1.x;
@@ -254,19 +310,36 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig
             SR.r = r3.y;
             SR.lm = r4.x;
             SR.lp = r4.y;
-        } else if (kScheme == SW2D_SCHEME_GODUNOV) {
-            const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
-            SL = godunov_side(sa.x, sa.y, sa.z, ca.x, ca.y, n.x, n.y);
-            SR = godunov_side(sb.x, sb.y, sb.z, cb.x, cb.y, n.x, n.y);
+            zbL = z.x;
+            zbR = z.y;
+            bL = bb.x;
+            bR = bb.y;
+            phL = ph.x;
+            phR = ph.y;
         } else {
-            const double4 sa = ld(&m.st[a]), sb = ld(&m.st[b]);
-            const double4 d = ld(&m.emc[e]);
-            const double2 ga = m.slope[a], gb = m.slope[b];
-            SL = evr_side(true, sa.x, sa.y, sa.z, ca.x, ca.y, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp, m.dry);
-            SR = evr_side(false, sb.x, sb.y, sb.z, cb.x, cb.y, sb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp, m.dry);
+            const int2 lr = ld(&m.lr[e]);
+            const int a = lr.x, b = lr.y;
+            n = ld(&m.nxy[e]);
+            sl = ld(&m.eslot[e]);
+            const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
+            const double4 qa = ld(&m.st[a]), qb = ld(&m.st[b]);
+            if (kScheme == SW2D_SCHEME_GODUNOV) {
+                SL = godunov_side(qa.x, qa.y, qa.z, ca.x, ca.y, n.x, n.y);
+                SR = godunov_side(qb.x, qb.y, qb.z, cb.x, cb.y, n.x, n.y);
+            } else {
+                const double4 d = ld(&m.emc[e]);
+                const double2 ga = m.slope[a], gb = m.slope[b];
+                SL = evr_side(true, qa.x, qa.y, qa.z, ca.x, ca.y, qa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp, m.dry);
+                SR = evr_side(false, qb.x, qb.y, qb.z, cb.x, cb.y, qb.w, gb.x, gb.y, d.z, d.w, n.x, n.y, dtp, m.dry);
+            }
+            zbL = ca.x;
+            zbR = cb.x;
+            bL = ca.y;
+            bR = cb.y;
+            phL = ca.z;
+            phR = cb.z;
         }
-        const int2 sl = ld(&m.eslot[e]);
-        const double hL = SL.z - ca.x, hR = SR.z - cb.x;
+        const double hL = SL.z - zbL, hR = SR.z - zbR;
         if (!((hL > m.h_min) || (hR > m.h_min))) {
             // flux not computed at this step: the slots keep their values and their adjoints
             ctb[sl.x] = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -275,7 +348,11 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig
             cts[sl.y] = make_double2(0.0, 0.0);
             return;
         }
-        const double2 cf = ld(&m.coef[e]);
+        if (!kStored) {
+            cf = ld(&m.coef[e]);
+            sa = ld_sig(&sig[sl.x]);
+            sb = ld_sig(&sig[sl.y]);
+        }
         const double nx = n.x, ny = n.y;
         EdgeFlux fb;
         fb.f1 = fb.f2 = fb.f3 = fb.sl = fb.sr = 0.0;
@@ -283,18 +360,18 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig
         {
             const double c = cf.x;
             const SlotFactors f{-c, -c * nx, +c * ny, +c * nx, -c * ny, -c * nx, +c * ny};
-            slot_rev(f, sig[sl.x], fb.f1, fb.f2, fb.f3, fb.sl);
+            slot_rev(f, sa, fb.f1, fb.f2, fb.f3, fb.sl);
         }
         {
             const double c = cf.y;
             const SlotFactors f{+c, +c * nx, -c * ny, +c * nx, +c * ny, +c * nx, +c * ny};
-            slot_rev(f, sig[sl.y], fb.f1, fb.f2, fb.f3, fb.sr);
+            slot_rev(f, sb, fb.f1, fb.f2, fb.f3, fb.sr);
         }
-        sig[sl.x] = make_double4(0.0, 0.0, 0.0, 0.0);
-        sig[sl.y] = make_double4(0.0, 0.0, 0.0, 0.0);
+        st_sig_zero(&sig[sl.x]);
+        st_sig_zero(&sig[sl.y]);
         SideBar Lb{0, 0, 0, 0, 0}, Rb{0, 0, 0, 0, 0};
         double zbLb = 0.0, zbRb = 0.0;
-        hllc_rev(kBlending, ca.y, cb.y, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min, fb, Lb, Rb, zbLb, zbRb);
+        hllc_rev(kBlending, bL, bR, phL, phR, zbL, zbR, SL, SR, m.h_min, m.phi_min, fb, Lb, Rb, zbLb, zbRb);
         // adjoints of the two Riemann states; k_cells_rev takes them back through the
         // reconstruction of each side
         ctb[sl.x] = make_double4(Lb.z, Lb.q, Lb.r, Lb.lm);
@@ -600,10 +677,10 @@ void launch_edges_rev_v(sw2d_handle* h, const DevMesh& m, double t, double dtp, 
     const unsigned n = (unsigned)(m.ni + m.nb);
     if (rs)
         k_edges_rev<kScheme, kBlending, B, M, true><<<(n + B - 1) / B, B, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t,
-                                                                                          dtp, rs);
+                                                                                          dtp, rs, a->eside);
     else
         k_edges_rev<kScheme, kBlending, B, M, false><<<(n + B - 1) / B, B, 0, h->stream>>>(m, a->sig, a->ctb, a->cts, t,
-                                                                                           dtp, rs);
+                                                                                           dtp, rs, nullptr);
 }
 
 template <int kScheme, bool kBlending>
@@ -684,6 +761,7 @@ int reverse_sweep(sw2d_handle* h)
     CK(cudaMemsetAsync(a->g_k1, 0, nc * sizeof(double), h->stream));
     CK(cudaMemsetAsync(a->g_k2, 0, nc * sizeof(double), h->stream));
     const unsigned gc = grid_for(nc);
+    if (a->seg_rs && h->ni) k_edge_sides<<<grid_for(h->ni), kBlock, 0, h->stream>>>(h->m, a->eside);
     int rc = SW2D_OK;
     if (h->adj_trace) {
         if (a->trace_steps != a->n_steps) {
@@ -797,13 +875,17 @@ int alloc_trajectory(sw2d_handle* h, int64_t n_steps, int64_t every)
     // reverse steps, when they fit in half of the free device memory (else rebuilt there)
     a->seg_slope = nullptr;
     a->seg_rs = nullptr;
+    a->eside = nullptr;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const size_t sl_b = h->p.scheme == SW2D_SCHEME_MUSCL_EVR ? (size_t)seg * nc * sizeof(double2) : 0;
         const size_t rs_b = (size_t)seg * h->ni * 5 * sizeof(double2);
         if (h->adj_store_states && sl_b + rs_b < free_b / 2) {
             if (sl_b && adj_alloc(h, L, seg * nc, &a->seg_slope)) a->seg_slope = nullptr;
-            if (h->ni && adj_alloc(h, L, seg * h->ni * 5, &a->seg_rs)) a->seg_rs = nullptr;
+            if (h->ni && (adj_alloc(h, L, seg * h->ni * 5, &a->seg_rs) || adj_alloc(h, L, 3 * h->ni, &a->eside))) {
+                a->seg_rs = nullptr;
+                a->eside = nullptr;
+            }
             h->err.clear();
         }
     }

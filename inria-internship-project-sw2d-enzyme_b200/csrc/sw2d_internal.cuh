@@ -130,8 +130,8 @@ struct DevMesh {
     const double* len;
     const double2* coef;     // {coefL, coefR}
     double2* flux;           // optional copy: 3 x double2 per edge {F1,F2},{F3,S2L},{S2R,-} (tests)
-    double2* rstate;         // optional: the two Riemann states per edge, 5 x double2 (the adjoint's
-                             // segment recompute keeps them for k_edges_rev)
+    double2* rstate;         // optional: the two Riemann states per edge, 5 planes of ni double2
+                             // (the adjoint's segment recompute keeps them for k_edges_rev)
     double* lmax;            // optional copy of lambda_max (tests)
     // boundary edges
     const int* bcell;
