@@ -468,25 +468,9 @@ struct UpdateParams {
     double h_min, v_max, fr_max, dt;
     double k1, k2, fcos, fsin;           // friction
     double hs, hk1, hk2, hcos, hsin;     // head loss
+    bool P_given = false;                // P = friction_power(h) of the friction stage is known
+    double P = 0.0;                      // (the forward recompute keeps it)
 };
-
-// friction_factor (sp_math.cuh) with P = exp(-4/3 log h) given: the same operations, hence the
-// same value, for a cell whose two directions share P
-SW2D_HD double friction_factor_p(int model, double k, double h, double un, double dt, double P)
-{
-    double factor = 1.0;
-    if (model == 1) {
-        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k / h * dt);
-        else factor = 0.0;
-    } else if (model == 2) {
-        if (h > kSmallReal) factor = sw2d_exp(-kGravity * un * k * k * P * dt);
-        else factor = 0.0;
-    } else {
-        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k * P * dt);
-        else factor = 0.0;
-    }
-    return factor;
-}
 
 // Reverse of friction_factor: f is the forward factor, P = exp(-4/3 log h) (Manning, Strickler)
 SW2D_HD void friction_factor_rev(int model, double k, double h, double un, double dt, double P, double f,
@@ -541,9 +525,9 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
             ul0 = u * p.fcos + v * p.fsin;
             vl0 = -u * p.fsin + v * p.fcos;
             un = sqrt(u * u + v * v);
-            if (p.friction != 1 && hh > kSmallReal) P = sw2d_exp(-4.0 / 3.0 * sw2d_log(hh));
+            if (p.friction != 1 && hh > kSmallReal) P = p.P_given ? p.P : friction_power(hh);
             f1 = friction_factor_p(p.friction, p.k1, hh, un, p.dt, P);
-            f2 = friction_factor_p(p.friction, p.k2, hh, un, p.dt, P);
+            f2 = (p.k2 == p.k1) ? f1 : friction_factor_p(p.friction, p.k2, hh, un, p.dt, P);
             const double ul = ul0 * f1, vl = vl0 * f2;
             qq = (ul * p.fcos - vl * p.fsin) * hh;
             rr = (ul * p.fsin + vl * p.fcos) * hh;

@@ -353,22 +353,33 @@ SW2D_HD unsigned boundary_flux(double bR, double phiR, double zbR, const SideSta
     return bad;
 }
 
+// h^(-4/3) of the Manning and Strickler factors, as the reference evaluates it: exp(-4/3 log h)
+SW2D_HD double friction_power(double h) { return sw2d_exp(-4.0 / 3.0 * sw2d_log(h)); }
+
 // swSource::frictionChezy1D / frictionManning1D / frictionStrickler1D
 // (models/common/swSourceFriction.cpp:7-79); model 1 chezy, 2 manning, 3 strickler.
-SW2D_HD double friction_factor(int model, double k, double h, double un, double dt)
+// friction_factor_p takes P = friction_power(h) (unused by Chezy), which the two directions of a
+// cell share: the same operations in the same order as the reference's expression.
+SW2D_HD double friction_factor_p(int model, double k, double h, double un, double dt, double P)
 {
     double factor = 1.0;
     if (model == 1) {
         if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k / h * dt);
         else factor = 0.0;
     } else if (model == 2) {
-        if (h > kSmallReal) factor = sw2d_exp(-kGravity * un * k * k * sw2d_exp(-4.0 / 3.0 * sw2d_log(h)) * dt);
+        if (h > kSmallReal) factor = sw2d_exp(-kGravity * un * k * k * P * dt);
         else factor = 0.0;
     } else {
-        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k * sw2d_exp(-4.0 / 3.0 * sw2d_log(h)) * dt);
+        if ((h > kSmallReal) && (k > kSmallReal)) factor = sw2d_exp(-kGravity * un / k / k * P * dt);
         else factor = 0.0;
     }
     return factor;
+}
+
+SW2D_HD double friction_factor(int model, double k, double h, double un, double dt)
+{
+    const double P = (model != 1 && h > kSmallReal) ? friction_power(h) : 0.0;
+    return friction_factor_p(model, k, h, un, dt, P);
 }
 
 }  // namespace sw2d

@@ -170,6 +170,12 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
     const int2 lr = ld(&m.lr[e]);
     const int a = lr.x, b = lr.y;
     const double2 n = ld(&m.nxy[e]);
+    // the edge's own tables, in flight with the cell gathers (else the slots and factors are
+    // loaded after the Riemann solve, which then waits for them)
+    const int2 sl = ld_now(&m.eslot[e]);
+    const double2 cf = ld_now(&m.coef[e]);
+    const double len_e = ld(&m.len[e]);
+    const double4 emc_e = (kScheme != SW2D_SCHEME_GODUNOV) ? ld(&m.emc[e]) : make_double4(0.0, 0.0, 0.0, 0.0);
     const double4 sa = L::in(&m.st[a]), sb = L::in(&m.st[b]);
     const double4 ca = ld(&m.cst[a]), cb = ld(&m.cst[b]);
     SideState SL, SR;
@@ -189,7 +195,7 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
         }
     } else {
         const double dtp = L::ctl(&m.ctrl->dt);
-        const double4 d = ld(&m.emc[e]);  // midpoint - centroid of L and R
+        const double4 d = emc_e;  // midpoint - centroid of L and R
         const double2 ga = L::in(&m.slope[a]), gb = L::in(&m.slope[b]);
         if (kDip) {
             SL = evr_side_dip(true, sa.x, sa.y, sa.z, ca.x, ca.y, xL, sa.w, ga.x, ga.y, d.x, d.y, n.x, n.y, dtp);
@@ -212,9 +218,8 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
         p[3 * ni] = make_double2(SR.q, SR.r);
         p[4 * ni] = make_double2(SR.lm, SR.lp);
     }
-    const double lw = lm * ld(&m.len[e]);
+    const double lw = lm * len_e;
     const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;
-    const int2 sl = ld(&m.eslot[e]);
     m.slot_w[sl.x] = wetL ? lw : 0.0;
     m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
     const double hL = SL.z - ca.x, hR = SR.z - cb.x;
@@ -231,7 +236,6 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
         }
         // factors of swSp::computeEdgeFactors (swSp.cpp:398-427) and the dt-free products of
         // hypComputeBalance (swSpHyp.cpp:237-262)
-        const double2 cf = ld(&m.coef[e]);
         const double nx = n.x, ny = n.y;
         {
             const double c = cf.x;
@@ -373,7 +377,7 @@ __device__ __forceinline__ void update_cell(const DevMesh& m, int c, double dt)
         const double4 mu = ld(&m.mu[c]);
         momentum_dissipation(mu.x, mu.y, mu.z, mu.w, s0.x, s0.y, s0.z, hh, qq, rr);
     }
-    if (kStoreB) m.bal[c] = make_double4(hh, qq, rr, 0.0);  // for the reverse sweep
+    const double hB = hh, qB = qq, rB = rr;  // the post-balance state, kept for the reverse sweep
     if (fabs(hh) < kSmallReal) hh = 0.;
     if (fabs(qq) < kSmallReal) qq = 0.;
     if (fabs(rr) < kSmallReal) rr = 0.;
@@ -385,7 +389,9 @@ __device__ __forceinline__ void update_cell(const DevMesh& m, int c, double dt)
         qq = 0.;
         rr = 0.;
     }
-    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr);
+    double P = 0.0;
+    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr, kStoreB ? &P : nullptr);
+    if (kStoreB) m.bal[c] = make_double4(hB, qB, rB, P);  // with the friction stage's h^(-4/3)
     // z = h + z_b of the new state, as the next step's reconstruction computes it
     // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
     m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));

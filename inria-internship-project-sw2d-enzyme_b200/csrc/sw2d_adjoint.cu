@@ -79,6 +79,7 @@ struct AdjointState {
     double* znb = nullptr;               // ncint: per-neighbour-entry z contributions
     double2* sgb = nullptr;              // nc: adjoint of each cell's limited slope
     int* mirror = nullptr;               // ncint: entry of the same edge in the neighbour's list
+    double4* sgeo = nullptr;             // ncint: {nx, ny, midpoint - centroid} of each entry's edge
     double* g_zb = nullptr;
     double* g_k1 = nullptr;
     double* g_k2 = nullptr;
@@ -166,6 +167,23 @@ __global__ void k_edge_sides(DevMesh m, double2* eside)
     eside[2 * ni + e] = make_double2(ca.z, cb.z);
 }
 
+// The slot adjoints, which k_update_rev accumulates and k_edges_rev resets, are loaded and
+// stored through volatile asms on the coherent path, in the order they stand (ld_now, in
+// sw2d_internal.cuh, covers the read-only tables).  Only {x, y, z} of a slot adjoint is used.
+__device__ __forceinline__ double4 ld_sig(const double4* p)
+{
+    double4 v;
+    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    asm volatile("ld.global.f64 %0, [%1+16];" : "=d"(v.z) : "l"(p));
+    v.w = 0.0;
+    return v;
+}
+__device__ __forceinline__ void st_sig(double4* p, double x, double y, double z)
+{
+    asm volatile("st.global.v2.f64 [%0], {%1, %2};\n\tst.global.f64 [%0+16], %3;" ::"l"(p), "d"(x), "d"(y), "d"(z));
+}
+__device__ __forceinline__ void st_sig_zero(double4* p) { st_sig(p, 0.0, 0.0, 0.0); }
+
 // Reverse of k_update for one step: lam holds the adjoint of the state after the step and
 // becomes the adjoint of the state before it (balance part); the slots' adjoints gain
 // dt * (adjoint of the post-balance state); friction-coefficient gradients accumulate.
@@ -209,6 +227,15 @@ __global__ void __launch_bounds__(kBlock) k_update_rev(DevMesh m, const double4*
     }
     const double4 B = bal[c];
     const double4 l = lam[c];
+    p.P_given = true;  // bal.w: h^(-4/3) of the recomputed step's friction stage
+    p.P = B.w;
+    // the adjoints of the cell's first kPre slots, in flight during the cell's reverse
+    constexpr int kPre = 4;
+    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
+    double4 s[kPre];
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (k0 + i < k1) s[i] = ld_sig(&sig[k0 + i]);
     double hb, qb, rb, k1b = 0.0, k2b = 0.0;
     update_cell_rev(p, B.x, B.y, B.z, l.x, l.y, l.z, hb, qb, rb, k1b, k2b);
     if (kFriction != SW2D_FRICTION_NONE) {
@@ -216,14 +243,13 @@ __global__ void __launch_bounds__(kBlock) k_update_rev(DevMesh m, const double4*
         gk2[c] += k2b;
     }
     lam[c] = make_double4(hb, qb, rb, 0.0);
-    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
     const double a = hb * dt, b = qb * dt, cc = rb * dt;
-    for (int k = k0; k < k1; k++) {
-        double4 s = sig[k];
-        s.x += a;
-        s.y += b;
-        s.z += cc;
-        sig[k] = s;
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (k0 + i < k1) st_sig(&sig[k0 + i], s[i].x + a, s[i].y + b, s[i].z + cc);
+    for (int k = k0 + kPre; k < k1; k++) {
+        const double4 t = ld_sig(&sig[k]);
+        st_sig(&sig[k], t.x + a, t.y + b, t.z + cc);
     }
 }
 
@@ -240,36 +266,6 @@ __device__ __forceinline__ void slot_rev(const SlotFactors& f, const double4& s,
     F2b += f.f2F2 * s.y + f.f3F2 * s.z;
     F3b += f.f2F3 * s.y + f.f3F3 * s.z;
     Sb += f.f2S2 * s.y + f.f3S2 * s.z;
-}
-
-// Loads issued where they stand: a volatile asm is neither sunk below the dry-edge test nor
-// reordered against the other volatile asms, so every load of an edge is in flight before the
-// first one is used.  ld_now reads data no kernel writes meanwhile; the slot adjoints, which
-// this kernel resets after reading, go through ld_sig / st_sig (coherent path).
-__device__ __forceinline__ double2 ld_now(const double2* p)
-{
-    double2 v;
-    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ int2 ld_now(const int2* p)
-{
-    int2 v;
-    asm volatile("ld.global.nc.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ double4 ld_sig(const double4* p)
-{
-    double4 v;
-    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
-    asm volatile("ld.global.f64 %0, [%1+16];" : "=d"(v.z) : "l"(p));
-    v.w = 0.0;
-    return v;
-}
-__device__ __forceinline__ void st_sig_zero(double4* p)
-{
-    asm volatile("st.global.v2.f64 [%0], {%1, %2};\n\tst.global.v2.f64 [%0+16], {%1, %2};" ::"l"(p), "d"(0.0),
-                 "d"(0.0));
 }
 
 // kStored: the two Riemann states of the step come from the segment's forward recompute
@@ -404,21 +400,90 @@ __global__ void __launch_bounds__(kB, kMinB) k_edges_rev(DevMesh m, double4* sig
     }
 }
 
+// The slot geometry of k_cells_rev: per entry k of the cells' neighbour lists (cint), the
+// normal of the entry's edge and the midpoint - centroid offset of the cell on that edge
+// {nx, ny, dx, dy}, so that a cell's loads all depend on its offsets alone
+__global__ void k_slot_geom(DevMesh m, double4* sgeo, int n)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
+    for (int k = e0; k < e1; k++) {
+        const int2 en = ld(&m.cint[k]);
+        const int e = en.x >> 1;
+        const double2 nn = ld(&m.nxy[e]);
+        const double4 d = ld(&m.emc[e]);
+        const bool left = (en.x & 1) == 0;
+        sgeo[k] = make_double4(nn.x, nn.y, left ? d.x : d.z, left ? d.y : d.w);
+    }
+}
+
+__device__ __forceinline__ double4 ld_now4(const double4* p)
+{
+    const double2 a = ld_now(reinterpret_cast<const double2*>(p)), b = ld_now(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ int ld_now_x(const int2* p)
+{
+    int v;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+// One internal slot of k_cells_rev: the reverse of the cell's reconstruction on that slot,
+// added to the cell's sums (skipped when the slot's adjoints are all zero)
+template <bool kMuscl>
+__device__ __forceinline__ void cell_slot_rev(const double4& a, const double2& b, int entry, const double4& geo,
+                                              const double4& s, const double4& cs, const double2& g, double dtp,
+                                              double& hb, double& qb, double& rb, double& zbb, double& sxb,
+                                              double& syb)
+{
+    if (a.x == 0.0 && a.y == 0.0 && a.z == 0.0 && a.w == 0.0 && b.x == 0.0 && b.y == 0.0) return;
+    const SideBar sb{a.x, a.y, a.z, a.w, b.x};
+    CellBar cb{0, 0, 0, 0, 0, 0, 0};
+    if (kMuscl) {
+        const bool left = (entry & 1) == 0;
+        evr_side_rev(left, s.x, s.y, s.z, cs.x, cs.y, s.w, g.x, g.y, geo.z, geo.w, geo.x, geo.y, dtp, sb, cb);
+    } else {
+        godunov_side_rev(s.x, s.y, s.z, cs.y, geo.x, geo.y, sb, cb);
+    }
+    // z_c = h + z_b of the cell
+    hb += cb.h + cb.zc;
+    qb += cb.q;
+    rb += cb.r;
+    zbb += cb.zb + b.y + cb.zc;
+    sxb += cb.sx;
+    syb += cb.sy;
+}
+
 // Ordered gather, over the slots of each cell in the reference's order: boundary slots hold
 // their final contributions; internal slots hold the adjoints of this cell's Riemann state,
 // taken back here through the cell's reconstruction (godunov_side / evr_side).  For MUSCL-EVR
-// the adjoint of the cell's limited slope goes to sgb for k_limiter_rev.
+// the adjoint of the cell's limited slope goes to sgb for k_limiter_rev.  The loads of the
+// first kPre internal slots are issued together, ahead of the boundary sums.
 template <int kScheme>
 __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, const double4* __restrict__ ctb,
                                                       const double2* __restrict__ cts, double* gzb, double2* sgb,
-                                                      double dtp)
+                                                      double dtp, const double4* __restrict__ sgeo)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
     constexpr bool kMuscl = kScheme == SW2D_SCHEME_MUSCL_EVR;
-    const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
-    const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
-    const int nbnd = (k1 - k0) - (e1 - e0);
+    constexpr int kPre = 3;
+    const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
+    const int k0 = o0.y, k1 = o1.y, e0 = o0.x, e1 = o1.x;
+    const int nint = e1 - e0, nbnd = (k1 - k0) - nint;
+    double4 A[kPre], G[kPre];
+    double2 Bv[kPre];
+    int En[kPre];
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (i < nint) {
+            A[i] = ld_now4(&ctb[k0 + nbnd + i]);
+            Bv[i] = ld_now(&cts[k0 + nbnd + i]);
+            En[i] = ld_now_x(&m.cint[e0 + i]);
+            G[i] = ld_now4(&sgeo[e0 + i]);
+        }
     double hb = 0.0, qb = 0.0, rb = 0.0, zbb = 0.0, sxb = 0.0, syb = 0.0;
     for (int k = k0; k < k0 + nbnd; k++) {
         const double4 v = ctb[k];
@@ -431,31 +496,13 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
     const double4 cs = ld(&m.cst[c]);
     double2 g = make_double2(0.0, 0.0);
     if (kMuscl) g = m.slope[c];
-    for (int i = 0; i < e1 - e0; i++) {
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (i < nint) cell_slot_rev<kMuscl>(A[i], Bv[i], En[i], G[i], s, cs, g, dtp, hb, qb, rb, zbb, sxb, syb);
+    for (int i = kPre; i < nint; i++) {
         const int k = k0 + nbnd + i;
-        const double4 a = ctb[k];
-        const double2 b = cts[k];
-        if (a.x == 0.0 && a.y == 0.0 && a.z == 0.0 && a.w == 0.0 && b.x == 0.0 && b.y == 0.0) continue;
-        const int2 en = ld(&m.cint[e0 + i]);
-        const int e = en.x >> 1;
-        const double2 n = ld(&m.nxy[e]);
-        const SideBar sb{a.x, a.y, a.z, a.w, b.x};
-        CellBar cb{0, 0, 0, 0, 0, 0, 0};
-        if (kMuscl) {
-            const bool left = (en.x & 1) == 0;
-            const double4 d = ld(&m.emc[e]);
-            evr_side_rev(left, s.x, s.y, s.z, cs.x, cs.y, s.w, g.x, g.y, left ? d.x : d.z, left ? d.y : d.w, n.x, n.y,
-                         dtp, sb, cb);
-        } else {
-            godunov_side_rev(s.x, s.y, s.z, cs.y, n.x, n.y, sb, cb);
-        }
-        // z_c = h + z_b of the cell
-        hb += cb.h + cb.zc;
-        qb += cb.q;
-        rb += cb.r;
-        zbb += cb.zb + b.y + cb.zc;
-        sxb += cb.sx;
-        syb += cb.sy;
+        cell_slot_rev<kMuscl>(ctb[k], cts[k], ld(&m.cint[e0 + i]).x, sgeo[e0 + i], s, cs, g, dtp, hb, qb, rb, zbb,
+                              sxb, syb);
     }
     if (kMuscl) sgb[c] = make_double2(sxb, syb);
     double4 l = lam[c];
@@ -522,13 +569,15 @@ int adjoint_fixed(sw2d_handle* h)
         (rc = adj_alloc(h, L, h->nc, &a->g_zb)) || (rc = adj_alloc(h, L, h->nc, &a->g_k1)) ||
         (rc = adj_alloc(h, L, h->nc, &a->g_k2)) || (rc = adj_alloc(h, L, 1, &a->ctrl_rev)) ||
         (rc = adj_alloc(h, L, kCostBlocks, &a->d_part)) ||
-        (rc = adj_alloc(h, L, h->nc, &a->stage)) || (rc = adj_alloc(h, L, 6, &a->d_nonfinite)))
+        (rc = adj_alloc(h, L, h->nc, &a->stage)) || (rc = adj_alloc(h, L, 6, &a->d_nonfinite)) ||
+        (rc = adj_alloc(h, L, a->ncint, &a->sgeo)))
         return rc;
     Ctrl cr{};
     cr.t = 0.0;
     cr.t_max = 1.0;
     CK(cudaMemcpyAsync(a->ctrl_rev, &cr, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
     if (h->nc > 0) k_mirror<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m.coff, h->m.cint, a->mirror, (int)h->nc);
+    if (h->nc > 0) k_slot_geom<<<grid_for(h->nc), kBlock, 0, h->stream>>>(h->m, a->sgeo, (int)h->nc);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     return SW2D_OK;
@@ -821,12 +870,12 @@ int reverse_sweep(sw2d_handle* h)
             const double dtp = j > 0 ? a->dt_seq[j - 1] : a->dt_before;
             if (muscl) {
                 k_cells_rev<SW2D_SCHEME_MUSCL_EVR><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
-                                                                                  a->sgb, dtp);
+                                                                                  a->sgb, dtp, a->sgeo);
                 k_limiter_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->sgb, a->lam, a->g_zb, a->znb);
                 k_nbr_rev<<<gc, kBlock, 0, h->stream>>>(mr, a->mirror, a->znb, a->lam, a->g_zb);
             } else {
                 k_cells_rev<SW2D_SCHEME_GODUNOV><<<gc, kBlock, 0, h->stream>>>(mr, a->lam, a->ctb, a->cts, a->g_zb,
-                                                                                a->sgb, dtp);
+                                                                                a->sgb, dtp, a->sgeo);
             }
             if (a->d_trace && j < a->trace_steps)
                 k_trace<<<gc, kBlock, 0, h->stream>>>(a->lam, (int)nc, a->d_trace + 4 * j);

@@ -120,7 +120,8 @@ struct DevMesh {
     Slot* slot;              // balance slots {a, b, c}
     double4* slot4;          // balance slots of the differentiated step {f1 F1, b, c, f1} (sw2d_assim.cu)
     double* slot_w;          // CFL contribution of the slot
-    double4* bal;            // post-balance state {h, q, r, -} (written only by the recording update)
+    double4* bal;            // post-balance state {h, q, r, P} with P = h^(-4/3) of the friction stage
+                             // (written only by the recording update)
     // internal edges
     const int2* lr;
     const int2* eslot;       // {slot of (L, e), slot of (R, e)}
@@ -187,6 +188,22 @@ __device__ __forceinline__ double4 ld(const double4* p)
     const double2* q = reinterpret_cast<const double2*>(p);
     const double2 a = __ldg(q), b = __ldg(q + 1);
     return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Loads issued where they stand: a volatile asm is neither sunk below a later branch nor
+// reordered against the other volatile asms, so a kernel can have all of an element's loads in
+// flight before it uses the first one.  For data no kernel writes meanwhile (non-coherent path).
+__device__ __forceinline__ double2 ld_now(const double2* p)
+{
+    double2 v;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int2 ld_now(const int2* p)
+{
+    int2 v;
+    asm volatile("ld.global.nc.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
 }
 
 __device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_max; }
@@ -325,7 +342,8 @@ void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m);
 // swSp.cpp:447-479; the DDP model applies the same formulas to thetaW and its momentum,
 // swDdpSourceFriction.cpp, swDdp.cpp:527-561).
 template <int kFriction, bool kHeadLoss>
-__device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt, double hh, double& qq, double& rr)
+__device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt, double hh, double& qq, double& rr,
+                                             double* P_out = nullptr)
 {
     const double hthr = smax(m.h_min, kSmallReal);
     // friction (swSpSourceFriction.cpp:39-171)
@@ -338,9 +356,12 @@ __device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt,
             double ul = u * ca + v * sa;
             double vl = -u * sa + v * ca;
             double un = sqrt(u * u + v * v);
-            // isotropic friction (equal coefficients): the same factor, computed once
-            double f1 = friction_factor(kFriction, fr.x, hh, un, dt);
-            double f2 = (fr.y == fr.x) ? f1 : friction_factor(kFriction, fr.y, hh, un, dt);
+            // h^(-4/3) once per cell; isotropic friction (equal coefficients): the same factor,
+            // computed once
+            const double P = (kFriction != SW2D_FRICTION_CHEZY && hh > kSmallReal) ? friction_power(hh) : 0.0;
+            if (P_out) *P_out = P;
+            double f1 = friction_factor_p(kFriction, fr.x, hh, un, dt, P);
+            double f2 = (fr.y == fr.x) ? f1 : friction_factor_p(kFriction, fr.y, hh, un, dt, P);
             ul *= f1;
             vl *= f2;
             qq = (ul * ca - vl * sa) * hh;
