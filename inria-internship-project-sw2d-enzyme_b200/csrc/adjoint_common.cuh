@@ -180,15 +180,28 @@ __global__ void __launch_bounds__(kBlock) k_limiter_rev(DevMesh m, const double2
 }
 
 
-// z contributions of the neighbours' slope limiters, gathered in the cell's entry order
+// z contributions of the neighbours' slope limiters, gathered in the cell's entry order (the
+// first kPre entries' loads in flight together)
 __global__ void __launch_bounds__(kBlock) k_nbr_rev(DevMesh m, const int* __restrict__ mirror,
                                                     const double* __restrict__ znb, double4* lam, double* gzb)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
+    constexpr int kPre = 4;
     const int e0 = ld(&m.coff[c].x), e1 = ld(&m.coff[c + 1].x);
+    int mk[kPre];
+    double z[kPre];
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (e0 + i < e1) mk[i] = ld_now(&mirror[e0 + i]);  // every internal edge has an entry on both sides
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (e0 + i < e1 && mk[i] >= 0) z[i] = ld_now(&znb[mk[i]]);
     double s = 0.0;
-    for (int k = e0; k < e1; k++) {
+#pragma unroll
+    for (int i = 0; i < kPre; i++)
+        if (e0 + i < e1 && mk[i] >= 0) s += z[i];
+    for (int k = e0 + kPre; k < e1; k++) {
         const int mk = ld(&mirror[k]);  // every internal edge has an entry on both sides
         if (mk >= 0) s += znb[mk];
     }

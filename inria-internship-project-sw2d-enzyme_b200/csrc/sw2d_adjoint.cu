@@ -423,12 +423,6 @@ __device__ __forceinline__ double4 ld_now4(const double4* p)
     const double2 a = ld_now(reinterpret_cast<const double2*>(p)), b = ld_now(reinterpret_cast<const double2*>(p) + 1);
     return make_double4(a.x, a.y, b.x, b.y);
 }
-__device__ __forceinline__ int ld_now_x(const int2* p)
-{
-    int v;
-    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
-    return v;
-}
 
 // One internal slot of k_cells_rev: the reverse of the cell's reconstruction on that slot,
 // added to the cell's sums (skipped when the slot's adjoints are all zero)
@@ -459,8 +453,9 @@ __device__ __forceinline__ void cell_slot_rev(const double4& a, const double2& b
 // Ordered gather, over the slots of each cell in the reference's order: boundary slots hold
 // their final contributions; internal slots hold the adjoints of this cell's Riemann state,
 // taken back here through the cell's reconstruction (godunov_side / evr_side).  For MUSCL-EVR
-// the adjoint of the cell's limited slope goes to sgb for k_limiter_rev.  The loads of the
-// first kPre internal slots are issued together, ahead of the boundary sums.
+// the adjoint of the cell's limited slope goes to sgb for k_limiter_rev.  The adjoints of the
+// first kPre internal slots are loaded together, ahead of the boundary sums; a slot's geometry
+// only when its adjoints are not all zero.
 template <int kScheme>
 __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, const double4* __restrict__ ctb,
                                                       const double2* __restrict__ cts, double* gzb, double2* sgb,
@@ -473,16 +468,13 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
     const int2 o0 = ld(&m.coff[c]), o1 = ld(&m.coff[c + 1]);
     const int k0 = o0.y, k1 = o1.y, e0 = o0.x, e1 = o1.x;
     const int nint = e1 - e0, nbnd = (k1 - k0) - nint;
-    double4 A[kPre], G[kPre];
+    double4 A[kPre];
     double2 Bv[kPre];
-    int En[kPre];
 #pragma unroll
     for (int i = 0; i < kPre; i++)
         if (i < nint) {
             A[i] = ld_now4(&ctb[k0 + nbnd + i]);
             Bv[i] = ld_now(&cts[k0 + nbnd + i]);
-            En[i] = ld_now_x(&m.cint[e0 + i]);
-            G[i] = ld_now4(&sgeo[e0 + i]);
         }
     double hb = 0.0, qb = 0.0, rb = 0.0, zbb = 0.0, sxb = 0.0, syb = 0.0;
     for (int k = k0; k < k0 + nbnd; k++) {
@@ -498,7 +490,12 @@ __global__ void __launch_bounds__(kBlock) k_cells_rev(DevMesh m, double4* lam, c
     if (kMuscl) g = m.slope[c];
 #pragma unroll
     for (int i = 0; i < kPre; i++)
-        if (i < nint) cell_slot_rev<kMuscl>(A[i], Bv[i], En[i], G[i], s, cs, g, dtp, hb, qb, rb, zbb, sxb, syb);
+        if (i < nint) {
+            const double4 a = A[i];
+            const double2 b = Bv[i];
+            if (a.x == 0.0 && a.y == 0.0 && a.z == 0.0 && a.w == 0.0 && b.x == 0.0 && b.y == 0.0) continue;
+            cell_slot_rev<kMuscl>(a, b, ld(&m.cint[e0 + i]).x, ld(&sgeo[e0 + i]), s, cs, g, dtp, hb, qb, rb, zbb, sxb, syb);
+        }
     for (int i = kPre; i < nint; i++) {
         const int k = k0 + nbnd + i;
         cell_slot_rev<kMuscl>(ctb[k], cts[k], ld(&m.cint[e0 + i]).x, sgeo[e0 + i], s, cs, g, dtp, hb, qb, rb, zbb,

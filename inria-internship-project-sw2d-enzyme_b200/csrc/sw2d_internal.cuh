@@ -206,6 +206,19 @@ __device__ __forceinline__ int2 ld_now(const int2* p)
     return v;
 }
 
+__device__ __forceinline__ int ld_now(const int* p)
+{
+    int v;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_now(const double* p)
+{
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
 __device__ __forceinline__ bool step_active(const Ctrl* c) { return c->t < c->t_max; }
 
 inline unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
