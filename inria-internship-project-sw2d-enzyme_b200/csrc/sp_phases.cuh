@@ -349,6 +349,11 @@ template <int kFriction, bool kHeadLoss, bool kStoreB, bool kDissip, class L>
 __device__ __forceinline__ void update_cell(const DevMesh& m, int c, double dt)
 {
     const double4 s0 = L::own(&m.st[c]);
+    // a cell wet at the start of the step loads its friction coefficients with its slots (one
+    // round trip less); dry cells, which mostly stay dry, leave them unread
+    const bool fr_early = kFriction != SW2D_FRICTION_NONE && s0.x > smax(m.h_min, kSmallReal);
+    double4 fr = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (fr_early) fr = ld(&m.fric[c]);
     double hh = s0.x, qq = s0.y, rr = s0.z;
     // hypComputeBalance (swSpHyp.cpp:214-273): h += (factor*F1)*dt, q += (...)*dt, r += (...)*dt
     // over the cell's slots, in the reference's order
@@ -390,7 +395,7 @@ __device__ __forceinline__ void update_cell(const DevMesh& m, int c, double dt)
         rr = 0.;
     }
     double P = 0.0;
-    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr, kStoreB ? &P : nullptr);
+    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr, kStoreB ? &P : nullptr, fr_early ? &fr : nullptr);
     if (kStoreB) m.bal[c] = make_double4(hB, qB, rB, P);  // with the friction stage's h^(-4/3)
     // z = h + z_b of the new state, as the next step's reconstruction computes it
     // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
