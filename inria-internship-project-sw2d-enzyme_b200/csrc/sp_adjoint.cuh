@@ -472,30 +472,31 @@ struct UpdateParams {
     double P = 0.0;                      // (the forward recompute keeps it)
 };
 
-// Reverse of friction_factor: f is the forward factor, P = exp(-4/3 log h) (Manning, Strickler)
+// Reverse of friction_factor: f is the forward factor, P = exp(-4/3 log h) (Manning, Strickler),
+// rh = 1 / h (the derivative terms multiply by it)
 SW2D_HD void friction_factor_rev(int model, double k, double h, double un, double dt, double P, double f,
-                                 double f_bar, double& k_bar, double& h_bar, double& un_bar)
+                                 double f_bar, double& k_bar, double& h_bar, double& un_bar, double rh)
 {
     if (model == 1) {
         if ((h > kSmallReal) && (k > kSmallReal)) {
             const double A_bar = f_bar * f * dt;
             un_bar += A_bar * (-kGravity / k / k / h);
             k_bar += A_bar * 2.0 * kGravity * un / (k * k * k) / h;
-            h_bar += A_bar * kGravity * un / k / k / (h * h);
+            h_bar += A_bar * kGravity * un / k / k * (1.0 / (h * h));
         }
     } else if (model == 2) {
         if (h > kSmallReal) {
             const double A_bar = f_bar * f * dt;
             un_bar += A_bar * (-kGravity * k * k * P);
             k_bar += A_bar * (-kGravity * un * 2.0 * k * P);
-            h_bar += A_bar * (-kGravity * un * k * k) * P * (-4.0 / 3.0) / h;
+            h_bar += A_bar * (-kGravity * un * k * k) * P * (-4.0 / 3.0) * rh;
         }
     } else {
         if ((h > kSmallReal) && (k > kSmallReal)) {
             const double A_bar = f_bar * f * dt;
             un_bar += A_bar * (-kGravity / k / k * P);
             k_bar += A_bar * 2.0 * kGravity * un / (k * k * k) * P;
-            h_bar += A_bar * (-kGravity * un / k / k) * P * (-4.0 / 3.0) / h;
+            h_bar += A_bar * (-kGravity * un / k / k) * P * (-4.0 / 3.0) * rh;
         }
     }
 }
@@ -634,18 +635,21 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
             double ul0_bar = ul_bar * f1, vl0_bar = vl_bar * f2;
             const double f1_bar = ul_bar * ul0, f2_bar = vl_bar * vl0;
             double un_bar = 0.0;
-            friction_factor_rev(p.friction, p.k1, h_f, un, p.dt, P, f1, f1_bar, k1b, h_bar, un_bar);
-            friction_factor_rev(p.friction, p.k2, h_f, un, p.dt, P, f2, f2_bar, k2b, h_bar, un_bar);
+            // the derivative terms multiply by the reciprocals of h and |u|, taken once
+            const double rh = 1.0 / h_f;
+            friction_factor_rev(p.friction, p.k1, h_f, un, p.dt, P, f1, f1_bar, k1b, h_bar, un_bar, rh);
+            friction_factor_rev(p.friction, p.k2, h_f, un, p.dt, P, f2, f2_bar, k2b, h_bar, un_bar, rh);
             double u_bar = ul0_bar * p.fcos - vl0_bar * p.fsin;
             double v_bar = ul0_bar * p.fsin + vl0_bar * p.fcos;
             if (un > 0.0) {
-                u_bar += un_bar * u / un;
-                v_bar += un_bar * v / un;
+                const double run = 1.0 / un;
+                u_bar += un_bar * u * run;
+                v_bar += un_bar * v * run;
             }
             // u = q / h, v = r / h
-            q_bar = u_bar / h_f;
-            r_bar = v_bar / h_f;
-            h_bar += -u_bar * u / h_f - v_bar * v / h_f;
+            q_bar = u_bar * rh;
+            r_bar = v_bar * rh;
+            h_bar += -u_bar * u * rh - v_bar * v * rh;
         } else {
             q_bar = 0.0;
             r_bar = 0.0;
