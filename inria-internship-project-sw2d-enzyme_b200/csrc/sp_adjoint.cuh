@@ -470,6 +470,8 @@ struct UpdateParams {
     double hs, hk1, hk2, hcos, hsin;     // head loss
     bool P_given = false;                // P = friction_power(h) of the friction stage is known
     double P = 0.0;                      // (the forward recompute keeps it)
+    bool cap_given = false;              // whether the velocity cap acted is known (cap_acted)
+    bool cap_acted = false;
 };
 
 // Reverse of friction_factor: f is the forward factor, P = exp(-4/3 log h) (Manning, Strickler),
@@ -569,7 +571,7 @@ SW2D_HD void update_cell_rev(const UpdateParams& p, double hB, double qB, double
     bool capped = false;
     double qn = 0, cc = 0, fact = 0;
     bool fact_from_v = false;
-    if (hh > p.h_min) {
+    if (hh > p.h_min && (!p.cap_given || p.cap_acted)) {  // the cap's test, unless known to be off
         qn = sqrt(qq * qq + rr * rr);
         cc = sqrt(kGravity * hh);
         const double Fr = qn / cc / hh;

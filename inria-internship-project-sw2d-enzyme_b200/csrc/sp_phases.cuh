@@ -220,8 +220,10 @@ __device__ __forceinline__ unsigned edge_internal(const DevMesh& m, int e)
     }
     const double lw = lm * len_e;
     const bool wetL = sa.x > m.h_min, wetR = sb.x > m.h_min;
-    m.slot_w[sl.x] = wetL ? lw : 0.0;
-    m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
+    if (m.slot_w) {
+        m.slot_w[sl.x] = wetL ? lw : 0.0;
+        m.slot_w[sl.y] = (wetL || wetR) ? lw : 0.0;
+    }
     const double hL = SL.z - ca.x, hR = SR.z - cb.x;
     if ((hL > m.h_min) || (hR > m.h_min)) {
         EdgeFlux f = kDip ? hllc_dip(kBlending, ca.y, cb.y, phiG, ca.z, cb.z, ca.x, cb.x, SL, SR, m.h_min, m.phi_min)
@@ -270,7 +272,7 @@ __device__ __forceinline__ unsigned edge_boundary(const DevMesh& m, int e)
     const double lm = (kScheme == SW2D_SCHEME_GODUNOV) ? smax(fabs(S.lp), fabs(S.lm)) : smax(fabs(S.lm), fabs(S.lp));
     if (m.lmaxb) m.lmaxb[e] = lm;
     const int sb = ld(&m.bslot[e]);
-    m.slot_w[sb] = (s.x > m.h_min) ? lm * g.z : 0.0;
+    if (m.slot_w) m.slot_w[sb] = (s.x > m.h_min) ? lm * g.z : 0.0;
     const int k = ld(&m.bbc[e]);
     const long long o0 = ld(&m.bcoff[k]), o1 = ld(&m.bcoff[k + 1]);
     const double v = bc_value(m.bctimes + o0, m.bcvals + o0, o1 - o0, L::ctl(&m.ctrl->t));
@@ -395,11 +397,14 @@ __device__ __forceinline__ void update_cell(const DevMesh& m, int c, double dt)
         rr = 0.;
     }
     double P = 0.0;
-    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr, kStoreB ? &P : nullptr, fr_early ? &fr : nullptr);
-    if (kStoreB) m.bal[c] = make_double4(hB, qB, rB, P);  // with the friction stage's h^(-4/3)
+    bool capped = false;
+    cell_sources<kFriction, kHeadLoss>(m, c, dt, hh, qq, rr, kStoreB ? &P : nullptr, fr_early ? &fr : nullptr,
+                                       kStoreB ? &capped : nullptr);
+    // with the friction stage's h^(-4/3) >= 0, its sign bit set where the velocity cap acted
+    if (kStoreB) m.bal[c] = make_double4(hB, qB, rB, capped ? -P : P);
     // z = h + z_b of the new state, as the next step's reconstruction computes it
     // (swSpHypMusclEvr.cpp:129, swSpHypGodunov.cpp:23)
-    m.st[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));
+    (m.st_out ? m.st_out : m.st)[c] = make_double4(hh, qq, rr, hh + ld(&m.zbv[c]));
 }
 
 }  // namespace sw2d

@@ -227,8 +227,12 @@ __global__ void __launch_bounds__(kBlock) k_update_rev(DevMesh m, const double4*
     }
     const double4 B = bal[c];
     const double4 l = lam[c];
-    p.P_given = true;  // bal.w: h^(-4/3) of the recomputed step's friction stage
-    p.P = B.w;
+    // bal.w: h^(-4/3) of the recomputed step's friction stage, its sign bit set where the
+    // velocity cap acted
+    p.P_given = true;
+    p.P = fabs(B.w);
+    p.cap_given = true;
+    p.cap_acted = signbit(B.w);
     // the adjoints of the cell's first kPre slots, in flight during the cell's reverse
     constexpr int kPre = 4;
     const int k0 = ld(&m.coff[c].y), k1 = ld(&m.coff[c + 1].y);
@@ -827,11 +831,15 @@ int reverse_sweep(sw2d_handle* h)
     for (int64_t s = a->n_ck - 1; s >= 0; s--) {
         const int64_t j0 = s * a->every, j1 = std::min(a->n_steps, j0 + a->every);
         if ((rc = ck_load(h, s))) return rc;
-        // recompute the segment, keeping each step's state and post-balance state
+        // recompute the segment, keeping each step's state and post-balance state: step j reads
+        // seg_st[j - j0] and writes seg_st[j + 1 - j0]; its dt is frozen, so the CFL
+        // contributions are not written
+        CK(cudaMemcpyAsync(a->seg_st, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
         for (int64_t j = j0; j < j1; j++) {
-            double4* stj = a->seg_st + (j - j0) * nc;
-            CK(cudaMemcpyAsync(stj, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
             DevMesh mj = h->m;
+            mj.st = a->seg_st + (j - j0) * nc;
+            mj.st_out = a->seg_st + (j + 1 - j0) * nc;
+            mj.slot_w = nullptr;
             mj.bal = a->seg_bal + (j - j0) * nc;
             if (a->seg_slope) mj.slope = a->seg_slope + (j - j0) * nc;
             if (a->seg_rs) mj.rstate = a->seg_rs + (j - j0) * 5 * h->ni;
@@ -840,10 +848,8 @@ int reverse_sweep(sw2d_handle* h)
             k_frozen_dt<<<1, 1, 0, h->stream>>>(h->ctrl, a->d_dt_seq, a->base_steps);
             launch_update_on(h, mj, true);
             const int k = obs_index(a, j + 1);
-            if (k >= 0) cost_at(h, k, h->m.st);
+            if (k >= 0) cost_at(h, k, mj.st_out);
         }
-        CK(cudaMemcpyAsync(a->seg_st + (j1 - j0) * nc, h->m.st, nc * sizeof(double4), cudaMemcpyDeviceToDevice,
-                           h->stream));
         // reverse steps
         for (int64_t j = j1 - 1; j >= j0; j--) {
             const int k = obs_index(a, j + 1);

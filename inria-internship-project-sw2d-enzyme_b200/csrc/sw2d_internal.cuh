@@ -107,6 +107,8 @@ struct DevMesh {
     int nc, ni, nb;
     // cells
     double4* st;             // {h, q, r, z}
+    double4* st_out;         // optional: where the cell update writes the new state (else st, in
+                             // place; the adjoint's recompute writes each step into its segment)
     const double4* cst;      // {z_b, boussinesq, phi, area}
     const double2* cxy;      // centroid
     double2* slope;          // MUSCL slopes
@@ -119,9 +121,11 @@ struct DevMesh {
     const int2* cint;        // {edge*2 + side, neighbour} (MUSCL slopes)
     Slot* slot;              // balance slots {a, b, c}
     double4* slot4;          // balance slots of the differentiated step {f1 F1, b, c, f1} (sw2d_assim.cu)
-    double* slot_w;          // CFL contribution of the slot
-    double4* bal;            // post-balance state {h, q, r, P} with P = h^(-4/3) of the friction stage
-                             // (written only by the recording update)
+    double* slot_w;          // CFL contribution of the slot (null: not written, for steps whose
+                             // dt is frozen)
+    double4* bal;            // post-balance state {h, q, r, ±P} with P = h^(-4/3) of the friction
+                             // stage, negative where the velocity cap acted (written only by the
+                             // recording update)
     // internal edges
     const int2* lr;
     const int2* eslot;       // {slot of (L, e), slot of (R, e)}
@@ -356,7 +360,8 @@ void launch_cfl_ddp_on(sw2d_handle* h, const DevMesh& m);
 // swDdpSourceFriction.cpp, swDdp.cpp:527-561).
 template <int kFriction, bool kHeadLoss>
 __device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt, double hh, double& qq, double& rr,
-                                             double* P_out = nullptr, const double4* fr_pre = nullptr)
+                                             double* P_out = nullptr, const double4* fr_pre = nullptr,
+                                             bool* capped_out = nullptr)
 {
     const double hthr = smax(m.h_min, kSmallReal);
     // friction (swSpSourceFriction.cpp:39-171); fr_pre: the cell's coefficients, when the caller
@@ -414,6 +419,7 @@ __device__ __forceinline__ void cell_sources(const DevMesh& m, int c, double dt,
         double Fr = qn / cc / hh;
         double fact = smax(qn / (hh * m.v_max), Fr / m.fr_max);
         if (fact > 1.0) {
+            if (capped_out) *capped_out = true;
             qq = qq / fact;
             rr = rr / fact;
         }
