@@ -285,12 +285,19 @@ class SpE:
         self.folder = folder
         self.n = model.n
         c = config
-        model.assim_configure(phi_transform=c.phi_transform, lambda_tanh=c.lambda_tanh,
-                              windowed=c.windowed_assimilation, window_duration=c.assimilation_window_duration,
-                              window_steps=c.assimilation_window_steps, n_windows=max(1, c.n_assimilation_windows),
-                              t_state_assimilation=c.t_state_assimilation, cost_normalize=c.cost_normalize,
-                              mask_wall_gradient=c.mask_wall_gradient)
+        self._conf = dict(phi_transform=c.phi_transform, lambda_tanh=c.lambda_tanh,
+                          windowed=c.windowed_assimilation, window_duration=c.assimilation_window_duration,
+                          window_steps=c.assimilation_window_steps, n_windows=max(1, c.n_assimilation_windows),
+                          t_state_assimilation=c.t_state_assimilation, cost_normalize=c.cost_normalize,
+                          mask_wall_gradient=c.mask_wall_gradient)
+        model.assim_configure(**self._conf)
         self.diag: Dict[str, object] = {}
+
+    def set_forced_first_segment(self, seg: int) -> None:
+        """forced_first_seg_ of the reference's L-BFGS-B driver (assim/swSpE_minimize.cpp:881-903):
+        while it is >= 0 every gradient's window starts at that segment; -1 lets each gradient cut
+        its window at its own truncation point again."""
+        self.model.assim_configure(**self._conf, forced_first_segment=int(seg))
 
     @classmethod
     def from_folder(cls, folder: str, device: int = 0, load_obs: bool = True) -> "SpE":
@@ -624,11 +631,18 @@ def free_cells(spe: SpE, phi_start) -> np.ndarray:
 
 
 def run_minimization(spe: SpE, phi_start, max_it: Optional[int] = None, alpha_reg: Optional[float] = None,
-                     descent_dir: Optional[str] = None, free=None, phi_ref=None) -> Dict[str, object]:
+                     descent_dir: Optional[str] = None, free=None, phi_ref=None,
+                     freeze_window: bool = False) -> Dict[str, object]:
     """swSpE::run_minimization (assim/swSpE_minimize.cpp:582-1073) with minimize_algo "lbfgsb"
     (scipy's L-BFGS-B on the box [phi_lower_bound, phi_upper_bound]) or "gd" (projected gradient
     descent with Armijo backtracking: c1 = 1e-4, shrink 0.5, grow 4, 40 backtracks).  Returns
-    {"phi", "J_final", "J_init", "n_grad", "history"}."""
+    {"phi", "J_final", "J_init", "n_grad", "history"}.
+
+    freeze_window (L-BFGS-B): the reference's probe evaluation at the start point, whose
+    truncation segment then stays the first segment of every gradient's window for the whole
+    solve (swSpE_minimize.cpp:881-903), J_final being the solver's value on that window.  Off by
+    default: on sp_toce with this gradient the frozen window stops the descent at J = 2.836
+    (-8.7 %), against 1.924 (-38 %) with each gradient's own window."""
     cfg = spe.cfg
     max_it = cfg.max_it if max_it is None else max_it
     alpha = cfg.alpha_reg if alpha_reg is None else alpha_reg
@@ -653,9 +667,28 @@ def run_minimization(spe: SpE, phi_start, max_it: Optional[int] = None, alpha_re
         opts = {"maxiter": max_it}
         if algo == "lbfgsb":
             opts.update(maxcor=int(cfg.lbfgsb_m), maxls=int(cfg.lbfgsb_max_linesearch), gtol=float(cfg.lbfgsb_epsilon))
-        res = minimize(fg, theta, jac=True, method="L-BFGS-B" if algo == "lbfgsb" else "BFGS", bounds=bounds,
-                       options=opts)
+        frozen = False
+        if algo == "lbfgsb" and freeze_window:
+            # the reference's probe (swSpE_minimize.cpp:881-892): one evaluation at the start point
+            # fixes the segment where the adjoint's window is cut, and the window stays there for
+            # the whole solve, so that every line-search trial computes J over the same window
+            # (a window that moves with theta makes J jump between trials and the line search fail)
+            fg(theta)
+            spe.set_forced_first_segment(max(0, int(spe.diag.get("truncation_segment", -1)) + 1))
+            frozen = True
+        try:
+            res = minimize(fg, theta, jac=True, method="L-BFGS-B" if algo == "lbfgsb" else "BFGS", bounds=bounds,
+                           options=opts)
+        finally:
+            if frozen:
+                spe.set_forced_first_segment(-1)
         theta = res.x
+        if frozen:
+            # J_final is the solver's value, on the frozen window (swSpE_minimize.cpp:906-909)
+            prob.close()
+            phi = spe.phi_correct(prob._map_theta(theta))
+            return {"phi": phi, "J_final": float(res.fun), "J_init": prob.J_init, "n_grad": prob.grad_calls,
+                    "history": history}
     elif algo == "gd":
         project = cfg.phi_transform in ("none", "clamp")
         c1, shrink, grow, max_bt = 1e-4, 0.5, 4.0, 40

@@ -115,6 +115,36 @@ def test_porosity_problem_gradient(transform):
     assert abs(prob.func(theta) - J) < 1e-12
 
 
+def test_lbfgsb_probe_freezes_the_truncation_window():
+    """run_minimization with L-BFGS-B and freeze_window (assim/swSpE_minimize.cpp:881-909): one probe evaluation at
+    the start point, whose truncation segment + 1 becomes every gradient's first segment for the
+    whole solve and is released after it; the probe and the solver's first evaluation are the same
+    point (the reference's descent log opens with two equal rows); J_final is the solver's value."""
+    pkg = load_pkg()
+    spe = _FakeSpE(pkg, 0, "none")
+    cfg = spe.cfg
+    cfg.alpha_l1 = cfg.alpha_spatial = cfg.alpha_phi_ref = 0.0
+    cfg.minimize_algo, cfg.max_it = "lbfgsb", 20
+    frozen = []
+    spe.set_forced_first_segment = frozen.append
+    exact = spe.get_spatial_gradient_checkpointed
+
+    def gradient(m, stride=None):
+        g = exact(m, stride)
+        spe.diag["truncation_segment"] = 6 if not frozen else 40   # the probe's truncation: segment 6
+        return g
+
+    spe.get_spatial_gradient_checkpointed = gradient
+    res = pkg.porosity.run_minimization(spe, np.full(spe.n, 0.8), freeze_window=True)
+    assert frozen == [7, -1]
+    assert res["history"][0] == res["history"][1]
+    assert res["J_final"] <= 1e-3 * res["J_init"]
+    assert res["n_grad"] == len(res["history"])
+    frozen.clear()
+    res = pkg.porosity.run_minimization(spe, np.full(spe.n, 0.8))   # the default: each gradient's own window
+    assert frozen == [] and res["J_final"] <= 1e-3 * res["J_init"]
+
+
 def test_free_cells_zone_map(tmp_path):
     """porosity_free_zone_map (assim/swSpE_minimize.cpp:648-668): of the cells the dry mask leaves
     free (here all), only those whose zone value is below 0.5; an unreadable map leaves the set
